@@ -1,0 +1,316 @@
+"""ctypes mirror of include/efl.h and a thin handle wrapper.
+
+`load()` opens the in-tree libefl_b200.so and fails loudly when it is
+missing or unusable: there is no CPU fallback behind this package.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+PKG_DIR = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG_DIR, "libefl_b200.so")
+
+MAX_SOLIDS = 256
+MAX_FLUID_SOURCE = 16
+
+# efl_status
+OK, ERR_INVALID_ARGUMENT, ERR_CUDA, ERR_OUT_OF_MEMORY, NOT_CONVERGED, ERR_TOO_MANY, \
+    ERR_UNSUPPORTED_SHAPE, ERR_STATE, ERR_NO_DEVICE = range(9)
+STATUS_NAMES = {0: "EFL_OK", 1: "EFL_ERR_INVALID_ARGUMENT", 2: "EFL_ERR_CUDA", 3: "EFL_ERR_OUT_OF_MEMORY",
+                4: "EFL_NOT_CONVERGED", 5: "EFL_ERR_TOO_MANY", 6: "EFL_ERR_UNSUPPORTED_SHAPE",
+                7: "EFL_ERR_STATE", 8: "EFL_ERR_NO_DEVICE"}
+
+PROJECTION_JACOBI, PROJECTION_GAUSS_SEIDEL, PROJECTION_MULTIGRID = 0, 1, 2
+REINIT_JUMP_FLOODING, REINIT_FAST_ITERATIVE = 0, 1
+SHAPE_CIRCLE, SHAPE_RECTANGLE, SHAPE_CAPSULE, SHAPE_TRIANGLE = 0, 1, 2, 4
+SOURCE_CIRCLE, SOURCE_AABB = 0, 1
+SOURCE_MODE_SOURCE, SOURCE_MODE_SINK = 0, 1
+
+# efl_field
+(FIELD_U, FIELD_V, FIELD_U1, FIELD_V1, FIELD_U_SOLID, FIELD_V_SOLID, FIELD_LEVELSET_AIR,
+ FIELD_LEVELSET_AIR1, FIELD_LEVELSET_SOLID, FIELD_SOLID_ID, FIELD_AREA_FRACTION, FIELD_DIVERGENCE,
+ FIELD_PRESSURE, FIELD_GRAD_LEVELSET, FIELD_JFA_SEEDS, FIELD_FIM_LABELS, FIELD_U_VALID, FIELD_V_VALID,
+ FIELD_AREA_FRACTION_U, FIELD_AREA_FRACTION_V) = range(20)
+FIELD_DTYPES = {FIELD_SOLID_ID: np.int32, FIELD_U_VALID: np.int32, FIELD_V_VALID: np.int32,
+                FIELD_FIM_LABELS: np.uint32}
+
+# efl_stage
+(STAGE_INIT, STAGE_UPDATE_SOLID, STAGE_AREA_FRACTION, STAGE_ADVECT_VELOCITY, STAGE_APPLY_FORCES,
+ STAGE_DIVERGENCE, STAGE_PROJECTION, STAGE_SOLVE_VELOCITY, STAGE_EXTRAPOLATE, STAGE_ADVECT_LEVELSET,
+ STAGE_FLUID_SOURCE, STAGE_REINITIALIZE, STAGE_LEVELSET_GRADIENT, STAGE_SOLID_FORCES) = range(14)
+
+
+class Projection(C.Structure):
+    _fields_ = [("method", C.c_int32), ("gs_iterations", C.c_uint32), ("sor_weight", C.c_float),
+                ("mg_pre", C.c_uint32), ("mg_post", C.c_uint32), ("mg_coarsest", C.c_uint32),
+                ("mg_levels", C.c_uint32), ("tolerance", C.c_float), ("max_iterations", C.c_uint32),
+                ("check_interval", C.c_uint32)]
+
+
+class Reinit(C.Structure):
+    _fields_ = [("method", C.c_int32), ("fim_iterations", C.c_uint32)]
+
+
+class Config(C.Structure):
+    _fields_ = [("nx", C.c_uint32), ("ny", C.c_uint32), ("length_unit", C.c_float), ("rho", C.c_float),
+                ("gravity", C.c_float * 2), ("transform", C.c_float * 16), ("projection", Projection),
+                ("reinit", Reinit), ("device", C.c_int32)]
+
+
+class SolidObstacle(C.Structure):
+    _fields_ = [("entity_id", C.c_uint32), ("shape", C.c_uint32), ("values", C.c_float * 6),
+                ("transform", C.c_float * 16), ("inverse_transform", C.c_float * 16),
+                ("linear_velocity", C.c_float * 2), ("angular_velocity", C.c_float), ("_pad", C.c_float)]
+
+
+class Force(C.Structure):
+    _fields_ = [("force", C.c_float * 2), ("position", C.c_float * 2)]
+
+
+class Source(C.Structure):
+    _fields_ = [("center", C.c_float * 2), ("data", C.c_float * 2), ("velocity", C.c_float * 2),
+                ("shape", C.c_uint32), ("mode", C.c_uint32)]
+
+
+class SolidForce(C.Structure):
+    _fields_ = [("force", C.c_float * 2), ("torque", C.c_float), ("_pad", C.c_float)]
+
+
+class StepStats(C.Structure):
+    _fields_ = [("initialized_only", C.c_int32), ("pressure_iterations", C.c_uint32), ("converged", C.c_int32),
+                ("_pad", C.c_int32), ("residual", C.c_double), ("residual_initial", C.c_double)]
+
+    def as_dict(self) -> dict:
+        return {"initialized_only": self.initialized_only, "pressure_iterations": self.pressure_iterations,
+                "converged": self.converged, "residual": self.residual,
+                "residual_initial": self.residual_initial}
+
+
+assert C.sizeof(SolidObstacle) == 176
+assert C.sizeof(Force) == 16
+assert C.sizeof(Source) == 32
+assert C.sizeof(SolidForce) == 16
+
+# Exported symbols of include/efl.h: name -> (restype, argtypes); "X" stands for the handle.
+SIGNATURES = {
+    "abi_version": (C.c_int32, []),
+    "default_config": (C.c_int, [C.c_uint32, C.c_uint32, C.POINTER(Config)]),
+    "create": (C.c_int, [C.POINTER(Config), C.POINTER(C.c_void_p)]),
+    "destroy": (C.c_int, ["X"]),
+    "last_error": (C.c_char_p, ["X"]),
+    "reset": (C.c_int, ["X"]),
+    "set_projection": (C.c_int, ["X", C.POINTER(Projection)]),
+    "set_reinit": (C.c_int, ["X", C.POINTER(Reinit)]),
+    "set_transform": (C.c_int, ["X", C.POINTER(C.c_float)]),
+    "set_obstacles": (C.c_int, ["X", C.POINTER(SolidObstacle), C.c_uint32]),
+    "set_local_forces": (C.c_int, ["X", C.POINTER(Force), C.c_uint32]),
+    "set_sources": (C.c_int, ["X", C.POINTER(Source), C.c_uint32, C.c_int32]),
+    "step": (C.c_int, ["X", C.c_float, C.POINTER(StepStats)]),
+    "run_stage": (C.c_int, ["X", C.c_int32, C.c_float, C.POINTER(StepStats)]),
+    "read_solid_forces": (C.c_int, ["X", C.POINTER(SolidForce)]),
+    "read_force_bins": (C.c_int, ["X", C.POINTER(C.c_int32)]),
+    "field_shape": (C.c_int, ["X", C.c_int32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
+                              C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
+    "get_field": (C.c_int, ["X", C.c_int32, C.c_void_p, C.c_size_t]),
+    "set_field": (C.c_int, ["X", C.c_int32, C.c_void_p, C.c_size_t]),
+    "field_device_ptr": (C.c_int, ["X", C.c_int32, C.POINTER(C.c_void_p), C.POINTER(C.c_size_t)]),
+    "stream": (C.c_int, ["X", C.POINTER(C.c_void_p)]),
+    "synchronize": (C.c_int, ["X"]),
+    "residual": (C.c_int, ["X", C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "fluid_volume": (C.c_int, ["X", C.POINTER(C.c_uint64)]),
+}
+# Functions of efl.h that the oracle restatement does not mirror.
+PRODUCT_ONLY = {"abi_version", "default_config", "field_device_ptr", "stream", "synchronize"}
+
+
+class EflError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+class Api:
+    """A bound function table for one library and symbol prefix ("efl_" or "eflo_")."""
+
+    def __init__(self, lib: C.CDLL, prefix: str):
+        self.lib = lib
+        self.prefix = prefix
+        self.fns = {}
+        for name, (res, args) in SIGNATURES.items():
+            sym = prefix + name
+            if not hasattr(lib, sym):
+                if prefix != "efl_" and name in PRODUCT_ONLY:
+                    continue
+                raise OSError(f"{sym} missing from {lib._name}")
+            fn = getattr(lib, sym)
+            fn.restype = res
+            fn.argtypes = [C.c_void_p if a == "X" else a for a in args]
+            self.fns[name] = fn
+
+    def __getattr__(self, name):
+        try:
+            return self.fns[name]
+        except KeyError as e:
+            raise AttributeError(name) from e
+
+
+_API: Optional[Api] = None
+
+
+def load(path: str = LIB_PATH) -> Api:
+    """Opens libefl_b200.so. Raises if it is missing: no fallback exists."""
+    global _API
+    if _API is not None and path == LIB_PATH:
+        return _API
+    if not os.path.exists(path):
+        raise ImportError(
+            f"{path} is missing: build it with `python -m bevy_eulerian_fluid_b200.build` "
+            "(the CUDA extension is required; there is no CPU fallback)")
+    api = Api(C.CDLL(path), "efl_")
+    if path == LIB_PATH:
+        _API = api
+    return api
+
+
+def default_config(nx: int, ny: int) -> Config:
+    """Reference defaults (matches efl_default_config), without loading the library."""
+    c = Config()
+    c.nx, c.ny = nx, ny
+    c.length_unit, c.rho = 1.0, 1.0
+    c.gravity[0], c.gravity[1] = 0.0, 9.8
+    for i in range(4):
+        c.transform[i * 5] = 1.0
+    p = c.projection
+    p.method, p.gs_iterations, p.sor_weight = PROJECTION_GAUSS_SEIDEL, 20, 1.9
+    p.mg_pre, p.mg_post, p.mg_coarsest, p.mg_levels = 2, 2, 3, 0
+    p.tolerance, p.max_iterations, p.check_interval = 0.0, 20000, 16
+    c.reinit.method, c.reinit.fim_iterations = REINIT_FAST_ITERATIVE, 10
+    c.device = 0
+    return c
+
+
+class Sim:
+    """One simulation handle on a bound Api (the CUDA library or the oracle)."""
+
+    def __init__(self, api: Api, cfg: Config):
+        self.api = api
+        self.cfg = cfg
+        h = C.c_void_p()
+        st = api.create(C.byref(cfg), C.byref(h))
+        if st != OK:
+            raise EflError(st, (api.last_error(None) or b"").decode())
+        self.h = h
+        self.nx, self.ny = cfg.nx, cfg.ny
+
+    # -- lifetime
+    def close(self):
+        if getattr(self, "h", None):
+            self.api.destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, st: int, allow=(OK,)) -> int:
+        if st not in allow:
+            raise EflError(st, (self.api.last_error(self.h) or b"").decode())
+        return st
+
+    # -- inputs
+    def reset(self):
+        self._check(self.api.reset(self.h))
+
+    def set_projection(self, p: Projection):
+        self._check(self.api.set_projection(self.h, C.byref(p)))
+        self.cfg.projection = p
+
+    def set_reinit(self, r: Reinit):
+        self._check(self.api.set_reinit(self.h, C.byref(r)))
+        self.cfg.reinit = r
+
+    def set_transform(self, m16):
+        arr = (C.c_float * 16)(*[float(v) for v in m16])
+        self._check(self.api.set_transform(self.h, arr))
+
+    def set_obstacles(self, obstacles):
+        arr = (SolidObstacle * max(1, len(obstacles)))(*obstacles)
+        self._check(self.api.set_obstacles(self.h, arr, len(obstacles)))
+
+    def set_local_forces(self, forces):
+        arr = (Force * max(1, len(forces)))(*forces)
+        self._check(self.api.set_local_forces(self.h, arr, len(forces)))
+
+    def set_sources(self, sources, oneshot: bool):
+        arr = (Source * max(1, len(sources)))(*sources)
+        self._check(self.api.set_sources(self.h, arr, len(sources), 1 if oneshot else 0))
+
+    # -- stepping
+    def step(self, dt: float, allow_not_converged: bool = True) -> StepStats:
+        st = StepStats()
+        allow = (OK, NOT_CONVERGED) if allow_not_converged else (OK,)
+        self._check(self.api.step(self.h, dt, C.byref(st)), allow)
+        return st
+
+    def run_stage(self, stage: int, dt: float = 0.0) -> StepStats:
+        st = StepStats()
+        self._check(self.api.run_stage(self.h, stage, dt, C.byref(st)), (OK, NOT_CONVERGED))
+        return st
+
+    # -- outputs
+    def field_shape(self, field: int):
+        w, h, ch, eb = C.c_uint32(), C.c_uint32(), C.c_uint32(), C.c_uint32()
+        self._check(self.api.field_shape(self.h, field, C.byref(w), C.byref(h), C.byref(ch), C.byref(eb)))
+        return w.value, h.value, ch.value
+
+    def get(self, field: int) -> np.ndarray:
+        w, h, ch = self.field_shape(field)
+        dt = FIELD_DTYPES.get(field, np.float32)
+        shape = (h, w) if ch == 1 else (h, w, ch)
+        out = np.empty(shape, dtype=dt)
+        self._check(self.api.get_field(self.h, field, out.ctypes.data_as(C.c_void_p), out.nbytes))
+        return out
+
+    def set(self, field: int, arr: np.ndarray):
+        w, h, ch = self.field_shape(field)
+        dt = FIELD_DTYPES.get(field, np.float32)
+        a = np.ascontiguousarray(arr, dtype=dt)
+        want = (h, w) if ch == 1 else (h, w, ch)
+        if a.shape != want:
+            raise ValueError(f"field {field}: expected shape {want}, got {a.shape}")
+        self._check(self.api.set_field(self.h, field, a.ctypes.data_as(C.c_void_p), a.nbytes))
+
+    def solid_forces(self) -> np.ndarray:
+        arr = (SolidForce * MAX_SOLIDS)()
+        self._check(self.api.read_solid_forces(self.h, arr))
+        return np.frombuffer(arr, dtype=np.float32).reshape(MAX_SOLIDS, 4)[:, :3].copy()
+
+    def force_bins(self) -> np.ndarray:
+        arr = (C.c_int32 * (3 * MAX_SOLIDS))()
+        self._check(self.api.read_force_bins(self.h, arr))
+        return np.frombuffer(arr, dtype=np.int32).reshape(3, MAX_SOLIDS).copy()
+
+    def residual(self):
+        rel, nr, nb = C.c_double(), C.c_double(), C.c_double()
+        self._check(self.api.residual(self.h, C.byref(rel), C.byref(nr), C.byref(nb)))
+        return rel.value, nr.value, nb.value
+
+    def fluid_volume(self) -> int:
+        c = C.c_uint64()
+        self._check(self.api.fluid_volume(self.h, C.byref(c)))
+        return c.value
+
+    def synchronize(self):
+        self._check(self.api.synchronize(self.h))

@@ -1,0 +1,916 @@
+// efl_sim.cu — host orchestration and C ABI of libefl_b200.so.
+//
+// One efl_sim is one fluid entity of the reference plugin: its textures
+// (setup_components.rs:38-328), its per-frame compute pass
+// (EulerFluidNode::run, render_node.rs:193-476) and its force read-back
+// (fluid_to_solid.rs:180-209).  All device work of a simulation is issued on
+// the simulation's own CUDA stream; nothing here falls back to the CPU.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/efl.h"
+#include "efl_kernels.cuh"
+#include "efl_solver.cuh"
+
+using namespace efl;
+
+namespace {
+
+std::string g_last_error;
+
+inline int round_up(int v, int m) { return (v + m - 1) / m * m; }
+inline dim3 grid2d(int w, int h, dim3 b) { return dim3((w + b.x - 1) / b.x, (h + b.y - 1) / b.y); }
+const dim3 kBlock(32, 8);
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+}  // namespace
+
+struct efl_sim {
+    efl_config cfg{};
+    int nx = 0, ny = 0, P = 0;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    int status = 0;  // 0: Reset/Uninitialized, 1: Initialized (fluid_status.rs:15-21)
+    Uniform U{};
+
+    std::vector<DevBuf> bufs;
+    // fields (see efl_kernels.cuh for the layout)
+    PF u0, u1, v0, v1, us, vs, ls_s, div, p0, p1, ls0, ls1, fu, fv, phiT, r0;
+    PI sid, uvi, uvo, vvi, vvo;
+    PU lab0, lab, labT, upd;
+    P2 grad, seeds[2], srcvel;
+    int seeds_final = 0;
+    std::vector<Level> mg;      // reference fixed-count solve (f32 iterate)
+    std::vector<Level64> mg64;  // tolerance-driven solve (f64 iterate), same geometry planes
+
+    efl_solid_obstacle* d_obs = nullptr;
+    int n_obs = 0;
+    efl_force* d_forces = nullptr;
+    int n_forces = 0, cap_forces = 0;
+    std::vector<efl_source> src_once, src_cont;
+    int* d_bins = nullptr;
+    efl_solid_force* d_forces_out = nullptr;
+    double2* d_partials = nullptr;
+    int n_partials = 0;
+    double* d_norms = nullptr;
+    double* h_norms = nullptr;  // pinned
+    unsigned long long* d_count = nullptr;
+    SolverWorkspace solver;
+
+    Dom dom() const { return Dom{nx, ny}; }
+};
+
+namespace {
+
+efl_status set_err(efl_sim* s, efl_status st, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if (s) s->err = buf;
+    else g_last_error = buf;
+    return st;
+}
+
+#define CU(call)                                                                                          \
+    do {                                                                                                  \
+        cudaError_t e_ = (call);                                                                          \
+        if (e_ != cudaSuccess)                                                                            \
+            return set_err(s, e_ == cudaErrorMemoryAllocation ? EFL_ERR_OUT_OF_MEMORY : EFL_ERR_CUDA,      \
+                           "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__);   \
+    } while (0)
+
+#define LAUNCH_CHECK()                                                                                    \
+    do {                                                                                                  \
+        cudaError_t e_ = cudaGetLastError();                                                              \
+        if (e_ != cudaSuccess)                                                                            \
+            return set_err(s, EFL_ERR_CUDA, "kernel launch failed: %s (%s:%d)", cudaGetErrorString(e_),   \
+                           __FILE__, __LINE__);                                                           \
+    } while (0)
+
+template <class T>
+efl_status alloc_plane(efl_sim* s, Plane<T>& pl, int w, int h, int pitch, int rows) {
+    DevBuf b;
+    b.bytes = (size_t)pitch * rows * sizeof(T);
+    CU(cudaMalloc(&b.p, b.bytes));
+    CU(cudaMemsetAsync(b.p, 0, b.bytes, s->stream));
+    s->bufs.push_back(b);
+    pl.p = (T*)b.p;
+    pl.w = w;
+    pl.h = h;
+    pl.P = pitch;
+    return EFL_OK;
+}
+template <class T>
+efl_status alloc_raw(efl_sim* s, T*& p, size_t count) {
+    DevBuf b;
+    b.bytes = count * sizeof(T);
+    CU(cudaMalloc(&b.p, b.bytes));
+    CU(cudaMemsetAsync(b.p, 0, b.bytes, s->stream));
+    s->bufs.push_back(b);
+    p = (T*)b.p;
+    return EFL_OK;
+}
+
+#define TRY(x)                                  \
+    do {                                        \
+        efl_status st_ = (x);                   \
+        if (st_ != EFL_OK) return st_;          \
+    } while (0)
+
+int mg_num_levels(const efl_config& c) {
+    if (c.projection.mg_levels > 0) return (int)c.projection.mg_levels;
+    int n = (int)std::log2((float)std::min(c.nx, c.ny)) - 2;  // multi_grid.rs:95-97
+    return std::max(1, n);
+}
+
+efl_status alloc_mg(efl_sim* s) {
+    int L = mg_num_levels(s->cfg);
+    // Coarse levels live in s->bufs like every other buffer; they are only
+    // rebuilt when the level count changes (efl_set_projection), and the
+    // replaced ones are released with the simulation.
+    s->mg.assign(L, Level{});
+    s->mg64.assign(L, Level64{});
+    int w = s->nx, h = s->ny;
+    for (int i = 0; i < L; ++i) {
+        Level& l = s->mg[i];
+        Level64& d = s->mg64[i];
+        l.nx = d.nx = w;
+        l.ny = d.ny = h;
+        int pitch = round_up(w + 1, 32);
+        if (i == 0) {
+            l.x = s->p0;
+            l.b = s->div;
+            l.ls = s->ls0;
+            l.fu = s->fu;
+            l.fv = s->fv;
+            l.r = s->r0;
+        } else {
+            TRY(alloc_plane(s, l.x, w, h, pitch, h + 1));
+            TRY(alloc_plane(s, l.b, w, h, pitch, h + 1));
+            TRY(alloc_plane(s, l.ls, w, h, pitch, h + 1));
+            TRY(alloc_plane(s, l.fu, w + 1, h, pitch, h + 1));
+            TRY(alloc_plane(s, l.fv, w, h + 1, pitch, h + 1));
+            TRY(alloc_plane(s, l.r, w, h, pitch, h + 1));
+        }
+        d.ls = l.ls;
+        d.fu = l.fu;
+        d.fv = l.fv;
+        TRY(alloc_plane(s, d.x, w, h, pitch, h + 1));
+        TRY(alloc_plane(s, d.b, w, h, pitch, h + 1));
+        TRY(alloc_plane(s, d.r, w, h, pitch, h + 1));
+        w /= 2;
+        h /= 2;
+    }
+    return EFL_OK;
+}
+
+efl_status validate_cfg(const efl_config* c) {
+    if (!c) return set_err(nullptr, EFL_ERR_INVALID_ARGUMENT, "null config");
+    if (!(c->length_unit > 0.0f))
+        return set_err(nullptr, EFL_ERR_INVALID_ARGUMENT, "length_unit must be positive value.");
+    if (c->nx < 16 || c->ny < 16 || c->nx % 8 || c->ny % 8)
+        return set_err(nullptr, EFL_ERR_INVALID_ARGUMENT, "grid size must be a multiple of 8 and at least 16 (got %ux%u)",
+                       c->nx, c->ny);
+    if (c->nx > 32768 || c->ny > 32768) return set_err(nullptr, EFL_ERR_INVALID_ARGUMENT, "grid size too large");
+    if (c->projection.method < 0 || c->projection.method > 2)
+        return set_err(nullptr, EFL_ERR_INVALID_ARGUMENT, "unknown projection method %d", c->projection.method);
+    if (c->reinit.method < 0 || c->reinit.method > 1)
+        return set_err(nullptr, EFL_ERR_INVALID_ARGUMENT, "unknown reinitialize method %d", c->reinit.method);
+    return EFL_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Stages (render_node.rs:219-466)
+
+efl_status st_init(efl_sim* s) {  // render_node.rs:219-277
+    Dom d = s->dom();
+    k_init_center<<<grid2d(d.nx, d.ny, kBlock), kBlock, 0, s->stream>>>(s->ls0, s->ls1, s->grad, d);
+    k_init_edge<<<grid2d(d.nx + 1, d.ny, kBlock), kBlock, 0, s->stream>>>(s->u0, s->u1, s->v0, s->v1, d);
+    LAUNCH_CHECK();
+    return EFL_OK;
+}
+
+efl_status st_fluid_source(efl_sim* s, const std::vector<efl_source>& src) {  // update_fluid_source.wgsl
+    Dom d = s->dom();
+    Sources S;
+    std::memset(&S, 0, sizeof(S));
+    S.n = (int)src.size();
+    for (int i = 0; i < S.n; ++i) S.s[i] = src[i];
+    k_fluid_source_cells<<<grid2d(d.nx, d.ny, kBlock), kBlock, 0, s->stream>>>(s->ls1, s->upd, s->srcvel, S, d);
+    k_fluid_source_faces<<<grid2d(d.nx + 1, d.ny + 1, kBlock), kBlock, 0, s->stream>>>(s->u0, s->v0, s->upd,
+                                                                                       s->srcvel, d);
+    LAUNCH_CHECK();
+    return EFL_OK;
+}
+
+std::vector<int> jfa_steps(int nx, int ny) {  // jump_flooding.rs:201-209
+    int mp = (int)std::floor(std::log2((float)std::max(nx, ny)) - 1.0f);
+    std::vector<int> st;
+    uint32_t step = 1u << (mp + 1);
+    for (int k = 0; k < mp + 1; ++k) {
+        step /= 2;
+        st.push_back((int)step);
+    }
+    return st;
+}
+
+efl_status st_reinit(efl_sim* s) {  // reinitialize_levelset.rs:162-243
+    Dom d = s->dom();
+    dim3 g = grid2d(d.nx, d.ny, kBlock);
+    if (s->cfg.reinit.method == EFL_REINIT_JUMP_FLOODING) {
+        k_jfa_init<<<g, kBlock, 0, s->stream>>>(s->ls1, s->seeds[0], d);
+        int src = 0, dst = 1;
+        for (int step : jfa_steps(d.nx, d.ny)) {
+            k_jfa_iterate<<<g, kBlock, 0, s->stream>>>(s->seeds[src], s->seeds[dst], step, d);
+            std::swap(src, dst);
+        }
+        s->seeds_final = src;
+        k_jfa_sdf<<<g, kBlock, 0, s->stream>>>(s->seeds[src], s->ls1, s->ls0, d);
+    } else {
+        k_fim_init<<<g, kBlock, 0, s->stream>>>(s->ls1, s->ls0, s->lab0, d);
+        k_fim_active<<<g, kBlock, 0, s->stream>>>(s->lab0, s->lab, d);
+        for (uint32_t k = 0; k < s->cfg.reinit.fim_iterations; ++k) {
+            k_fim_phase_a<<<g, kBlock, 0, s->stream>>>(s->ls0, s->lab, s->phiT, s->labT, d);
+            k_fim_phase_b<<<g, kBlock, 0, s->stream>>>(s->phiT, s->labT, s->ls0, s->lab, d);
+        }
+    }
+    LAUNCH_CHECK();
+    return EFL_OK;
+}
+
+efl_status run_init(efl_sim* s) {
+    TRY(st_init(s));
+    TRY(st_fluid_source(s, s->src_once));
+    TRY(st_reinit(s));
+    return EFL_OK;
+}
+
+efl_status st_update_solid(efl_sim* s) {
+    Dom d = s->dom();
+    k_update_solid<<<grid2d(d.nx, d.ny, kBlock), kBlock, 0, s->stream>>>(s->us, s->vs, s->ls_s, s->sid, s->d_obs,
+                                                                       s->n_obs, s->U, d);
+    LAUNCH_CHECK();
+    return EFL_OK;
+}
+efl_status st_area_fraction(efl_sim* s) {
+    Dom d = s->dom();
+    k_area_fraction<<<grid2d(d.nx, d.ny, kBlock), kBlock, 0, s->stream>>>(s->ls_s, s->fu, s->fv, d);
+    LAUNCH_CHECK();
+    return EFL_OK;
+}
+efl_status st_advect(efl_sim* s) {
+    Dom d = s->dom();
+    k_advect_u<<<grid2d(d.nx + 1, d.ny, kBlock), kBlock, 0, s->stream>>>(s->u0, s->v0, s->u1, s->U.dt, d);
+    k_advect_v<<<grid2d(d.nx, d.ny + 1, kBlock), kBlock, 0, s->stream>>>(s->u0, s->v0, s->v1, s->U.dt, d);
+    LAUNCH_CHECK();
+    return EFL_OK;
+}
+efl_status st_apply_forces(efl_sim* s) {
+    Dom d = s->dom();
+    k_apply_forces<0><<<grid2d(d.nx + 1, d.ny, kBlock), kBlock, 0, s->stream>>>(s->u1, s->ls0, s->fu, s->d_forces,
+                                                                              s->n_forces, s->U, d);
+    k_apply_forces<1><<<grid2d(d.nx, d.ny + 1, kBlock), kBlock, 0, s->stream>>>(s->v1, s->ls0, s->fv, s->d_forces,
+                                                                               s->n_forces, s->U, d);
+    LAUNCH_CHECK();
+    return EFL_OK;
+}
+efl_status st_divergence(efl_sim* s) {
+    Dom d = s->dom();
+    k_divergence<<<grid2d(d.nx, d.ny, kBlock), kBlock, 0, s->stream>>>(s->u1, s->v1, s->us, s->vs, s->fu, s->fv,
+                                                                     s->div, s->U.dx, d);
+    LAUNCH_CHECK();
+    return EFL_OK;
+}
+
+// ||b - A x||^2 and ||b||^2 at level 0 into d_norms (async).
+template <class T>
+efl_status launch_norms(efl_sim* s, const LevelT<T>& L0) {
+    k_residual_norm<T><<<s->n_partials, NORM_THREADS, 0, s->stream>>>(L0, s->U.dt, s->U.rho, s->U.dx,
+                                                                      s->d_partials);
+    k_norm_finalize<<<1, 32, 0, s->stream>>>(s->d_partials, s->n_partials, s->d_norms);
+    LAUNCH_CHECK();
+    return EFL_OK;
+}
+efl_status read_norms(efl_sim* s, double* R, double* B) {
+    CU(cudaMemcpyAsync(s->h_norms, s->d_norms, 2 * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    CU(cudaStreamSynchronize(s->stream));
+    *R = s->h_norms[0];
+    *B = s->h_norms[1];
+    return EFL_OK;
+}
+double rel_from(double R, double B) {
+    if (B > 0.0) return std::sqrt(R) / std::sqrt(B);
+    return R > 0.0 ? INFINITY : 0.0;
+}
+template <class T>
+efl_status relative_residual(efl_sim* s, const LevelT<T>& L0, double* rel) {
+    TRY(launch_norms(s, L0));
+    double R, B;
+    TRY(read_norms(s, &R, &B));
+    *rel = rel_from(R, B);
+    return EFL_OK;
+}
+
+template <class T>
+efl_status gs_iterations(efl_sim* s, const LevelT<T>& L, float weight, float res_scale, uint32_t n) {
+    float dxs = res_scale * s->U.dx;  // gauss_seidel.wgsl:57
+    dim3 g = grid2d((L.nx + 1) / 2, L.ny, kBlock);
+    for (uint32_t k = 0; k < n; ++k) {
+        k_gs_color<T><<<g, kBlock, 0, s->stream>>>(L, dxs, s->U.rho, s->U.dt, weight, 1);
+        k_gs_color<T><<<g, kBlock, 0, s->stream>>>(L, dxs, s->U.rho, s->U.dt, weight, 0);
+    }
+    LAUNCH_CHECK();
+    return EFL_OK;
+}
+
+// multi_grid.rs:390-475 (smoother weight 1.0, resolution_scale 2^i: multi_grid.rs:268-270)
+template <class T>
+efl_status v_cycle(efl_sim* s, std::vector<LevelT<T>>& mg, size_t i) {
+    const efl_projection& P = s->cfg.projection;
+    const LevelT<T>& L = mg[i];
+    float scale = (float)(1u << i);
+    if (i == mg.size() - 1) return gs_iterations(s, L, 1.0f, scale, P.mg_coarsest);
+    TRY(gs_iterations(s, L, 1.0f, scale, P.mg_pre));
+    const LevelT<T>& C = mg[i + 1];
+    k_residual<T><<<grid2d(L.nx, L.ny, kBlock), kBlock, 0, s->stream>>>(L, s->U.dt, s->U.rho, scale * s->U.dx);
+    k_restriction<T><<<grid2d(C.nx, C.ny, kBlock), kBlock, 0, s->stream>>>(L, C);
+    LAUNCH_CHECK();
+    TRY(v_cycle(s, mg, i + 1));
+    k_prolongation<T><<<grid2d(C.nx, C.ny, kBlock), kBlock, 0, s->stream>>>(L, C);
+    LAUNCH_CHECK();
+    return gs_iterations(s, L, 1.0f, scale, P.mg_post);
+}
+
+// projection.rs:89-164.  tolerance > 0 (an extension) solves to
+// ||b - A p|| / ||b|| <= tolerance with an FP64 iterate: an f32 pressure
+// cannot represent a solution that accurate when hydrostatic pressure
+// dominates.  p0 receives the f32 rounding of the converged iterate.
+efl_status st_projection(efl_sim* s, efl_step_stats* st) {
+    const efl_projection& P = s->cfg.projection;
+    Dom d = s->dom();
+    uint32_t iters = 0;
+    int conv = 1;
+    double r0 = -1.0, r1 = -1.0;
+    if (P.method == EFL_PROJECTION_JACOBI) {
+        dim3 g = grid2d(d.nx, d.ny, kBlock);
+        for (int it = 0; it < 50; ++it) {  // projection.rs:135-143
+            k_jacobi<<<g, kBlock, 0, s->stream>>>(s->p0, s->p1, s->ls0, s->fu, s->fv, s->div, s->U, d);
+            k_jacobi<<<g, kBlock, 0, s->stream>>>(s->p1, s->p0, s->ls0, s->fu, s->fv, s->div, s->U, d);
+        }
+        LAUNCH_CHECK();
+        iters = 50;
+    } else if (P.tolerance <= 0.0f) {
+        if (P.method == EFL_PROJECTION_GAUSS_SEIDEL) {
+            TRY(solve_gs_fixed(s->solver, s->mg[0], s->U, P.sor_weight, P.gs_iterations, s->stream));
+            LAUNCH_CHECK();
+            iters = P.gs_iterations;
+        } else {
+            TRY(v_cycle(s, s->mg, 0));
+            iters = 1;
+        }
+    } else {
+        const Level64& L = s->mg64[0];
+        dim3 g = grid2d(d.nx, d.ny, kBlock);
+        k_widen<<<g, kBlock, 0, s->stream>>>(s->p0, s->div, L.x, L.b);
+        LAUNCH_CHECK();
+        double r;
+        TRY(relative_residual(s, L, &r));
+        r0 = r;
+        if (P.method == EFL_PROJECTION_GAUSS_SEIDEL) {
+            uint32_t chk = std::max<uint32_t>(1, P.check_interval);
+            while (!(r <= (double)P.tolerance) && iters < P.max_iterations) {
+                uint32_t n = std::min(chk, P.max_iterations - iters);
+                TRY(gs_iterations(s, L, P.sor_weight, 1.0f, n));
+                iters += n;
+                TRY(relative_residual(s, L, &r));
+            }
+        } else {
+            while (!(r <= (double)P.tolerance) && iters < P.max_iterations) {
+                TRY(v_cycle(s, s->mg64, 0));
+                ++iters;
+                TRY(relative_residual(s, L, &r));
+            }
+        }
+        r1 = r;
+        conv = r <= (double)P.tolerance;
+        k_narrow<<<g, kBlock, 0, s->stream>>>(L.x, s->p0);
+        LAUNCH_CHECK();
+    }
+    if (st) {
+        st->pressure_iterations = iters;
+        st->converged = conv;
+        st->residual = r1;
+        st->residual_initial = r0;
+    }
+    return conv ? EFL_OK : EFL_NOT_CONVERGED;
+}
+
+efl_status st_solve_velocity(efl_sim* s) {
+    Dom d = s->dom();
+    k_solve_velocity<0><<<grid2d(d.nx + 1, d.ny, kBlock), kBlock, 0, s->stream>>>(s->u0, s->u1, s->us, s->p0,
+                                                                                s->ls0, s->fu, s->U, d);
+    k_solve_velocity<1><<<grid2d(d.nx, d.ny + 1, kBlock), kBlock, 0, s->stream>>>(s->v0, s->v1, s->vs, s->p0,
+                                                                                 s->ls0, s->fv, s->U, d);
+    LAUNCH_CHECK();
+    return EFL_OK;
+}
+efl_status st_extrapolate(efl_sim* s) {  // render_node.rs:540-608
+    Dom d = s->dom();
+    dim3 gu = grid2d(d.nx + 1, d.ny, kBlock), gv = grid2d(d.nx, d.ny + 1, kBlock);
+    int xrows = (d.ny / 64) * 64, ycols = (d.nx / 64) * 64;
+    k_init_valid<0><<<gu, kBlock, 0, s->stream>>>(s->uvi, s->ls0, d);
+    k_init_valid<1><<<gv, kBlock, 0, s->stream>>>(s->vvi, s->ls0, d);
+    for (int k = 0; k < 10 / 2; ++k) {
+        k_extrapolate<<<gu, kBlock, 0, s->stream>>>(s->u0, s->uvi, s->uvo, d.nx + 1, xrows);
+        k_extrapolate<<<gu, kBlock, 0, s->stream>>>(s->u0, s->uvo, s->uvi, d.nx + 1, xrows);
+        k_extrapolate<<<gv, kBlock, 0, s->stream>>>(s->v0, s->vvi, s->vvo, ycols, d.ny + 1);
+        k_extrapolate<<<gv, kBlock, 0, s->stream>>>(s->v0, s->vvo, s->vvi, ycols, d.ny + 1);
+    }
+    LAUNCH_CHECK();
+    return EFL_OK;
+}
+efl_status st_advect_levelset(efl_sim* s) {
+    Dom d = s->dom();
+    k_advect_levelset<<<grid2d(d.nx, d.ny, kBlock), kBlock, 0, s->stream>>>(s->u0, s->v0, s->ls0, s->ls1, s->U.dt, d);
+    LAUNCH_CHECK();
+    return EFL_OK;
+}
+efl_status st_gradient(efl_sim* s) {
+    Dom d = s->dom();
+    k_gradient<<<grid2d(d.nx, d.ny, kBlock), kBlock, 0, s->stream>>>(s->ls0, s->grad, d);
+    LAUNCH_CHECK();
+    return EFL_OK;
+}
+efl_status st_solid_forces(efl_sim* s) {  // render_node.rs:610-641; bins zeroed per frame (fluid_to_solid.rs:211-229)
+    Dom d = s->dom();
+    CU(cudaMemsetAsync(s->d_bins, 0, 3 * EFL_MAX_SOLIDS * sizeof(int), s->stream));
+    k_solid_forces<<<grid2d(d.nx, d.ny, kBlock), kBlock, 0, s->stream>>>(s->fu, s->fv, s->sid, s->p0, s->d_obs,
+                                                                       s->n_obs, s->U, d, s->d_bins);
+    k_accumulate_forces<<<1, EFL_MAX_SOLIDS, 0, s->stream>>>(s->d_bins, s->d_forces_out);
+    LAUNCH_CHECK();
+    return EFL_OK;
+}
+
+efl_status run_stage(efl_sim* s, int stage, efl_step_stats* st) {
+    switch (stage) {
+        case EFL_STAGE_INIT: TRY(run_init(s)); s->status = 1; return EFL_OK;
+        case EFL_STAGE_UPDATE_SOLID: return st_update_solid(s);
+        case EFL_STAGE_AREA_FRACTION: return st_area_fraction(s);
+        case EFL_STAGE_ADVECT_VELOCITY: return st_advect(s);
+        case EFL_STAGE_APPLY_FORCES: return st_apply_forces(s);
+        case EFL_STAGE_DIVERGENCE: return st_divergence(s);
+        case EFL_STAGE_PROJECTION: return st_projection(s, st);
+        case EFL_STAGE_SOLVE_VELOCITY: return st_solve_velocity(s);
+        case EFL_STAGE_EXTRAPOLATE: return st_extrapolate(s);
+        case EFL_STAGE_ADVECT_LEVELSET: return st_advect_levelset(s);
+        case EFL_STAGE_FLUID_SOURCE: return st_fluid_source(s, s->src_cont);
+        case EFL_STAGE_REINITIALIZE: return st_reinit(s);
+        case EFL_STAGE_LEVELSET_GRADIENT: return st_gradient(s);
+        case EFL_STAGE_SOLID_FORCES: return st_solid_forces(s);
+        default: return set_err(s, EFL_ERR_INVALID_ARGUMENT, "unknown stage %d", stage);
+    }
+}
+
+void init_stats(efl_step_stats* st) {
+    if (!st) return;
+    std::memset(st, 0, sizeof(*st));
+    st->residual = -1.0;
+    st->residual_initial = -1.0;
+    st->converged = 1;
+}
+
+struct FieldDesc {
+    void* base;
+    int w, h, ch, P;  // P in elements of ch*4 bytes
+};
+bool field_desc(const efl_sim* s, int f, FieldDesc* o) {
+    auto pf = [&](const PF& p) { *o = FieldDesc{p.p, p.w, p.h, 1, p.P}; };
+    auto pi = [&](const PI& p) { *o = FieldDesc{p.p, p.w, p.h, 1, p.P}; };
+    auto pu = [&](const PU& p) { *o = FieldDesc{p.p, p.w, p.h, 1, p.P}; };
+    auto p2 = [&](const P2& p) { *o = FieldDesc{p.p, p.w, p.h, 2, p.P}; };
+    switch (f) {
+        case EFL_FIELD_U: pf(s->u0); return true;
+        case EFL_FIELD_V: pf(s->v0); return true;
+        case EFL_FIELD_U1: pf(s->u1); return true;
+        case EFL_FIELD_V1: pf(s->v1); return true;
+        case EFL_FIELD_U_SOLID: pf(s->us); return true;
+        case EFL_FIELD_V_SOLID: pf(s->vs); return true;
+        case EFL_FIELD_LEVELSET_AIR: pf(s->ls0); return true;
+        case EFL_FIELD_LEVELSET_AIR1: pf(s->ls1); return true;
+        case EFL_FIELD_LEVELSET_SOLID: pf(s->ls_s); return true;
+        case EFL_FIELD_SOLID_ID: pi(s->sid); return true;
+        case EFL_FIELD_DIVERGENCE: pf(s->div); return true;
+        case EFL_FIELD_PRESSURE: pf(s->p0); return true;
+        case EFL_FIELD_GRAD_LEVELSET: p2(s->grad); return true;
+        case EFL_FIELD_JFA_SEEDS: p2(s->seeds[s->seeds_final]); return true;
+        case EFL_FIELD_FIM_LABELS: pu(s->lab); return true;
+        case EFL_FIELD_U_VALID: pi(s->uvi); return true;
+        case EFL_FIELD_V_VALID: pi(s->vvi); return true;
+        case EFL_FIELD_AREA_FRACTION_U: pf(s->fu); return true;
+        case EFL_FIELD_AREA_FRACTION_V: pf(s->fv); return true;
+        default: return false;
+    }
+}
+
+efl_status copy_field_out(efl_sim* s, const FieldDesc& fd, void* dst) {
+    size_t row = (size_t)fd.w * fd.ch * 4;
+    CU(cudaMemcpy2DAsync(dst, row, fd.base, (size_t)fd.P * fd.ch * 4, row, fd.h, cudaMemcpyDeviceToHost, s->stream));
+    CU(cudaStreamSynchronize(s->stream));
+    return EFL_OK;
+}
+efl_status copy_field_in(efl_sim* s, const FieldDesc& fd, const void* src) {
+    size_t row = (size_t)fd.w * fd.ch * 4;
+    CU(cudaMemcpy2DAsync(fd.base, (size_t)fd.P * fd.ch * 4, src, row, row, fd.h, cudaMemcpyHostToDevice, s->stream));
+    CU(cudaStreamSynchronize(s->stream));
+    return EFL_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t efl_abi_version(void) { return EFL_ABI_VERSION; }
+
+efl_status efl_default_config(uint32_t nx, uint32_t ny, efl_config* c) {
+    if (!c) return set_err(nullptr, EFL_ERR_INVALID_ARGUMENT, "null config");
+    std::memset(c, 0, sizeof(*c));
+    c->nx = nx;
+    c->ny = ny;
+    c->length_unit = 1.0f;
+    c->rho = 1.0f;
+    c->gravity[0] = 0.0f;
+    c->gravity[1] = 9.8f;
+    for (int i = 0; i < 4; ++i) c->transform[i * 5] = 1.0f;
+    c->projection.method = EFL_PROJECTION_GAUSS_SEIDEL;
+    c->projection.gs_iterations = 20;
+    c->projection.sor_weight = 1.9f;
+    c->projection.mg_pre = 2;
+    c->projection.mg_post = 2;
+    c->projection.mg_coarsest = 3;
+    c->projection.mg_levels = 0;
+    c->projection.tolerance = 0.0f;
+    c->projection.max_iterations = 20000;
+    c->projection.check_interval = 16;
+    c->reinit.method = EFL_REINIT_FAST_ITERATIVE;
+    c->reinit.fim_iterations = 10;
+    c->device = 0;
+    return EFL_OK;
+}
+
+efl_status efl_create(const efl_config* cfg, efl_sim** out) {
+    efl_sim* s = nullptr;
+    if (!out) return set_err(nullptr, EFL_ERR_INVALID_ARGUMENT, "null output pointer");
+    *out = nullptr;
+    efl_status vs = validate_cfg(cfg);
+    if (vs != EFL_OK) return vs;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0)
+        return set_err(nullptr, EFL_ERR_NO_DEVICE, "no CUDA device available: %s", cudaGetErrorString(e));
+    if (cfg->device < 0 || cfg->device >= ndev)
+        return set_err(nullptr, EFL_ERR_INVALID_ARGUMENT, "device %d out of range (%d devices)", cfg->device, ndev);
+    s = new efl_sim();
+    s->cfg = *cfg;
+    s->nx = (int)cfg->nx;
+    s->ny = (int)cfg->ny;
+    s->P = round_up(s->nx + 1, 32);
+    s->device = cfg->device;
+    auto fail = [&](efl_status st) {
+        g_last_error = s->err;
+        efl_destroy(s);
+        return st;
+    };
+#define CTRY(x)                          \
+    do {                                 \
+        efl_status st_ = (x);            \
+        if (st_ != EFL_OK) return fail(st_); \
+    } while (0)
+    if (cudaSetDevice(s->device) != cudaSuccess) return fail(set_err(s, EFL_ERR_CUDA, "cudaSetDevice failed"));
+    if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return fail(set_err(s, EFL_ERR_CUDA, "cudaStreamCreate failed"));
+    s->U.dx = 1.0f / cfg->length_unit;  // euler_fluid.rs:89
+    s->U.dt = 0.0f;
+    s->U.rho = cfg->rho;
+    s->U.g[0] = cfg->gravity[0];
+    s->U.g[1] = cfg->gravity[1];
+    std::memcpy(s->U.m, cfg->transform, sizeof(s->U.m));
+    s->U.size[0] = (float)s->nx;
+    s->U.size[1] = (float)s->ny;
+    const int nx = s->nx, ny = s->ny, P = s->P, R = ny + 1;
+    CTRY(alloc_plane(s, s->u0, nx + 1, ny, P, R));
+    CTRY(alloc_plane(s, s->u1, nx + 1, ny, P, R));
+    CTRY(alloc_plane(s, s->us, nx + 1, ny, P, R));
+    CTRY(alloc_plane(s, s->v0, nx, ny + 1, P, R));
+    CTRY(alloc_plane(s, s->v1, nx, ny + 1, P, R));
+    CTRY(alloc_plane(s, s->vs, nx, ny + 1, P, R));
+    CTRY(alloc_plane(s, s->ls_s, nx, ny, P, R));
+    CTRY(alloc_plane(s, s->div, nx, ny, P, R));
+    CTRY(alloc_plane(s, s->p0, nx, ny, P, R));
+    CTRY(alloc_plane(s, s->p1, nx, ny, P, R));
+    CTRY(alloc_plane(s, s->ls0, nx, ny, P, R));
+    CTRY(alloc_plane(s, s->ls1, nx, ny, P, R));
+    CTRY(alloc_plane(s, s->fu, nx + 1, ny, P, R));
+    CTRY(alloc_plane(s, s->fv, nx, ny + 1, P, R));
+    CTRY(alloc_plane(s, s->phiT, nx, ny, P, R));
+    CTRY(alloc_plane(s, s->r0, nx, ny, P, R));
+    CTRY(alloc_plane(s, s->sid, nx, ny, P, R));
+    CTRY(alloc_plane(s, s->uvi, nx + 1, ny, P, R));
+    CTRY(alloc_plane(s, s->uvo, nx + 1, ny, P, R));
+    CTRY(alloc_plane(s, s->vvi, nx, ny + 1, P, R));
+    CTRY(alloc_plane(s, s->vvo, nx, ny + 1, P, R));
+    CTRY(alloc_plane(s, s->lab0, nx, ny, P, R));
+    CTRY(alloc_plane(s, s->lab, nx, ny, P, R));
+    CTRY(alloc_plane(s, s->labT, nx, ny, P, R));
+    CTRY(alloc_plane(s, s->upd, nx, ny, P, R));
+    CTRY(alloc_plane(s, s->grad, nx, ny, P, R));
+    CTRY(alloc_plane(s, s->seeds[0], nx, ny, P, R));
+    CTRY(alloc_plane(s, s->seeds[1], nx, ny, P, R));
+    CTRY(alloc_plane(s, s->srcvel, nx, ny, P, R));
+    CTRY(alloc_raw(s, s->d_obs, EFL_MAX_SOLIDS));
+    CTRY(alloc_raw(s, s->d_bins, 3 * EFL_MAX_SOLIDS));
+    CTRY(alloc_raw(s, s->d_forces_out, EFL_MAX_SOLIDS));
+    s->n_partials = std::min(1024, std::max(1, (nx * ny + NORM_THREADS - 1) / NORM_THREADS));
+    CTRY(alloc_raw(s, s->d_partials, s->n_partials));
+    CTRY(alloc_raw(s, s->d_norms, 2));
+    CTRY(alloc_raw(s, s->d_count, 1));
+    if (cudaMallocHost(&s->h_norms, 4 * sizeof(double)) != cudaSuccess)
+        return fail(set_err(s, EFL_ERR_OUT_OF_MEMORY, "cudaMallocHost failed"));
+    CTRY(alloc_mg(s));
+    CTRY(solver_init(s->solver, nx, ny, s->device, &s->err));
+    if (cudaStreamSynchronize(s->stream) != cudaSuccess)
+        return fail(set_err(s, EFL_ERR_CUDA, "initial clear failed: %s", cudaGetErrorString(cudaGetLastError())));
+#undef CTRY
+    *out = s;
+    return EFL_OK;
+}
+
+efl_status efl_destroy(efl_sim* s) {
+    if (!s) return EFL_OK;
+    cudaSetDevice(s->device);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    solver_free(s->solver);
+    for (auto& b : s->bufs) cudaFree(b.p);
+    if (s->d_forces) cudaFree(s->d_forces);
+    if (s->h_norms) cudaFreeHost(s->h_norms);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+    return EFL_OK;
+}
+
+const char* efl_last_error(const efl_sim* s) { return s ? s->err.c_str() : g_last_error.c_str(); }
+
+efl_status efl_reset(efl_sim* s) {
+    if (!s) return set_err(nullptr, EFL_ERR_INVALID_ARGUMENT, "null sim");
+    s->status = 0;
+    return EFL_OK;
+}
+
+efl_status efl_set_projection(efl_sim* s, const efl_projection* p) {
+    if (!s || !p) return set_err(s, EFL_ERR_INVALID_ARGUMENT, "null argument");
+    if (p->method < 0 || p->method > 2) return set_err(s, EFL_ERR_INVALID_ARGUMENT, "unknown projection method");
+    cudaSetDevice(s->device);
+    int old = mg_num_levels(s->cfg);
+    s->cfg.projection = *p;
+    if (mg_num_levels(s->cfg) != old) TRY(alloc_mg(s));
+    return EFL_OK;
+}
+efl_status efl_set_reinit(efl_sim* s, const efl_reinit* r) {
+    if (!s || !r) return set_err(s, EFL_ERR_INVALID_ARGUMENT, "null argument");
+    if (r->method < 0 || r->method > 1) return set_err(s, EFL_ERR_INVALID_ARGUMENT, "unknown reinitialize method");
+    s->cfg.reinit = *r;
+    return EFL_OK;
+}
+efl_status efl_set_transform(efl_sim* s, const float t[16]) {
+    if (!s || !t) return set_err(s, EFL_ERR_INVALID_ARGUMENT, "null argument");
+    std::memcpy(s->U.m, t, sizeof(s->U.m));
+    std::memcpy(s->cfg.transform, t, sizeof(s->U.m));
+    return EFL_OK;
+}
+
+efl_status efl_set_obstacles(efl_sim* s, const efl_solid_obstacle* o, uint32_t n) {
+    if (!s || (n && !o)) return set_err(s, EFL_ERR_INVALID_ARGUMENT, "null argument");
+    if (n > EFL_MAX_SOLIDS) return set_err(s, EFL_ERR_TOO_MANY, "too many obstacles: %u (max %d)", n, EFL_MAX_SOLIDS);
+    for (uint32_t i = 0; i < n; ++i) {
+        uint32_t sh = o[i].shape;
+        if (sh != EFL_SHAPE_CIRCLE && sh != EFL_SHAPE_RECTANGLE && sh != EFL_SHAPE_CAPSULE && sh != EFL_SHAPE_TRIANGLE)
+            return set_err(s, EFL_ERR_UNSUPPORTED_SHAPE, "Unsupported shape type for solid: %u (obstacle %u)", sh, i);
+    }
+    cudaSetDevice(s->device);
+    if (n) CU(cudaMemcpyAsync(s->d_obs, o, n * sizeof(efl_solid_obstacle), cudaMemcpyHostToDevice, s->stream));
+    s->n_obs = (int)n;
+    return EFL_OK;
+}
+
+efl_status efl_set_local_forces(efl_sim* s, const efl_force* f, uint32_t n) {
+    if (!s || (n && !f)) return set_err(s, EFL_ERR_INVALID_ARGUMENT, "null argument");
+    cudaSetDevice(s->device);
+    if ((int)n > s->cap_forces) {
+        CU(cudaStreamSynchronize(s->stream));
+        if (s->d_forces) cudaFree(s->d_forces);
+        s->d_forces = nullptr;
+        s->cap_forces = 0;
+        int cap = std::max<int>(64, (int)n);
+        CU(cudaMalloc(&s->d_forces, (size_t)cap * sizeof(efl_force)));
+        s->cap_forces = cap;
+    }
+    if (n) CU(cudaMemcpyAsync(s->d_forces, f, n * sizeof(efl_force), cudaMemcpyHostToDevice, s->stream));
+    s->n_forces = (int)n;
+    return EFL_OK;
+}
+
+efl_status efl_set_sources(efl_sim* s, const efl_source* src, uint32_t n, int32_t oneshot) {
+    if (!s || (n && !src)) return set_err(s, EFL_ERR_INVALID_ARGUMENT, "null argument");
+    if (n > EFL_MAX_FLUID_SOURCE)
+        return set_err(s, EFL_ERR_TOO_MANY, "The maximum number of fluid source per fluid component is %d.",
+                       EFL_MAX_FLUID_SOURCE);
+    (oneshot ? s->src_once : s->src_cont).assign(src, src + n);
+    return EFL_OK;
+}
+
+efl_status efl_step(efl_sim* s, float dt, efl_step_stats* st) {
+    if (!s) return set_err(nullptr, EFL_ERR_INVALID_ARGUMENT, "null sim");
+    init_stats(st);
+    cudaSetDevice(s->device);
+    if (s->status == 0) {  // FluidStatus::Uninitialized: the init sequence only
+        TRY(run_init(s));
+        s->status = 1;
+        if (st) st->initialized_only = 1;
+        return EFL_OK;
+    }
+    s->U.dt = dt;
+    efl_status ret = EFL_OK;
+    for (int stage = EFL_STAGE_UPDATE_SOLID; stage <= EFL_STAGE_SOLID_FORCES; ++stage) {
+        efl_status r = run_stage(s, stage, st);
+        if (r == EFL_NOT_CONVERGED) ret = r;
+        else if (r != EFL_OK) return r;
+    }
+    s->n_forces = 0;  // apply_forces.rs:166 clears the forces after upload
+    return ret;
+}
+
+efl_status efl_run_stage(efl_sim* s, int32_t stage, float dt, efl_step_stats* st) {
+    if (!s) return set_err(nullptr, EFL_ERR_INVALID_ARGUMENT, "null sim");
+    init_stats(st);
+    cudaSetDevice(s->device);
+    s->U.dt = dt;
+    return run_stage(s, stage, st);
+}
+
+efl_status efl_read_solid_forces(efl_sim* s, efl_solid_force out[EFL_MAX_SOLIDS]) {
+    if (!s || !out) return set_err(s, EFL_ERR_INVALID_ARGUMENT, "null argument");
+    cudaSetDevice(s->device);
+    CU(cudaMemcpyAsync(out, s->d_forces_out, EFL_MAX_SOLIDS * sizeof(efl_solid_force), cudaMemcpyDeviceToHost,
+                       s->stream));
+    CU(cudaStreamSynchronize(s->stream));
+    return EFL_OK;
+}
+efl_status efl_read_force_bins(efl_sim* s, int32_t out[3 * EFL_MAX_SOLIDS]) {
+    if (!s || !out) return set_err(s, EFL_ERR_INVALID_ARGUMENT, "null argument");
+    cudaSetDevice(s->device);
+    CU(cudaMemcpyAsync(out, s->d_bins, 3 * EFL_MAX_SOLIDS * sizeof(int32_t), cudaMemcpyDeviceToHost, s->stream));
+    CU(cudaStreamSynchronize(s->stream));
+    return EFL_OK;
+}
+
+efl_status efl_field_shape(const efl_sim* s, int32_t field, uint32_t* w, uint32_t* h, uint32_t* ch, uint32_t* eb) {
+    if (!s) return set_err(nullptr, EFL_ERR_INVALID_ARGUMENT, "null sim");
+    uint32_t W, H, C = 1;
+    if (field == EFL_FIELD_AREA_FRACTION) {
+        W = s->nx;
+        H = s->ny;
+        C = 4;
+    } else {
+        FieldDesc fd;
+        if (!field_desc(s, field, &fd)) return set_err(const_cast<efl_sim*>(s), EFL_ERR_INVALID_ARGUMENT, "bad field %d", field);
+        W = fd.w;
+        H = fd.h;
+        C = fd.ch;
+    }
+    if (w) *w = W;
+    if (h) *h = H;
+    if (ch) *ch = C;
+    if (eb) *eb = 4;
+    return EFL_OK;
+}
+
+efl_status efl_get_field(efl_sim* s, int32_t field, void* dst, size_t bytes) {
+    if (!s || !dst) return set_err(s, EFL_ERR_INVALID_ARGUMENT, "null argument");
+    cudaSetDevice(s->device);
+    const int nx = s->nx, ny = s->ny;
+    if (field == EFL_FIELD_AREA_FRACTION) {  // RGBA view of the face planes
+        if (bytes != (size_t)nx * ny * 16) return set_err(s, EFL_ERR_INVALID_ARGUMENT, "size mismatch");
+        std::vector<float> fu((size_t)(nx + 1) * ny), fv((size_t)nx * (ny + 1));
+        FieldDesc a, b;
+        field_desc(s, EFL_FIELD_AREA_FRACTION_U, &a);
+        field_desc(s, EFL_FIELD_AREA_FRACTION_V, &b);
+        TRY(copy_field_out(s, a, fu.data()));
+        TRY(copy_field_out(s, b, fv.data()));
+        float* o = (float*)dst;
+        for (int y = 0; y < ny; ++y)
+            for (int x = 0; x < nx; ++x) {
+                float* c = o + ((size_t)y * nx + x) * 4;
+                c[0] = fu[(size_t)y * (nx + 1) + x];
+                c[1] = fu[(size_t)y * (nx + 1) + x + 1];
+                c[2] = fv[(size_t)y * nx + x];
+                c[3] = fv[(size_t)(y + 1) * nx + x];
+            }
+        return EFL_OK;
+    }
+    FieldDesc fd;
+    if (!field_desc(s, field, &fd)) return set_err(s, EFL_ERR_INVALID_ARGUMENT, "bad field %d", field);
+    if (bytes != (size_t)fd.w * fd.h * fd.ch * 4) return set_err(s, EFL_ERR_INVALID_ARGUMENT, "size mismatch");
+    return copy_field_out(s, fd, dst);
+}
+
+efl_status efl_set_field(efl_sim* s, int32_t field, const void* src, size_t bytes) {
+    if (!s || !src) return set_err(s, EFL_ERR_INVALID_ARGUMENT, "null argument");
+    cudaSetDevice(s->device);
+    const int nx = s->nx, ny = s->ny;
+    if (field == EFL_FIELD_AREA_FRACTION) {
+        // (i-1/2) and (j-1/2) components of every cell; (i+1/2) of the last
+        // column and (j+1/2) of the last row.
+        if (bytes != (size_t)nx * ny * 16) return set_err(s, EFL_ERR_INVALID_ARGUMENT, "size mismatch");
+        const float* a = (const float*)src;
+        std::vector<float> fu((size_t)(nx + 1) * ny), fv((size_t)nx * (ny + 1));
+        for (int y = 0; y < ny; ++y)
+            for (int x = 0; x < nx; ++x) {
+                const float* c = a + ((size_t)y * nx + x) * 4;
+                fu[(size_t)y * (nx + 1) + x] = c[0];
+                if (x == nx - 1) fu[(size_t)y * (nx + 1) + x + 1] = c[1];
+                fv[(size_t)y * nx + x] = c[2];
+                if (y == ny - 1) fv[(size_t)(y + 1) * nx + x] = c[3];
+            }
+        FieldDesc A, B;
+        field_desc(s, EFL_FIELD_AREA_FRACTION_U, &A);
+        field_desc(s, EFL_FIELD_AREA_FRACTION_V, &B);
+        TRY(copy_field_in(s, A, fu.data()));
+        return copy_field_in(s, B, fv.data());
+    }
+    FieldDesc fd;
+    if (!field_desc(s, field, &fd)) return set_err(s, EFL_ERR_INVALID_ARGUMENT, "bad field %d", field);
+    if (bytes != (size_t)fd.w * fd.h * fd.ch * 4) return set_err(s, EFL_ERR_INVALID_ARGUMENT, "size mismatch");
+    return copy_field_in(s, fd, src);
+}
+
+efl_status efl_field_device_ptr(efl_sim* s, int32_t field, void** dptr, size_t* pitch) {
+    if (!s || !dptr) return set_err(s, EFL_ERR_INVALID_ARGUMENT, "null argument");
+    FieldDesc fd;
+    if (!field_desc(s, field, &fd)) return set_err(s, EFL_ERR_INVALID_ARGUMENT, "field %d has no device plane", field);
+    *dptr = fd.base;
+    if (pitch) *pitch = (size_t)fd.P * fd.ch * 4;
+    return EFL_OK;
+}
+
+efl_status efl_stream(efl_sim* s, void** stream) {
+    if (!s || !stream) return set_err(s, EFL_ERR_INVALID_ARGUMENT, "null argument");
+    *stream = (void*)s->stream;
+    return EFL_OK;
+}
+
+efl_status efl_synchronize(efl_sim* s) {
+    if (!s) return set_err(nullptr, EFL_ERR_INVALID_ARGUMENT, "null sim");
+    cudaSetDevice(s->device);
+    CU(cudaStreamSynchronize(s->stream));
+    return EFL_OK;
+}
+
+efl_status efl_residual(efl_sim* s, double* rel, double* nr, double* nb) {
+    if (!s) return set_err(nullptr, EFL_ERR_INVALID_ARGUMENT, "null sim");
+    cudaSetDevice(s->device);
+    TRY(launch_norms(s, s->mg[0]));
+    double R, B;
+    TRY(read_norms(s, &R, &B));
+    if (nr) *nr = std::sqrt(R);
+    if (nb) *nb = std::sqrt(B);
+    if (rel) *rel = rel_from(R, B);
+    return EFL_OK;
+}
+
+efl_status efl_fluid_volume(efl_sim* s, uint64_t* cells) {
+    if (!s || !cells) return set_err(s, EFL_ERR_INVALID_ARGUMENT, "null argument");
+    cudaSetDevice(s->device);
+    CU(cudaMemsetAsync(s->d_count, 0, sizeof(unsigned long long), s->stream));
+    k_volume<<<grid2d(s->nx, s->ny, kBlock), kBlock, 0, s->stream>>>(s->ls0, s->d_count);
+    LAUNCH_CHECK();
+    unsigned long long c = 0;
+    CU(cudaMemcpyAsync(&c, s->d_count, sizeof(c), cudaMemcpyDeviceToHost, s->stream));
+    CU(cudaStreamSynchronize(s->stream));
+    *cells = c;
+    return EFL_OK;
+}
+
+}  // extern "C"

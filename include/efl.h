@@ -1,0 +1,317 @@
+/*
+ * efl.h — C ABI of the B200 Eulerian-fluid step library (libefl_b200.so).
+ *
+ * This boundary replaces the per-frame compute pass that the reference
+ * plugin records in `EulerFluidNode::run` (src/euler_fluid/render_node.rs:193-476)
+ * and the force read-back observer `forces_to_solid_readback`
+ * (src/euler_fluid/fluid_to_solid.rs:180-209).  The plugin-level types stay
+ * on the caller's side (FluidSettings, FluidSource, ForcesToFluid, the
+ * rigid-body query); the caller copies them into the plain structs below.
+ *
+ * Conventions
+ *  - Every function returns an efl_status; EFL_OK == 0.  On failure the
+ *    message is available from efl_last_error(sim) (or efl_last_error(NULL)
+ *    for errors raised before a handle exists).
+ *  - Host arrays passed in are caller-owned and copied before the call
+ *    returns.  Device memory is owned by the library.
+ *  - Each efl_sim owns one CUDA stream.  Calls on one handle must be
+ *    serialised by the caller; different handles are independent.
+ *  - All fields are f32 row-major, x fastest.  Grid index (x, y) has y
+ *    pointing down, as in the reference's textures.
+ *  - u faces are (nx+1) x ny, v faces nx x (ny+1), cell fields nx x ny.
+ *
+ * Out-of-bounds texture reads in the reference are backend defined; this
+ * library fixes them to "load returns 0, store is dropped" (robust-access
+ * behaviour of DX12/Vulkan), which is what the examples' DX12 backend does.
+ */
+#ifndef EFL_H
+#define EFL_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(_WIN32)
+#define EFL_API __declspec(dllexport)
+#else
+#define EFL_API __attribute__((visibility("default")))
+#endif
+
+#define EFL_ABI_VERSION 1
+
+/* Limits taken from the reference. */
+#define EFL_MAX_SOLIDS 256        /* fluid_to_solid.rs:28 MAX_SOLIDS               */
+#define EFL_MAX_FLUID_SOURCE 16   /* fluid_source_uniform.rs:19 MAX_FLUID_SOURCE   */
+
+typedef enum efl_status {
+    EFL_OK = 0,
+    EFL_ERR_INVALID_ARGUMENT = 1, /* bad size, null pointer, bad enum       */
+    EFL_ERR_CUDA = 2,             /* a CUDA runtime call failed             */
+    EFL_ERR_OUT_OF_MEMORY = 3,
+    EFL_NOT_CONVERGED = 4,        /* residual solve hit max_iterations      */
+    EFL_ERR_TOO_MANY = 5,         /* > EFL_MAX_SOLIDS / EFL_MAX_FLUID_SOURCE */
+    EFL_ERR_UNSUPPORTED_SHAPE = 6,/* obstacle shape id not 0/1/2/4           */
+    EFL_ERR_STATE = 7,            /* call not valid in the current state     */
+    EFL_ERR_NO_DEVICE = 8         /* no CUDA device / extension unusable     */
+} efl_status;
+
+/* ProjectionMethod (src/euler_fluid/projection.rs:44-52). */
+typedef enum efl_projection_method {
+    EFL_PROJECTION_JACOBI = 0,
+    EFL_PROJECTION_GAUSS_SEIDEL = 1,
+    EFL_PROJECTION_MULTIGRID = 2
+} efl_projection_method;
+
+/* ReinitializeMethod (src/euler_fluid/reinitialize_levelset.rs:36-40). */
+typedef enum efl_reinit_method {
+    EFL_REINIT_JUMP_FLOODING = 0,
+    EFL_REINIT_FAST_ITERATIVE = 1
+} efl_reinit_method;
+
+/*
+ * Pressure projection settings.
+ *  - gs_iterations / sor_weight: GaussSeidelConfig (gauss_seidel.rs:33-42,
+ *    weight 1.9 at gauss_seidel.rs:72).
+ *  - mg_pre/mg_post/mg_coarsest: MultiGridConfig (multi_grid.rs:56-71).
+ *  - mg_levels: 0 = the reference rule max(1, floor(log2(min(nx,ny))) - 2)
+ *    (multi_grid.rs:95-97); otherwise the explicit number of levels.
+ *  - tolerance: 0 = the reference's fixed iteration count (one V-cycle for
+ *    multigrid, gs_iterations red-black iterations for Gauss-Seidel).
+ *    > 0 = iterate until ||b - A p||_2 / ||b||_2 <= tolerance (FP64 norms
+ *    over cells with phi < 0 that are not fully solid), checking every
+ *    check_interval RB iterations (Gauss-Seidel) or every V-cycle
+ *    (multigrid), at most max_iterations iterations / V-cycles.
+ */
+typedef struct efl_projection {
+    int32_t method;          /* efl_projection_method                        */
+    uint32_t gs_iterations;  /* default 20                                    */
+    float sor_weight;        /* default 1.9                                   */
+    uint32_t mg_pre;         /* default 2                                     */
+    uint32_t mg_post;        /* default 2                                     */
+    uint32_t mg_coarsest;    /* default 3                                     */
+    uint32_t mg_levels;      /* default 0 (reference rule)                    */
+    float tolerance;         /* default 0 (fixed count)                       */
+    uint32_t max_iterations; /* default 20000                                 */
+    uint32_t check_interval; /* default 16 (Gauss-Seidel only)                */
+} efl_projection;
+
+typedef struct efl_reinit {
+    int32_t method;          /* efl_reinit_method; default FAST_ITERATIVE      */
+    uint32_t fim_iterations; /* FastIterativeMethodConfig, default 10          */
+} efl_reinit;
+
+/*
+ * Creation parameters: FluidPlugin::new(length_unit) (euler_fluid.rs:47-53)
+ * plus FluidSettings{rho, gravity, size} (settings.rs:110-114) plus the
+ * fluid entity's Transform (setup_components.rs:100-103), column-major 4x4
+ * as glam's Mat4.
+ */
+typedef struct efl_config {
+    uint32_t nx, ny;         /* FluidSettings.size; multiples of 8, >= 16    */
+    float length_unit;       /* dx = 1 / length_unit; must be > 0             */
+    float rho;
+    float gravity[2];        /* grid frame, y down: (0, +9.8) is downward     */
+    float transform[16];     /* column-major fluid transform                  */
+    efl_projection projection;
+    efl_reinit reinit;
+    int32_t device;          /* CUDA device ordinal                           */
+} efl_config;
+
+/* ShapeVariant ids (solid_obstacle.wgsl:4-7, parry2d ShapeType). */
+enum {
+    EFL_SHAPE_CIRCLE = 0,
+    EFL_SHAPE_RECTANGLE = 1,
+    EFL_SHAPE_CAPSULE = 2,
+    EFL_SHAPE_TRIANGLE = 4
+};
+
+/*
+ * SolidObstacle (obstacle.rs:24-32, solid_obstacle.wgsl:34-41).
+ * values: circle {radius}; rectangle {half_x, half_y};
+ * capsule {ax, ay, bx, by, radius}; triangle {ax, ay, bx, by, cx, cy}.
+ * entity_id is the obstacle's index in the caller's body list; force bins
+ * are keyed by it and obstacles[entity_id] gives the centre of mass
+ * (sample_forces.wgsl:40-41), as in the reference.  176 bytes.
+ */
+typedef struct efl_solid_obstacle {
+    uint32_t entity_id;
+    uint32_t shape;
+    float values[6];
+    float transform[16];         /* column-major world transform            */
+    float inverse_transform[16]; /* its inverse, as the reference uploads it */
+    float linear_velocity[2];
+    float angular_velocity;
+    float _pad;
+} efl_solid_obstacle;
+
+/* ForceToFluid (apply_forces.rs:36-40): force in m/s^2 at a grid-pixel
+ * position (y down).  The README's "LocalForces" is this type. */
+typedef struct efl_force {
+    float force[2];
+    float position[2];
+} efl_force;
+typedef efl_force efl_local_force;
+
+/* FluidSourceData (fluid_source_uniform.rs:48-55). */
+enum { EFL_SOURCE_CIRCLE = 0, EFL_SOURCE_AABB = 1 };
+enum { EFL_SOURCE_MODE_SOURCE = 0, EFL_SOURCE_MODE_SINK = 1 };
+typedef struct efl_source {
+    float center[2];   /* source Transform translation, grid-centred, y up  */
+    float data[2];     /* circle {radius, 0}; aabb {half_x, half_y}          */
+    float velocity[2]; /* FluidSourceVelocity (zero for one-shot sources)    */
+    uint32_t shape;
+    uint32_t mode;
+} efl_source;
+
+/* FluidToSolidForce (fluid_to_solid.rs:60-64): bins * 0.1. */
+typedef struct efl_solid_force {
+    float force[2];
+    float torque;
+    float _pad;
+} efl_solid_force;
+
+typedef struct efl_step_stats {
+    int32_t initialized_only;     /* 1: this call ran the init sequence only */
+    uint32_t pressure_iterations; /* RB iterations (GS), V-cycles (MG), 50 (Jacobi) */
+    int32_t converged;            /* 1 if tolerance met (or fixed-count mode) */
+    int32_t _pad;
+    double residual;              /* relative residual after the solve, -1 if not computed */
+    double residual_initial;      /* relative residual before the solve, -1 if not computed */
+} efl_step_stats;
+
+/* Field ids for efl_get_field / efl_set_field / efl_field_shape. */
+typedef enum efl_field {
+    EFL_FIELD_U = 0,              /* u0: FluidTextures.u      (nx+1) x ny   */
+    EFL_FIELD_V = 1,              /* v0: FluidTextures.v      nx x (ny+1)   */
+    EFL_FIELD_U1 = 2,             /* advected/forced u                      */
+    EFL_FIELD_V1 = 3,
+    EFL_FIELD_U_SOLID = 4,        /* FluidTextures.u_solid                  */
+    EFL_FIELD_V_SOLID = 5,        /* FluidTextures.v_solid                  */
+    EFL_FIELD_LEVELSET_AIR = 6,   /* phi0: FluidTextures.levelset_air       */
+    EFL_FIELD_LEVELSET_AIR1 = 7,  /* phi1                                   */
+    EFL_FIELD_LEVELSET_SOLID = 8, /* FluidTextures.levelset_solid           */
+    EFL_FIELD_SOLID_ID = 9,       /* i32                                    */
+    EFL_FIELD_AREA_FRACTION = 10, /* 4 x f32 per cell (i-1/2, i+1/2, j-1/2, j+1/2) */
+    EFL_FIELD_DIVERGENCE = 11,
+    EFL_FIELD_PRESSURE = 12,      /* p0                                     */
+    EFL_FIELD_GRAD_LEVELSET = 13, /* 2 x f32 per cell                        */
+    EFL_FIELD_JFA_SEEDS = 14,     /* 2 x f32 per cell, final pass output     */
+    EFL_FIELD_FIM_LABELS = 15,    /* u32                                     */
+    EFL_FIELD_U_VALID = 16,       /* i32, extrapolation validity of u faces  */
+    EFL_FIELD_V_VALID = 17,       /* i32                                     */
+    EFL_FIELD_AREA_FRACTION_U = 18, /* x-face fractions (nx+1) x ny (device layout) */
+    EFL_FIELD_AREA_FRACTION_V = 19, /* y-face fractions nx x (ny+1)          */
+    EFL_FIELD_COUNT = 20
+} efl_field;
+
+/* Pipeline stages, in the order EulerFluidNode::run records them
+ * (render_node.rs:290-463).  efl_run_stage runs one of them on the current
+ * state; it exists for per-kernel parity tests and debugging. */
+typedef enum efl_stage {
+    EFL_STAGE_INIT = 0,               /* render_node.rs:219-277 */
+    EFL_STAGE_UPDATE_SOLID = 1,       /* update_solid.wgsl      */
+    EFL_STAGE_AREA_FRACTION = 2,      /* update_area_fraction.wgsl */
+    EFL_STAGE_ADVECT_VELOCITY = 3,    /* advect_velocity.wgsl   */
+    EFL_STAGE_APPLY_FORCES = 4,       /* apply_forces.wgsl      */
+    EFL_STAGE_DIVERGENCE = 5,         /* divergence.wgsl        */
+    EFL_STAGE_PROJECTION = 6,         /* projection.rs:89-164   */
+    EFL_STAGE_SOLVE_VELOCITY = 7,     /* solve_velocity_{u,v}.wgsl */
+    EFL_STAGE_EXTRAPOLATE = 8,        /* render_node.rs:540-608 */
+    EFL_STAGE_ADVECT_LEVELSET = 9,    /* advect_levelset.wgsl   */
+    EFL_STAGE_FLUID_SOURCE = 10,      /* update_fluid_source.wgsl */
+    EFL_STAGE_REINITIALIZE = 11,      /* reinitialize_levelset.rs:162-243 */
+    EFL_STAGE_LEVELSET_GRADIENT = 12, /* levelset_gradient.wgsl */
+    EFL_STAGE_SOLID_FORCES = 13,      /* render_node.rs:610-641 */
+    EFL_STAGE_COUNT = 14
+} efl_stage;
+
+typedef struct efl_sim efl_sim;
+
+/* Library ABI version (EFL_ABI_VERSION). */
+EFL_API int32_t efl_abi_version(void);
+
+/* Fills *cfg with the reference defaults for an nx x ny grid:
+ * length_unit 1, rho 1, gravity (0, 9.8), identity transform,
+ * Gauss-Seidel 20 iterations at weight 1.9, FIM(10). */
+EFL_API efl_status efl_default_config(uint32_t nx, uint32_t ny, efl_config* cfg);
+
+/* Creates a simulation (watch_fluid_component, setup_components.rs:38-328).
+ * The new simulation is in FluidStatus::Reset: the next efl_step runs the
+ * init sequence. Errors: length_unit <= 0 (the reference panics,
+ * euler_fluid.rs:49-51), nx/ny not multiples of 8 or < 16. Sizes that are
+ * not multiples of 64 are accepted; as in the reference, the face kernels
+ * then cover floor(n/64)*64 rows/columns only (pipeline.rs:180-186). */
+EFL_API efl_status efl_create(const efl_config* cfg, efl_sim** out);
+EFL_API efl_status efl_destroy(efl_sim* sim);
+
+/* Message for the last error on this handle (NULL: the last error of a
+ * call that had no handle, e.g. a failed efl_create). */
+EFL_API const char* efl_last_error(const efl_sim* sim);
+
+/* FluidStatus::Reset (fluid_status.rs:15-38): the next efl_step re-runs
+ * the init sequence. */
+EFL_API efl_status efl_reset(efl_sim* sim);
+
+/* Runtime changes of the ProjectionMethod / ReinitializeMethod components. */
+EFL_API efl_status efl_set_projection(efl_sim* sim, const efl_projection* p);
+EFL_API efl_status efl_set_reinit(efl_sim* sim, const efl_reinit* r);
+EFL_API efl_status efl_set_transform(efl_sim* sim, const float transform[16]);
+
+/* construct_rigid_body_buffer_for_gpu (obstacle.rs:89-160): the full body
+ * list, kept until replaced. n <= EFL_MAX_SOLIDS. */
+EFL_API efl_status efl_set_obstacles(efl_sim* sim, const efl_solid_obstacle* obstacles, uint32_t n);
+
+/* apply_forces_and_clear (apply_forces.rs:157-168): forces used by the next
+ * step only, then cleared. */
+EFL_API efl_status efl_set_local_forces(efl_sim* sim, const efl_force* forces, uint32_t n);
+
+/* update_fluid_source_{init_,}buffer (fluid_source_uniform.rs:77-158).
+ * oneshot != 0: the FluidSourceOneshot list, applied by the init sequence;
+ * oneshot == 0: the continuous list, applied every step. n <= 16. */
+EFL_API efl_status efl_set_sources(efl_sim* sim, const efl_source* sources, uint32_t n, int32_t oneshot);
+
+/* One render-graph Update for this simulation: the init sequence if the
+ * simulation is not initialised (stats->initialized_only = 1), else one
+ * full step with time step dt (render_node.rs:278-466). Returns
+ * EFL_NOT_CONVERGED (state still advanced) if a tolerance-driven pressure
+ * solve hit max_iterations. stats may be NULL. */
+EFL_API efl_status efl_step(efl_sim* sim, float dt, efl_step_stats* stats);
+
+/* Runs one stage of the step on the current state (testing/debugging). */
+EFL_API efl_status efl_run_stage(efl_sim* sim, int32_t stage, float dt, efl_step_stats* stats);
+
+/* FluidToSolidForce[256] of the last step (fluid_to_solid.rs:180-209 reads
+ * these); bins as raw fixed-point i32 (3 x 256: fx, fy, torque). */
+EFL_API efl_status efl_read_solid_forces(efl_sim* sim, efl_solid_force out[EFL_MAX_SOLIDS]);
+EFL_API efl_status efl_read_force_bins(efl_sim* sim, int32_t out[3 * EFL_MAX_SOLIDS]);
+
+/* Field shape: width, height, channels and bytes per channel. */
+EFL_API efl_status efl_field_shape(const efl_sim* sim, int32_t field, uint32_t* width,
+                                   uint32_t* height, uint32_t* channels, uint32_t* elem_bytes);
+/* Dense (unpitched) host copies of a field; bytes must equal
+ * width*height*channels*elem_bytes. Synchronous. */
+EFL_API efl_status efl_get_field(efl_sim* sim, int32_t field, void* host_dst, size_t bytes);
+EFL_API efl_status efl_set_field(efl_sim* sim, int32_t field, const void* host_src, size_t bytes);
+/* Device pointer and row pitch (bytes) of a field for zero-copy readers.
+ * Not available for EFL_FIELD_AREA_FRACTION (stored as the two face
+ * arrays EFL_FIELD_AREA_FRACTION_U / _V). */
+EFL_API efl_status efl_field_device_ptr(efl_sim* sim, int32_t field, void** dptr, size_t* pitch_bytes);
+/* The simulation's CUDA stream (cudaStream_t). */
+EFL_API efl_status efl_stream(efl_sim* sim, void** stream);
+EFL_API efl_status efl_synchronize(efl_sim* sim);
+
+/* Relative residual ||b - A p||_2 / ||b||_2 of the current pressure against
+ * the current divergence (operator of residual.wgsl:33-54), FP64 norms. */
+EFL_API efl_status efl_residual(efl_sim* sim, double* relative, double* norm_r, double* norm_b);
+
+/* Number of cells with levelset_air < 0 (calculate_volume.wgsl:11-75). */
+EFL_API efl_status efl_fluid_volume(efl_sim* sim, uint64_t* cells);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* EFL_H */

@@ -1,0 +1,1544 @@
+// efl_oracle.cpp — TEST INFRASTRUCTURE, not product code.
+//
+// CPU restatement of the reference's per-step Eulerian fluid pipeline
+// (narasan49/bevy_eulerian_fluid v0.4.0).  Every kernel below follows one
+// WGSL entry point, statement by statement and in the same floating-point
+// operation order, with these fixed semantics:
+//   * texture loads out of bounds return 0, out-of-bounds stores are
+//     dropped (robust buffer access, the DX12 behaviour the examples use);
+//   * no FMA contraction (built with -ffp-contract=off), IEEE division and
+//     sqrt, WGSL round() = round-half-to-even, clamp(NaN,0,1) = 0 (the
+//     maxNum/minNum behaviour of GPUs), f32->i32 truncates and saturates,
+//     NaN -> 0;
+//   * every kernel covers exactly the invocation domain of its reference
+//     dispatch (pipeline.rs:175-186, render_node.rs:226-230);
+//   * racy reference kernels get a fixed resolution that the CUDA library
+//     shares: update_fluid_source's shared faces take the value of the
+//     raster-last writer; the FIM update is the deterministic two-phase
+//     form documented at fim_update_two_phase().
+//
+// Only tests/, __graft_entry__.smoke() and bench.py's CPU leg use this file.
+// Parity is unpinned (the reference has no golden vectors); the oracle's
+// known-answer tests pin it.
+
+#include "efl_oracle.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+#include <string>
+#include <vector>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+constexpr float LARGE_FLOAT_SOLID = 1.0e6f;   // update_solid.wgsl:4
+constexpr float LARGE_FLOAT_SOURCE = 1.0e6f;  // update_fluid_source.wgsl:22
+constexpr float FIM_LARGE = 1e30f;            // fast_iterative_method/initialize.wgsl:5
+constexpr float FIM_EPS = 1e-6f;              // fast_iterative_method/update.wgsl:9
+constexpr float SQRT2_F = 1.41421356237309504880f;  // update.wgsl:11 (f32)
+constexpr uint32_t LABEL_NONE = 0, LABEL_SOURCE = 1, LABEL_ACTIVE = 2, LABEL_CONVERGED = 3;
+
+int g_threads = 0;
+
+struct F2 { float x, y; };
+struct F4 { float x, y, z, w; };
+
+template <class T>
+struct Tex {
+    int w = 0, h = 0;
+    std::vector<T> a;
+    void init(int w_, int h_) { w = w_; h = h_; a.assign((size_t)w * h, T{}); }
+    inline bool in(int x, int y) const { return x >= 0 && y >= 0 && x < w && y < h; }
+    inline T ld(int x, int y) const { return in(x, y) ? a[(size_t)y * w + x] : T{}; }
+    inline void st(int x, int y, T v) { if (in(x, y)) a[(size_t)y * w + x] = v; }
+    inline T& at(int x, int y) { return a[(size_t)y * w + x]; }
+};
+
+// WGSL helpers ---------------------------------------------------------------
+inline float fclamp01(float v) { return std::fmin(std::fmax(v, 0.0f), 1.0f); }
+inline float fclamp(float v, float lo, float hi) { return std::fmin(std::fmax(v, lo), hi); }
+inline float wsign(float v) { return v > 0.0f ? 1.0f : (v < 0.0f ? -1.0f : 0.0f); }
+inline float wlength(float x, float y) { return std::sqrt(x * x + y * y); }
+inline float wmix(float a, float b, float t) { return a * (1.0f - t) + b * t; }
+inline int32_t f2i(float v) {  // WGSL i32(f32): truncate, saturate, NaN -> 0
+    if (std::isnan(v)) return 0;
+    if (v >= 2147483647.0f) return std::numeric_limits<int32_t>::max();
+    if (v <= -2147483648.0f) return std::numeric_limits<int32_t>::min();
+    return (int32_t)v;
+}
+// mat4 (column-major) * vec4(x, y, 0, 1), .xy
+inline F2 mat_xy(const float* m, float x, float y) {
+    F2 r;
+    r.x = ((m[0] * x + m[4] * y) + m[8] * 0.0f) + m[12] * 1.0f;
+    r.y = ((m[1] * x + m[5] * y) + m[9] * 0.0f) + m[13] * 1.0f;
+    return r;
+}
+// determinant of a column-major 4x4 (only compared against 0)
+inline float det4(const float* m) {
+    auto a = [&](int r, int c) { return m[c * 4 + r]; };
+    float s0 = a(0, 0) * a(1, 1) - a(1, 0) * a(0, 1);
+    float s1 = a(0, 0) * a(1, 2) - a(1, 0) * a(0, 2);
+    float s2 = a(0, 0) * a(1, 3) - a(1, 0) * a(0, 3);
+    float s3 = a(0, 1) * a(1, 2) - a(1, 1) * a(0, 2);
+    float s4 = a(0, 1) * a(1, 3) - a(1, 1) * a(0, 3);
+    float s5 = a(0, 2) * a(1, 3) - a(1, 2) * a(0, 3);
+    float c5 = a(2, 2) * a(3, 3) - a(3, 2) * a(2, 3);
+    float c4 = a(2, 1) * a(3, 3) - a(3, 1) * a(2, 3);
+    float c3 = a(2, 1) * a(3, 2) - a(3, 1) * a(2, 2);
+    float c2 = a(2, 0) * a(3, 3) - a(3, 0) * a(2, 3);
+    float c1 = a(2, 0) * a(3, 2) - a(3, 0) * a(2, 2);
+    float c0 = a(2, 0) * a(3, 1) - a(3, 0) * a(2, 1);
+    return s0 * c5 - s1 * c4 + s2 * c3 + s3 * c2 - s4 * c1 + s5 * c0;
+}
+
+// utils/area_fraction.wgsl:10-12
+inline float area_fraction(float l0, float l1) {
+    return fclamp01(std::fmax(l0, l1) / std::fabs(l0 - l1));
+}
+// utils/area_fraction.wgsl:14-56
+inline F4 area_fractions(const Tex<float>& ls, int x, int y) {
+    float c0 = ls.ld(x - 1, y - 1), c1 = ls.ld(x, y - 1), c2 = ls.ld(x + 1, y - 1);
+    float c3 = ls.ld(x - 1, y), c4 = ls.ld(x, y), c5 = ls.ld(x + 1, y);
+    float c6 = ls.ld(x - 1, y + 1), c7 = ls.ld(x, y + 1), c8 = ls.ld(x + 1, y + 1);
+    float mm = 0.25f * (c0 + c1 + c3 + c4);
+    float pm = 0.25f * (c1 + c2 + c4 + c5);
+    float mp = 0.25f * (c3 + c4 + c6 + c7);
+    float pp = 0.25f * (c4 + c5 + c7 + c8);
+    return F4{area_fraction(mm, mp), area_fraction(pm, pp), area_fraction(mm, pm), area_fraction(mp, pp)};
+}
+
+struct Uniform {  // fluid_uniform.wgsl:3-10
+    float dx, dt, rho;
+    float g[2];
+    float m[16];
+    float size[2];
+};
+
+// One multigrid level (multi_grid.rs:77-83).  The iterate x, right-hand
+// side b and residual r are of type T: f32 in the reference's fixed-count
+// mode, f64 in the tolerance-driven mode; the level set and the area
+// fractions are always the reference's f32 data.
+template <class T>
+struct LevelT {
+    int nx, ny;
+    Tex<T> x, b, r;
+    Tex<float> ls;
+    Tex<F4> af;
+};
+using Level = LevelT<float>;
+using Level64 = LevelT<double>;
+
+}  // namespace
+
+struct eflo_sim {
+    efl_config cfg;
+    int nx, ny;
+    Uniform U;
+    std::string err;
+    int status = 0;  // 0 = Reset/Uninitialized, 1 = Initialized
+    bool fim_serial = false;
+
+    Tex<float> u0, u1, v0, v1, us, vs, ls_solid, div, p0, p1, ls0, ls1;
+    Tex<int32_t> solid_id, u_valid_in, u_valid_out, v_valid_in, v_valid_out;
+    Tex<F4> af;
+    Tex<F2> grad, seeds[2];
+    int seeds_final = 0;
+    Tex<uint32_t> labels0, labels, labelsT;
+    Tex<float> phiT;
+    std::vector<Level> mg;
+    std::vector<Level64> mg64;
+
+    std::vector<efl_solid_obstacle> obstacles;
+    std::vector<efl_force> forces;
+    std::vector<efl_source> src_once, src_cont;
+    int32_t bins[3][EFL_MAX_SOLIDS];
+    efl_solid_force out_forces[EFL_MAX_SOLIDS];
+
+    // dispatch domains (pipeline.rs:175-186)
+    int cx() const { return (nx / 8) * 8; }
+    int cy() const { return (ny / 8) * 8; }
+    int xrows() const { return (ny / 64) * 64; }
+    int ycols() const { return (nx / 64) * 64; }
+};
+
+namespace {
+
+efl_status fail(eflo_sim* s, efl_status st, const std::string& m) {
+    if (s) s->err = m;
+    return st;
+}
+
+template <class F>
+inline void par_rows(int y0, int y1, F f) {
+#pragma omp parallel for schedule(static) if (g_threads != 1)
+    for (int y = y0; y < y1; ++y) f(y);
+}
+
+// ---------------------------------------------------------------------------
+// initialize_grid_center.wgsl:5-15 (dispatch_center)
+void k_init_center(eflo_sim& s) {
+    par_rows(0, s.cy(), [&](int y) {
+        for (int x = 0; x < s.cx(); ++x) {
+            float level = (float)(uint32_t)(s.ny - y);
+            s.ls0.st(x, y, level);
+            s.ls1.st(x, y, level);
+            s.grad.st(x, y, F2{0.0f, -1.0f});
+        }
+    });
+}
+// initialize_grid_edge.wgsl:6-17, dispatched (nx+1, ny/64) x (1,64), v transposed
+void k_init_edge(eflo_sim& s) {
+    for (int gy = 0; gy < s.xrows(); ++gy)
+        for (int gx = 0; gx <= s.nx; ++gx) {
+            s.u0.st(gx, gy, 0.0f);
+            s.v0.st(gy, gx, 0.0f);
+            s.u1.st(gx, gy, 0.0f);
+            s.v1.st(gy, gx, 0.0f);
+        }
+}
+
+// update_solid.wgsl:80-85
+inline F2 to_world(const Uniform& U, float px, float py, int nx, int ny) {
+    float uvx = px / (float)nx, uvy = py / (float)ny;
+    float xx = (uvx - 0.5f) * U.size[0];
+    float yy = (-uvy + 0.5f) * U.size[1];
+    return mat_xy(U.m, xx, yy);
+}
+// update_solid.wgsl:164-169
+inline float dist_segment(F2 x, F2 a, F2 b) {
+    float abx = b.x - a.x, aby = b.y - a.y;
+    float t = fclamp(((x.x - a.x) * abx + (x.y - a.y) * aby) / (abx * abx + aby * aby), 0.0f, 1.0f);
+    float px = a.x + t * abx, py = a.y + t * aby;
+    return wlength(x.x - px, x.y - py);
+}
+// update_solid.wgsl:171-175
+inline float dist_sign(F2 x, F2 a, F2 b) {
+    float x1x = x.x - a.x, x1y = x.y - a.y;
+    float abx = b.x - a.x, aby = b.y - a.y;
+    return wsign(x1y * abx - x1x * aby);
+}
+// update_solid.wgsl:87-109
+inline float level_rectangle(const efl_solid_obstacle& o, F2 x) {
+    float level = LARGE_FLOAT_SOLID;
+    if (det4(o.transform) == 0.0f) return level;
+    F2 x0 = mat_xy(o.inverse_transform, x.x, x.y);
+    float hx = o.values[0], hy = o.values[1];
+    bool ix = std::fabs(x0.x) < hx, iy = std::fabs(x0.y) < hy;
+    if (ix) {
+        if (iy) level = std::fmax(std::fabs(x0.x) - hx, std::fabs(x0.y) - hy);
+        else level = std::fabs(x0.y) - hy;
+    } else {
+        if (iy) level = std::fabs(x0.x) - hx;
+        else level = wlength(std::fabs(x0.x) - hx, std::fabs(x0.y) - hy);
+    }
+    return level;
+}
+// update_solid.wgsl:121-162
+inline float level_obstacle(const efl_solid_obstacle& o, F2 x) {
+    switch (o.shape) {
+        case EFL_SHAPE_CIRCLE:
+            return wlength(x.x - o.transform[12], x.y - o.transform[13]) - o.values[0];
+        case EFL_SHAPE_RECTANGLE:
+            return level_rectangle(o, x);
+        case EFL_SHAPE_CAPSULE: {
+            F2 a = mat_xy(o.transform, o.values[0], o.values[1]);
+            F2 b = mat_xy(o.transform, o.values[2], o.values[3]);
+            return dist_segment(x, a, b) - o.values[4];
+        }
+        case EFL_SHAPE_TRIANGLE: {
+            F2 p0 = mat_xy(o.transform, o.values[0], o.values[1]);
+            F2 p1 = mat_xy(o.transform, o.values[2], o.values[3]);
+            F2 p2 = mat_xy(o.transform, o.values[4], o.values[5]);
+            float d0 = dist_segment(x, p0, p1), d1 = dist_segment(x, p1, p2), d2 = dist_segment(x, p2, p0);
+            float s0 = dist_sign(x, p0, p1), s1 = dist_sign(x, p1, p2), s2 = dist_sign(x, p2, p0);
+            float m = std::fmin(std::fmin(d0, d1), d2);
+            if (s0 > 0.0f && s1 > 0.0f && s2 > 0.0f) return -m;
+            return m;
+        }
+        default:
+            return LARGE_FLOAT_SOLID;
+    }
+}
+// update_solid.wgsl:111-119
+inline F2 velocity_at(const efl_solid_obstacle& o, F2 x) {
+    float rx = x.x - o.transform[12], ry = x.y - o.transform[13];
+    float w = o.angular_velocity;
+    return F2{o.linear_velocity[0] + -w * ry, o.linear_velocity[1] + w * rx};
+}
+// update_solid.wgsl:15-78 (dispatch_center)
+void k_update_solid(eflo_sim& s) {
+    const int nx = s.nx, ny = s.ny;
+    par_rows(0, s.cy(), [&](int y) {
+        for (int x = 0; x < s.cx(); ++x) {
+            F2 xc = to_world(s.U, (float)x, (float)y, nx, ny);
+            F2 xex = to_world(s.U, (float)x - 0.5f, (float)y - 0.0f, nx, ny);
+            F2 xey = to_world(s.U, (float)x - 0.0f, (float)y - 0.5f, nx, ny);
+            if (x == 0 || y == 0 || x == nx - 1 || y == ny - 1) {
+                s.ls_solid.st(x, y, 0.0f);
+                s.us.st(x, y, 0.0f);
+                s.vs.st(x, y, 0.0f);
+                s.solid_id.st(x, y, -1);
+                continue;
+            }
+            int tx = std::min(x, std::abs(nx - 1 - x)), ty = std::min(y, std::abs(ny - 1 - y));
+            float level = (float)std::min(tx, ty);
+            float u = 0.0f, v = 0.0f;
+            int32_t sid = -1;
+            for (const auto& o : s.obstacles) {
+                float lo = level_obstacle(o, xc);
+                if (lo < level) level = lo;
+                if (lo < 0.5f) sid = (int32_t)o.entity_id;
+                float lex = level_obstacle(o, xex);
+                if (lex < 0.5f) u = velocity_at(o, xex).x;
+                float ley = level_obstacle(o, xey);
+                if (ley < 0.5f) v = -velocity_at(o, xey).y;
+            }
+            s.us.st(x, y, u);
+            s.vs.st(x, y, v);
+            s.ls_solid.st(x, y, level);
+            s.solid_id.st(x, y, sid);
+        }
+    });
+}
+// update_area_fraction.wgsl:6-14
+void k_area_fraction(eflo_sim& s) {
+    par_rows(0, s.cy(), [&](int y) {
+        for (int x = 0; x < s.cx(); ++x) s.af.st(x, y, area_fractions(s.ls_solid, x, y));
+    });
+}
+
+// utils/coordinate.wgsl:51-81
+inline float interp_edge_x(const Tex<float>& u, float px, float py) {
+    int i = f2i(std::rint(px));
+    int j = f2i(std::floor(py));
+    float fi = px + 0.5f - (float)i;
+    float fj = py - (float)j;
+    float u00 = u.ld(i, j), u10 = u.ld(i + 1, j), u01 = u.ld(i, j + 1), u11 = u.ld(i + 1, j + 1);
+    return wmix(wmix(u00, u10, fi), wmix(u01, u11, fi), fj);
+}
+inline float interp_edge_y(const Tex<float>& v, float px, float py) {
+    int i = f2i(std::floor(px));
+    int j = f2i(std::rint(py));
+    float fi = px - (float)i;
+    float fj = py + 0.5f - (float)j;
+    float v00 = v.ld(i, j), v10 = v.ld(i + 1, j), v01 = v.ld(i, j + 1), v11 = v.ld(i + 1, j + 1);
+    return wmix(wmix(v00, v10, fi), wmix(v01, v11, fi), fj);
+}
+// utils/coordinate.wgsl:83-94
+inline F2 runge_kutta(const Tex<float>& u, const Tex<float>& v, float px, float py, float dt) {
+    float vx = interp_edge_x(u, px, py), vy = interp_edge_y(v, px, py);
+    float h = 0.5f * dt;
+    float mx = px - h * vx, my = py - h * vy;
+    float wx = interp_edge_x(u, mx, my), wy = interp_edge_y(v, mx, my);
+    return F2{px - dt * wx, py - dt * wy};
+}
+// advect_velocity.wgsl:11-52
+void k_advect(eflo_sim& s) {
+    const float dt = s.U.dt;
+    // advect_u: dispatch_x_major
+    par_rows(0, s.xrows(), [&](int y) {
+        for (int x = 0; x <= s.nx; ++x) {
+            float px = (float)x + -0.5f, py = (float)y + 0.0f;
+            F2 b = runge_kutta(s.u0, s.v0, px, py, dt);
+            float dimx = (float)s.u0.w, dimy = (float)s.u0.h;
+            bool inside = b.x >= 0.0f && b.y >= 0.0f && b.x <= dimx - 1.0f && b.y <= dimy - 1.0f;
+            s.u1.st(x, y, inside ? interp_edge_x(s.u0, b.x, b.y) : s.u0.ld(x, y));
+        }
+    });
+    // advect_v: dispatch_y_major
+    par_rows(0, s.ny + 1, [&](int y) {
+        for (int x = 0; x < s.ycols(); ++x) {
+            float px = (float)x + 0.0f, py = (float)y + -0.5f;
+            F2 b = runge_kutta(s.u0, s.v0, px, py, dt);
+            float dimx = (float)s.v0.w, dimy = (float)s.v0.h;
+            bool inside = b.x >= 0.0f && b.y >= 0.0f && b.x <= dimx - 1.0f && b.y <= dimy - 1.0f;
+            s.v1.st(x, y, inside ? interp_edge_y(s.v0, b.x, b.y) : s.v0.ld(x, y));
+        }
+    });
+}
+
+// apply_forces.wgsl:73-76
+inline float gaussian_2d(float x, float y, float x0, float y0, float sigma) {
+    float b = -1.0f / (2.0f * sigma * sigma);
+    float dx = x - x0, dy = y - y0;
+    return std::exp(b * (dx * dx + dy * dy));
+}
+// apply_forces.wgsl:17-71
+void k_apply_forces(eflo_sim& s) {
+    const Uniform& U = s.U;
+    par_rows(0, s.xrows(), [&](int y) {
+        for (int x = 0; x <= s.nx; ++x) {
+            F4 f = area_fractions(s.ls0, x, y);
+            float fs = s.af.ld(x, y).x;
+            if (f.x == 1.0f || fs == 0.0f) { s.u1.st(x, y, 0.0f); continue; }
+            float net = U.g[0];
+            for (size_t n = s.forces.size(); n > 0; --n) {
+                const efl_force& F = s.forces[n - 1];
+                net = net + F.force[0] * gaussian_2d((float)x, (float)y, F.position[0], F.position[1], 10.0f);
+            }
+            float uv = s.u1.ld(x, y);
+            s.u1.st(x, y, uv + net * U.dt / U.dx);
+        }
+    });
+    par_rows(0, s.ny + 1, [&](int y) {
+        for (int x = 0; x < s.ycols(); ++x) {
+            F4 f = area_fractions(s.ls0, x, y);
+            float fs = s.af.ld(x, y).z;
+            if (f.z == 1.0f || fs == 0.0f) { s.v1.st(x, y, 0.0f); continue; }
+            float net = U.g[1];
+            for (size_t n = s.forces.size(); n > 0; --n) {
+                const efl_force& F = s.forces[n - 1];
+                net = net + F.force[1] * gaussian_2d((float)x, (float)y, F.position[0], F.position[1], 10.0f);
+            }
+            float vv = s.v1.ld(x, y);
+            s.v1.st(x, y, vv + net * U.dt / U.dx);
+        }
+    });
+}
+
+// divergence.wgsl:16-42 (dispatch_center)
+void k_divergence(eflo_sim& s) {
+    const float dx = s.U.dx;
+    par_rows(0, s.cy(), [&](int y) {
+        for (int x = 0; x < s.cx(); ++x) {
+            F4 f = area_fractions(s.ls_solid, x, y);
+            float u_ij = s.u1.ld(x, y), u_ip = s.u1.ld(x + 1, y);
+            float v_ij = s.v1.ld(x, y), v_jp = s.v1.ld(x, y + 1);
+            float du_f = f.y * u_ip - f.x * u_ij;
+            float dv_f = f.w * v_jp - f.z * v_ij;
+            float us_m = s.us.ld(x, y), us_p = s.us.ld(x + 1, y);
+            float vs_m = s.vs.ld(x, y), vs_p = s.vs.ld(x, y + 1);
+            float du_s = (1.0f - f.y) * us_p - (1.0f - f.x) * us_m;
+            float dv_s = (1.0f - f.w) * vs_p - (1.0f - f.z) * vs_m;
+            float rhs = -(du_f + dv_f + du_s + dv_s) / dx;
+            s.div.st(x, y, rhs);
+        }
+    });
+}
+
+// projection/shaders/gauss_seidel.wgsl:44-88 (update_pressure).  With
+// T = float this is the reference's f32 arithmetic; with T = double the
+// same expression tree is evaluated in f64 from the f32 inputs.
+template <class T>
+inline T gs_update(const Tex<T>& p, const Tex<T>& b, const Tex<float>& ls, const Tex<F4>& af, const Uniform& U,
+                   float weight, float res_scale, int x, int y) {
+    float lij = ls.ld(x, y);
+    if (lij >= 0.0f) return T(0);
+    F4 f = af.ld(x, y);
+    bool fully_solid = f.x == 0.0f && f.y == 0.0f && f.z == 0.0f && f.w == 0.0f;
+    T p_old = p.ld(x, y);
+    if (fully_solid) return T(0);
+    T denom = T(0);
+    T dx = (T)(res_scale * U.dx);
+    T nume = dx * dx * (T)U.rho / (T)U.dt * b.ld(x, y);
+    static const int off[4][2] = {{-1, 0}, {1, 0}, {0, -1}, {0, 1}};
+    const T fv[4] = {(T)f.x, (T)f.y, (T)f.z, (T)f.w};
+    for (int i = 0; i < 4; ++i) {
+        int jx = x + off[i][0], jy = y + off[i][1];
+        if (jx >= 0 && jy >= 0 && jx < ls.w && jy < ls.h) {
+            float level = ls.ld(jx, jy);
+            if (level < 0.0f) {
+                denom += fv[i];
+                nume += fv[i] * p.ld(jx, jy);
+            } else {
+                denom += fv[i] * (T(1) - (T)level / (T)lij);
+            }
+        }
+    }
+    if (std::fabs(denom) < (T)1.0e-6f) return T(0);
+    T p_new = nume / denom;
+    T w = (T)weight;
+    return w * p_new + (T(1) - w) * p_old;
+}
+// gauss_seidel.wgsl:12-42: red = (x+y) odd, black = (x+y) even; dispatched
+// over ceil(dim/8)*8 with a dim guard, so every cell of the level.
+template <class T>
+void gs_half(Tex<T>& p, const Tex<T>& b, const Tex<float>& ls, const Tex<F4>& af, const Uniform& U, float weight,
+             float res_scale, int parity) {
+    par_rows(0, p.h, [&](int y) {
+        for (int x = (y + parity) & 1; x < p.w; x += 2) p.at(x, y) = gs_update(p, b, ls, af, U, weight, res_scale, x, y);
+    });
+}
+template <class T>
+void gs_iterations(Tex<T>& p, const Tex<T>& b, const Tex<float>& ls, const Tex<F4>& af, const Uniform& U,
+                   float weight, float res_scale, uint32_t n) {
+    for (uint32_t k = 0; k < n; ++k) {
+        gs_half(p, b, ls, af, U, weight, res_scale, 1);  // red
+        gs_half(p, b, ls, af, U, weight, res_scale, 0);  // black
+    }
+}
+
+// projection/shaders/residual.wgsl:12-57
+template <class T>
+inline T residual_at(const Tex<T>& xt, const Tex<T>& b, const Tex<float>& ls, const Tex<F4>& af, const Uniform& U,
+                     float res_scale, int x, int y, bool* counted) {
+    *counted = false;
+    float phi = ls.ld(x, y);
+    if (phi >= 0.0f) return T(0);
+    F4 f = af.ld(x, y);
+    if (f.x == 0.0f && f.y == 0.0f && f.z == 0.0f && f.w == 0.0f) return T(0);
+    *counted = true;
+    T xc = xt.ld(x, y);
+    T dx = (T)(U.dx * res_scale);
+    T factor = (T)U.dt / (T)U.rho / dx / dx;
+    T r = b.ld(x, y);
+    static const int off[4][2] = {{-1, 0}, {1, 0}, {0, -1}, {0, 1}};
+    const T fv[4] = {(T)f.x, (T)f.y, (T)f.z, (T)f.w};
+    for (int i = 0; i < 4; ++i) {
+        int jx = x + off[i][0], jy = y + off[i][1];
+        if (jx >= 0 && jy >= 0 && jx < ls.w && jy < ls.h) {
+            float pn = ls.ld(jx, jy);
+            if (pn < 0.0f) r -= fv[i] * (xc - xt.ld(jx, jy)) * factor;
+            else r -= fv[i] * (T(1) - (T)pn / (T)phi) * xc * factor;
+        }
+    }
+    return r;
+}
+template <class T>
+void k_residual(LevelT<T>& L, const Uniform& U, float res_scale) {
+    par_rows(0, L.ny, [&](int y) {
+        bool c;
+        for (int x = 0; x < L.nx; ++x) L.r.at(x, y) = residual_at(L.x, L.b, L.ls, L.af, U, res_scale, x, y, &c);
+    });
+}
+// restriction.wgsl:10-60
+template <class T>
+void k_restriction(const LevelT<T>& F, LevelT<T>& C) {
+    par_rows(0, C.ny, [&](int y) {
+        for (int x = 0; x < C.nx; ++x) {
+            int fx = 2 * x, fy = 2 * y;
+            T br = T(0.25) * (F.r.ld(fx, fy) + F.r.ld(fx, fy + 1) + F.r.ld(fx + 1, fy) + F.r.ld(fx + 1, fy + 1));
+            float ph0 = F.ls.ld(fx, fy), ph1 = F.ls.ld(fx, fy + 1), ph2 = F.ls.ld(fx + 1, fy),
+                  ph3 = F.ls.ld(fx + 1, fy + 1);
+            float pr = ph0;
+            if (std::fabs(ph1) < std::fabs(pr)) pr = ph1;
+            if (std::fabs(ph2) < std::fabs(pr)) pr = ph2;
+            if (std::fabs(ph3) < std::fabs(pr)) pr = ph3;
+            F4 a0 = F.af.ld(fx, fy), a1 = F.af.ld(fx + 1, fy), a2 = F.af.ld(fx, fy + 1), a3 = F.af.ld(fx + 1, fy + 1);
+            F4 fr{0.5f * (a0.x + a2.x), 0.5f * (a1.y + a3.y), 0.5f * (a0.z + a1.z), 0.5f * (a2.w + a3.w)};
+            C.b.st(x, y, br);
+            C.ls.st(x, y, pr);
+            C.af.st(x, y, fr);
+            C.x.st(x, y, T(0));
+        }
+    });
+}
+// prolongation.wgsl:5-34
+template <class T>
+void k_prolongation(LevelT<T>& F, const LevelT<T>& C) {
+    par_rows(0, C.ny, [&](int y) {
+        for (int x = 0; x < C.nx; ++x) {
+            T corr = C.x.ld(x, y);
+            static const int off[4][2] = {{0, 0}, {1, 0}, {0, 1}, {1, 1}};
+            for (int i = 0; i < 4; ++i) {
+                int fx = 2 * x + off[i][0], fy = 2 * y + off[i][1];
+                if (F.ls.ld(fx, fy) < 0.0f && F.x.in(fx, fy)) F.x.at(fx, fy) = corr + F.x.at(fx, fy);
+            }
+        }
+    });
+}
+// multi_grid.rs:390-475; smoother weight 1.0 and resolution_scale 2^i (multi_grid.rs:268-270)
+template <class T>
+void v_cycle(std::vector<LevelT<T>>& mg, const Uniform& U, size_t i, const efl_projection& P) {
+    LevelT<T>& L = mg[i];
+    float scale = (float)(1u << i);
+    if (i == mg.size() - 1) {
+        gs_iterations(L.x, L.b, L.ls, L.af, U, 1.0f, scale, P.mg_coarsest);
+        return;
+    }
+    gs_iterations(L.x, L.b, L.ls, L.af, U, 1.0f, scale, P.mg_pre);
+    k_residual(L, U, scale);
+    k_restriction(L, mg[i + 1]);
+    v_cycle(mg, U, i + 1, P);
+    k_prolongation(L, mg[i + 1]);
+    gs_iterations(L.x, L.b, L.ls, L.af, U, 1.0f, scale, P.mg_post);
+}
+
+// shaders/jacobi_iteration.wgsl:39-91 (levelset_solid fractions = af)
+inline float jacobi_update(const Tex<float>& p, const eflo_sim& s, int x, int y) {
+    float lij = s.ls0.ld(x, y);
+    if (lij >= 0.0f) return 0.0f;
+    F4 f = area_fractions(s.ls_solid, x, y);
+    bool fully_solid = f.x == 0.0f && f.y == 0.0f && f.z == 0.0f && f.w == 0.0f;
+    if (fully_solid) return p.ld(x, y);
+    float p_m = p.ld(x - 1, y), p_p = p.ld(x + 1, y), p_jm = p.ld(x, y - 1), p_jp = p.ld(x, y + 1);
+    float l_m = s.ls0.ld(x - 1, y), l_p = s.ls0.ld(x + 1, y), l_jm = s.ls0.ld(x, y - 1), l_jp = s.ls0.ld(x, y + 1);
+    float ff_m = std::fmin(0.0f, l_m / lij), ff_p = std::fmin(0.0f, l_p / lij);
+    float ff_jm = std::fmin(0.0f, l_jm / lij), ff_jp = std::fmin(0.0f, l_jp / lij);
+    float coef = f.x * (1.0f - ff_m) + f.y * (1.0f - ff_p) + f.z * (1.0f - ff_jm) + f.w * (1.0f - ff_jp);
+    if (std::fabs(coef) < 1.0e-6f) return 0.0f;
+    float div_ij = s.div.ld(x, y);
+    float factor = s.U.dx * s.U.rho / s.U.dt;
+    auto step0 = [](float v) { return v >= 0.0f ? 1.0f : 0.0f; };
+    float d00 = f.x * step0(ff_m) * p_m;
+    float d10 = f.y * step0(ff_p) * p_p;
+    float d01 = f.z * step0(ff_jm) * p_jm;
+    float d11 = f.w * step0(ff_jp) * p_jp;
+    return (d00 + d10 + d01 + d11 - factor * div_ij) / coef;
+}
+void k_jacobi(eflo_sim& s) {  // projection.rs:135-143, dispatch_center
+    for (int it = 0; it < 50; ++it) {
+        par_rows(0, s.cy(), [&](int y) {
+            for (int x = 0; x < s.cx(); ++x) s.p1.st(x, y, jacobi_update(s.p0, s, x, y));
+        });
+        par_rows(0, s.cy(), [&](int y) {
+            for (int x = 0; x < s.cx(); ++x) s.p0.st(x, y, jacobi_update(s.p1, s, x, y));
+        });
+    }
+}
+
+// ||b - A x||^2 and ||b||^2 at level 0 over cells with phi < 0 that are
+// not fully solid (FP64 accumulation, per-row partials summed in order).
+template <class T>
+void residual_norms(const Tex<T>& xt, const Tex<T>& b, const Tex<float>& ls, const Tex<F4>& af, const Uniform& U,
+                    double* rr, double* bb) {
+    const int W = ls.w, H = ls.h;
+    std::vector<double> pr(H, 0.0), pb(H, 0.0);
+    par_rows(0, H, [&](int y) {
+        double sr = 0.0, sb = 0.0;
+        for (int x = 0; x < W; ++x) {
+            bool c;
+            T r = residual_at(xt, b, ls, af, U, 1.0f, x, y, &c);
+            if (c) {
+                double bv = (double)b.ld(x, y);
+                sr += (double)r * (double)r;
+                sb += bv * bv;
+            }
+        }
+        pr[y] = sr;
+        pb[y] = sb;
+    });
+    double R = 0.0, B = 0.0;
+    for (int y = 0; y < H; ++y) { R += pr[y]; B += pb[y]; }
+    *rr = R;
+    *bb = B;
+}
+double rel_from(double R, double B) {
+    if (B > 0.0) return std::sqrt(R) / std::sqrt(B);
+    return R > 0.0 ? std::numeric_limits<double>::infinity() : 0.0;
+}
+void residual_norms_f32(const eflo_sim& s, double* R, double* B) {
+    residual_norms(s.p0, s.div, s.ls0, s.af, s.U, R, B);
+}
+
+void mg_copy_level0(eflo_sim& s) {
+    Level& L = s.mg[0];
+    L.x = s.p0;
+    L.b = s.div;
+    L.ls = s.ls0;
+    L.af = s.af;
+}
+// FP64 iterate of the tolerance-driven solve: x = p0, b = div (widened).
+void mg64_load_level0(eflo_sim& s) {
+    Level64& L = s.mg64[0];
+    for (size_t i = 0; i < L.x.a.size(); ++i) {
+        L.x.a[i] = (double)s.p0.a[i];
+        L.b.a[i] = (double)s.div.a[i];
+    }
+    L.ls = s.ls0;
+    L.af = s.af;
+}
+void mg64_store_p0(eflo_sim& s) {
+    const Level64& L = s.mg64[0];
+    for (size_t i = 0; i < L.x.a.size(); ++i) s.p0.a[i] = (float)L.x.a[i];
+}
+
+// projection.rs:89-164.  tolerance > 0 (an extension) solves to
+// ||b - A p|| / ||b|| <= tolerance with an FP64 iterate: the f32 pressure
+// cannot represent a solution that accurate when the hydrostatic pressure
+// dominates.  p0 receives the f32 rounding of the converged iterate.
+efl_status k_projection(eflo_sim& s, efl_step_stats* st) {
+    const efl_projection& P = s.cfg.projection;
+    efl_status ret = EFL_OK;
+    uint32_t iters = 0;
+    int conv = 1;
+    double r0 = -1.0, r1 = -1.0;
+    if (P.method == EFL_PROJECTION_JACOBI) {
+        k_jacobi(s);
+        iters = 50;
+    } else if (P.tolerance <= 0.0f) {
+        if (P.method == EFL_PROJECTION_GAUSS_SEIDEL) {
+            gs_iterations(s.p0, s.div, s.ls0, s.af, s.U, P.sor_weight, 1.0f, P.gs_iterations);
+            iters = P.gs_iterations;
+        } else {
+            mg_copy_level0(s);  // level 0 aliases p0/div/phi0/af (multi_grid.rs:104-107)
+            v_cycle(s.mg, s.U, 0, P);
+            iters = 1;
+            s.p0 = s.mg[0].x;
+        }
+    } else {
+        mg64_load_level0(s);
+        Level64& L = s.mg64[0];
+        auto rel = [&]() {
+            double R, B;
+            residual_norms(L.x, L.b, L.ls, L.af, s.U, &R, &B);
+            return rel_from(R, B);
+        };
+        double r = rel();
+        r0 = r;
+        if (P.method == EFL_PROJECTION_GAUSS_SEIDEL) {
+            uint32_t chk = std::max<uint32_t>(1, P.check_interval);
+            while (!(r <= (double)P.tolerance) && iters < P.max_iterations) {
+                uint32_t n = std::min(chk, P.max_iterations - iters);
+                gs_iterations(L.x, L.b, L.ls, L.af, s.U, P.sor_weight, 1.0f, n);
+                iters += n;
+                r = rel();
+            }
+        } else {
+            while (!(r <= (double)P.tolerance) && iters < P.max_iterations) {
+                v_cycle(s.mg64, s.U, 0, P);
+                ++iters;
+                r = rel();
+            }
+        }
+        r1 = r;
+        conv = r <= (double)P.tolerance;
+        mg64_store_p0(s);
+    }
+    if (!conv) ret = EFL_NOT_CONVERGED;
+    if (st) {
+        st->pressure_iterations = iters;
+        st->converged = conv;
+        st->residual = r1;
+        st->residual_initial = r0;
+    }
+    return ret;
+}
+
+// solve_velocity_u.wgsl:15-47 / solve_velocity_v.wgsl:15-45
+void k_solve_velocity(eflo_sim& s) {
+    const float factor = s.U.dt / (s.U.dx * s.U.rho);
+    par_rows(0, s.xrows(), [&](int y) {
+        for (int x = 0; x <= s.nx; ++x) {
+            float fr = s.af.ld(x, y).x;
+            if (fr == 0.0f) { s.u0.st(x, y, s.us.ld(x, y)); continue; }
+            float pij = s.p0.ld(x, y), pim = s.p0.ld(x - 1, y);
+            float lp = s.ls0.ld(x, y), lm = s.ls0.ld(x - 1, y);
+            if (lm >= 0.0f && lp < 0.0f) pim = lm / lp * pij;
+            else if (lm < 0.0f && lp >= 0.0f) pij = lp / lm * pim;
+            else if (lm >= 0.0f && lp >= 0.0f) { s.u0.st(x, y, 0.0f); continue; }
+            float u = s.u1.ld(x, y);
+            s.u0.st(x, y, u - factor * (pij - pim));
+        }
+    });
+    par_rows(0, s.ny + 1, [&](int y) {
+        for (int x = 0; x < s.ycols(); ++x) {
+            float fr = s.af.ld(x, y).z;
+            if (fr == 0.0f) { s.v0.st(x, y, s.vs.ld(x, y)); continue; }
+            float pij = s.p0.ld(x, y), pjm = s.p0.ld(x, y - 1);
+            float lp = s.ls0.ld(x, y), lm = s.ls0.ld(x, y - 1);
+            if (lm >= 0.0f && lp < 0.0f) pjm = lm / lp * pij;
+            else if (lm < 0.0f && lp >= 0.0f) pij = lp / lm * pjm;
+            float v = s.v1.ld(x, y);
+            s.v0.st(x, y, v - factor * (pij - pjm));
+        }
+    });
+}
+
+// extrapolate/initialize_{u,v}_valid.wgsl:6-30
+void k_init_valid(eflo_sim& s) {
+    par_rows(0, s.xrows(), [&](int y) {
+        for (int x = 0; x <= s.nx; ++x) {
+            float c0 = s.ls0.ld(x - 1, y - 1), c1 = s.ls0.ld(x, y - 1), c2 = s.ls0.ld(x - 1, y),
+                  c3 = s.ls0.ld(x, y), c4 = s.ls0.ld(x - 1, y + 1), c5 = s.ls0.ld(x, y + 1);
+            float vm = 0.25f * (c0 + c1 + c2 + c3);
+            float vp = 0.25f * (c2 + c3 + c4 + c5);
+            s.u_valid_in.st(x, y, area_fraction(vm, vp) > 0.0f ? 0 : 1);
+        }
+    });
+    par_rows(0, s.ny + 1, [&](int y) {
+        for (int x = 0; x < s.ycols(); ++x) {
+            float c0 = s.ls0.ld(x - 1, y - 1), c1 = s.ls0.ld(x - 1, y), c2 = s.ls0.ld(x, y - 1),
+                  c3 = s.ls0.ld(x, y), c4 = s.ls0.ld(x + 1, y - 1), c5 = s.ls0.ld(x + 1, y);
+            float vm = 0.25f * (c0 + c1 + c2 + c3);
+            float vp = 0.25f * (c2 + c3 + c4 + c5);
+            s.v_valid_in.st(x, y, area_fraction(vm, vp) > 0.0f ? 0 : 1);
+        }
+    });
+}
+// extrapolate/extrapolate_{u,v}.wgsl:5-63 (one dispatch over [x0,x1) x [y0,y1))
+void extrap_pass(Tex<float>& f, const Tex<int32_t>& vin, Tex<int32_t>& vout, int x1, int y1) {
+    const int dx_ = vin.w, dy_ = vin.h;
+    par_rows(0, y1, [&](int y) {
+        for (int x = 0; x < x1; ++x) {
+            if (vin.ld(x, y) == 1) { vout.st(x, y, 1); continue; }
+            int count = 0;
+            float nu = 0.0f;
+            if (x + 1 < dx_ && y < dy_ && vin.ld(x + 1, y) == 1) { nu += f.ld(x + 1, y); count += 1; }
+            if (x - 1 > 0 && y > 0 && vin.ld(x - 1, y) == 1) { nu += f.ld(x - 1, y); count += 1; }
+            if (x < dx_ && y + 1 < dy_ && vin.ld(x, y + 1) == 1) { nu += f.ld(x, y + 1); count += 1; }
+            if (x > 0 && y - 1 > 0 && vin.ld(x, y - 1) == 1) { nu += f.ld(x, y - 1); count += 1; }
+            if (count > 0) {
+                nu /= (float)count;
+                f.st(x, y, nu);
+                vout.st(x, y, 1);
+            } else {
+                vout.st(x, y, 0);
+            }
+        }
+    });
+}
+// render_node.rs:540-608
+void k_extrapolate(eflo_sim& s) {
+    k_init_valid(s);
+    for (int k = 0; k < 10 / 2; ++k) {
+        extrap_pass(s.u0, s.u_valid_in, s.u_valid_out, s.nx + 1, s.xrows());
+        extrap_pass(s.u0, s.u_valid_out, s.u_valid_in, s.nx + 1, s.xrows());
+        extrap_pass(s.v0, s.v_valid_in, s.v_valid_out, s.ycols(), s.ny + 1);
+        extrap_pass(s.v0, s.v_valid_out, s.v_valid_in, s.ycols(), s.ny + 1);
+    }
+}
+
+// advect_levelset.wgsl:49-61
+inline float cubic1d(float y0, float y1, float y2, float y3, float t) {
+    float d1 = 0.5f * (y2 - y0);
+    float d2 = 0.5f * (y3 - y1);
+    float a0 = y1, a1 = d1;
+    float a2 = -2.0f * d1 - d2 + 3.0f * (y2 - y1);
+    float a3 = d1 + d2 - 2.0f * (y2 - y1);
+    return a3 * t * t * t + a2 * t * t + a1 * t + a0;
+}
+inline float cubic1d_x(const Tex<float>& t, int bx, int by, float tx) {
+    return cubic1d(t.ld(bx - 1, by), t.ld(bx, by), t.ld(bx + 1, by), t.ld(bx + 2, by), tx);
+}
+// advect_levelset.wgsl:11-34 with CUBIC (advect_levelset.rs:62)
+void k_advect_levelset(eflo_sim& s) {
+    const float dt = s.U.dt;
+    par_rows(0, s.cy(), [&](int y) {
+        for (int x = 0; x < s.cx(); ++x) {
+            F2 xn = runge_kutta(s.u0, s.v0, (float)x, (float)y, dt);
+            xn.x = fclamp(xn.x, 0.0f, (float)s.nx - 1.0f);
+            xn.y = fclamp(xn.y, 0.0f, (float)s.ny - 1.0f);
+            int bx = f2i(xn.x), by = f2i(xn.y);
+            float tx = xn.x - (float)bx, ty = xn.y - (float)by;
+            float y0 = cubic1d_x(s.ls0, bx, by - 1, tx), y1 = cubic1d_x(s.ls0, bx, by, tx);
+            float y2 = cubic1d_x(s.ls0, bx, by + 1, tx), y3 = cubic1d_x(s.ls0, bx, by + 2, tx);
+            float nl = cubic1d(y0, y1, y2, y3, ty);
+            if (std::fabs(nl) < 1000.0f) s.ls1.st(x, y, nl);
+        }
+    });
+}
+
+// update_fluid_source.wgsl:89-107
+inline float level_aabb(float hx, float hy, float cx, float cy, float px, float py) {
+    float level = LARGE_FLOAT_SOURCE;
+    float dx = std::fabs(cx - px) - hx, dy = std::fabs(cy - py) - hy;
+    bool ix = dx < 0.0f, iy = dy < 0.0f;
+    if (ix) level = iy ? std::fmax(dx, dy) : dy;
+    else level = iy ? dx : wlength(dx, dy);
+    return level;
+}
+// update_fluid_source.wgsl:72-87
+inline float level_source(const efl_source& d, float px, float py) {
+    switch (d.shape) {
+        case EFL_SOURCE_CIRCLE: return wlength(d.center[0] - px, d.center[1] - py) - d.data[0];
+        case EFL_SOURCE_AABB: return level_aabb(d.data[0], d.data[1], d.center[0], d.center[1], px, py);
+        default: return 0.0f;
+    }
+}
+// update_fluid_source.wgsl:30-70 (dispatch_center).  Faces written by two
+// invocations take the raster-last writer's value.
+void k_fluid_source(eflo_sim& s, const std::vector<efl_source>& src) {
+    const int W = s.cx(), H = s.cy();
+    std::vector<uint8_t> upd((size_t)W * H, 0);
+    std::vector<F2> vel((size_t)W * H, F2{0, 0});
+    const float dimx = (float)s.nx, dimy = (float)s.ny;
+    par_rows(0, H, [&](int y) {
+        for (int x = 0; x < W; ++x) {
+            float uvx = (float)(uint32_t)x / dimx, uvy = (float)(uint32_t)y / dimy;
+            float ndcx = uvx * 2.0f + -1.0f, ndcy = uvy * -2.0f + 1.0f;  // bevy uv_to_ndc
+            float px = 0.5f * dimx * ndcx, py = 0.5f * dimy * ndcy;
+            float nl = s.ls1.ld(x, y);
+            float vx = 0.0f, vy = 0.0f;
+            bool has_source = false, vu = false;
+            for (const auto& d : src) {
+                float sdf = level_source(d, px, py);
+                if (d.mode == EFL_SOURCE_MODE_SOURCE) {
+                    nl = std::fmin(nl, sdf);
+                    has_source = true;
+                    if (sdf < 0.0f) { vx = vx + d.velocity[0]; vy = vy + d.velocity[1]; vu = true; }
+                } else {
+                    if (!has_source) nl = std::fmax(nl, -sdf);
+                }
+            }
+            s.ls1.st(x, y, nl);
+            upd[(size_t)y * W + x] = vu;
+            vel[(size_t)y * W + x] = F2{vx, vy};
+        }
+    });
+    for (int y = 0; y < H; ++y)
+        for (int x = 0; x < W; ++x) {
+            size_t i = (size_t)y * W + x;
+            if (!upd[i]) continue;
+            s.u0.st(x, y, vel[i].x);
+            s.u0.st(x + 1, y, vel[i].x);
+            s.v0.st(x, y, vel[i].y);
+            s.v0.st(x, y + 1, vel[i].y);
+        }
+}
+
+// jump_flooding/initialize.wgsl:8-41
+void k_jfa_init(eflo_sim& s) {
+    Tex<F2>& sd = s.seeds[0];
+    par_rows(0, s.cy(), [&](int y) {
+        for (int x = 0; x < s.cx(); ++x) {
+            float md = 10.0f;
+            F2 seed{-1.0f, -1.0f};
+            float level = s.ls1.ld(x, y);
+            for (int i = -1; i <= 1; ++i)
+                for (int j = -1; j <= 1; ++j) {
+                    if (i == 0 && j == 0) continue;
+                    int nx_ = x + i, ny_ = y + j;
+                    if (nx_ < 0 || ny_ < 0 || nx_ >= s.nx || ny_ >= s.ny) continue;
+                    float nl = s.ls1.ld(nx_, ny_);
+                    if (nl >= 0.0f && !(level >= 0.0f)) {
+                        float t = level / (level - nl);
+                        if (std::fabs(t) < md) {
+                            md = std::fabs(t);
+                            seed = F2{(float)x + t * (float)i, (float)y + t * (float)j};
+                        }
+                    }
+                }
+            sd.st(x, y, seed);
+        }
+    });
+}
+inline bool valid_seed(F2 s) { return s.x != -1.0f && s.y != -1.0f; }
+// jump_flooding/iterate.wgsl:18-56
+void k_jfa_iterate(const Tex<F2>& in, Tex<F2>& out, int step, int cx, int cy) {
+    par_rows(0, cy, [&](int y) {
+        for (int x = 0; x < cx; ++x) {
+            F2 cur = in.ld(x, y), best = cur;
+            float bd = 1e10f;
+            if (valid_seed(cur)) bd = wlength(cur.x - (float)x, cur.y - (float)y);
+            for (int i = -1; i <= 1; ++i)
+                for (int j = -1; j <= 1; ++j) {
+                    if (i == 0 && j == 0) continue;
+                    int nx_ = x + i * step, ny_ = y + j * step;
+                    if (nx_ < 0 || ny_ < 0 || nx_ >= in.w || ny_ >= in.h) continue;
+                    F2 ns = in.ld(nx_, ny_);
+                    if (!valid_seed(ns)) continue;
+                    float cd = wlength(ns.x - (float)x, ns.y - (float)y);
+                    if (cd < bd) { best = ns; bd = cd; }
+                }
+            out.st(x, y, best);
+        }
+    });
+}
+// jump_flooding/calculate_sdf.wgsl:9-23
+void k_jfa_sdf(eflo_sim& s, const Tex<F2>& sd) {
+    par_rows(0, s.cy(), [&](int y) {
+        for (int x = 0; x < s.cx(); ++x) {
+            F2 seed = sd.ld(x, y);
+            float sdf = wlength(seed.x - (float)x, seed.y - (float)y);
+            float level = s.ls1.ld(x, y);
+            float sg = level < 0.0f ? -1.0f : 1.0f;
+            s.ls0.st(x, y, sdf * sg);
+        }
+    });
+}
+// jump_flooding.rs:201-209: steps 2^max_power .. 1, max_power = floor(log2(max(nx,ny)) - 1)
+std::vector<int> jfa_steps(int nx, int ny) {
+    int mp = (int)std::floor(std::log2((float)std::max(nx, ny)) - 1.0f);
+    std::vector<int> st;
+    uint32_t step = 1u << (mp + 1);
+    for (int k = 0; k < mp + 1; ++k) { step /= 2; st.push_back((int)step); }
+    return st;
+}
+void k_jfa(eflo_sim& s) {  // reinitialize_levelset.rs:170-206
+    k_jfa_init(s);
+    int src = 0, dst = 1;
+    for (int step : jfa_steps(s.nx, s.ny)) {
+        k_jfa_iterate(s.seeds[src], s.seeds[dst], step, s.cx(), s.cy());
+        std::swap(src, dst);
+    }
+    s.seeds_final = src;
+    k_jfa_sdf(s, s.seeds[src]);
+}
+
+// fast_iterative_method/initialize.wgsl:10-40
+void k_fim_init(eflo_sim& s) {
+    par_rows(0, s.cy(), [&](int y) {
+        for (int x = 0; x < s.cx(); ++x) {
+            float level = s.ls1.ld(x, y);
+            static const int off[4][2] = {{-1, 0}, {1, 0}, {0, -1}, {0, 1}};
+            bool src = false;
+            for (int i = 0; i < 4 && !src; ++i) {
+                int jx = x + off[i][0], jy = y + off[i][1];
+                if (jx >= 0 && jy >= 0 && jx < s.nx && jy < s.ny) {
+                    if (level * s.ls1.ld(jx, jy) <= 0.0f) src = true;
+                }
+            }
+            if (src) { s.ls0.st(x, y, level); s.labels0.st(x, y, LABEL_SOURCE); }
+            else { s.ls0.st(x, y, wsign(level) * FIM_LARGE); s.labels0.st(x, y, LABEL_NONE); }
+        }
+    });
+}
+// fast_iterative_method/initialize_active_label.wgsl:8-40
+void k_fim_active(eflo_sim& s) {
+    par_rows(0, s.cy(), [&](int y) {
+        for (int x = 0; x < s.cx(); ++x) {
+            uint32_t l = s.labels0.ld(x, y);
+            if (l == LABEL_SOURCE) { s.labels.st(x, y, LABEL_SOURCE); continue; }
+            static const int off[4][2] = {{-1, 0}, {1, 0}, {0, -1}, {0, 1}};
+            uint32_t out = LABEL_NONE;
+            for (int i = 0; i < 4; ++i) {
+                int jx = x + off[i][0], jy = y + off[i][1];
+                if (jx >= 0 && jy >= 0 && jx < s.nx && jy < s.ny && s.labels0.ld(jx, jy) == LABEL_SOURCE) {
+                    out = LABEL_ACTIVE;
+                    break;
+                }
+            }
+            s.labels.st(x, y, out);
+        }
+    });
+}
+// fast_iterative_method/update.wgsl:73-83
+inline float abs_get_phi(const Tex<float>& p, int x, int y) {
+    if (x < 0 || y < 0 || x >= p.w || y >= p.h) return FIM_LARGE;
+    return std::fabs(p.ld(x, y));
+}
+// fast_iterative_method/update.wgsl:56-71
+inline float solve_quadratic_2d(const Tex<float>& p, int x, int y) {
+    float xm = std::fmin(abs_get_phi(p, x - 1, y), abs_get_phi(p, x + 1, y));
+    float ym = std::fmin(abs_get_phi(p, x, y - 1), abs_get_phi(p, x, y + 1));
+    float d = xm - ym;
+    if (d > SQRT2_F) return ym + 1.0f;
+    if (d < -SQRT2_F) return xm + 1.0f;
+    return 0.5f * (xm + ym + std::sqrt(2.0f - d * d));
+}
+// Deterministic resolution of fast_iterative_method/update.wgsl:13-54.
+// The reference writes neighbours' phi and labels from inside one dispatch
+// (a data race).  Both the oracle and the CUDA library run it as two
+// phases per iteration:
+//   A (every ACTIVE cell, reading the iteration-start phi S): q = solve(S)*sign(p);
+//     the cell keeps q; it is marked converged if !(|p-q| > eps).
+//   B (every cell whose label was NONE): if any 4-neighbour converged in A,
+//     the writer is the raster-last such neighbour (down, right, left, up);
+//     q_c = solve(phi after A); if |phi_c| > q_c the cell takes q_c*sign(writer)
+//     and becomes ACTIVE.  Converged cells become NONE.
+void fim_update_two_phase(eflo_sim& s) {
+    Tex<float>& S = s.ls0;
+    Tex<float>& T = s.phiT;
+    Tex<uint32_t>& L = s.labels;
+    Tex<uint32_t>& LT = s.labelsT;
+    const int W = s.cx(), H = s.cy();
+    par_rows(0, H, [&](int y) {  // phase A
+        for (int x = 0; x < W; ++x) {
+            uint32_t l = L.ld(x, y);
+            float p = S.ld(x, y);
+            if (l != LABEL_ACTIVE) { T.st(x, y, p); LT.st(x, y, l); continue; }
+            float q = solve_quadratic_2d(S, x, y) * wsign(p);
+            T.st(x, y, q);
+            LT.st(x, y, (std::fabs(p - q) > FIM_EPS) ? LABEL_ACTIVE : LABEL_CONVERGED);
+        }
+    });
+    par_rows(0, H, [&](int y) {  // phase B
+        for (int x = 0; x < W; ++x) {
+            uint32_t l = LT.ld(x, y);
+            float t = T.ld(x, y);
+            if (l == LABEL_NONE) {
+                // writers in raster-last order: (x,y+1), (x+1,y), (x-1,y), (x,y-1)
+                static const int wo[4][2] = {{0, 1}, {1, 0}, {-1, 0}, {0, -1}};
+                int wx = -1, wy = -1;
+                for (int k = 0; k < 4; ++k) {
+                    int ax = x + wo[k][0], ay = y + wo[k][1];
+                    if (ax >= 0 && ay >= 0 && ax < W && ay < H && LT.ld(ax, ay) == LABEL_CONVERGED) {
+                        wx = ax; wy = ay;
+                        break;
+                    }
+                }
+                if (wx >= 0) {
+                    float pn = std::fabs(t);
+                    float qn = solve_quadratic_2d(T, x, y);
+                    if (pn > qn) {
+                        S.st(x, y, qn * wsign(T.ld(wx, wy)));
+                        L.st(x, y, LABEL_ACTIVE);
+                        continue;
+                    }
+                }
+                S.st(x, y, t);
+                L.st(x, y, LABEL_NONE);
+            } else {
+                S.st(x, y, t);
+                L.st(x, y, l == LABEL_CONVERGED ? LABEL_NONE : l);
+            }
+        }
+    });
+}
+// Literal single-invocation-at-a-time raster execution of update.wgsl:13-54.
+void fim_update_serial(eflo_sim& s) {
+    Tex<float>& phi = s.ls0;
+    Tex<uint32_t>& lab = s.labels;
+    for (int y = 0; y < s.cy(); ++y)
+        for (int x = 0; x < s.cx(); ++x) {
+            if (lab.ld(x, y) != LABEL_ACTIVE) continue;
+            float p = phi.ld(x, y);
+            float q = solve_quadratic_2d(phi, x, y) * wsign(p);
+            phi.st(x, y, q);
+            if (std::fabs(p - q) > FIM_EPS) continue;
+            lab.st(x, y, LABEL_NONE);
+            static const int off[4][2] = {{-1, 0}, {1, 0}, {0, -1}, {0, 1}};
+            for (int i = 0; i < 4; ++i) {
+                int jx = x + off[i][0], jy = y + off[i][1];
+                if (jx >= 0 && jy >= 0 && jx < s.nx && jy < s.ny) {
+                    uint32_t ln = lab.ld(jx, jy);
+                    if (ln != LABEL_ACTIVE && ln != LABEL_SOURCE) {
+                        float pn = std::fabs(phi.ld(jx, jy));
+                        float qn = solve_quadratic_2d(phi, jx, jy);
+                        if (pn > qn) {
+                            phi.st(jx, jy, qn * wsign(p));
+                            lab.st(jx, jy, LABEL_ACTIVE);
+                        }
+                    }
+                }
+            }
+        }
+}
+void k_fim(eflo_sim& s) {  // reinitialize_levelset.rs:207-241
+    k_fim_init(s);
+    k_fim_active(s);
+    for (uint32_t k = 0; k < s.cfg.reinit.fim_iterations; ++k) {
+        if (s.fim_serial) fim_update_serial(s);
+        else fim_update_two_phase(s);
+    }
+}
+void k_reinit(eflo_sim& s) {
+    if (s.cfg.reinit.method == EFL_REINIT_JUMP_FLOODING) k_jfa(s);
+    else k_fim(s);
+}
+
+// levelset_gradient.wgsl:4-21
+void k_gradient(eflo_sim& s) {
+    par_rows(0, s.cy(), [&](int y) {
+        for (int x = 0; x < s.cx(); ++x) {
+            if (x == 0 || y == 0 || x >= s.nx || y >= s.ny) continue;
+            F2 g{0.5f * (s.ls0.ld(x + 1, y) - s.ls0.ld(x - 1, y)), 0.5f * (s.ls0.ld(x, y + 1) - s.ls0.ld(x, y - 1))};
+            s.grad.st(x, y, g);
+        }
+    });
+}
+
+// solid_obstacle.wgsl:67-89
+inline F2 center_of_mass(const efl_solid_obstacle& o) {
+    switch (o.shape) {
+        case EFL_SHAPE_CIRCLE:
+        case EFL_SHAPE_RECTANGLE:
+        case EFL_SHAPE_CAPSULE:
+            return F2{o.transform[12], o.transform[13]};
+        case EFL_SHAPE_TRIANGLE: {
+            float lx = (o.values[0] + o.values[2] + o.values[4]) / 3.0f;
+            float ly = (o.values[1] + o.values[3] + o.values[5]) / 3.0f;
+            return mat_xy(o.transform, lx, ly);
+        }
+        default:
+            return F2{0.0f, 0.0f};
+    }
+}
+// fixed_point_conversion.wgsl:2-13
+inline int32_t f32_to_i32(float v) { return f2i(v * 10.0f); }
+inline float i32_to_f32(int32_t v) { return (float)v * 0.1f; }
+// sample_forces.wgsl:20-53 + accumulate_forces.wgsl:16-32; bins zeroed
+// every frame (fluid_to_solid.rs:211-229).
+void k_solid_forces(eflo_sim& s) {
+    std::memset(s.bins, 0, sizeof(s.bins));
+    const Uniform& U = s.U;
+    efl_solid_obstacle zero_ob;
+    std::memset(&zero_ob, 0, sizeof(zero_ob));
+    // integer atomics are order-independent: accumulate row partials
+    for (int y = 0; y < s.cy(); ++y)
+        for (int x = 0; x < s.cx(); ++x) {
+            F4 f = area_fractions(s.ls_solid, x, y);
+            if (f.x == 0.0f && f.y == 0.0f && f.z == 0.0f && f.w == 0.0f) continue;
+            int32_t id = s.solid_id.ld(x, y);
+            if (id == -1) continue;
+            float p = s.p0.ld(x, y);
+            float fx = -(f.y - f.x) * p * U.dx;
+            float fy = -(f.w - f.z) * p * U.dx;
+            const efl_solid_obstacle& o =
+                (id >= 0 && (uint32_t)id < s.obstacles.size()) ? s.obstacles[id] : zero_ob;
+            F2 c = center_of_mass(o);
+            float uvx = (float)x / U.size[0], uvy = (float)y / U.size[1];
+            float xx = (uvx - 0.5f) * U.size[0], yy = (-uvy + 0.5f) * U.size[1];
+            F2 w = mat_xy(U.m, xx, yy);
+            float rx = w.x - c.x, ry = w.y - c.y;
+            float torque = rx * fy - ry * fx;
+            if (id >= 0 && id < EFL_MAX_SOLIDS) {
+                s.bins[0][id] += f32_to_i32(fx);
+                s.bins[1][id] += f32_to_i32(fy);
+                s.bins[2][id] += f32_to_i32(torque);
+            }
+        }
+    for (int i = 0; i < EFL_MAX_SOLIDS; ++i) {
+        s.out_forces[i].force[0] = i32_to_f32(s.bins[0][i]);
+        s.out_forces[i].force[1] = i32_to_f32(s.bins[1][i]);
+        s.out_forces[i].torque = i32_to_f32(s.bins[2][i]);
+        s.out_forces[i]._pad = 0.0f;
+    }
+}
+
+// render_node.rs:219-277
+void run_init(eflo_sim& s) {
+    k_init_center(s);
+    k_init_edge(s);
+    k_fluid_source(s, s.src_once);
+    k_reinit(s);
+}
+
+efl_status run_stage(eflo_sim& s, int stage, efl_step_stats* st) {
+    switch (stage) {
+        case EFL_STAGE_INIT: run_init(s); s.status = 1; return EFL_OK;
+        case EFL_STAGE_UPDATE_SOLID: k_update_solid(s); return EFL_OK;
+        case EFL_STAGE_AREA_FRACTION: k_area_fraction(s); return EFL_OK;
+        case EFL_STAGE_ADVECT_VELOCITY: k_advect(s); return EFL_OK;
+        case EFL_STAGE_APPLY_FORCES: k_apply_forces(s); return EFL_OK;
+        case EFL_STAGE_DIVERGENCE: k_divergence(s); return EFL_OK;
+        case EFL_STAGE_PROJECTION: return k_projection(s, st);
+        case EFL_STAGE_SOLVE_VELOCITY: k_solve_velocity(s); return EFL_OK;
+        case EFL_STAGE_EXTRAPOLATE: k_extrapolate(s); return EFL_OK;
+        case EFL_STAGE_ADVECT_LEVELSET: k_advect_levelset(s); return EFL_OK;
+        case EFL_STAGE_FLUID_SOURCE: k_fluid_source(s, s.src_cont); return EFL_OK;
+        case EFL_STAGE_REINITIALIZE: k_reinit(s); return EFL_OK;
+        case EFL_STAGE_LEVELSET_GRADIENT: k_gradient(s); return EFL_OK;
+        case EFL_STAGE_SOLID_FORCES: k_solid_forces(s); return EFL_OK;
+        default: return fail(&s, EFL_ERR_INVALID_ARGUMENT, "unknown stage");
+    }
+}
+
+int mg_num_levels(const efl_config& c) {
+    if (c.projection.mg_levels > 0) return (int)c.projection.mg_levels;
+    int n = (int)std::log2((float)std::min(c.nx, c.ny)) - 2;  // multi_grid.rs:95-97
+    return std::max(1, n);
+}
+
+template <class T>
+void alloc_levels(std::vector<LevelT<T>>& mg, int L, int w, int h) {
+    mg.clear();
+    mg.resize(L);
+    for (int i = 0; i < L; ++i) {
+        LevelT<T>& l = mg[i];
+        l.nx = w; l.ny = h;
+        l.x.init(w, h); l.b.init(w, h); l.ls.init(w, h); l.r.init(w, h); l.af.init(w, h);
+        w /= 2; h /= 2;
+    }
+}
+void alloc_mg(eflo_sim& s) {
+    int L = mg_num_levels(s.cfg);
+    alloc_levels(s.mg, L, s.nx, s.ny);
+    alloc_levels(s.mg64, L, s.nx, s.ny);
+}
+
+efl_status validate_cfg(const efl_config* c, std::string* why) {
+    if (!c) { *why = "null config"; return EFL_ERR_INVALID_ARGUMENT; }
+    if (!(c->length_unit > 0.0f)) { *why = "length_unit must be positive value."; return EFL_ERR_INVALID_ARGUMENT; }
+    if (c->nx < 16 || c->ny < 16 || c->nx % 8 || c->ny % 8) {
+        *why = "grid size must be a multiple of 8 and at least 16";
+        return EFL_ERR_INVALID_ARGUMENT;
+    }
+    if (c->nx > 32768 || c->ny > 32768) { *why = "grid size too large"; return EFL_ERR_INVALID_ARGUMENT; }
+    const efl_projection& p = c->projection;
+    if (p.method < 0 || p.method > 2) { *why = "unknown projection method"; return EFL_ERR_INVALID_ARGUMENT; }
+    if (c->reinit.method < 0 || c->reinit.method > 1) { *why = "unknown reinitialize method"; return EFL_ERR_INVALID_ARGUMENT; }
+    return EFL_OK;
+}
+
+std::string g_err;
+
+}  // namespace
+
+extern "C" {
+
+efl_status eflo_create(const efl_config* cfg, eflo_sim** out) {
+    if (!out) { g_err = "null output pointer"; return EFL_ERR_INVALID_ARGUMENT; }
+    *out = nullptr;
+    std::string why;
+    efl_status st = validate_cfg(cfg, &why);
+    if (st != EFL_OK) { g_err = why; return st; }
+    eflo_sim* s = new eflo_sim();
+    s->cfg = *cfg;
+    s->nx = (int)cfg->nx;
+    s->ny = (int)cfg->ny;
+    int nx = s->nx, ny = s->ny;
+    s->U.dx = 1.0f / cfg->length_unit;  // euler_fluid.rs:89
+    s->U.dt = 0.0f;
+    s->U.rho = cfg->rho;
+    s->U.g[0] = cfg->gravity[0];
+    s->U.g[1] = cfg->gravity[1];
+    std::memcpy(s->U.m, cfg->transform, sizeof(s->U.m));
+    s->U.size[0] = (float)nx;
+    s->U.size[1] = (float)ny;
+    s->u0.init(nx + 1, ny); s->u1.init(nx + 1, ny); s->us.init(nx + 1, ny);
+    s->v0.init(nx, ny + 1); s->v1.init(nx, ny + 1); s->vs.init(nx, ny + 1);
+    s->u_valid_in.init(nx + 1, ny); s->u_valid_out.init(nx + 1, ny);
+    s->v_valid_in.init(nx, ny + 1); s->v_valid_out.init(nx, ny + 1);
+    s->solid_id.init(nx, ny); s->ls_solid.init(nx, ny); s->div.init(nx, ny);
+    s->p0.init(nx, ny); s->p1.init(nx, ny); s->ls0.init(nx, ny); s->ls1.init(nx, ny);
+    s->af.init(nx, ny); s->grad.init(nx, ny); s->seeds[0].init(nx, ny); s->seeds[1].init(nx, ny);
+    s->labels0.init(nx, ny); s->labels.init(nx, ny); s->labelsT.init(nx, ny); s->phiT.init(nx, ny);
+    alloc_mg(*s);
+    std::memset(s->bins, 0, sizeof(s->bins));
+    std::memset(s->out_forces, 0, sizeof(s->out_forces));
+    *out = s;
+    return EFL_OK;
+}
+
+efl_status eflo_destroy(eflo_sim* s) {
+    delete s;
+    return EFL_OK;
+}
+
+const char* eflo_last_error(const eflo_sim* s) { return s ? s->err.c_str() : g_err.c_str(); }
+
+efl_status eflo_reset(eflo_sim* s) {
+    if (!s) return EFL_ERR_INVALID_ARGUMENT;
+    s->status = 0;
+    return EFL_OK;
+}
+
+efl_status eflo_set_projection(eflo_sim* s, const efl_projection* p) {
+    if (!s || !p) return EFL_ERR_INVALID_ARGUMENT;
+    if (p->method < 0 || p->method > 2) return fail(s, EFL_ERR_INVALID_ARGUMENT, "unknown projection method");
+    s->cfg.projection = *p;
+    alloc_mg(*s);
+    return EFL_OK;
+}
+efl_status eflo_set_reinit(eflo_sim* s, const efl_reinit* r) {
+    if (!s || !r) return EFL_ERR_INVALID_ARGUMENT;
+    if (r->method < 0 || r->method > 1) return fail(s, EFL_ERR_INVALID_ARGUMENT, "unknown reinitialize method");
+    s->cfg.reinit = *r;
+    return EFL_OK;
+}
+efl_status eflo_set_transform(eflo_sim* s, const float t[16]) {
+    if (!s || !t) return EFL_ERR_INVALID_ARGUMENT;
+    std::memcpy(s->U.m, t, sizeof(s->U.m));
+    std::memcpy(s->cfg.transform, t, sizeof(s->U.m));
+    return EFL_OK;
+}
+efl_status eflo_set_obstacles(eflo_sim* s, const efl_solid_obstacle* o, uint32_t n) {
+    if (!s || (n && !o)) return EFL_ERR_INVALID_ARGUMENT;
+    if (n > EFL_MAX_SOLIDS) return fail(s, EFL_ERR_TOO_MANY, "too many obstacles (max 256)");
+    for (uint32_t i = 0; i < n; ++i) {
+        uint32_t sh = o[i].shape;
+        if (sh != 0 && sh != 1 && sh != 2 && sh != 4) return fail(s, EFL_ERR_UNSUPPORTED_SHAPE, "Unsupported shape type for solid");
+    }
+    s->obstacles.assign(o, o + n);
+    return EFL_OK;
+}
+efl_status eflo_set_local_forces(eflo_sim* s, const efl_force* f, uint32_t n) {
+    if (!s || (n && !f)) return EFL_ERR_INVALID_ARGUMENT;
+    s->forces.assign(f, f + n);
+    return EFL_OK;
+}
+efl_status eflo_set_sources(eflo_sim* s, const efl_source* src, uint32_t n, int32_t oneshot) {
+    if (!s || (n && !src)) return EFL_ERR_INVALID_ARGUMENT;
+    if (n > EFL_MAX_FLUID_SOURCE)
+        return fail(s, EFL_ERR_TOO_MANY, "The maximum number of fluid source per fluid component is 16.");
+    (oneshot ? s->src_once : s->src_cont).assign(src, src + n);
+    return EFL_OK;
+}
+
+efl_status eflo_step(eflo_sim* s, float dt, efl_step_stats* st) {
+    if (!s) return EFL_ERR_INVALID_ARGUMENT;
+    if (st) {
+        std::memset(st, 0, sizeof(*st));
+        st->residual = -1.0;
+        st->residual_initial = -1.0;
+        st->converged = 1;
+    }
+    if (s->status == 0) {  // FluidStatus::Uninitialized -> init sequence only
+        run_init(*s);
+        s->status = 1;
+        if (st) st->initialized_only = 1;
+        return EFL_OK;
+    }
+    s->U.dt = dt;
+    efl_status ret = EFL_OK;
+    for (int stage = EFL_STAGE_UPDATE_SOLID; stage <= EFL_STAGE_SOLID_FORCES; ++stage) {
+        efl_status r = run_stage(*s, stage, st);
+        if (r == EFL_NOT_CONVERGED) ret = r;
+        else if (r != EFL_OK) return r;
+    }
+    s->forces.clear();  // apply_forces.rs:166
+    return ret;
+}
+
+efl_status eflo_run_stage(eflo_sim* s, int32_t stage, float dt, efl_step_stats* st) {
+    if (!s) return EFL_ERR_INVALID_ARGUMENT;
+    if (st) {
+        std::memset(st, 0, sizeof(*st));
+        st->residual = -1.0;
+        st->residual_initial = -1.0;
+        st->converged = 1;
+    }
+    s->U.dt = dt;
+    return run_stage(*s, stage, st);
+}
+
+efl_status eflo_read_solid_forces(eflo_sim* s, efl_solid_force out[EFL_MAX_SOLIDS]) {
+    if (!s || !out) return EFL_ERR_INVALID_ARGUMENT;
+    std::memcpy(out, s->out_forces, sizeof(s->out_forces));
+    return EFL_OK;
+}
+efl_status eflo_read_force_bins(eflo_sim* s, int32_t out[3 * EFL_MAX_SOLIDS]) {
+    if (!s || !out) return EFL_ERR_INVALID_ARGUMENT;
+    std::memcpy(out, s->bins, sizeof(s->bins));
+    return EFL_OK;
+}
+
+efl_status eflo_field_shape(const eflo_sim* s, int32_t field, uint32_t* w, uint32_t* h, uint32_t* ch,
+                            uint32_t* eb) {
+    if (!s) return EFL_ERR_INVALID_ARGUMENT;
+    uint32_t nx = s->nx, ny = s->ny, W = nx, H = ny, C = 1;
+    switch (field) {
+        case EFL_FIELD_U: case EFL_FIELD_U1: case EFL_FIELD_U_SOLID: case EFL_FIELD_U_VALID:
+        case EFL_FIELD_AREA_FRACTION_U: W = nx + 1; break;
+        case EFL_FIELD_V: case EFL_FIELD_V1: case EFL_FIELD_V_SOLID: case EFL_FIELD_V_VALID:
+        case EFL_FIELD_AREA_FRACTION_V: H = ny + 1; break;
+        case EFL_FIELD_AREA_FRACTION: C = 4; break;
+        case EFL_FIELD_GRAD_LEVELSET: case EFL_FIELD_JFA_SEEDS: C = 2; break;
+        case EFL_FIELD_LEVELSET_AIR: case EFL_FIELD_LEVELSET_AIR1: case EFL_FIELD_LEVELSET_SOLID:
+        case EFL_FIELD_SOLID_ID: case EFL_FIELD_DIVERGENCE: case EFL_FIELD_PRESSURE: case EFL_FIELD_FIM_LABELS:
+            break;
+        default: return EFL_ERR_INVALID_ARGUMENT;
+    }
+    if (w) *w = W;
+    if (h) *h = H;
+    if (ch) *ch = C;
+    if (eb) *eb = 4;
+    return EFL_OK;
+}
+
+}  // extern "C"
+
+namespace {
+template <class T>
+efl_status copy_out(const Tex<T>& t, void* dst, size_t bytes) {
+    if (bytes != t.a.size() * sizeof(T)) return EFL_ERR_INVALID_ARGUMENT;
+    std::memcpy(dst, t.a.data(), bytes);
+    return EFL_OK;
+}
+template <class T>
+efl_status copy_in(Tex<T>& t, const void* src, size_t bytes) {
+    if (bytes != t.a.size() * sizeof(T)) return EFL_ERR_INVALID_ARGUMENT;
+    std::memcpy(t.a.data(), src, bytes);
+    return EFL_OK;
+}
+// x-face / y-face fraction views of the RGBA texture
+void af_faces(const eflo_sim& s, std::vector<float>& fu, std::vector<float>& fv) {
+    int nx = s.nx, ny = s.ny;
+    fu.assign((size_t)(nx + 1) * ny, 0.0f);
+    fv.assign((size_t)nx * (ny + 1), 0.0f);
+    for (int y = 0; y < ny; ++y)
+        for (int x = 0; x < nx; ++x) {
+            F4 f = s.af.a[(size_t)y * nx + x];
+            fu[(size_t)y * (nx + 1) + x] = f.x;
+            if (x == nx - 1) fu[(size_t)y * (nx + 1) + x + 1] = f.y;
+            fv[(size_t)y * nx + x] = f.z;
+            if (y == ny - 1) fv[(size_t)(y + 1) * nx + x] = f.w;
+        }
+}
+}  // namespace
+
+extern "C" {
+
+efl_status eflo_get_field(eflo_sim* s, int32_t field, void* dst, size_t bytes) {
+    if (!s || !dst) return EFL_ERR_INVALID_ARGUMENT;
+    switch (field) {
+        case EFL_FIELD_U: return copy_out(s->u0, dst, bytes);
+        case EFL_FIELD_V: return copy_out(s->v0, dst, bytes);
+        case EFL_FIELD_U1: return copy_out(s->u1, dst, bytes);
+        case EFL_FIELD_V1: return copy_out(s->v1, dst, bytes);
+        case EFL_FIELD_U_SOLID: return copy_out(s->us, dst, bytes);
+        case EFL_FIELD_V_SOLID: return copy_out(s->vs, dst, bytes);
+        case EFL_FIELD_LEVELSET_AIR: return copy_out(s->ls0, dst, bytes);
+        case EFL_FIELD_LEVELSET_AIR1: return copy_out(s->ls1, dst, bytes);
+        case EFL_FIELD_LEVELSET_SOLID: return copy_out(s->ls_solid, dst, bytes);
+        case EFL_FIELD_SOLID_ID: return copy_out(s->solid_id, dst, bytes);
+        case EFL_FIELD_AREA_FRACTION: return copy_out(s->af, dst, bytes);
+        case EFL_FIELD_DIVERGENCE: return copy_out(s->div, dst, bytes);
+        case EFL_FIELD_PRESSURE: return copy_out(s->p0, dst, bytes);
+        case EFL_FIELD_GRAD_LEVELSET: return copy_out(s->grad, dst, bytes);
+        case EFL_FIELD_JFA_SEEDS: return copy_out(s->seeds[s->seeds_final], dst, bytes);
+        case EFL_FIELD_FIM_LABELS: return copy_out(s->labels, dst, bytes);
+        case EFL_FIELD_U_VALID: return copy_out(s->u_valid_in, dst, bytes);
+        case EFL_FIELD_V_VALID: return copy_out(s->v_valid_in, dst, bytes);
+        case EFL_FIELD_AREA_FRACTION_U:
+        case EFL_FIELD_AREA_FRACTION_V: {
+            std::vector<float> fu, fv;
+            af_faces(*s, fu, fv);
+            const std::vector<float>& v = field == EFL_FIELD_AREA_FRACTION_U ? fu : fv;
+            if (bytes != v.size() * 4) return EFL_ERR_INVALID_ARGUMENT;
+            std::memcpy(dst, v.data(), bytes);
+            return EFL_OK;
+        }
+        default: return EFL_ERR_INVALID_ARGUMENT;
+    }
+}
+
+efl_status eflo_set_field(eflo_sim* s, int32_t field, const void* src, size_t bytes) {
+    if (!s || !src) return EFL_ERR_INVALID_ARGUMENT;
+    switch (field) {
+        case EFL_FIELD_U: return copy_in(s->u0, src, bytes);
+        case EFL_FIELD_V: return copy_in(s->v0, src, bytes);
+        case EFL_FIELD_U1: return copy_in(s->u1, src, bytes);
+        case EFL_FIELD_V1: return copy_in(s->v1, src, bytes);
+        case EFL_FIELD_U_SOLID: return copy_in(s->us, src, bytes);
+        case EFL_FIELD_V_SOLID: return copy_in(s->vs, src, bytes);
+        case EFL_FIELD_LEVELSET_AIR: return copy_in(s->ls0, src, bytes);
+        case EFL_FIELD_LEVELSET_AIR1: return copy_in(s->ls1, src, bytes);
+        case EFL_FIELD_LEVELSET_SOLID: return copy_in(s->ls_solid, src, bytes);
+        case EFL_FIELD_SOLID_ID: return copy_in(s->solid_id, src, bytes);
+        case EFL_FIELD_AREA_FRACTION: return copy_in(s->af, src, bytes);
+        case EFL_FIELD_DIVERGENCE: return copy_in(s->div, src, bytes);
+        case EFL_FIELD_PRESSURE: return copy_in(s->p0, src, bytes);
+        case EFL_FIELD_GRAD_LEVELSET: return copy_in(s->grad, src, bytes);
+        case EFL_FIELD_JFA_SEEDS: return copy_in(s->seeds[s->seeds_final], src, bytes);
+        case EFL_FIELD_FIM_LABELS: return copy_in(s->labels, src, bytes);
+        case EFL_FIELD_U_VALID: return copy_in(s->u_valid_in, src, bytes);
+        case EFL_FIELD_V_VALID: return copy_in(s->v_valid_in, src, bytes);
+        default: return EFL_ERR_INVALID_ARGUMENT;
+    }
+}
+
+efl_status eflo_residual(eflo_sim* s, double* rel, double* nr, double* nb) {
+    if (!s) return EFL_ERR_INVALID_ARGUMENT;
+    double R, B;
+    residual_norms_f32(*s, &R, &B);
+    if (nr) *nr = std::sqrt(R);
+    if (nb) *nb = std::sqrt(B);
+    if (rel) *rel = B > 0.0 ? std::sqrt(R) / std::sqrt(B) : (R > 0.0 ? std::numeric_limits<double>::infinity() : 0.0);
+    return EFL_OK;
+}
+
+efl_status eflo_fluid_volume(eflo_sim* s, uint64_t* cells) {
+    if (!s || !cells) return EFL_ERR_INVALID_ARGUMENT;
+    uint64_t c = 0;
+    for (float v : s->ls0.a) c += v < 0.0f;
+    *cells = c;
+    return EFL_OK;
+}
+
+void eflo_set_threads(int32_t n) {
+    g_threads = n;
+#ifdef _OPENMP
+    if (n > 0) omp_set_num_threads(n);
+#endif
+}
+int32_t eflo_get_threads(void) {
+#ifdef _OPENMP
+    return g_threads > 0 ? g_threads : omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+void eflo_set_fim_serial(eflo_sim* s, int32_t on) {
+    if (s) s->fim_serial = on != 0;
+}
+
+}  // extern "C"
