@@ -122,9 +122,12 @@ SIGNATURES = {
     "synchronize": (C.c_int, ["X"]),
     "residual": (C.c_int, ["X", C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "fluid_volume": (C.c_int, ["X", C.POINTER(C.c_uint64)]),
+    "kernel_launches": (C.c_uint64, []),
+    "pressure_sweeps": (C.c_int, ["X", C.c_int32, C.c_uint32]),
 }
 # Functions of efl.h that the oracle restatement does not mirror.
-PRODUCT_ONLY = {"abi_version", "default_config", "field_device_ptr", "stream", "synchronize"}
+PRODUCT_ONLY = {"abi_version", "default_config", "field_device_ptr", "stream", "synchronize", "kernel_launches",
+                "pressure_sweeps"}
 
 
 class EflError(RuntimeError):
@@ -314,3 +317,11 @@ class Sim:
 
     def synchronize(self):
         self._check(self.api.synchronize(self.h))
+
+    def stream(self) -> int:
+        p = C.c_void_p()
+        self._check(self.api.stream(self.h, C.byref(p)))
+        return p.value or 0
+
+    def pressure_sweeps(self, precision: int, iterations: int):
+        self._check(self.api.pressure_sweeps(self.h, precision, iterations))

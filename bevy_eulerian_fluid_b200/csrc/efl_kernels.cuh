@@ -26,6 +26,12 @@ namespace efl {
 
 #define EFL_DEV __device__ __forceinline__
 
+// Number of kernels this library has launched (all simulations, all
+// devices).  Evaluated in every launch configuration as the dynamic
+// shared-memory size argument, which it leaves at 0.
+uint64_t launches_total();
+size_t count_launch();
+
 constexpr float LARGE_FLOAT = 1.0e6f;      // update_solid.wgsl:4, update_fluid_source.wgsl:22
 constexpr float FIM_LARGE = 1e30f;         // fast_iterative_method/initialize.wgsl:5
 constexpr float FIM_EPS = 1e-6f;           // fast_iterative_method/update.wgsl:9

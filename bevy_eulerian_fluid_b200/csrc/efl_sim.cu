@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -20,6 +21,15 @@
 #include "efl_solver.cuh"
 
 using namespace efl;
+
+namespace efl {
+static std::atomic<uint64_t> g_launches{0};
+uint64_t launches_total() { return g_launches.load(std::memory_order_relaxed); }
+size_t count_launch() {
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    return 0;
+}
+}  // namespace efl
 
 namespace {
 
@@ -198,8 +208,8 @@ efl_status validate_cfg(const efl_config* c) {
 
 efl_status st_init(efl_sim* s) {  // render_node.rs:219-277
     Dom d = s->dom();
-    k_init_center<<<grid2d(d.nx, d.ny, kBlock), kBlock, 0, s->stream>>>(s->ls0, s->ls1, s->grad, d);
-    k_init_edge<<<grid2d(d.nx + 1, d.ny, kBlock), kBlock, 0, s->stream>>>(s->u0, s->u1, s->v0, s->v1, d);
+    k_init_center<<<grid2d(d.nx, d.ny, kBlock), kBlock, count_launch(), s->stream>>>(s->ls0, s->ls1, s->grad, d);
+    k_init_edge<<<grid2d(d.nx + 1, d.ny, kBlock), kBlock, count_launch(), s->stream>>>(s->u0, s->u1, s->v0, s->v1, d);
     LAUNCH_CHECK();
     return EFL_OK;
 }
@@ -210,8 +220,8 @@ efl_status st_fluid_source(efl_sim* s, const std::vector<efl_source>& src) {  //
     std::memset(&S, 0, sizeof(S));
     S.n = (int)src.size();
     for (int i = 0; i < S.n; ++i) S.s[i] = src[i];
-    k_fluid_source_cells<<<grid2d(d.nx, d.ny, kBlock), kBlock, 0, s->stream>>>(s->ls1, s->upd, s->srcvel, S, d);
-    k_fluid_source_faces<<<grid2d(d.nx + 1, d.ny + 1, kBlock), kBlock, 0, s->stream>>>(s->u0, s->v0, s->upd,
+    k_fluid_source_cells<<<grid2d(d.nx, d.ny, kBlock), kBlock, count_launch(), s->stream>>>(s->ls1, s->upd, s->srcvel, S, d);
+    k_fluid_source_faces<<<grid2d(d.nx + 1, d.ny + 1, kBlock), kBlock, count_launch(), s->stream>>>(s->u0, s->v0, s->upd,
                                                                                        s->srcvel, d);
     LAUNCH_CHECK();
     return EFL_OK;
@@ -232,20 +242,20 @@ efl_status st_reinit(efl_sim* s) {  // reinitialize_levelset.rs:162-243
     Dom d = s->dom();
     dim3 g = grid2d(d.nx, d.ny, kBlock);
     if (s->cfg.reinit.method == EFL_REINIT_JUMP_FLOODING) {
-        k_jfa_init<<<g, kBlock, 0, s->stream>>>(s->ls1, s->seeds[0], d);
+        k_jfa_init<<<g, kBlock, count_launch(), s->stream>>>(s->ls1, s->seeds[0], d);
         int src = 0, dst = 1;
         for (int step : jfa_steps(d.nx, d.ny)) {
-            k_jfa_iterate<<<g, kBlock, 0, s->stream>>>(s->seeds[src], s->seeds[dst], step, d);
+            k_jfa_iterate<<<g, kBlock, count_launch(), s->stream>>>(s->seeds[src], s->seeds[dst], step, d);
             std::swap(src, dst);
         }
         s->seeds_final = src;
-        k_jfa_sdf<<<g, kBlock, 0, s->stream>>>(s->seeds[src], s->ls1, s->ls0, d);
+        k_jfa_sdf<<<g, kBlock, count_launch(), s->stream>>>(s->seeds[src], s->ls1, s->ls0, d);
     } else {
-        k_fim_init<<<g, kBlock, 0, s->stream>>>(s->ls1, s->ls0, s->lab0, d);
-        k_fim_active<<<g, kBlock, 0, s->stream>>>(s->lab0, s->lab, d);
+        k_fim_init<<<g, kBlock, count_launch(), s->stream>>>(s->ls1, s->ls0, s->lab0, d);
+        k_fim_active<<<g, kBlock, count_launch(), s->stream>>>(s->lab0, s->lab, d);
         for (uint32_t k = 0; k < s->cfg.reinit.fim_iterations; ++k) {
-            k_fim_phase_a<<<g, kBlock, 0, s->stream>>>(s->ls0, s->lab, s->phiT, s->labT, d);
-            k_fim_phase_b<<<g, kBlock, 0, s->stream>>>(s->phiT, s->labT, s->ls0, s->lab, d);
+            k_fim_phase_a<<<g, kBlock, count_launch(), s->stream>>>(s->ls0, s->lab, s->phiT, s->labT, d);
+            k_fim_phase_b<<<g, kBlock, count_launch(), s->stream>>>(s->phiT, s->labT, s->ls0, s->lab, d);
         }
     }
     LAUNCH_CHECK();
@@ -261,36 +271,36 @@ efl_status run_init(efl_sim* s) {
 
 efl_status st_update_solid(efl_sim* s) {
     Dom d = s->dom();
-    k_update_solid<<<grid2d(d.nx, d.ny, kBlock), kBlock, 0, s->stream>>>(s->us, s->vs, s->ls_s, s->sid, s->d_obs,
+    k_update_solid<<<grid2d(d.nx, d.ny, kBlock), kBlock, count_launch(), s->stream>>>(s->us, s->vs, s->ls_s, s->sid, s->d_obs,
                                                                        s->n_obs, s->U, d);
     LAUNCH_CHECK();
     return EFL_OK;
 }
 efl_status st_area_fraction(efl_sim* s) {
     Dom d = s->dom();
-    k_area_fraction<<<grid2d(d.nx, d.ny, kBlock), kBlock, 0, s->stream>>>(s->ls_s, s->fu, s->fv, d);
+    k_area_fraction<<<grid2d(d.nx, d.ny, kBlock), kBlock, count_launch(), s->stream>>>(s->ls_s, s->fu, s->fv, d);
     LAUNCH_CHECK();
     return EFL_OK;
 }
 efl_status st_advect(efl_sim* s) {
     Dom d = s->dom();
-    k_advect_u<<<grid2d(d.nx + 1, d.ny, kBlock), kBlock, 0, s->stream>>>(s->u0, s->v0, s->u1, s->U.dt, d);
-    k_advect_v<<<grid2d(d.nx, d.ny + 1, kBlock), kBlock, 0, s->stream>>>(s->u0, s->v0, s->v1, s->U.dt, d);
+    k_advect_u<<<grid2d(d.nx + 1, d.ny, kBlock), kBlock, count_launch(), s->stream>>>(s->u0, s->v0, s->u1, s->U.dt, d);
+    k_advect_v<<<grid2d(d.nx, d.ny + 1, kBlock), kBlock, count_launch(), s->stream>>>(s->u0, s->v0, s->v1, s->U.dt, d);
     LAUNCH_CHECK();
     return EFL_OK;
 }
 efl_status st_apply_forces(efl_sim* s) {
     Dom d = s->dom();
-    k_apply_forces<0><<<grid2d(d.nx + 1, d.ny, kBlock), kBlock, 0, s->stream>>>(s->u1, s->ls0, s->fu, s->d_forces,
+    k_apply_forces<0><<<grid2d(d.nx + 1, d.ny, kBlock), kBlock, count_launch(), s->stream>>>(s->u1, s->ls0, s->fu, s->d_forces,
                                                                               s->n_forces, s->U, d);
-    k_apply_forces<1><<<grid2d(d.nx, d.ny + 1, kBlock), kBlock, 0, s->stream>>>(s->v1, s->ls0, s->fv, s->d_forces,
+    k_apply_forces<1><<<grid2d(d.nx, d.ny + 1, kBlock), kBlock, count_launch(), s->stream>>>(s->v1, s->ls0, s->fv, s->d_forces,
                                                                                s->n_forces, s->U, d);
     LAUNCH_CHECK();
     return EFL_OK;
 }
 efl_status st_divergence(efl_sim* s) {
     Dom d = s->dom();
-    k_divergence<<<grid2d(d.nx, d.ny, kBlock), kBlock, 0, s->stream>>>(s->u1, s->v1, s->us, s->vs, s->fu, s->fv,
+    k_divergence<<<grid2d(d.nx, d.ny, kBlock), kBlock, count_launch(), s->stream>>>(s->u1, s->v1, s->us, s->vs, s->fu, s->fv,
                                                                      s->div, s->U.dx, d);
     LAUNCH_CHECK();
     return EFL_OK;
@@ -299,9 +309,9 @@ efl_status st_divergence(efl_sim* s) {
 // ||b - A x||^2 and ||b||^2 at level 0 into d_norms (async).
 template <class T>
 efl_status launch_norms(efl_sim* s, const LevelT<T>& L0) {
-    k_residual_norm<T><<<s->n_partials, NORM_THREADS, 0, s->stream>>>(L0, s->U.dt, s->U.rho, s->U.dx,
+    k_residual_norm<T><<<s->n_partials, NORM_THREADS, count_launch(), s->stream>>>(L0, s->U.dt, s->U.rho, s->U.dx,
                                                                       s->d_partials);
-    k_norm_finalize<<<1, 32, 0, s->stream>>>(s->d_partials, s->n_partials, s->d_norms);
+    k_norm_finalize<<<1, 32, count_launch(), s->stream>>>(s->d_partials, s->n_partials, s->d_norms);
     LAUNCH_CHECK();
     return EFL_OK;
 }
@@ -330,8 +340,8 @@ efl_status gs_iterations(efl_sim* s, const LevelT<T>& L, float weight, float res
     float dxs = res_scale * s->U.dx;  // gauss_seidel.wgsl:57
     dim3 g = grid2d((L.nx + 1) / 2, L.ny, kBlock);
     for (uint32_t k = 0; k < n; ++k) {
-        k_gs_color<T><<<g, kBlock, 0, s->stream>>>(L, dxs, s->U.rho, s->U.dt, weight, 1);
-        k_gs_color<T><<<g, kBlock, 0, s->stream>>>(L, dxs, s->U.rho, s->U.dt, weight, 0);
+        k_gs_color<T><<<g, kBlock, count_launch(), s->stream>>>(L, dxs, s->U.rho, s->U.dt, weight, 1);
+        k_gs_color<T><<<g, kBlock, count_launch(), s->stream>>>(L, dxs, s->U.rho, s->U.dt, weight, 0);
     }
     LAUNCH_CHECK();
     return EFL_OK;
@@ -346,11 +356,11 @@ efl_status v_cycle(efl_sim* s, std::vector<LevelT<T>>& mg, size_t i) {
     if (i == mg.size() - 1) return gs_iterations(s, L, 1.0f, scale, P.mg_coarsest);
     TRY(gs_iterations(s, L, 1.0f, scale, P.mg_pre));
     const LevelT<T>& C = mg[i + 1];
-    k_residual<T><<<grid2d(L.nx, L.ny, kBlock), kBlock, 0, s->stream>>>(L, s->U.dt, s->U.rho, scale * s->U.dx);
-    k_restriction<T><<<grid2d(C.nx, C.ny, kBlock), kBlock, 0, s->stream>>>(L, C);
+    k_residual<T><<<grid2d(L.nx, L.ny, kBlock), kBlock, count_launch(), s->stream>>>(L, s->U.dt, s->U.rho, scale * s->U.dx);
+    k_restriction<T><<<grid2d(C.nx, C.ny, kBlock), kBlock, count_launch(), s->stream>>>(L, C);
     LAUNCH_CHECK();
     TRY(v_cycle(s, mg, i + 1));
-    k_prolongation<T><<<grid2d(C.nx, C.ny, kBlock), kBlock, 0, s->stream>>>(L, C);
+    k_prolongation<T><<<grid2d(C.nx, C.ny, kBlock), kBlock, count_launch(), s->stream>>>(L, C);
     LAUNCH_CHECK();
     return gs_iterations(s, L, 1.0f, scale, P.mg_post);
 }
@@ -368,8 +378,8 @@ efl_status st_projection(efl_sim* s, efl_step_stats* st) {
     if (P.method == EFL_PROJECTION_JACOBI) {
         dim3 g = grid2d(d.nx, d.ny, kBlock);
         for (int it = 0; it < 50; ++it) {  // projection.rs:135-143
-            k_jacobi<<<g, kBlock, 0, s->stream>>>(s->p0, s->p1, s->ls0, s->fu, s->fv, s->div, s->U, d);
-            k_jacobi<<<g, kBlock, 0, s->stream>>>(s->p1, s->p0, s->ls0, s->fu, s->fv, s->div, s->U, d);
+            k_jacobi<<<g, kBlock, count_launch(), s->stream>>>(s->p0, s->p1, s->ls0, s->fu, s->fv, s->div, s->U, d);
+            k_jacobi<<<g, kBlock, count_launch(), s->stream>>>(s->p1, s->p0, s->ls0, s->fu, s->fv, s->div, s->U, d);
         }
         LAUNCH_CHECK();
         iters = 50;
@@ -385,7 +395,7 @@ efl_status st_projection(efl_sim* s, efl_step_stats* st) {
     } else {
         const Level64& L = s->mg64[0];
         dim3 g = grid2d(d.nx, d.ny, kBlock);
-        k_widen<<<g, kBlock, 0, s->stream>>>(s->p0, s->div, L.x, L.b);
+        k_widen<<<g, kBlock, count_launch(), s->stream>>>(s->p0, s->div, L.x, L.b);
         LAUNCH_CHECK();
         double r;
         TRY(relative_residual(s, L, &r));
@@ -394,7 +404,8 @@ efl_status st_projection(efl_sim* s, efl_step_stats* st) {
             uint32_t chk = std::max<uint32_t>(1, P.check_interval);
             while (!(r <= (double)P.tolerance) && iters < P.max_iterations) {
                 uint32_t n = std::min(chk, P.max_iterations - iters);
-                TRY(gs_iterations(s, L, P.sor_weight, 1.0f, n));
+                TRY(solve_gs_fixed(s->solver, L, s->U, P.sor_weight, n, s->stream));
+                LAUNCH_CHECK();
                 iters += n;
                 TRY(relative_residual(s, L, &r));
             }
@@ -407,7 +418,7 @@ efl_status st_projection(efl_sim* s, efl_step_stats* st) {
         }
         r1 = r;
         conv = r <= (double)P.tolerance;
-        k_narrow<<<g, kBlock, 0, s->stream>>>(L.x, s->p0);
+        k_narrow<<<g, kBlock, count_launch(), s->stream>>>(L.x, s->p0);
         LAUNCH_CHECK();
     }
     if (st) {
@@ -421,9 +432,9 @@ efl_status st_projection(efl_sim* s, efl_step_stats* st) {
 
 efl_status st_solve_velocity(efl_sim* s) {
     Dom d = s->dom();
-    k_solve_velocity<0><<<grid2d(d.nx + 1, d.ny, kBlock), kBlock, 0, s->stream>>>(s->u0, s->u1, s->us, s->p0,
+    k_solve_velocity<0><<<grid2d(d.nx + 1, d.ny, kBlock), kBlock, count_launch(), s->stream>>>(s->u0, s->u1, s->us, s->p0,
                                                                                 s->ls0, s->fu, s->U, d);
-    k_solve_velocity<1><<<grid2d(d.nx, d.ny + 1, kBlock), kBlock, 0, s->stream>>>(s->v0, s->v1, s->vs, s->p0,
+    k_solve_velocity<1><<<grid2d(d.nx, d.ny + 1, kBlock), kBlock, count_launch(), s->stream>>>(s->v0, s->v1, s->vs, s->p0,
                                                                                  s->ls0, s->fv, s->U, d);
     LAUNCH_CHECK();
     return EFL_OK;
@@ -432,35 +443,35 @@ efl_status st_extrapolate(efl_sim* s) {  // render_node.rs:540-608
     Dom d = s->dom();
     dim3 gu = grid2d(d.nx + 1, d.ny, kBlock), gv = grid2d(d.nx, d.ny + 1, kBlock);
     int xrows = (d.ny / 64) * 64, ycols = (d.nx / 64) * 64;
-    k_init_valid<0><<<gu, kBlock, 0, s->stream>>>(s->uvi, s->ls0, d);
-    k_init_valid<1><<<gv, kBlock, 0, s->stream>>>(s->vvi, s->ls0, d);
+    k_init_valid<0><<<gu, kBlock, count_launch(), s->stream>>>(s->uvi, s->ls0, d);
+    k_init_valid<1><<<gv, kBlock, count_launch(), s->stream>>>(s->vvi, s->ls0, d);
     for (int k = 0; k < 10 / 2; ++k) {
-        k_extrapolate<<<gu, kBlock, 0, s->stream>>>(s->u0, s->uvi, s->uvo, d.nx + 1, xrows);
-        k_extrapolate<<<gu, kBlock, 0, s->stream>>>(s->u0, s->uvo, s->uvi, d.nx + 1, xrows);
-        k_extrapolate<<<gv, kBlock, 0, s->stream>>>(s->v0, s->vvi, s->vvo, ycols, d.ny + 1);
-        k_extrapolate<<<gv, kBlock, 0, s->stream>>>(s->v0, s->vvo, s->vvi, ycols, d.ny + 1);
+        k_extrapolate<<<gu, kBlock, count_launch(), s->stream>>>(s->u0, s->uvi, s->uvo, d.nx + 1, xrows);
+        k_extrapolate<<<gu, kBlock, count_launch(), s->stream>>>(s->u0, s->uvo, s->uvi, d.nx + 1, xrows);
+        k_extrapolate<<<gv, kBlock, count_launch(), s->stream>>>(s->v0, s->vvi, s->vvo, ycols, d.ny + 1);
+        k_extrapolate<<<gv, kBlock, count_launch(), s->stream>>>(s->v0, s->vvo, s->vvi, ycols, d.ny + 1);
     }
     LAUNCH_CHECK();
     return EFL_OK;
 }
 efl_status st_advect_levelset(efl_sim* s) {
     Dom d = s->dom();
-    k_advect_levelset<<<grid2d(d.nx, d.ny, kBlock), kBlock, 0, s->stream>>>(s->u0, s->v0, s->ls0, s->ls1, s->U.dt, d);
+    k_advect_levelset<<<grid2d(d.nx, d.ny, kBlock), kBlock, count_launch(), s->stream>>>(s->u0, s->v0, s->ls0, s->ls1, s->U.dt, d);
     LAUNCH_CHECK();
     return EFL_OK;
 }
 efl_status st_gradient(efl_sim* s) {
     Dom d = s->dom();
-    k_gradient<<<grid2d(d.nx, d.ny, kBlock), kBlock, 0, s->stream>>>(s->ls0, s->grad, d);
+    k_gradient<<<grid2d(d.nx, d.ny, kBlock), kBlock, count_launch(), s->stream>>>(s->ls0, s->grad, d);
     LAUNCH_CHECK();
     return EFL_OK;
 }
 efl_status st_solid_forces(efl_sim* s) {  // render_node.rs:610-641; bins zeroed per frame (fluid_to_solid.rs:211-229)
     Dom d = s->dom();
     CU(cudaMemsetAsync(s->d_bins, 0, 3 * EFL_MAX_SOLIDS * sizeof(int), s->stream));
-    k_solid_forces<<<grid2d(d.nx, d.ny, kBlock), kBlock, 0, s->stream>>>(s->fu, s->fv, s->sid, s->p0, s->d_obs,
+    k_solid_forces<<<grid2d(d.nx, d.ny, kBlock), kBlock, count_launch(), s->stream>>>(s->fu, s->fv, s->sid, s->p0, s->d_obs,
                                                                        s->n_obs, s->U, d, s->d_bins);
-    k_accumulate_forces<<<1, EFL_MAX_SOLIDS, 0, s->stream>>>(s->d_bins, s->d_forces_out);
+    k_accumulate_forces<<<1, EFL_MAX_SOLIDS, count_launch(), s->stream>>>(s->d_bins, s->d_forces_out);
     LAUNCH_CHECK();
     return EFL_OK;
 }
@@ -904,12 +915,25 @@ efl_status efl_fluid_volume(efl_sim* s, uint64_t* cells) {
     if (!s || !cells) return set_err(s, EFL_ERR_INVALID_ARGUMENT, "null argument");
     cudaSetDevice(s->device);
     CU(cudaMemsetAsync(s->d_count, 0, sizeof(unsigned long long), s->stream));
-    k_volume<<<grid2d(s->nx, s->ny, kBlock), kBlock, 0, s->stream>>>(s->ls0, s->d_count);
+    k_volume<<<grid2d(s->nx, s->ny, kBlock), kBlock, count_launch(), s->stream>>>(s->ls0, s->d_count);
     LAUNCH_CHECK();
     unsigned long long c = 0;
     CU(cudaMemcpyAsync(&c, s->d_count, sizeof(c), cudaMemcpyDeviceToHost, s->stream));
     CU(cudaStreamSynchronize(s->stream));
     *cells = c;
+    return EFL_OK;
+}
+
+uint64_t efl_kernel_launches(void) { return efl::launches_total(); }
+
+efl_status efl_pressure_sweeps(efl_sim* s, int32_t precision, uint32_t iterations) {
+    if (!s) return set_err(nullptr, EFL_ERR_INVALID_ARGUMENT, "null sim");
+    if (precision != 32 && precision != 64) return set_err(s, EFL_ERR_INVALID_ARGUMENT, "precision must be 32 or 64");
+    cudaSetDevice(s->device);
+    const float w = s->cfg.projection.sor_weight;
+    if (precision == 32) TRY(solve_gs_fixed(s->solver, s->mg[0], s->U, w, iterations, s->stream));
+    else TRY(solve_gs_fixed(s->solver, s->mg64[0], s->U, w, iterations, s->stream));
+    LAUNCH_CHECK();
     return EFL_OK;
 }
 

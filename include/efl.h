@@ -310,6 +310,18 @@ EFL_API efl_status efl_residual(efl_sim* sim, double* relative, double* norm_r, 
 /* Number of cells with levelset_air < 0 (calculate_volume.wgsl:11-75). */
 EFL_API efl_status efl_fluid_volume(efl_sim* sim, uint64_t* cells);
 
+/* ---- Diagnostics ------------------------------------------------------ */
+
+/* Kernels this library has launched since it was loaded (all handles). */
+EFL_API uint64_t efl_kernel_launches(void);
+
+/* Runs exactly `iterations` red-black pressure iterations on the current
+ * state, with the current dt and no residual checks, to time the sweep:
+ * precision 32 = the reference's f32 sweep on the pressure field
+ * (gauss_seidel.wgsl:12-88 at the configured SOR weight), 64 = the FP64
+ * iterate of the tolerance-driven solve, in place. */
+EFL_API efl_status efl_pressure_sweeps(efl_sim* sim, int32_t precision, uint32_t iterations);
+
 #ifdef __cplusplus
 }
 #endif
