@@ -127,64 +127,65 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.samples)}
 
 
-def cpu_baseline(size: int, seconds_budget: float = 40.0):
-    """The CPU oracle on the host cores: init, then full steps of the same scene."""
+def coupled_cpu_run(size: int, warmup: int, steps: int, budget_s: float):
+    """The CPU oracle through the same coupled loop as the GPU arm: init, `warmup`
+    untimed steps, then up to `steps` timed steps (stopping early past budget_s)."""
     from bevy_eulerian_fluid_b200 import scenes
+    from bevy_eulerian_fluid_b200.plugin import pack_obstacles
+    from bevy_eulerian_fluid_b200.rigid import RigidWorld
     from oracle import py_oracle
     api = py_oracle.load()
-    cores = os.cpu_count() or 1
-    py_oracle.set_threads(cores)
+    py_oracle.set_threads(os.cpu_count() or 1)
     sc = scenes.coupled(size)
     sim = sc.make(api)
-    sim.step(sc.dt)
-    t0 = time.perf_counter()
-    steps, iters = 0, []
-    while True:
+    rigid = RigidWorld(list(sc.bodies), (size, size), gravity=9.8 * scenes.LENGTH_UNIT,
+                       grid_length=1.0 / scenes.LENGTH_UNIT)
+
+    def coupled_step():
         st = sim.step(sc.dt)
-        steps += 1
+        rigid.apply_fluid_forces(sim.solid_forces(), sc.dt)
+        rigid.step(sc.dt)
+        sim.set_obstacles(pack_obstacles(rigid.bodies))
+        return st
+
+    sim.step(sc.dt)
+    for _ in range(warmup):
+        coupled_step()
+    t0 = time.perf_counter()
+    n, iters = 0, []
+    while n < steps:
+        st = coupled_step()
+        n += 1
         iters.append(int(st.pressure_iterations))
-        if time.perf_counter() - t0 > seconds_budget or steps >= 3:
+        if time.perf_counter() - t0 > budget_s:
             break
     el = time.perf_counter() - t0
     sim.close()
-    return {"value": sc.cells * steps / el, "unit": "cell-steps/s", "cores": py_oracle.get_threads(),
-            "kind": "port",
-            "sample": f"{steps} full step(s) of coupled_{size} after init on the CPU oracle "
-                      f"({cores} host threads), pressure iterations/step {iters}"}
+    return sc.cells * n / el, n, iters, el, py_oracle.get_threads()
+
+
+def cpu_baseline(size: int, warmup: int, steps: int):
+    val, n, iters, el, cores = coupled_cpu_run(size, warmup, steps, 60.0)
+    return {"value": val, "unit": "cell-steps/s", "cores": cores, "kind": "port",
+            "sample": f"the first {n} timed step(s) of the GPU arm's coupled loop (same scene, same {warmup} warm-up "
+                      f"steps) on the CPU oracle, {cores} host threads, {el:.1f} s, pressure iterations/step {iters}"}
 
 
 def run_reference(args, world, rank):
+    """The reference's algorithm on the host cores (the CPU oracle), same workload and metric."""
     if world > 1 and rank != 0:
         return 0
-    from bevy_eulerian_fluid_b200 import scenes
-    from oracle import py_oracle
-    api = py_oracle.load()
-    cores = os.cpu_count() or 1
-    py_oracle.set_threads(cores)
-    sc = scenes.coupled(args.size)
-    sim = sc.make(api)
-    sim.step(sc.dt)
-    for _ in range(min(args.warmup, 1)):
-        sim.step(sc.dt)
     budget = 150.0
-    t0 = time.perf_counter()
-    steps, iters = 0, []
-    while steps < args.steps:
-        st = sim.step(sc.dt)
-        steps += 1
-        iters.append(int(st.pressure_iterations))
-        if time.perf_counter() - t0 > budget:
-            break
-    el = time.perf_counter() - t0
-    val = sc.cells * steps / el
+    val, n, iters, el, cores = coupled_cpu_run(args.size, args.warmup, args.steps, budget)
     line = {"impl": "reference", "metric": "cell-steps/s to 1e-5 rel. residual", "value": val, "unit": "cell-steps/s",
-            "n_gpus": world, "steps": steps, "warmup": min(args.warmup, 1), "ms_per_step": 1000 * el / steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64",
-            "data": "synthetic",
-            "config": {"workload": f"coupled_{args.size}", "cells": sc.cells, "bodies": 24, "reinit": "jump flooding",
-                       "solver": "RBGS (SOR 1.9), FP64 iterate, to 1e-5 relative residual"},
-            "cpu_baseline": {"value": val, "unit": "cell-steps/s", "cores": py_oracle.get_threads(), "kind": "port",
-                             "sample": f"{steps} full steps (budget {budget:.0f} s), pressure iterations {iters}"},
+            "n_gpus": world, "steps": n, "warmup": args.warmup, "ms_per_step": 1000 * el / n,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64", "data": "synthetic",
+            "config": {"workload": f"coupled_{args.size}", "cells": args.size * args.size, "bodies": 24,
+                       "reinit": "jump flooding",
+                       "solver": "RBGS (SOR 1.9) on an FP64 iterate to 1e-5 relative residual",
+                       "pressure_iterations_per_step": iters},
+            "cpu_baseline": {"value": val, "unit": "cell-steps/s", "cores": cores, "kind": "port",
+                             "sample": f"{n} coupled steps after {args.warmup} warm-up steps (budget {budget:.0f} s)"},
             "e2e": {"value": val, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -233,50 +234,41 @@ def main():
         coupled_step()
     torch.cuda.synchronize()
 
-    # ---- value: device-resident state, per-step CUDA events, L2 flushed between steps
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    # ---- one coupled loop: per step, events around the device step (value) and
+    # around the whole coupled iteration (e2e); L2 flushed before each step, outside both.
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
     iters = []
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     launches0 = api.kernel_launches()
+    launches = 0
     with ClockSampler(local) as clk:
         for k in range(args.steps):
             with torch.cuda.stream(stream):
                 flush.zero_()
-            evs[k][0].record(stream)
+            ev[k][0].record(stream)
+            l0 = api.kernel_launches()
             st = sim.step(sc.dt)
-            evs[k][1].record(stream)
+            launches += api.kernel_launches() - l0
+            ev[k][1].record(stream)
+            forces = sim.solid_forces()  # D2H: FluidToSolidForce[256]
+            rigid.apply_fluid_forces(forces, sc.dt)
+            rigid.step(sc.dt)
+            sim.set_obstacles(pack_obstacles(rigid.bodies))  # H2D: packed obstacles
+            ev[k][2].record(stream)
             iters.append(int(st.pressure_iterations))
             if not st.converged:
                 print(f"warning: step {k} not converged (residual {st.residual})", file=sys.stderr)
         torch.cuda.synchronize()
-    launches = api.kernel_launches() - launches0
-    dev_ms = sum(a.elapsed_time(b) for a, b in evs)
+    dev_ms = sum(e[0].elapsed_time(e[1]) for e in ev)
+    e2e_ms = sum(e[0].elapsed_time(e[2]) for e in ev)
     if dist:
-        t = torch.tensor([dev_ms], device=f"cuda:{local}")
+        t = torch.tensor([dev_ms, e2e_ms], device=f"cuda:{local}")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dev_ms = float(t.item())
+        dev_ms, e2e_ms = float(t[0].item()), float(t[1].item())
         dist.barrier()
     value = world * sc.cells * args.steps / (dev_ms / 1e3)
-
-    # ---- e2e: plugin API with the coupling loop (host buffers both ways)
-    e2e_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    e2e_iters = []
-    torch.cuda.synchronize()
-    for k in range(args.steps):
-        with torch.cuda.stream(stream):
-            flush.zero_()
-        e2e_ev[k][0].record(stream)
-        st = coupled_step()
-        e2e_ev[k][1].record(stream)
-        e2e_iters.append(int(st.pressure_iterations))
-    torch.cuda.synchronize()
-    e2e_ms = sum(a.elapsed_time(b) for a, b in e2e_ev)
-    if dist:
-        t = torch.tensor([e2e_ms], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
     e2e_value = world * sc.cells * args.steps / (e2e_ms / 1e3)
     h2d = len(bodies) * 176
     d2h = capi.MAX_SOLIDS * 16
@@ -313,7 +305,7 @@ def main():
 
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(args.size)
+        cpu = cpu_baseline(args.size, args.warmup, min(args.steps, 3))
 
     line = {
         "metric": "cell-steps/s to 1e-5 rel. residual", "value": value, "unit": "cell-steps/s", "n_gpus": world,
@@ -324,7 +316,7 @@ def main():
                    "pressure_iterations_per_step": iters, "l2": "flushed (256 MiB write) between timed steps",
                    "parallelism": f"replicas x{world}"},
         "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "ms_per_step": e2e_ms / args.steps, "pressure_iterations_per_step": e2e_iters},
+                "ms_per_step": e2e_ms / args.steps},
         "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(), "gpu_launches": int(launches),
     }
     if micro:

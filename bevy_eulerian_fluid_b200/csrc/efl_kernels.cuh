@@ -307,11 +307,32 @@ __global__ void k_advect_v(PF u0, PF v0, PF v1, float dt, Dom d) {
     v1.st(x, y, inside ? interp_edge_y(v0, b.x, b.y) : v0.ld(x, y));
 }
 
+// exp for the Gaussian force splat.  WGSL's exp is implementation-defined
+// (any few-ulp result is conforming), so the library and the CPU oracle both
+// evaluate this restatement of the Cody-Waite method: x = k ln2 + r with ln2
+// split into an exactly-multipliable high part and a low part, |r| <= ln2/2,
+// exp(r) by its degree-7 Taylor polynomial in Horner form (truncation error
+// < 1e-8 relative), exact scaling by 2^k.  Within 2 ulp of exp.
+EFL_DEV float efl_exp(float x) {
+    if (x < -104.0f) return 0.0f;
+    if (x > 88.5f) return __int_as_float(0x7f800000);
+    float kf = rintf(x * 1.44269504088896341f);
+    float r = (x - kf * 0.693145751953125f) - kf * 1.42860682030941723e-6f;
+    float p = 1.98412698412698413e-4f;  // 1/7!
+    p = p * r + 1.38888888888888889e-3f;
+    p = p * r + 8.33333333333333333e-3f;
+    p = p * r + 4.16666666666666667e-2f;
+    p = p * r + 1.66666666666666667e-1f;
+    p = p * r + 0.5f;
+    p = p * r + 1.0f;
+    p = p * r + 1.0f;
+    return ldexpf(p, (int)kf);
+}
 // apply_forces.wgsl:73-76
 EFL_DEV float gaussian_2d(float x, float y, float x0, float y0, float sigma) {
     float b = -1.0f / (2.0f * sigma * sigma);
     float dx = x - x0, dy = y - y0;
-    return expf(b * (dx * dx + dy * dy));
+    return efl_exp(b * (dx * dx + dy * dy));
 }
 // apply_forces.wgsl:17-43 / 45-71 (comp 0 = u, x-major; comp 1 = v, y-major)
 template <int COMP>

@@ -363,12 +363,32 @@ void k_advect(eflo_sim& s) {
     });
 }
 
+// exp of the Gaussian force splat: WGSL's exp is implementation-defined, so
+// the oracle and the CUDA library share one restated method -- Cody-Waite
+// reduction x = k ln2 + r (ln2 split hi/lo, |r| <= ln2/2), degree-7 Taylor
+// polynomial for exp(r) in Horner form, exact scaling by 2^k.
+inline float efl_exp(float x) {
+    if (x < -104.0f) return 0.0f;
+    if (x > 88.5f) return std::numeric_limits<float>::infinity();
+    float kf = std::rint(x * 1.44269504088896341f);
+    float r = (x - kf * 0.693145751953125f) - kf * 1.42860682030941723e-6f;
+    float p = 1.98412698412698413e-4f;
+    p = p * r + 1.38888888888888889e-3f;
+    p = p * r + 8.33333333333333333e-3f;
+    p = p * r + 4.16666666666666667e-2f;
+    p = p * r + 1.66666666666666667e-1f;
+    p = p * r + 0.5f;
+    p = p * r + 1.0f;
+    p = p * r + 1.0f;
+    return std::ldexp(p, (int)kf);
+}
 // apply_forces.wgsl:73-76
 inline float gaussian_2d(float x, float y, float x0, float y0, float sigma) {
     float b = -1.0f / (2.0f * sigma * sigma);
     float dx = x - x0, dy = y - y0;
-    return std::exp(b * (dx * dx + dy * dy));
+    return efl_exp(b * (dx * dx + dy * dy));
 }
+float exp_for_test(float x) { return efl_exp(x); }
 // apply_forces.wgsl:17-71
 void k_apply_forces(eflo_sim& s) {
     const Uniform& U = s.U;
@@ -1537,6 +1557,8 @@ int32_t eflo_get_threads(void) {
     return 1;
 #endif
 }
+float eflo_exp(float x) { return exp_for_test(x); }
+
 void eflo_set_fim_serial(eflo_sim* s, int32_t on) {
     if (s) s->fim_serial = on != 0;
 }

@@ -56,6 +56,9 @@ EFL_API int32_t eflo_get_threads(void);
  * the deterministic two-phase variant. 1 = use it, 0 = two-phase. */
 EFL_API void eflo_set_fim_serial(eflo_sim* sim, int32_t on);
 
+/* The shared exp restatement used by the Gaussian force splat. */
+EFL_API float eflo_exp(float x);
+
 #ifdef __cplusplus
 }
 #endif
