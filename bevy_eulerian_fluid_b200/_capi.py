@@ -124,10 +124,13 @@ SIGNATURES = {
     "fluid_volume": (C.c_int, ["X", C.POINTER(C.c_uint64)]),
     "kernel_launches": (C.c_uint64, []),
     "pressure_sweeps": (C.c_int, ["X", C.c_int32, C.c_uint32]),
+    "residual_norms_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
+                                         C.c_uint32, C.c_size_t, C.c_float, C.c_float, C.c_float, C.c_void_p,
+                                         C.c_void_p]),
 }
 # Functions of efl.h that the oracle restatement does not mirror.
 PRODUCT_ONLY = {"abi_version", "default_config", "field_device_ptr", "stream", "synchronize", "kernel_launches",
-                "pressure_sweeps"}
+                "pressure_sweeps", "residual_norms_noalloc"}
 
 
 class EflError(RuntimeError):
@@ -322,6 +325,12 @@ class Sim:
         p = C.c_void_p()
         self._check(self.api.stream(self.h, C.byref(p)))
         return p.value or 0
+
+    def device_ptr(self, field: int):
+        """(device pointer, row pitch in bytes) of a field plane."""
+        p, pitch = C.c_void_p(), C.c_size_t()
+        self._check(self.api.field_device_ptr(self.h, field, C.byref(p), C.byref(pitch)))
+        return p.value, pitch.value
 
     def pressure_sweeps(self, precision: int, iterations: int):
         self._check(self.api.pressure_sweeps(self.h, precision, iterations))

@@ -9,6 +9,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <mutex>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -938,3 +939,95 @@ efl_status efl_pressure_sweeps(efl_sim* s, int32_t precision, uint32_t iteration
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free residual norms.
+//
+// Some callers cannot let a library allocate device memory: an engine that
+// owns every GPU buffer through its own arena (for example fields exported
+// from its renderer), or a real-time frame loop that forbids allocation once
+// it is running.  efl_residual_norms_noalloc serves them: it reads the
+// caller's buffers, writes the caller's output, and keeps its per-block
+// partial sums in the fixed file-scope array below instead of in memory from
+// cudaMalloc.  Every GPU that loads this library holds the array (256 KiB)
+// until the process exits.
+namespace {
+
+constexpr int kNoAllocCellsPerBlock = 1024;  // NORM_THREADS threads x 4 cells
+constexpr int kNoAllocMaxBlocks = 16384;
+constexpr uint64_t kNoAllocMaxCells = (uint64_t)kNoAllocMaxBlocks * kNoAllocCellsPerBlock;  // 4096 x 4096
+constexpr int kNoAllocMaxDevices = 64;
+
+static __device__ __align__(256) double2 g_noalloc_partials[kNoAllocMaxBlocks];
+
+// Device address of g_noalloc_partials per device ordinal.  Host code must
+// not pass the symbol itself to a kernel: on the host it only names a
+// stand-in object.
+std::mutex g_noalloc_mu;
+double2* g_noalloc_addr[kNoAllocMaxDevices] = {};
+
+__global__ void k_norm_finalize_rel(const double2* partials, int n, double* out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double r = 0.0, b = 0.0;
+    for (int i = 0; i < n; ++i) {
+        r += partials[i].x;
+        b += partials[i].y;
+    }
+    double nr = sqrt(r), nb = sqrt(b);
+    out[0] = b > 0.0 ? nr / nb : (r > 0.0 ? INFINITY : 0.0);
+    out[1] = nr;
+    out[2] = nb;
+}
+
+}  // namespace
+
+extern "C" efl_status efl_residual_norms_noalloc(const float* pressure, const float* divergence,
+                                                 const float* levelset_air, const float* area_fraction_u,
+                                                 const float* area_fraction_v, uint32_t nx, uint32_t ny,
+                                                 size_t pitch_bytes, float dx, float dt, float rho,
+                                                 double* out_device, void* stream) {
+    efl_sim* s = nullptr;  // errors go to efl_last_error(NULL)
+    if (!pressure || !divergence || !levelset_air || !area_fraction_u || !area_fraction_v || !out_device)
+        return set_err(s, EFL_ERR_INVALID_ARGUMENT, "efl_residual_norms_noalloc: null pointer argument");
+    if (nx == 0 || ny == 0)
+        return set_err(s, EFL_ERR_INVALID_ARGUMENT, "efl_residual_norms_noalloc: empty grid %ux%u", nx, ny);
+    if ((uint64_t)nx * ny > kNoAllocMaxCells)
+        return set_err(s, EFL_ERR_INVALID_ARGUMENT,
+                       "efl_residual_norms_noalloc: %ux%u = %llu cells exceeds the fixed scratch limit of %llu cells "
+                       "(4096 x 4096); use efl_residual on an efl_sim for larger grids",
+                       nx, ny, (unsigned long long)nx * ny, (unsigned long long)kNoAllocMaxCells);
+    if (pitch_bytes % sizeof(float) != 0 || pitch_bytes < (size_t)(nx + 1) * sizeof(float))
+        return set_err(s, EFL_ERR_INVALID_ARGUMENT,
+                       "efl_residual_norms_noalloc: pitch %zu bytes must be a multiple of 4 and hold nx+1 floats",
+                       pitch_bytes);
+    int dev = 0;
+    CU(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kNoAllocMaxDevices)
+        return set_err(s, EFL_ERR_INVALID_ARGUMENT, "efl_residual_norms_noalloc: device ordinal %d unsupported", dev);
+    double2* partials = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_noalloc_mu);
+        if (!g_noalloc_addr[dev]) {  // once per device, with that device current
+            void* p = nullptr;
+            CU(cudaGetSymbolAddress(&p, g_noalloc_partials));
+            g_noalloc_addr[dev] = (double2*)p;
+        }
+        partials = g_noalloc_addr[dev];
+    }
+    const int P = (int)(pitch_bytes / sizeof(float));
+    Level L{};
+    L.nx = (int)nx;
+    L.ny = (int)ny;
+    L.x = PF{const_cast<float*>(pressure), (int)nx, (int)ny, P};
+    L.b = PF{const_cast<float*>(divergence), (int)nx, (int)ny, P};
+    L.r = L.x;  // not read by the norm kernel
+    L.ls = PF{const_cast<float*>(levelset_air), (int)nx, (int)ny, P};
+    L.fu = PF{const_cast<float*>(area_fraction_u), (int)nx + 1, (int)ny, P};
+    L.fv = PF{const_cast<float*>(area_fraction_v), (int)nx, (int)ny + 1, P};
+    const int blocks = (int)(((uint64_t)nx * ny + kNoAllocCellsPerBlock - 1) / kNoAllocCellsPerBlock);
+    cudaStream_t st = (cudaStream_t)stream;
+    k_residual_norm<float><<<blocks, NORM_THREADS, count_launch(), st>>>(L, dt, rho, dx, partials);
+    k_norm_finalize_rel<<<1, 32, count_launch(), st>>>(partials, blocks, out_device);
+    LAUNCH_CHECK();
+    return EFL_OK;
+}

@@ -322,6 +322,38 @@ EFL_API uint64_t efl_kernel_launches(void);
  * iterate of the tolerance-driven solve, in place. */
 EFL_API efl_status efl_pressure_sweeps(efl_sim* sim, int32_t precision, uint32_t iterations);
 
+/* ---- Allocation-free entry point -------------------------------------- */
+
+/* Relative residual ||b - A p||_2 / ||b||_2 (operator of residual.wgsl:33-54,
+ * FP64 norms over cells with phi < 0 that are not fully solid) of fields held
+ * in caller-owned device memory, for callers that cannot let a library
+ * allocate device memory (an engine that owns all GPU buffers through its own
+ * arena, a frame loop that forbids allocation once running).  It has no
+ * counterpart in the reference.
+ *  - Inputs: device planes sharing one row pitch (bytes, multiple of 4, at
+ *    least (nx+1)*4): pressure, divergence and levelset_air (nx x ny),
+ *    area_fraction_u ((nx+1) x ny) and area_fraction_v (nx x (ny+1)), the
+ *    layout efl_field_device_ptr returns; dx = 1/length_unit, dt, rho as in
+ *    the step.
+ *  - Output: out_device[0..2] = relative residual, ||r||_2, ||b||_2 (device
+ *    memory), written asynchronously on `stream` (NULL: the legacy stream).
+ *  - Allocates nothing: the per-block partial sums live in a fixed 256 KiB
+ *    device array inside the library, which every GPU that loads the library
+ *    holds until exit.  Grids above 4096 x 4096 = 16,777,216 cells are
+ *    rejected with EFL_ERR_INVALID_ARGUMENT.
+ *  - The first call on a device looks up that array's device address (with
+ *    that device current); make that first call before any stream capture.
+ *  - All calls share the one array: calls whose work overlaps on the GPU
+ *    (different streams, or different host threads, at the same time) race
+ *    and may return wrong norms.  Each call overwrites every partial it
+ *    reads, so nothing carries over from the previous call.
+ * Errors are reported through efl_last_error(NULL). */
+EFL_API efl_status efl_residual_norms_noalloc(const float* pressure, const float* divergence,
+                                              const float* levelset_air, const float* area_fraction_u,
+                                              const float* area_fraction_v, uint32_t nx, uint32_t ny,
+                                              size_t pitch_bytes, float dx, float dt, float rho,
+                                              double* out_device, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
