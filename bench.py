@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--size", type=int, default=512)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-microbench", action="store_true")
+    ap.add_argument("--only", choices=["coupled", "microbench"], default=None,
+                    help="profiling aid: run one part only and print its numbers")
     return ap.parse_args()
 
 
@@ -204,6 +206,9 @@ def main():
     from bevy_eulerian_fluid_b200.rigid import RigidWorld
 
     torch.cuda.set_device(local)
+    if args.only == "microbench":
+        print(json.dumps(microbench(capi.load(), None, torch, measured_peaks()[0])), flush=True)
+        return 0
     dist = None
     if world > 1:
         import datetime
@@ -293,7 +298,7 @@ def main():
                 "note": f"32 B/cell/RB-iteration x {sc.cells} cells; working set is L2-resident at this size"}
 
     micro = None
-    if not args.no_microbench and rank == 0:
+    if not args.no_microbench and rank == 0 and args.only is None:
         micro = microbench(api, stream, torch, peak)
 
     sim.close()

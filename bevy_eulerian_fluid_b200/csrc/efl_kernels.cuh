@@ -415,7 +415,11 @@ EFL_DEV T gs_update(const LevelT<T>& L, T c_div, T weight, int x, int y) {
         }
     }
     if (fabs(denom) < (T)1.0e-6f) return T(0);
-    T p_new = nume / denom;
+    // f32: the reference's division; f64 (tolerance-driven, an extension):
+    // nume * (1/denom), the form the persistent solver evaluates.
+    T p_new;
+    if constexpr (sizeof(T) == 8) p_new = nume * (T(1) / denom);
+    else p_new = nume / denom;
     return weight * p_new + (T(1) - weight) * p_old;
 }
 // ((dx*dx)*rho)/dt as gauss_seidel.wgsl:58 evaluates it, dx = resolution_scale*dx.
@@ -440,6 +444,9 @@ EFL_DEV T residual_factor(float dt, float rho, float dx_scaled) {
     T d = (T)dx_scaled;
     return (T)dt / (T)rho / d / d;
 }
+// f32: the reference's operation order.  f64: the same operator in
+// factored form r = b - factor * (denom * x - sum_fluid f * x_nb), denom
+// accumulated in the reference's neighbour order.
 template <class T>
 EFL_DEV T residual_at(const LevelT<T>& L, T factor, int x, int y, bool* counted) {
     *counted = false;
@@ -449,19 +456,37 @@ EFL_DEV T residual_at(const LevelT<T>& L, T factor, int x, int y, bool* counted)
     if (f0 == 0.0f && f1 == 0.0f && f2 == 0.0f && f3 == 0.0f) return T(0);
     *counted = true;
     T xc = L.x.at(x, y);
-    T r = L.b.at(x, y);
     const int ox[4] = {-1, 1, 0, 0}, oy[4] = {0, 0, -1, 1};
     const T fvv[4] = {(T)f0, (T)f1, (T)f2, (T)f3};
+    if constexpr (sizeof(T) == 8) {
+        T denom = T(0), sum = T(0);
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        int jx = x + ox[i], jy = y + oy[i];
-        if ((unsigned)jx < (unsigned)L.nx && (unsigned)jy < (unsigned)L.ny) {
-            float pn = L.ls.at(jx, jy);
-            if (pn < 0.0f) r -= fvv[i] * (xc - L.x.at(jx, jy)) * factor;
-            else r -= fvv[i] * (T(1) - (T)pn / (T)phi) * xc * factor;
+        for (int i = 0; i < 4; ++i) {
+            int jx = x + ox[i], jy = y + oy[i];
+            if ((unsigned)jx < (unsigned)L.nx && (unsigned)jy < (unsigned)L.ny) {
+                float pn = L.ls.at(jx, jy);
+                if (pn < 0.0f) {
+                    denom += fvv[i];
+                    sum += fvv[i] * L.x.at(jx, jy);
+                } else {
+                    denom += fvv[i] * (T(1) - (T)pn / (T)phi);
+                }
+            }
         }
+        return L.b.at(x, y) - factor * (denom * xc - sum);
+    } else {
+        T r = L.b.at(x, y);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            int jx = x + ox[i], jy = y + oy[i];
+            if ((unsigned)jx < (unsigned)L.nx && (unsigned)jy < (unsigned)L.ny) {
+                float pn = L.ls.at(jx, jy);
+                if (pn < 0.0f) r -= fvv[i] * (xc - L.x.at(jx, jy)) * factor;
+                else r -= fvv[i] * (T(1) - (T)pn / (T)phi) * xc * factor;
+            }
+        }
+        return r;
     }
-    return r;
 }
 template <class T>
 __global__ void k_residual(LevelT<T> L, float dt, float rho, float dx_scaled) {

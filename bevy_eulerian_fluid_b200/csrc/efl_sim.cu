@@ -398,23 +398,41 @@ efl_status st_projection(efl_sim* s, efl_step_stats* st) {
         dim3 g = grid2d(d.nx, d.ny, kBlock);
         k_widen<<<g, kBlock, count_launch(), s->stream>>>(s->p0, s->div, L.x, L.b);
         LAUNCH_CHECK();
-        double r;
-        TRY(relative_residual(s, L, &r));
-        r0 = r;
+        double r = -1.0;
+        bool done = false;
         if (P.method == EFL_PROJECTION_GAUSS_SEIDEL) {
-            uint32_t chk = std::max<uint32_t>(1, P.check_interval);
-            while (!(r <= (double)P.tolerance) && iters < P.max_iterations) {
-                uint32_t n = std::min(chk, P.max_iterations - iters);
-                TRY(solve_gs_fixed(s->solver, L, s->U, P.sor_weight, n, s->stream));
-                LAUNCH_CHECK();
-                iters += n;
-                TRY(relative_residual(s, L, &r));
+            // One cooperative launch for the whole solve when the grid fits.
+            SolveResult res{};
+            std::string perr;
+            efl_status ps = solve_gs64_persistent(s->solver, L, s->U, P.sor_weight, (double)P.tolerance,
+                                                  P.max_iterations, P.check_interval, s->stream, &res, &perr);
+            if (ps == EFL_OK) {
+                iters = res.iterations;
+                r0 = res.r0;
+                r = res.r1;
+                done = true;
+            } else if (ps != EFL_ERR_STATE) {
+                return set_err(s, ps, "%s", perr.c_str());
             }
-        } else {
-            while (!(r <= (double)P.tolerance) && iters < P.max_iterations) {
-                TRY(v_cycle(s, s->mg64, 0));
-                ++iters;
-                TRY(relative_residual(s, L, &r));
+        }
+        if (!done) {
+            TRY(relative_residual(s, L, &r));
+            r0 = r;
+            if (P.method == EFL_PROJECTION_GAUSS_SEIDEL) {
+                uint32_t chk = std::max<uint32_t>(1, P.check_interval);
+                while (!(r <= (double)P.tolerance) && iters < P.max_iterations) {
+                    uint32_t n = std::min(chk, P.max_iterations - iters);
+                    TRY(solve_gs_fixed(s->solver, L, s->U, P.sor_weight, n, s->stream));
+                    LAUNCH_CHECK();
+                    iters += n;
+                    TRY(relative_residual(s, L, &r));
+                }
+            } else {
+                while (!(r <= (double)P.tolerance) && iters < P.max_iterations) {
+                    TRY(v_cycle(s, s->mg64, 0));
+                    ++iters;
+                    TRY(relative_residual(s, L, &r));
+                }
             }
         }
         r1 = r;
@@ -932,8 +950,18 @@ efl_status efl_pressure_sweeps(efl_sim* s, int32_t precision, uint32_t iteration
     if (precision != 32 && precision != 64) return set_err(s, EFL_ERR_INVALID_ARGUMENT, "precision must be 32 or 64");
     cudaSetDevice(s->device);
     const float w = s->cfg.projection.sor_weight;
-    if (precision == 32) TRY(solve_gs_fixed(s->solver, s->mg[0], s->U, w, iterations, s->stream));
-    else TRY(solve_gs_fixed(s->solver, s->mg64[0], s->U, w, iterations, s->stream));
+    if (precision == 32) {
+        TRY(solve_gs_fixed(s->solver, s->mg[0], s->U, w, iterations, s->stream));
+    } else {
+        // The tolerance-driven solver with an unreachable tolerance: exactly
+        // `iterations` iterations, residual evaluated before and after only.
+        SolveResult res{};
+        std::string perr;
+        efl_status ps = solve_gs64_persistent(s->solver, s->mg64[0], s->U, w, 0.0, iterations,
+                                              std::max<uint32_t>(1, iterations), s->stream, &res, &perr);
+        if (ps == EFL_ERR_STATE) TRY(solve_gs_fixed(s->solver, s->mg64[0], s->U, w, iterations, s->stream));
+        else if (ps != EFL_OK) return set_err(s, ps, "%s", perr.c_str());
+    }
     LAUNCH_CHECK();
     return EFL_OK;
 }

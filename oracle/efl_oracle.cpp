@@ -29,6 +29,7 @@
 #include <cstring>
 #include <limits>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #ifdef _OPENMP
@@ -443,8 +444,10 @@ void k_divergence(eflo_sim& s) {
 }
 
 // projection/shaders/gauss_seidel.wgsl:44-88 (update_pressure).  With
-// T = float this is the reference's f32 arithmetic; with T = double the
-// same expression tree is evaluated in f64 from the f32 inputs.
+// T = float this is the reference's f32 arithmetic.  With T = double (the
+// tolerance-driven solve, an extension) the same loop runs in f64 from the
+// f32 inputs and the final division is nume * (1/denom): the CUDA solver
+// keeps 1/denom per cell for the whole solve.
 template <class T>
 inline T gs_update(const Tex<T>& p, const Tex<T>& b, const Tex<float>& ls, const Tex<F4>& af, const Uniform& U,
                    float weight, float res_scale, int x, int y) {
@@ -472,7 +475,9 @@ inline T gs_update(const Tex<T>& p, const Tex<T>& b, const Tex<float>& ls, const
         }
     }
     if (std::fabs(denom) < (T)1.0e-6f) return T(0);
-    T p_new = nume / denom;
+    T p_new;
+    if (std::is_same<T, double>::value) p_new = nume * (T(1) / denom);
+    else p_new = nume / denom;
     T w = (T)weight;
     return w * p_new + (T(1) - w) * p_old;
 }
@@ -494,7 +499,10 @@ void gs_iterations(Tex<T>& p, const Tex<T>& b, const Tex<float>& ls, const Tex<F
     }
 }
 
-// projection/shaders/residual.wgsl:12-57
+// projection/shaders/residual.wgsl:12-57.  T = float: the reference's
+// operation order.  T = double: the same operator in factored form,
+// r = b - factor * (denom * x - sum_fluid f * x_nb), with denom accumulated
+// in the reference's neighbour order (the CUDA solver keeps denom per cell).
 template <class T>
 inline T residual_at(const Tex<T>& xt, const Tex<T>& b, const Tex<float>& ls, const Tex<F4>& af, const Uniform& U,
                      float res_scale, int x, int y, bool* counted) {
@@ -507,9 +515,25 @@ inline T residual_at(const Tex<T>& xt, const Tex<T>& b, const Tex<float>& ls, co
     T xc = xt.ld(x, y);
     T dx = (T)(U.dx * res_scale);
     T factor = (T)U.dt / (T)U.rho / dx / dx;
-    T r = b.ld(x, y);
     static const int off[4][2] = {{-1, 0}, {1, 0}, {0, -1}, {0, 1}};
     const T fv[4] = {(T)f.x, (T)f.y, (T)f.z, (T)f.w};
+    if (std::is_same<T, double>::value) {
+        T denom = T(0), sum = T(0);
+        for (int i = 0; i < 4; ++i) {
+            int jx = x + off[i][0], jy = y + off[i][1];
+            if (jx >= 0 && jy >= 0 && jx < ls.w && jy < ls.h) {
+                float pn = ls.ld(jx, jy);
+                if (pn < 0.0f) {
+                    denom += fv[i];
+                    sum += fv[i] * xt.ld(jx, jy);
+                } else {
+                    denom += fv[i] * (T(1) - (T)pn / (T)phi);
+                }
+            }
+        }
+        return b.ld(x, y) - factor * (denom * xc - sum);
+    }
+    T r = b.ld(x, y);
     for (int i = 0; i < 4; ++i) {
         int jx = x + off[i][0], jy = y + off[i][1];
         if (jx >= 0 && jy >= 0 && jx < ls.w && jy < ls.h) {
