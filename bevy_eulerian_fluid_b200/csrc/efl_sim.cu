@@ -386,7 +386,10 @@ efl_status st_projection(efl_sim* s, efl_step_stats* st) {
         iters = 50;
     } else if (P.tolerance <= 0.0f) {
         if (P.method == EFL_PROJECTION_GAUSS_SEIDEL) {
-            TRY(solve_gs_fixed(s->solver, s->mg[0], s->U, P.sor_weight, P.gs_iterations, s->stream));
+            if (solve_gs32_tiled(s->mg[0], s->p1, s->U.dx, s->U.rho, s->U.dt, P.sor_weight, P.gs_iterations,
+                                 s->stream) != EFL_OK)
+                return set_err(s, EFL_ERR_CUDA, "tiled Gauss-Seidel launch failed: %s",
+                               cudaGetErrorString(cudaGetLastError()));
             LAUNCH_CHECK();
             iters = P.gs_iterations;
         } else {
@@ -951,7 +954,8 @@ efl_status efl_pressure_sweeps(efl_sim* s, int32_t precision, uint32_t iteration
     cudaSetDevice(s->device);
     const float w = s->cfg.projection.sor_weight;
     if (precision == 32) {
-        TRY(solve_gs_fixed(s->solver, s->mg[0], s->U, w, iterations, s->stream));
+        if (solve_gs32_tiled(s->mg[0], s->p1, s->U.dx, s->U.rho, s->U.dt, w, iterations, s->stream) != EFL_OK)
+            return set_err(s, EFL_ERR_CUDA, "tiled Gauss-Seidel launch failed");
     } else {
         // The tolerance-driven solver with an unreachable tolerance: exactly
         // `iterations` iterations, residual evaluated before and after only.

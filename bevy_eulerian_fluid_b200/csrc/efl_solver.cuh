@@ -102,98 +102,78 @@ struct PersistentParams {
     SolveResult* result;
 };
 
-constexpr unsigned char M_DOMAIN = 1, M_FLUID = 2, M_COUNTED = 4, M_UPDATE = 8;
-
-struct PsSmem {
-    double* p;
-    double* b;
-    double* den;
-    double* inv;
-    float* fu;  // (EX+1) x EY: face lx sits between cells lx-1 and lx
-    float* fv;  // EX x (EY+1)
-    unsigned char* m;
-    int EX, EY;
+// Shared-memory image of one extended tile (EX x EY cells, EX even), stored
+// per colour in checkerboard-compressed form: cell (lx, ly) of colour
+// c = (gx + gy) & 1 lives at [c][ly][lx >> 1].  A cell's left / right
+// neighbours are the other colour's entries (lx >> 1) - 1 + (lx & 1) and
+// (lx >> 1) + (lx & 1) of the same row, up / down are entry lx >> 1 of the
+// rows above and below, so a warp reads consecutive doubles.
+template <int EX, int EY>
+struct PsTile {
+    static constexpr int W2 = EX / 2;
+    static constexpr int N2 = W2 * EY;  // entries per colour
+    double p[2][N2];
+    double b[2][N2];
+    double inv[2][N2];   // 1/denom, 0 where the cell does not update
+    double den[2][N2];   // denom (residual)
+    float4 w[2][N2];     // neighbour weights (-x, +x, -y, +y): face fraction, or 0 for air / outside
+    unsigned char mode[2][N2];  // MODE_*
 };
+constexpr unsigned char MODE_SKIP = 0;     // outside the domain or on the tile's outer ring
+constexpr unsigned char MODE_ZERO = 1;     // air, fully solid or |denom| < 1e-6: p = 0
+constexpr unsigned char MODE_UPDATE = 2;   // regular update
+constexpr unsigned char MODE_COUNTED = 4;  // counted in the residual norms
 
-EFL_DEV PsSmem ps_carve(unsigned char* base, int EX, int EY) {
-    PsSmem s;
-    const int n = EX * EY;
-    s.EX = EX;
-    s.EY = EY;
-    s.p = reinterpret_cast<double*>(base);
-    s.b = s.p + n;
-    s.den = s.b + n;
-    s.inv = s.den + n;
-    s.fu = reinterpret_cast<float*>(s.inv + n);
-    s.fv = s.fu + (EX + 1) * EY;
-    s.m = reinterpret_cast<unsigned char*>(s.fv + EX * (EY + 1));
-    return s;
-}
-inline size_t ps_smem_bytes(int EX, int EY) {
-    const size_t n = (size_t)EX * EY;
-    return n * 4 * sizeof(double) + (size_t)(EX + 1) * EY * 4 + (size_t)EX * (EY + 1) * 4 + n;
-}
-
-// One half-sweep of colour `color` ((x+y)&1 == color) over the extended
-// tile minus its outer ring.  Update of the tolerance-driven mode:
-// p = w * ((cdiv*b + sum w_k p_k) * (1/denom)) + (1-w) * p, neighbour order
-// (-x, +x, -y, +y) as gauss_seidel.wgsl:68-79; w_k = 0 for air or
-// out-of-domain neighbours.
-EFL_DEV void ps_half_sweep(const PsSmem& s, int gx0, int gy0, int color, double cdiv, double w, double omw) {
-    const int EX = s.EX, EY = s.EY;
-    const int half = (EX - 2 + 1) / 2;
-    const int total = half * (EY - 2);
-    for (int i = threadIdx.x; i < total; i += blockDim.x) {
-        const int ly = 1 + i / half;
-        const int j = i - (ly - 1) * half;
-        const int lx0 = 1 + ((color + gx0 + gy0 + ly + 1) & 1);
-        const int lx = lx0 + 2 * j;
-        if (lx > EX - 2) continue;
-        const int c = ly * EX + lx;
-        const unsigned char m = s.m[c];
-        if (!(m & M_DOMAIN)) continue;
-        if (!(m & M_UPDATE)) {
-            s.p[c] = 0.0;
-            continue;
+template <int EX, int EY>
+EFL_DEV void ps_half_sweep(PsTile<EX, EY>& T, int base, int c, double cdiv, double w, double omw) {
+    constexpr int W2 = EX / 2;
+    constexpr int TOTAL = (EY - 2) * W2;
+    const int o = 1 - c;
+#pragma unroll 2
+    for (int i = threadIdx.x; i < TOTAL; i += PS_THREADS) {
+        const int ly = 1 + i / W2;
+        const int j = i - (ly - 1) * W2;
+        const int k = ly * W2 + j;
+        const unsigned char m = T.mode[c][k];
+        if (m & MODE_UPDATE) {
+            const int odd = (base + ly + c) & 1;  // lx & 1 of a colour-c cell in row ly
+            const float4 wk = T.w[c][k];
+            double nume = cdiv * T.b[c][k];
+            nume = nume + (double)wk.x * T.p[o][k - 1 + odd];
+            nume = nume + (double)wk.y * T.p[o][k + odd];
+            nume = nume + (double)wk.z * T.p[o][k - W2];
+            nume = nume + (double)wk.w * T.p[o][k + W2];
+            T.p[c][k] = w * (nume * T.inv[c][k]) + omw * T.p[c][k];
+        } else if (m & MODE_ZERO) {
+            T.p[c][k] = 0.0;
         }
-        const double w0 = (s.m[c - 1] & M_FLUID) ? (double)s.fu[ly * (EX + 1) + lx] : 0.0;
-        const double w1 = (s.m[c + 1] & M_FLUID) ? (double)s.fu[ly * (EX + 1) + lx + 1] : 0.0;
-        const double w2 = (s.m[c - EX] & M_FLUID) ? (double)s.fv[ly * EX + lx] : 0.0;
-        const double w3 = (s.m[c + EX] & M_FLUID) ? (double)s.fv[(ly + 1) * EX + lx] : 0.0;
-        double nume = cdiv * s.b[c];
-        nume = nume + w0 * s.p[c - 1];
-        nume = nume + w1 * s.p[c + 1];
-        nume = nume + w2 * s.p[c - EX];
-        nume = nume + w3 * s.p[c + EX];
-        s.p[c] = w * (nume * s.inv[c]) + omw * s.p[c];
     }
 }
 
-// ||r||^2 and ||b||^2 over the owned cells of this tile (all halo cells
-// valid), r = b - factor * (denom * p - sum w_k p_k).
-EFL_DEV double2 ps_residual_partial(const PsSmem& s, int H, int tx, int ty, double factor) {
-    const int EX = s.EX;
+// ||r||^2 and ||b||^2 over the owned cells (all halo values valid),
+// r = b - factor * (denom * p - sum w_k p_k).
+template <int EX, int EY>
+EFL_DEV double2 ps_residual_partial(const PsTile<EX, EY>& T, int base, int H, int tx, int ty, double factor) {
+    constexpr int W2 = EX / 2;
     double ar = 0.0, ab = 0.0;
-    for (int i = threadIdx.x; i < tx * ty; i += blockDim.x) {
+    for (int i = threadIdx.x; i < tx * ty; i += PS_THREADS) {
         const int ly = H + i / tx, lx = H + i % tx;
-        const int c = ly * EX + lx;
-        const unsigned char m = s.m[c];
-        if ((m & (M_DOMAIN | M_COUNTED)) != (M_DOMAIN | M_COUNTED)) continue;
-        const double w0 = (s.m[c - 1] & M_FLUID) ? (double)s.fu[ly * (EX + 1) + lx] : 0.0;
-        const double w1 = (s.m[c + 1] & M_FLUID) ? (double)s.fu[ly * (EX + 1) + lx + 1] : 0.0;
-        const double w2 = (s.m[c - EX] & M_FLUID) ? (double)s.fv[ly * EX + lx] : 0.0;
-        const double w3 = (s.m[c + EX] & M_FLUID) ? (double)s.fv[(ly + 1) * EX + lx] : 0.0;
-        double sum = w0 * s.p[c - 1];
-        sum = sum + w1 * s.p[c + 1];
-        sum = sum + w2 * s.p[c - EX];
-        sum = sum + w3 * s.p[c + EX];
-        const double r = s.b[c] - factor * (s.den[c] * s.p[c] - sum);
+        const int c = (base + lx + ly) & 1, o = 1 - c, odd = lx & 1;
+        const int k = ly * W2 + (lx >> 1);
+        if (!(T.mode[c][k] & MODE_COUNTED)) continue;
+        const float4 wk = T.w[c][k];
+        double sum = (double)wk.x * T.p[o][k - 1 + odd];
+        sum = sum + (double)wk.y * T.p[o][k + odd];
+        sum = sum + (double)wk.z * T.p[o][k - W2];
+        sum = sum + (double)wk.w * T.p[o][k + W2];
+        const double bb = T.b[c][k];
+        const double r = bb - factor * (T.den[c][k] * T.p[c][k] - sum);
         ar += r * r;
-        ab += s.b[c] * s.b[c];
+        ab += bb * bb;
     }
     ar = warp_sum(ar);
     ab = warp_sum(ab);
-    __shared__ double red_r[32], red_b[32];
+    __shared__ double red_r[PS_THREADS / 32], red_b[PS_THREADS / 32];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     if (lane == 0) {
         red_r[wid] = ar;
@@ -202,7 +182,7 @@ EFL_DEV double2 ps_residual_partial(const PsSmem& s, int H, int tx, int ty, doub
     __syncthreads();
     double2 out = make_double2(0.0, 0.0);
     if (threadIdx.x == 0) {
-        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) {
+        for (int k = 0; k < PS_THREADS / 32; ++k) {
             out.x += red_r[k];
             out.y += red_b[k];
         }
@@ -211,19 +191,24 @@ EFL_DEV double2 ps_residual_partial(const PsSmem& s, int H, int tx, int ty, doub
     return out;
 }
 
-EFL_DEV void ps_load_p(const PsSmem& s, const Level64& L, int gx0, int gy0) {
-    const int n = s.EX * s.EY;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        const int ly = i / s.EX, lx = i - ly * s.EX;
+template <int EX, int EY>
+EFL_DEV void ps_load_p(PsTile<EX, EY>& T, const Level64& L, int gx0, int gy0, int base) {
+    for (int i = threadIdx.x; i < EX * EY; i += PS_THREADS) {
+        const int ly = i / EX, lx = i - ly * EX;
         const int gx = gx0 + lx, gy = gy0 + ly;
-        s.p[i] = (s.m[i] & M_DOMAIN) ? __ldcg(&L.x.p[(size_t)gy * L.x.P + gx]) : 0.0;
+        const int c = (base + lx + ly) & 1;
+        const bool in = (unsigned)gx < (unsigned)L.nx && (unsigned)gy < (unsigned)L.ny;
+        T.p[c][ly * (EX / 2) + (lx >> 1)] = in ? __ldcg(&L.x.p[(size_t)gy * L.x.P + gx]) : 0.0;
     }
 }
-EFL_DEV void ps_store_owned(const PsSmem& s, const Level64& L, int gx0, int gy0, int H, int tx, int ty) {
-    for (int i = threadIdx.x; i < tx * ty; i += blockDim.x) {
+template <int EX, int EY>
+EFL_DEV void ps_store_owned(const PsTile<EX, EY>& T, const Level64& L, int gx0, int gy0, int base, int H, int tx,
+                            int ty) {
+    for (int i = threadIdx.x; i < tx * ty; i += PS_THREADS) {
         const int ly = H + i / tx, lx = H + i % tx;
-        const int c = ly * s.EX + lx;
-        if (s.m[c] & M_DOMAIN) __stcg(&L.x.p[(size_t)(gy0 + ly) * L.x.P + gx0 + lx], s.p[c]);
+        const int gx = gx0 + lx, gy = gy0 + ly;
+        if ((unsigned)gx < (unsigned)L.nx && (unsigned)gy < (unsigned)L.ny)
+            __stcg(&L.x.p[(size_t)gy * L.x.P + gx], T.p[(base + lx + ly) & 1][ly * (EX / 2) + (lx >> 1)]);
     }
 }
 // Sum of all CTAs' partials in CTA order; identical in every CTA.
@@ -244,70 +229,74 @@ EFL_DEV double ps_total_relative(const double2* partials, int nblocks) {
     return v;
 }
 
+template <int EX, int EY, int KMAX>
 __global__ void __launch_bounds__(PS_THREADS, 1) k_gs64_persistent(PersistentParams P) {
     extern __shared__ __align__(16) unsigned char ps_raw[];
-    const int H = P.halo;
-    const int EX = P.tx + 2 * H, EY = P.ty + 2 * H;
-    const PsSmem s = ps_carve(ps_raw, EX, EY);
+    PsTile<EX, EY>& T = *reinterpret_cast<PsTile<EX, EY>*>(ps_raw);
+    constexpr int H = 2 * KMAX;
+    constexpr int W2 = EX / 2;
+    const int tx = EX - 2 * H, ty = EY - 2 * H;
     const Level64& L = P.L;
     const int tile = blockIdx.x;
-    const int gx0 = (tile % P.tiles_x) * P.tx - H, gy0 = (tile / P.tiles_x) * P.ty - H;
+    const int gx0 = (tile % P.tiles_x) * tx - H, gy0 = (tile / P.tiles_x) * ty - H;
+    const int base = (gx0 + gy0) & 1;
     const unsigned nblocks = gridDim.x;
 
-    // Per-solve coefficients of the extended tile (gauss_seidel.wgsl:44-80 and
-    // residual.wgsl:21-54, neighbour order of the reference).
-    const int n = EX * EY;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    // Per-solve coefficients (gauss_seidel.wgsl:44-80 and residual.wgsl:21-54
+    // in the reference's neighbour order).
+    for (int i = threadIdx.x; i < EX * EY; i += PS_THREADS) {
         const int ly = i / EX, lx = i - ly * EX;
         const int gx = gx0 + lx, gy = gy0 + ly;
-        unsigned char m = 0;
+        const int c = (base + lx + ly) & 1, k = ly * W2 + (lx >> 1);
+        unsigned char m = MODE_SKIP;
         double den = 0.0, inv = 0.0, bb = 0.0;
+        float4 wk = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         if ((unsigned)gx < (unsigned)L.nx && (unsigned)gy < (unsigned)L.ny) {
-            m |= M_DOMAIN;
+            const bool ring = lx == 0 || ly == 0 || lx == EX - 1 || ly == EY - 1;
             const float phi = L.ls.at(gx, gy);
             bb = L.b.at(gx, gy);
+            bool update = false;
             if (phi < 0.0f) {
-                m |= M_FLUID;
                 const float f[4] = {L.fu.at(gx, gy), L.fu.at(gx + 1, gy), L.fv.at(gx, gy), L.fv.at(gx, gy + 1)};
                 if (!(f[0] == 0.0f && f[1] == 0.0f && f[2] == 0.0f && f[3] == 0.0f)) {
-                    m |= M_COUNTED;
+                    m |= MODE_COUNTED;
                     const int ox[4] = {-1, 1, 0, 0}, oy[4] = {0, 0, -1, 1};
+                    float wv[4] = {0.0f, 0.0f, 0.0f, 0.0f};
 #pragma unroll
-                    for (int k = 0; k < 4; ++k) {
-                        const int jx = gx + ox[k], jy = gy + oy[k];
+                    for (int q = 0; q < 4; ++q) {
+                        const int jx = gx + ox[q], jy = gy + oy[q];
                         if ((unsigned)jx < (unsigned)L.nx && (unsigned)jy < (unsigned)L.ny) {
                             const float level = L.ls.at(jx, jy);
-                            if (level < 0.0f) den += (double)f[k];
-                            else den += (double)f[k] * (1.0 - (double)level / (double)phi);
+                            if (level < 0.0f) {
+                                den += (double)f[q];
+                                wv[q] = f[q];
+                            } else {
+                                den += (double)f[q] * (1.0 - (double)level / (double)phi);
+                            }
                         }
                     }
+                    wk = make_float4(wv[0], wv[1], wv[2], wv[3]);
                     if (!(fabs(den) < (double)1.0e-6f)) {
-                        m |= M_UPDATE;
+                        update = true;
                         inv = 1.0 / den;
                     }
                 }
             }
+            if (!ring) m |= update ? MODE_UPDATE : MODE_ZERO;
         }
-        s.m[i] = m;
-        s.den[i] = den;
-        s.inv[i] = inv;
-        s.b[i] = bb;
-    }
-    for (int i = threadIdx.x; i < (EX + 1) * EY; i += blockDim.x) {
-        const int ly = i / (EX + 1), lx = i - ly * (EX + 1);
-        s.fu[i] = L.fu.ld(gx0 + lx, gy0 + ly);
-    }
-    for (int i = threadIdx.x; i < EX * (EY + 1); i += blockDim.x) {
-        const int ly = i / EX, lx = i - ly * EX;
-        s.fv[i] = L.fv.ld(gx0 + lx, gy0 + ly);
+        T.mode[c][k] = m;
+        T.den[c][k] = den;
+        T.inv[c][k] = inv;
+        T.b[c][k] = bb;
+        T.w[c][k] = wk;
     }
     __syncthreads();
-    ps_load_p(s, L, gx0, gy0);
+    ps_load_p(T, L, gx0, gy0, base);
     __syncthreads();
 
     const double w = P.weight, omw = 1.0 - P.weight;
     unsigned iters = 0;
-    double2 part = ps_residual_partial(s, H, P.tx, P.ty, P.factor);
+    double2 part = ps_residual_partial(T, base, H, tx, ty, P.factor);
     if (threadIdx.x == 0) P.partials[blockIdx.x] = part;
     bool ok = grid_barrier(P.barrier, nblocks);
     double r = ok ? ps_total_relative(P.partials, nblocks) : 0.0;
@@ -315,23 +304,23 @@ __global__ void __launch_bounds__(PS_THREADS, 1) k_gs64_persistent(PersistentPar
     while (ok && !(r <= P.tol) && iters < P.max_iters) {
         unsigned todo = min(P.check_interval, P.max_iters - iters);
         while (ok && todo > 0) {
-            const unsigned kk = min((unsigned)P.kmax, todo);
+            const unsigned kk = min((unsigned)KMAX, todo);
             for (unsigned it = 0; it < kk; ++it) {
-                ps_half_sweep(s, gx0, gy0, 1, P.cdiv, w, omw);  // red: (x+y) odd
+                ps_half_sweep(T, base, 1, P.cdiv, w, omw);  // red: (x+y) odd
                 __syncthreads();
-                ps_half_sweep(s, gx0, gy0, 0, P.cdiv, w, omw);  // black
+                ps_half_sweep(T, base, 0, P.cdiv, w, omw);  // black
                 __syncthreads();
             }
-            ps_store_owned(s, L, gx0, gy0, H, P.tx, P.ty);
+            ps_store_owned(T, L, gx0, gy0, base, H, tx, ty);
             ok = grid_barrier(P.barrier, nblocks);
             if (!ok) break;
-            ps_load_p(s, L, gx0, gy0);
+            ps_load_p(T, L, gx0, gy0, base);
             __syncthreads();
             todo -= kk;
             iters += kk;
         }
         if (!ok) break;
-        part = ps_residual_partial(s, H, P.tx, P.ty, P.factor);
+        part = ps_residual_partial(T, base, H, tx, ty, P.factor);
         if (threadIdx.x == 0) P.partials[blockIdx.x] = part;
         ok = grid_barrier(P.barrier, nblocks);
         if (!ok) break;
@@ -389,28 +378,181 @@ inline efl_status solve_gs_fixed(SolverWorkspace&, const LevelT<T>& L, const Uni
     return EFL_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Fixed-count f32 sweeps (the reference's mode) as tiled, temporally blocked
+// launches: each CTA loads its tile plus a halo of 2K cells, builds the
+// per-cell coefficients of gauss_seidel.wgsl:44-80 in the reference's f32
+// operation order (c*div, denom, neighbour weights), runs K red-black
+// iterations from shared memory and writes its owned cells to the other
+// buffer of a ping-pong pair.  Bit-identical to K global red/black sweeps.
+template <int EX, int EY>
+struct GsTile32 {
+    static constexpr int W2 = EX / 2;
+    static constexpr int N2 = W2 * EY;
+    float p[2][N2];
+    float cb[2][N2];
+    float den[2][N2];
+    float4 w[2][N2];
+    unsigned char mode[2][N2];
+};
+constexpr int GT_THREADS = 256;
+
+template <int EX, int EY, int K>
+__global__ void __launch_bounds__(GT_THREADS) k_gs32_tile(Level L, PF out, float dx_scaled, float rho, float dt,
+                                                          float weight, int tiles_x, int iters) {
+    extern __shared__ __align__(16) unsigned char gt_raw[];
+    GsTile32<EX, EY>& T = *reinterpret_cast<GsTile32<EX, EY>*>(gt_raw);
+    constexpr int H = 2 * K, W2 = EX / 2, TX = EX - 2 * H, TY = EY - 2 * H;
+    const int gx0 = (blockIdx.x % tiles_x) * TX - H, gy0 = (blockIdx.x / tiles_x) * TY - H;
+    const int base = (gx0 + gy0) & 1;
+    const float cdiv = dx_scaled * dx_scaled * rho / dt;  // gauss_seidel.wgsl:58
+    for (int i = threadIdx.x; i < EX * EY; i += GT_THREADS) {
+        const int ly = i / EX, lx = i - ly * EX;
+        const int gx = gx0 + lx, gy = gy0 + ly;
+        const int c = (base + lx + ly) & 1, k = ly * W2 + (lx >> 1);
+        unsigned char m = MODE_SKIP;
+        float den = 0.0f, cb = 0.0f, pv = 0.0f;
+        float4 wk = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if ((unsigned)gx < (unsigned)L.nx && (unsigned)gy < (unsigned)L.ny) {
+            pv = L.x.at(gx, gy);
+            const float lij = L.ls.at(gx, gy);
+            bool update = false;
+            if (lij < 0.0f) {
+                const float f[4] = {L.fu.at(gx, gy), L.fu.at(gx + 1, gy), L.fv.at(gx, gy), L.fv.at(gx, gy + 1)};
+                if (!(f[0] == 0.0f && f[1] == 0.0f && f[2] == 0.0f && f[3] == 0.0f)) {
+                    cb = cdiv * L.b.at(gx, gy);
+                    const int ox[4] = {-1, 1, 0, 0}, oy[4] = {0, 0, -1, 1};
+                    float wv[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const int jx = gx + ox[q], jy = gy + oy[q];
+                        if ((unsigned)jx < (unsigned)L.nx && (unsigned)jy < (unsigned)L.ny) {
+                            const float level = L.ls.at(jx, jy);
+                            if (level < 0.0f) {
+                                den += f[q];
+                                wv[q] = f[q];
+                            } else {
+                                den += f[q] * (1.0f - level / lij);
+                            }
+                        }
+                    }
+                    wk = make_float4(wv[0], wv[1], wv[2], wv[3]);
+                    update = !(fabsf(den) < 1.0e-6f);
+                }
+            }
+            const bool ring = lx == 0 || ly == 0 || lx == EX - 1 || ly == EY - 1;
+            if (!ring) m = update ? MODE_UPDATE : MODE_ZERO;
+        }
+        T.p[c][k] = pv;
+        T.cb[c][k] = cb;
+        T.den[c][k] = den;
+        T.w[c][k] = wk;
+        T.mode[c][k] = m;
+    }
+    __syncthreads();
+    const float omw = 1.0f - weight;
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+        for (int half = 0; half < 2; ++half) {
+            const int c = half == 0 ? 1 : 0, o = 1 - c;  // red ((x+y) odd) first
+            constexpr int TOTAL = (EY - 2) * W2;
+            for (int i = threadIdx.x; i < TOTAL; i += GT_THREADS) {
+                const int ly = 1 + i / W2;
+                const int k = ly * W2 + (i - (ly - 1) * W2);
+                const unsigned char m = T.mode[c][k];
+                if (m & MODE_UPDATE) {
+                    const int odd = (base + ly + c) & 1;
+                    const float4 wk = T.w[c][k];
+                    float nume = T.cb[c][k];
+                    nume = nume + wk.x * T.p[o][k - 1 + odd];
+                    nume = nume + wk.y * T.p[o][k + odd];
+                    nume = nume + wk.z * T.p[o][k - W2];
+                    nume = nume + wk.w * T.p[o][k + W2];
+                    const float pn = nume / T.den[c][k];
+                    T.p[c][k] = weight * pn + omw * T.p[c][k];
+                } else if (m & MODE_ZERO) {
+                    T.p[c][k] = 0.0f;
+                }
+            }
+            __syncthreads();
+        }
+    }
+    for (int i = threadIdx.x; i < TX * TY; i += GT_THREADS) {
+        const int ly = H + i / TX, lx = H + i % TX;
+        const int gx = gx0 + lx, gy = gy0 + ly;
+        if ((unsigned)gx < (unsigned)L.nx && (unsigned)gy < (unsigned)L.ny)
+            out.at(gx, gy) = T.p[(base + lx + ly) & 1][ly * W2 + (lx >> 1)];
+    }
+}
+
+// n fixed f32 red-black iterations on level L, ping-ponging between L.x and
+// `alt` (same extent and pitch); the result ends in L.x.
+inline efl_status solve_gs32_tiled(const Level& L, const PF& alt, float dx_scaled, float rho, float dt, float weight,
+                                   uint32_t n, cudaStream_t stream) {
+    constexpr int K = 2, EX = 64 + 4 * K, EY = 32 + 4 * K;  // 64 x 32 owned, two CTAs per SM
+    constexpr int TX = EX - 4 * K, TY = EY - 4 * K;
+    const size_t smem = sizeof(GsTile32<EX, EY>);
+    int dev = 0;
+    cudaGetDevice(&dev);
+    static bool attr_done[64] = {};
+    if (dev < 0 || dev >= 64) return EFL_ERR_CUDA;
+    if (!attr_done[dev]) {
+        if (cudaFuncSetAttribute(k_gs32_tile<EX, EY, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+            cudaSuccess)
+            return EFL_ERR_CUDA;
+        attr_done[dev] = true;
+    }
+    const int tiles_x = (L.nx + TX - 1) / TX, tiles_y = (L.ny + TY - 1) / TY;
+    Level cur = L;
+    PF dst = alt;
+    uint32_t launches = 0;
+    for (uint32_t done = 0; done < n;) {
+        const int k = (int)std::min<uint32_t>(K, n - done);
+        k_gs32_tile<EX, EY, K><<<tiles_x * tiles_y, GT_THREADS, smem + count_launch(), stream>>>(
+            cur, dst, dx_scaled, rho, dt, weight, tiles_x, k);
+        PF prev = cur.x;
+        cur.x = dst;
+        dst = prev;
+        done += (uint32_t)k;
+        ++launches;
+    }
+    if (launches & 1) {  // result is in alt: copy back
+        if (cudaMemcpy2DAsync(L.x.p, (size_t)L.x.P * 4, alt.p, (size_t)alt.P * 4, (size_t)L.nx * 4, L.ny,
+                              cudaMemcpyDeviceToDevice, stream) != cudaSuccess)
+            return EFL_ERR_CUDA;
+    }
+    return EFL_OK;
+}
+
 struct PersistentPlan {
     int tx = 0, ty = 0, kmax = 0, tiles_x = 0, tiles_y = 0;
     size_t smem = 0;
+    const void* kernel = nullptr;
     bool ok = false;
 };
 
-// Deepest temporal blocking and a tile shape whose CTAs are all co-resident
-// (one per SM) and whose extended tile fits in shared memory.
+// The tile shapes the persistent solver is instantiated for: (KMAX, tx, ty).
+// Deeper temporal blocking first; all CTAs must be co-resident (one per SM).
+template <int EX, int EY, int KMAX>
+inline bool try_plan(const SolverWorkspace& ws, int nx, int ny, PersistentPlan* p) {
+    const int tx = EX - 4 * KMAX, ty = EY - 4 * KMAX;
+    p->kmax = KMAX;
+    p->tx = tx;
+    p->ty = ty;
+    p->tiles_x = (nx + tx - 1) / tx;
+    p->tiles_y = (ny + ty - 1) / ty;
+    p->smem = sizeof(PsTile<EX, EY>);
+    p->kernel = (const void*)k_gs64_persistent<EX, EY, KMAX>;
+    if (p->smem + 1024 > ws.max_smem) return false;
+    if (p->tiles_x * p->tiles_y > ws.num_sms || p->tiles_x * p->tiles_y > ws.max_blocks) return false;
+    return true;
+}
 inline PersistentPlan plan_persistent(const SolverWorkspace& ws, int nx, int ny) {
-    static const int cand[][3] = {{4, 64, 32}, {4, 32, 32}, {2, 64, 32}, {2, 64, 64}, {4, 32, 16}, {2, 32, 32},
-                                  {1, 64, 64}, {1, 128, 64}};
-    for (const auto& c : cand) {
-        PersistentPlan p;
-        p.kmax = c[0];
-        p.tx = c[1];
-        p.ty = c[2];
-        p.tiles_x = (nx + p.tx - 1) / p.tx;
-        p.tiles_y = (ny + p.ty - 1) / p.ty;
-        const int H = 2 * p.kmax;
-        p.smem = ps_smem_bytes(p.tx + 2 * H, p.ty + 2 * H) + 64;
-        if (p.smem + 1024 > ws.max_smem) continue;  // room for the kernel's static shared memory
-        if (p.tiles_x * p.tiles_y > ws.num_sms || p.tiles_x * p.tiles_y > ws.max_blocks) continue;
+    PersistentPlan p;
+    if (try_plan<80, 48, 4>(ws, nx, ny, &p) ||   // 64 x 32 owned
+        try_plan<48, 48, 4>(ws, nx, ny, &p) ||   // 32 x 32
+        try_plan<72, 56, 2>(ws, nx, ny, &p) ||   // 64 x 48
+        try_plan<40, 40, 4>(ws, nx, ny, &p)) {   // 24 x 24
         p.ok = true;
         return p;
     }
@@ -425,16 +567,17 @@ inline efl_status solve_gs64_persistent(SolverWorkspace& ws, const Level64& L, c
                                         cudaStream_t stream, SolveResult* out, std::string* err) {
     PersistentPlan plan = plan_persistent(ws, L.nx, L.ny);
     if (!plan.ok) return EFL_ERR_STATE;
-    if (cudaFuncSetAttribute(k_gs64_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plan.smem) !=
+    if (cudaFuncSetAttribute(plan.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plan.smem) !=
         cudaSuccess) {
         cudaGetLastError();
         return EFL_ERR_STATE;
     }
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gs64_persistent, PS_THREADS, plan.smem) !=
-            cudaSuccess ||
-        per_sm < 1 || plan.tiles_x * plan.tiles_y > per_sm * ws.num_sms)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, plan.kernel, PS_THREADS, plan.smem) != cudaSuccess ||
+        per_sm < 1 || plan.tiles_x * plan.tiles_y > per_sm * ws.num_sms) {
+        cudaGetLastError();
         return EFL_ERR_STATE;
+    }
     PersistentParams P;
     P.L = L;
     P.tx = plan.tx;
@@ -458,8 +601,8 @@ inline efl_status solve_gs64_persistent(SolverWorkspace& ws, const Level64& L, c
     }
     void* args[] = {&P};
     count_launch();
-    cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_gs64_persistent, dim3(plan.tiles_x * plan.tiles_y),
-                                                dim3(PS_THREADS), args, plan.smem, stream);
+    cudaError_t e = cudaLaunchCooperativeKernel(plan.kernel, dim3(plan.tiles_x * plan.tiles_y), dim3(PS_THREADS),
+                                                args, plan.smem, stream);
     if (e != cudaSuccess) {
         *err = std::string("cooperative launch of the persistent solver failed: ") + cudaGetErrorString(e);
         return EFL_ERR_CUDA;
