@@ -20,6 +20,7 @@
 #include "../../include/efl.h"
 #include "efl_kernels.cuh"
 #include "efl_solver.cuh"
+#include "efl_sweep_tma.cuh"
 
 using namespace efl;
 
@@ -79,6 +80,8 @@ struct efl_sim {
     double* h_norms = nullptr;  // pinned
     unsigned long long* d_count = nullptr;
     SolverWorkspace solver;
+    SweepTma tma;
+    int* h_err = nullptr;  // pinned copy of the TMA sweep's error flag
 
     Dom dom() const { return Dom{nx, ny}; }
 };
@@ -366,6 +369,37 @@ efl_status v_cycle(efl_sim* s, std::vector<LevelT<T>>& mg, size_t i) {
     return gs_iterations(s, L, 1.0f, scale, P.mg_post);
 }
 
+// n reference (f32) red-black iterations on the pressure field: the TMA
+// streaming kernel, or the shared-memory tiled kernel where TMA is
+// unavailable.
+efl_status sweeps_f32(efl_sim* s, float weight, uint32_t n) {
+    std::string e;
+    efl_status st = solve_gs32_tma(s->tma, s->mg[0], s->p1, s->solver.num_sms, s->U.dx, s->U.rho, s->U.dt, weight, n,
+                                   s->stream, &e);
+    if (st == EFL_ERR_STATE) {
+        if (solve_gs32_tiled(s->mg[0], s->p1, s->U.dx, s->U.rho, s->U.dt, weight, n, s->stream) != EFL_OK)
+            return set_err(s, EFL_ERR_CUDA, "tiled Gauss-Seidel launch failed: %s",
+                           cudaGetErrorString(cudaGetLastError()));
+    } else if (st != EFL_OK) {
+        return set_err(s, st, "%s", e.c_str());
+    }
+    LAUNCH_CHECK();
+    return EFL_OK;
+}
+
+// Errors that kernels report through device flags (a bounded wait that gave
+// up); called after the stream has been synchronised.
+efl_status check_device_errors(efl_sim* s) {
+    if (!s->tma.d_err) return EFL_OK;
+    CU(cudaMemcpy(s->h_err, s->tma.d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (*s->h_err) {
+        *s->h_err = 0;
+        cudaMemset(s->tma.d_err, 0, sizeof(int));
+        return set_err(s, EFL_ERR_CUDA, "TMA sweep: an mbarrier wait timed out");
+    }
+    return EFL_OK;
+}
+
 // projection.rs:89-164.  tolerance > 0 (an extension) solves to
 // ||b - A p|| / ||b|| <= tolerance with an FP64 iterate: an f32 pressure
 // cannot represent a solution that accurate when hydrostatic pressure
@@ -386,11 +420,7 @@ efl_status st_projection(efl_sim* s, efl_step_stats* st) {
         iters = 50;
     } else if (P.tolerance <= 0.0f) {
         if (P.method == EFL_PROJECTION_GAUSS_SEIDEL) {
-            if (solve_gs32_tiled(s->mg[0], s->p1, s->U.dx, s->U.rho, s->U.dt, P.sor_weight, P.gs_iterations,
-                                 s->stream) != EFL_OK)
-                return set_err(s, EFL_ERR_CUDA, "tiled Gauss-Seidel launch failed: %s",
-                               cudaGetErrorString(cudaGetLastError()));
-            LAUNCH_CHECK();
+            TRY(sweeps_f32(s, P.sor_weight, P.gs_iterations));
             iters = P.gs_iterations;
         } else {
             TRY(v_cycle(s, s->mg, 0));
@@ -684,6 +714,11 @@ efl_status efl_create(const efl_config* cfg, efl_sim** out) {
         return fail(set_err(s, EFL_ERR_OUT_OF_MEMORY, "cudaMallocHost failed"));
     CTRY(alloc_mg(s));
     CTRY(solver_init(s->solver, nx, ny, s->device, &s->err));
+    if (cudaMallocHost(&s->h_err, sizeof(int)) != cudaSuccess)
+        return fail(set_err(s, EFL_ERR_OUT_OF_MEMORY, "cudaMallocHost failed"));
+    *s->h_err = 0;
+    sweep_tma_init(s->tma, s->mg[0], s->p1);  // falls back to the tiled kernel if unavailable
+    cudaGetLastError();
     if (cudaStreamSynchronize(s->stream) != cudaSuccess)
         return fail(set_err(s, EFL_ERR_CUDA, "initial clear failed: %s", cudaGetErrorString(cudaGetLastError())));
 #undef CTRY
@@ -696,6 +731,8 @@ efl_status efl_destroy(efl_sim* s) {
     cudaSetDevice(s->device);
     if (s->stream) cudaStreamSynchronize(s->stream);
     solver_free(s->solver);
+    sweep_tma_free(s->tma);
+    if (s->h_err) cudaFreeHost(s->h_err);
     for (auto& b : s->bufs) cudaFree(b.p);
     if (s->d_forces) cudaFree(s->d_forces);
     if (s->h_norms) cudaFreeHost(s->h_norms);
@@ -809,7 +846,7 @@ efl_status efl_read_solid_forces(efl_sim* s, efl_solid_force out[EFL_MAX_SOLIDS]
     CU(cudaMemcpyAsync(out, s->d_forces_out, EFL_MAX_SOLIDS * sizeof(efl_solid_force), cudaMemcpyDeviceToHost,
                        s->stream));
     CU(cudaStreamSynchronize(s->stream));
-    return EFL_OK;
+    return check_device_errors(s);
 }
 efl_status efl_read_force_bins(efl_sim* s, int32_t out[3 * EFL_MAX_SOLIDS]) {
     if (!s || !out) return set_err(s, EFL_ERR_INVALID_ARGUMENT, "null argument");
@@ -918,7 +955,7 @@ efl_status efl_synchronize(efl_sim* s) {
     if (!s) return set_err(nullptr, EFL_ERR_INVALID_ARGUMENT, "null sim");
     cudaSetDevice(s->device);
     CU(cudaStreamSynchronize(s->stream));
-    return EFL_OK;
+    return check_device_errors(s);
 }
 
 efl_status efl_residual(efl_sim* s, double* rel, double* nr, double* nb) {
@@ -954,8 +991,7 @@ efl_status efl_pressure_sweeps(efl_sim* s, int32_t precision, uint32_t iteration
     cudaSetDevice(s->device);
     const float w = s->cfg.projection.sor_weight;
     if (precision == 32) {
-        if (solve_gs32_tiled(s->mg[0], s->p1, s->U.dx, s->U.rho, s->U.dt, w, iterations, s->stream) != EFL_OK)
-            return set_err(s, EFL_ERR_CUDA, "tiled Gauss-Seidel launch failed");
+        TRY(sweeps_f32(s, w, iterations));
     } else {
         // The tolerance-driven solver with an unreachable tolerance: exactly
         // `iterations` iterations, residual evaluated before and after only.
