@@ -34,7 +34,7 @@ constexpr int TS_TX = 64, TS_TY = 32;
 constexpr int TS_EX = TS_TX + 2 * TS_H;  // 72
 constexpr int TS_EY = TS_TY + 2 * TS_H;  // 40
 constexpr int TS_W2 = TS_EX / 2;
-constexpr int TS_THREADS = 512;
+constexpr int TS_THREADS = 1024;
 // TMA boxes (columns x rows); x origins are multiples of 4 floats.
 constexpr int BOX_PHI_W = TS_EX + 8, BOX_PHI_H = TS_EY + 2;  // from (gx0 - 4, gy0 - 1)
 constexpr int BOX_FU_W = TS_EX + 4, BOX_FU_H = TS_EY;        // from (gx0, gy0)
@@ -92,7 +92,6 @@ __global__ void __launch_bounds__(TS_THREADS, 1)
     k_gs32_tma(const __grid_constant__ SweepMaps maps, int nx, int ny, PF out, int pin, float dx_scaled, float rho,
                float dt, float weight, int tiles_x, int ntiles, int iters, int* err) {
     extern __shared__ __align__(128) unsigned char sm[];
-    unsigned char* stage[2] = {sm, sm + ST_BYTES};
     GsTile32<TS_EX, TS_EY>& T = *reinterpret_cast<GsTile32<TS_EX, TS_EY>*>(sm + TS_TILE_OFF);
     uint64_t* bars = reinterpret_cast<uint64_t*>(sm + TS_BAR_OFF);
     if (threadIdx.x == 0) {
@@ -103,12 +102,13 @@ __global__ void __launch_bounds__(TS_THREADS, 1)
     __syncthreads();
     auto issue = [&](int t, int b) {
         const int gx0 = (t % tiles_x) * TS_TX - TS_H, gy0 = (t / tiles_x) * TS_TY - TS_H;
+        unsigned char* st = sm + b * ST_BYTES;
         mbar_expect_tx(&bars[b], TS_TX_BYTES);
-        tma_load_2d(stage[b] + ST_PHI, &maps.phi, gx0 - 4, gy0 - 1, &bars[b]);
-        tma_load_2d(stage[b] + ST_FU, &maps.fu, gx0, gy0, &bars[b]);
-        tma_load_2d(stage[b] + ST_FV, &maps.fv, gx0, gy0, &bars[b]);
-        tma_load_2d(stage[b] + ST_DIV, &maps.div, gx0, gy0, &bars[b]);
-        tma_load_2d(stage[b] + ST_P, &maps.p[pin], gx0, gy0, &bars[b]);
+        tma_load_2d(st + ST_PHI, &maps.phi, gx0 - 4, gy0 - 1, &bars[b]);
+        tma_load_2d(st + ST_FU, &maps.fu, gx0, gy0, &bars[b]);
+        tma_load_2d(st + ST_FV, &maps.fv, gx0, gy0, &bars[b]);
+        tma_load_2d(st + ST_DIV, &maps.div, gx0, gy0, &bars[b]);
+        tma_load_2d(st + ST_P, pin ? &maps.p[1] : &maps.p[0], gx0, gy0, &bars[b]);
     };
     const float cdiv = dx_scaled * dx_scaled * rho / dt;  // gauss_seidel.wgsl:58
     const float omw = 1.0f - weight;
@@ -121,18 +121,19 @@ __global__ void __launch_bounds__(TS_THREADS, 1)
             fence_proxy_async();  // generic reads of stage[b^1] (previous tile) before the async writes
             issue(t + gridDim.x, b ^ 1);
         }
-        const bool got = mbar_wait(&bars[b], (n >> 1) & 1);
+        const bool got = mbar_wait(&bars[b], (n >> 1) & 1);  // (the wait is uniform per CTA)
         if (__syncthreads_or(!got)) {
             if (threadIdx.x == 0) atomicExch(err, 1);
             mbar_wait(&bars[b], (n >> 1) & 1);  // copies of this CTA still in flight
             if (next) mbar_wait(&bars[b ^ 1], ((n + 1) >> 1) & 1);
             return;
         }
-        const float* phi_s = reinterpret_cast<const float*>(stage[b] + ST_PHI);
-        const float* fu_s = reinterpret_cast<const float*>(stage[b] + ST_FU);
-        const float* fv_s = reinterpret_cast<const float*>(stage[b] + ST_FV);
-        const float* div_s = reinterpret_cast<const float*>(stage[b] + ST_DIV);
-        const float* p_s = reinterpret_cast<const float*>(stage[b] + ST_P);
+        const unsigned char* stb = sm + b * ST_BYTES;
+        const float* phi_s = reinterpret_cast<const float*>(stb + ST_PHI);
+        const float* fu_s = reinterpret_cast<const float*>(stb + ST_FU);
+        const float* fv_s = reinterpret_cast<const float*>(stb + ST_FV);
+        const float* div_s = reinterpret_cast<const float*>(stb + ST_DIV);
+        const float* p_s = reinterpret_cast<const float*>(stb + ST_P);
         const int gx0 = (t % tiles_x) * TS_TX - TS_H, gy0 = (t / tiles_x) * TS_TY - TS_H;
         const int base = (gx0 + gy0) & 1;
         // Coefficients of every cell of the extended tile (gauss_seidel.wgsl:44-80).
