@@ -51,37 +51,38 @@ struct SolverWorkspace {
 };
 
 constexpr int PS_THREADS = 512;
-constexpr long long kBarrierSpinLimit = 1ll << 22;  // x ~100 ns sleeps: well under a second
+constexpr long long kBarrierSpinLimit = 1ll << 25;  // acquire polls (~ 1 s)
 
 // Grid-wide barrier for a cooperative launch (all CTAs co-resident), with a
-// bounded spin: a CTA that waits more than kBarrierSpinLimit polls sets
-// barrier->error and every CTA leaves the solve.
+// bounded spin: a CTA that polls more than kBarrierSpinLimit times sets
+// barrier->error and every CTA leaves the solve.  Arrival is an acq_rel
+// atomic, the release of the generation a release reduction, polling an
+// acquire load (about 2 us for 128 CTAs on B200).
 EFL_DEV bool grid_barrier(GridBarrier* gb, unsigned nblocks) {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
         int ok = 1;
-        volatile unsigned* vgen = &gb->gen;
-        const unsigned gen = *vgen;
-        __threadfence();
-        const unsigned arrived = atomicAdd(&gb->count, 1u);
+        unsigned gen, arrived, cur;
+        asm volatile("ld.acquire.gpu.u32 %0, [%1];" : "=r"(gen) : "l"(&gb->gen) : "memory");
+        asm volatile("atom.acq_rel.gpu.add.u32 %0, [%1], 1;" : "=r"(arrived) : "l"(&gb->count) : "memory");
         if (arrived == nblocks - 1) {
-            atomicExch(&gb->count, 0u);
-            __threadfence();
-            atomicAdd(&gb->gen, 1u);
+            asm volatile("st.relaxed.gpu.u32 [%0], 0;" ::"l"(&gb->count) : "memory");
+            asm volatile("red.release.gpu.add.u32 [%0], 1;" ::"l"(&gb->gen) : "memory");
         } else {
             long long spins = 0;
-            while (*vgen == gen) {
+            do {
+                asm volatile("ld.acquire.gpu.u32 %0, [%1];" : "=r"(cur) : "l"(&gb->gen) : "memory");
                 if (++spins > kBarrierSpinLimit) {
                     atomicExch(&gb->error, 1);
                     ok = 0;
                     break;
                 }
-                __nanosleep(100);
-            }
+            } while (cur == gen);
         }
-        __threadfence();
-        if (*(volatile int*)&gb->error) ok = 0;
+        int e;
+        asm volatile("ld.acquire.gpu.s32 %0, [%1];" : "=r"(e) : "l"(&gb->error) : "memory");
+        if (e) ok = 0;
         s_ok = ok;
     }
     __syncthreads();
@@ -125,18 +126,22 @@ constexpr unsigned char MODE_UPDATE = 2;   // regular update
 constexpr unsigned char MODE_COUNTED = 4;  // counted in the residual norms
 
 template <int EX, int EY>
-EFL_DEV void ps_half_sweep(PsTile<EX, EY>& T, int base, int c, double cdiv, double w, double omw) {
+EFL_DEV void ps_half_sweep(PsTile<EX, EY>& T, int base, int c, int h, double cdiv, double w, double omw) {
+    // Half-sweep h of a round: after it only rings > h of the tile hold
+    // correct values, so cells of rings <= h are left alone.
     constexpr int W2 = EX / 2;
-    constexpr int TOTAL = (EY - 2) * W2;
     const int o = 1 - c;
-#pragma unroll 2
-    for (int i = threadIdx.x; i < TOTAL; i += PS_THREADS) {
-        const int ly = 1 + i / W2;
-        const int j = i - (ly - 1) * W2;
+    const int rows = EY - 2 - 2 * h;
+    const int total = rows * W2;
+    for (int i = threadIdx.x; i < total; i += PS_THREADS) {
+        const int ly = 1 + h + i / W2;
+        const int j = i - (ly - 1 - h) * W2;
+        const int odd = (base + ly + c) & 1;  // lx & 1 of a colour-c cell in row ly
+        const int lx = 2 * j + odd;
+        if (lx < 1 + h || lx > EX - 2 - h) continue;
         const int k = ly * W2 + j;
         const unsigned char m = T.mode[c][k];
         if (m & MODE_UPDATE) {
-            const int odd = (base + ly + c) & 1;  // lx & 1 of a colour-c cell in row ly
             const float4 wk = T.w[c][k];
             double nume = cdiv * T.b[c][k];
             nume = nume + (double)wk.x * T.p[o][k - 1 + odd];
@@ -192,9 +197,11 @@ EFL_DEV double2 ps_residual_partial(const PsTile<EX, EY>& T, int base, int H, in
 }
 
 template <int EX, int EY>
-EFL_DEV void ps_load_p(PsTile<EX, EY>& T, const Level64& L, int gx0, int gy0, int base) {
+EFL_DEV void ps_load_p(PsTile<EX, EY>& T, const Level64& L, int gx0, int gy0, int base, int H, int tx, int ty,
+                       bool halo_only) {
     for (int i = threadIdx.x; i < EX * EY; i += PS_THREADS) {
         const int ly = i / EX, lx = i - ly * EX;
+        if (halo_only && lx >= H && lx < H + tx && ly >= H && ly < H + ty) continue;  // owned: already current
         const int gx = gx0 + lx, gy = gy0 + ly;
         const int c = (base + lx + ly) & 1;
         const bool in = (unsigned)gx < (unsigned)L.nx && (unsigned)gy < (unsigned)L.ny;
@@ -291,7 +298,7 @@ __global__ void __launch_bounds__(PS_THREADS, 1) k_gs64_persistent(PersistentPar
         T.w[c][k] = wk;
     }
     __syncthreads();
-    ps_load_p(T, L, gx0, gy0, base);
+    ps_load_p(T, L, gx0, gy0, base, H, tx, ty, false);
     __syncthreads();
 
     const double w = P.weight, omw = 1.0 - P.weight;
@@ -306,15 +313,15 @@ __global__ void __launch_bounds__(PS_THREADS, 1) k_gs64_persistent(PersistentPar
         while (ok && todo > 0) {
             const unsigned kk = min((unsigned)KMAX, todo);
             for (unsigned it = 0; it < kk; ++it) {
-                ps_half_sweep(T, base, 1, P.cdiv, w, omw);  // red: (x+y) odd
+                ps_half_sweep(T, base, 1, 2 * it, P.cdiv, w, omw);  // red: (x+y) odd
                 __syncthreads();
-                ps_half_sweep(T, base, 0, P.cdiv, w, omw);  // black
+                ps_half_sweep(T, base, 0, 2 * it + 1, P.cdiv, w, omw);  // black
                 __syncthreads();
             }
             ps_store_owned(T, L, gx0, gy0, base, H, tx, ty);
             ok = grid_barrier(P.barrier, nblocks);
             if (!ok) break;
-            ps_load_p(T, L, gx0, gy0, base);
+            ps_load_p(T, L, gx0, gy0, base, H, tx, ty, true);
             __syncthreads();
             todo -= kk;
             iters += kk;
