@@ -81,6 +81,8 @@ struct efl_sim {
     unsigned long long* d_count = nullptr;
     SolverWorkspace solver;
     SweepTma tma;
+    MixPlanes mixp{};  // global-memory planes of the mixed solve, allocated on first use
+    bool mixp_ready = false;
     int* h_err = nullptr;  // pinned copy of the TMA sweep's error flag
 
     Dom dom() const { return Dom{nx, ny}; }
@@ -387,6 +389,32 @@ efl_status sweeps_f32(efl_sim* s, float weight, uint32_t n) {
     return EFL_OK;
 }
 
+// The tolerance-driven red-black solve (mixed-precision refinement) on the
+// FP64 iterate of level 0: one cooperative launch when the grid fits the
+// persistent scheme, else global-memory kernels.
+efl_status gs_mixed(efl_sim* s, float weight, double tol, uint32_t max_iters, uint32_t check, SolveResult* res) {
+    const Level64& L = s->mg64[0];
+    std::string perr;
+    efl_status ps = solve_gsmix_persistent(s->solver, L, s->r0, s->U, weight, tol, max_iters, check, s->stream, res,
+                                           &perr);
+    if (ps == EFL_OK) return EFL_OK;
+    if (ps != EFL_ERR_STATE) return set_err(s, ps, "%s", perr.c_str());
+    if (!s->mixp_ready) {
+        const int nx = s->nx, ny = s->ny, P = s->P, R = ny + 1;
+        TRY(alloc_plane(s, s->mixp.w, nx, ny, P, R));
+        TRY(alloc_plane(s, s->mixp.inv, nx, ny, P, R));
+        TRY(alloc_plane(s, s->mixp.rc, nx, ny, P, R));
+        TRY(alloc_plane(s, s->mixp.d, nx, ny, P, R));
+        TRY(alloc_plane(s, s->mixp.den, nx, ny, P, R));
+        TRY(alloc_plane(s, s->mixp.mode, nx, ny, P, R));
+        s->mixp_ready = true;
+    }
+    ps = solve_gsmix_global(s->solver, L, s->mixp, s->U, weight, tol, max_iters, check, s->stream, res, &perr);
+    if (ps != EFL_OK) return set_err(s, ps == EFL_ERR_STATE ? EFL_ERR_CUDA : ps, "%s", perr.c_str());
+    LAUNCH_CHECK();
+    return EFL_OK;
+}
+
 // Errors that kernels report through device flags (a bounded wait that gave
 // up); called after the stream has been synchronised.
 efl_status check_device_errors(efl_sim* s) {
@@ -434,19 +462,12 @@ efl_status st_projection(efl_sim* s, efl_step_stats* st) {
         double r = -1.0;
         bool done = false;
         if (P.method == EFL_PROJECTION_GAUSS_SEIDEL) {
-            // One cooperative launch for the whole solve when the grid fits.
             SolveResult res{};
-            std::string perr;
-            efl_status ps = solve_gs64_persistent(s->solver, L, s->U, P.sor_weight, (double)P.tolerance,
-                                                  P.max_iterations, P.check_interval, s->stream, &res, &perr);
-            if (ps == EFL_OK) {
-                iters = res.iterations;
-                r0 = res.r0;
-                r = res.r1;
-                done = true;
-            } else if (ps != EFL_ERR_STATE) {
-                return set_err(s, ps, "%s", perr.c_str());
-            }
+            TRY(gs_mixed(s, P.sor_weight, (double)P.tolerance, P.max_iterations, P.check_interval, &res));
+            iters = res.iterations;
+            r0 = res.r0;
+            r = res.r1;
+            done = true;
         }
         if (!done) {
             TRY(relative_residual(s, L, &r));
@@ -996,11 +1017,7 @@ efl_status efl_pressure_sweeps(efl_sim* s, int32_t precision, uint32_t iteration
         // The tolerance-driven solver with an unreachable tolerance: exactly
         // `iterations` iterations, residual evaluated before and after only.
         SolveResult res{};
-        std::string perr;
-        efl_status ps = solve_gs64_persistent(s->solver, s->mg64[0], s->U, w, 0.0, iterations,
-                                              std::max<uint32_t>(1, iterations), s->stream, &res, &perr);
-        if (ps == EFL_ERR_STATE) TRY(solve_gs_fixed(s->solver, s->mg64[0], s->U, w, iterations, s->stream));
-        else if (ps != EFL_OK) return set_err(s, ps, "%s", perr.c_str());
+        TRY(gs_mixed(s, w, 0.0, iterations, std::max<uint32_t>(1, iterations), &res));
     }
     LAUNCH_CHECK();
     return EFL_OK;

@@ -18,7 +18,9 @@
 #pragma once
 
 #include <algorithm>
+#include <cmath>
 #include <string>
+#include <vector>
 
 #include "efl_kernels.cuh"
 
@@ -386,6 +388,354 @@ inline efl_status solve_gs_fixed(SolverWorkspace&, const LevelT<T>& L, const Uni
 }
 
 // ---------------------------------------------------------------------------
+// Tolerance-driven solve in mixed-precision iterative-refinement form.
+// Every check block of n iterations: the FP64 residual r of the FP64 iterate
+// p (operator of residual.wgsl in factored form) gives the convergence test
+// and the f32 right-hand side rc = f32(cdiv * r); n SOR red-black
+// iterations then run in f32 on the correction d (starting at 0) with f32
+// coefficients w_k (face fraction of fluid in-bounds neighbours, else 0) and
+// inv = f32(1/denom); then p += d in FP64, and the cells the reference sets
+// to zero (air, fully solid, |denom| < 1e-6) get p = 0.  SOR is affine, so
+// in exact arithmetic these are the RBGS iterates themselves: the
+// iteration counts are those of red-black Gauss-Seidel, while the sweeps move
+// f32 data.
+template <int EX, int EY>
+struct MixTile {
+    static constexpr int W2 = EX / 2;
+    static constexpr int N2 = W2 * EY;
+    double p[2][N2];  // FP64 iterate
+    double b[2][N2];
+    double den[2][N2];
+    float4 w[2][N2];
+    float d[2][N2];   // f32 correction
+    float rc[2][N2];  // f32 right-hand side of the correction
+    float inv[2][N2];
+    unsigned char mode[2][N2];
+};
+
+template <int EX, int EY>
+EFL_DEV void mix_half_sweep(MixTile<EX, EY>& T, int base, int c, int h, float w, float omw) {
+    constexpr int W2 = EX / 2;
+    const int o = 1 - c;
+    const int total = (EY - 2 - 2 * h) * W2;
+    for (int i = threadIdx.x; i < total; i += PS_THREADS) {
+        const int ly = 1 + h + i / W2;
+        const int j = i - (ly - 1 - h) * W2;
+        const int odd = (base + ly + c) & 1;
+        const int lx = 2 * j + odd;
+        if (lx < 1 + h || lx > EX - 2 - h) continue;
+        const int k = ly * W2 + j;
+        if (T.mode[c][k] & MODE_UPDATE) {
+            const float4 wk = T.w[c][k];
+            float nume = T.rc[c][k];
+            nume = nume + wk.x * T.d[o][k - 1 + odd];
+            nume = nume + wk.y * T.d[o][k + odd];
+            nume = nume + wk.z * T.d[o][k - W2];
+            nume = nume + wk.w * T.d[o][k + W2];
+            T.d[c][k] = w * (nume * T.inv[c][k]) + omw * T.d[c][k];
+        }
+    }
+}
+
+// FP64 residual at every cell of rings >= 1 (rc = f32(cdiv * r) for cells
+// that update, d = 0) and the norms over the owned cells.
+template <int EX, int EY>
+EFL_DEV double2 mix_check(MixTile<EX, EY>& T, int base, int H, int tx, int ty, double cdiv, double factor) {
+    constexpr int W2 = EX / 2;
+    double ar = 0.0, ab = 0.0;
+    for (int i = threadIdx.x; i < EX * EY; i += PS_THREADS) {
+        const int ly = i / EX, lx = i - ly * EX;
+        const int c = (base + lx + ly) & 1, o = 1 - c, odd = lx & 1;
+        const int k = ly * W2 + (lx >> 1);
+        const unsigned char m = T.mode[c][k];
+        float rcv = 0.0f;
+        const bool ring0 = lx == 0 || ly == 0 || lx == EX - 1 || ly == EY - 1;
+        if ((m & MODE_COUNTED) && !ring0) {
+            const float4 wk = T.w[c][k];
+            double sum = (double)wk.x * T.p[o][k - 1 + odd];
+            sum = sum + (double)wk.y * T.p[o][k + odd];
+            sum = sum + (double)wk.z * T.p[o][k - W2];
+            sum = sum + (double)wk.w * T.p[o][k + W2];
+            const double bb = T.b[c][k];
+            const double r = bb - factor * (T.den[c][k] * T.p[c][k] - sum);
+            if (m & MODE_UPDATE) rcv = (float)(cdiv * r);
+            if (lx >= H && lx < H + tx && ly >= H && ly < H + ty) {
+                ar += r * r;
+                ab += bb * bb;
+            }
+        }
+        T.rc[c][k] = rcv;
+        T.d[c][k] = 0.0f;
+    }
+    ar = warp_sum(ar);
+    ab = warp_sum(ab);
+    __shared__ double red_r[PS_THREADS / 32], red_b[PS_THREADS / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) {
+        red_r[wid] = ar;
+        red_b[wid] = ab;
+    }
+    __syncthreads();
+    double2 out = make_double2(0.0, 0.0);
+    if (threadIdx.x == 0) {
+        for (int q = 0; q < PS_THREADS / 32; ++q) {
+            out.x += red_r[q];
+            out.y += red_b[q];
+        }
+    }
+    __syncthreads();
+    return out;
+}
+
+template <int EX, int EY, int KMAX>
+__global__ void __launch_bounds__(PS_THREADS, 1) k_gsmix_persistent(PersistentParams P, PF dbuf) {
+    extern __shared__ __align__(16) unsigned char ps_raw[];
+    MixTile<EX, EY>& T = *reinterpret_cast<MixTile<EX, EY>*>(ps_raw);
+    constexpr int H = 2 * KMAX;
+    constexpr int W2 = EX / 2;
+    const int tx = EX - 2 * H, ty = EY - 2 * H;
+    const Level64& L = P.L;
+    const int tile = blockIdx.x;
+    const int gx0 = (tile % P.tiles_x) * tx - H, gy0 = (tile / P.tiles_x) * ty - H;
+    const int base = (gx0 + gy0) & 1;
+    const unsigned nblocks = gridDim.x;
+    auto owned = [&](int lx, int ly) { return lx >= H && lx < H + tx && ly >= H && ly < H + ty; };
+
+    for (int i = threadIdx.x; i < EX * EY; i += PS_THREADS) {
+        const int ly = i / EX, lx = i - ly * EX;
+        const int gx = gx0 + lx, gy = gy0 + ly;
+        const int c = (base + lx + ly) & 1, k = ly * W2 + (lx >> 1);
+        unsigned char m = MODE_SKIP;
+        double den = 0.0, bb = 0.0, pv = 0.0;
+        float inv = 0.0f;
+        float4 wk = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if ((unsigned)gx < (unsigned)L.nx && (unsigned)gy < (unsigned)L.ny) {
+            const bool ring = lx == 0 || ly == 0 || lx == EX - 1 || ly == EY - 1;
+            const float phi = L.ls.at(gx, gy);
+            bb = L.b.at(gx, gy);
+            pv = __ldcg(&L.x.p[(size_t)gy * L.x.P + gx]);
+            bool update = false, counted = false;
+            if (phi < 0.0f) {
+                const float f[4] = {L.fu.at(gx, gy), L.fu.at(gx + 1, gy), L.fv.at(gx, gy), L.fv.at(gx, gy + 1)};
+                if (!(f[0] == 0.0f && f[1] == 0.0f && f[2] == 0.0f && f[3] == 0.0f)) {
+                    counted = true;
+                    const int ox[4] = {-1, 1, 0, 0}, oy[4] = {0, 0, -1, 1};
+                    float wv[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const int jx = gx + ox[q], jy = gy + oy[q];
+                        if ((unsigned)jx < (unsigned)L.nx && (unsigned)jy < (unsigned)L.ny) {
+                            const float level = L.ls.at(jx, jy);
+                            if (level < 0.0f) {
+                                den += (double)f[q];
+                                wv[q] = f[q];
+                            } else {
+                                den += (double)f[q] * (1.0 - (double)level / (double)phi);
+                            }
+                        }
+                    }
+                    wk = make_float4(wv[0], wv[1], wv[2], wv[3]);
+                    if (!(fabs(den) < (double)1.0e-6f)) {
+                        update = true;
+                        inv = (float)(1.0 / den);
+                    }
+                }
+            }
+            if (counted) m |= MODE_COUNTED;
+            if (!ring) m |= update ? MODE_UPDATE : MODE_ZERO;  // the outer ring never updates here
+        }
+        T.mode[c][k] = m;
+        T.den[c][k] = den;
+        T.inv[c][k] = inv;
+        T.b[c][k] = bb;
+        T.w[c][k] = wk;
+        T.p[c][k] = pv;
+    }
+    __syncthreads();
+    const double cdiv = P.cdiv, factor = P.factor;
+    const float w = (float)P.weight, omw = 1.0f - (float)P.weight;
+    unsigned iters = 0;
+    double2 part = mix_check(T, base, H, tx, ty, cdiv, factor);
+    if (threadIdx.x == 0) P.partials[blockIdx.x] = part;
+    bool ok = grid_barrier(P.barrier, nblocks);
+    double r = ok ? ps_total_relative(P.partials, nblocks) : 0.0;
+    const double r0 = r;
+    while (ok && !(r <= P.tol) && iters < P.max_iters) {
+        unsigned todo = min(P.check_interval, P.max_iters - iters);
+        while (ok && todo > 0) {
+            const unsigned kk = min((unsigned)KMAX, todo);
+            for (unsigned it = 0; it < kk; ++it) {
+                mix_half_sweep(T, base, 1, 2 * it, w, omw);  // red: (x+y) odd
+                __syncthreads();
+                mix_half_sweep(T, base, 0, 2 * it + 1, w, omw);  // black
+                __syncthreads();
+            }
+            todo -= kk;
+            iters += kk;
+            if (todo > 0) {  // exchange the correction's halo
+                for (int i = threadIdx.x; i < tx * ty; i += PS_THREADS) {
+                    const int ly = H + i / tx, lx = H + i % tx, gx = gx0 + lx, gy = gy0 + ly;
+                    if ((unsigned)gx < (unsigned)L.nx && (unsigned)gy < (unsigned)L.ny)
+                        __stcg(&dbuf.p[(size_t)gy * dbuf.P + gx], T.d[(base + lx + ly) & 1][ly * W2 + (lx >> 1)]);
+                }
+                ok = grid_barrier(P.barrier, nblocks);
+                if (!ok) break;
+                for (int i = threadIdx.x; i < EX * EY; i += PS_THREADS) {
+                    const int ly = i / EX, lx = i - ly * EX;
+                    if (owned(lx, ly)) continue;
+                    const int gx = gx0 + lx, gy = gy0 + ly;
+                    const bool in = (unsigned)gx < (unsigned)L.nx && (unsigned)gy < (unsigned)L.ny;
+                    T.d[(base + lx + ly) & 1][ly * W2 + (lx >> 1)] =
+                        in ? __ldcg(&dbuf.p[(size_t)gy * dbuf.P + gx]) : 0.0f;
+                }
+                __syncthreads();
+            }
+        }
+        if (!ok) break;
+        // p += d on the owned cells (0 where the reference zeroes p), then exchange p.
+        for (int i = threadIdx.x; i < tx * ty; i += PS_THREADS) {
+            const int ly = H + i / tx, lx = H + i % tx, gx = gx0 + lx, gy = gy0 + ly;
+            const int c = (base + lx + ly) & 1, k = ly * W2 + (lx >> 1);
+            if ((unsigned)gx < (unsigned)L.nx && (unsigned)gy < (unsigned)L.ny) {
+                const double pv = (T.mode[c][k] & MODE_UPDATE) ? T.p[c][k] + (double)T.d[c][k] : 0.0;
+                T.p[c][k] = pv;
+                __stcg(&L.x.p[(size_t)gy * L.x.P + gx], pv);
+            }
+        }
+        ok = grid_barrier(P.barrier, nblocks);
+        if (!ok) break;
+        for (int i = threadIdx.x; i < EX * EY; i += PS_THREADS) {
+            const int ly = i / EX, lx = i - ly * EX;
+            if (owned(lx, ly)) continue;
+            const int gx = gx0 + lx, gy = gy0 + ly;
+            const bool in = (unsigned)gx < (unsigned)L.nx && (unsigned)gy < (unsigned)L.ny;
+            T.p[(base + lx + ly) & 1][ly * W2 + (lx >> 1)] = in ? __ldcg(&L.x.p[(size_t)gy * L.x.P + gx]) : 0.0;
+        }
+        __syncthreads();
+        part = mix_check(T, base, H, tx, ty, cdiv, factor);
+        if (threadIdx.x == 0) P.partials[blockIdx.x] = part;
+        ok = grid_barrier(P.barrier, nblocks);
+        if (!ok) break;
+        r = ps_total_relative(P.partials, nblocks);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        P.result->iterations = iters;
+        P.result->converged = (ok && r <= P.tol) ? 1 : 0;
+        P.result->error = ok ? 0 : 1;
+        P.result->r0 = r0;
+        P.result->r1 = r;
+    }
+}
+
+// Global-memory form of the same solve for grids the persistent scheme
+// cannot hold (one launch per step of the algorithm).
+struct MixPlanes {
+    Plane<float4> w;
+    PF inv, rc, d;
+    Plane<double> den;
+    Plane<unsigned char> mode;
+};
+__global__ void k_mix_coefficients(Level64 L, MixPlanes M) {
+    const int gx = blockIdx.x * blockDim.x + threadIdx.x, gy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (gx >= L.nx || gy >= L.ny) return;
+    unsigned char m = MODE_ZERO;
+    double den = 0.0;
+    float inv = 0.0f;
+    float4 wk = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    const float phi = L.ls.at(gx, gy);
+    if (phi < 0.0f) {
+        const float f[4] = {L.fu.at(gx, gy), L.fu.at(gx + 1, gy), L.fv.at(gx, gy), L.fv.at(gx, gy + 1)};
+        if (!(f[0] == 0.0f && f[1] == 0.0f && f[2] == 0.0f && f[3] == 0.0f)) {
+            m |= MODE_COUNTED;
+            const int ox[4] = {-1, 1, 0, 0}, oy[4] = {0, 0, -1, 1};
+            float wv[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int jx = gx + ox[q], jy = gy + oy[q];
+                if ((unsigned)jx < (unsigned)L.nx && (unsigned)jy < (unsigned)L.ny) {
+                    const float level = L.ls.at(jx, jy);
+                    if (level < 0.0f) {
+                        den += (double)f[q];
+                        wv[q] = f[q];
+                    } else {
+                        den += (double)f[q] * (1.0 - (double)level / (double)phi);
+                    }
+                }
+            }
+            wk = make_float4(wv[0], wv[1], wv[2], wv[3]);
+            if (!(fabs(den) < (double)1.0e-6f)) {
+                m = (unsigned char)((m & MODE_COUNTED) | MODE_UPDATE);
+                inv = (float)(1.0 / den);
+            }
+        }
+    }
+    M.mode.at(gx, gy) = m;
+    M.den.at(gx, gy) = den;
+    M.inv.at(gx, gy) = inv;
+    M.w.at(gx, gy) = wk;
+}
+__global__ void __launch_bounds__(NORM_THREADS) k_mix_residual(Level64 L, MixPlanes M, double cdiv, double factor,
+                                                               double2* partials) {
+    __shared__ double sr[NORM_THREADS / 32], sb[NORM_THREADS / 32];
+    double ar = 0.0, ab = 0.0;
+    const int n = L.nx * L.ny;
+    for (int i = blockIdx.x * NORM_THREADS + threadIdx.x; i < n; i += gridDim.x * NORM_THREADS) {
+        const int y = i / L.nx, x = i - y * L.nx;
+        const unsigned char m = M.mode.at(x, y);
+        float rcv = 0.0f;
+        if (m & MODE_COUNTED) {
+            const float4 wk = M.w.at(x, y);
+            double sum = (double)wk.x * L.x.ld(x - 1, y);
+            sum = sum + (double)wk.y * L.x.ld(x + 1, y);
+            sum = sum + (double)wk.z * L.x.ld(x, y - 1);
+            sum = sum + (double)wk.w * L.x.ld(x, y + 1);
+            const double bb = L.b.at(x, y);
+            const double r = bb - factor * (M.den.at(x, y) * L.x.at(x, y) - sum);
+            if (m & MODE_UPDATE) rcv = (float)(cdiv * r);
+            ar += r * r;
+            ab += bb * bb;
+        }
+        M.rc.at(x, y) = rcv;
+        M.d.at(x, y) = 0.0f;
+    }
+    ar = warp_sum(ar);
+    ab = warp_sum(ab);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) {
+        sr[wid] = ar;
+        sb[wid] = ab;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double tr = 0.0, tb = 0.0;
+        for (int k = 0; k < NORM_THREADS / 32; ++k) {
+            tr += sr[k];
+            tb += sb[k];
+        }
+        partials[blockIdx.x] = make_double2(tr, tb);
+    }
+}
+__global__ void k_mix_sweep(MixPlanes M, int nx, int ny, float w, int color) {
+    const int tx = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int x = 2 * tx + ((y + color) & 1);
+    if (x >= nx || y >= ny) return;
+    if (!(M.mode.at(x, y) & MODE_UPDATE)) return;
+    const float4 wk = M.w.at(x, y);
+    float nume = M.rc.at(x, y);
+    nume = nume + wk.x * M.d.ld(x - 1, y);
+    nume = nume + wk.y * M.d.ld(x + 1, y);
+    nume = nume + wk.z * M.d.ld(x, y - 1);
+    nume = nume + wk.w * M.d.ld(x, y + 1);
+    M.d.at(x, y) = w * (nume * M.inv.at(x, y)) + (1.0f - w) * M.d.at(x, y);
+}
+__global__ void k_mix_apply(Level64 L, MixPlanes M) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= L.nx || y >= L.ny) return;
+    double& pv = L.x.at(x, y);
+    pv = (M.mode.at(x, y) & MODE_UPDATE) ? pv + (double)M.d.at(x, y) : 0.0;
+}
+
+// ---------------------------------------------------------------------------
 // Fixed-count f32 sweeps (the reference's mode) as tiled, temporally blocked
 // launches: each CTA loads its tile plus a halo of 2K cells, builds the
 // per-cell coefficients of gauss_seidel.wgsl:44-80 in the reference's f32
@@ -624,6 +974,150 @@ inline efl_status solve_gs64_persistent(SolverWorkspace& ws, const Level64& L, c
         *err = "persistent solver: a grid barrier timed out";
         return EFL_ERR_CUDA;
     }
+    return EFL_OK;
+}
+
+// Plans for the mixed persistent solve (MixTile: 53 bytes per cell).
+template <int EX, int EY, int KMAX>
+inline bool try_plan_mix(const SolverWorkspace& ws, int nx, int ny, PersistentPlan* p) {
+    const int tx = EX - 4 * KMAX, ty = EY - 4 * KMAX;
+    p->kmax = KMAX;
+    p->tx = tx;
+    p->ty = ty;
+    p->tiles_x = (nx + tx - 1) / tx;
+    p->tiles_y = (ny + ty - 1) / ty;
+    p->smem = sizeof(MixTile<EX, EY>);
+    p->kernel = (const void*)k_gsmix_persistent<EX, EY, KMAX>;
+    if (p->smem + 1024 > ws.max_smem) return false;
+    if (p->tiles_x * p->tiles_y > ws.num_sms || p->tiles_x * p->tiles_y > ws.max_blocks) return false;
+    return true;
+}
+inline PersistentPlan plan_mix(const SolverWorkspace& ws, int nx, int ny) {
+    PersistentPlan p;
+    if (try_plan_mix<80, 48, 4>(ws, nx, ny, &p) ||  // 64 x 32 owned
+        try_plan_mix<48, 48, 4>(ws, nx, ny, &p) ||  // 32 x 32
+        try_plan_mix<72, 56, 2>(ws, nx, ny, &p) ||  // 64 x 48
+        try_plan_mix<40, 40, 4>(ws, nx, ny, &p)) {  // 24 x 24
+        p.ok = true;
+        return p;
+    }
+    return PersistentPlan{};
+}
+
+// Tolerance-driven solve, one cooperative launch.  dbuf: an f32 plane of the
+// level's extent for the correction's halo exchange.  EFL_ERR_STATE: the grid
+// does not fit the persistent scheme.
+inline efl_status solve_gsmix_persistent(SolverWorkspace& ws, const Level64& L, const PF& dbuf, const Uniform& U,
+                                         float weight, double tol, uint32_t max_iters, uint32_t check_interval,
+                                         cudaStream_t stream, SolveResult* out, std::string* err) {
+    PersistentPlan plan = plan_mix(ws, L.nx, L.ny);
+    if (!plan.ok) return EFL_ERR_STATE;
+    if (cudaFuncSetAttribute(plan.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plan.smem) !=
+        cudaSuccess) {
+        cudaGetLastError();
+        return EFL_ERR_STATE;
+    }
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, plan.kernel, PS_THREADS, plan.smem) != cudaSuccess ||
+        per_sm < 1 || plan.tiles_x * plan.tiles_y > per_sm * ws.num_sms) {
+        cudaGetLastError();
+        return EFL_ERR_STATE;
+    }
+    PersistentParams P;
+    P.L = L;
+    P.tx = plan.tx;
+    P.ty = plan.ty;
+    P.kmax = plan.kmax;
+    P.halo = 2 * plan.kmax;
+    P.tiles_x = plan.tiles_x;
+    const double dx = (double)U.dx;
+    P.cdiv = dx * dx * (double)U.rho / (double)U.dt;
+    P.factor = (double)U.dt / (double)U.rho / dx / dx;
+    P.weight = (double)weight;
+    P.tol = tol;
+    P.max_iters = max_iters;
+    P.check_interval = std::max<uint32_t>(1, check_interval);
+    P.partials = ws.partials;
+    P.barrier = ws.barrier;
+    P.result = ws.result;
+    if (cudaMemsetAsync(ws.barrier, 0, sizeof(GridBarrier), stream) != cudaSuccess) {
+        *err = "barrier reset failed";
+        return EFL_ERR_CUDA;
+    }
+    PF db = dbuf;
+    void* args[] = {&P, &db};
+    count_launch();
+    cudaError_t e = cudaLaunchCooperativeKernel(plan.kernel, dim3(plan.tiles_x * plan.tiles_y), dim3(PS_THREADS),
+                                                args, plan.smem, stream);
+    if (e != cudaSuccess) {
+        *err = std::string("cooperative launch of the mixed solver failed: ") + cudaGetErrorString(e);
+        return EFL_ERR_CUDA;
+    }
+    if (cudaMemcpyAsync(ws.h_result, ws.result, sizeof(SolveResult), cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+        cudaStreamSynchronize(stream) != cudaSuccess) {
+        *err = std::string("mixed solver failed: ") + cudaGetErrorString(cudaGetLastError());
+        return EFL_ERR_CUDA;
+    }
+    *out = *ws.h_result;
+    if (out->error) {
+        *err = "mixed solver: a grid barrier timed out";
+        return EFL_ERR_CUDA;
+    }
+    return EFL_OK;
+}
+
+// The same solve with global-memory kernels and a host loop (grids beyond the
+// persistent scheme).  M must hold planes of the level's extent.
+inline efl_status solve_gsmix_global(SolverWorkspace& ws, const Level64& L, const MixPlanes& M, const Uniform& U,
+                                     float weight, double tol, uint32_t max_iters, uint32_t check_interval,
+                                     cudaStream_t stream, SolveResult* out, std::string* err) {
+    const dim3 b(32, 8);
+    const dim3 g((L.nx + 31) / 32, (L.ny + 7) / 8);
+    const dim3 gh(((L.nx + 1) / 2 + 31) / 32, (L.ny + 7) / 8);
+    const double dx = (double)U.dx;
+    const double cdiv = dx * dx * (double)U.rho / (double)U.dt;
+    const double factor = (double)U.dt / (double)U.rho / dx / dx;
+    const int nblocks = std::min(1024, std::max(1, (L.nx * L.ny + NORM_THREADS - 1) / NORM_THREADS));
+    if (nblocks > ws.max_blocks) return EFL_ERR_STATE;
+    k_mix_coefficients<<<g, b, count_launch(), stream>>>(L, M);
+    auto residual = [&](double* rel) -> efl_status {
+        k_mix_residual<<<nblocks, NORM_THREADS, count_launch(), stream>>>(L, M, cdiv, factor, ws.partials);
+        std::vector<double2> h(nblocks);
+        if (cudaMemcpyAsync(h.data(), ws.partials, nblocks * sizeof(double2), cudaMemcpyDeviceToHost, stream) !=
+                cudaSuccess ||
+            cudaStreamSynchronize(stream) != cudaSuccess) {
+            *err = std::string("mixed solver (global): ") + cudaGetErrorString(cudaGetLastError());
+            return EFL_ERR_CUDA;
+        }
+        double r = 0.0, bb = 0.0;
+        for (int i = 0; i < nblocks; ++i) {
+            r += h[i].x;
+            bb += h[i].y;
+        }
+        *rel = bb > 0.0 ? std::sqrt(r) / std::sqrt(bb) : (r > 0.0 ? INFINITY : 0.0);
+        return EFL_OK;
+    };
+    double rel;
+    efl_status st = residual(&rel);
+    if (st != EFL_OK) return st;
+    out->r0 = rel;
+    uint32_t iters = 0;
+    const uint32_t chk = std::max<uint32_t>(1, check_interval);
+    while (!(rel <= tol) && iters < max_iters) {
+        const uint32_t n = std::min(chk, max_iters - iters);
+        for (uint32_t it = 0; it < n; ++it) {
+            k_mix_sweep<<<gh, b, count_launch(), stream>>>(M, L.nx, L.ny, weight, 1);
+            k_mix_sweep<<<gh, b, count_launch(), stream>>>(M, L.nx, L.ny, weight, 0);
+        }
+        k_mix_apply<<<g, b, count_launch(), stream>>>(L, M);
+        iters += n;
+        st = residual(&rel);
+        if (st != EFL_OK) return st;
+    }
+    out->iterations = iters;
+    out->r1 = rel;
+    out->converged = rel <= tol ? 1 : 0;
+    out->error = 0;
     return EFL_OK;
 }
 

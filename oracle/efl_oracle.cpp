@@ -693,6 +693,150 @@ void mg64_store_p0(eflo_sim& s) {
     for (size_t i = 0; i < L.x.a.size(); ++i) s.p0.a[i] = (float)L.x.a[i];
 }
 
+// Tolerance-driven red-black Gauss-Seidel (an extension of projection.rs,
+// gauss_seidel.wgsl:44-88) in mixed-precision iterative-refinement form.
+// Every check block of n iterations: the FP64 residual r of the FP64 iterate
+// p (factored operator, see residual_at<double>) gives the convergence test
+// and the f32 right-hand side rc = f32(cdiv * r); n SOR red-black iterations
+// then run in f32 on the correction d (start 0) with the per-cell f32
+// coefficients w_k (face fraction of fluid in-bounds neighbours, else 0) and
+// inv = f32(1 / denom); finally p += d (f64), and cells the reference sets to
+// zero (air, fully solid, |denom| < 1e-6) get p = 0.  In exact arithmetic
+// this is the SOR iteration itself (it is affine), so iteration counts are
+// those of RBGS; the f32 sweeps only carry the correction.
+struct MixCell {
+    unsigned char mode;  // 0 skip, 1 zero, 2 update; +4 counted
+    float w[4];
+    float inv;
+    double den;
+};
+void mix_coefficients(const eflo_sim& s, std::vector<MixCell>& cells) {
+    const int W = s.nx, Hh = s.ny;
+    cells.assign((size_t)W * Hh, MixCell{});
+    par_rows(0, Hh, [&](int y) {
+        static const int off[4][2] = {{-1, 0}, {1, 0}, {0, -1}, {0, 1}};
+        for (int x = 0; x < W; ++x) {
+            MixCell& c = cells[(size_t)y * W + x];
+            c.mode = 1;
+            float lij = s.ls0.ld(x, y);
+            if (!(lij < 0.0f)) continue;
+            F4 f = s.af.ld(x, y);
+            if (f.x == 0.0f && f.y == 0.0f && f.z == 0.0f && f.w == 0.0f) continue;
+            c.mode |= 4;
+            const float fv[4] = {f.x, f.y, f.z, f.w};
+            double den = 0.0;
+            for (int i = 0; i < 4; ++i) {
+                int jx = x + off[i][0], jy = y + off[i][1];
+                if (jx >= 0 && jy >= 0 && jx < W && jy < Hh) {
+                    float level = s.ls0.ld(jx, jy);
+                    if (level < 0.0f) {
+                        den += (double)fv[i];
+                        c.w[i] = fv[i];
+                    } else {
+                        den += (double)fv[i] * (1.0 - (double)level / (double)lij);
+                    }
+                }
+            }
+            c.den = den;
+            if (!(std::fabs(den) < (double)1.0e-6f)) {
+                c.mode = (unsigned char)((c.mode & 4) | 2);
+                c.inv = (float)(1.0 / den);
+            }
+        }
+    });
+}
+efl_status gs_mixed_solve(eflo_sim& s, uint32_t* iters_out, double* r0_out, double* r1_out) {
+    const efl_projection& P = s.cfg.projection;
+    const int W = s.nx, Hh = s.ny;
+    Level64& L = s.mg64[0];
+    std::vector<MixCell> cells;
+    mix_coefficients(s, cells);
+    const double dx = (double)s.U.dx;
+    const double cdiv = dx * dx * (double)s.U.rho / (double)s.U.dt;
+    const double factor = (double)s.U.dt / (double)s.U.rho / dx / dx;
+    const float w = P.sor_weight, omw = 1.0f - P.sor_weight;
+    std::vector<double> r((size_t)W * Hh);
+    std::vector<float> rc((size_t)W * Hh), d((size_t)W * Hh);
+    auto residual = [&]() {  // fills r, returns the relative residual
+        std::vector<double> pr(Hh), pb(Hh);
+        par_rows(0, Hh, [&](int y) {
+            double sr = 0.0, sb = 0.0;
+            static const int off[4][2] = {{-1, 0}, {1, 0}, {0, -1}, {0, 1}};
+            for (int x = 0; x < W; ++x) {
+                const MixCell& c = cells[(size_t)y * W + x];
+                double rv = 0.0;
+                if (c.mode & 4) {
+                    double sum = 0.0;
+                    for (int i = 0; i < 4; ++i) {
+                        int jx = x + off[i][0], jy = y + off[i][1];
+                        double pn = (jx >= 0 && jy >= 0 && jx < W && jy < Hh) ? L.x.at(jx, jy) : 0.0;
+                        if (i == 0) sum = (double)c.w[0] * pn;
+                        else sum = sum + (double)c.w[i] * pn;
+                    }
+                    const double bv = L.b.at(x, y);
+                    rv = bv - factor * (c.den * L.x.at(x, y) - sum);
+                    sr += rv * rv;
+                    sb += bv * bv;
+                }
+                r[(size_t)y * W + x] = rv;
+            }
+            pr[y] = sr;
+            pb[y] = sb;
+        });
+        double R = 0.0, B = 0.0;
+        for (int y = 0; y < Hh; ++y) {
+            R += pr[y];
+            B += pb[y];
+        }
+        return rel_from(R, B);
+    };
+    uint32_t iters = 0;
+    double rel = residual();
+    *r0_out = rel;
+    const uint32_t chk = std::max<uint32_t>(1, P.check_interval);
+    while (!(rel <= (double)P.tolerance) && iters < P.max_iterations) {
+        const uint32_t n = std::min(chk, P.max_iterations - iters);
+        par_rows(0, Hh, [&](int y) {
+            for (int x = 0; x < W; ++x) {
+                size_t i = (size_t)y * W + x;
+                rc[i] = (cells[i].mode & 2) ? (float)(cdiv * r[i]) : 0.0f;
+                d[i] = 0.0f;
+            }
+        });
+        for (uint32_t it = 0; it < n; ++it) {
+            for (int color = 1; color >= 0; --color) {  // red ((x+y) odd) then black
+                par_rows(0, Hh, [&](int y) {
+                    for (int x = (y + color) & 1; x < W; x += 2) {
+                        size_t i = (size_t)y * W + x;
+                        const MixCell& c = cells[i];
+                        if (!(c.mode & 2)) continue;
+                        const float dl = x > 0 ? d[i - 1] : 0.0f, dr = x + 1 < W ? d[i + 1] : 0.0f;
+                        const float du = y > 0 ? d[i - W] : 0.0f, dd = y + 1 < Hh ? d[i + W] : 0.0f;
+                        float nume = rc[i];
+                        nume = nume + c.w[0] * dl;
+                        nume = nume + c.w[1] * dr;
+                        nume = nume + c.w[2] * du;
+                        nume = nume + c.w[3] * dd;
+                        d[i] = w * (nume * c.inv) + omw * d[i];
+                    }
+                });
+            }
+        }
+        par_rows(0, Hh, [&](int y) {
+            for (int x = 0; x < W; ++x) {
+                size_t i = (size_t)y * W + x;
+                double& pv = L.x.at(x, y);
+                pv = (cells[i].mode & 2) ? pv + (double)d[i] : 0.0;
+            }
+        });
+        iters += n;
+        rel = residual();
+    }
+    *iters_out = iters;
+    *r1_out = rel;
+    return EFL_OK;
+}
+
 // projection.rs:89-164.  tolerance > 0 (an extension) solves to
 // ||b - A p|| / ||b|| <= tolerance with an FP64 iterate: the f32 pressure
 // cannot represent a solution that accurate when the hydrostatic pressure
@@ -727,13 +871,10 @@ efl_status k_projection(eflo_sim& s, efl_step_stats* st) {
         double r = rel();
         r0 = r;
         if (P.method == EFL_PROJECTION_GAUSS_SEIDEL) {
-            uint32_t chk = std::max<uint32_t>(1, P.check_interval);
-            while (!(r <= (double)P.tolerance) && iters < P.max_iterations) {
-                uint32_t n = std::min(chk, P.max_iterations - iters);
-                gs_iterations(L.x, L.b, L.ls, L.af, s.U, P.sor_weight, 1.0f, n);
-                iters += n;
-                r = rel();
-            }
+            double a, b;
+            gs_mixed_solve(s, &iters, &a, &b);
+            r0 = a;
+            r = b;
         } else {
             while (!(r <= (double)P.tolerance) && iters < P.max_iterations) {
                 v_cycle(s.mg64, s.U, 0, P);

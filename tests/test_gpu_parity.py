@@ -145,3 +145,21 @@ def test_local_forces_consumed_once(oracle_api, gpu_api):
         s.step(sc.dt)
     assert not compare_fields(g, o)
     assert u_before.shape == g.get(capi.FIELD_U1).shape
+
+
+def test_coupled_tolerance_global_path(oracle_api, gpu_api):
+    """1024 x 512 does not fit the persistent scheme: the global-memory form of the
+    mixed-precision solve runs, with the same iteration count and bit-exact fields."""
+    sc = small_coupled(1024, tolerance=1e-5, n_per_shape=1)
+    sc.cfg.ny = 512
+    sc.oneshot[0].center[1] = -256.0 + 0.5 * 0.4 * 512
+    sc.oneshot[0].data[1] = 0.5 * 0.4 * 512
+    o, g = make_pair(sc, oracle_api, gpu_api)
+    o.step(sc.dt)
+    g.step(sc.dt)
+    so, sg = o.step(sc.dt), g.step(sc.dt)
+    assert so.converged and sg.converged
+    assert so.pressure_iterations == sg.pressure_iterations
+    assert abs(so.residual - sg.residual) <= 1e-9 * max(1.0, abs(so.residual))
+    for f in (capi.FIELD_PRESSURE, capi.FIELD_U, capi.FIELD_V, capi.FIELD_LEVELSET_AIR):
+        assert np.array_equal(g.get(f), o.get(f)), f
