@@ -410,7 +410,9 @@ efl_status gs_mixed(efl_sim* s, float weight, double tol, uint32_t max_iters, ui
         s->mixp_ready = true;
     }
     ps = solve_gsmix_global(s->solver, L, s->mixp, s->U, weight, tol, max_iters, check, s->stream, res, &perr);
-    if (ps != EFL_OK) return set_err(s, ps == EFL_ERR_STATE ? EFL_ERR_CUDA : ps, "%s", perr.c_str());
+    if (ps != EFL_OK)
+        return set_err(s, ps == EFL_ERR_STATE ? EFL_ERR_CUDA : ps, "mixed solve (global form) failed: %s",
+                       perr.empty() ? "no workspace for this grid" : perr.c_str());
     LAUNCH_CHECK();
     return EFL_OK;
 }

@@ -1077,8 +1077,7 @@ inline efl_status solve_gsmix_global(SolverWorkspace& ws, const Level64& L, cons
     const double dx = (double)U.dx;
     const double cdiv = dx * dx * (double)U.rho / (double)U.dt;
     const double factor = (double)U.dt / (double)U.rho / dx / dx;
-    const int nblocks = std::min(1024, std::max(1, (L.nx * L.ny + NORM_THREADS - 1) / NORM_THREADS));
-    if (nblocks > ws.max_blocks) return EFL_ERR_STATE;
+    const int nblocks = std::min(ws.max_blocks, std::max(1, (L.nx * L.ny + NORM_THREADS - 1) / NORM_THREADS));
     k_mix_coefficients<<<g, b, count_launch(), stream>>>(L, M);
     auto residual = [&](double* rel) -> efl_status {
         k_mix_residual<<<nblocks, NORM_THREADS, count_launch(), stream>>>(L, M, cdiv, factor, ws.partials);
