@@ -1,0 +1,107 @@
+"""Host-side logic of the plugin-API mirror (no GPU, no compute calls)."""
+import math
+import warnings
+
+import numpy as np
+import pytest
+
+from bevy_eulerian_fluid_b200 import _capi as capi
+from bevy_eulerian_fluid_b200 import scenes
+from bevy_eulerian_fluid_b200.plugin import (Collider, FastIterativeMethodConfig, FluidPlugin, FluidSourceShape,
+                                             GaussSeidelConfig, MultiGridConfig, ProjectionMethod,
+                                             ReinitializeMethod, RigidBody, RigidBodyKind, pack_obstacles)
+from bevy_eulerian_fluid_b200.rigid import RigidWorld
+
+
+def test_fluid_plugin_rejects_non_positive_length_unit():
+    with pytest.raises(ValueError, match="length_unit must be positive value."):
+        FluidPlugin(0.0)
+    assert FluidPlugin(10.0).grid_length == pytest.approx(0.1)
+
+
+def test_projection_and_reinit_display_and_c_structs():
+    assert str(ProjectionMethod.Jacobi()) == "Jacobi"
+    assert str(ProjectionMethod.GaussSeidel(GaussSeidelConfig(20))) == "Gauss-Seidel(20)"
+    assert str(ProjectionMethod.MultiGrid(MultiGridConfig())) == "Multigrid(2-3-2)"
+    assert str(ReinitializeMethod.JumpFlooding()) == "Jump Flooding"
+    assert str(ReinitializeMethod.FastIterative(FastIterativeMethodConfig(7))) == "Fast Iterative(7)"
+    p = ProjectionMethod.MultiGrid().to_c()
+    assert (p.method, p.mg_pre, p.mg_post, p.mg_coarsest) == (capi.PROJECTION_MULTIGRID, 2, 2, 3)
+    assert ProjectionMethod.default().to_c().gs_iterations == 20
+    assert abs(ProjectionMethod.default().to_c().sor_weight - 1.9) < 1e-6
+    r = ReinitializeMethod.default().to_c()
+    assert (r.method, r.fim_iterations) == (capi.REINIT_FAST_ITERATIVE, 10)
+
+
+def test_source_shapes():
+    c = FluidSourceShape.Circle(3.0)
+    a = FluidSourceShape.Aabb((4.0, 5.0))
+    assert (c.to_vec2(), c.shape_type_digit()) == ((3.0, 0.0), 0)
+    assert (a.to_vec2(), a.shape_type_digit()) == ((4.0, 5.0), 1)
+
+
+def test_obstacle_packing_layout_and_inverse():
+    b = RigidBody(Collider.rectangle(10.0, 4.0), (12.0, -3.0), 0.7, (1.0, 2.0), 0.3)
+    o = pack_obstacles([b])[0]
+    assert o.shape == capi.SHAPE_RECTANGLE and tuple(o.values[:2]) == (5.0, 2.0)
+    m = np.array(o.transform, np.float64).reshape(4, 4).T  # column-major
+    inv = np.array(o.inverse_transform, np.float64).reshape(4, 4).T
+    assert np.allclose(m @ inv, np.eye(4), atol=1e-6)
+    assert m[0, 3] == pytest.approx(12.0) and m[1, 3] == pytest.approx(-3.0)
+    assert (o.linear_velocity[0], o.linear_velocity[1], o.angular_velocity) == pytest.approx((1.0, 2.0, 0.3))
+
+
+def test_collider_areas():
+    assert Collider.circle(2.0).area() == pytest.approx(math.pi * 4)
+    assert Collider.rectangle(2.0, 3.0).area() == pytest.approx(6.0)
+    assert Collider.triangle((0, 0), (2, 0), (0, 2)).area() == pytest.approx(2.0)
+    assert Collider.capsule(1.0, 4.0).area() == pytest.approx(math.pi + 8.0)
+
+
+def test_scenes_are_deterministic():
+    a, b = scenes.coupled(512), scenes.coupled(512)
+    assert len(a.bodies) == 24
+    assert [bytes(pack_obstacles(a.bodies)[i]) for i in range(24)] == \
+        [bytes(pack_obstacles(b.bodies)[i]) for i in range(24)]
+    shapes = [x.collider.shape for x in a.bodies]
+    assert shapes == [0] * 6 + [1] * 6 + [2] * 6 + [4] * 6
+    for x in a.bodies:
+        assert -256 < x.position[0] < 256 and 0 < x.position[1] < 256
+        assert 0.5 * scenes.RHO <= x.density <= 2.0 * scenes.RHO
+    d = scenes.dam_break(256)
+    s = d.oneshot[0]
+    assert (s.center[0], s.center[1], s.data[0], s.data[1]) == pytest.approx((0.0, -51.2, 128.0, 76.8))
+    phi, b = scenes.microbench_inputs(64)
+    assert abs(float(b.astype(np.float64).mean())) < 1e-6 and np.all(phi == -1)
+
+
+def test_rigid_world_gravity_and_walls():
+    body = RigidBody(Collider.circle(5.0), (0.0, 0.0), density=1.0)
+    w = RigidWorld([body], (64, 64), gravity=98.0, grid_length=0.1)
+    for _ in range(600):
+        w.step(1 / 60)
+    assert body.position[1] == pytest.approx(-32 + 1 + 5)  # rests on the floor
+    assert body.linear_velocity[1] == 0.0
+    static = RigidBody(Collider.circle(5.0), (10.0, 10.0), kind=RigidBodyKind.Static)
+    w2 = RigidWorld([static], (64, 64), gravity=98.0, grid_length=0.1)
+    w2.step(1 / 60)
+    assert static.position == (10.0, 10.0)
+
+
+def test_rigid_world_applies_fluid_force_like_the_reference():
+    """forces_to_solid_readback: force * dt / grid_length, y flipped, torque negated."""
+    body = RigidBody(Collider.circle(2.0), (0.0, 0.0), density=1.0)
+    w = RigidWorld([body], (512, 512), gravity=0.0, grid_length=0.1)
+    w.apply_fluid_forces(np.array([[10.0, 20.0, 5.0]]), 0.1)
+    w.step(0.1)
+    m = math.pi * 4
+    assert body.linear_velocity[0] == pytest.approx(10.0 * 0.1 / 0.1 / m * 0.1)
+    assert body.linear_velocity[1] == pytest.approx(-20.0 * 0.1 / 0.1 / m * 0.1)
+    assert body.angular_velocity < 0
+
+
+def test_default_config_matches_reference_defaults():
+    c = capi.default_config(256, 128)
+    assert (c.nx, c.ny, c.length_unit, c.rho) == (256, 128, 1.0, 1.0)
+    assert tuple(c.gravity) == pytest.approx((0.0, 9.8))
+    assert list(c.transform) == [1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1]
