@@ -127,10 +127,16 @@ SIGNATURES = {
     "residual_norms_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
                                          C.c_uint32, C.c_size_t, C.c_float, C.c_float, C.c_float, C.c_void_p,
                                          C.c_void_p]),
+    "batch_create": (C.c_int, [C.POINTER(Config), C.c_uint32, C.POINTER(C.c_void_p)]),
+    "batch_destroy": (C.c_int, [C.c_void_p]),
+    "batch_last_error": (C.c_char_p, [C.c_void_p]),
+    "batch_sim": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(C.c_void_p)]),
+    "batch_step": (C.c_int, [C.c_void_p, C.c_float, C.POINTER(StepStats)]),
 }
 # Functions of efl.h that the oracle restatement does not mirror.
 PRODUCT_ONLY = {"abi_version", "default_config", "field_device_ptr", "stream", "synchronize", "kernel_launches",
-                "pressure_sweeps", "residual_norms_noalloc"}
+                "pressure_sweeps", "residual_norms_noalloc", "batch_create", "batch_destroy", "batch_last_error",
+                "batch_sim", "batch_step"}
 
 
 class EflError(RuntimeError):
@@ -212,10 +218,20 @@ class Sim:
         self.h = h
         self.nx, self.ny = cfg.nx, cfg.ny
 
+    @classmethod
+    def borrowed(cls, api: Api, h: C.c_void_p, cfg: Config) -> "Sim":
+        """A view of a simulation owned by a Batch (close() does not destroy it)."""
+        self = cls.__new__(cls)
+        self.api, self.cfg, self.h = api, cfg, h
+        self.nx, self.ny = cfg.nx, cfg.ny
+        self._borrowed = True
+        return self
+
     # -- lifetime
     def close(self):
         if getattr(self, "h", None):
-            self.api.destroy(self.h)
+            if not getattr(self, "_borrowed", False):
+                self.api.destroy(self.h)
             self.h = None
 
     def __del__(self):
@@ -334,3 +350,60 @@ class Sim:
 
     def pressure_sweeps(self, precision: int, iterations: int):
         self._check(self.api.pressure_sweeps(self.h, precision, iterations))
+
+
+class Batch:
+    """N independent simulations stepped together (efl_batch_*): one shared
+    stream and one cooperative launch for all tolerance-driven solves."""
+
+    def __init__(self, api: Api, cfgs):
+        self.api = api
+        self.cfgs = list(cfgs)
+        arr = (Config * len(self.cfgs))(*self.cfgs)
+        h = C.c_void_p()
+        st = api.batch_create(arr, len(self.cfgs), C.byref(h))
+        if st != OK:
+            raise EflError(st, (api.batch_last_error(None) or b"").decode())
+        self.h = h
+        self.sims = []
+        for i, c in enumerate(self.cfgs):
+            sh = C.c_void_p()
+            self._check(api.batch_sim(self.h, i, C.byref(sh)))
+            self.sims.append(Sim.borrowed(api, sh, c))
+
+    def __len__(self):
+        return len(self.sims)
+
+    def __getitem__(self, i) -> Sim:
+        return self.sims[i]
+
+    def _check(self, st: int, allow=(OK,)) -> int:
+        if st not in allow:
+            raise EflError(st, (self.api.batch_last_error(self.h) or b"").decode())
+        return st
+
+    def step(self, dt: float, allow_not_converged: bool = True):
+        """One frame of every simulation; returns the per-simulation StepStats."""
+        stats = (StepStats * len(self.sims))()
+        allow = (OK, NOT_CONVERGED) if allow_not_converged else (OK,)
+        self._check(self.api.batch_step(self.h, dt, stats), allow)
+        return list(stats)
+
+    def close(self):
+        if getattr(self, "h", None):
+            for s in self.sims:
+                s.h = None
+            self.api.batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

@@ -21,6 +21,7 @@
 #include "efl_kernels.cuh"
 #include "efl_solver.cuh"
 #include "efl_sweep_tma.cuh"
+#include "efl_batch.cuh"
 
 using namespace efl;
 
@@ -83,6 +84,8 @@ struct efl_sim {
     SweepTma tma;
     MixPlanes mixp{};  // global-memory planes of the mixed solve, allocated on first use
     bool mixp_ready = false;
+    PF mix_d2{};       // second correction buffer (batched solve)
+    bool owns_stream = true;
     int* h_err = nullptr;  // pinned copy of the TMA sweep's error flag
 
     Dom dom() const { return Dom{nx, ny}; }
@@ -389,6 +392,20 @@ efl_status sweeps_f32(efl_sim* s, float weight, uint32_t n) {
     return EFL_OK;
 }
 
+efl_status ensure_mix_planes(efl_sim* s) {
+    if (s->mixp_ready) return EFL_OK;
+    const int nx = s->nx, ny = s->ny, P = s->P, R = ny + 1;
+    TRY(alloc_plane(s, s->mixp.w, nx, ny, P, R));
+    TRY(alloc_plane(s, s->mixp.inv, nx, ny, P, R));
+    TRY(alloc_plane(s, s->mixp.rc, nx, ny, P, R));
+    TRY(alloc_plane(s, s->mixp.d, nx, ny, P, R));
+    TRY(alloc_plane(s, s->mixp.den, nx, ny, P, R));
+    TRY(alloc_plane(s, s->mixp.mode, nx, ny, P, R));
+    TRY(alloc_plane(s, s->mix_d2, nx, ny, P, R));
+    s->mixp_ready = true;
+    return EFL_OK;
+}
+
 // The tolerance-driven red-black solve (mixed-precision refinement) on the
 // FP64 iterate of level 0: one cooperative launch when the grid fits the
 // persistent scheme, else global-memory kernels.
@@ -399,16 +416,7 @@ efl_status gs_mixed(efl_sim* s, float weight, double tol, uint32_t max_iters, ui
                                            &perr);
     if (ps == EFL_OK) return EFL_OK;
     if (ps != EFL_ERR_STATE) return set_err(s, ps, "%s", perr.c_str());
-    if (!s->mixp_ready) {
-        const int nx = s->nx, ny = s->ny, P = s->P, R = ny + 1;
-        TRY(alloc_plane(s, s->mixp.w, nx, ny, P, R));
-        TRY(alloc_plane(s, s->mixp.inv, nx, ny, P, R));
-        TRY(alloc_plane(s, s->mixp.rc, nx, ny, P, R));
-        TRY(alloc_plane(s, s->mixp.d, nx, ny, P, R));
-        TRY(alloc_plane(s, s->mixp.den, nx, ny, P, R));
-        TRY(alloc_plane(s, s->mixp.mode, nx, ny, P, R));
-        s->mixp_ready = true;
-    }
+    TRY(ensure_mix_planes(s));
     ps = solve_gsmix_global(s->solver, L, s->mixp, s->U, weight, tol, max_iters, check, s->stream, res, &perr);
     if (ps != EFL_OK)
         return set_err(s, ps == EFL_ERR_STATE ? EFL_ERR_CUDA : ps, "mixed solve (global form) failed: %s",
@@ -759,7 +767,7 @@ efl_status efl_destroy(efl_sim* s) {
     for (auto& b : s->bufs) cudaFree(b.p);
     if (s->d_forces) cudaFree(s->d_forces);
     if (s->h_norms) cudaFreeHost(s->h_norms);
-    if (s->stream) cudaStreamDestroy(s->stream);
+    if (s->stream && s->owns_stream) cudaStreamDestroy(s->stream);
     delete s;
     return EFL_OK;
 }
@@ -1118,3 +1126,259 @@ extern "C" efl_status efl_residual_norms_noalloc(const float* pressure, const fl
     LAUNCH_CHECK();
     return EFL_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Batches of simulations.
+
+struct efl_batch {
+    std::vector<efl_sim*> sims;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    BatchSim* d_sims = nullptr;
+    int2* d_tiles = nullptr;
+    double2* d_partials = nullptr;
+    BatchState* d_state = nullptr;
+    BatchState* h_state = nullptr;  // pinned
+    GridBarrier* d_barrier = nullptr;
+    int ntiles = 0;
+    std::vector<int> tile_start;
+};
+
+namespace {
+constexpr int BT_TX = 64, BT_TY = 32, BT_K = 2;
+std::string g_batch_error;
+
+efl_status batch_err(efl_batch* b, efl_status st, const std::string& m) {
+    if (b) b->err = m;
+    else g_batch_error = m;
+    return st;
+}
+
+void batch_free(efl_batch* b) {
+    if (!b) return;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    for (efl_sim* s : b->sims) efl_destroy(s);
+    cudaFree(b->d_sims);
+    cudaFree(b->d_tiles);
+    cudaFree(b->d_partials);
+    cudaFree(b->d_state);
+    cudaFree(b->d_barrier);
+    if (b->h_state) cudaFreeHost(b->h_state);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+}
+
+// One cooperative launch for the tolerance-driven solves of the batch's
+// simulations listed in `which` (equal check_interval, max_iterations and
+// tolerance), results into stats.
+efl_status batch_solve(efl_batch* b, const std::vector<int>& which, efl_step_stats* stats) {
+    if (which.empty()) return EFL_OK;
+    std::vector<BatchSim> hs;
+    std::vector<int2> tiles;
+    for (int idx : which) {
+        efl_sim* s = b->sims[idx];
+        BatchSim S{};
+        S.L = s->mg64[0];
+        S.M = s->mixp;
+        S.d[0] = s->mixp.d;
+        S.d[1] = s->mix_d2;
+        const double dx = (double)s->U.dx;
+        S.cdiv = dx * dx * (double)s->U.rho / (double)s->U.dt;
+        S.factor = (double)s->U.dt / (double)s->U.rho / dx / dx;
+        S.weight = s->cfg.projection.sor_weight;
+        S.tiles_x = (s->nx + BT_TX - 1) / BT_TX;
+        const int ty = (s->ny + BT_TY - 1) / BT_TY;
+        S.tile_start = (int)tiles.size();
+        S.tile_count = S.tiles_x * ty;
+        for (int t = 0; t < S.tile_count; ++t) tiles.push_back(make_int2((int)hs.size(), t));
+        hs.push_back(S);
+    }
+    const int ns = (int)hs.size(), nt = (int)tiles.size();
+    if (nt > b->ntiles || ns > (int)b->sims.size()) return batch_err(b, EFL_ERR_STATE, "batch tile list overflow");
+    cudaStream_t st = b->stream;
+    if (cudaMemcpyAsync(b->d_sims, hs.data(), ns * sizeof(BatchSim), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaMemcpyAsync(b->d_tiles, tiles.data(), nt * sizeof(int2), cudaMemcpyHostToDevice, st) != cudaSuccess)
+        return batch_err(b, EFL_ERR_CUDA, "batch upload failed");
+    for (int i = 0; i < ns; ++i) {
+        b->h_state[i] = BatchState{};
+        b->h_state[i].active = 1;
+    }
+    if (cudaMemcpyAsync(b->d_state, b->h_state, ns * sizeof(BatchState), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaMemsetAsync(b->d_barrier, 0, sizeof(GridBarrier), st) != cudaSuccess)
+        return batch_err(b, EFL_ERR_CUDA, "batch state upload failed");
+    const efl_projection& P0 = b->sims[which[0]]->cfg.projection;
+    BatchParams Pm;
+    Pm.sims = b->d_sims;
+    Pm.nsims = ns;
+    Pm.ntiles = nt;
+    Pm.tiles = b->d_tiles;
+    Pm.tol = (double)P0.tolerance;
+    Pm.max_iters = P0.max_iterations;
+    Pm.check_interval = std::max<uint32_t>(1, P0.check_interval);
+    Pm.partials = b->d_partials;
+    Pm.state = b->d_state;
+    Pm.barrier = b->d_barrier;
+    constexpr int EX = BT_TX + 4 * BT_K, EY = BT_TY + 4 * BT_K;
+    const size_t smem = sizeof(BatchTile<EX, EY>);
+    const void* kern = (const void*)k_batch_mix<BT_TX, BT_TY, BT_K>;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return batch_err(b, EFL_ERR_CUDA, "batched solver: shared-memory attribute refused");
+    int per_sm = 0, sms = b->sims[which[0]]->solver.num_sms;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, BT_THREADS, smem) != cudaSuccess || per_sm < 1)
+        return batch_err(b, EFL_ERR_CUDA, "batched solver: no co-resident CTA fits");
+    const int grid = std::min(per_sm * sms, std::max(1, nt));
+    void* args[] = {&Pm};
+    count_launch();
+    cudaError_t e = cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(BT_THREADS), args, smem, st);
+    if (e != cudaSuccess)
+        return batch_err(b, EFL_ERR_CUDA, std::string("batched solver launch failed: ") + cudaGetErrorString(e));
+    GridBarrier hb{};
+    if (cudaMemcpyAsync(b->h_state, b->d_state, ns * sizeof(BatchState), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaMemcpyAsync(&hb, b->d_barrier, sizeof(hb), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return batch_err(b, EFL_ERR_CUDA, std::string("batched solver failed: ") + cudaGetErrorString(cudaGetLastError()));
+    if (hb.error) return batch_err(b, EFL_ERR_CUDA, "batched solver: a grid barrier timed out");
+    for (int i = 0; i < ns; ++i) {
+        efl_step_stats* o = stats ? &stats[which[i]] : nullptr;
+        if (!o) continue;
+        o->pressure_iterations = b->h_state[i].iterations;
+        o->converged = b->h_state[i].converged;
+        o->residual = b->h_state[i].r1;
+        o->residual_initial = b->h_state[i].r0;
+    }
+    return EFL_OK;
+}
+}  // namespace
+
+extern "C" {
+
+efl_status efl_batch_create(const efl_config* cfgs, uint32_t n, efl_batch** out) {
+    if (!out || !cfgs || n == 0) return batch_err(nullptr, EFL_ERR_INVALID_ARGUMENT, "null argument or empty batch");
+    *out = nullptr;
+    efl_batch* b = new efl_batch();
+    b->device = cfgs[0].device;
+    for (uint32_t i = 0; i < n; ++i)
+        if (cfgs[i].device != b->device) {
+            delete b;
+            return batch_err(nullptr, EFL_ERR_INVALID_ARGUMENT, "all simulations of a batch must be on one device");
+        }
+    if (cudaSetDevice(b->device) != cudaSuccess || cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete b;
+        return batch_err(nullptr, EFL_ERR_CUDA, "batch stream creation failed");
+    }
+    int total_tiles = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        efl_sim* s = nullptr;
+        efl_status st = efl_create(&cfgs[i], &s);
+        if (st != EFL_OK) {
+            std::string m = std::string("simulation ") + std::to_string(i) + ": " + efl_last_error(nullptr);
+            batch_free(b);
+            return batch_err(nullptr, st, m);
+        }
+        cudaStreamSynchronize(s->stream);
+        cudaStreamDestroy(s->stream);
+        s->stream = b->stream;
+        s->owns_stream = false;
+        b->sims.push_back(s);
+        if (ensure_mix_planes(s) != EFL_OK) {
+            std::string m = s->err;
+            batch_free(b);
+            return batch_err(nullptr, EFL_ERR_OUT_OF_MEMORY, m);
+        }
+        total_tiles += ((s->nx + BT_TX - 1) / BT_TX) * ((s->ny + BT_TY - 1) / BT_TY);
+    }
+    b->ntiles = total_tiles;
+    if (cudaMalloc(&b->d_sims, n * sizeof(BatchSim)) != cudaSuccess ||
+        cudaMalloc(&b->d_tiles, total_tiles * sizeof(int2)) != cudaSuccess ||
+        cudaMalloc(&b->d_partials, total_tiles * sizeof(double2)) != cudaSuccess ||
+        cudaMalloc(&b->d_state, n * sizeof(BatchState)) != cudaSuccess ||
+        cudaMalloc(&b->d_barrier, sizeof(GridBarrier)) != cudaSuccess ||
+        cudaMallocHost(&b->h_state, n * sizeof(BatchState)) != cudaSuccess) {
+        batch_free(b);
+        return batch_err(nullptr, EFL_ERR_OUT_OF_MEMORY, "batch workspace allocation failed");
+    }
+    *out = b;
+    return EFL_OK;
+}
+
+efl_status efl_batch_destroy(efl_batch* b) {
+    batch_free(b);
+    return EFL_OK;
+}
+
+const char* efl_batch_last_error(const efl_batch* b) { return b ? b->err.c_str() : g_batch_error.c_str(); }
+
+efl_status efl_batch_sim(efl_batch* b, uint32_t i, efl_sim** sim) {
+    if (!b || !sim || i >= b->sims.size()) return batch_err(b, EFL_ERR_INVALID_ARGUMENT, "bad batch index");
+    *sim = b->sims[i];
+    return EFL_OK;
+}
+
+efl_status efl_batch_step(efl_batch* b, float dt, efl_step_stats* stats) {
+    if (!b) return batch_err(nullptr, EFL_ERR_INVALID_ARGUMENT, "null batch");
+    cudaSetDevice(b->device);
+    const size_t n = b->sims.size();
+    for (size_t i = 0; i < n; ++i) init_stats(stats ? &stats[i] : nullptr);
+    std::vector<int> solve_batched;
+    std::vector<char> init_only(n, 0);
+    efl_status ret = EFL_OK;
+    auto fail = [&](efl_sim* s, efl_status st) { return batch_err(b, st, s->err); };
+    for (size_t i = 0; i < n; ++i) {
+        efl_sim* s = b->sims[i];
+        if (s->status == 0) {
+            efl_status st = run_init(s);
+            if (st != EFL_OK) return fail(s, st);
+            s->status = 1;
+            init_only[i] = 1;
+            if (stats) stats[i].initialized_only = 1;
+            continue;
+        }
+        s->U.dt = dt;
+        for (int stage = EFL_STAGE_UPDATE_SOLID; stage <= EFL_STAGE_DIVERGENCE; ++stage) {
+            efl_status st = run_stage(s, stage, stats ? &stats[i] : nullptr);
+            if (st != EFL_OK) return fail(s, st);
+        }
+        const efl_projection& P = s->cfg.projection;
+        const efl_projection& Q = b->sims[solve_batched.empty() ? i : solve_batched[0]]->cfg.projection;
+        const bool batchable = P.method == EFL_PROJECTION_GAUSS_SEIDEL && P.tolerance > 0.0f &&
+                               P.tolerance == Q.tolerance && P.max_iterations == Q.max_iterations &&
+                               P.check_interval == Q.check_interval;
+        if (batchable) {
+            const Level64& L = s->mg64[0];
+            k_widen<<<grid2d(s->nx, s->ny, kBlock), kBlock, count_launch(), s->stream>>>(s->p0, s->div, L.x, L.b);
+            solve_batched.push_back((int)i);
+        } else {
+            efl_status st = run_stage(s, EFL_STAGE_PROJECTION, stats ? &stats[i] : nullptr);
+            if (st == EFL_NOT_CONVERGED) ret = st;
+            else if (st != EFL_OK) return fail(s, st);
+        }
+    }
+    std::vector<efl_step_stats> local;
+    if (!stats) {
+        local.resize(n);
+        for (auto& x : local) init_stats(&x);
+    }
+    efl_step_stats* sp = stats ? stats : local.data();
+    efl_status st = batch_solve(b, solve_batched, sp);
+    if (st != EFL_OK) return st;
+    for (int idx : solve_batched) {
+        efl_sim* s = b->sims[idx];
+        k_narrow<<<grid2d(s->nx, s->ny, kBlock), kBlock, count_launch(), s->stream>>>(s->mg64[0].x, s->p0);
+        if (!sp[idx].converged) ret = EFL_NOT_CONVERGED;
+    }
+    for (size_t i = 0; i < n; ++i) {
+        efl_sim* s = b->sims[i];
+        if (init_only[i]) continue;
+        for (int stage = EFL_STAGE_SOLVE_VELOCITY; stage <= EFL_STAGE_SOLID_FORCES; ++stage) {
+            efl_status st2 = run_stage(s, stage, nullptr);
+            if (st2 != EFL_OK) return fail(s, st2);
+        }
+        s->n_forces = 0;
+    }
+    if (cudaGetLastError() != cudaSuccess) return batch_err(b, EFL_ERR_CUDA, "batch step launch failed");
+    return ret;
+}
+
+}  // extern "C"

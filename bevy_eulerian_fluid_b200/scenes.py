@@ -16,6 +16,13 @@ No public dataset is involved: every scene is generated from a seed.
                   multigrid V-cycles (2/2, coarsest 16^2) to 1e-5.
   pressure_microbench  all-fluid domain, walls only, N(0,1) divergence with
                   its mean removed (seed 0xC3).
+  batch_96        96 independent simulations (seed 0xC4), each sized
+                  uniformly from {128^2, 256x128, 256^2, 384x256, 512^2,
+                  768x512} (examples/multiple.rs steps several fluids side by
+                  side); a pool of depth U[0.2,0.5]*H, 1-4 circular droplets
+                  (r U[0.05,0.15]*min(W,H)) in the upper half, and every 30
+                  steps 8 local forces at random cells with magnitude
+                  U[0,50] m/s^2 in random directions; RBGS to 1e-5.
 """
 from __future__ import annotations
 
@@ -160,3 +167,71 @@ def microbench_inputs(n: int, seed: int = 0xC3):
     b -= b.mean(dtype=np.float64).astype(np.float32)
     phi = -np.ones((n, n), dtype=np.float32)
     return phi, b
+
+
+BATCH_SHAPES = [(128, 128), (256, 128), (256, 256), (384, 256), (512, 512), (768, 512)]
+
+
+@dataclass
+class BatchScene:
+    name: str
+    scenes: List[Scene]
+    seed: int
+    steps: int = 500
+    force_every: int = 30
+    forces_per_event: int = 8
+
+    @property
+    def cells(self) -> int:
+        return sum(sc.cells for sc in self.scenes)
+
+    def configs(self) -> List[capi.Config]:
+        return [_copy_cfg(sc.cfg) for sc in self.scenes]
+
+    def forces(self, i: int, step: int) -> List[capi.Force]:
+        """Local forces of simulation i before frame `step` (every force_every frames, none at frame 0)."""
+        if step == 0 or step % self.force_every:
+            return []
+        sc = self.scenes[i]
+        rng = np.random.default_rng([self.seed, i, step])
+        out = []
+        for _ in range(self.forces_per_event):
+            f = capi.Force()
+            mag = float(rng.uniform(0.0, 50.0))
+            ang = float(rng.uniform(0.0, 2.0 * math.pi))
+            f.force[0], f.force[1] = mag * math.cos(ang), mag * math.sin(ang)
+            f.position[0] = float(rng.integers(0, sc.cfg.nx))
+            f.position[1] = float(rng.integers(0, sc.cfg.ny))
+            out.append(f)
+        return out
+
+    def setup(self, sims) -> None:
+        """Uploads each scene's sources to the matching simulation handle."""
+        for sc, sim in zip(self.scenes, sims):
+            sim.set_sources(sc.oneshot, True)
+            sim.set_sources(sc.continuous, False)
+
+
+def batch(n: int = 96, steps: int = 500, tolerance: float = 1e-5, seed: int = 0xC4,
+          shapes: Optional[List[tuple]] = None) -> BatchScene:
+    """C4: n independent pools with droplets and periodic local forces, RBGS to tolerance."""
+    rng = np.random.default_rng(seed)
+    shapes = shapes or BATCH_SHAPES
+    scenes = []
+    for i in range(n):
+        nx, ny = shapes[int(rng.integers(0, len(shapes)))]
+        cfg = base_config(nx, ny)
+        cfg.projection.method = capi.PROJECTION_GAUSS_SEIDEL
+        cfg.projection.tolerance = tolerance
+        cfg.projection.max_iterations = 20000
+        cfg.projection.check_interval = 16
+        depth = float(rng.uniform(0.2, 0.5)) * ny
+        pool = aabb_source((0.0, -0.5 * ny + 0.5 * depth), (0.5 * nx, 0.5 * depth))
+        drops = []
+        for _ in range(int(rng.integers(1, 5))):
+            r = float(rng.uniform(0.05, 0.15)) * min(nx, ny)
+            cx = float(rng.uniform(-0.5 * nx + r, 0.5 * nx - r))
+            cy = float(rng.uniform(r, 0.5 * ny - r))
+            drops.append(circle_source((cx, cy), r))
+        scenes.append(Scene(f"batch_{i}_{nx}x{ny}", cfg, oneshot=[pool] + drops, steps=steps))
+    return BatchScene(f"batch_{n}", scenes, seed, steps=steps)

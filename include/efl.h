@@ -310,6 +310,26 @@ EFL_API efl_status efl_residual(efl_sim* sim, double* relative, double* norm_r, 
 /* Number of cells with levelset_air < 0 (calculate_volume.wgsl:11-75). */
 EFL_API efl_status efl_fluid_volume(efl_sim* sim, uint64_t* cells);
 
+/* ---- Batches of independent simulations ------------------------------ */
+
+/* N independent simulations of possibly different sizes stepped together
+ * (the reference steps each fluid entity with its own dispatches,
+ * render_node.rs:205-217; examples/multiple.rs spawns several).  The
+ * simulations share one CUDA stream.  Their tolerance-driven red-black
+ * pressure solves run as ONE cooperative launch over a packed list of
+ * (simulation, tile) items; each simulation's result and iteration count are
+ * those of its own efl_step.  Simulations whose projection is not the
+ * tolerance-driven Gauss-Seidel solve are projected one by one. */
+typedef struct efl_batch efl_batch;
+EFL_API efl_status efl_batch_create(const efl_config* configs, uint32_t n, efl_batch** out);
+EFL_API efl_status efl_batch_destroy(efl_batch* batch);
+EFL_API const char* efl_batch_last_error(const efl_batch* batch);
+/* The handle of simulation i, for the per-simulation calls (sources,
+ * obstacles, local forces, fields).  Owned by the batch: do not destroy it. */
+EFL_API efl_status efl_batch_sim(efl_batch* batch, uint32_t i, efl_sim** sim);
+/* One frame for every simulation (efl_step semantics); stats: n entries or NULL. */
+EFL_API efl_status efl_batch_step(efl_batch* batch, float dt, efl_step_stats* stats);
+
 /* ---- Diagnostics ------------------------------------------------------ */
 
 /* Kernels this library has launched since it was loaded (all handles). */
