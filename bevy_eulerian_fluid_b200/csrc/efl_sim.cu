@@ -1138,6 +1138,9 @@ struct efl_batch {
     BatchSim* d_sims = nullptr;
     int2* d_tiles = nullptr;
     double2* d_partials = nullptr;
+    int* d_n_active = nullptr;
+    int2* d_work = nullptr;
+    int* d_work_count = nullptr;
     BatchState* d_state = nullptr;
     BatchState* h_state = nullptr;  // pinned
     GridBarrier* d_barrier = nullptr;
@@ -1163,6 +1166,9 @@ void batch_free(efl_batch* b) {
     cudaFree(b->d_sims);
     cudaFree(b->d_tiles);
     cudaFree(b->d_partials);
+    cudaFree(b->d_n_active);
+    cudaFree(b->d_work);
+    cudaFree(b->d_work_count);
     cudaFree(b->d_state);
     cudaFree(b->d_barrier);
     if (b->h_state) cudaFreeHost(b->h_state);
@@ -1218,6 +1224,9 @@ efl_status batch_solve(efl_batch* b, const std::vector<int>& which, efl_step_sta
     Pm.max_iters = P0.max_iterations;
     Pm.check_interval = std::max<uint32_t>(1, P0.check_interval);
     Pm.partials = b->d_partials;
+    Pm.n_active = b->d_n_active;
+    Pm.work = b->d_work;
+    Pm.work_count = b->d_work_count;
     Pm.state = b->d_state;
     Pm.barrier = b->d_barrier;
     constexpr int EX = BT_TX + 4 * BT_K, EY = BT_TY + 4 * BT_K;
@@ -1229,6 +1238,10 @@ efl_status batch_solve(efl_batch* b, const std::vector<int>& which, efl_step_sta
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, BT_THREADS, smem) != cudaSuccess || per_sm < 1)
         return batch_err(b, EFL_ERR_CUDA, "batched solver: no co-resident CTA fits");
     const int grid = std::min(per_sm * sms, std::max(1, nt));
+    if (nt > BT_MAX_OWN * grid)
+        return batch_err(b, EFL_ERR_INVALID_ARGUMENT,
+                         "batch too large: " + std::to_string(nt) + " tiles of 64 x 32 cells, at most " +
+                             std::to_string(BT_MAX_OWN * grid) + " per cooperative launch");
     void* args[] = {&Pm};
     count_launch();
     cudaError_t e = cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(BT_THREADS), args, smem, st);
@@ -1293,6 +1306,9 @@ efl_status efl_batch_create(const efl_config* cfgs, uint32_t n, efl_batch** out)
     if (cudaMalloc(&b->d_sims, n * sizeof(BatchSim)) != cudaSuccess ||
         cudaMalloc(&b->d_tiles, total_tiles * sizeof(int2)) != cudaSuccess ||
         cudaMalloc(&b->d_partials, total_tiles * sizeof(double2)) != cudaSuccess ||
+        cudaMalloc(&b->d_n_active, sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&b->d_work, total_tiles * sizeof(int2)) != cudaSuccess ||
+        cudaMalloc(&b->d_work_count, sizeof(int)) != cudaSuccess ||
         cudaMalloc(&b->d_state, n * sizeof(BatchState)) != cudaSuccess ||
         cudaMalloc(&b->d_barrier, sizeof(GridBarrier)) != cudaSuccess ||
         cudaMallocHost(&b->h_state, n * sizeof(BatchState)) != cudaSuccess) {
