@@ -4,7 +4,8 @@ Workload (configs[1] of the reference benchmark list): coupled_512 -- a
 512x512 MAC grid, water in the lower 40 %, 24 rigid bodies drawn from seed
 0xC2 (6 circles, rectangles, capsules, triangles), jump-flooding level-set
 reinitialisation every step, and a pressure solve that iterates red-black
-Gauss-Seidel (SOR 1.9) on an FP64 iterate until ||b - A p|| / ||b|| <= 1e-5.
+Gauss-Seidel (SOR 1.9) until ||b - A p|| / ||b|| <= 1e-5 (FP64 iterate and
+residual, f32 sweeps on the correction: mixed-precision refinement).
 
 metric: cell-steps/s to 1e-5 relative residual = cells x steps / time.
   value  -- device-resident state, obstacles fixed, CUDA events on the
@@ -12,18 +13,25 @@ metric: cell-steps/s to 1e-5 relative residual = cells x steps / time.
             write) between steps and excluded from the time.
   e2e    -- the same steps through the plugin API with the two-way
             coupling loop: H2D upload of the 24 packed obstacles, the step,
-            D2H read-back of the force bins, host rigid integration.
-  roofline -- the sweep kernel alone (efl_pressure_sweeps, 64-bit iterate)
-            at the workload's state, 32 algorithmic bytes per cell per
-            red-black iteration (p read+write 8, div 4, phi 4, area
-            fractions 16), against the measured HBM copy bandwidth.
+            D2H read-back of the solid forces, host rigid integration.
+  roofline -- the dominant kernel, k_gsmix_persistent (one cooperative
+            launch = one whole tolerance-driven solve), re-run from the same
+            pre-projection state: 32 algorithmic bytes per cell per red-black
+            iteration (p read+write 8, div 4, phi 4, area fractions 16) x
+            cells x iterations / the launch's device time, against the
+            measured HBM copy bandwidth.
+  batch  -- the C4 batch (96 simulations of uneven sizes, seed 0xC4): the
+            batched path (efl_batch_step, one cooperative solve for all
+            simulations) next to the plain path (efl_step per simulation),
+            with the pressure-solve milliseconds of each.
   microbench -- f32 reference sweeps on the 4096^2 all-fluid pressure
             microbench (N(0,1) divergence, mean removed).
   cpu_baseline -- the CPU oracle (a C++ port of the reference's kernels)
             on the host cores, one full step of the same scene.
 
-Multi-GPU (torchrun): one independent replica per rank (a single fluid
-domain does not shard here), weak scaling, max-over-ranks device time.
+Multi-GPU (torchrun): the coupled scene runs as one independent replica per
+rank (weak scaling); the C4 batch is split across ranks (simulation i on
+rank i % N).  Device times are the max over ranks.
 """
 from __future__ import annotations
 
@@ -54,7 +62,9 @@ def parse():
     ap.add_argument("--size", type=int, default=512)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-microbench", action="store_true")
-    ap.add_argument("--only", choices=["coupled", "microbench"], default=None,
+    ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--batch-sims", type=int, default=96, help="simulations of the C4 batch (96 in the benchmark)")
+    ap.add_argument("--only", choices=["coupled", "microbench", "batch"], default=None,
                     help="profiling aid: run one part only and print its numbers")
     return ap.parse_args()
 
@@ -76,8 +86,9 @@ def measured_peaks():
 
 
 def profile_traffic():
-    """Per-launch DRAM bytes of the sweep kernel from the committed ncu summary, if any."""
-    p = os.path.join(REPO, "profiles", "gs_sweep_f64_coupled_512.txt")
+    """DRAM bytes per red-black iteration of the persistent mixed solve, from the
+    committed ncu summary of that kernel on coupled_512 (None if absent)."""
+    p = os.path.join(REPO, "profiles", "k_gsmix_persistent_coupled_512.txt")
     if not os.path.exists(p):
         return None
     for line in open(p):
@@ -209,6 +220,19 @@ def main():
     if args.only == "microbench":
         print(json.dumps(microbench(capi.load(), None, torch, measured_peaks()[0])), flush=True)
         return 0
+    if args.only == "batch":
+        dist = None
+        if world > 1:
+            import datetime
+            import torch.distributed as dist
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        out = batch_leg(capi.load(), torch, args, world, rank, local, dist)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        if rank == 0:
+            print(json.dumps(out), flush=True)
+        return 0
     dist = None
     if world > 1:
         import datetime
@@ -278,28 +302,40 @@ def main():
     h2d = len(bodies) * 176
     d2h = capi.MAX_SOLIDS * 16
 
-    # ---- roofline of the sweep kernel (FP64 iterate) at this state
-    n_sw = 400
-    sim.pressure_sweeps(64, 20)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    e0.record(stream)
-    sim.pressure_sweeps(64, n_sw)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    it_ms = e0.elapsed_time(e1) / n_sw
+    # ---- roofline of the dominant kernel: the persistent mixed-precision solve,
+    # re-run three times from the same pre-projection state.
+    for stage in range(capi.STAGE_UPDATE_SOLID, capi.STAGE_DIVERGENCE + 1):
+        sim.run_stage(stage, sc.dt)
+    p_in = sim.get(capi.FIELD_PRESSURE)
+    solve = []
+    for _ in range(3):
+        sim.set(capi.FIELD_PRESSURE, p_in)
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        st = sim.run_stage(capi.STAGE_PROJECTION, sc.dt)
+        solve.append((sim.projection_ms(), int(st.pressure_iterations)))
+    solve_ms = statistics.median(x[0] for x in solve)
+    solve_it = solve[0][1]
+    it_ms = solve_ms / max(1, solve_it)
     peak, peak_kind = measured_peaks()
-    achieved = ALGO_BYTES_PER_CELL_ITER * sc.cells / (it_ms / 1e3) / 1e9
-    traffic = profile_traffic()
+    achieved = ALGO_BYTES_PER_CELL_ITER * sc.cells * solve_it / (solve_ms / 1e3) / 1e9
+    per_it = profile_traffic()
+    traffic = per_it * solve_it if per_it is not None else None
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": traffic,
-                "kernel": "k_gs_color<double> red+black (one RB iteration)",
+                "kernel": "k_gsmix_persistent (one launch = one tolerance-driven solve)",
+                "launch_ms": round(solve_ms, 3), "iterations_per_launch": solve_it,
                 "iteration_us": round(it_ms * 1e3, 3), "peak_kind": peak_kind,
-                "note": f"32 B/cell/RB-iteration x {sc.cells} cells; working set is L2-resident at this size"}
+                "note": f"32 B/cell/RB-iteration x {sc.cells} cells x {solve_it} iterations per launch; "
+                        "the launch keeps its tiles in shared memory, so DRAM traffic (ncu) is far "
+                        "below the algorithmic bytes"}
 
     micro = None
     if not args.no_microbench and rank == 0 and args.only is None:
         micro = microbench(api, stream, torch, peak)
+    batch = None
+    if not args.no_batch and args.only is None:
+        batch = batch_leg(api, torch, args, world, rank, local, dist)
 
     sim.close()
     if dist:
@@ -326,8 +362,122 @@ def main():
     }
     if micro:
         line["microbench"] = micro
+    if batch:
+        line["batch"] = batch
     print(json.dumps(line), flush=True)
     return 0
+
+
+def batch_shard(n_sims: int, world: int, rank: int):
+    """Simulations of the C4 batch that rank `rank` steps: i % world == rank."""
+    return list(range(rank, n_sims, world))
+
+
+def batch_leg(api, torch, args, world, rank, local, dist):
+    """C4: the batched path and the plain path over this rank's shard of the
+    96-simulation batch; value = all ranks' cells x steps / max-over-ranks time."""
+    from bevy_eulerian_fluid_b200 import _capi as capi
+    from bevy_eulerian_fluid_b200 import scenes
+    bs = scenes.batch(args.batch_sims)
+    shard = batch_shard(len(bs.scenes), world, rank)
+    cfgs = bs.configs()
+    for c in cfgs:
+        c.device = local
+    steps = max(1, min(args.steps, 20))
+    dt = scenes.DT
+
+    def forces(sims, k):
+        for j, i in enumerate(shard):
+            f = bs.forces(i, k)
+            if f:
+                sims[j].set_local_forces(f)
+
+    # batched
+    bt = capi.Batch(api, [cfgs[i] for i in shard])
+    for j, i in enumerate(shard):
+        bt[j].set_sources(bs.scenes[i].oneshot, True)
+    bstream = torch.cuda.ExternalStream(bt[0].stream(), device=f"cuda:{local}")
+    bt.step(dt)
+    k = 0
+    for _ in range(args.warmup):
+        k += 1
+        forces(bt.sims, k)
+        bt.step(dt)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    solve_b, iters = [], []
+    launches0 = api.kernel_launches()
+    e0.record(bstream)
+    for _ in range(steps):
+        k += 1
+        forces(bt.sims, k)
+        st = bt.step(dt)
+        solve_b.append(bt.projection_ms())
+        iters.extend(int(x.pressure_iterations) for x in st)
+    e1.record(bstream)
+    torch.cuda.synchronize()
+    launches_b = api.kernel_launches() - launches0
+    ms_b = e0.elapsed_time(e1)
+    bt.close()
+
+    # plain: efl_step per simulation, device time summed over the simulations' streams
+    sims = []
+    for i in shard:
+        sc = bs.scenes[i]
+        sc.cfg.device = local
+        sims.append(sc.make(api))
+    for s_ in sims:
+        s_.step(dt)
+    k = 0
+    for _ in range(args.warmup):
+        k += 1
+        forces(sims, k)
+        for s_ in sims:
+            s_.step(dt)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    streams = [torch.cuda.ExternalStream(s_.stream(), device=f"cuda:{local}") for s_ in sims]
+    ev = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in sims]
+          for _ in range(steps)]
+    solve_p = []
+    for t in range(steps):
+        k += 1
+        forces(sims, k)
+        tot = 0.0
+        for j, s_ in enumerate(sims):
+            ev[t][j][0].record(streams[j])
+            s_.step(dt)
+            ev[t][j][1].record(streams[j])
+            tot += s_.projection_ms()
+        solve_p.append(tot)
+    torch.cuda.synchronize()
+    ms_p = sum(a.elapsed_time(b) for row in ev for a, b in row)
+    for s_ in sims:
+        s_.close()
+
+    cells_rank = sum(bs.scenes[i].cells for i in shard)
+    t = [ms_b, ms_p, sum(solve_b), sum(solve_p)]
+    if dist:
+        tt = torch.tensor(t, device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t = [float(x) for x in tt.tolist()]
+        dist.barrier()
+    cells = bs.cells
+    return {"workload": f"batch_{len(bs.scenes)}: {len(bs.scenes)} simulations, sizes from {128^2, 256x128, 256^2, 384x256, 512^2, 768x512}, "
+                        "pools with droplets, 8 local forces every 30 steps, seed 0xC4, RBGS to 1e-5",
+            "cells": cells, "cells_this_rank": cells_rank, "steps": steps, "warmup": args.warmup,
+            "value": cells * steps / (t[0] / 1e3), "plain_value": cells * steps / (t[1] / 1e3),
+            "unit": "cell-steps/s", "speedup_vs_plain": round(t[1] / t[0], 3),
+            "ms_per_step": {"batched": t[0] / steps, "plain": t[1] / steps},
+            "pressure_solve_ms_per_step": {"batched": t[2] / steps, "plain": t[3] / steps},
+            "pressure_iterations": {"max": max(iters), "mean": round(sum(iters) / len(iters), 1)},
+            "kernel": "k_batch_mix<64,32,2> (one cooperative launch per step for all simulations)",
+            "gpu_launches_batched": int(launches_b),
+            "l2": "not flushed: the batch's working set (GBs) exceeds L2",
+            "sharding": f"simulation i on rank i % {world}"}
 
 
 def microbench(api, stream, torch, peak):

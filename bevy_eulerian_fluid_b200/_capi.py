@@ -132,11 +132,13 @@ SIGNATURES = {
     "batch_last_error": (C.c_char_p, [C.c_void_p]),
     "batch_sim": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(C.c_void_p)]),
     "batch_step": (C.c_int, [C.c_void_p, C.c_float, C.POINTER(StepStats)]),
+    "batch_projection_ms": (C.c_int, [C.c_void_p, C.POINTER(C.c_float)]),
+    "projection_ms": (C.c_int, ["X", C.POINTER(C.c_float)]),
 }
 # Functions of efl.h that the oracle restatement does not mirror.
 PRODUCT_ONLY = {"abi_version", "default_config", "field_device_ptr", "stream", "synchronize", "kernel_launches",
                 "pressure_sweeps", "residual_norms_noalloc", "batch_create", "batch_destroy", "batch_last_error",
-                "batch_sim", "batch_step"}
+                "batch_sim", "batch_step", "batch_projection_ms", "projection_ms"}
 
 
 class EflError(RuntimeError):
@@ -348,6 +350,12 @@ class Sim:
         self._check(self.api.field_device_ptr(self.h, field, C.byref(p), C.byref(pitch)))
         return p.value, pitch.value
 
+    def projection_ms(self) -> float:
+        """Device time of the last projection stage (ms)."""
+        ms = C.c_float()
+        self._check(self.api.projection_ms(self.h, C.byref(ms)))
+        return ms.value
+
     def pressure_sweeps(self, precision: int, iterations: int):
         self._check(self.api.pressure_sweeps(self.h, precision, iterations))
 
@@ -388,6 +396,12 @@ class Batch:
         allow = (OK, NOT_CONVERGED) if allow_not_converged else (OK,)
         self._check(self.api.batch_step(self.h, dt, stats), allow)
         return list(stats)
+
+    def projection_ms(self) -> float:
+        """Device time of the last batched pressure solve (ms)."""
+        ms = C.c_float()
+        self._check(self.api.batch_projection_ms(self.h, C.byref(ms)))
+        return ms.value
 
     def close(self):
         if getattr(self, "h", None):

@@ -87,6 +87,8 @@ struct efl_sim {
     PF mix_d2{};       // second correction buffer (batched solve)
     bool owns_stream = true;
     int* h_err = nullptr;  // pinned copy of the TMA sweep's error flag
+    cudaEvent_t ev_proj[2] = {nullptr, nullptr};  // around the last projection stage
+    bool proj_timed = false;
 
     Dom dom() const { return Dom{nx, ny}; }
 };
@@ -567,7 +569,17 @@ efl_status run_stage(efl_sim* s, int stage, efl_step_stats* st) {
         case EFL_STAGE_ADVECT_VELOCITY: return st_advect(s);
         case EFL_STAGE_APPLY_FORCES: return st_apply_forces(s);
         case EFL_STAGE_DIVERGENCE: return st_divergence(s);
-        case EFL_STAGE_PROJECTION: return st_projection(s, st);
+        case EFL_STAGE_PROJECTION: {
+            if (!s->ev_proj[0]) {
+                CU(cudaEventCreate(&s->ev_proj[0]));
+                CU(cudaEventCreate(&s->ev_proj[1]));
+            }
+            CU(cudaEventRecord(s->ev_proj[0], s->stream));
+            const efl_status r = st_projection(s, st);
+            CU(cudaEventRecord(s->ev_proj[1], s->stream));
+            s->proj_timed = true;
+            return r;
+        }
         case EFL_STAGE_SOLVE_VELOCITY: return st_solve_velocity(s);
         case EFL_STAGE_EXTRAPOLATE: return st_extrapolate(s);
         case EFL_STAGE_ADVECT_LEVELSET: return st_advect_levelset(s);
@@ -767,6 +779,8 @@ efl_status efl_destroy(efl_sim* s) {
     for (auto& b : s->bufs) cudaFree(b.p);
     if (s->d_forces) cudaFree(s->d_forces);
     if (s->h_norms) cudaFreeHost(s->h_norms);
+    for (cudaEvent_t e : s->ev_proj)
+        if (e) cudaEventDestroy(e);
     if (s->stream && s->owns_stream) cudaStreamDestroy(s->stream);
     delete s;
     return EFL_OK;
@@ -861,6 +875,14 @@ efl_status efl_step(efl_sim* s, float dt, efl_step_stats* st) {
     }
     s->n_forces = 0;  // apply_forces.rs:166 clears the forces after upload
     return ret;
+}
+
+efl_status efl_projection_ms(efl_sim* s, float* ms) {
+    if (!s || !ms) return set_err(s, EFL_ERR_INVALID_ARGUMENT, "null argument");
+    if (!s->proj_timed) return set_err(s, EFL_ERR_STATE, "no projection has run yet");
+    CU(cudaEventSynchronize(s->ev_proj[1]));
+    CU(cudaEventElapsedTime(ms, s->ev_proj[0], s->ev_proj[1]));
+    return EFL_OK;
 }
 
 efl_status efl_run_stage(efl_sim* s, int32_t stage, float dt, efl_step_stats* st) {
@@ -1146,6 +1168,8 @@ struct efl_batch {
     GridBarrier* d_barrier = nullptr;
     int ntiles = 0;
     std::vector<int> tile_start;
+    cudaEvent_t ev[2] = {nullptr, nullptr};  // around the last batched solve
+    bool timed = false;
 };
 
 namespace {
@@ -1172,6 +1196,8 @@ void batch_free(efl_batch* b) {
     cudaFree(b->d_state);
     cudaFree(b->d_barrier);
     if (b->h_state) cudaFreeHost(b->h_state);
+    for (cudaEvent_t e : b->ev)
+        if (e) cudaEventDestroy(e);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
 }
@@ -1244,7 +1270,12 @@ efl_status batch_solve(efl_batch* b, const std::vector<int>& which, efl_step_sta
                              std::to_string(BT_MAX_OWN * grid) + " per cooperative launch");
     void* args[] = {&Pm};
     count_launch();
+    if (!b->ev[0] && (cudaEventCreate(&b->ev[0]) != cudaSuccess || cudaEventCreate(&b->ev[1]) != cudaSuccess))
+        return batch_err(b, EFL_ERR_CUDA, "event creation failed");
+    cudaEventRecord(b->ev[0], st);
     cudaError_t e = cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(BT_THREADS), args, smem, st);
+    cudaEventRecord(b->ev[1], st);
+    b->timed = true;
     if (e != cudaSuccess)
         return batch_err(b, EFL_ERR_CUDA, std::string("batched solver launch failed: ") + cudaGetErrorString(e));
     GridBarrier hb{};
@@ -1329,6 +1360,14 @@ const char* efl_batch_last_error(const efl_batch* b) { return b ? b->err.c_str()
 efl_status efl_batch_sim(efl_batch* b, uint32_t i, efl_sim** sim) {
     if (!b || !sim || i >= b->sims.size()) return batch_err(b, EFL_ERR_INVALID_ARGUMENT, "bad batch index");
     *sim = b->sims[i];
+    return EFL_OK;
+}
+
+efl_status efl_batch_projection_ms(efl_batch* b, float* ms) {
+    if (!b || !ms) return batch_err(b, EFL_ERR_INVALID_ARGUMENT, "null argument");
+    if (!b->timed) return batch_err(b, EFL_ERR_STATE, "no batched solve has run yet");
+    if (cudaEventSynchronize(b->ev[1]) != cudaSuccess || cudaEventElapsedTime(ms, b->ev[0], b->ev[1]) != cudaSuccess)
+        return batch_err(b, EFL_ERR_CUDA, "event timing failed");
     return EFL_OK;
 }
 

@@ -306,6 +306,10 @@ EFL_API efl_status efl_synchronize(efl_sim* sim);
 /* Relative residual ||b - A p||_2 / ||b||_2 of the current pressure against
  * the current divergence (operator of residual.wgsl:33-54), FP64 norms. */
 EFL_API efl_status efl_residual(efl_sim* sim, double* relative, double* norm_r, double* norm_b);
+/* Device time of the last projection stage (efl_step or efl_run_stage), in
+ * milliseconds; waits for it to finish.  No reference counterpart (the
+ * reference has no per-stage timing). */
+EFL_API efl_status efl_projection_ms(efl_sim* sim, float* ms);
 
 /* Number of cells with levelset_air < 0 (calculate_volume.wgsl:11-75). */
 EFL_API efl_status efl_fluid_volume(efl_sim* sim, uint64_t* cells);
@@ -329,6 +333,9 @@ EFL_API const char* efl_batch_last_error(const efl_batch* batch);
 EFL_API efl_status efl_batch_sim(efl_batch* batch, uint32_t i, efl_sim** sim);
 /* One frame for every simulation (efl_step semantics); stats: n entries or NULL. */
 EFL_API efl_status efl_batch_step(efl_batch* batch, float dt, efl_step_stats* stats);
+/* Device time of the last batched pressure solve (the cooperative launch), in
+ * milliseconds; waits for it to finish. */
+EFL_API efl_status efl_batch_projection_ms(efl_batch* batch, float* ms);
 
 /* ---- Diagnostics ------------------------------------------------------ */
 
