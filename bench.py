@@ -466,7 +466,8 @@ def batch_leg(api, torch, args, world, rank, local, dist):
         t = [float(x) for x in tt.tolist()]
         dist.barrier()
     cells = bs.cells
-    return {"workload": f"batch_{len(bs.scenes)}: {len(bs.scenes)} simulations, sizes from {128^2, 256x128, 256^2, 384x256, 512^2, 768x512}, "
+    return {"workload": f"batch_{len(bs.scenes)}: {len(bs.scenes)} simulations, sizes from "
+                        "{128^2, 256x128, 256^2, 384x256, 512^2, 768x512}, "
                         "pools with droplets, 8 local forces every 30 steps, seed 0xC4, RBGS to 1e-5",
             "cells": cells, "cells_this_rank": cells_rank, "steps": steps, "warmup": args.warmup,
             "value": cells * steps / (t[0] / 1e3), "plain_value": cells * steps / (t[1] / 1e3),
