@@ -105,3 +105,35 @@ def test_default_config_matches_reference_defaults():
     assert (c.nx, c.ny, c.length_unit, c.rho) == (256, 128, 1.0, 1.0)
     assert tuple(c.gravity) == pytest.approx((0.0, 9.8))
     assert list(c.transform) == [1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1]
+
+
+def test_batch_scene_matches_c4_spec():
+    from bevy_eulerian_fluid_b200 import _capi as capi
+    from bevy_eulerian_fluid_b200 import scenes
+    b = scenes.batch(96)
+    again = scenes.batch(96)
+    assert [(s.cfg.nx, s.cfg.ny) for s in b.scenes] == [(s.cfg.nx, s.cfg.ny) for s in again.scenes]
+    shapes = {(s.cfg.nx, s.cfg.ny) for s in b.scenes}
+    assert shapes <= set(scenes.BATCH_SHAPES) and len(shapes) == 6
+    for s in b.scenes:
+        nx, ny = s.cfg.nx, s.cfg.ny
+        pool, drops = s.oneshot[0], s.oneshot[1:]
+        depth = 2 * pool.data[1]
+        assert 0.2 * ny <= depth <= 0.5 * ny
+        assert pool.shape == capi.SOURCE_AABB and abs(pool.center[1] - (-0.5 * ny + 0.5 * depth)) < 1e-3
+        assert 1 <= len(drops) <= 4
+        for d in drops:
+            r = d.data[0]
+            assert d.shape == capi.SOURCE_CIRCLE
+            assert 0.05 * min(nx, ny) <= r <= 0.15 * min(nx, ny)
+            assert d.center[1] >= r - 1e-3  # upper half
+        assert s.cfg.projection.tolerance == pytest.approx(1e-5)
+        assert s.cfg.projection.method == capi.PROJECTION_GAUSS_SEIDEL
+    assert b.forces(3, 0) == [] and b.forces(3, 29) == []
+    f = b.forces(3, 30)
+    assert len(f) == 8
+    for x in f:
+        assert (x.force[0] ** 2 + x.force[1] ** 2) ** 0.5 <= 50.0 + 1e-4
+        assert 0 <= x.position[0] < b.scenes[3].cfg.nx and 0 <= x.position[1] < b.scenes[3].cfg.ny
+    g = scenes.batch(96).forces(3, 30)
+    assert [(x.force[0], x.position[0]) for x in f] == [(x.force[0], x.position[0]) for x in g]
