@@ -481,24 +481,13 @@ efl_status st_projection(efl_sim* s, efl_step_stats* st) {
             r = res.r1;
             done = true;
         }
-        if (!done) {
+        if (!done) {  // multigrid: FP64 V-cycles with a host-side residual test
             TRY(relative_residual(s, L, &r));
             r0 = r;
-            if (P.method == EFL_PROJECTION_GAUSS_SEIDEL) {
-                uint32_t chk = std::max<uint32_t>(1, P.check_interval);
-                while (!(r <= (double)P.tolerance) && iters < P.max_iterations) {
-                    uint32_t n = std::min(chk, P.max_iterations - iters);
-                    TRY(solve_gs_fixed(s->solver, L, s->U, P.sor_weight, n, s->stream));
-                    LAUNCH_CHECK();
-                    iters += n;
-                    TRY(relative_residual(s, L, &r));
-                }
-            } else {
-                while (!(r <= (double)P.tolerance) && iters < P.max_iterations) {
-                    TRY(v_cycle(s, s->mg64, 0));
-                    ++iters;
-                    TRY(relative_residual(s, L, &r));
-                }
+            while (!(r <= (double)P.tolerance) && iters < P.max_iterations) {
+                TRY(v_cycle(s, s->mg64, 0));
+                ++iters;
+                TRY(relative_residual(s, L, &r));
             }
         }
         r1 = r;

@@ -1,20 +1,24 @@
 // efl_solver.cuh — red-black Gauss-Seidel pressure solves
 // (projection/shaders/gauss_seidel.wgsl:12-88, host loop gauss_seidel.rs:142-147).
 //
-// Two forms:
+// Forms:
 //  * solve_gs_fixed: n red-black iterations as one launch per colour
 //    (k_gs_color), f32 (the reference's fixed-count mode) or f64.
-//  * solve_gs64_persistent: the tolerance-driven FP64 solve as ONE
-//    cooperative launch.  Each CTA owns a tile of the grid and keeps the
-//    tile plus a halo of 2k cells in shared memory -- the iterate, the
-//    right-hand side, the per-cell diagonal and its reciprocal, the face
-//    fractions and the fluid flags -- so that k red-black iterations run
-//    from shared memory between two halo exchanges (temporal blocking; the
-//    result is identical to k global sweeps because a half-sweep only reads
-//    the other colour).  Halos are exchanged through L2 behind a grid
-//    barrier whose spin is bounded; the relative residual is reduced and
-//    tested on the device every check_interval iterations, so the whole
-//    solve needs no host round trip.
+//  * solve_gsmix_persistent: the tolerance-driven solve (mixed-precision
+//    iterative refinement, below) as ONE cooperative launch.  Each CTA owns a
+//    tile of the grid and keeps the tile plus a halo of 2k cells in shared
+//    memory -- FP64 iterate, right-hand side and diagonal, f32 correction,
+//    coefficients and residual, the cell modes -- so that k red-black
+//    iterations run from shared memory between two halo exchanges (temporal
+//    blocking; the result is identical to k global sweeps because a
+//    half-sweep only reads the other colour).  Halos are exchanged through
+//    L2 behind a grid barrier whose spin is bounded; the relative residual is
+//    reduced and tested on the device every check_interval iterations, so the
+//    whole solve needs no host round trip.
+//  * solve_gsmix_global: the same solve with global-memory kernels and a host
+//    loop, for grids the persistent scheme does not cover.
+//  * solve_gs32_tiled: fixed-count f32 sweeps through shared-memory tiles
+//    (used when the TMA sweep of efl_sweep_tma.cuh is unavailable).
 #pragma once
 
 #include <algorithm>
@@ -105,121 +109,11 @@ struct PersistentParams {
     SolveResult* result;
 };
 
-// Shared-memory image of one extended tile (EX x EY cells, EX even), stored
-// per colour in checkerboard-compressed form: cell (lx, ly) of colour
-// c = (gx + gy) & 1 lives at [c][ly][lx >> 1].  A cell's left / right
-// neighbours are the other colour's entries (lx >> 1) - 1 + (lx & 1) and
-// (lx >> 1) + (lx & 1) of the same row, up / down are entry lx >> 1 of the
-// rows above and below, so a warp reads consecutive doubles.
-template <int EX, int EY>
-struct PsTile {
-    static constexpr int W2 = EX / 2;
-    static constexpr int N2 = W2 * EY;  // entries per colour
-    double p[2][N2];
-    double b[2][N2];
-    double inv[2][N2];   // 1/denom, 0 where the cell does not update
-    double den[2][N2];   // denom (residual)
-    float4 w[2][N2];     // neighbour weights (-x, +x, -y, +y): face fraction, or 0 for air / outside
-    unsigned char mode[2][N2];  // MODE_*
-};
 constexpr unsigned char MODE_SKIP = 0;     // outside the domain or on the tile's outer ring
 constexpr unsigned char MODE_ZERO = 1;     // air, fully solid or |denom| < 1e-6: p = 0
 constexpr unsigned char MODE_UPDATE = 2;   // regular update
 constexpr unsigned char MODE_COUNTED = 4;  // counted in the residual norms
 
-template <int EX, int EY>
-EFL_DEV void ps_half_sweep(PsTile<EX, EY>& T, int base, int c, int h, double cdiv, double w, double omw) {
-    // Half-sweep h of a round: after it only rings > h of the tile hold
-    // correct values, so cells of rings <= h are left alone.
-    constexpr int W2 = EX / 2;
-    const int o = 1 - c;
-    const int rows = EY - 2 - 2 * h;
-    const int total = rows * W2;
-    for (int i = threadIdx.x; i < total; i += PS_THREADS) {
-        const int ly = 1 + h + i / W2;
-        const int j = i - (ly - 1 - h) * W2;
-        const int odd = (base + ly + c) & 1;  // lx & 1 of a colour-c cell in row ly
-        const int lx = 2 * j + odd;
-        if (lx < 1 + h || lx > EX - 2 - h) continue;
-        const int k = ly * W2 + j;
-        const unsigned char m = T.mode[c][k];
-        if (m & MODE_UPDATE) {
-            const float4 wk = T.w[c][k];
-            double nume = cdiv * T.b[c][k];
-            nume = nume + (double)wk.x * T.p[o][k - 1 + odd];
-            nume = nume + (double)wk.y * T.p[o][k + odd];
-            nume = nume + (double)wk.z * T.p[o][k - W2];
-            nume = nume + (double)wk.w * T.p[o][k + W2];
-            T.p[c][k] = w * (nume * T.inv[c][k]) + omw * T.p[c][k];
-        } else if (m & MODE_ZERO) {
-            T.p[c][k] = 0.0;
-        }
-    }
-}
-
-// ||r||^2 and ||b||^2 over the owned cells (all halo values valid),
-// r = b - factor * (denom * p - sum w_k p_k).
-template <int EX, int EY>
-EFL_DEV double2 ps_residual_partial(const PsTile<EX, EY>& T, int base, int H, int tx, int ty, double factor) {
-    constexpr int W2 = EX / 2;
-    double ar = 0.0, ab = 0.0;
-    for (int i = threadIdx.x; i < tx * ty; i += PS_THREADS) {
-        const int ly = H + i / tx, lx = H + i % tx;
-        const int c = (base + lx + ly) & 1, o = 1 - c, odd = lx & 1;
-        const int k = ly * W2 + (lx >> 1);
-        if (!(T.mode[c][k] & MODE_COUNTED)) continue;
-        const float4 wk = T.w[c][k];
-        double sum = (double)wk.x * T.p[o][k - 1 + odd];
-        sum = sum + (double)wk.y * T.p[o][k + odd];
-        sum = sum + (double)wk.z * T.p[o][k - W2];
-        sum = sum + (double)wk.w * T.p[o][k + W2];
-        const double bb = T.b[c][k];
-        const double r = bb - factor * (T.den[c][k] * T.p[c][k] - sum);
-        ar += r * r;
-        ab += bb * bb;
-    }
-    ar = warp_sum(ar);
-    ab = warp_sum(ab);
-    __shared__ double red_r[PS_THREADS / 32], red_b[PS_THREADS / 32];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    if (lane == 0) {
-        red_r[wid] = ar;
-        red_b[wid] = ab;
-    }
-    __syncthreads();
-    double2 out = make_double2(0.0, 0.0);
-    if (threadIdx.x == 0) {
-        for (int k = 0; k < PS_THREADS / 32; ++k) {
-            out.x += red_r[k];
-            out.y += red_b[k];
-        }
-    }
-    __syncthreads();
-    return out;
-}
-
-template <int EX, int EY>
-EFL_DEV void ps_load_p(PsTile<EX, EY>& T, const Level64& L, int gx0, int gy0, int base, int H, int tx, int ty,
-                       bool halo_only) {
-    for (int i = threadIdx.x; i < EX * EY; i += PS_THREADS) {
-        const int ly = i / EX, lx = i - ly * EX;
-        if (halo_only && lx >= H && lx < H + tx && ly >= H && ly < H + ty) continue;  // owned: already current
-        const int gx = gx0 + lx, gy = gy0 + ly;
-        const int c = (base + lx + ly) & 1;
-        const bool in = (unsigned)gx < (unsigned)L.nx && (unsigned)gy < (unsigned)L.ny;
-        T.p[c][ly * (EX / 2) + (lx >> 1)] = in ? __ldcg(&L.x.p[(size_t)gy * L.x.P + gx]) : 0.0;
-    }
-}
-template <int EX, int EY>
-EFL_DEV void ps_store_owned(const PsTile<EX, EY>& T, const Level64& L, int gx0, int gy0, int base, int H, int tx,
-                            int ty) {
-    for (int i = threadIdx.x; i < tx * ty; i += PS_THREADS) {
-        const int ly = H + i / tx, lx = H + i % tx;
-        const int gx = gx0 + lx, gy = gy0 + ly;
-        if ((unsigned)gx < (unsigned)L.nx && (unsigned)gy < (unsigned)L.ny)
-            __stcg(&L.x.p[(size_t)gy * L.x.P + gx], T.p[(base + lx + ly) & 1][ly * (EX / 2) + (lx >> 1)]);
-    }
-}
 // Sum of all CTAs' partials in CTA order; identical in every CTA.
 EFL_DEV double ps_total_relative(const double2* partials, int nblocks) {
     __shared__ double s_rel;
@@ -236,112 +130,6 @@ EFL_DEV double ps_total_relative(const double2* partials, int nblocks) {
     double v = s_rel;
     __syncthreads();
     return v;
-}
-
-template <int EX, int EY, int KMAX>
-__global__ void __launch_bounds__(PS_THREADS, 1) k_gs64_persistent(PersistentParams P) {
-    extern __shared__ __align__(16) unsigned char ps_raw[];
-    PsTile<EX, EY>& T = *reinterpret_cast<PsTile<EX, EY>*>(ps_raw);
-    constexpr int H = 2 * KMAX;
-    constexpr int W2 = EX / 2;
-    const int tx = EX - 2 * H, ty = EY - 2 * H;
-    const Level64& L = P.L;
-    const int tile = blockIdx.x;
-    const int gx0 = (tile % P.tiles_x) * tx - H, gy0 = (tile / P.tiles_x) * ty - H;
-    const int base = (gx0 + gy0) & 1;
-    const unsigned nblocks = gridDim.x;
-
-    // Per-solve coefficients (gauss_seidel.wgsl:44-80 and residual.wgsl:21-54
-    // in the reference's neighbour order).
-    for (int i = threadIdx.x; i < EX * EY; i += PS_THREADS) {
-        const int ly = i / EX, lx = i - ly * EX;
-        const int gx = gx0 + lx, gy = gy0 + ly;
-        const int c = (base + lx + ly) & 1, k = ly * W2 + (lx >> 1);
-        unsigned char m = MODE_SKIP;
-        double den = 0.0, inv = 0.0, bb = 0.0;
-        float4 wk = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        if ((unsigned)gx < (unsigned)L.nx && (unsigned)gy < (unsigned)L.ny) {
-            const bool ring = lx == 0 || ly == 0 || lx == EX - 1 || ly == EY - 1;
-            const float phi = L.ls.at(gx, gy);
-            bb = L.b.at(gx, gy);
-            bool update = false;
-            if (phi < 0.0f) {
-                const float f[4] = {L.fu.at(gx, gy), L.fu.at(gx + 1, gy), L.fv.at(gx, gy), L.fv.at(gx, gy + 1)};
-                if (!(f[0] == 0.0f && f[1] == 0.0f && f[2] == 0.0f && f[3] == 0.0f)) {
-                    m |= MODE_COUNTED;
-                    const int ox[4] = {-1, 1, 0, 0}, oy[4] = {0, 0, -1, 1};
-                    float wv[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        const int jx = gx + ox[q], jy = gy + oy[q];
-                        if ((unsigned)jx < (unsigned)L.nx && (unsigned)jy < (unsigned)L.ny) {
-                            const float level = L.ls.at(jx, jy);
-                            if (level < 0.0f) {
-                                den += (double)f[q];
-                                wv[q] = f[q];
-                            } else {
-                                den += (double)f[q] * (1.0 - (double)level / (double)phi);
-                            }
-                        }
-                    }
-                    wk = make_float4(wv[0], wv[1], wv[2], wv[3]);
-                    if (!(fabs(den) < (double)1.0e-6f)) {
-                        update = true;
-                        inv = 1.0 / den;
-                    }
-                }
-            }
-            if (!ring) m |= update ? MODE_UPDATE : MODE_ZERO;
-        }
-        T.mode[c][k] = m;
-        T.den[c][k] = den;
-        T.inv[c][k] = inv;
-        T.b[c][k] = bb;
-        T.w[c][k] = wk;
-    }
-    __syncthreads();
-    ps_load_p(T, L, gx0, gy0, base, H, tx, ty, false);
-    __syncthreads();
-
-    const double w = P.weight, omw = 1.0 - P.weight;
-    unsigned iters = 0;
-    double2 part = ps_residual_partial(T, base, H, tx, ty, P.factor);
-    if (threadIdx.x == 0) P.partials[blockIdx.x] = part;
-    bool ok = grid_barrier(P.barrier, nblocks);
-    double r = ok ? ps_total_relative(P.partials, nblocks) : 0.0;
-    const double r0 = r;
-    while (ok && !(r <= P.tol) && iters < P.max_iters) {
-        unsigned todo = min(P.check_interval, P.max_iters - iters);
-        while (ok && todo > 0) {
-            const unsigned kk = min((unsigned)KMAX, todo);
-            for (unsigned it = 0; it < kk; ++it) {
-                ps_half_sweep(T, base, 1, 2 * it, P.cdiv, w, omw);  // red: (x+y) odd
-                __syncthreads();
-                ps_half_sweep(T, base, 0, 2 * it + 1, P.cdiv, w, omw);  // black
-                __syncthreads();
-            }
-            ps_store_owned(T, L, gx0, gy0, base, H, tx, ty);
-            ok = grid_barrier(P.barrier, nblocks);
-            if (!ok) break;
-            ps_load_p(T, L, gx0, gy0, base, H, tx, ty, true);
-            __syncthreads();
-            todo -= kk;
-            iters += kk;
-        }
-        if (!ok) break;
-        part = ps_residual_partial(T, base, H, tx, ty, P.factor);
-        if (threadIdx.x == 0) P.partials[blockIdx.x] = part;
-        ok = grid_barrier(P.barrier, nblocks);
-        if (!ok) break;
-        r = ps_total_relative(P.partials, nblocks);
-    }
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        P.result->iterations = iters;
-        P.result->converged = (ok && r <= P.tol) ? 1 : 0;
-        P.result->error = ok ? 0 : 1;
-        P.result->r0 = r0;
-        P.result->r1 = r;
-    }
 }
 
 inline efl_status solver_init(SolverWorkspace& ws, int nx, int ny, int device, std::string* err) {
@@ -399,6 +187,12 @@ inline efl_status solve_gs_fixed(SolverWorkspace&, const LevelT<T>& L, const Uni
 // in exact arithmetic these are the RBGS iterates themselves: the
 // iteration counts are those of red-black Gauss-Seidel, while the sweeps move
 // f32 data.
+// Shared-memory image of one extended tile (EX x EY cells, EX even), stored
+// per colour in checkerboard-compressed form: cell (lx, ly) of colour
+// c = (gx + gy) & 1 lives at [c][ly][lx >> 1].  A cell's left / right
+// neighbours are the other colour's entries (lx >> 1) - 1 + (lx & 1) and
+// (lx >> 1) + (lx & 1) of the same row, up / down are entry lx >> 1 of the
+// rows above and below, so a warp reads consecutive words.
 template <int EX, int EY>
 struct MixTile {
     static constexpr int W2 = EX / 2;
@@ -887,95 +681,6 @@ struct PersistentPlan {
     const void* kernel = nullptr;
     bool ok = false;
 };
-
-// The tile shapes the persistent solver is instantiated for: (KMAX, tx, ty).
-// Deeper temporal blocking first; all CTAs must be co-resident (one per SM).
-template <int EX, int EY, int KMAX>
-inline bool try_plan(const SolverWorkspace& ws, int nx, int ny, PersistentPlan* p) {
-    const int tx = EX - 4 * KMAX, ty = EY - 4 * KMAX;
-    p->kmax = KMAX;
-    p->tx = tx;
-    p->ty = ty;
-    p->tiles_x = (nx + tx - 1) / tx;
-    p->tiles_y = (ny + ty - 1) / ty;
-    p->smem = sizeof(PsTile<EX, EY>);
-    p->kernel = (const void*)k_gs64_persistent<EX, EY, KMAX>;
-    if (p->smem + 1024 > ws.max_smem) return false;
-    if (p->tiles_x * p->tiles_y > ws.num_sms || p->tiles_x * p->tiles_y > ws.max_blocks) return false;
-    return true;
-}
-inline PersistentPlan plan_persistent(const SolverWorkspace& ws, int nx, int ny) {
-    PersistentPlan p;
-    if (try_plan<80, 48, 4>(ws, nx, ny, &p) ||   // 64 x 32 owned
-        try_plan<48, 48, 4>(ws, nx, ny, &p) ||   // 32 x 32
-        try_plan<72, 56, 2>(ws, nx, ny, &p) ||   // 64 x 48
-        try_plan<40, 40, 4>(ws, nx, ny, &p)) {   // 24 x 24
-        p.ok = true;
-        return p;
-    }
-    return PersistentPlan{};
-}
-
-// Tolerance-driven FP64 solve in one cooperative launch.  Returns
-// EFL_ERR_STATE if the grid does not fit the persistent scheme (the caller
-// then uses the host-driven loop).
-inline efl_status solve_gs64_persistent(SolverWorkspace& ws, const Level64& L, const Uniform& U, float weight,
-                                        double tol, uint32_t max_iters, uint32_t check_interval,
-                                        cudaStream_t stream, SolveResult* out, std::string* err) {
-    PersistentPlan plan = plan_persistent(ws, L.nx, L.ny);
-    if (!plan.ok) return EFL_ERR_STATE;
-    if (cudaFuncSetAttribute(plan.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plan.smem) !=
-        cudaSuccess) {
-        cudaGetLastError();
-        return EFL_ERR_STATE;
-    }
-    int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, plan.kernel, PS_THREADS, plan.smem) != cudaSuccess ||
-        per_sm < 1 || plan.tiles_x * plan.tiles_y > per_sm * ws.num_sms) {
-        cudaGetLastError();
-        return EFL_ERR_STATE;
-    }
-    PersistentParams P;
-    P.L = L;
-    P.tx = plan.tx;
-    P.ty = plan.ty;
-    P.kmax = plan.kmax;
-    P.halo = 2 * plan.kmax;
-    P.tiles_x = plan.tiles_x;
-    const double dx = (double)U.dx;
-    P.cdiv = dx * dx * (double)U.rho / (double)U.dt;
-    P.factor = (double)U.dt / (double)U.rho / dx / dx;
-    P.weight = (double)weight;
-    P.tol = tol;
-    P.max_iters = max_iters;
-    P.check_interval = std::max<uint32_t>(1, check_interval);
-    P.partials = ws.partials;
-    P.barrier = ws.barrier;
-    P.result = ws.result;
-    if (cudaMemsetAsync(ws.barrier, 0, sizeof(GridBarrier), stream) != cudaSuccess) {
-        *err = "barrier reset failed";
-        return EFL_ERR_CUDA;
-    }
-    void* args[] = {&P};
-    count_launch();
-    cudaError_t e = cudaLaunchCooperativeKernel(plan.kernel, dim3(plan.tiles_x * plan.tiles_y), dim3(PS_THREADS),
-                                                args, plan.smem, stream);
-    if (e != cudaSuccess) {
-        *err = std::string("cooperative launch of the persistent solver failed: ") + cudaGetErrorString(e);
-        return EFL_ERR_CUDA;
-    }
-    if (cudaMemcpyAsync(ws.h_result, ws.result, sizeof(SolveResult), cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
-        cudaStreamSynchronize(stream) != cudaSuccess) {
-        *err = std::string("persistent solver failed: ") + cudaGetErrorString(cudaGetLastError());
-        return EFL_ERR_CUDA;
-    }
-    *out = *ws.h_result;
-    if (out->error) {
-        *err = "persistent solver: a grid barrier timed out";
-        return EFL_ERR_CUDA;
-    }
-    return EFL_OK;
-}
 
 // Plans for the mixed persistent solve (MixTile: 53 bytes per cell).
 template <int EX, int EY, int KMAX>
