@@ -24,7 +24,7 @@ STATUS_NAMES = {0: "EFL_OK", 1: "EFL_ERR_INVALID_ARGUMENT", 2: "EFL_ERR_CUDA", 3
                 4: "EFL_NOT_CONVERGED", 5: "EFL_ERR_TOO_MANY", 6: "EFL_ERR_UNSUPPORTED_SHAPE",
                 7: "EFL_ERR_STATE", 8: "EFL_ERR_NO_DEVICE"}
 
-PROJECTION_JACOBI, PROJECTION_GAUSS_SEIDEL, PROJECTION_MULTIGRID = 0, 1, 2
+PROJECTION_JACOBI, PROJECTION_GAUSS_SEIDEL, PROJECTION_MULTIGRID, PROJECTION_MGPCG = 0, 1, 2, 3
 REINIT_JUMP_FLOODING, REINIT_FAST_ITERATIVE = 0, 1
 SHAPE_CIRCLE, SHAPE_RECTANGLE, SHAPE_CAPSULE, SHAPE_TRIANGLE = 0, 1, 2, 4
 SOURCE_CIRCLE, SOURCE_AABB = 0, 1

@@ -22,6 +22,7 @@
 #include "efl_solver.cuh"
 #include "efl_sweep_tma.cuh"
 #include "efl_batch.cuh"
+#include "efl_mgpcg.cuh"
 
 using namespace efl;
 
@@ -84,6 +85,8 @@ struct efl_sim {
     SweepTma tma;
     MixPlanes mixp{};  // global-memory planes of the mixed solve, allocated on first use
     bool mixp_ready = false;
+    CgPlanes cg{};  // MGPCG vectors, allocated on first use
+    bool cg_ready = false;
     PF mix_d2{};       // second correction buffer (batched solve)
     bool owns_stream = true;
     int* h_err = nullptr;  // pinned copy of the TMA sweep's error flag
@@ -207,8 +210,10 @@ efl_status validate_cfg(const efl_config* c) {
         return set_err(nullptr, EFL_ERR_INVALID_ARGUMENT, "grid size must be a multiple of 8 and at least 16 (got %ux%u)",
                        c->nx, c->ny);
     if (c->nx > 32768 || c->ny > 32768) return set_err(nullptr, EFL_ERR_INVALID_ARGUMENT, "grid size too large");
-    if (c->projection.method < 0 || c->projection.method > 2)
+    if (c->projection.method < 0 || c->projection.method > 3)
         return set_err(nullptr, EFL_ERR_INVALID_ARGUMENT, "unknown projection method %d", c->projection.method);
+    if (c->projection.method == EFL_PROJECTION_MGPCG && !(c->projection.tolerance > 0.0f))
+        return set_err(nullptr, EFL_ERR_INVALID_ARGUMENT, "MGPCG needs a tolerance > 0");
     if (c->reinit.method < 0 || c->reinit.method > 1)
         return set_err(nullptr, EFL_ERR_INVALID_ARGUMENT, "unknown reinitialize method %d", c->reinit.method);
     return EFL_OK;
@@ -347,20 +352,23 @@ efl_status relative_residual(efl_sim* s, const LevelT<T>& L0, double* rel) {
 }
 
 template <class T>
-efl_status gs_iterations(efl_sim* s, const LevelT<T>& L, float weight, float res_scale, uint32_t n) {
+efl_status gs_iterations(efl_sim* s, const LevelT<T>& L, float weight, float res_scale, uint32_t n,
+                         bool black_first = false) {
     float dxs = res_scale * s->U.dx;  // gauss_seidel.wgsl:57
     dim3 g = grid2d((L.nx + 1) / 2, L.ny, kBlock);
+    const int c0 = black_first ? 0 : 1;  // the reference sweeps red ((x+y) odd) first
     for (uint32_t k = 0; k < n; ++k) {
-        k_gs_color<T><<<g, kBlock, count_launch(), s->stream>>>(L, dxs, s->U.rho, s->U.dt, weight, 1);
-        k_gs_color<T><<<g, kBlock, count_launch(), s->stream>>>(L, dxs, s->U.rho, s->U.dt, weight, 0);
+        k_gs_color<T><<<g, kBlock, count_launch(), s->stream>>>(L, dxs, s->U.rho, s->U.dt, weight, c0);
+        k_gs_color<T><<<g, kBlock, count_launch(), s->stream>>>(L, dxs, s->U.rho, s->U.dt, weight, 1 - c0);
     }
     LAUNCH_CHECK();
     return EFL_OK;
 }
 
-// multi_grid.rs:390-475 (smoother weight 1.0, resolution_scale 2^i: multi_grid.rs:268-270)
+// multi_grid.rs:390-475 (smoother weight 1.0, resolution_scale 2^i: multi_grid.rs:268-270).
+// symmetric (the MGPCG preconditioner): post-smoothing black then red.
 template <class T>
-efl_status v_cycle(efl_sim* s, std::vector<LevelT<T>>& mg, size_t i) {
+efl_status v_cycle(efl_sim* s, std::vector<LevelT<T>>& mg, size_t i, bool symmetric = false) {
     const efl_projection& P = s->cfg.projection;
     const LevelT<T>& L = mg[i];
     float scale = (float)(1u << i);
@@ -370,10 +378,10 @@ efl_status v_cycle(efl_sim* s, std::vector<LevelT<T>>& mg, size_t i) {
     k_residual<T><<<grid2d(L.nx, L.ny, kBlock), kBlock, count_launch(), s->stream>>>(L, s->U.dt, s->U.rho, scale * s->U.dx);
     k_restriction<T><<<grid2d(C.nx, C.ny, kBlock), kBlock, count_launch(), s->stream>>>(L, C);
     LAUNCH_CHECK();
-    TRY(v_cycle(s, mg, i + 1));
+    TRY(v_cycle(s, mg, i + 1, symmetric));
     k_prolongation<T><<<grid2d(C.nx, C.ny, kBlock), kBlock, count_launch(), s->stream>>>(L, C);
     LAUNCH_CHECK();
-    return gs_iterations(s, L, 1.0f, scale, P.mg_post);
+    return gs_iterations(s, L, 1.0f, scale, P.mg_post, symmetric);
 }
 
 // n reference (f32) red-black iterations on the pressure field: the TMA
@@ -427,6 +435,104 @@ efl_status gs_mixed(efl_sim* s, float weight, double tol, uint32_t max_iters, ui
     return EFL_OK;
 }
 
+// A fixed-order reduction (k_chunk_sums, k_chunk_rows, k_rows_total), read to the host.
+template <class Term>
+efl_status cg_sum(efl_sim* s, const Term& term, double2* out) {
+    const int nch = (s->nx + RS_CHUNK - 1) / RS_CHUNK;
+    k_chunk_sums<Term><<<dim3(nch, (s->ny + RS_CHUNK - 1) / RS_CHUNK), RS_THREADS, count_launch(), s->stream>>>(
+        term, s->nx, s->ny, nch, s->cg.part);
+    k_chunk_rows<<<(s->ny + 127) / 128, 128, count_launch(), s->stream>>>(s->cg.part, nch, s->ny, s->cg.rowsum);
+    k_rows_total<<<1, 1024, count_launch(), s->stream>>>(s->cg.rowsum, s->ny, s->cg.total);
+    LAUNCH_CHECK();
+    CU(cudaMemcpyAsync(s->cg.h_total, s->cg.total, sizeof(double2), cudaMemcpyDeviceToHost, s->stream));
+    CU(cudaStreamSynchronize(s->stream));
+    *out = *s->cg.h_total;
+    return EFL_OK;
+}
+
+// EFL_PROJECTION_MGPCG on the FP64 level 0 (x = iterate, b = widened div):
+// conjugate gradients preconditioned by one symmetric f32 V-cycle of the
+// reference's structure.  Same steps and arithmetic as the oracle's
+// mgpcg_solve, reductions included (fixed order), so results are bit-exact.
+efl_status mgpcg(efl_sim* s, SolveResult* res) {
+    const efl_projection& P = s->cfg.projection;
+    const int nx = s->nx, ny = s->ny;
+    TRY(ensure_mix_planes(s));
+    if (!s->cg_ready) {
+        const int R = ny + 1;
+        TRY(alloc_plane(s, s->cg.r, nx, ny, s->P, R));
+        TRY(alloc_plane(s, s->cg.p, nx, ny, s->P, R));
+        TRY(alloc_plane(s, s->cg.ap, nx, ny, s->P, R));
+        TRY(alloc_plane(s, s->cg.r32, nx, ny, s->P, R));
+        TRY(alloc_plane(s, s->cg.z32, nx, ny, s->P, R));
+        TRY(alloc_raw(s, s->cg.part, (size_t)ny * ((nx + RS_CHUNK - 1) / RS_CHUNK)));
+        TRY(alloc_raw(s, s->cg.rowsum, (size_t)ny));
+        TRY(alloc_raw(s, s->cg.total, 1));
+        CU(cudaMallocHost(&s->cg.h_total, sizeof(double2)));
+        s->cg_ready = true;
+    }
+    Level64& L = s->mg64[0];
+    const MixPlanes& M = s->mixp;
+    CgPlanes& C = s->cg;
+    const dim3 g = grid2d(nx, ny, kBlock);
+    const double dx = (double)s->U.dx;
+    const double factor = (double)s->U.dt / (double)s->U.rho / dx / dx;
+    k_mix_coefficients<<<g, kBlock, count_launch(), s->stream>>>(L, M);
+    LAUNCH_CHECK();
+    auto true_rel = [&](double* rel) -> efl_status {
+        double2 t;
+        TRY(cg_sum(s, TermNorm{L.x, L.b, M, factor, nx, ny}, &t));
+        *rel = rel_from(t.x, t.y);
+        return EFL_OK;
+    };
+    // The preconditioner's f32 levels: level 0 is (x = z32, b = r32, the
+    // current phi and fractions, r0 as scratch); coarse levels as usual.
+    std::vector<Level> pre = s->mg;
+    pre[0].x = C.z32;
+    pre[0].b = C.r32;
+    auto precondition = [&](double* rz) -> efl_status {
+        CU(cudaMemset2DAsync(C.z32.p, (size_t)C.z32.P * sizeof(float), 0, (size_t)nx * sizeof(float), ny, s->stream));
+        TRY(v_cycle(s, pre, 0, true));
+        double2 t;
+        TRY(cg_sum(s, TermDotRZ{C.r, C.z32, M}, &t));
+        *rz = t.x;
+        return EFL_OK;
+    };
+    double rel;
+    TRY(true_rel(&rel));
+    res->r0 = rel;
+    uint32_t iters = 0;
+    if (!(rel <= (double)P.tolerance) && P.max_iterations > 0) {
+        k_cg_mask<<<g, kBlock, count_launch(), s->stream>>>(L.x, M, nx, ny);
+        k_cg_residual<<<g, kBlock, count_launch(), s->stream>>>(L.x, L.b, C.r, C.r32, M, factor, nx, ny);
+        LAUNCH_CHECK();
+        double rz;
+        TRY(precondition(&rz));
+        k_cg_direction<<<g, kBlock, count_launch(), s->stream>>>(C.p, C.z32, M, 0.0, 1, nx, ny);
+        while (iters < P.max_iterations) {
+            double2 t;
+            TRY(cg_sum(s, TermMatvecDot{C.p, C.ap, M, factor, nx, ny}, &t));  // ap = A p, p . ap
+            const double pap = t.x;
+            if (!(pap > 0.0)) break;  // breakdown: not positive definite here
+            const double alpha = rz / pap;
+            k_cg_axpy<<<g, kBlock, count_launch(), s->stream>>>(L.x, C.r, C.r32, C.p, C.ap, M, alpha, nx, ny);
+            ++iters;
+            TRY(true_rel(&rel));
+            if (rel <= (double)P.tolerance) break;
+            double rz1;
+            TRY(precondition(&rz1));
+            const double beta = rz1 / rz;
+            rz = rz1;
+            k_cg_direction<<<g, kBlock, count_launch(), s->stream>>>(C.p, C.z32, M, beta, 0, nx, ny);
+        }
+        LAUNCH_CHECK();
+    }
+    res->iterations = iters;
+    res->r1 = rel;
+    res->converged = rel <= (double)P.tolerance ? 1 : 0;
+    return EFL_OK;
+}
+
 // Errors that kernels report through device flags (a bounded wait that gave
 // up); called after the stream has been synchronised.
 efl_status check_device_errors(efl_sim* s) {
@@ -473,9 +579,12 @@ efl_status st_projection(efl_sim* s, efl_step_stats* st) {
         LAUNCH_CHECK();
         double r = -1.0;
         bool done = false;
-        if (P.method == EFL_PROJECTION_GAUSS_SEIDEL) {
+        if (P.method == EFL_PROJECTION_GAUSS_SEIDEL || P.method == EFL_PROJECTION_MGPCG) {
             SolveResult res{};
-            TRY(gs_mixed(s, P.sor_weight, (double)P.tolerance, P.max_iterations, P.check_interval, &res));
+            if (P.method == EFL_PROJECTION_GAUSS_SEIDEL)
+                TRY(gs_mixed(s, P.sor_weight, (double)P.tolerance, P.max_iterations, P.check_interval, &res));
+            else
+                TRY(mgpcg(s, &res));
             iters = res.iterations;
             r0 = res.r0;
             r = res.r1;
@@ -768,6 +877,7 @@ efl_status efl_destroy(efl_sim* s) {
     for (auto& b : s->bufs) cudaFree(b.p);
     if (s->d_forces) cudaFree(s->d_forces);
     if (s->h_norms) cudaFreeHost(s->h_norms);
+    if (s->cg.h_total) cudaFreeHost(s->cg.h_total);
     for (cudaEvent_t e : s->ev_proj)
         if (e) cudaEventDestroy(e);
     if (s->stream && s->owns_stream) cudaStreamDestroy(s->stream);
@@ -785,7 +895,9 @@ efl_status efl_reset(efl_sim* s) {
 
 efl_status efl_set_projection(efl_sim* s, const efl_projection* p) {
     if (!s || !p) return set_err(s, EFL_ERR_INVALID_ARGUMENT, "null argument");
-    if (p->method < 0 || p->method > 2) return set_err(s, EFL_ERR_INVALID_ARGUMENT, "unknown projection method");
+    if (p->method < 0 || p->method > 3) return set_err(s, EFL_ERR_INVALID_ARGUMENT, "unknown projection method");
+    if (p->method == EFL_PROJECTION_MGPCG && !(p->tolerance > 0.0f))
+        return set_err(s, EFL_ERR_INVALID_ARGUMENT, "MGPCG needs a tolerance > 0");
     cudaSetDevice(s->device);
     int old = mg_num_levels(s->cfg);
     s->cfg.projection = *p;

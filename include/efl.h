@@ -62,7 +62,12 @@ typedef enum efl_status {
 typedef enum efl_projection_method {
     EFL_PROJECTION_JACOBI = 0,
     EFL_PROJECTION_GAUSS_SEIDEL = 1,
-    EFL_PROJECTION_MULTIGRID = 2
+    EFL_PROJECTION_MULTIGRID = 2,
+    /* Extension, no reference counterpart: conjugate gradients on the FP64
+     * system preconditioned by one symmetric V-cycle of the reference's
+     * multigrid structure (post-smoothing black then red); tolerance > 0
+     * required, pressure_iterations counts CG iterations. */
+    EFL_PROJECTION_MGPCG = 3
 } efl_projection_method;
 
 /* ReinitializeMethod (src/euler_fluid/reinitialize_levelset.rs:36-40). */

@@ -492,10 +492,10 @@ void gs_half(Tex<T>& p, const Tex<T>& b, const Tex<float>& ls, const Tex<F4>& af
 }
 template <class T>
 void gs_iterations(Tex<T>& p, const Tex<T>& b, const Tex<float>& ls, const Tex<F4>& af, const Uniform& U,
-                   float weight, float res_scale, uint32_t n) {
+                   float weight, float res_scale, uint32_t n, bool black_first = false) {
     for (uint32_t k = 0; k < n; ++k) {
-        gs_half(p, b, ls, af, U, weight, res_scale, 1);  // red
-        gs_half(p, b, ls, af, U, weight, res_scale, 0);  // black
+        gs_half(p, b, ls, af, U, weight, res_scale, black_first ? 0 : 1);  // red first in the reference
+        gs_half(p, b, ls, af, U, weight, res_scale, black_first ? 1 : 0);
     }
 }
 
@@ -588,8 +588,10 @@ void k_prolongation(LevelT<T>& F, const LevelT<T>& C) {
     });
 }
 // multi_grid.rs:390-475; smoother weight 1.0 and resolution_scale 2^i (multi_grid.rs:268-270)
+// symmetric = true (the MGPCG preconditioner, an extension): post-smoothing
+// runs black then red, the reverse of pre-smoothing.
 template <class T>
-void v_cycle(std::vector<LevelT<T>>& mg, const Uniform& U, size_t i, const efl_projection& P) {
+void v_cycle(std::vector<LevelT<T>>& mg, const Uniform& U, size_t i, const efl_projection& P, bool symmetric = false) {
     LevelT<T>& L = mg[i];
     float scale = (float)(1u << i);
     if (i == mg.size() - 1) {
@@ -599,9 +601,9 @@ void v_cycle(std::vector<LevelT<T>>& mg, const Uniform& U, size_t i, const efl_p
     gs_iterations(L.x, L.b, L.ls, L.af, U, 1.0f, scale, P.mg_pre);
     k_residual(L, U, scale);
     k_restriction(L, mg[i + 1]);
-    v_cycle(mg, U, i + 1, P);
+    v_cycle(mg, U, i + 1, P, symmetric);
     k_prolongation(L, mg[i + 1]);
-    gs_iterations(L.x, L.b, L.ls, L.af, U, 1.0f, scale, P.mg_post);
+    gs_iterations(L.x, L.b, L.ls, L.af, U, 1.0f, scale, P.mg_post, symmetric);
 }
 
 // shaders/jacobi_iteration.wgsl:39-91 (levelset_solid fractions = af)
@@ -837,6 +839,166 @@ efl_status gs_mixed_solve(eflo_sim& s, uint32_t* iters_out, double* r0_out, doub
     return EFL_OK;
 }
 
+// Reductions of the MGPCG solve, in a fixed order that the CUDA kernels
+// reproduce: per row, chunks of 32 columns are each summed in x order from
+// 0.0, the chunk sums are added in chunk order from 0.0, and the row sums are
+// added in row order from 0.0.
+struct D2 {
+    double x, y;
+};
+template <class F>
+D2 row_ordered_sum(int W, int H, F term) {
+    std::vector<D2> rows(H);
+    par_rows(0, H, [&](int y) {
+        D2 row{0.0, 0.0};
+        for (int c = 0; c < W; c += 32) {
+            D2 ch{0.0, 0.0};
+            for (int x = c; x < std::min(W, c + 32); ++x) {
+                D2 t = term(x, y);
+                ch.x = ch.x + t.x;
+                ch.y = ch.y + t.y;
+            }
+            row.x = row.x + ch.x;
+            row.y = row.y + ch.y;
+        }
+        rows[y] = row;
+    });
+    D2 tot{0.0, 0.0};
+    for (int y = 0; y < H; ++y) {
+        tot.x = tot.x + rows[y].x;
+        tot.y = tot.y + rows[y].y;
+    }
+    return tot;
+}
+
+// Multigrid-preconditioned conjugate gradients (EFL_PROJECTION_MGPCG, an
+// extension: the reference iterates neither solver to a tolerance).  The
+// unknowns are the update cells of the mixed solve (fluid, not fully solid,
+// |denom| >= 1e-6); A is the factored FP64 operator of residual_at<double>
+// restricted to them (every other cell is held at p = 0).  The
+// preconditioner is one f32 V-cycle of the reference's structure
+// (multi_grid.rs:390-475: smoother weight 1, mg_pre / mg_post / mg_coarsest
+// sweeps, the reference's restriction and prolongation, the f32 arithmetic of
+// the reference's shaders) applied to f32(r) from a zero start and made
+// symmetric by running post-smoothing black-then-red; its result is widened
+// to FP64.  The convergence test is the true relative residual over the
+// counted cells after every iteration.
+efl_status mgpcg_solve(eflo_sim& s, uint32_t* iters_out, double* r0_out, double* r1_out) {
+    const efl_projection& P = s.cfg.projection;
+    const int W = s.nx, Hh = s.ny;
+    Level64& L = s.mg64[0];
+    std::vector<MixCell> cells;
+    mix_coefficients(s, cells);
+    const double dx = (double)s.U.dx;
+    const double factor = (double)s.U.dt / (double)s.U.rho / dx / dx;
+    static const int off[4][2] = {{-1, 0}, {1, 0}, {0, -1}, {0, 1}};
+    const int PW = L.x.w;  // row stride of the level's textures
+    std::vector<double>& X = L.x.a;
+    const std::vector<double>& B = L.b.a;
+    auto upd = [&](int x, int y) { return (cells[(size_t)y * W + x].mode & 2) != 0; };
+    // (A v)(x, y), the factored operator, v = 0 off the unknowns.
+    auto apply_at = [&](const std::vector<double>& v, int x, int y) {
+        const MixCell& c = cells[(size_t)y * W + x];
+        double sum = 0.0;
+        for (int i = 0; i < 4; ++i) {
+            int jx = x + off[i][0], jy = y + off[i][1];
+            double pn = (jx >= 0 && jy >= 0 && jx < W && jy < Hh) ? v[(size_t)jy * PW + jx] : 0.0;
+            if (i == 0) sum = (double)c.w[0] * pn;
+            else sum = sum + (double)c.w[i] * pn;
+        }
+        return factor * (c.den * v[(size_t)y * PW + x] - sum);
+    };
+    auto true_rel = [&]() {
+        D2 t = row_ordered_sum(W, Hh, [&](int x, int y) {
+            if (!(cells[(size_t)y * W + x].mode & 4)) return D2{0.0, 0.0};
+            const double bv = B[(size_t)y * PW + x];
+            const double rv = bv - apply_at(X, x, y);
+            return D2{rv * rv, bv * bv};
+        });
+        return rel_from(t.x, t.y);
+    };
+    // z = M r: the f32 V-cycle on the f32 levels with level 0 set to
+    // (x = 0, b = f32(r), the current phi and fractions); z is widened and
+    // zero off the unknowns.
+    Level& F = s.mg[0];
+    auto precondition = [&](const std::vector<double>& r, std::vector<double>& z) {
+        for (size_t i = 0; i < F.x.a.size(); ++i) {
+            F.x.a[i] = 0.0f;
+            F.b.a[i] = (float)r[i];
+        }
+        F.ls = s.ls0;
+        F.af = s.af;
+        v_cycle(s.mg, s.U, 0, P, true);
+        par_rows(0, Hh, [&](int y) {
+            for (int x = 0; x < W; ++x) z[(size_t)y * PW + x] = upd(x, y) ? (double)F.x.at(x, y) : 0.0;
+        });
+    };
+    double rel = true_rel();
+    *r0_out = rel;
+    uint32_t iters = 0;
+    if (!(rel <= (double)P.tolerance) && P.max_iterations > 0) {
+        const size_t M = X.size();
+        par_rows(0, Hh, [&](int y) {
+            for (int x = 0; x < W; ++x)
+                if (!upd(x, y)) X[(size_t)y * PW + x] = 0.0;
+        });
+        std::vector<double> r(M, 0.0), z(M, 0.0), p(M, 0.0), ap(M, 0.0);
+        par_rows(0, Hh, [&](int y) {
+            for (int x = 0; x < W; ++x) {
+                size_t i = (size_t)y * PW + x;
+                r[i] = upd(x, y) ? B[i] - apply_at(X, x, y) : 0.0;
+            }
+        });
+        precondition(r, z);
+        p = z;
+        double rz = row_ordered_sum(W, Hh, [&](int x, int y) {
+                        size_t i = (size_t)y * PW + x;
+                        return D2{upd(x, y) ? r[i] * z[i] : 0.0, 0.0};
+                    }).x;
+        while (iters < P.max_iterations) {
+            // ap = A p and p . ap in one pass
+            const double pap = row_ordered_sum(W, Hh, [&](int x, int y) {
+                                   size_t i = (size_t)y * PW + x;
+                                   if (!upd(x, y)) {
+                                       ap[i] = 0.0;
+                                       return D2{0.0, 0.0};
+                                   }
+                                   ap[i] = apply_at(p, x, y);
+                                   return D2{p[i] * ap[i], 0.0};
+                               }).x;
+            if (!(pap > 0.0)) break;  // breakdown: not positive definite here
+            const double alpha = rz / pap;
+            par_rows(0, Hh, [&](int y) {
+                for (int x = 0; x < W; ++x) {
+                    if (!upd(x, y)) continue;
+                    size_t i = (size_t)y * PW + x;
+                    X[i] = X[i] + alpha * p[i];
+                    r[i] = r[i] - alpha * ap[i];
+                }
+            });
+            ++iters;
+            rel = true_rel();
+            if (rel <= (double)P.tolerance) break;
+            precondition(r, z);
+            const double rz1 = row_ordered_sum(W, Hh, [&](int x, int y) {
+                                   size_t i = (size_t)y * PW + x;
+                                   return D2{upd(x, y) ? r[i] * z[i] : 0.0, 0.0};
+                               }).x;
+            const double beta = rz1 / rz;
+            rz = rz1;
+            par_rows(0, Hh, [&](int y) {
+                for (int x = 0; x < W; ++x) {
+                    size_t i = (size_t)y * PW + x;
+                    p[i] = upd(x, y) ? z[i] + beta * p[i] : 0.0;
+                }
+            });
+        }
+    }
+    *iters_out = iters;
+    *r1_out = rel;
+    return EFL_OK;
+}
+
 // projection.rs:89-164.  tolerance > 0 (an extension) solves to
 // ||b - A p|| / ||b|| <= tolerance with an FP64 iterate: the f32 pressure
 // cannot represent a solution that accurate when the hydrostatic pressure
@@ -870,9 +1032,10 @@ efl_status k_projection(eflo_sim& s, efl_step_stats* st) {
         };
         double r = rel();
         r0 = r;
-        if (P.method == EFL_PROJECTION_GAUSS_SEIDEL) {
+        if (P.method == EFL_PROJECTION_GAUSS_SEIDEL || P.method == EFL_PROJECTION_MGPCG) {
             double a, b;
-            gs_mixed_solve(s, &iters, &a, &b);
+            if (P.method == EFL_PROJECTION_GAUSS_SEIDEL) gs_mixed_solve(s, &iters, &a, &b);
+            else mgpcg_solve(s, &iters, &a, &b);
             r0 = a;
             r = b;
         } else {
@@ -1428,7 +1591,8 @@ efl_status validate_cfg(const efl_config* c, std::string* why) {
     }
     if (c->nx > 32768 || c->ny > 32768) { *why = "grid size too large"; return EFL_ERR_INVALID_ARGUMENT; }
     const efl_projection& p = c->projection;
-    if (p.method < 0 || p.method > 2) { *why = "unknown projection method"; return EFL_ERR_INVALID_ARGUMENT; }
+    if (p.method < 0 || p.method > 3) { *why = "unknown projection method"; return EFL_ERR_INVALID_ARGUMENT; }
+    if (p.method == EFL_PROJECTION_MGPCG && !(p.tolerance > 0.0f)) { *why = "MGPCG needs a tolerance > 0"; return EFL_ERR_INVALID_ARGUMENT; }
     if (c->reinit.method < 0 || c->reinit.method > 1) { *why = "unknown reinitialize method"; return EFL_ERR_INVALID_ARGUMENT; }
     return EFL_OK;
 }
@@ -1488,7 +1652,9 @@ efl_status eflo_reset(eflo_sim* s) {
 
 efl_status eflo_set_projection(eflo_sim* s, const efl_projection* p) {
     if (!s || !p) return EFL_ERR_INVALID_ARGUMENT;
-    if (p->method < 0 || p->method > 2) return fail(s, EFL_ERR_INVALID_ARGUMENT, "unknown projection method");
+    if (p->method < 0 || p->method > 3) return fail(s, EFL_ERR_INVALID_ARGUMENT, "unknown projection method");
+    if (p->method == EFL_PROJECTION_MGPCG && !(p->tolerance > 0.0f))
+        return fail(s, EFL_ERR_INVALID_ARGUMENT, "MGPCG needs a tolerance > 0");
     s->cfg.projection = *p;
     alloc_mg(*s);
     return EFL_OK;

@@ -164,3 +164,20 @@ def test_coupled_tolerance_global_path(oracle_api, gpu_api):
     assert abs(so.residual - sg.residual) <= 1e-9 * max(1.0, abs(so.residual))
     for f in (capi.FIELD_PRESSURE, capi.FIELD_U, capi.FIELD_V, capi.FIELD_LEVELSET_AIR):
         assert np.array_equal(g.get(f), o.get(f)), f
+
+
+def test_mgpcg_bit_exact(oracle_api, gpu_api):
+    """MG-preconditioned CG (row-ordered reductions on both sides): same CG
+    iteration counts and bit-exact fields on the C3 scene at 256^2."""
+    sc = scenes.scale(256)
+    sc.cfg.projection.method = capi.PROJECTION_MGPCG
+    o, g = make_pair(sc, oracle_api, gpu_api)
+    o.step(sc.dt)
+    g.step(sc.dt)
+    for _ in range(3):
+        so, sg = o.step(sc.dt), g.step(sc.dt)
+        assert so.converged and sg.converged
+        assert so.pressure_iterations == sg.pressure_iterations
+        assert so.residual == sg.residual and so.residual_initial == sg.residual_initial
+    bad = compare_fields(g, o)
+    assert not bad, bad

@@ -137,3 +137,27 @@ def test_batch_scene_matches_c4_spec():
         assert 0 <= x.position[0] < b.scenes[3].cfg.nx and 0 <= x.position[1] < b.scenes[3].cfg.ny
     g = scenes.batch(96).forces(3, 30)
     assert [(x.force[0], x.position[0]) for x in f] == [(x.force[0], x.position[0]) for x in g]
+
+
+def test_oracle_mgpcg_converges_fast(oracle_api):
+    """The multigrid-preconditioned CG reaches 1e-5 in a few tens of iterations
+    where plain V-cycles of the same structure need over a hundred."""
+    sc = scenes.scale(128)
+    sc.cfg.projection.method = capi.PROJECTION_MGPCG
+    sim = sc.make(oracle_api)
+    sim.step(sc.dt)
+    st = sim.step(sc.dt)
+    assert st.converged and st.residual <= 1e-5 and 0 < st.pressure_iterations <= 40
+    sc.cfg.projection.method = capi.PROJECTION_MULTIGRID
+    ref = sc.make(oracle_api)
+    ref.step(sc.dt)
+    sv = ref.step(sc.dt)
+    assert sv.converged and sv.pressure_iterations > 3 * st.pressure_iterations
+
+
+def test_mgpcg_requires_tolerance(oracle_api):
+    cfg = scenes.base_config(64, 64)
+    cfg.projection.method = capi.PROJECTION_MGPCG
+    cfg.projection.tolerance = 0.0
+    with pytest.raises(capi.EflError):
+        capi.Sim(oracle_api, cfg)
