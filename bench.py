@@ -24,6 +24,10 @@ metric: cell-steps/s to 1e-5 relative residual = cells x steps / time.
             batched path (efl_batch_step, one cooperative solve for all
             simulations) next to the plain path (efl_step per simulation),
             with the pressure-solve milliseconds of each.
+  c3     -- the 4096^2 scale scene (static circle r = 256) to 1e-5 each step:
+            MGPCG (CG preconditioned by a symmetric f32 V-cycle of the
+            reference's multigrid) next to the reference's V-cycle iterated
+            until the tolerance.
   microbench -- f32 reference sweeps on the 4096^2 all-fluid pressure
             microbench (N(0,1) divergence, mean removed).
   cpu_baseline -- the CPU oracle (a C++ port of the reference's kernels)
@@ -63,8 +67,10 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-microbench", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-c3", action="store_true")
+    ap.add_argument("--c3-size", type=int, default=4096, help="grid of the C3 scale scene (4096 in the benchmark)")
     ap.add_argument("--batch-sims", type=int, default=96, help="simulations of the C4 batch (96 in the benchmark)")
-    ap.add_argument("--only", choices=["coupled", "microbench", "batch"], default=None,
+    ap.add_argument("--only", choices=["coupled", "microbench", "batch", "c3"], default=None,
                     help="profiling aid: run one part only and print its numbers")
     return ap.parse_args()
 
@@ -220,6 +226,9 @@ def main():
     if args.only == "microbench":
         print(json.dumps(microbench(capi.load(), None, torch, measured_peaks()[0])), flush=True)
         return 0
+    if args.only == "c3":
+        print(json.dumps(c3_leg(capi.load(), torch, args, local, measured_peaks()[0])), flush=True)
+        return 0
     if args.only == "batch":
         dist = None
         if world > 1:
@@ -330,12 +339,20 @@ def main():
                         "the launch keeps its tiles in shared memory, so DRAM traffic (ncu) is far "
                         "below the algorithmic bytes"}
 
+    # ---- the same coupled loop with the MGPCG projection (an extension), device time per step
+    alt = None
+    if args.only is None:
+        alt = coupled_mgpcg(api, torch, args, local, flush, dist)
+
     micro = None
     if not args.no_microbench and rank == 0 and args.only is None:
         micro = microbench(api, stream, torch, peak)
     batch = None
     if not args.no_batch and args.only is None:
         batch = batch_leg(api, torch, args, world, rank, local, dist)
+    c3 = None
+    if not args.no_c3 and rank == 0 and args.only is None:
+        c3 = c3_leg(api, torch, args, local, peak)
 
     sim.close()
     if dist:
@@ -362,8 +379,12 @@ def main():
     }
     if micro:
         line["microbench"] = micro
+    if alt:
+        line["coupled_mgpcg"] = alt
     if batch:
         line["batch"] = batch
+    if c3:
+        line["c3"] = c3
     print(json.dumps(line), flush=True)
     return 0
 
@@ -479,6 +500,105 @@ def batch_leg(api, torch, args, world, rank, local, dist):
             "gpu_launches_batched": int(launches_b),
             "l2": "not flushed: the batch's working set (GBs) exceeds L2",
             "sharding": f"simulation i on rank i % {world}"}
+
+
+def coupled_mgpcg(api, torch, args, local, flush, dist):
+    """coupled_512 with EFL_PROJECTION_MGPCG instead of RBGS: same scene, same
+    coupling loop, same tolerance; device time per step, L2 flushed between steps."""
+    from bevy_eulerian_fluid_b200 import _capi as capi
+    from bevy_eulerian_fluid_b200 import scenes
+    from bevy_eulerian_fluid_b200.plugin import pack_obstacles
+    from bevy_eulerian_fluid_b200.rigid import RigidWorld
+    sc = scenes.coupled(args.size, method=capi.PROJECTION_MGPCG)
+    sc.cfg.device = local
+    sim = sc.make(api)
+    stream = torch.cuda.ExternalStream(sim.stream(), device=f"cuda:{local}")
+    rigid = RigidWorld(list(sc.bodies), (args.size, args.size), gravity=9.8 * scenes.LENGTH_UNIT,
+                       grid_length=1.0 / scenes.LENGTH_UNIT)
+
+    def coupled_step(timed=None):
+        if timed:
+            timed[0].record(stream)
+        st = sim.step(sc.dt)
+        if timed:
+            timed[1].record(stream)
+        rigid.apply_fluid_forces(sim.solid_forces(), sc.dt)
+        rigid.step(sc.dt)
+        sim.set_obstacles(pack_obstacles(rigid.bodies))
+        return st
+
+    sim.step(sc.dt)
+    for _ in range(args.warmup):
+        coupled_step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    iters, solve = [], []
+    for k in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        st = coupled_step(ev[k])
+        iters.append(int(st.pressure_iterations))
+        solve.append(sim.projection_ms())
+    torch.cuda.synchronize()
+    ms = sum(a.elapsed_time(b) for a, b in ev)
+    if dist:
+        t = torch.tensor([ms], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t[0].item())
+    sim.close()
+    world = dist.get_world_size() if dist else 1
+    return {"solver": "MGPCG (CG on the FP64 system, symmetric f32 V-cycle of the reference multigrid as "
+                      "preconditioner) to 1e-5 relative residual, an extension",
+            "value": world * sc.cells * args.steps / (ms / 1e3), "unit": "cell-steps/s",
+            "ms_per_step": ms / args.steps, "pressure_solve_ms_per_step": sum(solve) / args.steps,
+            "cg_iterations_per_step": iters}
+
+
+def c3_leg(api, torch, args, local, peak):
+    """C3: the 4096^2 dam break with a static circle r = 256, solved to 1e-5 each
+    step by MGPCG (CG preconditioned by a symmetric f32 V-cycle of the
+    reference's multigrid) next to iterated V-cycles (the reference's V-cycle
+    repeated until the tolerance)."""
+    from bevy_eulerian_fluid_b200 import _capi as capi
+    from bevy_eulerian_fluid_b200 import scenes
+    n = args.c3_size
+    out = {"workload": f"scale_{n}: {n}^2 dam break, static circle r={n // 16} at the centre, "
+                       "MG 2/2 sweeps, coarsest 16^2, to 1e-5 relative residual",
+           "cells": n * n, "unit": "cell-steps/s",
+           "l2": "not flushed: the working set (GBs) exceeds L2"}
+    for name, method, steps in (("mgpcg", capi.PROJECTION_MGPCG, max(1, min(args.steps, 10))),
+                                ("vcycles", capi.PROJECTION_MULTIGRID, 2)):
+        sc = scenes.scale(n)
+        sc.cfg.projection.method = method
+        sc.cfg.device = local
+        sim = sc.make(api)
+        stream = torch.cuda.ExternalStream(sim.stream(), device=f"cuda:{local}")
+        sim.step(sc.dt)
+        for _ in range(args.warmup):
+            sim.step(sc.dt)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        iters, solve = [], []
+        e0.record(stream)
+        for _ in range(steps):
+            st = sim.step(sc.dt)
+            iters.append(int(st.pressure_iterations))
+            solve.append(sim.projection_ms())
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        sim.close()
+        vcycles = sum(iters) + (steps if method == capi.PROJECTION_MGPCG else 0)  # MGPCG: one more per solve
+        vc_gbs = 272 * n * n * vcycles / (sum(solve) / 1e3) / 1e9
+        out[name] = {"value": n * n * steps / (ms / 1e3), "steps": steps, "ms_per_step": ms / steps,
+                     "pressure_solve_ms_per_step": sum(solve) / steps, "iterations": iters,
+                     "v_cycle_rate": {"achieved": round(vc_gbs, 1), "unit": "GB/s", "frac": round(vc_gbs / peak, 4),
+                                      "note": "272 algorithmic B per fine cell per V-cycle x V-cycles / solve time"}}
+    out["value"] = out["mgpcg"]["value"]
+    out["speedup_mgpcg_vs_vcycles"] = round(out["mgpcg"]["value"] / out["vcycles"]["value"], 2)
+    return out
 
 
 def microbench(api, stream, torch, peak):

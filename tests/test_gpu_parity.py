@@ -181,3 +181,19 @@ def test_mgpcg_bit_exact(oracle_api, gpu_api):
         assert so.residual == sg.residual and so.residual_initial == sg.residual_initial
     bad = compare_fields(g, o)
     assert not bad, bad
+
+
+def test_mgpcg_with_bodies_bit_exact(oracle_api, gpu_api):
+    """MGPCG on the coupled scene (bodies, fractional faces, JFA)."""
+    sc = small_coupled(128, method=capi.PROJECTION_MGPCG)
+    o, g = make_pair(sc, oracle_api, gpu_api)
+    o.step(sc.dt)
+    g.step(sc.dt)
+    for _ in range(4):
+        so, sg = o.step(sc.dt), g.step(sc.dt)
+        assert so.converged and sg.converged
+        assert so.pressure_iterations == sg.pressure_iterations
+        assert so.residual == sg.residual
+    bad = compare_fields(g, o)
+    assert not bad, bad
+    assert np.array_equal(g.force_bins(), o.force_bins())
