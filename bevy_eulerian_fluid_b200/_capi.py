@@ -134,11 +134,12 @@ SIGNATURES = {
     "batch_step": (C.c_int, [C.c_void_p, C.c_float, C.POINTER(StepStats)]),
     "batch_projection_ms": (C.c_int, [C.c_void_p, C.POINTER(C.c_float)]),
     "projection_ms": (C.c_int, ["X", C.POINTER(C.c_float)]),
+    "set_graph_capture": (C.c_int, ["X", C.c_int32]),
 }
 # Functions of efl.h that the oracle restatement does not mirror.
 PRODUCT_ONLY = {"abi_version", "default_config", "field_device_ptr", "stream", "synchronize", "kernel_launches",
                 "pressure_sweeps", "residual_norms_noalloc", "batch_create", "batch_destroy", "batch_last_error",
-                "batch_sim", "batch_step", "batch_projection_ms", "projection_ms"}
+                "batch_sim", "batch_step", "batch_projection_ms", "projection_ms", "set_graph_capture"}
 
 
 class EflError(RuntimeError):
@@ -349,6 +350,10 @@ class Sim:
         p, pitch = C.c_void_p(), C.c_size_t()
         self._check(self.api.field_device_ptr(self.h, field, C.byref(p), C.byref(pitch)))
         return p.value, pitch.value
+
+    def set_graph_capture(self, enable: bool):
+        """Replay repeating step segments as CUDA graphs (default on)."""
+        self._check(self.api.set_graph_capture(self.h, 1 if enable else 0))
 
     def projection_ms(self) -> float:
         """Device time of the last projection stage (ms)."""

@@ -23,13 +23,23 @@
 
 namespace efl {
 
+struct CgScalars {
+    double rz, alpha, beta;
+    int breakdown, pad;
+};
+struct CgRead {  // what the host reads after each iteration
+    double2 norm;   // (||r||^2, ||b||^2) over the counted cells
+    int breakdown;  // p . ap <= 0 in this iteration
+    int pad;
+};
 struct CgPlanes {
     Plane<double> r, p, ap;  // residual, direction, A * direction (the iterate is level 0's x)
     PF r32, z32;             // the preconditioner's level 0: b = f32(r), x = z
     double2* part = nullptr;    // chunk sums, ny x ceil(nx / 32)
     double2* rowsum = nullptr;  // one per row
-    double2* total = nullptr;   // device result of the last reduction
-    double2* h_total = nullptr; // pinned
+    double2* totals = nullptr;  // [0] p . ap, [1] norms, [2] r . z
+    CgScalars* sc = nullptr;
+    CgRead* h_read = nullptr;   // pinned
 };
 
 // A v on update cells (0 elsewhere), v = 0 off the unknowns.
@@ -149,24 +159,48 @@ __global__ void k_cg_residual(Plane<double> x, Plane<double> b, Plane<double> r,
     r.at(gx, gy) = v;
     r32.at(gx, gy) = (float)v;
 }
-// x += alpha p, r -= alpha ap on the unknowns; r32 = f32(r).
+enum { CG_RESET = 0, CG_RZ = 1, CG_ALPHA = 2, CG_BETA = 3 };
+// The CG scalar recurrences (one thread): the same IEEE double operations as
+// the host-side restatement.
+__global__ void k_cg_scalar(int op, const double2* totals, CgScalars* sc) {
+    if (op == CG_RESET) {
+        sc->breakdown = 0;
+    } else if (op == CG_RZ) {
+        sc->rz = totals[2].x;
+    } else if (op == CG_ALPHA) {
+        const double pap = totals[0].x;
+        if (pap > 0.0) {
+            sc->alpha = sc->rz / pap;
+        } else {
+            sc->alpha = 0.0;
+            sc->breakdown = 1;
+        }
+    } else {
+        const double rz1 = totals[2].x;
+        sc->beta = rz1 / sc->rz;
+        sc->rz = rz1;
+    }
+}
+// x += alpha p, r -= alpha ap on the unknowns; r32 = f32(r).  Nothing moves
+// after a breakdown.
 __global__ void k_cg_axpy(Plane<double> x, Plane<double> r, PF r32, Plane<double> p, Plane<double> ap, MixPlanes M,
-                          double alpha, int nx, int ny) {
+                          const CgScalars* sc, int nx, int ny) {
     const int gx = blockIdx.x * blockDim.x + threadIdx.x, gy = blockIdx.y * blockDim.y + threadIdx.y;
-    if (gx >= nx || gy >= ny || !(M.mode.at(gx, gy) & MODE_UPDATE)) return;
+    if (gx >= nx || gy >= ny || !(M.mode.at(gx, gy) & MODE_UPDATE) || sc->breakdown) return;
+    const double alpha = sc->alpha;
     x.at(gx, gy) = x.at(gx, gy) + alpha * p.at(gx, gy);
     const double rv = r.at(gx, gy) - alpha * ap.at(gx, gy);
     r.at(gx, gy) = rv;
     r32.at(gx, gy) = (float)rv;
 }
 // p = z (first) or z + beta p on the unknowns, 0 elsewhere (z widened from f32).
-__global__ void k_cg_direction(Plane<double> p, PF z, MixPlanes M, double beta, int first, int nx, int ny) {
+__global__ void k_cg_direction(Plane<double> p, PF z, MixPlanes M, const CgScalars* sc, int first, int nx, int ny) {
     const int gx = blockIdx.x * blockDim.x + threadIdx.x, gy = blockIdx.y * blockDim.y + threadIdx.y;
     if (gx >= nx || gy >= ny) return;
     double v = 0.0;
     if (M.mode.at(gx, gy) & MODE_UPDATE) {
         const double zv = (double)z.at(gx, gy);
-        v = first ? zv : zv + beta * p.at(gx, gy);
+        v = first ? zv : zv + sc->beta * p.at(gx, gy);
     }
     p.at(gx, gy) = v;
 }

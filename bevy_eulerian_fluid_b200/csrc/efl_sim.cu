@@ -29,6 +29,7 @@ using namespace efl;
 namespace efl {
 static std::atomic<uint64_t> g_launches{0};
 uint64_t launches_total() { return g_launches.load(std::memory_order_relaxed); }
+void add_launches(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 size_t count_launch() {
     g_launches.fetch_add(1, std::memory_order_relaxed);
     return 0;
@@ -87,6 +88,18 @@ struct efl_sim {
     bool mixp_ready = false;
     CgPlanes cg{};  // MGPCG vectors, allocated on first use
     bool cg_ready = false;
+    // Captured CUDA graphs of step segments, keyed by the host-side values their
+    // kernels were launched with (graph_epoch counts the setters that change them).
+    struct Graph {
+        uint64_t sig = 0;
+        cudaGraphExec_t exec = nullptr;
+        uint64_t kernels = 0;
+    };
+    Graph graphs[6];
+    int graph_next = 0;
+    uint64_t graph_epoch = 1;
+    uint64_t last_sig[4] = {0, 0, 0, 0};  // per segment: signature of the last eager run
+    bool graphs_on = true;
     PF mix_d2{};       // second correction buffer (batched solve)
     bool owns_stream = true;
     int* h_err = nullptr;  // pinned copy of the TMA sweep's error flag
@@ -435,25 +448,95 @@ efl_status gs_mixed(efl_sim* s, float weight, double tol, uint32_t max_iters, ui
     return EFL_OK;
 }
 
-// A fixed-order reduction (k_chunk_sums, k_chunk_rows, k_rows_total), read to the host.
+// Step segments that are replayed as CUDA graphs.
+enum { SEG_FULL = 0, SEG_PRE = 1, SEG_POST = 2, SEG_CG = 3 };
+
+uint64_t fnv(uint64_t h, uint64_t v) {
+    for (int i = 0; i < 8; ++i) {
+        h ^= (v >> (8 * i)) & 0xffu;
+        h *= 1099511628211ull;
+    }
+    return h;
+}
+// The host-side values a segment's kernels are launched with.
+uint64_t segment_sig(const efl_sim* s, int seg) {
+    uint64_t h = 1469598103934665603ull;
+    uint32_t dtb;
+    std::memcpy(&dtb, &s->U.dt, 4);
+    h = fnv(h, (uint64_t)seg);
+    h = fnv(h, s->graph_epoch);
+    h = fnv(h, dtb);
+    h = fnv(h, (uint64_t)s->n_obs);
+    h = fnv(h, (uint64_t)s->n_forces);
+    h = fnv(h, (uint64_t)(uintptr_t)s->d_forces);
+    return h | 1;  // never 0
+}
+
+// Runs body() on the simulation's stream.  A segment whose signature repeats
+// is captured into a CUDA graph on its second run and replayed from then on
+// (the first run of a signature stays eager, so lazily created resources are
+// made outside any capture).  If capture fails, graphs are switched off for
+// this simulation and the body runs eagerly.
+template <class F>
+efl_status run_segment(efl_sim* s, int seg, F body) {
+    if (!s->graphs_on) return body();
+    const uint64_t sig = segment_sig(s, seg);
+    for (auto& g : s->graphs)
+        if (g.exec && g.sig == sig) {
+            CU(cudaGraphLaunch(g.exec, s->stream));
+            add_launches(g.kernels);
+            return EFL_OK;
+        }
+    if (s->last_sig[seg] != sig) {
+        s->last_sig[seg] = sig;
+        return body();
+    }
+    const uint64_t n0 = launches_total();
+    if (cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaGetLastError();
+        s->graphs_on = false;
+        return body();
+    }
+    const efl_status st = body();
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(s->stream, &graph);
+    cudaGraphExec_t exec = nullptr;
+    if (st != EFL_OK || e != cudaSuccess || !graph || cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        s->graphs_on = false;
+        if (st != EFL_OK) return st;
+        return body();  // nothing ran during the failed capture
+    }
+    cudaGraphDestroy(graph);
+    auto& slot = s->graphs[s->graph_next];
+    s->graph_next = (s->graph_next + 1) % (int)(sizeof(s->graphs) / sizeof(s->graphs[0]));
+    if (slot.exec) cudaGraphExecDestroy(slot.exec);
+    slot.sig = sig;
+    slot.exec = exec;
+    slot.kernels = launches_total() - n0;  // counted once at capture: this first launch
+    CU(cudaGraphLaunch(exec, s->stream));
+    return EFL_OK;
+}
+
+// A fixed-order reduction (k_chunk_sums, k_chunk_rows, k_rows_total) into
+// C.totals[slot], enqueued on the simulation's stream.
 template <class Term>
-efl_status cg_sum(efl_sim* s, const Term& term, double2* out) {
+void cg_sum_enqueue(efl_sim* s, const Term& term, int slot) {
     const int nch = (s->nx + RS_CHUNK - 1) / RS_CHUNK;
     k_chunk_sums<Term><<<dim3(nch, (s->ny + RS_CHUNK - 1) / RS_CHUNK), RS_THREADS, count_launch(), s->stream>>>(
         term, s->nx, s->ny, nch, s->cg.part);
     k_chunk_rows<<<(s->ny + 127) / 128, 128, count_launch(), s->stream>>>(s->cg.part, nch, s->ny, s->cg.rowsum);
-    k_rows_total<<<1, 1024, count_launch(), s->stream>>>(s->cg.rowsum, s->ny, s->cg.total);
-    LAUNCH_CHECK();
-    CU(cudaMemcpyAsync(s->cg.h_total, s->cg.total, sizeof(double2), cudaMemcpyDeviceToHost, s->stream));
-    CU(cudaStreamSynchronize(s->stream));
-    *out = *s->cg.h_total;
-    return EFL_OK;
+    k_rows_total<<<1, 1024, count_launch(), s->stream>>>(s->cg.rowsum, s->ny, s->cg.totals + slot);
 }
 
 // EFL_PROJECTION_MGPCG on the FP64 level 0 (x = iterate, b = widened div):
 // conjugate gradients preconditioned by one symmetric f32 V-cycle of the
 // reference's structure.  Same steps and arithmetic as the oracle's
 // mgpcg_solve, reductions included (fixed order), so results are bit-exact.
+// The CG scalars stay on the device; one CG iteration is one segment (a CUDA
+// graph from the third iteration of a signature on) followed by one read of
+// the residual norms.
 efl_status mgpcg(efl_sim* s, SolveResult* res) {
     const efl_projection& P = s->cfg.projection;
     const int nx = s->nx, ny = s->ny;
@@ -467,8 +550,9 @@ efl_status mgpcg(efl_sim* s, SolveResult* res) {
         TRY(alloc_plane(s, s->cg.z32, nx, ny, s->P, R));
         TRY(alloc_raw(s, s->cg.part, (size_t)ny * ((nx + RS_CHUNK - 1) / RS_CHUNK)));
         TRY(alloc_raw(s, s->cg.rowsum, (size_t)ny));
-        TRY(alloc_raw(s, s->cg.total, 1));
-        CU(cudaMallocHost(&s->cg.h_total, sizeof(double2)));
+        TRY(alloc_raw(s, s->cg.totals, 3));
+        TRY(alloc_raw(s, s->cg.sc, 1));
+        CU(cudaMallocHost(&s->cg.h_read, sizeof(CgRead)));
         s->cg_ready = true;
     }
     Level64& L = s->mg64[0];
@@ -479,10 +563,9 @@ efl_status mgpcg(efl_sim* s, SolveResult* res) {
     const double factor = (double)s->U.dt / (double)s->U.rho / dx / dx;
     k_mix_coefficients<<<g, kBlock, count_launch(), s->stream>>>(L, M);
     LAUNCH_CHECK();
-    auto true_rel = [&](double* rel) -> efl_status {
-        double2 t;
-        TRY(cg_sum(s, TermNorm{L.x, L.b, M, factor, nx, ny}, &t));
-        *rel = rel_from(t.x, t.y);
+    auto read_back = [&]() -> efl_status {  // C.h_read <- (norm totals, breakdown flag)
+        CU(cudaMemcpyAsync(&C.h_read->norm, C.totals + 1, sizeof(double2), cudaMemcpyDeviceToHost, s->stream));
+        CU(cudaMemcpyAsync(&C.h_read->breakdown, &C.sc->breakdown, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
         return EFL_OK;
     };
     // The preconditioner's f32 levels: level 0 is (x = z32, b = r32, the
@@ -490,42 +573,49 @@ efl_status mgpcg(efl_sim* s, SolveResult* res) {
     std::vector<Level> pre = s->mg;
     pre[0].x = C.z32;
     pre[0].b = C.r32;
-    auto precondition = [&](double* rz) -> efl_status {
+    auto precondition = [&]() -> efl_status {  // z = M r, then r . z into totals[2]
         CU(cudaMemset2DAsync(C.z32.p, (size_t)C.z32.P * sizeof(float), 0, (size_t)nx * sizeof(float), ny, s->stream));
         TRY(v_cycle(s, pre, 0, true));
-        double2 t;
-        TRY(cg_sum(s, TermDotRZ{C.r, C.z32, M}, &t));
-        *rz = t.x;
+        cg_sum_enqueue(s, TermDotRZ{C.r, C.z32, M}, 2);
         return EFL_OK;
     };
-    double rel;
-    TRY(true_rel(&rel));
+    cg_sum_enqueue(s, TermNorm{L.x, L.b, M, factor, nx, ny}, 1);
+    k_cg_scalar<<<1, 1, count_launch(), s->stream>>>(CG_RESET, C.totals, C.sc);
+    TRY(read_back());
+    CU(cudaStreamSynchronize(s->stream));
+    double rel = rel_from(C.h_read->norm.x, C.h_read->norm.y);
     res->r0 = rel;
     uint32_t iters = 0;
     if (!(rel <= (double)P.tolerance) && P.max_iterations > 0) {
         k_cg_mask<<<g, kBlock, count_launch(), s->stream>>>(L.x, M, nx, ny);
         k_cg_residual<<<g, kBlock, count_launch(), s->stream>>>(L.x, L.b, C.r, C.r32, M, factor, nx, ny);
+        TRY(precondition());
+        k_cg_scalar<<<1, 1, count_launch(), s->stream>>>(CG_RZ, C.totals, C.sc);
+        k_cg_direction<<<g, kBlock, count_launch(), s->stream>>>(C.p, C.z32, M, C.sc, 1, nx, ny);
         LAUNCH_CHECK();
-        double rz;
-        TRY(precondition(&rz));
-        k_cg_direction<<<g, kBlock, count_launch(), s->stream>>>(C.p, C.z32, M, 0.0, 1, nx, ny);
+        // One iteration: ap = A p and p . ap; alpha = rz / p.ap (0 and a
+        // breakdown flag unless p.ap > 0); x += alpha p, r -= alpha ap; the
+        // true residual norms; z = M r and r . z; beta = rz' / rz; p = z + beta p.
+        // The last three only matter when the host continues.
+        auto iteration = [&]() -> efl_status {
+            cg_sum_enqueue(s, TermMatvecDot{C.p, C.ap, M, factor, nx, ny}, 0);
+            k_cg_scalar<<<1, 1, count_launch(), s->stream>>>(CG_ALPHA, C.totals, C.sc);
+            k_cg_axpy<<<g, kBlock, count_launch(), s->stream>>>(L.x, C.r, C.r32, C.p, C.ap, M, C.sc, nx, ny);
+            cg_sum_enqueue(s, TermNorm{L.x, L.b, M, factor, nx, ny}, 1);
+            TRY(precondition());
+            k_cg_scalar<<<1, 1, count_launch(), s->stream>>>(CG_BETA, C.totals, C.sc);
+            k_cg_direction<<<g, kBlock, count_launch(), s->stream>>>(C.p, C.z32, M, C.sc, 0, nx, ny);
+            LAUNCH_CHECK();
+            return read_back();
+        };
         while (iters < P.max_iterations) {
-            double2 t;
-            TRY(cg_sum(s, TermMatvecDot{C.p, C.ap, M, factor, nx, ny}, &t));  // ap = A p, p . ap
-            const double pap = t.x;
-            if (!(pap > 0.0)) break;  // breakdown: not positive definite here
-            const double alpha = rz / pap;
-            k_cg_axpy<<<g, kBlock, count_launch(), s->stream>>>(L.x, C.r, C.r32, C.p, C.ap, M, alpha, nx, ny);
+            TRY(run_segment(s, SEG_CG, iteration));
+            CU(cudaStreamSynchronize(s->stream));
+            if (C.h_read->breakdown) break;  // p . ap <= 0: not positive definite here (x unchanged)
             ++iters;
-            TRY(true_rel(&rel));
+            rel = rel_from(C.h_read->norm.x, C.h_read->norm.y);
             if (rel <= (double)P.tolerance) break;
-            double rz1;
-            TRY(precondition(&rz1));
-            const double beta = rz1 / rz;
-            rz = rz1;
-            k_cg_direction<<<g, kBlock, count_launch(), s->stream>>>(C.p, C.z32, M, beta, 0, nx, ny);
         }
-        LAUNCH_CHECK();
     }
     res->iterations = iters;
     res->r1 = rel;
@@ -877,9 +967,11 @@ efl_status efl_destroy(efl_sim* s) {
     for (auto& b : s->bufs) cudaFree(b.p);
     if (s->d_forces) cudaFree(s->d_forces);
     if (s->h_norms) cudaFreeHost(s->h_norms);
-    if (s->cg.h_total) cudaFreeHost(s->cg.h_total);
+    if (s->cg.h_read) cudaFreeHost(s->cg.h_read);
     for (cudaEvent_t e : s->ev_proj)
         if (e) cudaEventDestroy(e);
+    for (auto& g : s->graphs)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
     if (s->stream && s->owns_stream) cudaStreamDestroy(s->stream);
     delete s;
     return EFL_OK;
@@ -890,6 +982,7 @@ const char* efl_last_error(const efl_sim* s) { return s ? s->err.c_str() : g_las
 efl_status efl_reset(efl_sim* s) {
     if (!s) return set_err(nullptr, EFL_ERR_INVALID_ARGUMENT, "null sim");
     s->status = 0;
+    ++s->graph_epoch;
     return EFL_OK;
 }
 
@@ -901,6 +994,7 @@ efl_status efl_set_projection(efl_sim* s, const efl_projection* p) {
     cudaSetDevice(s->device);
     int old = mg_num_levels(s->cfg);
     s->cfg.projection = *p;
+    ++s->graph_epoch;
     if (mg_num_levels(s->cfg) != old) TRY(alloc_mg(s));
     return EFL_OK;
 }
@@ -908,12 +1002,14 @@ efl_status efl_set_reinit(efl_sim* s, const efl_reinit* r) {
     if (!s || !r) return set_err(s, EFL_ERR_INVALID_ARGUMENT, "null argument");
     if (r->method < 0 || r->method > 1) return set_err(s, EFL_ERR_INVALID_ARGUMENT, "unknown reinitialize method");
     s->cfg.reinit = *r;
+    ++s->graph_epoch;
     return EFL_OK;
 }
 efl_status efl_set_transform(efl_sim* s, const float t[16]) {
     if (!s || !t) return set_err(s, EFL_ERR_INVALID_ARGUMENT, "null argument");
     std::memcpy(s->U.m, t, sizeof(s->U.m));
     std::memcpy(s->cfg.transform, t, sizeof(s->U.m));
+    ++s->graph_epoch;
     return EFL_OK;
 }
 
@@ -942,6 +1038,7 @@ efl_status efl_set_local_forces(efl_sim* s, const efl_force* f, uint32_t n) {
         int cap = std::max<int>(64, (int)n);
         CU(cudaMalloc(&s->d_forces, (size_t)cap * sizeof(efl_force)));
         s->cap_forces = cap;
+        ++s->graph_epoch;
     }
     if (n) CU(cudaMemcpyAsync(s->d_forces, f, n * sizeof(efl_force), cudaMemcpyHostToDevice, s->stream));
     s->n_forces = (int)n;
@@ -954,8 +1051,31 @@ efl_status efl_set_sources(efl_sim* s, const efl_source* src, uint32_t n, int32_
         return set_err(s, EFL_ERR_TOO_MANY, "The maximum number of fluid source per fluid component is %d.",
                        EFL_MAX_FLUID_SOURCE);
     (oneshot ? s->src_once : s->src_cont).assign(src, src + n);
+    if (!oneshot) ++s->graph_epoch;
     return EFL_OK;
 }
+
+}  // extern "C"
+
+namespace {
+efl_status run_stages(efl_sim* s, int first, int last, efl_step_stats* st) {
+    efl_status ret = EFL_OK;
+    for (int stage = first; stage <= last; ++stage) {
+        efl_status r = run_stage(s, stage, st);
+        if (r == EFL_NOT_CONVERGED) ret = r;
+        else if (r != EFL_OK) return r;
+    }
+    return ret;
+}
+
+// Iteration count of a fixed-count projection (projection.rs:89-164).
+uint32_t fixed_iterations(const efl_projection& P) {
+    if (P.method == EFL_PROJECTION_JACOBI) return 50;
+    return P.method == EFL_PROJECTION_GAUSS_SEIDEL ? P.gs_iterations : 1;
+}
+}  // namespace
+
+extern "C" {
 
 efl_status efl_step(efl_sim* s, float dt, efl_step_stats* st) {
     if (!s) return set_err(nullptr, EFL_ERR_INVALID_ARGUMENT, "null sim");
@@ -969,13 +1089,34 @@ efl_status efl_step(efl_sim* s, float dt, efl_step_stats* st) {
     }
     s->U.dt = dt;
     efl_status ret = EFL_OK;
-    for (int stage = EFL_STAGE_UPDATE_SOLID; stage <= EFL_STAGE_SOLID_FORCES; ++stage) {
-        efl_status r = run_stage(s, stage, st);
-        if (r == EFL_NOT_CONVERGED) ret = r;
-        else if (r != EFL_OK) return r;
+    const efl_projection& P = s->cfg.projection;
+    if (P.method == EFL_PROJECTION_JACOBI || P.tolerance <= 0.0f) {
+        // No host round trip anywhere: the whole step is one segment.
+        TRY(run_segment(s, SEG_FULL, [&] { return run_stages(s, EFL_STAGE_UPDATE_SOLID, EFL_STAGE_SOLID_FORCES, nullptr); }));
+        if (st) st->pressure_iterations = fixed_iterations(P);
+    } else {
+        TRY(run_segment(s, SEG_PRE, [&] { return run_stages(s, EFL_STAGE_UPDATE_SOLID, EFL_STAGE_DIVERGENCE, nullptr); }));
+        ret = run_stage(s, EFL_STAGE_PROJECTION, st);
+        if (ret != EFL_OK && ret != EFL_NOT_CONVERGED) return ret;
+        TRY(run_segment(s, SEG_POST, [&] { return run_stages(s, EFL_STAGE_SOLVE_VELOCITY, EFL_STAGE_SOLID_FORCES, nullptr); }));
     }
     s->n_forces = 0;  // apply_forces.rs:166 clears the forces after upload
     return ret;
+}
+
+efl_status efl_set_graph_capture(efl_sim* s, int32_t enable) {
+    if (!s) return set_err(nullptr, EFL_ERR_INVALID_ARGUMENT, "null sim");
+    cudaSetDevice(s->device);
+    s->graphs_on = enable != 0;
+    if (!s->graphs_on) {
+        CU(cudaStreamSynchronize(s->stream));
+        for (auto& g : s->graphs) {
+            if (g.exec) cudaGraphExecDestroy(g.exec);
+            g = efl_sim::Graph{};
+        }
+    }
+    for (auto& l : s->last_sig) l = 0;
+    return EFL_OK;
 }
 
 efl_status efl_projection_ms(efl_sim* s, float* ms) {

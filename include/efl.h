@@ -311,6 +311,13 @@ EFL_API efl_status efl_synchronize(efl_sim* sim);
 /* Relative residual ||b - A p||_2 / ||b||_2 of the current pressure against
  * the current divergence (operator of residual.wgsl:33-54), FP64 norms. */
 EFL_API efl_status efl_residual(efl_sim* sim, double* relative, double* norm_r, double* norm_b);
+/* efl_step replays each step segment whose kernel arguments repeat (the
+ * whole step for fixed-count projections; the stages before and after the
+ * projection for tolerance-driven ones) as a captured CUDA graph, from the
+ * second time the same arguments occur.  enable = 0 runs every kernel as its
+ * own launch (results are identical).  Default on.  No reference
+ * counterpart (the reference records wgpu command buffers per frame). */
+EFL_API efl_status efl_set_graph_capture(efl_sim* sim, int32_t enable);
 /* Device time of the last projection stage (efl_step or efl_run_stage), in
  * milliseconds; waits for it to finish.  No reference counterpart (the
  * reference has no per-stage timing). */
