@@ -51,6 +51,27 @@ struct DevBuf {
 
 }  // namespace
 
+// Captured CUDA graphs of step segments, keyed by a signature of the
+// host-side values their kernels were launched with.
+struct GraphCache {
+    struct Graph {
+        uint64_t sig = 0;
+        cudaGraphExec_t exec = nullptr;
+        uint64_t kernels = 0;
+    };
+    Graph graphs[8];
+    int next = 0;
+    uint64_t last_sig[4] = {0, 0, 0, 0};  // per segment: signature of the last eager run
+    bool on = true;
+    void clear() {
+        for (auto& g : graphs) {
+            if (g.exec) cudaGraphExecDestroy(g.exec);
+            g = Graph{};
+        }
+        for (auto& l : last_sig) l = 0;
+    }
+};
+
 struct efl_sim {
     efl_config cfg{};
     int nx = 0, ny = 0, P = 0;
@@ -88,18 +109,8 @@ struct efl_sim {
     bool mixp_ready = false;
     CgPlanes cg{};  // MGPCG vectors, allocated on first use
     bool cg_ready = false;
-    // Captured CUDA graphs of step segments, keyed by the host-side values their
-    // kernels were launched with (graph_epoch counts the setters that change them).
-    struct Graph {
-        uint64_t sig = 0;
-        cudaGraphExec_t exec = nullptr;
-        uint64_t kernels = 0;
-    };
-    Graph graphs[6];
-    int graph_next = 0;
-    uint64_t graph_epoch = 1;
-    uint64_t last_sig[4] = {0, 0, 0, 0};  // per segment: signature of the last eager run
-    bool graphs_on = true;
+    GraphCache gc;                // captured step segments
+    uint64_t graph_epoch = 1;     // counts the setters that change kernel arguments
     PF mix_d2{};       // second correction buffer (batched solve)
     bool owns_stream = true;
     int* h_err = nullptr;  // pinned copy of the TMA sweep's error flag
@@ -472,51 +483,56 @@ uint64_t segment_sig(const efl_sim* s, int seg) {
     return h | 1;  // never 0
 }
 
-// Runs body() on the simulation's stream.  A segment whose signature repeats
-// is captured into a CUDA graph on its second run and replayed from then on
-// (the first run of a signature stays eager, so lazily created resources are
-// made outside any capture).  If capture fails, graphs are switched off for
-// this simulation and the body runs eagerly.
+// Runs body() on `stream`.  A segment whose signature repeats is captured
+// into a CUDA graph on its second run and replayed from then on (the first
+// run of a signature stays eager, so lazily created resources are made
+// outside any capture).  If capture fails, graphs are switched off for this
+// cache and the body runs eagerly.
 template <class F>
-efl_status run_segment(efl_sim* s, int seg, F body) {
-    if (!s->graphs_on) return body();
-    const uint64_t sig = segment_sig(s, seg);
-    for (auto& g : s->graphs)
+efl_status run_segment(GraphCache& gc, cudaStream_t stream, uint64_t sig, int seg, F body) {
+    if (!gc.on) return body();
+    for (auto& g : gc.graphs)
         if (g.exec && g.sig == sig) {
-            CU(cudaGraphLaunch(g.exec, s->stream));
+            if (cudaGraphLaunch(g.exec, stream) != cudaSuccess) return EFL_ERR_CUDA;
             add_launches(g.kernels);
             return EFL_OK;
         }
-    if (s->last_sig[seg] != sig) {
-        s->last_sig[seg] = sig;
+    if (gc.last_sig[seg] != sig) {
+        gc.last_sig[seg] = sig;
         return body();
     }
     const uint64_t n0 = launches_total();
-    if (cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    if (cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
         cudaGetLastError();
-        s->graphs_on = false;
+        gc.on = false;
         return body();
     }
     const efl_status st = body();
     cudaGraph_t graph = nullptr;
-    const cudaError_t e = cudaStreamEndCapture(s->stream, &graph);
+    const cudaError_t e = cudaStreamEndCapture(stream, &graph);
     cudaGraphExec_t exec = nullptr;
     if (st != EFL_OK || e != cudaSuccess || !graph || cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) {
         if (graph) cudaGraphDestroy(graph);
         cudaGetLastError();
-        s->graphs_on = false;
+        gc.on = false;
         if (st != EFL_OK) return st;
         return body();  // nothing ran during the failed capture
     }
     cudaGraphDestroy(graph);
-    auto& slot = s->graphs[s->graph_next];
-    s->graph_next = (s->graph_next + 1) % (int)(sizeof(s->graphs) / sizeof(s->graphs[0]));
+    auto& slot = gc.graphs[gc.next];
+    gc.next = (gc.next + 1) % (int)(sizeof(gc.graphs) / sizeof(gc.graphs[0]));
     if (slot.exec) cudaGraphExecDestroy(slot.exec);
     slot.sig = sig;
     slot.exec = exec;
     slot.kernels = launches_total() - n0;  // counted once at capture: this first launch
-    CU(cudaGraphLaunch(exec, s->stream));
+    if (cudaGraphLaunch(exec, stream) != cudaSuccess) return EFL_ERR_CUDA;
     return EFL_OK;
+}
+template <class F>
+efl_status run_segment(efl_sim* s, int seg, F body) {
+    const efl_status st = run_segment(s->gc, s->stream, segment_sig(s, seg), seg, body);
+    if (st == EFL_ERR_CUDA && s->err.empty()) set_err(s, st, "graph launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+    return st;
 }
 
 // A fixed-order reduction (k_chunk_sums, k_chunk_rows, k_rows_total) into
@@ -970,8 +986,7 @@ efl_status efl_destroy(efl_sim* s) {
     if (s->cg.h_read) cudaFreeHost(s->cg.h_read);
     for (cudaEvent_t e : s->ev_proj)
         if (e) cudaEventDestroy(e);
-    for (auto& g : s->graphs)
-        if (g.exec) cudaGraphExecDestroy(g.exec);
+    s->gc.clear();
     if (s->stream && s->owns_stream) cudaStreamDestroy(s->stream);
     delete s;
     return EFL_OK;
@@ -1107,15 +1122,9 @@ efl_status efl_step(efl_sim* s, float dt, efl_step_stats* st) {
 efl_status efl_set_graph_capture(efl_sim* s, int32_t enable) {
     if (!s) return set_err(nullptr, EFL_ERR_INVALID_ARGUMENT, "null sim");
     cudaSetDevice(s->device);
-    s->graphs_on = enable != 0;
-    if (!s->graphs_on) {
-        CU(cudaStreamSynchronize(s->stream));
-        for (auto& g : s->graphs) {
-            if (g.exec) cudaGraphExecDestroy(g.exec);
-            g = efl_sim::Graph{};
-        }
-    }
-    for (auto& l : s->last_sig) l = 0;
+    CU(cudaStreamSynchronize(s->stream));
+    s->gc.clear();
+    s->gc.on = enable != 0;
     return EFL_OK;
 }
 
@@ -1412,6 +1421,7 @@ struct efl_batch {
     std::vector<int> tile_start;
     cudaEvent_t ev[2] = {nullptr, nullptr};  // around the last batched solve
     bool timed = false;
+    GraphCache gc;  // the stages before and after the batched solve, all simulations
 };
 
 namespace {
@@ -1440,6 +1450,7 @@ void batch_free(efl_batch* b) {
     if (b->h_state) cudaFreeHost(b->h_state);
     for (cudaEvent_t e : b->ev)
         if (e) cudaEventDestroy(e);
+    b->gc.clear();
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
 }
@@ -1622,6 +1633,60 @@ efl_status efl_batch_step(efl_batch* b, float dt, efl_step_stats* stats) {
     std::vector<char> init_only(n, 0);
     efl_status ret = EFL_OK;
     auto fail = [&](efl_sim* s, efl_status st) { return batch_err(b, st, s->err); };
+    // Common case: every simulation initialised and solved by the batched
+    // solve.  The stages before and after it then run as two segments over
+    // all simulations (CUDA graphs once their arguments repeat).
+    bool fast = true;
+    for (size_t i = 0; i < n && fast; ++i) {
+        const efl_sim* s = b->sims[i];
+        const efl_projection& P = s->cfg.projection;
+        const efl_projection& Q = b->sims[0]->cfg.projection;
+        fast = s->status != 0 && P.method == EFL_PROJECTION_GAUSS_SEIDEL && P.tolerance > 0.0f &&
+               P.tolerance == Q.tolerance && P.max_iterations == Q.max_iterations &&
+               P.check_interval == Q.check_interval;
+    }
+    if (fast) {
+        uint64_t sig_pre = 1469598103934665603ull, sig_post = sig_pre;
+        for (efl_sim* s : b->sims) {
+            s->U.dt = dt;
+            sig_pre = fnv(sig_pre, segment_sig(s, SEG_PRE));
+            sig_post = fnv(sig_post, segment_sig(s, SEG_POST));
+        }
+        efl_status st = run_segment(b->gc, b->stream, sig_pre | 1, SEG_PRE, [&]() -> efl_status {
+            for (efl_sim* s : b->sims) {
+                efl_status r = run_stages(s, EFL_STAGE_UPDATE_SOLID, EFL_STAGE_DIVERGENCE, nullptr);
+                if (r != EFL_OK) return r;
+                const Level64& L = s->mg64[0];
+                k_widen<<<grid2d(s->nx, s->ny, kBlock), kBlock, count_launch(), s->stream>>>(s->p0, s->div, L.x, L.b);
+            }
+            return EFL_OK;
+        });
+        if (st != EFL_OK) return batch_err(b, st, "batched stages before the solve failed");
+        std::vector<int> all(n);
+        for (size_t i = 0; i < n; ++i) all[i] = (int)i;
+        std::vector<efl_step_stats> local;
+        if (!stats) {
+            local.resize(n);
+            for (auto& x : local) init_stats(&x);
+        }
+        efl_step_stats* sp = stats ? stats : local.data();
+        st = batch_solve(b, all, sp);
+        if (st != EFL_OK) return st;
+        for (size_t i = 0; i < n; ++i)
+            if (!sp[i].converged) ret = EFL_NOT_CONVERGED;
+        st = run_segment(b->gc, b->stream, sig_post | 1, SEG_POST, [&]() -> efl_status {
+            for (efl_sim* s : b->sims) {
+                k_narrow<<<grid2d(s->nx, s->ny, kBlock), kBlock, count_launch(), s->stream>>>(s->mg64[0].x, s->p0);
+                efl_status r = run_stages(s, EFL_STAGE_SOLVE_VELOCITY, EFL_STAGE_SOLID_FORCES, nullptr);
+                if (r != EFL_OK) return r;
+            }
+            return EFL_OK;
+        });
+        if (st != EFL_OK) return batch_err(b, st, "batched stages after the solve failed");
+        for (efl_sim* s : b->sims) s->n_forces = 0;
+        if (cudaGetLastError() != cudaSuccess) return batch_err(b, EFL_ERR_CUDA, "batch step launch failed");
+        return ret;
+    }
     for (size_t i = 0; i < n; ++i) {
         efl_sim* s = b->sims[i];
         if (s->status == 0) {

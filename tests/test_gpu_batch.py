@@ -77,3 +77,17 @@ def test_batch_rejects_bad_index(gpu_api):
         import ctypes as C
         h = C.c_void_p()
         assert gpu_api.batch_sim(batch.h, 5, C.byref(h)) == capi.ERR_INVALID_ARGUMENT
+
+
+def test_batch_fast_path_graphs_match_oracle(oracle_api, gpu_api):
+    """All members batched: the stages around the solve run as captured CUDA
+    graphs (recaptured when local forces appear, replayed after); every member
+    still equals the oracle alone."""
+    b = _small_batch(5, seed=0xC5)
+    oracles = [sc.make(oracle_api) for sc in b.scenes]
+    with capi.Batch(gpu_api, b.configs()) as batch:
+        b.setup(batch.sims)
+        _step_both(b, batch, oracles, 8)
+        for i, (g, o) in enumerate(zip(batch.sims, oracles)):
+            bad = compare_fields(g, o)
+            assert not bad, (i, bad)
