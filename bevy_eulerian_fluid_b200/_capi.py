@@ -135,11 +135,24 @@ SIGNATURES = {
     "batch_projection_ms": (C.c_int, [C.c_void_p, C.POINTER(C.c_float)]),
     "projection_ms": (C.c_int, ["X", C.POINTER(C.c_float)]),
     "set_graph_capture": (C.c_int, ["X", C.c_int32]),
+    "unet_create": (C.c_int, [C.c_int32, C.c_uint32, C.c_uint32, C.c_uint64, C.POINTER(C.c_void_p)]),
+    "unet_destroy": (C.c_int, [C.c_void_p]),
+    "unet_last_error": (C.c_char_p, [C.c_void_p]),
+    "unet_num_params": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
+    "unet_get_params": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64]),
+    "unet_set_params": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64]),
+    "unet_forward": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p]),
+    "unet_gradients": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p,
+                                 C.POINTER(C.c_float), C.c_void_p]),
+    "unet_attach": (C.c_int, ["X", C.c_void_p, C.c_uint32]),
+    "unet_train_step": (C.c_int, [C.c_void_p, C.c_float, C.POINTER(C.c_float)]),
 }
 # Functions of efl.h that the oracle restatement does not mirror.
 PRODUCT_ONLY = {"abi_version", "default_config", "field_device_ptr", "stream", "synchronize", "kernel_launches",
                 "pressure_sweeps", "residual_norms_noalloc", "batch_create", "batch_destroy", "batch_last_error",
-                "batch_sim", "batch_step", "batch_projection_ms", "projection_ms", "set_graph_capture"}
+                "batch_sim", "batch_step", "batch_projection_ms", "projection_ms", "set_graph_capture",
+                "unet_create", "unet_destroy", "unet_last_error", "unet_num_params", "unet_get_params",
+                "unet_set_params", "unet_forward", "unet_gradients", "unet_attach", "unet_train_step"}
 
 
 class EflError(RuntimeError):
@@ -426,3 +439,73 @@ class Batch:
 
     def __exit__(self, *a):
         self.close()
+
+
+UNET_WARM_START, UNET_RECORD = 1, 2
+
+
+class UNet:
+    """The learned warm start's network (efl_unet_*)."""
+
+    def __init__(self, api: Api, max_nx: int, max_ny: int, seed: int = 0, device: int = 0):
+        self.api = api
+        h = C.c_void_p()
+        st = api.unet_create(device, max_nx, max_ny, seed, C.byref(h))
+        if st != OK:
+            raise EflError(st, (api.unet_last_error(None) or b"").decode())
+        self.h = h
+        n = C.c_uint64()
+        self._check(api.unet_num_params(self.h, C.byref(n)))
+        self.n_params = n.value
+
+    def _check(self, st: int):
+        if st != OK:
+            raise EflError(st, (self.api.unet_last_error(self.h) or b"").decode())
+
+    def get_params(self) -> np.ndarray:
+        out = np.empty(self.n_params, np.float32)
+        self._check(self.api.unet_get_params(self.h, out.ctypes.data_as(C.c_void_p), self.n_params))
+        return out
+
+    def set_params(self, p: np.ndarray):
+        p = np.ascontiguousarray(p, np.float32)
+        assert p.size == self.n_params
+        self._check(self.api.unet_set_params(self.h, p.ctypes.data_as(C.c_void_p), self.n_params))
+
+    def forward(self, feats: np.ndarray) -> np.ndarray:
+        ny, nx = feats.shape[:2]
+        f = np.ascontiguousarray(feats, np.float32)
+        out = np.empty((ny, nx), np.float32)
+        self._check(self.api.unet_forward(self.h, nx, ny, f.ctypes.data_as(C.c_void_p), out.ctypes.data_as(C.c_void_p)))
+        return out
+
+    def gradients(self, feats, target, mask):
+        ny, nx = feats.shape[:2]
+        f = np.ascontiguousarray(feats, np.float32)
+        t = np.ascontiguousarray(target, np.float32)
+        m = np.ascontiguousarray(mask, np.uint8)
+        g = np.empty(self.n_params, np.float32)
+        loss = C.c_float()
+        self._check(self.api.unet_gradients(self.h, nx, ny, f.ctypes.data_as(C.c_void_p), t.ctypes.data_as(C.c_void_p),
+                                            m.ctypes.data_as(C.c_void_p), C.byref(loss), g.ctypes.data_as(C.c_void_p)))
+        return loss.value, g
+
+    def attach(self, sim: "Sim", warm_start: bool = True, record: bool = False):
+        flags = (UNET_WARM_START if warm_start else 0) | (UNET_RECORD if record else 0)
+        self._check(self.api.unet_attach(sim.h, self.h if flags else None, flags))
+
+    def train_step(self, lr: float = 1e-3) -> float:
+        loss = C.c_float()
+        self._check(self.api.unet_train_step(self.h, lr, C.byref(loss)))
+        return loss.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.api.unet_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

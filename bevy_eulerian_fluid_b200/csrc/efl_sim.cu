@@ -16,6 +16,7 @@
 #include <cstring>
 #include <string>
 #include <vector>
+#include <random>
 
 #include "../../include/efl.h"
 #include "efl_kernels.cuh"
@@ -23,6 +24,7 @@
 #include "efl_sweep_tma.cuh"
 #include "efl_batch.cuh"
 #include "efl_mgpcg.cuh"
+#include "efl_unet.cuh"
 
 using namespace efl;
 
@@ -50,6 +52,12 @@ struct DevBuf {
 };
 
 }  // namespace
+
+struct efl_unet {
+    UNet net;
+    int rec_nx = 0, rec_ny = 0;  // size of the recorded training sample (0: none)
+    double rec_scale = 0.0;
+};
 
 // Captured CUDA graphs of step segments, keyed by a signature of the
 // host-side values their kernels were launched with.
@@ -113,6 +121,8 @@ struct efl_sim {
     uint64_t graph_epoch = 1;     // counts the setters that change kernel arguments
     PF mix_d2{};       // second correction buffer (batched solve)
     bool owns_stream = true;
+    struct efl_unet* unet = nullptr;  // learned warm start / training recorder
+    uint32_t unet_flags = 0;
     int* h_err = nullptr;  // pinned copy of the TMA sweep's error flag
     cudaEvent_t ev_proj[2] = {nullptr, nullptr};  // around the last projection stage
     bool proj_timed = false;
@@ -173,6 +183,11 @@ efl_status alloc_raw(efl_sim* s, T*& p, size_t count) {
     return EFL_OK;
 }
 
+#define TRY_U(x)                       \
+    do {                               \
+        efl_status _s = (x);           \
+        if (_s != EFL_OK) return _s;   \
+    } while (0)
 #define TRY(x)                                  \
     do {                                        \
         efl_status st_ = (x);                   \
@@ -652,6 +667,40 @@ efl_status check_device_errors(efl_sim* s) {
     return EFL_OK;
 }
 
+// Learned warm start: the features of the system about to be solved, and
+// (when warm-starting) x += s * prediction on the fluid cells.
+double unet_scale(const efl_sim* s) {
+    const double g = std::sqrt((double)s->cfg.gravity[0] * s->cfg.gravity[0] +
+                               (double)s->cfg.gravity[1] * s->cfg.gravity[1]);
+    return (double)s->cfg.rho * (g > 0.0 ? g : 9.8) * (double)s->ny * (double)s->U.dx;
+}
+efl_status unet_before_solve(efl_sim* s) {
+    UNet& n = s->unet->net;
+    const Level64& L = s->mg64[0];
+    const dim3 g = grid2d(s->nx, s->ny, kBlock);
+    const double dx = (double)s->U.dx;
+    UnetFeatureArgs a{s->div, s->ls0, s->fu, s->fv, L.x, dx * dx * (double)s->U.rho / (double)s->U.dt,
+                      unet_scale(s), s->nx, s->ny};
+    k_unet_features<<<g, kBlock, count_launch(), s->stream>>>(a, n.X0, n.prev32, n.mask);
+    if (s->unet_flags & EFL_UNET_WARM_START) {
+        unet_forward(n, s->ny, s->nx, s->stream);
+        k_unet_warm<<<g, kBlock, count_launch(), s->stream>>>(L.x, n.out, n.mask, a.scale, s->nx, s->ny);
+    }
+    LAUNCH_CHECK();
+    return EFL_OK;
+}
+efl_status unet_after_solve(efl_sim* s) {
+    UNet& n = s->unet->net;
+    const double scale = unet_scale(s);
+    k_unet_target<<<grid2d(s->nx, s->ny, kBlock), kBlock, count_launch(), s->stream>>>(s->mg64[0].x, n.prev32, scale,
+                                                                                      s->nx, s->ny, n.target);
+    LAUNCH_CHECK();
+    s->unet->rec_nx = s->nx;
+    s->unet->rec_ny = s->ny;
+    s->unet->rec_scale = scale;
+    return EFL_OK;
+}
+
 // projection.rs:89-164.  tolerance > 0 (an extension) solves to
 // ||b - A p|| / ||b|| <= tolerance with an FP64 iterate: an f32 pressure
 // cannot represent a solution that accurate when hydrostatic pressure
@@ -683,6 +732,7 @@ efl_status st_projection(efl_sim* s, efl_step_stats* st) {
         dim3 g = grid2d(d.nx, d.ny, kBlock);
         k_widen<<<g, kBlock, count_launch(), s->stream>>>(s->p0, s->div, L.x, L.b);
         LAUNCH_CHECK();
+        if (s->unet && s->unet_flags) TRY(unet_before_solve(s));
         double r = -1.0;
         bool done = false;
         if (P.method == EFL_PROJECTION_GAUSS_SEIDEL || P.method == EFL_PROJECTION_MGPCG) {
@@ -707,6 +757,7 @@ efl_status st_projection(efl_sim* s, efl_step_stats* st) {
         }
         r1 = r;
         conv = r <= (double)P.tolerance;
+        if (s->unet && (s->unet_flags & EFL_UNET_RECORD)) TRY(unet_after_solve(s));
         k_narrow<<<g, kBlock, count_launch(), s->stream>>>(L.x, s->p0);
         LAUNCH_CHECK();
     }
@@ -1741,6 +1792,206 @@ efl_status efl_batch_step(efl_batch* b, float dt, efl_step_stats* stats) {
     }
     if (cudaGetLastError() != cudaSuccess) return batch_err(b, EFL_ERR_CUDA, "batch step launch failed");
     return ret;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// The learned warm start's network.
+
+namespace {
+std::string g_unet_error;
+efl_status unet_err(efl_unet* u, efl_status st, const std::string& m) {
+    if (u) u->net.last_error = m;
+    else g_unet_error = m;
+    return st;
+}
+// Sets up the kernels' shared-memory limits once per device.
+bool unet_kernel_attrs() {
+    return cudaFuncSetAttribute(k_conv3x3_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, CV_SMEM) == cudaSuccess &&
+           cudaFuncSetAttribute(k_wgrad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, WG_SMEM) == cudaSuccess;
+}
+efl_status unet_finish(efl_unet* u, cudaStream_t st) {
+    if (cudaStreamSynchronize(st) != cudaSuccess)
+        return unet_err(u, EFL_ERR_CUDA, std::string("network kernels failed: ") + cudaGetErrorString(cudaGetLastError()));
+    int e = 0;
+    cudaMemcpy(&e, u->net.err, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e) {
+        cudaMemset(u->net.err, 0, sizeof(int));
+        return unet_err(u, EFL_ERR_CUDA, "a tensor-core MMA did not complete (bounded wait gave up)");
+    }
+    return EFL_OK;
+}
+__global__ void k_f32_to_bf16(const float* a, size_t n, bf16* b) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) b[i] = __float2bfloat16_rn(a[i]);
+}
+__global__ void k_copy_f32(const float* a, size_t n, size_t stride, float* b) {  // channel 0 of [n][stride]
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) b[i] = a[i * stride];
+}
+// Loss on the sample in X0/target/mask; fills g_out, returns the mean squared error.
+efl_status unet_loss_and_grads(efl_unet* u, int H, int W, cudaStream_t st, float* loss) {
+    UNet& n = u->net;
+    const int npix = H * W;
+    cudaMemsetAsync(n.count, 0, sizeof(unsigned int), st);
+    k_mask_count<<<(npix + 255) / 256, 256, count_launch(), st>>>(n.mask, npix, n.count);
+    unsigned int cnt = 0;
+    cudaMemcpyAsync(&cnt, n.count, sizeof(cnt), cudaMemcpyDeviceToHost, st);
+    unet_forward(n, H, W, st);
+    TRY_U(unet_finish(u, st));
+    const int blocks = (npix + 1023) / 1024;
+    k_unet_loss<<<blocks, 256, count_launch(), st>>>(n.out, n.target, n.mask, npix, 1024,
+                                                       cnt ? 1.0f / (float)cnt : 0.0f, n.g_out, n.lpart);
+    unet_backward(n, H, W, st);
+    std::vector<float2> part(blocks);
+    cudaMemcpyAsync(part.data(), n.lpart, blocks * sizeof(float2), cudaMemcpyDeviceToHost, st);
+    TRY_U(unet_finish(u, st));
+    double se = 0.0;
+    for (auto& q : part) se += q.x;
+    *loss = cnt ? (float)(se / cnt) : 0.0f;
+    return EFL_OK;
+}
+}  // namespace
+
+extern "C" {
+
+efl_status efl_unet_create(int32_t device, uint32_t max_nx, uint32_t max_ny, uint64_t seed, efl_unet** out) {
+    if (!out) return unet_err(nullptr, EFL_ERR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    if (max_nx < 16 || max_ny < 16 || max_nx % 8 || max_ny % 8 || max_nx > 4096 || max_ny > 4096)
+        return unet_err(nullptr, EFL_ERR_INVALID_ARGUMENT, "network grid must be a multiple of 8 in [16, 4096]");
+    if (cudaSetDevice(device) != cudaSuccess) return unet_err(nullptr, EFL_ERR_NO_DEVICE, "no such CUDA device");
+    if (!unet_kernel_attrs()) return unet_err(nullptr, EFL_ERR_CUDA, "tensor-core kernels unavailable on this device");
+    efl_unet* u = new efl_unet();
+    u->net.device = device;
+    if (unet_alloc(u->net, (int)max_ny, (int)max_nx) != cudaSuccess) {
+        if (u->net.arena) cudaFree(u->net.arena);
+        delete u;
+        return unet_err(nullptr, EFL_ERR_OUT_OF_MEMORY, "network allocation failed");
+    }
+    // He-normal weights for the ReLU layers, a zero head (the warm start
+    // begins as the previous pressure), zero biases.
+    std::vector<float> h(u->net.nparams, 0.0f);
+    std::mt19937_64 rng(seed);
+    for (int i = 0; i < UNET_NCONV; ++i) {
+        if (!kUnetSpec[i].relu) continue;
+        std::normal_distribution<float> nd(0.0f, std::sqrt(2.0f / (9.0f * kUnetSpec[i].cin)));
+        for (size_t k = 0; k < (size_t)9 * kUnetSpec[i].cin * kUnetSpec[i].cout; ++k) h[u->net.woff[i] + k] = nd(rng);
+    }
+    cudaMemcpy(u->net.params, h.data(), h.size() * 4, cudaMemcpyHostToDevice);
+    unet_sync_weights(u->net, 0);
+    if (cudaDeviceSynchronize() != cudaSuccess) {
+        cudaFree(u->net.arena);
+        delete u;
+        return unet_err(nullptr, EFL_ERR_CUDA, "network initialisation failed");
+    }
+    *out = u;
+    return EFL_OK;
+}
+
+efl_status efl_unet_destroy(efl_unet* u) {
+    if (!u) return EFL_OK;
+    cudaSetDevice(u->net.device);
+    cudaDeviceSynchronize();
+    cudaFree(u->net.arena);
+    delete u;
+    return EFL_OK;
+}
+
+const char* efl_unet_last_error(const efl_unet* u) { return u ? u->net.last_error.c_str() : g_unet_error.c_str(); }
+
+efl_status efl_unet_num_params(const efl_unet* u, uint64_t* n) {
+    if (!u || !n) return unet_err(nullptr, EFL_ERR_INVALID_ARGUMENT, "null argument");
+    *n = u->net.nparams;
+    return EFL_OK;
+}
+
+efl_status efl_unet_get_params(efl_unet* u, float* host, uint64_t n) {
+    if (!u || !host || n != u->net.nparams) return unet_err(u, EFL_ERR_INVALID_ARGUMENT, "bad parameter buffer");
+    cudaSetDevice(u->net.device);
+    if (cudaMemcpy(host, u->net.params, n * 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return unet_err(u, EFL_ERR_CUDA, "copy failed");
+    return EFL_OK;
+}
+
+efl_status efl_unet_set_params(efl_unet* u, const float* host, uint64_t n) {
+    if (!u || !host || n != u->net.nparams) return unet_err(u, EFL_ERR_INVALID_ARGUMENT, "bad parameter buffer");
+    cudaSetDevice(u->net.device);
+    if (cudaMemcpy(u->net.params, host, n * 4, cudaMemcpyHostToDevice) != cudaSuccess)
+        return unet_err(u, EFL_ERR_CUDA, "copy failed");
+    unet_sync_weights(u->net, 0);
+    cudaMemset(u->net.adam_m, 0, n * 4);
+    cudaMemset(u->net.adam_v, 0, n * 4);
+    u->net.adam_t = 0;
+    return unet_finish(u, 0);
+}
+
+// Host features [ny][nx][16] into X0 (the network's input).
+static efl_status unet_upload_features(efl_unet* u, uint32_t nx, uint32_t ny, const float* features) {
+    UNet& n = u->net;
+    if (nx < 16 || ny < 16 || nx % 8 || ny % 8 || (int)nx > n.maxW || (int)ny > n.maxH)
+        return unet_err(u, EFL_ERR_INVALID_ARGUMENT, "grid larger than the network was created for, or not a multiple of 8");
+    const size_t cnt = (size_t)nx * ny * 16;
+    if (cudaMemcpy(n.g_out, features, cnt * 4, cudaMemcpyHostToDevice) != cudaSuccess)
+        return unet_err(u, EFL_ERR_CUDA, "copy failed");
+    k_f32_to_bf16<<<lin_grid(cnt), 256, count_launch(), 0>>>(n.g_out, cnt, n.X0);
+    return EFL_OK;
+}
+
+efl_status efl_unet_forward(efl_unet* u, uint32_t nx, uint32_t ny, const float* features, float* pred) {
+    if (!u || !features || !pred) return unet_err(u, EFL_ERR_INVALID_ARGUMENT, "null argument");
+    cudaSetDevice(u->net.device);
+    TRY_U(unet_upload_features(u, nx, ny, features));
+    unet_forward(u->net, (int)ny, (int)nx, 0);
+    const size_t np = (size_t)nx * ny;
+    k_copy_f32<<<lin_grid(np), 256, count_launch(), 0>>>(u->net.out, np, 16, u->net.target);
+    TRY_U(unet_finish(u, 0));
+    if (cudaMemcpy(pred, u->net.target, np * 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return unet_err(u, EFL_ERR_CUDA, "copy failed");
+    return EFL_OK;
+}
+
+efl_status efl_unet_gradients(efl_unet* u, uint32_t nx, uint32_t ny, const float* features, const float* target,
+                              const uint8_t* mask, float* loss, float* grads) {
+    if (!u || !features || !target || !mask || !loss || !grads)
+        return unet_err(u, EFL_ERR_INVALID_ARGUMENT, "null argument");
+    cudaSetDevice(u->net.device);
+    TRY_U(unet_upload_features(u, nx, ny, features));
+    const size_t np = (size_t)nx * ny;
+    cudaMemcpy(u->net.target, target, np * 4, cudaMemcpyHostToDevice);
+    cudaMemcpy(u->net.mask, mask, np, cudaMemcpyHostToDevice);
+    TRY_U(unet_loss_and_grads(u, (int)ny, (int)nx, 0, loss));
+    if (cudaMemcpy(grads, u->net.grads, u->net.nparams * 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return unet_err(u, EFL_ERR_CUDA, "copy failed");
+    return EFL_OK;
+}
+
+efl_status efl_unet_attach(efl_sim* s, efl_unet* u, uint32_t flags) {
+    if (!s) return unet_err(u, EFL_ERR_INVALID_ARGUMENT, "null sim");
+    if (u && (s->nx > u->net.maxW || s->ny > u->net.maxH || s->cfg.device != u->net.device))
+        return unet_err(u, EFL_ERR_INVALID_ARGUMENT, "simulation larger than the network, or on another device");
+    s->unet = flags ? u : nullptr;
+    s->unet_flags = u ? flags : 0;
+    return EFL_OK;
+}
+
+efl_status efl_unet_train_step(efl_unet* u, float lr, float* loss) {
+    if (!u || !loss) return unet_err(u, EFL_ERR_INVALID_ARGUMENT, "null argument");
+    if (!u->rec_nx) return unet_err(u, EFL_ERR_STATE, "no training sample recorded (attach with EFL_UNET_RECORD and step)");
+    cudaSetDevice(u->net.device);
+    UNet& n = u->net;
+    // The sample was written on the simulation's stream: wait for it.
+    if (cudaDeviceSynchronize() != cudaSuccess)
+        return unet_err(u, EFL_ERR_CUDA, std::string("device error: ") + cudaGetErrorString(cudaGetLastError()));
+    TRY_U(unet_loss_and_grads(u, u->rec_ny, u->rec_nx, 0, loss));
+    ++n.adam_t;
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = 1.0f - std::pow(b1, (float)n.adam_t), c2 = 1.0f - std::pow(b2, (float)n.adam_t);
+    k_adam<<<lin_grid(n.nparams), 256, count_launch(), 0>>>(n.params, n.grads, n.adam_m, n.adam_v, (int)n.nparams,
+                                                             lr, b1, b2, 1e-8f, c1, c2);
+    unet_sync_weights(n, 0);
+    return unet_finish(u, 0);
 }
 
 }  // extern "C"

@@ -1,0 +1,751 @@
+// efl_unet.cuh — the learned warm start (an extension with no reference
+// counterpart): a small U-Net in BF16 with FP32 accumulation whose 3x3
+// convolutions run on the 5th-generation tensor cores (tcgen05.mma,
+// kind::f16, operands in shared memory, accumulator in tensor memory).
+//
+// Activations are NHWC bf16 with the channel count a multiple of 16; a tensor
+// may be a channel slice (stride, offset) of a wider one, which is how the
+// skip connections are concatenated without copies.  Weights are bf16
+// [tap = 9][cout][cin] (tap = (dy + 1) * 3 + (dx + 1)); biases fp32.
+//
+// One convolution = one implicit GEMM per CTA: 128 consecutive output pixels
+// (M = 128) x cout (N), accumulated over 9 taps x cin / 16 MMAs of K = 16.
+// Operand tiles use the canonical K-major, non-swizzled core-matrix layout
+// (8 rows x 16 bytes per core matrix, core matrices along K 128 bytes apart
+// (LBO), along M/N (K/8) * 128 bytes apart (SBO)).  The backward pass over
+// the data is the same kernel with the weights flipped in space and
+// transposed; the weight gradient is a second tcgen05 GEMM whose reduction
+// dimension is the pixels.  Every wait on an mbarrier is bounded.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "efl_sweep_tma.cuh"
+
+namespace efl {
+
+using bf16 = __nv_bfloat16;
+
+// ---------------------------------------------------------------------------
+// tcgen05 helpers
+
+// Shared-memory matrix descriptor: start address, leading (K) and stride
+// (M/N) byte offsets in 16-byte units, version 1, no swizzle.
+EFL_DEV uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1 << 46;
+    return d;
+}
+// Instruction descriptor of kind::f16: D f32, A and B bf16, both K-major.
+__host__ __device__ constexpr uint32_t umma_idesc_bf16(int m, int n) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
+}
+EFL_DEV void umma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
+        "l"(da), "l"(db), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+        : "memory");
+}
+EFL_DEV void umma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+EFL_DEV void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+EFL_DEV void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+EFL_DEV void tmem_alloc(uint32_t* dst_smem, uint32_t ncols) {  // whole warp
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(dst_smem)),
+                 "r"(ncols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+EFL_DEV void tmem_dealloc(uint32_t taddr, uint32_t ncols) {  // whole warp
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+// 16 consecutive fp32 columns of this thread's TMEM lane.
+EFL_DEV void tmem_ld16(uint32_t taddr, float* v) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+__host__ __device__ constexpr uint32_t tmem_cols(int n) { return n <= 32 ? 32u : n <= 64 ? 64u : n <= 128 ? 128u : 256u; }
+
+// Byte offset of element (row, k) in a K-major non-swizzled tile with K columns.
+EFL_DEV uint32_t kmajor_off(int row, int k, int K) {
+    return (uint32_t)((row >> 3) * (K >> 3) * 128 + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2);
+}
+
+// ---------------------------------------------------------------------------
+// 3x3 convolution, stride 1, zero padding.
+
+constexpr int CV_THREADS = 128, CV_MAX_CIN = 128, CV_MAX_COUT = 128;
+constexpr int CV_SMEM = 128 * CV_MAX_CIN * 2 + CV_MAX_COUT * CV_MAX_CIN * 2 + 64;
+
+struct ConvArgs {
+    const bf16* x;  // input [H*W][xs], channels [xo, xo + cin)
+    int xs, xo;
+    const bf16* w;       // [9][cout][cin]
+    const float* bias;   // [cout] or null
+    bf16* y;             // bf16 output [H*W][ys] at [yo, yo + cout), or null
+    int ys, yo;
+    float* yf;           // fp32 output [H*W][ys] at [yo, yo + cout) (used when y is null)
+    int relu;
+    int H, W, cin, cout;
+    int* err;
+};
+
+__global__ void __launch_bounds__(CV_THREADS) k_conv3x3_tc(ConvArgs a) {
+    extern __shared__ __align__(128) unsigned char cv_smem[];
+    unsigned char* As = cv_smem;                        // 128 x cin
+    unsigned char* Bs = cv_smem + 128 * CV_MAX_CIN * 2;  // cout x cin
+    uint64_t* bar = reinterpret_cast<uint64_t*>(cv_smem + 128 * CV_MAX_CIN * 2 + CV_MAX_COUT * CV_MAX_CIN * 2);
+    __shared__ uint32_t s_tmem;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int npix = a.H * a.W, p0 = blockIdx.x * 128;
+    const uint32_t ncols = tmem_cols(a.cout);
+    if (warp == 0) tmem_alloc(&s_tmem, ncols);
+    if (tid == 0) {
+        mbar_init(bar, 1);
+        fence_mbar_init();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = s_tmem;
+    const uint32_t idesc = umma_idesc_bf16(128, a.cout);
+    const int kg = a.cin >> 3;  // 16-byte groups per row
+    const uint32_t sbo_a = (uint32_t)kg * 128, sbo_b = sbo_a;
+    const int m = tid, p = p0 + m;
+    const int py = p / a.W, px = p - py * a.W;
+    bool ok = true;
+    for (int tap = 0; tap < 9 && ok; ++tap) {
+        const int dy = tap / 3 - 1, dx = tap % 3 - 1;
+        const int sy = py + dy, sx = px + dx;
+        const bool valid = p < npix && (unsigned)sy < (unsigned)a.H && (unsigned)sx < (unsigned)a.W;
+        const uint4* src = reinterpret_cast<const uint4*>(a.x + (size_t)(valid ? sy * a.W + sx : 0) * a.xs + a.xo);
+        for (int j = 0; j < kg; ++j) {
+            const uint4 v = valid ? __ldg(src + j) : make_uint4(0u, 0u, 0u, 0u);
+            *reinterpret_cast<uint4*>(As + kmajor_off(m, 8 * j, a.cin)) = v;
+        }
+        const uint4* wsrc = reinterpret_cast<const uint4*>(a.w + (size_t)tap * a.cout * a.cin);
+        for (int c = tid; c < a.cout * kg; c += CV_THREADS) {
+            const int n = c / kg, j = c - n * kg;
+            *reinterpret_cast<uint4*>(Bs + kmajor_off(n, 8 * j, a.cin)) = __ldg(wsrc + c);
+        }
+        fence_proxy_async();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+            const uint32_t sa = smem_u32(As), sb = smem_u32(Bs);
+            for (int kc = 0; kc < (a.cin >> 4); ++kc)
+                umma_bf16(tmem, umma_desc(sa + kc * 256, 128, sbo_a), umma_desc(sb + kc * 256, 128, sbo_b), idesc,
+                          (tap | kc) != 0);
+            umma_commit(bar);
+        }
+        ok = mbar_wait(bar, tap & 1);
+        if (__syncthreads_or(!ok)) ok = false;
+    }
+    if (!ok) {
+        if (tid == 0) atomicExch(a.err, 1);
+        mbar_wait(bar, 0);  // give outstanding MMAs a last bounded chance before releasing TMEM
+    }
+    tc_fence_after();
+    if (ok) {
+        const int row = 32 * warp + lane, pp = p0 + row;
+        const uint32_t taddr = tmem + ((uint32_t)(32 * warp) << 16);
+        for (int c0 = 0; c0 < a.cout; c0 += 16) {
+            float v[16];
+            tmem_ld16(taddr + (uint32_t)c0, v);
+            if (pp >= npix) continue;
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+                float t = v[i] + (a.bias ? a.bias[c0 + i] : 0.0f);
+                if (a.relu) t = fmaxf(t, 0.0f);
+                v[i] = t;
+            }
+            if (a.y) {
+                __align__(16) bf16 o[16];
+#pragma unroll
+                for (int i = 0; i < 16; ++i) o[i] = __float2bfloat16_rn(v[i]);
+                uint4* dst = reinterpret_cast<uint4*>(a.y + (size_t)pp * a.ys + a.yo + c0);
+                dst[0] = reinterpret_cast<const uint4*>(o)[0];
+                dst[1] = reinterpret_cast<const uint4*>(o)[1];
+            } else {
+                float* dst = a.yf + (size_t)pp * a.ys + a.yo + c0;
+#pragma unroll
+                for (int i = 0; i < 16; ++i) dst[i] = v[i];
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(tmem, ncols);
+}
+
+// ---------------------------------------------------------------------------
+// Weight gradient: dW[tap][co][ci] = sum_p dy[p][co] * x[p + tap][ci].
+// GEMM D[(tap, ci)][co] over K = pixels: A rows r = tap * cin + ci (M tiles of
+// 128 rows; rows beyond 9 * cin are zero), B rows co.  Each CTA reduces one
+// chunk of pixels for one M tile and writes its partial D; k_wgrad_reduce
+// sums the chunks in order.
+
+constexpr int WG_THREADS = 128, WG_K = 64;  // pixels per staged block
+constexpr int WG_SMEM = 128 * WG_K * 2 + CV_MAX_COUT * WG_K * 2 + 64;
+
+struct WgradArgs {
+    const bf16* x;  // forward input [H*W][xs] at xo
+    int xs, xo;
+    const bf16* dy;  // [H*W][cout] dense
+    int H, W, cin, cout;
+    int pix_per_cta;  // multiple of WG_K
+    float* part;      // [chunks][mtiles][128][cout]
+    int* err;
+};
+
+__global__ void __launch_bounds__(WG_THREADS) k_wgrad_tc(WgradArgs a) {
+    extern __shared__ __align__(128) unsigned char wg_smem[];
+    unsigned char* As = wg_smem;                  // 128 x WG_K
+    unsigned char* Bs = wg_smem + 128 * WG_K * 2;  // cout x WG_K
+    uint64_t* bar = reinterpret_cast<uint64_t*>(wg_smem + 128 * WG_K * 2 + CV_MAX_COUT * WG_K * 2);
+    __shared__ uint32_t s_tmem;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int npix = a.H * a.W;
+    const int chunk = blockIdx.x, tile = blockIdx.y, mtiles = gridDim.y;
+    const uint32_t ncols = tmem_cols(a.cout);
+    if (warp == 0) tmem_alloc(&s_tmem, ncols);
+    if (tid == 0) {
+        mbar_init(bar, 1);
+        fence_mbar_init();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = s_tmem;
+    const uint32_t idesc = umma_idesc_bf16(128, a.cout);
+    const uint32_t sbo = (WG_K / 8) * 128;
+    const int cg = a.cin >> 3, og = a.cout >> 3;
+    const int pbeg = chunk * a.pix_per_cta, pend = min(npix, pbeg + a.pix_per_cta);
+    bool ok = true;
+    int stage = 0;
+    for (int pb = pbeg; pb < pend && ok; pb += WG_K, ++stage) {
+        // A: 16 row groups of 8 (tap, ci) rows x WG_K pixels; one 16-byte load = 8 channels of one pixel.
+        for (int i = tid; i < 16 * WG_K; i += WG_THREADS) {
+            const int g = i / WG_K, k = i - g * WG_K;
+            const int r0 = tile * 128 + 8 * g;  // first row of the group
+            const int tap = r0 / a.cin, ci0 = r0 - tap * a.cin;
+            const int pp = pb + k;
+            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+            if (tap < 9 && pp < pend) {
+                const int py = pp / a.W, px = pp - py * a.W;
+                const int sy = py + tap / 3 - 1, sx = px + tap % 3 - 1;
+                if ((unsigned)sy < (unsigned)a.H && (unsigned)sx < (unsigned)a.W)
+                    v = __ldg(reinterpret_cast<const uint4*>(a.x + (size_t)(sy * a.W + sx) * a.xs + a.xo + ci0));
+            }
+            const bf16* e = reinterpret_cast<const bf16*>(&v);
+#pragma unroll
+            for (int q = 0; q < 8; ++q) *reinterpret_cast<bf16*>(As + kmajor_off(8 * g + q, k, WG_K)) = e[q];
+        }
+        // B: cout rows x WG_K pixels.
+        for (int i = tid; i < og * WG_K; i += WG_THREADS) {
+            const int g = i / WG_K, k = i - g * WG_K;
+            const int pp = pb + k;
+            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+            if (pp < pend) v = __ldg(reinterpret_cast<const uint4*>(a.dy + (size_t)pp * a.cout + 8 * g));
+            const bf16* e = reinterpret_cast<const bf16*>(&v);
+#pragma unroll
+            for (int q = 0; q < 8; ++q) *reinterpret_cast<bf16*>(Bs + kmajor_off(8 * g + q, k, WG_K)) = e[q];
+        }
+        fence_proxy_async();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+            const uint32_t sa = smem_u32(As), sb = smem_u32(Bs);
+            for (int kc = 0; kc < WG_K / 16; ++kc)
+                umma_bf16(tmem, umma_desc(sa + kc * 256, 128, sbo), umma_desc(sb + kc * 256, 128, sbo), idesc,
+                          (stage | kc) != 0);
+            umma_commit(bar);
+        }
+        ok = mbar_wait(bar, stage & 1);
+        if (__syncthreads_or(!ok)) ok = false;
+    }
+    if (!ok) {
+        if (tid == 0) atomicExch(a.err, 1);
+        mbar_wait(bar, 0);
+    }
+    tc_fence_after();
+    const int row = 32 * warp + lane;
+    float* dst = a.part + (((size_t)chunk * mtiles + tile) * 128 + row) * a.cout;
+    const uint32_t taddr = tmem + ((uint32_t)(32 * warp) << 16);
+    for (int c0 = 0; c0 < a.cout; c0 += 16) {
+        float v[16];
+        tmem_ld16(taddr + (uint32_t)c0, v);
+#pragma unroll
+        for (int i = 0; i < 16; ++i) dst[c0 + i] = (ok && stage > 0) ? v[i] : 0.0f;
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(tmem, ncols);
+}
+
+// dw[tap][co][ci] = sum over chunks in order of part[chunk][tile][r][co], r = tap * cin + ci - 128 * tile.
+__global__ void k_wgrad_reduce(const float* part, int chunks, int mtiles, int cin, int cout, float* dw) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;  // over 9 * cout * cin
+    if (i >= 9 * cout * cin) return;
+    const int tap = i / (cout * cin), rem = i - tap * cout * cin, co = rem / cin, ci = rem - co * cin;
+    const int r = tap * cin + ci, tile = r >> 7, row = r & 127;
+    float s = 0.0f;
+    for (int c = 0; c < chunks; ++c) s += part[(((size_t)c * mtiles + tile) * 128 + row) * cout + co];
+    dw[i] = s;
+}
+
+// db[co] = sum over pixels of dy[p][co] (per-block partials, then in order).
+__global__ void k_bgrad_partial(const bf16* dy, int npix, int cout, int pix_per_block, float* part) {
+    const int co = threadIdx.x;
+    if (co >= cout) return;
+    const int p0 = blockIdx.x * pix_per_block, p1 = min(npix, p0 + pix_per_block);
+    float s = 0.0f;
+    for (int p = p0; p < p1; ++p) s += __bfloat162float(dy[(size_t)p * cout + co]);
+    part[(size_t)blockIdx.x * cout + co] = s;
+}
+__global__ void k_bgrad_reduce(const float* part, int blocks, int cout, float* db) {
+    const int co = threadIdx.x;
+    if (co >= cout) return;
+    float s = 0.0f;
+    for (int b = 0; b < blocks; ++b) s += part[(size_t)b * cout + co];
+    db[co] = s;
+}
+
+// ---------------------------------------------------------------------------
+// Elementwise parts of the network.
+
+// out[Y, X] = mean of the 2x2 block of in (bf16, fp32 sum).
+__global__ void k_pool2(const bf16* in, int is, int io, int H, int W, int C, bf16* out) {
+    const int h = H / 2, w = W / 2;
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (size_t)h * w * C) return;
+    const int c = (int)(i % C);
+    const int q = (int)(i / C), Y = q / w, X = q - Y * w;
+    auto at = [&](int y, int x) { return __bfloat162float(in[(size_t)(y * W + x) * is + io + c]); };
+    const float s = ((at(2 * Y, 2 * X) + at(2 * Y, 2 * X + 1)) + at(2 * Y + 1, 2 * X)) + at(2 * Y + 1, 2 * X + 1);
+    out[(size_t)q * C + c] = __float2bfloat16_rn(0.25f * s);
+}
+// g_in[2Y+i, 2X+j] += g_out[Y, X] / 4 (fp32 gradients; g_in is a channel slice).
+__global__ void k_pool2_bwd(const float* gout, int H, int W, int C, float* gin, int gs, int go) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (size_t)H * W * C) return;
+    const int c = (int)(i % C);
+    const int q = (int)(i / C), y = q / W, x = q - y * W;
+    const int w = W / 2;
+    gin[(size_t)q * gs + go + c] += 0.25f * gout[(size_t)((y >> 1) * w + (x >> 1)) * C + c];
+}
+// out slice [y, x] = in[y / 2, x / 2] (nearest upsampling into a channel slice).
+__global__ void k_up2(const bf16* in, int H, int W, int C, bf16* out, int os, int oo) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (size_t)H * W * C) return;
+    const int c = (int)(i % C);
+    const int q = (int)(i / C), y = q / W, x = q - y * W;
+    out[(size_t)q * os + oo + c] = in[(size_t)((y >> 1) * (W / 2) + (x >> 1)) * C + c];
+}
+// g_in[Y, X] = sum of the 2x2 block of g_out's channel slice.
+__global__ void k_up2_bwd(const float* gout, int gs, int go, int H, int W, int C, float* gin) {
+    const int h = H / 2, w = W / 2;
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (size_t)h * w * C) return;
+    const int c = (int)(i % C);
+    const int q = (int)(i / C), Y = q / w, X = q - Y * w;
+    auto at = [&](int y, int x) { return gout[(size_t)(y * W + x) * gs + go + c]; };
+    gin[(size_t)q * C + c] = ((at(2 * Y, 2 * X) + at(2 * Y, 2 * X + 1)) + at(2 * Y + 1, 2 * X)) + at(2 * Y + 1, 2 * X + 1);
+}
+// dy = bf16(g) where the forward output y > 0 (relu) or everywhere (relu = 0).
+__global__ void k_relu_bwd(const float* g, int gs, int go, const bf16* y, int ys, int yo, int npix, int C, int relu,
+                           bf16* dy) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (size_t)npix * C) return;
+    const int c = (int)(i % C);
+    const size_t p = i / C;
+    float v = g[p * gs + go + c];
+    if (relu && !(__bfloat162float(y[p * ys + yo + c]) > 0.0f)) v = 0.0f;
+    dy[i] = __float2bfloat16_rn(v);
+}
+// Weights for the backward pass over the data: wt[tap'][ci][co] = w[8 - tap'][co][ci].
+__global__ void k_flip_transpose(const float* w32, int cin, int cout, bf16* w16, bf16* wt16) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= 9 * cin * cout) return;
+    const int tap = i / (cout * cin), rem = i - tap * cout * cin, co = rem / cin, ci = rem - co * cin;
+    const bf16 v = __float2bfloat16_rn(w32[i]);
+    w16[i] = v;
+    wt16[((size_t)(8 - tap) * cin + ci) * cout + co] = v;
+}
+// Adam (decoupled from the loss scale), fp32 master parameters.
+__global__ void k_adam(float* p, const float* g, float* m, float* v, int n, float lr, float b1, float b2, float eps,
+                       float c1, float c2) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1.0f - b1) * gi;
+    const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+}
+
+}  // namespace efl
+
+namespace efl {
+
+// ---------------------------------------------------------------------------
+// Features of one pressure system and the warm start.
+//
+// Channels (16, zero beyond 5): 0 = cdiv * div / s (the right-hand side in
+// pressure units), 1 / 2 = the u / v face fractions averaged to the cell
+// centre, 3 = phi / ny clamped to [-1, 1], 4 = the previous pressure / s;
+// s = rho * g * ny * dx, the hydrostatic pressure of a full column.  The
+// network predicts the change of the pressure over the step, (p - p_prev) / s.
+
+EFL_DEV float warp_sum_f(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+struct UnetFeatureArgs {
+    PF div, ls, fu, fv;
+    Plane<double> prev;  // the solve's start iterate (previous pressure, widened)
+    double cdiv, scale;
+    int nx, ny;
+};
+__global__ void k_unet_features(UnetFeatureArgs a, bf16* x0, float* prev32, unsigned char* mask) {
+    const int gx = blockIdx.x * blockDim.x + threadIdx.x, gy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (gx >= a.nx || gy >= a.ny) return;
+    const size_t p = (size_t)gy * a.nx + gx;
+    const float phi = a.ls.at(gx, gy);
+    const float f0 = a.fu.at(gx, gy), f1 = a.fu.at(gx + 1, gy), f2 = a.fv.at(gx, gy), f3 = a.fv.at(gx, gy + 1);
+    const double pv = a.prev.at(gx, gy);
+    __align__(16) bf16 v[16];
+#pragma unroll
+    for (int c = 0; c < 16; ++c) v[c] = __float2bfloat16_rn(0.0f);
+    v[0] = __float2bfloat16_rn((float)(a.cdiv * (double)a.div.at(gx, gy) / a.scale));
+    v[1] = __float2bfloat16_rn(0.5f * (f0 + f1));
+    v[2] = __float2bfloat16_rn(0.5f * (f2 + f3));
+    v[3] = __float2bfloat16_rn(fminf(1.0f, fmaxf(-1.0f, phi / (float)a.ny)));
+    v[4] = __float2bfloat16_rn((float)(pv / a.scale));
+    uint4* dst = reinterpret_cast<uint4*>(x0 + p * 16);
+    dst[0] = reinterpret_cast<const uint4*>(v)[0];
+    dst[1] = reinterpret_cast<const uint4*>(v)[1];
+    prev32[p] = (float)pv;
+    mask[p] = (phi < 0.0f && !(f0 == 0.0f && f1 == 0.0f && f2 == 0.0f && f3 == 0.0f)) ? 1 : 0;
+}
+// x += s * prediction on the masked cells (the solve's start iterate).
+__global__ void k_unet_warm(Plane<double> x, const float* out16, const unsigned char* mask, double scale, int nx,
+                            int ny) {
+    const int gx = blockIdx.x * blockDim.x + threadIdx.x, gy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (gx >= nx || gy >= ny) return;
+    const size_t p = (size_t)gy * nx + gx;
+    if (mask[p]) x.at(gx, gy) = x.at(gx, gy) + scale * (double)out16[p * 16];
+}
+// Training target after the solve: (p - p_prev) / s.
+__global__ void k_unet_target(Plane<double> x, const float* prev32, double scale, int nx, int ny, float* target) {
+    const int gx = blockIdx.x * blockDim.x + threadIdx.x, gy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (gx >= nx || gy >= ny) return;
+    const size_t p = (size_t)gy * nx + gx;
+    target[p] = (float)((x.at(gx, gy) - (double)prev32[p]) / scale);
+}
+// Masked squared error: g_out[p][0] = 2 (pred - t) / count, partial sums of (pred - t)^2 and count.
+__global__ void k_unet_loss(const float* out16, const float* target, const unsigned char* mask, int npix,
+                            int pix_per_block, float inv_count, float* g_out16, float2* part) {
+    float se = 0.0f, cnt = 0.0f;
+    const int p0 = blockIdx.x * pix_per_block;
+    for (int i = threadIdx.x; i < pix_per_block; i += blockDim.x) {
+        const int p = p0 + i;
+        if (p >= npix) break;
+        float g = 0.0f;
+        if (mask[p]) {
+            const float d = out16[(size_t)p * 16] - target[p];
+            se += d * d;
+            cnt += 1.0f;
+            g = 2.0f * d * inv_count;
+        }
+        float* gp = g_out16 + (size_t)p * 16;
+        gp[0] = g;
+#pragma unroll
+        for (int c = 1; c < 16; ++c) gp[c] = 0.0f;
+    }
+    se = warp_sum_f(se);
+    cnt = warp_sum_f(cnt);
+    __shared__ float2 red[32];
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = make_float2(se, cnt);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float2 t = make_float2(0.0f, 0.0f);
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+            t.x += red[w].x;
+            t.y += red[w].y;
+        }
+        part[blockIdx.x] = t;
+    }
+}
+__global__ void k_mask_count(const unsigned char* mask, int npix, unsigned int* count) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    const unsigned int c = __syncthreads_count(p < npix && mask[p]);
+    if (threadIdx.x == 0 && c) atomicAdd(count, c);
+}
+
+// ---------------------------------------------------------------------------
+// The network: 4 levels, channels 16/32/64/64, two 3x3 convolutions + ReLU
+// per level, 2x2 average pooling down, nearest upsampling and concatenation
+// up, a linear 3x3 head (16 outputs, channel 0 used).
+
+struct UConvSpec {
+    int cin, cout, relu;
+};
+constexpr int UNET_NCONV = 15;
+constexpr UConvSpec kUnetSpec[UNET_NCONV] = {
+    {16, 16, 1}, {16, 16, 1},   // level 0
+    {16, 32, 1}, {32, 32, 1},   // level 1
+    {32, 64, 1}, {64, 64, 1},   // level 2
+    {64, 64, 1}, {64, 64, 1},   // level 3 (bottleneck)
+    {128, 64, 1}, {64, 64, 1},  // up to level 2 (64 up + 64 skip)
+    {96, 32, 1}, {32, 32, 1},   // up to level 1 (64 up + 32 skip)
+    {48, 16, 1}, {16, 16, 1},   // up to level 0 (32 up + 16 skip)
+    {16, 16, 0},                // head
+};
+
+struct UNet {
+    int device = 0, maxH = 0, maxW = 0;
+    size_t woff[UNET_NCONV], boff[UNET_NCONV], nparams = 0;
+    float *params = nullptr, *grads = nullptr, *adam_m = nullptr, *adam_v = nullptr;
+    bf16 *w16[UNET_NCONV], *wt16[UNET_NCONV];
+    int adam_t = 0;
+    // activations (bf16), sized for maxH x maxW
+    bf16 *X0, *t0, *cat0, *p1, *t1, *cat1, *p2, *t2, *cat2, *p3, *t3, *u3, *t4, *u4, *t5, *u5, *t6, *u6;
+    float* out;  // [H*W][16] fp32 head output
+    // gradients (fp32)
+    float *g_out, *g_u6, *g_t6, *g_cat0, *g_u5, *g_t5, *g_cat1, *g_u4, *g_t4, *g_cat2, *g_u3, *g_t3, *g_p3, *g_t2,
+        *g_p2, *g_t1, *g_p1, *g_t0;
+    bf16* dym;
+    float *wpart, *bpart;
+    size_t wpart_elems = 0;
+    float2* lpart;
+    float *target, *prev32;
+    unsigned char* mask;
+    unsigned int* count;
+    int* err;
+    void* arena = nullptr;
+    std::vector<void*> extra;
+    std::string last_error;
+};
+
+inline size_t up256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+// One allocation for everything: parameters, Adam moments, bf16 weights,
+// activations and gradients for maxH x maxW.
+inline cudaError_t unet_alloc(UNet& n, int maxH, int maxW) {
+    n.maxH = maxH;
+    n.maxW = maxW;
+    size_t off = 0;
+    for (int i = 0; i < UNET_NCONV; ++i) {
+        n.woff[i] = off;
+        off += (size_t)9 * kUnetSpec[i].cin * kUnetSpec[i].cout;
+        n.boff[i] = off;
+        off += kUnetSpec[i].cout;
+    }
+    n.nparams = off;
+    const size_t P0 = (size_t)maxH * maxW, P1 = P0 / 4, P2 = P0 / 16, P3 = P0 / 64;
+    struct Item {
+        void** ptr;
+        size_t bytes;
+    };
+    std::vector<Item> items;
+    auto F = [&](float** p, size_t n_) { items.push_back({(void**)p, up256(n_ * 4)}); };
+    auto B = [&](bf16** p, size_t n_) { items.push_back({(void**)p, up256(n_ * 2)}); };
+    F(&n.params, n.nparams);
+    F(&n.grads, n.nparams);
+    F(&n.adam_m, n.nparams);
+    F(&n.adam_v, n.nparams);
+    for (int i = 0; i < UNET_NCONV; ++i) {
+        B(&n.w16[i], (size_t)9 * kUnetSpec[i].cin * kUnetSpec[i].cout);
+        B(&n.wt16[i], (size_t)9 * kUnetSpec[i].cin * kUnetSpec[i].cout);
+    }
+    B(&n.X0, P0 * 16); B(&n.t0, P0 * 16); B(&n.cat0, P0 * 48);
+    B(&n.p1, P1 * 16); B(&n.t1, P1 * 32); B(&n.cat1, P1 * 96);
+    B(&n.p2, P2 * 32); B(&n.t2, P2 * 64); B(&n.cat2, P2 * 128);
+    B(&n.p3, P3 * 64); B(&n.t3, P3 * 64); B(&n.u3, P3 * 64);
+    B(&n.t4, P2 * 64); B(&n.u4, P2 * 64); B(&n.t5, P1 * 32); B(&n.u5, P1 * 32);
+    B(&n.t6, P0 * 16); B(&n.u6, P0 * 16);
+    F(&n.out, P0 * 16);
+    F(&n.g_out, P0 * 16); F(&n.g_u6, P0 * 16); F(&n.g_t6, P0 * 16); F(&n.g_cat0, P0 * 48);
+    F(&n.g_u5, P1 * 32); F(&n.g_t5, P1 * 32); F(&n.g_cat1, P1 * 96);
+    F(&n.g_u4, P2 * 64); F(&n.g_t4, P2 * 64); F(&n.g_cat2, P2 * 128);
+    F(&n.g_u3, P3 * 64); F(&n.g_t3, P3 * 64); F(&n.g_p3, P3 * 64);
+    F(&n.g_t2, P2 * 64); F(&n.g_p2, P2 * 32); F(&n.g_t1, P1 * 32); F(&n.g_p1, P1 * 16); F(&n.g_t0, P0 * 16);
+    B(&n.dym, P0 * 16);
+    // weight-gradient partials: chunks of 4096 pixels x up to 9 row tiles x 128 x 64
+    n.wpart_elems = ((P0 + 4095) / 4096) * 9 * 128 * 64;
+    F(&n.wpart, n.wpart_elems);
+    F(&n.bpart, ((P0 + 1023) / 1024) * 64);
+    items.push_back({(void**)&n.lpart, up256(((P0 + 1023) / 1024) * sizeof(float2))});
+    F(&n.target, P0);
+    F(&n.prev32, P0);
+    items.push_back({(void**)&n.mask, up256(P0)});
+    items.push_back({(void**)&n.count, 256});
+    items.push_back({(void**)&n.err, 256});
+    size_t total = 0;
+    for (auto& it : items) total += it.bytes;
+    cudaError_t e = cudaMalloc(&n.arena, total);
+    if (e != cudaSuccess) return e;
+    e = cudaMemset(n.arena, 0, total);
+    if (e != cudaSuccess) return e;
+    char* base = (char*)n.arena;
+    for (auto& it : items) {
+        *it.ptr = base;
+        base += it.bytes;
+    }
+    return cudaSuccess;
+}
+
+inline dim3 lin_grid(size_t n, int block = 256) { return dim3((unsigned)((n + block - 1) / block)); }
+
+// Refreshes the bf16 weights (and their flipped transposes) from the fp32 master copy.
+inline void unet_sync_weights(UNet& n, cudaStream_t st) {
+    for (int i = 0; i < UNET_NCONV; ++i) {
+        const int c = 9 * kUnetSpec[i].cin * kUnetSpec[i].cout;
+        k_flip_transpose<<<lin_grid(c), 256, count_launch(), st>>>(n.params + n.woff[i], kUnetSpec[i].cin,
+                                                                   kUnetSpec[i].cout, n.w16[i], n.wt16[i]);
+    }
+}
+
+inline void unet_conv(UNet& n, int i, const bf16* x, int xs, int xo, int H, int W, bf16* y, int ys, int yo,
+                      float* yf, cudaStream_t st) {
+    ConvArgs a;
+    a.x = x;
+    a.xs = xs;
+    a.xo = xo;
+    a.w = n.w16[i];
+    a.bias = n.params + n.boff[i];
+    a.y = y;
+    a.yf = yf;
+    a.ys = ys;
+    a.yo = yo;
+    a.relu = kUnetSpec[i].relu;
+    a.H = H;
+    a.W = W;
+    a.cin = kUnetSpec[i].cin;
+    a.cout = kUnetSpec[i].cout;
+    a.err = n.err;
+    k_conv3x3_tc<<<(H * W + 127) / 128, CV_THREADS, CV_SMEM + count_launch(), st>>>(a);
+}
+
+inline void unet_forward(UNet& n, int H, int W, cudaStream_t st) {
+    const int H1 = H / 2, W1 = W / 2, H2 = H / 4, W2 = W / 4, H3 = H / 8, W3 = W / 8;
+    unet_conv(n, 0, n.X0, 16, 0, H, W, n.t0, 16, 0, nullptr, st);
+    unet_conv(n, 1, n.t0, 16, 0, H, W, n.cat0, 48, 32, nullptr, st);
+    k_pool2<<<lin_grid((size_t)H1 * W1 * 16), 256, count_launch(), st>>>(n.cat0, 48, 32, H, W, 16, n.p1);
+    unet_conv(n, 2, n.p1, 16, 0, H1, W1, n.t1, 32, 0, nullptr, st);
+    unet_conv(n, 3, n.t1, 32, 0, H1, W1, n.cat1, 96, 64, nullptr, st);
+    k_pool2<<<lin_grid((size_t)H2 * W2 * 32), 256, count_launch(), st>>>(n.cat1, 96, 64, H1, W1, 32, n.p2);
+    unet_conv(n, 4, n.p2, 32, 0, H2, W2, n.t2, 64, 0, nullptr, st);
+    unet_conv(n, 5, n.t2, 64, 0, H2, W2, n.cat2, 128, 64, nullptr, st);
+    k_pool2<<<lin_grid((size_t)H3 * W3 * 64), 256, count_launch(), st>>>(n.cat2, 128, 64, H2, W2, 64, n.p3);
+    unet_conv(n, 6, n.p3, 64, 0, H3, W3, n.t3, 64, 0, nullptr, st);
+    unet_conv(n, 7, n.t3, 64, 0, H3, W3, n.u3, 64, 0, nullptr, st);
+    k_up2<<<lin_grid((size_t)H2 * W2 * 64), 256, count_launch(), st>>>(n.u3, H2, W2, 64, n.cat2, 128, 0);
+    unet_conv(n, 8, n.cat2, 128, 0, H2, W2, n.t4, 64, 0, nullptr, st);
+    unet_conv(n, 9, n.t4, 64, 0, H2, W2, n.u4, 64, 0, nullptr, st);
+    k_up2<<<lin_grid((size_t)H1 * W1 * 64), 256, count_launch(), st>>>(n.u4, H1, W1, 64, n.cat1, 96, 0);
+    unet_conv(n, 10, n.cat1, 96, 0, H1, W1, n.t5, 32, 0, nullptr, st);
+    unet_conv(n, 11, n.t5, 32, 0, H1, W1, n.u5, 32, 0, nullptr, st);
+    k_up2<<<lin_grid((size_t)H * W * 32), 256, count_launch(), st>>>(n.u5, H, W, 32, n.cat0, 48, 0);
+    unet_conv(n, 12, n.cat0, 48, 0, H, W, n.t6, 16, 0, nullptr, st);
+    unet_conv(n, 13, n.t6, 16, 0, H, W, n.u6, 16, 0, nullptr, st);
+    unet_conv(n, 14, n.u6, 16, 0, H, W, nullptr, 16, 0, n.out, st);
+}
+
+// Backward of conv i: dy = relu'(y) * g (bf16), weight and bias gradients,
+// and (if gx) the gradient of its input, written over gx's slice.
+inline void unet_conv_bwd(UNet& n, int i, const bf16* x, int xs, int xo, const bf16* y, int ys, int yo,
+                          const float* g, int gs, int go, int H, int W, float* gx, int gxs, int gxo,
+                          cudaStream_t st) {
+    const int cin = kUnetSpec[i].cin, cout = kUnetSpec[i].cout, npix = H * W;
+    k_relu_bwd<<<lin_grid((size_t)npix * cout), 256, count_launch(), st>>>(g, gs, go, y, ys, yo, npix, cout,
+                                                                           kUnetSpec[i].relu, n.dym);
+    // weight gradient
+    WgradArgs w;
+    w.x = x;
+    w.xs = xs;
+    w.xo = xo;
+    w.dy = n.dym;
+    w.H = H;
+    w.W = W;
+    w.cin = cin;
+    w.cout = cout;
+    w.pix_per_cta = 4096;
+    w.part = n.wpart;
+    w.err = n.err;
+    const int chunks = (npix + 4095) / 4096, mtiles = (9 * cin + 127) / 128;
+    k_wgrad_tc<<<dim3(chunks, mtiles), WG_THREADS, WG_SMEM + count_launch(), st>>>(w);
+    k_wgrad_reduce<<<lin_grid((size_t)9 * cin * cout), 256, count_launch(), st>>>(n.wpart, chunks, mtiles, cin, cout,
+                                                                                  n.grads + n.woff[i]);
+    const int bblocks = (npix + 1023) / 1024;
+    k_bgrad_partial<<<bblocks, 64, count_launch(), st>>>(n.dym, npix, cout, 1024, n.bpart);
+    k_bgrad_reduce<<<1, 64, count_launch(), st>>>(n.bpart, bblocks, cout, n.grads + n.boff[i]);
+    if (gx) {
+        ConvArgs a;
+        a.x = n.dym;
+        a.xs = cout;
+        a.xo = 0;
+        a.w = n.wt16[i];
+        a.bias = nullptr;
+        a.y = nullptr;
+        a.yf = gx;
+        a.ys = gxs;
+        a.yo = gxo;
+        a.relu = 0;
+        a.H = H;
+        a.W = W;
+        a.cin = cout;
+        a.cout = cin;
+        a.err = n.err;
+        k_conv3x3_tc<<<(npix + 127) / 128, CV_THREADS, CV_SMEM + count_launch(), st>>>(a);
+    }
+}
+
+// Backward pass from n.g_out; fills n.grads.
+inline void unet_backward(UNet& n, int H, int W, cudaStream_t st) {
+    const int H1 = H / 2, W1 = W / 2, H2 = H / 4, W2 = W / 4, H3 = H / 8, W3 = W / 8;
+    unet_conv_bwd(n, 14, n.u6, 16, 0, nullptr, 16, 0, n.g_out, 16, 0, H, W, n.g_u6, 16, 0, st);
+    unet_conv_bwd(n, 13, n.t6, 16, 0, n.u6, 16, 0, n.g_u6, 16, 0, H, W, n.g_t6, 16, 0, st);
+    unet_conv_bwd(n, 12, n.cat0, 48, 0, n.t6, 16, 0, n.g_t6, 16, 0, H, W, n.g_cat0, 48, 0, st);
+    k_up2_bwd<<<lin_grid((size_t)H1 * W1 * 32), 256, count_launch(), st>>>(n.g_cat0, 48, 0, H, W, 32, n.g_u5);
+    unet_conv_bwd(n, 11, n.t5, 32, 0, n.u5, 32, 0, n.g_u5, 32, 0, H1, W1, n.g_t5, 32, 0, st);
+    unet_conv_bwd(n, 10, n.cat1, 96, 0, n.t5, 32, 0, n.g_t5, 32, 0, H1, W1, n.g_cat1, 96, 0, st);
+    k_up2_bwd<<<lin_grid((size_t)H2 * W2 * 64), 256, count_launch(), st>>>(n.g_cat1, 96, 0, H1, W1, 64, n.g_u4);
+    unet_conv_bwd(n, 9, n.t4, 64, 0, n.u4, 64, 0, n.g_u4, 64, 0, H2, W2, n.g_t4, 64, 0, st);
+    unet_conv_bwd(n, 8, n.cat2, 128, 0, n.t4, 64, 0, n.g_t4, 64, 0, H2, W2, n.g_cat2, 128, 0, st);
+    k_up2_bwd<<<lin_grid((size_t)H3 * W3 * 64), 256, count_launch(), st>>>(n.g_cat2, 128, 0, H2, W2, 64, n.g_u3);
+    unet_conv_bwd(n, 7, n.t3, 64, 0, n.u3, 64, 0, n.g_u3, 64, 0, H3, W3, n.g_t3, 64, 0, st);
+    unet_conv_bwd(n, 6, n.p3, 64, 0, n.t3, 64, 0, n.g_t3, 64, 0, H3, W3, n.g_p3, 64, 0, st);
+    k_pool2_bwd<<<lin_grid((size_t)H2 * W2 * 64), 256, count_launch(), st>>>(n.g_p3, H2, W2, 64, n.g_cat2, 128, 64);
+    unet_conv_bwd(n, 5, n.t2, 64, 0, n.cat2, 128, 64, n.g_cat2, 128, 64, H2, W2, n.g_t2, 64, 0, st);
+    unet_conv_bwd(n, 4, n.p2, 32, 0, n.t2, 64, 0, n.g_t2, 64, 0, H2, W2, n.g_p2, 32, 0, st);
+    k_pool2_bwd<<<lin_grid((size_t)H1 * W1 * 32), 256, count_launch(), st>>>(n.g_p2, H1, W1, 32, n.g_cat1, 96, 64);
+    unet_conv_bwd(n, 3, n.t1, 32, 0, n.cat1, 96, 64, n.g_cat1, 96, 64, H1, W1, n.g_t1, 32, 0, st);
+    unet_conv_bwd(n, 2, n.p1, 16, 0, n.t1, 32, 0, n.g_t1, 32, 0, H1, W1, n.g_p1, 16, 0, st);
+    k_pool2_bwd<<<lin_grid((size_t)H * W * 16), 256, count_launch(), st>>>(n.g_p1, H, W, 16, n.g_cat0, 48, 32);
+    unet_conv_bwd(n, 1, n.t0, 16, 0, n.cat0, 48, 32, n.g_cat0, 48, 32, H, W, n.g_t0, 16, 0, st);
+    unet_conv_bwd(n, 0, n.X0, 16, 0, n.t0, 16, 0, n.g_t0, 16, 0, H, W, nullptr, 0, 0, st);
+}
+
+}  // namespace efl

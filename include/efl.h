@@ -349,6 +349,40 @@ EFL_API efl_status efl_batch_step(efl_batch* batch, float dt, efl_step_stats* st
  * milliseconds; waits for it to finish. */
 EFL_API efl_status efl_batch_projection_ms(efl_batch* batch, float* ms);
 
+/* ---- Learned warm start ------------------------------------------------ */
+
+/* Extension, no reference counterpart.  A small U-Net (BF16 weights and
+ * activations, FP32 accumulation; 4 levels, 16/32/64/64 channels, 3x3
+ * convolutions on the tensor cores) predicts the change of the pressure
+ * over a step from the system about to be solved; its prediction only
+ * warm-starts the tolerance-driven solve, which still iterates to the same
+ * residual.  Features per cell, 16 channels (5 used): cdiv * div / s, the u
+ * and v face fractions averaged to the centre, phi / ny clamped to [-1, 1],
+ * the previous pressure / s, with s = rho * |g| * ny * dx; output channel 0
+ * = (p - p_prev) / s.  The head starts at zero, so an untrained network
+ * warm-starts from the previous pressure exactly. */
+typedef struct efl_unet efl_unet;
+enum { EFL_UNET_WARM_START = 1, EFL_UNET_RECORD = 2 };
+EFL_API efl_status efl_unet_create(int32_t device, uint32_t max_nx, uint32_t max_ny, uint64_t seed, efl_unet** out);
+EFL_API efl_status efl_unet_destroy(efl_unet* net);
+EFL_API const char* efl_unet_last_error(const efl_unet* net);
+EFL_API efl_status efl_unet_num_params(const efl_unet* net, uint64_t* n);
+EFL_API efl_status efl_unet_get_params(efl_unet* net, float* params, uint64_t n);
+EFL_API efl_status efl_unet_set_params(efl_unet* net, const float* params, uint64_t n);
+/* Forward pass on host features [ny][nx][16]; pred [ny][nx] = output channel 0. */
+EFL_API efl_status efl_unet_forward(efl_unet* net, uint32_t nx, uint32_t ny, const float* features, float* pred);
+/* Forward + backward of the masked mean squared error against target
+ * [ny][nx] over mask [ny][nx] != 0; loss and the gradient of every
+ * parameter (efl_unet_num_params floats, the order of get/set_params). */
+EFL_API efl_status efl_unet_gradients(efl_unet* net, uint32_t nx, uint32_t ny, const float* features,
+                                      const float* target, const uint8_t* mask, float* loss, float* grads);
+/* flags: EFL_UNET_WARM_START (warm-start sim's tolerance-driven solves),
+ * EFL_UNET_RECORD (record each solve as a training sample); 0 detaches.
+ * Batches (efl_batch_step) do not use it. */
+EFL_API efl_status efl_unet_attach(efl_sim* sim, efl_unet* net, uint32_t flags);
+/* One Adam step (lr; beta 0.9 / 0.999) on the last recorded sample. */
+EFL_API efl_status efl_unet_train_step(efl_unet* net, float lr, float* loss);
+
 /* ---- Diagnostics ------------------------------------------------------ */
 
 /* Kernels this library has launched since it was loaded (all handles). */
