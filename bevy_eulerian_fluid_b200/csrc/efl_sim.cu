@@ -56,7 +56,6 @@ struct DevBuf {
 struct efl_unet {
     UNet net;
     int rec_nx = 0, rec_ny = 0;  // size of the recorded training sample (0: none)
-    double rec_scale = 0.0;
 };
 
 // Captured CUDA graphs of step segments, keyed by a signature of the
@@ -668,36 +667,31 @@ efl_status check_device_errors(efl_sim* s) {
 }
 
 // Learned warm start: the features of the system about to be solved, and
-// (when warm-starting) x += s * prediction on the fluid cells.
-double unet_scale(const efl_sim* s) {
-    const double g = std::sqrt((double)s->cfg.gravity[0] * s->cfg.gravity[0] +
-                               (double)s->cfg.gravity[1] * s->cfg.gravity[1]);
-    return (double)s->cfg.rho * (g > 0.0 ? g : 9.8) * (double)s->ny * (double)s->U.dx;
-}
+// (when warm-starting) x += sigma * prediction on the counted cells.
 efl_status unet_before_solve(efl_sim* s) {
     UNet& n = s->unet->net;
     const Level64& L = s->mg64[0];
     const dim3 g = grid2d(s->nx, s->ny, kBlock);
     const double dx = (double)s->U.dx;
-    UnetFeatureArgs a{s->div, s->ls0, s->fu, s->fv, L.x, dx * dx * (double)s->U.rho / (double)s->U.dt,
-                      unet_scale(s), s->nx, s->ny};
-    k_unet_features<<<g, kBlock, count_launch(), s->stream>>>(a, n.X0, n.prev32, n.mask);
+    UnetFeatureArgs a{s->ls0, s->fu, s->fv, L.x, L.b, dx * dx * (double)s->U.rho / (double)s->U.dt,
+                      (double)s->U.dt / (double)s->U.rho / dx / dx, s->nx, s->ny};
+    k_unet_residual<<<g, kBlock, count_launch(), s->stream>>>(a, n.res32, n.prev32, n.mask, n.lpart);
+    k_unet_sigma<<<1, 32, count_launch(), s->stream>>>(n.lpart, (int)(g.x * g.y), n.sigma);
+    k_unet_features<<<g, kBlock, count_launch(), s->stream>>>(n.res32, a, n.mask, n.sigma, n.X0);
     if (s->unet_flags & EFL_UNET_WARM_START) {
         unet_forward(n, s->ny, s->nx, s->stream);
-        k_unet_warm<<<g, kBlock, count_launch(), s->stream>>>(L.x, n.out, n.mask, a.scale, s->nx, s->ny);
+        k_unet_warm<<<g, kBlock, count_launch(), s->stream>>>(L.x, n.out, n.mask, n.sigma, s->nx, s->ny);
     }
     LAUNCH_CHECK();
     return EFL_OK;
 }
 efl_status unet_after_solve(efl_sim* s) {
     UNet& n = s->unet->net;
-    const double scale = unet_scale(s);
-    k_unet_target<<<grid2d(s->nx, s->ny, kBlock), kBlock, count_launch(), s->stream>>>(s->mg64[0].x, n.prev32, scale,
+    k_unet_target<<<grid2d(s->nx, s->ny, kBlock), kBlock, count_launch(), s->stream>>>(s->mg64[0].x, n.prev32, n.sigma,
                                                                                       s->nx, s->ny, n.target);
     LAUNCH_CHECK();
     s->unet->rec_nx = s->nx;
     s->unet->rec_ny = s->ny;
-    s->unet->rec_scale = scale;
     return EFL_OK;
 }
 
@@ -1830,26 +1824,26 @@ __global__ void k_copy_f32(const float* a, size_t n, size_t stride, float* b) { 
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) b[i] = a[i * stride];
 }
-// Loss on the sample in X0/target/mask; fills g_out, returns the mean squared error.
+// Loss on the sample in X0/target/mask (relative squared error, see
+// k_unet_loss); fills g_out and the parameter gradients.
 efl_status unet_loss_and_grads(efl_unet* u, int H, int W, cudaStream_t st, float* loss) {
     UNet& n = u->net;
-    const int npix = H * W;
-    cudaMemsetAsync(n.count, 0, sizeof(unsigned int), st);
-    k_mask_count<<<(npix + 255) / 256, 256, count_launch(), st>>>(n.mask, npix, n.count);
-    unsigned int cnt = 0;
-    cudaMemcpyAsync(&cnt, n.count, sizeof(cnt), cudaMemcpyDeviceToHost, st);
+    const int npix = H * W, blocks = (npix + 1023) / 1024;
+    std::vector<float2> part(blocks);
+    k_target_stats<<<blocks, 256, count_launch(), st>>>(n.target, n.mask, npix, 1024, n.lpart);
+    cudaMemcpyAsync(part.data(), n.lpart, blocks * sizeof(float2), cudaMemcpyDeviceToHost, st);
     unet_forward(n, H, W, st);
     TRY_U(unet_finish(u, st));
-    const int blocks = (npix + 1023) / 1024;
-    k_unet_loss<<<blocks, 256, count_launch(), st>>>(n.out, n.target, n.mask, npix, 1024,
-                                                       cnt ? 1.0f / (float)cnt : 0.0f, n.g_out, n.lpart);
+    double t2 = 0.0;
+    for (auto& q : part) t2 += q.y;
+    const float inv = t2 > 0.0 ? (float)(1.0 / t2) : 0.0f;
+    k_unet_loss<<<blocks, 256, count_launch(), st>>>(n.out, n.target, n.mask, npix, 1024, inv, n.g_out, n.lpart);
     unet_backward(n, H, W, st);
-    std::vector<float2> part(blocks);
     cudaMemcpyAsync(part.data(), n.lpart, blocks * sizeof(float2), cudaMemcpyDeviceToHost, st);
     TRY_U(unet_finish(u, st));
     double se = 0.0;
     for (auto& q : part) se += q.x;
-    *loss = cnt ? (float)(se / cnt) : 0.0f;
+    *loss = (float)(se * (double)inv);
     return EFL_OK;
 }
 }  // namespace

@@ -409,11 +409,13 @@ namespace efl {
 // ---------------------------------------------------------------------------
 // Features of one pressure system and the warm start.
 //
-// Channels (16, zero beyond 5): 0 = cdiv * div / s (the right-hand side in
-// pressure units), 1 / 2 = the u / v face fractions averaged to the cell
-// centre, 3 = phi / ny clamped to [-1, 1], 4 = the previous pressure / s;
-// s = rho * g * ny * dx, the hydrostatic pressure of a full column.  The
-// network predicts the change of the pressure over the step, (p - p_prev) / s.
+// The start iterate p_prev (the previous step's pressure) leaves the residual
+// r = b - A p_prev on the new system; the exact correction e = A^-1 r is what
+// the network approximates.  Both are scaled by sigma, the RMS of cdiv * r
+// over the counted cells (cdiv * r is in pressure units), so the map is
+// scale-free.  Channels (16, zero beyond 5): 0 = cdiv * r / sigma, 1 / 2 =
+// the u / v face fractions averaged to the cell centre, 3 = phi / ny clamped
+// to [-1, 1], 4 = 1 on the counted cells; output channel 0 = e / sigma.
 
 EFL_DEV float warp_sum_f(float v) {
 #pragma unroll
@@ -422,51 +424,114 @@ EFL_DEV float warp_sum_f(float v) {
 }
 
 struct UnetFeatureArgs {
-    PF div, ls, fu, fv;
-    Plane<double> prev;  // the solve's start iterate (previous pressure, widened)
-    double cdiv, scale;
+    PF ls, fu, fv;
+    Plane<double> prev, b;  // the solve's start iterate and right-hand side
+    double cdiv, factor;    // dx^2 rho / dt, dt / (rho dx^2)
     int nx, ny;
 };
-__global__ void k_unet_features(UnetFeatureArgs a, bf16* x0, float* prev32, unsigned char* mask) {
+// res[p] = cdiv * (b - A prev) on the counted cells (the operator of
+// residual.wgsl:33-54 in factored form, as the mixed solve builds it), the
+// mask, prev32 = prev, and per-block partial sums (res^2, count).
+__global__ void __launch_bounds__(256) k_unet_residual(UnetFeatureArgs a, float* res, float* prev32, unsigned char* mask,
+                                                        float2* part) {
+    const int gx = blockIdx.x * blockDim.x + threadIdx.x, gy = blockIdx.y * blockDim.y + threadIdx.y;
+    float r2 = 0.0f, c = 0.0f;
+    if (gx < a.nx && gy < a.ny) {
+        const size_t p = (size_t)gy * a.nx + gx;
+        const float phi = a.ls.at(gx, gy);
+        const float f[4] = {a.fu.at(gx, gy), a.fu.at(gx + 1, gy), a.fv.at(gx, gy), a.fv.at(gx, gy + 1)};
+        const bool counted = phi < 0.0f && !(f[0] == 0.0f && f[1] == 0.0f && f[2] == 0.0f && f[3] == 0.0f);
+        float rv = 0.0f;
+        if (counted) {
+            const int ox[4] = {-1, 1, 0, 0}, oy[4] = {0, 0, -1, 1};
+            double den = 0.0, sum = 0.0;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int jx = gx + ox[q], jy = gy + oy[q];
+                if ((unsigned)jx < (unsigned)a.nx && (unsigned)jy < (unsigned)a.ny) {
+                    const float level = a.ls.at(jx, jy);
+                    if (level < 0.0f) {
+                        den += (double)f[q];
+                        sum += (double)f[q] * a.prev.at(jx, jy);
+                    } else {
+                        den += (double)f[q] * (1.0 - (double)level / (double)phi);
+                    }
+                }
+            }
+            rv = (float)(a.cdiv * (a.b.at(gx, gy) - a.factor * (den * a.prev.at(gx, gy) - sum)));
+            r2 = rv * rv;
+            c = 1.0f;
+        }
+        res[p] = rv;
+        prev32[p] = (float)a.prev.at(gx, gy);
+        mask[p] = counted ? 1 : 0;
+    }
+    r2 = warp_sum_f(r2);
+    c = warp_sum_f(c);
+    __shared__ float2 red[8];
+    const int t = threadIdx.y * blockDim.x + threadIdx.x;
+    if ((t & 31) == 0) red[t >> 5] = make_float2(r2, c);
+    __syncthreads();
+    if (t == 0) {
+        float2 s2 = make_float2(0.0f, 0.0f);
+        for (int w = 0; w < (int)(blockDim.x * blockDim.y) / 32; ++w) {
+            s2.x += red[w].x;
+            s2.y += red[w].y;
+        }
+        part[blockIdx.y * gridDim.x + blockIdx.x] = s2;
+    }
+}
+// sigma = RMS of the residual over the counted cells (1 if there are none), in order.
+__global__ void k_unet_sigma(const float2* part, int n, float* sigma) {
+    if (threadIdx.x != 0) return;
+    double r2 = 0.0, c = 0.0;
+    for (int i = 0; i < n; ++i) {
+        r2 += part[i].x;
+        c += part[i].y;
+    }
+    const double v = c > 0.0 ? sqrt(r2 / c) : 0.0;
+    *sigma = v > 0.0 ? (float)v : 1.0f;
+}
+__global__ void k_unet_features(const float* res, const UnetFeatureArgs a, const unsigned char* mask,
+                                const float* sigma, bf16* x0) {
     const int gx = blockIdx.x * blockDim.x + threadIdx.x, gy = blockIdx.y * blockDim.y + threadIdx.y;
     if (gx >= a.nx || gy >= a.ny) return;
     const size_t p = (size_t)gy * a.nx + gx;
-    const float phi = a.ls.at(gx, gy);
-    const float f0 = a.fu.at(gx, gy), f1 = a.fu.at(gx + 1, gy), f2 = a.fv.at(gx, gy), f3 = a.fv.at(gx, gy + 1);
-    const double pv = a.prev.at(gx, gy);
+    const float inv = 1.0f / *sigma;
     __align__(16) bf16 v[16];
 #pragma unroll
     for (int c = 0; c < 16; ++c) v[c] = __float2bfloat16_rn(0.0f);
-    v[0] = __float2bfloat16_rn((float)(a.cdiv * (double)a.div.at(gx, gy) / a.scale));
-    v[1] = __float2bfloat16_rn(0.5f * (f0 + f1));
-    v[2] = __float2bfloat16_rn(0.5f * (f2 + f3));
-    v[3] = __float2bfloat16_rn(fminf(1.0f, fmaxf(-1.0f, phi / (float)a.ny)));
-    v[4] = __float2bfloat16_rn((float)(pv / a.scale));
+    v[0] = __float2bfloat16_rn(res[p] * inv);
+    v[1] = __float2bfloat16_rn(0.5f * (a.fu.at(gx, gy) + a.fu.at(gx + 1, gy)));
+    v[2] = __float2bfloat16_rn(0.5f * (a.fv.at(gx, gy) + a.fv.at(gx, gy + 1)));
+    v[3] = __float2bfloat16_rn(fminf(1.0f, fmaxf(-1.0f, a.ls.at(gx, gy) / (float)a.ny)));
+    v[4] = __float2bfloat16_rn(mask[p] ? 1.0f : 0.0f);
     uint4* dst = reinterpret_cast<uint4*>(x0 + p * 16);
     dst[0] = reinterpret_cast<const uint4*>(v)[0];
     dst[1] = reinterpret_cast<const uint4*>(v)[1];
-    prev32[p] = (float)pv;
-    mask[p] = (phi < 0.0f && !(f0 == 0.0f && f1 == 0.0f && f2 == 0.0f && f3 == 0.0f)) ? 1 : 0;
 }
-// x += s * prediction on the masked cells (the solve's start iterate).
-__global__ void k_unet_warm(Plane<double> x, const float* out16, const unsigned char* mask, double scale, int nx,
+// x += sigma * prediction on the masked cells (the solve's start iterate).
+__global__ void k_unet_warm(Plane<double> x, const float* out16, const unsigned char* mask, const float* sigma, int nx,
                             int ny) {
     const int gx = blockIdx.x * blockDim.x + threadIdx.x, gy = blockIdx.y * blockDim.y + threadIdx.y;
     if (gx >= nx || gy >= ny) return;
     const size_t p = (size_t)gy * nx + gx;
-    if (mask[p]) x.at(gx, gy) = x.at(gx, gy) + scale * (double)out16[p * 16];
+    if (mask[p]) x.at(gx, gy) = x.at(gx, gy) + (double)*sigma * (double)out16[p * 16];
 }
-// Training target after the solve: (p - p_prev) / s.
-__global__ void k_unet_target(Plane<double> x, const float* prev32, double scale, int nx, int ny, float* target) {
+// Training target after the solve: (p - p_prev) / sigma.
+__global__ void k_unet_target(Plane<double> x, const float* prev32, const float* sigma, int nx, int ny,
+                              float* target) {
     const int gx = blockIdx.x * blockDim.x + threadIdx.x, gy = blockIdx.y * blockDim.y + threadIdx.y;
     if (gx >= nx || gy >= ny) return;
     const size_t p = (size_t)gy * nx + gx;
-    target[p] = (float)((x.at(gx, gy) - (double)prev32[p]) / scale);
+    target[p] = (float)((x.at(gx, gy) - (double)prev32[p]) / (double)*sigma);
 }
-// Masked squared error: g_out[p][0] = 2 (pred - t) / count, partial sums of (pred - t)^2 and count.
+// Relative squared error of one sample, sum_mask (pred - t)^2 / sum_mask t^2:
+// g_out[p][0] = 2 (pred - t) * inv_norm (inv_norm = 1 / sum_mask t^2), and
+// per-block partial sums of (pred - t)^2.
 __global__ void k_unet_loss(const float* out16, const float* target, const unsigned char* mask, int npix,
-                            int pix_per_block, float inv_count, float* g_out16, float2* part) {
-    float se = 0.0f, cnt = 0.0f;
+                            int pix_per_block, float inv_norm, float* g_out16, float2* part) {
+    float se = 0.0f;
     const int p0 = blockIdx.x * pix_per_block;
     for (int i = threadIdx.x; i < pix_per_block; i += blockDim.x) {
         const int p = p0 + i;
@@ -475,8 +540,7 @@ __global__ void k_unet_loss(const float* out16, const float* target, const unsig
         if (mask[p]) {
             const float d = out16[(size_t)p * 16] - target[p];
             se += d * d;
-            cnt += 1.0f;
-            g = 2.0f * d * inv_count;
+            g = 2.0f * d * inv_norm;
         }
         float* gp = g_out16 + (size_t)p * 16;
         gp[0] = g;
@@ -484,9 +548,32 @@ __global__ void k_unet_loss(const float* out16, const float* target, const unsig
         for (int c = 1; c < 16; ++c) gp[c] = 0.0f;
     }
     se = warp_sum_f(se);
-    cnt = warp_sum_f(cnt);
+    __shared__ float red[32];
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = se;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float t = 0.0f;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+        part[blockIdx.x] = make_float2(t, 0.0f);
+    }
+}
+// Per-block partial sums of (count, t^2) over the masked cells.
+__global__ void k_target_stats(const float* target, const unsigned char* mask, int npix, int pix_per_block,
+                               float2* part) {
+    float c = 0.0f, t2 = 0.0f;
+    const int p0 = blockIdx.x * pix_per_block;
+    for (int i = threadIdx.x; i < pix_per_block; i += blockDim.x) {
+        const int p = p0 + i;
+        if (p >= npix) break;
+        if (mask[p]) {
+            c += 1.0f;
+            t2 += target[p] * target[p];
+        }
+    }
+    c = warp_sum_f(c);
+    t2 = warp_sum_f(t2);
     __shared__ float2 red[32];
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = make_float2(se, cnt);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = make_float2(c, t2);
     __syncthreads();
     if (threadIdx.x == 0) {
         float2 t = make_float2(0.0f, 0.0f);
@@ -496,11 +583,6 @@ __global__ void k_unet_loss(const float* out16, const float* target, const unsig
         }
         part[blockIdx.x] = t;
     }
-}
-__global__ void k_mask_count(const unsigned char* mask, int npix, unsigned int* count) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    const unsigned int c = __syncthreads_count(p < npix && mask[p]);
-    if (threadIdx.x == 0 && c) atomicAdd(count, c);
 }
 
 // ---------------------------------------------------------------------------
@@ -539,9 +621,8 @@ struct UNet {
     float *wpart, *bpart;
     size_t wpart_elems = 0;
     float2* lpart;
-    float *target, *prev32;
+    float *target, *prev32, *res32, *sigma;
     unsigned char* mask;
-    unsigned int* count;
     int* err;
     void* arena = nullptr;
     std::vector<void*> extra;
@@ -596,11 +677,13 @@ inline cudaError_t unet_alloc(UNet& n, int maxH, int maxW) {
     n.wpart_elems = ((P0 + 4095) / 4096) * 9 * 128 * 64;
     F(&n.wpart, n.wpart_elems);
     F(&n.bpart, ((P0 + 1023) / 1024) * 64);
-    items.push_back({(void**)&n.lpart, up256(((P0 + 1023) / 1024) * sizeof(float2))});
+    // per-block partials: loss blocks of 1024 pixels, residual blocks of 32 x 8 cells
+    items.push_back({(void**)&n.lpart, up256((P0 / 256 + (size_t)maxW / 32 + (size_t)maxH / 8 + 8) * sizeof(float2))});
     F(&n.target, P0);
     F(&n.prev32, P0);
+    F(&n.res32, P0);
+    F(&n.sigma, 64);
     items.push_back({(void**)&n.mask, up256(P0)});
-    items.push_back({(void**)&n.count, 256});
     items.push_back({(void**)&n.err, 256});
     size_t total = 0;
     for (auto& it : items) total += it.bytes;

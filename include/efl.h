@@ -353,14 +353,15 @@ EFL_API efl_status efl_batch_projection_ms(efl_batch* batch, float* ms);
 
 /* Extension, no reference counterpart.  A small U-Net (BF16 weights and
  * activations, FP32 accumulation; 4 levels, 16/32/64/64 channels, 3x3
- * convolutions on the tensor cores) predicts the change of the pressure
- * over a step from the system about to be solved; its prediction only
- * warm-starts the tolerance-driven solve, which still iterates to the same
- * residual.  Features per cell, 16 channels (5 used): cdiv * div / s, the u
- * and v face fractions averaged to the centre, phi / ny clamped to [-1, 1],
- * the previous pressure / s, with s = rho * |g| * ny * dx; output channel 0
- * = (p - p_prev) / s.  The head starts at zero, so an untrained network
- * warm-starts from the previous pressure exactly. */
+ * convolutions on the tensor cores) approximates the correction e = A^-1 r
+ * that the previous step's pressure p_prev needs on the new system
+ * (r = b - A p_prev); its prediction only warm-starts the tolerance-driven
+ * solve (x = p_prev + prediction), which still iterates to the same
+ * residual.  Features per cell, 16 channels (5 used): cdiv * r / sigma, the
+ * u and v face fractions averaged to the centre, phi / ny clamped to
+ * [-1, 1], 1 on the counted cells; sigma = RMS of cdiv * r over the counted
+ * cells; output channel 0 = e / sigma.  The head starts at zero, so an
+ * untrained network warm-starts from the previous pressure exactly. */
 typedef struct efl_unet efl_unet;
 enum { EFL_UNET_WARM_START = 1, EFL_UNET_RECORD = 2 };
 EFL_API efl_status efl_unet_create(int32_t device, uint32_t max_nx, uint32_t max_ny, uint64_t seed, efl_unet** out);
@@ -371,9 +372,11 @@ EFL_API efl_status efl_unet_get_params(efl_unet* net, float* params, uint64_t n)
 EFL_API efl_status efl_unet_set_params(efl_unet* net, const float* params, uint64_t n);
 /* Forward pass on host features [ny][nx][16]; pred [ny][nx] = output channel 0. */
 EFL_API efl_status efl_unet_forward(efl_unet* net, uint32_t nx, uint32_t ny, const float* features, float* pred);
-/* Forward + backward of the masked mean squared error against target
- * [ny][nx] over mask [ny][nx] != 0; loss and the gradient of every
- * parameter (efl_unet_num_params floats, the order of get/set_params). */
+/* Forward + backward of the relative squared error against target [ny][nx]
+ * over mask [ny][nx] != 0, sum (pred - t)^2 / sum t^2 (every sample weighs
+ * the same whatever the size of its pressure change); loss and the
+ * gradient of every parameter (efl_unet_num_params floats, the order of
+ * get/set_params). */
 EFL_API efl_status efl_unet_gradients(efl_unet* net, uint32_t nx, uint32_t ny, const float* features,
                                       const float* target, const uint8_t* mask, float* loss, float* grads);
 /* flags: EFL_UNET_WARM_START (warm-start sim's tolerance-driven solves),

@@ -138,14 +138,16 @@ class Net:
         return a["out"][:, :, 0]
 
     def backward(self, target, mask):
-        """Masked mean squared error of output channel 0; returns (loss, gradient vector)."""
+        """Relative squared error of output channel 0 over the mask,
+        sum (pred - t)^2 / sum t^2; returns (loss, gradient vector)."""
         a, r = self.a, self.r
         m = mask.astype(bool)
-        cnt = max(1, int(m.sum()))
+        t2 = float((np.asarray(target, np.float64)[m] ** 2).sum())
+        inv = 1.0 / t2 if t2 > 0 else 0.0
         d = a["out"][:, :, 0] - target
-        loss = float((d[m] ** 2).sum() / cnt)
+        loss = float((d[m] ** 2).sum() * inv)
         g = np.zeros_like(a["out"])
-        g[:, :, 0] = np.where(m, 2.0 * d / cnt, 0.0)
+        g[:, :, 0] = np.where(m, 2.0 * d * inv, 0.0)
         grads = [None] * len(SPEC)
 
         def cb(i, x, y, g, need_dx=True):
