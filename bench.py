@@ -68,9 +68,10 @@ def parse():
     ap.add_argument("--no-microbench", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-c3", action="store_true")
+    ap.add_argument("--no-learned", action="store_true")
     ap.add_argument("--c3-size", type=int, default=4096, help="grid of the C3 scale scene (4096 in the benchmark)")
     ap.add_argument("--batch-sims", type=int, default=96, help="simulations of the C4 batch (96 in the benchmark)")
-    ap.add_argument("--only", choices=["coupled", "microbench", "batch", "c3"], default=None,
+    ap.add_argument("--only", choices=["coupled", "microbench", "batch", "c3", "learned"], default=None,
                     help="profiling aid: run one part only and print its numbers")
     return ap.parse_args()
 
@@ -226,6 +227,9 @@ def main():
     if args.only == "microbench":
         print(json.dumps(microbench(capi.load(), None, torch, measured_peaks()[0])), flush=True)
         return 0
+    if args.only == "learned":
+        print(json.dumps(learned_leg(capi.load(), args, local)), flush=True)
+        return 0
     if args.only == "c3":
         print(json.dumps(c3_leg(capi.load(), torch, args, local, measured_peaks()[0])), flush=True)
         return 0
@@ -353,6 +357,9 @@ def main():
     c3 = None
     if not args.no_c3 and rank == 0 and args.only is None:
         c3 = c3_leg(api, torch, args, local, peak)
+    lw = None
+    if not args.no_learned and rank == 0 and args.only is None:
+        lw = learned_leg(api, args, local)
 
     sim.close()
     if dist:
@@ -385,6 +392,8 @@ def main():
         line["batch"] = batch
     if c3:
         line["c3"] = c3
+    if lw:
+        line["learned"] = lw
     print(json.dumps(line), flush=True)
     return 0
 
@@ -554,6 +563,47 @@ def coupled_mgpcg(api, torch, args, local, flush, dist):
             "value": world * sc.cells * args.steps / (ms / 1e3), "unit": "cell-steps/s",
             "ms_per_step": ms / args.steps, "pressure_solve_ms_per_step": sum(solve) / args.steps,
             "cg_iterations_per_step": iters}
+
+
+def tensor_peak():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        if "bf16_tflops" in d:
+            return float(d["bf16_tflops"]), "measured"
+    return 1590.0, "fallback"
+
+
+def learned_leg(api, args, local):
+    """The learned warm start: trained on the GPU (tensor-core forward and
+    backward) from C2-style scenes with seeds 1-8 at 256^2, then coupled_512
+    (the benchmark scene, RBGS to 1e-5) stepped twice from the same states,
+    warm-started by the network and from the previous pressure."""
+    from bevy_eulerian_fluid_b200 import learned, scenes
+    net, log = learned.train(api, size=256, seeds=tuple(range(1, 9)), steps=100, lr=1e-3, max_size=args.size,
+                             device=local)
+    sc = scenes.coupled(args.size)
+    sc.cfg.device = local
+    cmp = learned.compare(api, net, sc, warmup=args.warmup, steps=max(1, min(args.steps, 6)))
+    ms = net.time_forward(args.size, args.size, 20)
+    tf = learned.forward_flops(args.size, args.size) / (ms / 1e3) / 1e12
+    peak, kind = tensor_peak()
+    q = len(log.losses) // 4
+    out = {"training": {"samples": log.samples, "seconds": round(log.seconds, 2), "grid": "256^2",
+                        "relative_loss_by_quarter": [round(sum(log.losses[i * q:(i + 1) * q]) / max(1, q), 4)
+                                                     for i in range(4)]},
+           "workload": f"coupled_{args.size} (RBGS to 1e-5), {len(cmp['plain'])} steps after {args.warmup} warm-up",
+           "iterations": {"learned": [x[0] for x in cmp["learned"]], "plain": [x[0] for x in cmp["plain"]]},
+           "initial_residual": {"learned": [round(x[1], 5) for x in cmp["learned"]],
+                                "plain": [round(x[1], 5) for x in cmp["plain"]]},
+           "pressure_solve_ms_per_step": {"learned": sum(x[2] for x in cmp["learned"]) / len(cmp["learned"]),
+                                          "plain": sum(x[2] for x in cmp["plain"]) / len(cmp["plain"])},
+           "forward": {"ms": round(ms, 4), "grid": f"{args.size}^2", "tflops": round(tf, 2), "peak": peak,
+                       "peak_kind": kind, "frac": round(tf / peak, 4),
+                       "kernel": "k_conv3x3_tc (tcgen05.mma kind::f16, BF16 x BF16 -> FP32 in TMEM)"}}
+    net.close()
+    return out
 
 
 def c3_leg(api, torch, args, local, peak):

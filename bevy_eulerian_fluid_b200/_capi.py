@@ -146,13 +146,15 @@ SIGNATURES = {
                                  C.POINTER(C.c_float), C.c_void_p]),
     "unet_attach": (C.c_int, ["X", C.c_void_p, C.c_uint32]),
     "unet_train_step": (C.c_int, [C.c_void_p, C.c_float, C.POINTER(C.c_float)]),
+    "unet_time_forward": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(C.c_float)]),
 }
 # Functions of efl.h that the oracle restatement does not mirror.
 PRODUCT_ONLY = {"abi_version", "default_config", "field_device_ptr", "stream", "synchronize", "kernel_launches",
                 "pressure_sweeps", "residual_norms_noalloc", "batch_create", "batch_destroy", "batch_last_error",
                 "batch_sim", "batch_step", "batch_projection_ms", "projection_ms", "set_graph_capture",
                 "unet_create", "unet_destroy", "unet_last_error", "unet_num_params", "unet_get_params",
-                "unet_set_params", "unet_forward", "unet_gradients", "unet_attach", "unet_train_step"}
+                "unet_set_params", "unet_forward", "unet_gradients", "unet_attach", "unet_train_step",
+                "unet_time_forward"}
 
 
 class EflError(RuntimeError):
@@ -493,6 +495,12 @@ class UNet:
     def attach(self, sim: "Sim", warm_start: bool = True, record: bool = False):
         flags = (UNET_WARM_START if warm_start else 0) | (UNET_RECORD if record else 0)
         self._check(self.api.unet_attach(sim.h, self.h if flags else None, flags))
+
+    def time_forward(self, nx: int, ny: int, reps: int = 20) -> float:
+        """Device ms of one forward pass at nx x ny."""
+        ms = C.c_float()
+        self._check(self.api.unet_time_forward(self.h, nx, ny, reps, C.byref(ms)))
+        return ms.value
 
     def train_step(self, lr: float = 1e-3) -> float:
         loss = C.c_float()

@@ -1961,6 +1961,27 @@ efl_status efl_unet_gradients(efl_unet* u, uint32_t nx, uint32_t ny, const float
     return EFL_OK;
 }
 
+efl_status efl_unet_time_forward(efl_unet* u, uint32_t nx, uint32_t ny, uint32_t reps, float* ms) {
+    if (!u || !ms || !reps) return unet_err(u, EFL_ERR_INVALID_ARGUMENT, "null argument");
+    if (nx < 16 || ny < 16 || nx % 8 || ny % 8 || (int)nx > u->net.maxW || (int)ny > u->net.maxH)
+        return unet_err(u, EFL_ERR_INVALID_ARGUMENT, "bad grid");
+    cudaSetDevice(u->net.device);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    unet_forward(u->net, (int)ny, (int)nx, 0);  // warm-up
+    cudaEventRecord(e0, 0);
+    for (uint32_t i = 0; i < reps; ++i) unet_forward(u->net, (int)ny, (int)nx, 0);
+    cudaEventRecord(e1, 0);
+    efl_status st = unet_finish(u, 0);
+    float t = 0.0f;
+    cudaEventElapsedTime(&t, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *ms = t / (float)reps;
+    return st;
+}
+
 efl_status efl_unet_attach(efl_sim* s, efl_unet* u, uint32_t flags) {
     if (!s) return unet_err(u, EFL_ERR_INVALID_ARGUMENT, "null sim");
     if (u && (s->nx > u->net.maxW || s->ny > u->net.maxH || s->cfg.device != u->net.device))

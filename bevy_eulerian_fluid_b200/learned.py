@@ -18,6 +18,17 @@ from . import _capi as capi
 from . import scenes
 
 
+# (cin, cout) of the network's 15 convolutions and the level each runs at
+# (resolution / 2^level), for FLOP counts.
+UNET_CONVS = [(16, 16, 0), (16, 16, 0), (16, 32, 1), (32, 32, 1), (32, 64, 2), (64, 64, 2), (64, 64, 3), (64, 64, 3),
+              (128, 64, 2), (64, 64, 2), (96, 32, 1), (32, 32, 1), (48, 16, 0), (16, 16, 0), (16, 16, 0)]
+
+
+def forward_flops(nx: int, ny: int) -> float:
+    """Multiply-adds x 2 of one forward pass (the padded channels included)."""
+    return float(sum(2 * 9 * ci * co * (nx >> lv) * (ny >> lv) for ci, co, lv in UNET_CONVS))
+
+
 @dataclass
 class TrainLog:
     losses: List[float] = field(default_factory=list)

@@ -109,3 +109,18 @@ def test_unet_training_reduces_loss(gpu_api):
     sim.step(sc.dt)
     losses = [net.train_step(1e-3) for _ in range(60)]
     assert losses[-1] < 0.5 * losses[0]
+
+
+@pytest.mark.gpu
+def test_learned_warm_start_gain(gpu_api):
+    """What the trained network gains: after a short training on C2-style
+    scenes (other seeds), the initial relative residual of the benchmark
+    scene's solves falls well below that of the previous-pressure start,
+    and every solve still reaches the tolerance."""
+    from bevy_eulerian_fluid_b200 import learned, scenes
+    net, log = learned.train(gpu_api, size=128, seeds=(1, 2, 3, 4), steps=60, lr=1e-3, n_per_shape=2)
+    assert log.losses[-1] < log.losses[0]
+    out = learned.compare(gpu_api, net, scenes.coupled(128, n_per_shape=2), warmup=4, steps=4)
+    r_l = np.mean([x[1] for x in out["learned"]])
+    r_p = np.mean([x[1] for x in out["plain"]])
+    assert r_l < 0.7 * r_p, (r_l, r_p)
