@@ -77,8 +77,9 @@ def copy_state(src: capi.Sim, dst: capi.Sim):
 
 def compare(api: capi.Api, net: capi.UNet, scene: scenes.Scene, warmup: int = 5, steps: int = 10) -> dict:
     """Steps two copies of `scene` in lockstep, one warm-started by the
-    network, one from the previous pressure; per step the solver's iterations,
-    initial relative residual and solve time of each."""
+    network, one from the previous pressure (the same state before every
+    step); per step and copy: (iterations, initial relative residual, solve
+    ms, converged)."""
     a, b = scene.make(api), scene.make(api)
     for sim in (a, b):
         sim.step(scene.dt)
@@ -89,8 +90,10 @@ def compare(api: capi.Api, net: capi.UNet, scene: scenes.Scene, warmup: int = 5,
     out = {"learned": [], "plain": []}
     for _ in range(steps):
         sa, sb = a.step(scene.dt), b.step(scene.dt)
-        out["learned"].append((int(sa.pressure_iterations), float(sa.residual_initial), a.projection_ms()))
-        out["plain"].append((int(sb.pressure_iterations), float(sb.residual_initial), b.projection_ms()))
+        out["learned"].append((int(sa.pressure_iterations), float(sa.residual_initial), a.projection_ms(),
+                               bool(sa.converged)))
+        out["plain"].append((int(sb.pressure_iterations), float(sb.residual_initial), b.projection_ms(),
+                             bool(sb.converged)))
         copy_state(b, a)  # the same state again for the next step
     net.attach(a, warm_start=False)
     a.close()
