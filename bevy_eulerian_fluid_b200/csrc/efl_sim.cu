@@ -2000,11 +2000,21 @@ efl_status efl_unet_train_step(efl_unet* u, float lr, float* loss) {
     if (cudaDeviceSynchronize() != cudaSuccess)
         return unet_err(u, EFL_ERR_CUDA, std::string("device error: ") + cudaGetErrorString(cudaGetLastError()));
     TRY_U(unet_loss_and_grads(u, u->rec_ny, u->rec_nx, 0, loss));
+    // Global-norm clip at 1 (a sample far from the network's range would
+    // otherwise inflate Adam's second moments for thousands of steps).
+    const int nb = (int)((n.nparams + 1023) / 1024);
+    k_sumsq<<<nb, 256, count_launch(), 0>>>(n.grads, (int)n.nparams, n.wpart);
+    std::vector<float> part(nb);
+    cudaMemcpy(part.data(), n.wpart, nb * sizeof(float), cudaMemcpyDeviceToHost);
+    double g2 = 0.0;
+    for (float q : part) g2 += q;
+    const double gn = std::sqrt(g2);
+    const float gscale = (gn > 1.0 && std::isfinite(gn)) ? (float)(1.0 / gn) : (std::isfinite(gn) ? 1.0f : 0.0f);
     ++n.adam_t;
     const float b1 = 0.9f, b2 = 0.999f;
     const float c1 = 1.0f - std::pow(b1, (float)n.adam_t), c2 = 1.0f - std::pow(b2, (float)n.adam_t);
     k_adam<<<lin_grid(n.nparams), 256, count_launch(), 0>>>(n.params, n.grads, n.adam_m, n.adam_v, (int)n.nparams,
-                                                             lr, b1, b2, 1e-8f, c1, c2);
+                                                             lr, b1, b2, 1e-8f, c1, c2, gscale);
     unet_sync_weights(n, 0);
     return unet_finish(u, 0);
 }

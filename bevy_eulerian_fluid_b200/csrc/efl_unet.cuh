@@ -83,6 +83,12 @@ EFL_DEV void tmem_ld16(uint32_t taddr, float* v) {
 }
 __host__ __device__ constexpr uint32_t tmem_cols(int n) { return n <= 32 ? 32u : n <= 64 ? 64u : n <= 128 ? 128u : 256u; }
 
+EFL_DEV float warp_sum_f(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
 // Byte offset of element (row, k) in a K-major non-swizzled tile with K columns.
 EFL_DEV uint32_t kmajor_off(int row, int k, int K) {
     return (uint32_t)((row >> 3) * (K >> 3) * 128 + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2);
@@ -311,14 +317,24 @@ __global__ void k_wgrad_reduce(const float* part, int chunks, int mtiles, int ci
     dw[i] = s;
 }
 
-// db[co] = sum over pixels of dy[p][co] (per-block partials, then in order).
-__global__ void k_bgrad_partial(const bf16* dy, int npix, int cout, int pix_per_block, float* part) {
-    const int co = threadIdx.x;
-    if (co >= cout) return;
+// db[co] = sum over pixels of dy[p][co]: per block of pix_per_block pixels,
+// thread t sums channel t % cout over pixels t / cout, t / cout + 256 / cout,
+// ... in order; the groups are then added in order (deterministic).
+__global__ void __launch_bounds__(256) k_bgrad_partial(const bf16* dy, int npix, int cout, int pix_per_block,
+                                                       float* part) {
+    __shared__ float red[256];
+    const int t = threadIdx.x, groups = 256 / cout, c = t % cout, g = t / cout;
     const int p0 = blockIdx.x * pix_per_block, p1 = min(npix, p0 + pix_per_block);
     float s = 0.0f;
-    for (int p = p0; p < p1; ++p) s += __bfloat162float(dy[(size_t)p * cout + co]);
-    part[(size_t)blockIdx.x * cout + co] = s;
+    if (g < groups)
+        for (int p = p0 + g; p < p1; p += groups) s += __bfloat162float(dy[(size_t)p * cout + c]);
+    red[t] = s;
+    __syncthreads();
+    if (t < cout) {
+        float tot = 0.0f;
+        for (int q = 0; q < groups; ++q) tot += red[q * cout + t];
+        part[(size_t)blockIdx.x * cout + t] = tot;
+    }
 }
 __global__ void k_bgrad_reduce(const float* part, int blocks, int cout, float* db) {
     const int co = threadIdx.x;
@@ -389,12 +405,28 @@ __global__ void k_flip_transpose(const float* w32, int cin, int cout, bf16* w16,
     w16[i] = v;
     wt16[((size_t)(8 - tap) * cin + ci) * cout + co] = v;
 }
-// Adam (decoupled from the loss scale), fp32 master parameters.
+// Per-block sums of g^2 (1024 elements per block), for the global-norm clip.
+__global__ void __launch_bounds__(256) k_sumsq(const float* g, int n, float* part) {
+    float s = 0.0f;
+    const int i0 = blockIdx.x * 1024;
+    for (int i = i0 + threadIdx.x; i < min(n, i0 + 1024); i += 256) s += g[i] * g[i];
+    s = warp_sum_f(s);
+    __shared__ float red[8];
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float t = 0.0f;
+        for (int w = 0; w < 8; ++w) t += red[w];
+        part[blockIdx.x] = t;
+    }
+}
+// Adam on fp32 master parameters; the gradient is scaled by gscale first
+// (global-norm clipping).
 __global__ void k_adam(float* p, const float* g, float* m, float* v, int n, float lr, float b1, float b2, float eps,
-                       float c1, float c2) {
+                       float c1, float c2, float gscale) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const float gi = g[i];
+    const float gi = g[i] * gscale;
     const float mi = b1 * m[i] + (1.0f - b1) * gi;
     const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
     m[i] = mi;
@@ -416,12 +448,6 @@ namespace efl {
 // scale-free.  Channels (16, zero beyond 5): 0 = cdiv * r / sigma, 1 / 2 =
 // the u / v face fractions averaged to the cell centre, 3 = phi / ny clamped
 // to [-1, 1], 4 = 1 on the counted cells; output channel 0 = e / sigma.
-
-EFL_DEV float warp_sum_f(float v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
 
 struct UnetFeatureArgs {
     PF ls, fu, fv;
@@ -673,8 +699,8 @@ inline cudaError_t unet_alloc(UNet& n, int maxH, int maxW) {
     F(&n.g_u3, P3 * 64); F(&n.g_t3, P3 * 64); F(&n.g_p3, P3 * 64);
     F(&n.g_t2, P2 * 64); F(&n.g_p2, P2 * 32); F(&n.g_t1, P1 * 32); F(&n.g_p1, P1 * 16); F(&n.g_t0, P0 * 16);
     B(&n.dym, P0 * 16);
-    // weight-gradient partials: chunks of 4096 pixels x up to 9 row tiles x 128 x 64
-    n.wpart_elems = ((P0 + 4095) / 4096) * 9 * 128 * 64;
+    // weight-gradient partials: chunks of 1024 pixels x up to 9 row tiles x 128 x 64
+    n.wpart_elems = ((P0 + 1023) / 1024) * 9 * 128 * 64;
     F(&n.wpart, n.wpart_elems);
     F(&n.bpart, ((P0 + 1023) / 1024) * 64);
     // per-block partials: loss blocks of 1024 pixels, residual blocks of 32 x 8 cells
@@ -774,15 +800,15 @@ inline void unet_conv_bwd(UNet& n, int i, const bf16* x, int xs, int xo, const b
     w.W = W;
     w.cin = cin;
     w.cout = cout;
-    w.pix_per_cta = 4096;
+    w.pix_per_cta = 1024;
     w.part = n.wpart;
     w.err = n.err;
-    const int chunks = (npix + 4095) / 4096, mtiles = (9 * cin + 127) / 128;
+    const int chunks = (npix + 1023) / 1024, mtiles = (9 * cin + 127) / 128;
     k_wgrad_tc<<<dim3(chunks, mtiles), WG_THREADS, WG_SMEM + count_launch(), st>>>(w);
     k_wgrad_reduce<<<lin_grid((size_t)9 * cin * cout), 256, count_launch(), st>>>(n.wpart, chunks, mtiles, cin, cout,
                                                                                   n.grads + n.woff[i]);
     const int bblocks = (npix + 1023) / 1024;
-    k_bgrad_partial<<<bblocks, 64, count_launch(), st>>>(n.dym, npix, cout, 1024, n.bpart);
+    k_bgrad_partial<<<bblocks, 256, count_launch(), st>>>(n.dym, npix, cout, 1024, n.bpart);
     k_bgrad_reduce<<<1, 64, count_launch(), st>>>(n.bpart, bblocks, cout, n.grads + n.boff[i]);
     if (gx) {
         ConvArgs a;

@@ -386,7 +386,8 @@ EFL_API efl_status efl_unet_time_forward(efl_unet* net, uint32_t nx, uint32_t ny
  * EFL_UNET_RECORD (record each solve as a training sample); 0 detaches.
  * Batches (efl_batch_step) do not use it. */
 EFL_API efl_status efl_unet_attach(efl_sim* sim, efl_unet* net, uint32_t flags);
-/* One Adam step (lr; beta 0.9 / 0.999) on the last recorded sample. */
+/* One Adam step (lr; beta 0.9 / 0.999; gradient clipped to global norm 1)
+ * on the last recorded sample. */
 EFL_API efl_status efl_unet_train_step(efl_unet* net, float lr, float* loss);
 
 /* ---- Diagnostics ------------------------------------------------------ */
