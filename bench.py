@@ -429,7 +429,8 @@ def batch_leg(api, torch, args, world, rank, local, dist):
     bstream = torch.cuda.ExternalStream(bt[0].stream(), device=f"cuda:{local}")
     bt.step(dt)
     k = 0
-    for _ in range(args.warmup):
+    warm_b = max(args.warmup, 5)  # the tile autotuner tries its four configurations on the first four solves
+    for _ in range(warm_b):
         k += 1
         forces(bt.sims, k)
         bt.step(dt)
@@ -450,6 +451,7 @@ def batch_leg(api, torch, args, world, rank, local, dist):
     torch.cuda.synchronize()
     launches_b = api.kernel_launches() - launches0
     ms_b = e0.elapsed_time(e1)
+    tiles, tile_cost = bt.tiles()
     bt.close()
 
     # plain: efl_step per simulation, device time summed over the simulations' streams
@@ -461,7 +463,7 @@ def batch_leg(api, torch, args, world, rank, local, dist):
     for s_ in sims:
         s_.step(dt)
     k = 0
-    for _ in range(args.warmup):
+    for _ in range(warm_b):
         k += 1
         forces(sims, k)
         for s_ in sims:
@@ -499,13 +501,16 @@ def batch_leg(api, torch, args, world, rank, local, dist):
     return {"workload": f"batch_{len(bs.scenes)}: {len(bs.scenes)} simulations, sizes from "
                         "{128^2, 256x128, 256^2, 384x256, 512^2, 768x512}, "
                         "pools with droplets, 8 local forces every 30 steps, seed 0xC4, RBGS to 1e-5",
-            "cells": cells, "cells_this_rank": cells_rank, "steps": steps, "warmup": args.warmup,
+            "cells": cells, "cells_this_rank": cells_rank, "steps": steps, "warmup": warm_b,
             "value": cells * steps / (t[0] / 1e3), "plain_value": cells * steps / (t[1] / 1e3),
             "unit": "cell-steps/s", "speedup_vs_plain": round(t[1] / t[0], 3),
             "ms_per_step": {"batched": t[0] / steps, "plain": t[1] / steps},
             "pressure_solve_ms_per_step": {"batched": t[2] / steps, "plain": t[3] / steps},
             "pressure_iterations": {"max": max(iters), "mean": round(sum(iters) / len(iters), 1)},
-            "kernel": "k_batch_mix<64,32,2> (one cooperative launch per step for all simulations)",
+            "kernel": f"k_batch_mix<{tiles[0]},{tiles[1]},{tiles[2]}> (one cooperative launch per step for all "
+                      "simulations; tile shape and iterations per round chosen by the autotuner)",
+            "autotuner_ns_per_cell_iteration": {"64x32x2": round(tile_cost[0], 4), "64x32x4": round(tile_cost[1], 4),
+                                                "32x32x2": round(tile_cost[2], 4), "64x32x8": round(tile_cost[3], 4)},
             "gpu_launches_batched": int(launches_b),
             "l2": "not flushed: the batch's working set (GBs) exceeds L2",
             "sharding": f"simulation i on rank i % {world}"}

@@ -133,6 +133,9 @@ SIGNATURES = {
     "batch_sim": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(C.c_void_p)]),
     "batch_step": (C.c_int, [C.c_void_p, C.c_float, C.POINTER(StepStats)]),
     "batch_projection_ms": (C.c_int, [C.c_void_p, C.POINTER(C.c_float)]),
+    "batch_set_tiles": (C.c_int, [C.c_void_p, C.c_int32]),
+    "batch_tiles": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                              C.POINTER(C.c_double)]),
     "projection_ms": (C.c_int, ["X", C.POINTER(C.c_float)]),
     "set_graph_capture": (C.c_int, ["X", C.c_int32]),
     "unet_create": (C.c_int, [C.c_int32, C.c_uint32, C.c_uint32, C.c_uint64, C.POINTER(C.c_void_p)]),
@@ -151,7 +154,7 @@ SIGNATURES = {
 # Functions of efl.h that the oracle restatement does not mirror.
 PRODUCT_ONLY = {"abi_version", "default_config", "field_device_ptr", "stream", "synchronize", "kernel_launches",
                 "pressure_sweeps", "residual_norms_noalloc", "batch_create", "batch_destroy", "batch_last_error",
-                "batch_sim", "batch_step", "batch_projection_ms", "projection_ms", "set_graph_capture",
+                "batch_sim", "batch_step", "batch_projection_ms", "batch_set_tiles", "batch_tiles", "projection_ms", "set_graph_capture",
                 "unet_create", "unet_destroy", "unet_last_error", "unet_num_params", "unet_get_params",
                 "unet_set_params", "unet_forward", "unet_gradients", "unet_attach", "unet_train_step",
                 "unet_time_forward"}
@@ -416,6 +419,17 @@ class Batch:
         allow = (OK, NOT_CONVERGED) if allow_not_converged else (OK,)
         self._check(self.api.batch_step(self.h, dt, stats), allow)
         return list(stats)
+
+    def set_tiles(self, config: int):
+        """-1 = autotune (default), 0 / 1 / 2 / 3 = 64x32x2, 64x32x4, 32x32x2, 64x32x8."""
+        self._check(self.api.batch_set_tiles(self.h, config))
+
+    def tiles(self):
+        """((tx, ty, k) in use or (0, 0, 0) while tuning, [ns per cell-iteration of each configuration])."""
+        tx, ty, k = C.c_int32(), C.c_int32(), C.c_int32()
+        cost = (C.c_double * 4)()
+        self._check(self.api.batch_tiles(self.h, C.byref(tx), C.byref(ty), C.byref(k), cost))
+        return (tx.value, ty.value, k.value), list(cost)
 
     def projection_ms(self) -> float:
         """Device time of the last batched pressure solve (ms)."""

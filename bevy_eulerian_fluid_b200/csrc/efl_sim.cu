@@ -1467,10 +1467,34 @@ struct efl_batch {
     cudaEvent_t ev[2] = {nullptr, nullptr};  // around the last batched solve
     bool timed = false;
     GraphCache gc;  // the stages before and after the batched solve, all simulations
+    // Autotuner of the batched solve's tile shape and iterations per round:
+    // the first solves try each configuration once, timing ns per
+    // cell-iteration; the fastest is kept.
+    int tile_cfg = -1;           // chosen configuration, -1 while tuning
+    int tile_fixed = -1;         // set by efl_batch_set_tiles, -1 = autotune
+    int tune_next = 0;
+    std::vector<double> tune_cost;  // ns per cell-iteration, per configuration (0 = not tried)
 };
 
 namespace {
-constexpr int BT_TX = 64, BT_TY = 32, BT_K = 2;
+// Tile shapes (owned cells) and red-black iterations per streamed round of
+// the batched solve.  32 x 32 is the smallest tile: buffers are sized for it.
+struct BatchTileConfig {
+    int tx, ty, k;
+    const void* kern;
+    size_t smem;
+};
+template <int TX, int TY, int K>
+BatchTileConfig batch_config() {
+    constexpr int EX = TX + 4 * K, EY = TY + 4 * K;
+    return {TX, TY, K, (const void*)k_batch_mix<TX, TY, K>, sizeof(BatchTile<EX, EY>)};
+}
+const BatchTileConfig& batch_configs(int i) {
+    static const BatchTileConfig c[] = {batch_config<64, 32, 2>(), batch_config<64, 32, 4>(), batch_config<32, 32, 2>(),
+                                        batch_config<64, 32, 8>()};
+    return c[i];
+}
+constexpr int kBatchConfigs = 4, kMinTile = 32;
 std::string g_batch_error;
 
 efl_status batch_err(efl_batch* b, efl_status st, const std::string& m) {
@@ -1505,6 +1529,9 @@ void batch_free(efl_batch* b) {
 // tolerance), results into stats.
 efl_status batch_solve(efl_batch* b, const std::vector<int>& which, efl_step_stats* stats) {
     if (which.empty()) return EFL_OK;
+    if ((int)b->tune_cost.size() != kBatchConfigs) b->tune_cost.assign(kBatchConfigs, 0.0);
+    const int ci = b->tile_fixed >= 0 ? b->tile_fixed : (b->tile_cfg >= 0 ? b->tile_cfg : b->tune_next);
+    const BatchTileConfig& cfg = batch_configs(ci);
     std::vector<BatchSim> hs;
     std::vector<int2> tiles;
     for (int idx : which) {
@@ -1518,8 +1545,8 @@ efl_status batch_solve(efl_batch* b, const std::vector<int>& which, efl_step_sta
         S.cdiv = dx * dx * (double)s->U.rho / (double)s->U.dt;
         S.factor = (double)s->U.dt / (double)s->U.rho / dx / dx;
         S.weight = s->cfg.projection.sor_weight;
-        S.tiles_x = (s->nx + BT_TX - 1) / BT_TX;
-        const int ty = (s->ny + BT_TY - 1) / BT_TY;
+        S.tiles_x = (s->nx + cfg.tx - 1) / cfg.tx;
+        const int ty = (s->ny + cfg.ty - 1) / cfg.ty;
         S.tile_start = (int)tiles.size();
         S.tile_count = S.tiles_x * ty;
         for (int t = 0; t < S.tile_count; ++t) tiles.push_back(make_int2((int)hs.size(), t));
@@ -1553,9 +1580,8 @@ efl_status batch_solve(efl_batch* b, const std::vector<int>& which, efl_step_sta
     Pm.work_count = b->d_work_count;
     Pm.state = b->d_state;
     Pm.barrier = b->d_barrier;
-    constexpr int EX = BT_TX + 4 * BT_K, EY = BT_TY + 4 * BT_K;
-    const size_t smem = sizeof(BatchTile<EX, EY>);
-    const void* kern = (const void*)k_batch_mix<BT_TX, BT_TY, BT_K>;
+    const size_t smem = cfg.smem;
+    const void* kern = cfg.kern;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return batch_err(b, EFL_ERR_CUDA, "batched solver: shared-memory attribute refused");
     int per_sm = 0, sms = b->sims[which[0]]->solver.num_sms;
@@ -1564,7 +1590,7 @@ efl_status batch_solve(efl_batch* b, const std::vector<int>& which, efl_step_sta
     const int grid = std::min(per_sm * sms, std::max(1, nt));
     if (nt > BT_MAX_OWN * grid)
         return batch_err(b, EFL_ERR_INVALID_ARGUMENT,
-                         "batch too large: " + std::to_string(nt) + " tiles of 64 x 32 cells, at most " +
+                         "batch too large: " + std::to_string(nt) + " tiles, at most " +
                              std::to_string(BT_MAX_OWN * grid) + " per cooperative launch");
     void* args[] = {&Pm};
     count_launch();
@@ -1582,6 +1608,25 @@ efl_status batch_solve(efl_batch* b, const std::vector<int>& which, efl_step_sta
         cudaStreamSynchronize(st) != cudaSuccess)
         return batch_err(b, EFL_ERR_CUDA, std::string("batched solver failed: ") + cudaGetErrorString(cudaGetLastError()));
     if (hb.error) return batch_err(b, EFL_ERR_CUDA, "batched solver: a grid barrier timed out");
+    // Autotuner bookkeeping: device time per cell-iteration of this configuration.
+    double work = 0.0;
+    for (int i = 0; i < ns; ++i) {
+        const efl_sim* s = b->sims[which[i]];
+        work += (double)s->nx * s->ny * b->h_state[i].iterations;
+    }
+    float ms = 0.0f;
+    if (work > 0.0 && cudaEventElapsedTime(&ms, b->ev[0], b->ev[1]) == cudaSuccess) {
+        const double cost = ms * 1e6 / work;
+        if (b->tune_cost[ci] == 0.0 || cost < b->tune_cost[ci]) b->tune_cost[ci] = cost;
+        if (b->tile_fixed < 0 && b->tile_cfg < 0) {
+            if (++b->tune_next == kBatchConfigs) {
+                int best = 0;
+                for (int c = 1; c < kBatchConfigs; ++c)
+                    if (b->tune_cost[c] < b->tune_cost[best]) best = c;
+                b->tile_cfg = best;
+            }
+        }
+    }
     for (int i = 0; i < ns; ++i) {
         efl_step_stats* o = stats ? &stats[which[i]] : nullptr;
         if (!o) continue;
@@ -1629,7 +1674,7 @@ efl_status efl_batch_create(const efl_config* cfgs, uint32_t n, efl_batch** out)
             batch_free(b);
             return batch_err(nullptr, EFL_ERR_OUT_OF_MEMORY, m);
         }
-        total_tiles += ((s->nx + BT_TX - 1) / BT_TX) * ((s->ny + BT_TY - 1) / BT_TY);
+        total_tiles += ((s->nx + kMinTile - 1) / kMinTile) * ((s->ny + kMinTile - 1) / kMinTile);
     }
     b->ntiles = total_tiles;
     if (cudaMalloc(&b->d_sims, n * sizeof(BatchSim)) != cudaSuccess ||
@@ -1658,6 +1703,25 @@ const char* efl_batch_last_error(const efl_batch* b) { return b ? b->err.c_str()
 efl_status efl_batch_sim(efl_batch* b, uint32_t i, efl_sim** sim) {
     if (!b || !sim || i >= b->sims.size()) return batch_err(b, EFL_ERR_INVALID_ARGUMENT, "bad batch index");
     *sim = b->sims[i];
+    return EFL_OK;
+}
+
+efl_status efl_batch_set_tiles(efl_batch* b, int32_t config) {
+    if (!b || config < -1 || config >= kBatchConfigs) return batch_err(b, EFL_ERR_INVALID_ARGUMENT, "bad tile configuration");
+    b->tile_fixed = config;
+    return EFL_OK;
+}
+
+efl_status efl_batch_tiles(const efl_batch* b, int32_t* tx, int32_t* ty, int32_t* k, double* ns_per_cell_iteration) {
+    if (!b) return batch_err(nullptr, EFL_ERR_INVALID_ARGUMENT, "null batch");
+    const int ci = b->tile_fixed >= 0 ? b->tile_fixed : (b->tile_cfg >= 0 ? b->tile_cfg : -1);
+    const BatchTileConfig* c = ci >= 0 ? &batch_configs(ci) : nullptr;
+    if (tx) *tx = c ? c->tx : 0;
+    if (ty) *ty = c ? c->ty : 0;
+    if (k) *k = c ? c->k : 0;
+    if (ns_per_cell_iteration)
+        for (int i = 0; i < kBatchConfigs; ++i)
+            ns_per_cell_iteration[i] = i < (int)b->tune_cost.size() ? b->tune_cost[i] : 0.0;
     return EFL_OK;
 }
 

@@ -345,6 +345,18 @@ EFL_API const char* efl_batch_last_error(const efl_batch* batch);
 EFL_API efl_status efl_batch_sim(efl_batch* batch, uint32_t i, efl_sim** sim);
 /* One frame for every simulation (efl_step semantics); stats: n entries or NULL. */
 EFL_API efl_status efl_batch_step(efl_batch* batch, float dt, efl_step_stats* stats);
+/* Tile configurations of the batched solve (owned tile and red-black
+ * iterations per streamed round): 0 = 64 x 32 x 2, 1 = 64 x 32 x 4,
+ * 2 = 32 x 32 x 2, 3 = 64 x 32 x 8.  By default (config = -1) an autotuner
+ * runs the first four batched solves with one configuration each, timing
+ * device ns per
+ * cell-iteration, and keeps the fastest; every configuration gives the same
+ * iterates and iteration counts.  No reference counterpart. */
+EFL_API efl_status efl_batch_set_tiles(efl_batch* batch, int32_t config);
+/* The configuration in use (0, 0, 0 while tuning) and the measured cost of
+ * each (ns_per_cell_iteration: 4 entries or NULL; 0 = not tried). */
+EFL_API efl_status efl_batch_tiles(const efl_batch* batch, int32_t* tx, int32_t* ty, int32_t* k,
+                                   double* ns_per_cell_iteration);
 /* Device time of the last batched pressure solve (the cooperative launch), in
  * milliseconds; waits for it to finish. */
 EFL_API efl_status efl_batch_projection_ms(efl_batch* batch, float* ms);
