@@ -80,6 +80,12 @@ class SolidForce(C.Structure):
     _fields_ = [("force", C.c_float * 2), ("torque", C.c_float), ("_pad", C.c_float)]
 
 
+class RigidBodyC(C.Structure):  # efl_rigid_body
+    _fields_ = [("position", C.c_double * 2), ("rotation", C.c_double), ("linear_velocity", C.c_double * 2),
+                ("angular_velocity", C.c_double), ("mass", C.c_double), ("inertia", C.c_double),
+                ("extent", C.c_double), ("dynamic", C.c_int32), ("obstacle", C.c_int32)]
+
+
 class StepStats(C.Structure):
     _fields_ = [("initialized_only", C.c_int32), ("pressure_iterations", C.c_uint32), ("converged", C.c_int32),
                 ("_pad", C.c_int32), ("residual", C.c_double), ("residual_initial", C.c_double)]
@@ -138,6 +144,8 @@ SIGNATURES = {
                               C.POINTER(C.c_double)]),
     "projection_ms": (C.c_int, ["X", C.POINTER(C.c_float)]),
     "set_graph_capture": (C.c_int, ["X", C.c_int32]),
+    "set_rigid_bodies": (C.c_int, ["X", C.POINTER(RigidBodyC), C.c_uint32, C.c_double, C.c_double, C.c_uint32]),
+    "get_rigid_bodies": (C.c_int, ["X", C.POINTER(RigidBodyC), C.c_uint32]),
     "unet_create": (C.c_int, [C.c_int32, C.c_uint32, C.c_uint32, C.c_uint64, C.POINTER(C.c_void_p)]),
     "unet_destroy": (C.c_int, [C.c_void_p]),
     "unet_last_error": (C.c_char_p, [C.c_void_p]),
@@ -154,7 +162,7 @@ SIGNATURES = {
 # Functions of efl.h that the oracle restatement does not mirror.
 PRODUCT_ONLY = {"abi_version", "default_config", "field_device_ptr", "stream", "synchronize", "kernel_launches",
                 "pressure_sweeps", "residual_norms_noalloc", "batch_create", "batch_destroy", "batch_last_error",
-                "batch_sim", "batch_step", "batch_projection_ms", "batch_set_tiles", "batch_tiles", "projection_ms", "set_graph_capture",
+                "batch_sim", "batch_step", "batch_projection_ms", "batch_set_tiles", "batch_tiles", "projection_ms", "set_graph_capture", "set_rigid_bodies", "get_rigid_bodies",
                 "unet_create", "unet_destroy", "unet_last_error", "unet_num_params", "unet_get_params",
                 "unet_set_params", "unet_forward", "unet_gradients", "unet_attach", "unet_train_step",
                 "unet_time_forward"}
@@ -368,6 +376,16 @@ class Sim:
         p, pitch = C.c_void_p(), C.c_size_t()
         self._check(self.api.field_device_ptr(self.h, field, C.byref(p), C.byref(pitch)))
         return p.value, pitch.value
+
+    def set_rigid_bodies(self, bodies, gravity: float, grid_length: float, substeps: int = 1):
+        """Device-side coupling: bodies (RigidBodyC) integrated at the end of every step."""
+        arr = (RigidBodyC * max(1, len(bodies)))(*bodies)
+        self._check(self.api.set_rigid_bodies(self.h, arr, len(bodies), gravity, grid_length, substeps))
+
+    def get_rigid_bodies(self, n: int):
+        arr = (RigidBodyC * max(1, n))()
+        self._check(self.api.get_rigid_bodies(self.h, arr, n))
+        return list(arr)[:n]
 
     def set_graph_capture(self, enable: bool):
         """Replay repeating step segments as CUDA graphs (default on)."""

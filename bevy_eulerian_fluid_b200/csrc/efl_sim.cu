@@ -120,6 +120,10 @@ struct efl_sim {
     uint64_t graph_epoch = 1;     // counts the setters that change kernel arguments
     PF mix_d2{};       // second correction buffer (batched solve)
     bool owns_stream = true;
+    efl_rigid_body* d_rigid = nullptr;  // device-integrated bodies (efl_set_rigid_bodies)
+    int n_rigid = 0;
+    double rigid_gravity = 0.0, rigid_grid_length = 1.0;
+    int rigid_substeps = 1;
     struct efl_unet* unet = nullptr;  // learned warm start / training recorder
     uint32_t unet_flags = 0;
     int* h_err = nullptr;  // pinned copy of the TMA sweep's error flag
@@ -810,6 +814,73 @@ efl_status st_solid_forces(efl_sim* s) {  // render_node.rs:610-641; bins zeroed
     return EFL_OK;
 }
 
+// Semi-implicit Euler of the device-coupled bodies (one thread per body),
+// then their obstacles' column-major transforms, inverses and velocities.
+__global__ void k_rigid_step(efl_rigid_body* bodies, int n, const efl_solid_force* forces, efl_solid_obstacle* obs,
+                             double gravity, double grid_length, double dt, int substeps, double half_w,
+                             double half_h) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    efl_rigid_body b = bodies[i];
+    if (b.dynamic) {
+        const efl_solid_force f = forces[b.obstacle];
+        const double sc = dt / grid_length;
+        const double fx = (double)f.force[0] * sc, fy = -(double)f.force[1] * sc, tq = -(double)f.torque * sc;
+        const double h = dt / substeps;
+        for (int k = 0; k < substeps; ++k) {
+            double vx = b.linear_velocity[0], vy = b.linear_velocity[1];
+            vx += (fx / b.mass) * h;
+            vy += (fy / b.mass - gravity) * h;
+            const double w = b.inertia > 0.0 ? b.angular_velocity + (tq / b.inertia) * h : b.angular_velocity;
+            double px = b.position[0] + vx * h, py = b.position[1] + vy * h;
+            const double lox = -half_w + 1.0 + b.extent, hix = half_w - 1.0 - b.extent;
+            const double loy = -half_h + 1.0 + b.extent, hiy = half_h - 1.0 - b.extent;
+            if (px < lox) {
+                px = lox;
+                vx = fmax(vx, 0.0);
+            } else if (px > hix) {
+                px = hix;
+                vx = fmin(vx, 0.0);
+            }
+            if (py < loy) {
+                py = loy;
+                vy = fmax(vy, 0.0);
+            } else if (py > hiy) {
+                py = hiy;
+                vy = fmin(vy, 0.0);
+            }
+            b.position[0] = px;
+            b.position[1] = py;
+            b.linear_velocity[0] = vx;
+            b.linear_velocity[1] = vy;
+            b.angular_velocity = w;
+            b.rotation = fmod(b.rotation + w * h, 6.283185307179586);
+        }
+        bodies[i] = b;
+    }
+    efl_solid_obstacle& o = obs[b.obstacle];
+    const double c = cos(b.rotation), sn = sin(b.rotation), px = b.position[0], py = b.position[1];
+    float* m = o.transform;
+    float* v = o.inverse_transform;
+    for (int q = 0; q < 16; ++q) m[q] = v[q] = 0.0f;
+    m[0] = (float)c, m[1] = (float)sn, m[4] = (float)-sn, m[5] = (float)c, m[10] = 1.0f, m[12] = (float)px,
+    m[13] = (float)py, m[15] = 1.0f;
+    v[0] = (float)c, v[1] = (float)-sn, v[4] = (float)sn, v[5] = (float)c, v[10] = 1.0f,
+    v[12] = (float)(-(c * px + sn * py)), v[13] = (float)(sn * px - c * py), v[15] = 1.0f;
+    o.linear_velocity[0] = (float)b.linear_velocity[0];
+    o.linear_velocity[1] = (float)b.linear_velocity[1];
+    o.angular_velocity = (float)b.angular_velocity;
+}
+
+efl_status st_rigid(efl_sim* s) {
+    if (!s->n_rigid) return EFL_OK;
+    k_rigid_step<<<(s->n_rigid + 63) / 64, 64, count_launch(), s->stream>>>(
+        s->d_rigid, s->n_rigid, s->d_forces_out, s->d_obs, s->rigid_gravity, s->rigid_grid_length, (double)s->U.dt,
+        s->rigid_substeps, 0.5 * s->nx, 0.5 * s->ny);
+    LAUNCH_CHECK();
+    return EFL_OK;
+}
+
 efl_status run_stage(efl_sim* s, int stage, efl_step_stats* st) {
     switch (stage) {
         case EFL_STAGE_INIT: TRY(run_init(s)); s->status = 1; return EFL_OK;
@@ -835,7 +906,7 @@ efl_status run_stage(efl_sim* s, int stage, efl_step_stats* st) {
         case EFL_STAGE_FLUID_SOURCE: return st_fluid_source(s, s->src_cont);
         case EFL_STAGE_REINITIALIZE: return st_reinit(s);
         case EFL_STAGE_LEVELSET_GRADIENT: return st_gradient(s);
-        case EFL_STAGE_SOLID_FORCES: return st_solid_forces(s);
+        case EFL_STAGE_SOLID_FORCES: TRY(st_solid_forces(s)); return st_rigid(s);
         default: return set_err(s, EFL_ERR_INVALID_ARGUMENT, "unknown stage %d", stage);
     }
 }
@@ -1085,6 +1156,35 @@ efl_status efl_set_obstacles(efl_sim* s, const efl_solid_obstacle* o, uint32_t n
     if (n) CU(cudaMemcpyAsync(s->d_obs, o, n * sizeof(efl_solid_obstacle), cudaMemcpyHostToDevice, s->stream));
     s->n_obs = (int)n;
     return EFL_OK;
+}
+
+efl_status efl_set_rigid_bodies(efl_sim* s, const efl_rigid_body* b, uint32_t n, double gravity, double grid_length,
+                                uint32_t substeps) {
+    if (!s || (n && !b)) return set_err(s, EFL_ERR_INVALID_ARGUMENT, "null argument");
+    if (n > EFL_MAX_SOLIDS) return set_err(s, EFL_ERR_TOO_MANY, "too many rigid bodies: %u (max %d)", n, EFL_MAX_SOLIDS);
+    if (n && !(grid_length > 0.0)) return set_err(s, EFL_ERR_INVALID_ARGUMENT, "grid_length must be positive");
+    for (uint32_t i = 0; i < n; ++i)
+        if (b[i].obstacle < 0 || b[i].obstacle >= s->n_obs || (b[i].dynamic && !(b[i].mass > 0.0)))
+            return set_err(s, EFL_ERR_INVALID_ARGUMENT, "rigid body %u: obstacle index or mass out of range", i);
+    cudaSetDevice(s->device);
+    if (n && !s->d_rigid) TRY(alloc_raw(s, s->d_rigid, EFL_MAX_SOLIDS));
+    if (n) CU(cudaMemcpyAsync(s->d_rigid, b, n * sizeof(efl_rigid_body), cudaMemcpyHostToDevice, s->stream));
+    CU(cudaStreamSynchronize(s->stream));
+    s->n_rigid = (int)n;
+    s->rigid_gravity = gravity;
+    s->rigid_grid_length = grid_length;
+    s->rigid_substeps = std::max<uint32_t>(1, substeps);
+    ++s->graph_epoch;
+    return EFL_OK;
+}
+
+efl_status efl_get_rigid_bodies(efl_sim* s, efl_rigid_body* b, uint32_t n) {
+    if (!s || (n && !b)) return set_err(s, EFL_ERR_INVALID_ARGUMENT, "null argument");
+    if ((int)n > s->n_rigid) return set_err(s, EFL_ERR_INVALID_ARGUMENT, "only %d rigid bodies", s->n_rigid);
+    cudaSetDevice(s->device);
+    if (n) CU(cudaMemcpyAsync(b, s->d_rigid, n * sizeof(efl_rigid_body), cudaMemcpyDeviceToHost, s->stream));
+    CU(cudaStreamSynchronize(s->stream));
+    return check_device_errors(s);
 }
 
 efl_status efl_set_local_forces(efl_sim* s, const efl_force* f, uint32_t n) {

@@ -76,3 +76,24 @@ def _extent(b: RigidBody) -> float:
     if b.collider.shape == 2:
         return max(math.hypot(v[0], v[1]), math.hypot(v[2], v[3])) + v[4]
     return max(math.hypot(v[0], v[1]), math.hypot(v[2], v[3]), math.hypot(v[4], v[5]))
+
+
+def device_bodies(bodies: Sequence[RigidBody]):
+    """The bodies as efl_rigid_body records for the device-side coupling
+    (body i drives obstacle i of pack_obstacles)."""
+    from . import _capi as capi
+    out = []
+    for i, b in enumerate(bodies):
+        r = capi.RigidBodyC()
+        r.position[0], r.position[1] = b.position
+        r.rotation = b.rotation
+        r.linear_velocity[0], r.linear_velocity[1] = b.linear_velocity
+        r.angular_velocity = b.angular_velocity
+        m = b.density * b.collider.area()
+        r.mass = m
+        r.inertia = m * b.collider.inertia_per_mass()
+        r.extent = _extent(b)
+        r.dynamic = 1 if b.kind == RigidBodyKind.Dynamic else 0
+        r.obstacle = i
+        out.append(r)
+    return out

@@ -178,6 +178,26 @@ typedef struct efl_solid_force {
     float _pad;
 } efl_solid_force;
 
+/* A rigid body integrated on the device at the end of every step, from the
+ * step's FluidToSolidForce, moving the obstacle it drives for the next step
+ * (extension: the reference hands the forces to avian2d on the host,
+ * fluid_to_solid.rs:180-209, and reads them back a frame late).  World units
+ * are grid cells, centred on the domain, y up.  Per step: force * dt /
+ * grid_length with y flipped and the torque negated, semi-implicit Euler
+ * under gravity (world units / s^2 along -y) in `substeps` equal substeps,
+ * and a clamp keeping the centre `extent` + 1 inside the walls. */
+typedef struct efl_rigid_body {
+    double position[2];
+    double rotation;         /* radians */
+    double linear_velocity[2];
+    double angular_velocity;
+    double mass;
+    double inertia;          /* 0: the rotation is not integrated */
+    double extent;
+    int32_t dynamic;         /* 0: left in place */
+    int32_t obstacle;        /* index into the efl_set_obstacles list */
+} efl_rigid_body;
+
 typedef struct efl_step_stats {
     int32_t initialized_only;     /* 1: this call ran the init sequence only */
     uint32_t pressure_iterations; /* RB iterations (GS), V-cycles (MG), 50 (Jacobi) */
@@ -325,6 +345,15 @@ EFL_API efl_status efl_projection_ms(efl_sim* sim, float* ms);
 
 /* Number of cells with levelset_air < 0 (calculate_volume.wgsl:11-75). */
 EFL_API efl_status efl_fluid_volume(efl_sim* sim, uint64_t* cells);
+
+/* Device-side coupling: after efl_set_rigid_bodies (n <= 256, each driving
+ * one obstacle already set with efl_set_obstacles) every efl_step ends by
+ * integrating the bodies and rewriting their obstacles' transforms and
+ * velocities on the device -- no force read-back and no obstacle upload
+ * per step.  n = 0 switches it off.  efl_get_rigid_bodies reads the state. */
+EFL_API efl_status efl_set_rigid_bodies(efl_sim* sim, const efl_rigid_body* bodies, uint32_t n, double gravity,
+                                        double grid_length, uint32_t substeps);
+EFL_API efl_status efl_get_rigid_bodies(efl_sim* sim, efl_rigid_body* bodies, uint32_t n);
 
 /* ---- Batches of independent simulations ------------------------------ */
 
