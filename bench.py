@@ -345,8 +345,11 @@ def main():
 
     # ---- the same coupled loop with the MGPCG projection (an extension), device time per step
     alt = None
+    dev_rbgs = dev_mgpcg = None
     if args.only is None:
         alt = coupled_mgpcg(api, torch, args, local, flush, dist)
+        dev_rbgs = coupled_device(api, torch, args, local, flush, capi.PROJECTION_GAUSS_SEIDEL)
+        dev_mgpcg = coupled_device(api, torch, args, local, flush, capi.PROJECTION_MGPCG)
 
     micro = None
     if not args.no_microbench and rank == 0 and args.only is None:
@@ -388,6 +391,10 @@ def main():
         line["microbench"] = micro
     if alt:
         line["coupled_mgpcg"] = alt
+    if dev_rbgs:
+        line["coupled_device_coupling"] = {"note": "bodies integrated on the GPU (no per-step force read-back or "
+                                                   "obstacle upload); the body states read back each step",
+                                           "rbgs": dev_rbgs, "mgpcg": dev_mgpcg}
     if batch:
         line["batch"] = batch
     if c3:
@@ -514,6 +521,46 @@ def batch_leg(api, torch, args, world, rank, local, dist):
             "gpu_launches_batched": int(launches_b),
             "l2": "not flushed: the batch's working set (GBs) exceeds L2",
             "sharding": f"simulation i on rank i % {world}"}
+
+
+def coupled_device(api, torch, args, local, flush, method):
+    """coupled_512 with the bodies integrated on the device (efl_set_rigid_bodies):
+    per step the efl_step call and a read-back of the 24 body states; device
+    time per step (value) and the same with the read-back included (e2e)."""
+    from bevy_eulerian_fluid_b200 import _capi as capi
+    from bevy_eulerian_fluid_b200 import scenes
+    from bevy_eulerian_fluid_b200.rigid import device_bodies
+    sc = scenes.coupled(args.size, method=method)
+    sc.cfg.device = local
+    sim = sc.make(api)
+    stream = torch.cuda.ExternalStream(sim.stream(), device=f"cuda:{local}")
+    sim.step(sc.dt)
+    sim.set_rigid_bodies(device_bodies(sc.bodies), 9.8 * scenes.LENGTH_UNIT, 1.0 / scenes.LENGTH_UNIT)
+    nb = len(sc.bodies)
+    for _ in range(args.warmup):
+        sim.step(sc.dt)
+        sim.get_rigid_bodies(nb)
+    torch.cuda.synchronize()
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    iters = []
+    for k in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        ev[k][0].record(stream)
+        st = sim.step(sc.dt)
+        ev[k][1].record(stream)
+        sim.get_rigid_bodies(nb)  # D2H: body states for the caller
+        ev[k][2].record(stream)
+        iters.append(int(st.pressure_iterations))
+    torch.cuda.synchronize()
+    dev_ms = sum(e[0].elapsed_time(e[1]) for e in ev)
+    e2e_ms = sum(e[0].elapsed_time(e[2]) for e in ev)
+    sim.close()
+    return {"value": sc.cells * args.steps / (dev_ms / 1e3), "unit": "cell-steps/s",
+            "ms_per_step": dev_ms / args.steps,
+            "e2e": {"value": sc.cells * args.steps / (e2e_ms / 1e3), "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": nb * 80},
+            "iterations_per_step": iters}
 
 
 def coupled_mgpcg(api, torch, args, local, flush, dist):

@@ -100,6 +100,9 @@ EFL_DEV uint32_t kmajor_off(int row, int k, int K) {
 constexpr int CV_THREADS = 128, CV_MAX_CIN = 128, CV_MAX_COUT = 128;
 constexpr int CV_SMEM = 128 * CV_MAX_CIN * 2 + CV_MAX_COUT * CV_MAX_CIN * 2 + 64;
 
+// Dynamic shared memory of one convolution CTA: the A and B tiles, then the mbarrier.
+__host__ __device__ constexpr int conv_smem_bytes(int cin, int cout) { return 128 * cin * 2 + cout * cin * 2 + 64; }
+
 struct ConvArgs {
     const bf16* x;  // input [H*W][xs], channels [xo, xo + cin)
     int xs, xo;
@@ -115,9 +118,9 @@ struct ConvArgs {
 
 __global__ void __launch_bounds__(CV_THREADS) k_conv3x3_tc(ConvArgs a) {
     extern __shared__ __align__(128) unsigned char cv_smem[];
-    unsigned char* As = cv_smem;                        // 128 x cin
-    unsigned char* Bs = cv_smem + 128 * CV_MAX_CIN * 2;  // cout x cin
-    uint64_t* bar = reinterpret_cast<uint64_t*>(cv_smem + 128 * CV_MAX_CIN * 2 + CV_MAX_COUT * CV_MAX_CIN * 2);
+    unsigned char* As = cv_smem;                  // 128 x cin
+    unsigned char* Bs = cv_smem + 128 * a.cin * 2;  // cout x cin
+    uint64_t* bar = reinterpret_cast<uint64_t*>(cv_smem + conv_smem_bytes(a.cin, a.cout) - 64);
     __shared__ uint32_t s_tmem;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int npix = a.H * a.W, p0 = blockIdx.x * 128;
@@ -754,7 +757,7 @@ inline void unet_conv(UNet& n, int i, const bf16* x, int xs, int xo, int H, int 
     a.cin = kUnetSpec[i].cin;
     a.cout = kUnetSpec[i].cout;
     a.err = n.err;
-    k_conv3x3_tc<<<(H * W + 127) / 128, CV_THREADS, CV_SMEM + count_launch(), st>>>(a);
+    k_conv3x3_tc<<<(H * W + 127) / 128, CV_THREADS, conv_smem_bytes(a.cin, a.cout) + count_launch(), st>>>(a);
 }
 
 inline void unet_forward(UNet& n, int H, int W, cudaStream_t st) {
@@ -827,7 +830,7 @@ inline void unet_conv_bwd(UNet& n, int i, const bf16* x, int xs, int xo, const b
         a.cin = cout;
         a.cout = cin;
         a.err = n.err;
-        k_conv3x3_tc<<<(npix + 127) / 128, CV_THREADS, CV_SMEM + count_launch(), st>>>(a);
+        k_conv3x3_tc<<<(npix + 127) / 128, CV_THREADS, conv_smem_bytes(a.cin, a.cout) + count_launch(), st>>>(a);
     }
 }
 
