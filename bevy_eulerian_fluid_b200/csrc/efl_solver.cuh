@@ -116,15 +116,23 @@ constexpr unsigned char MODE_COUNTED = 4;  // counted in the residual norms
 
 // Sum of all CTAs' partials in CTA order; identical in every CTA.
 EFL_DEV double ps_total_relative(const double2* partials, int nblocks) {
+    // Warp 0: lane l adds partials l, l + 32, ... in order (independent loads,
+    // one round of latency), then a fixed xor-shuffle tree; the same in every CTA.
     __shared__ double s_rel;
-    if (threadIdx.x == 0) {
+    if (threadIdx.x < 32) {
         double r = 0.0, b = 0.0;
-        for (int i = 0; i < nblocks; ++i) {
-            double2 v = __ldcg(&partials[i]);
+        for (int i = threadIdx.x; i < nblocks; i += 32) {
+            const double2 v = __ldcg(&partials[i]);
             r += v.x;
             b += v.y;
         }
-        s_rel = b > 0.0 ? sqrt(r) / sqrt(b) : (r > 0.0 ? __longlong_as_double(0x7ff0000000000000ll) : 0.0);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            r += __shfl_xor_sync(0xffffffffu, r, o);
+            b += __shfl_xor_sync(0xffffffffu, b, o);
+        }
+        if (threadIdx.x == 0)
+            s_rel = b > 0.0 ? sqrt(r) / sqrt(b) : (r > 0.0 ? __longlong_as_double(0x7ff0000000000000ll) : 0.0);
     }
     __syncthreads();
     double v = s_rel;
