@@ -15,8 +15,9 @@
 // restated exactly by the CPU oracle: per row, every chunk of 32 columns is
 // summed in x order from 0.0 (one thread per chunk row, the 32 x 32 tile
 // staged through shared memory so that loads stay coalesced), the chunk sums
-// are added in chunk order, and the row sums in row order.  Cells outside the
-// sum contribute +0.0, which leaves a running sum unchanged.
+// are added in chunk order; the row sums are added in row order within groups
+// of 32 rows, and the group sums in group order.  Cells outside the sum
+// contribute +0.0, which leaves a running sum unchanged.
 #pragma once
 
 #include "efl_solver.cuh"
@@ -117,6 +118,7 @@ __global__ void k_chunk_rows(const double2* part, int nch, int ny, double2* rows
     const int y = blockIdx.x * blockDim.x + threadIdx.x;
     if (y >= ny) return;
     double2 acc = make_double2(0.0, 0.0);
+#pragma unroll 8
     for (int c = 0; c < nch; ++c) {
         const double2 v = part[(size_t)y * nch + c];
         acc.x = acc.x + v.x;
@@ -125,22 +127,29 @@ __global__ void k_chunk_rows(const double2* part, int nch, int ny, double2* rows
     rowsum[y] = acc;
 }
 
-// total = sum over y in order of rowsum[y] (one block; thread 0 adds).
+// total = sum over groups of 32 rows, in group order, of each group's rows
+// summed in row order (one block: thread g adds group g, thread 0 the groups).
 __global__ void __launch_bounds__(1024) k_rows_total(const double2* rowsum, int ny, double2* total) {
-    __shared__ double2 buf[2048];
-    double2 acc = make_double2(0.0, 0.0);
-    for (int y0 = 0; y0 < ny; y0 += 2048) {
-        const int n = min(2048, ny - y0);
-        for (int i = threadIdx.x; i < n; i += blockDim.x) buf[i] = rowsum[y0 + i];
-        __syncthreads();
-        if (threadIdx.x == 0)
-            for (int i = 0; i < n; ++i) {
-                acc.x = acc.x + buf[i].x;
-                acc.y = acc.y + buf[i].y;
-            }
-        __syncthreads();
+    __shared__ double2 grp[1024];
+    const int ngroups = (ny + 31) / 32;  // ny <= 32768
+    for (int g = threadIdx.x; g < ngroups; g += blockDim.x) {
+        double2 acc = make_double2(0.0, 0.0);
+        for (int y = 32 * g; y < min(ny, 32 * g + 32); ++y) {
+            const double2 v = rowsum[y];
+            acc.x = acc.x + v.x;
+            acc.y = acc.y + v.y;
+        }
+        grp[g] = acc;
     }
-    if (threadIdx.x == 0) *total = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double2 acc = make_double2(0.0, 0.0);
+        for (int g = 0; g < ngroups; ++g) {
+            acc.x = acc.x + grp[g].x;
+            acc.y = acc.y + grp[g].y;
+        }
+        *total = acc;
+    }
 }
 
 // x = 0 off the unknowns.

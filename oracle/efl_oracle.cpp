@@ -841,8 +841,9 @@ efl_status gs_mixed_solve(eflo_sim& s, uint32_t* iters_out, double* r0_out, doub
 
 // Reductions of the MGPCG solve, in a fixed order that the CUDA kernels
 // reproduce: per row, chunks of 32 columns are each summed in x order from
-// 0.0, the chunk sums are added in chunk order from 0.0, and the row sums are
-// added in row order from 0.0.
+// 0.0, the chunk sums are added in chunk order from 0.0; the row sums are
+// added in row order within groups of 32 rows and the group sums in group
+// order, each from 0.0.
 struct D2 {
     double x, y;
 };
@@ -864,9 +865,14 @@ D2 row_ordered_sum(int W, int H, F term) {
         rows[y] = row;
     });
     D2 tot{0.0, 0.0};
-    for (int y = 0; y < H; ++y) {
-        tot.x = tot.x + rows[y].x;
-        tot.y = tot.y + rows[y].y;
+    for (int g = 0; g < H; g += 32) {  // rows in order within groups of 32, groups in order
+        D2 grp{0.0, 0.0};
+        for (int y = g; y < std::min(H, g + 32); ++y) {
+            grp.x = grp.x + rows[y].x;
+            grp.y = grp.y + rows[y].y;
+        }
+        tot.x = tot.x + grp.x;
+        tot.y = tot.y + grp.y;
     }
     return tot;
 }
