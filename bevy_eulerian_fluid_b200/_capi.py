@@ -128,6 +128,7 @@ SIGNATURES = {
     "synchronize": (C.c_int, ["X"]),
     "residual": (C.c_int, ["X", C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "fluid_volume": (C.c_int, ["X", C.POINTER(C.c_uint64)]),
+    "velocity_magnitude": (C.c_int, ["X", C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "kernel_launches": (C.c_uint64, []),
     "pressure_sweeps": (C.c_int, ["X", C.c_int32, C.c_uint32]),
     "residual_norms_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
@@ -362,6 +363,12 @@ class Sim:
         c = C.c_uint64()
         self._check(self.api.fluid_volume(self.h, C.byref(c)))
         return c.value
+
+    def velocity_magnitude(self):
+        """(min over fluid cells, max) of the cell-centred speed, as the reference's diagnostics compute them."""
+        a, b = C.c_float(), C.c_float()
+        self._check(self.api.velocity_magnitude(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
 
     def synchronize(self):
         self._check(self.api.synchronize(self.h))

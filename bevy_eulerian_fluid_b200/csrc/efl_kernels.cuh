@@ -1033,4 +1033,55 @@ __global__ void k_volume(PF ls0, unsigned long long* out) {
     if ((threadIdx.x & 31) == 0 && mask) atomicAdd(out, (unsigned long long)__popc(mask));
 }
 
+// diagnostics/{min,max}_velocity.wgsl partial_reduction: one 16 x 16 block
+// per workgroup; min over fluid cells (1e30 elsewhere), max over all cells.
+__global__ void __launch_bounds__(256) k_velocity_partial(PF u, PF v, PF ls, float* pmin, float* pmax) {
+    __shared__ float smin[256], smax[256];
+    const int x = blockIdx.x * 16 + threadIdx.x, y = blockIdx.y * 16 + threadIdx.y;
+    const int lid = threadIdx.y * 16 + threadIdx.x;
+    const float u0 = 0.5f * (u.ld(x, y) + u.ld(x + 1, y));
+    const float v0 = 0.5f * (v.ld(x, y) + v.ld(x, y + 1));
+    const float mag = sqrtf(u0 * u0 + v0 * v0);
+    smin[lid] = ls.ld(x, y) < 0.0f ? mag : 1e30f;
+    smax[lid] = mag;
+    __syncthreads();
+    for (int st = 128; st > 0; st >>= 1) {
+        if (lid < st) {
+            smin[lid] = fminf(smin[lid], smin[lid + st]);
+            smax[lid] = fmaxf(smax[lid], smax[lid + st]);
+        }
+        __syncthreads();
+    }
+    if (lid == 0) {
+        const int w = blockIdx.x + blockIdx.y * gridDim.x;
+        pmin[w] = smin[0];
+        pmax[w] = smax[0];
+    }
+}
+// diagnostics/{min,max}_velocity.wgsl reduction: 512 lanes each ADD their
+// partials i = lane, lane + 512, ... from 0.0 (as the reference does), then min / max.
+__global__ void __launch_bounds__(512) k_velocity_final(const float* pmin, const float* pmax, int n, float* out) {
+    __shared__ float smin[512], smax[512];
+    const int lid = threadIdx.x;
+    float a = 0.0f, b = 0.0f;
+    for (int i = lid; i < n; i += 512) {
+        a += pmin[i];
+        b += pmax[i];
+    }
+    smin[lid] = a;
+    smax[lid] = b;
+    __syncthreads();
+    for (int st = 256; st > 0; st >>= 1) {
+        if (lid < st) {
+            smin[lid] = fminf(smin[lid], smin[lid + st]);
+            smax[lid] = fmaxf(smax[lid], smax[lid + st]);
+        }
+        __syncthreads();
+    }
+    if (lid == 0) {
+        out[0] = smin[0];
+        out[1] = smax[0];
+    }
+}
+
 }  // namespace efl

@@ -120,6 +120,8 @@ struct efl_sim {
     uint64_t graph_epoch = 1;     // counts the setters that change kernel arguments
     PF mix_d2{};       // second correction buffer (batched solve)
     bool owns_stream = true;
+    float* d_vel = nullptr;  // velocity-magnitude partials (efl_velocity_magnitude)
+    int cap_vel = 0;
     efl_rigid_body* d_rigid = nullptr;  // device-integrated bodies (efl_set_rigid_bodies)
     int n_rigid = 0;
     double rigid_gravity = 0.0, rigid_grid_length = 1.0;
@@ -1100,6 +1102,7 @@ efl_status efl_destroy(efl_sim* s) {
     if (s->d_forces) cudaFree(s->d_forces);
     if (s->h_norms) cudaFreeHost(s->h_norms);
     if (s->cg.h_read) cudaFreeHost(s->cg.h_read);
+    if (s->d_vel) cudaFree(s->d_vel);
     for (cudaEvent_t e : s->ev_proj)
         if (e) cudaEventDestroy(e);
     s->gc.clear();
@@ -1429,6 +1432,28 @@ efl_status efl_fluid_volume(efl_sim* s, uint64_t* cells) {
     CU(cudaMemcpyAsync(&c, s->d_count, sizeof(c), cudaMemcpyDeviceToHost, s->stream));
     CU(cudaStreamSynchronize(s->stream));
     *cells = c;
+    return EFL_OK;
+}
+
+efl_status efl_velocity_magnitude(efl_sim* s, float* min_mag, float* max_mag) {
+    if (!s) return set_err(nullptr, EFL_ERR_INVALID_ARGUMENT, "null sim");
+    cudaSetDevice(s->device);
+    const int gx = s->nx / 16, gy = s->ny / 16, n = gx * gy;
+    if (s->cap_vel < n) {
+        if (s->d_vel) cudaFree(s->d_vel);
+        s->d_vel = nullptr;
+        CU(cudaMalloc(&s->d_vel, (size_t)(2 * n + 2) * sizeof(float)));
+        s->cap_vel = n;
+    }
+    k_velocity_partial<<<dim3(gx, gy), dim3(16, 16), count_launch(), s->stream>>>(s->u0, s->v0, s->ls0, s->d_vel,
+                                                                                  s->d_vel + n);
+    k_velocity_final<<<1, 512, count_launch(), s->stream>>>(s->d_vel, s->d_vel + n, n, s->d_vel + 2 * n);
+    LAUNCH_CHECK();
+    float r[2];
+    CU(cudaMemcpyAsync(r, s->d_vel + 2 * n, sizeof(r), cudaMemcpyDeviceToHost, s->stream));
+    CU(cudaStreamSynchronize(s->stream));
+    if (min_mag) *min_mag = r[0];
+    if (max_mag) *max_mag = r[1];
     return EFL_OK;
 }
 

@@ -465,5 +465,25 @@ class Fluid:
         n = capi.MAX_SOLIDS if n is None else n
         return [FluidToSolidForce((float(a[0]), float(a[1])), float(a[2])) for a in arr[:n]]
 
+    # diagnostics (diagnostics/component.rs: FluidVolume, FluidMin/MaxVelocityMagnitude)
+    def diagnostics(self) -> "FluidDiagnostics":
+        mn, mx = self.sim.velocity_magnitude()
+        return FluidDiagnostics(volume=self.sim.fluid_volume(), min_velocity_magnitude=mn, max_velocity_magnitude=mx)
+
     def close(self):
         self.sim.close()
+
+
+@dataclass
+class FluidDiagnostics:
+    volume: int                    # fluid cells (calculate_volume.wgsl)
+    min_velocity_magnitude: float  # min_velocity.wgsl, grid units per second
+    max_velocity_magnitude: float  # max_velocity.wgsl
+
+
+def cfl_dt(max_velocity_magnitude: float, cfl: float = 1.0, dt_max: float = 1.0 / 60.0) -> float:
+    """A time step that moves no fluid more than `cfl` cells (adaptive dt from
+    the max-velocity monitor): min(dt_max, cfl / max_velocity_magnitude)."""
+    if not (max_velocity_magnitude > 0.0):
+        return dt_max
+    return min(dt_max, cfl / max_velocity_magnitude)

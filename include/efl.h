@@ -345,6 +345,16 @@ EFL_API efl_status efl_projection_ms(efl_sim* sim, float* ms);
 
 /* Number of cells with levelset_air < 0 (calculate_volume.wgsl:11-75). */
 EFL_API efl_status efl_fluid_volume(efl_sim* sim, uint64_t* cells);
+/* FluidMinVelocityMagnitude / FluidMaxVelocityMagnitude
+ * (diagnostics/min_velocity.wgsl, max_velocity.wgsl): the cell-centred
+ * speed |(u, v)| reduced by 16 x 16 workgroups (the minimum over fluid cells,
+ * 1e30 elsewhere; the maximum over all cells), then by the reference's second
+ * pass, which first ADDS the partials i, i + 512, i + 1024, ... from 0.0 per
+ * lane before the min / max over 512 lanes -- so a grid of fewer than 512
+ * workgroups reports a minimum of 0 and a grid of more than 512 can report a
+ * maximum above the true one.  Both quirks are kept for parity; use them as
+ * the reference's monitor, e.g. for a CFL time step. */
+EFL_API efl_status efl_velocity_magnitude(efl_sim* sim, float* min_mag, float* max_mag);
 
 /* Device-side coupling: after efl_set_rigid_bodies (n <= 256, each driving
  * one obstacle already set with efl_set_obstacles) every efl_step ends by

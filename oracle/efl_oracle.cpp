@@ -1873,6 +1873,45 @@ efl_status eflo_residual(eflo_sim* s, double* rel, double* nr, double* nb) {
     return EFL_OK;
 }
 
+// diagnostics/{min,max}_velocity.wgsl: partial_reduction over 16 x 16
+// workgroups of the cells x < nx, y < ny, then `reduction` with 512 lanes,
+// each adding its partials in order from 0.0 before the min / max.
+efl_status eflo_velocity_magnitude(eflo_sim* s, float* min_mag, float* max_mag) {
+    if (!s) return EFL_ERR_INVALID_ARGUMENT;
+    const int gx = s->nx / 16, gy = s->ny / 16, n = gx * gy;
+    std::vector<float> pmin(n), pmax(n);
+    for (int wy = 0; wy < gy; ++wy)
+        for (int wx = 0; wx < gx; ++wx) {
+            float mn = 0.0f, mx = 0.0f;
+            bool first = true;
+            for (int y = 16 * wy; y < 16 * wy + 16; ++y)
+                for (int x = 16 * wx; x < 16 * wx + 16; ++x) {
+                    const float u0 = 0.5f * (s->u0.ld(x, y) + s->u0.ld(x + 1, y));
+                    const float v0 = 0.5f * (s->v0.ld(x, y) + s->v0.ld(x, y + 1));
+                    const float mag = std::sqrt(u0 * u0 + v0 * v0);
+                    const float lo = s->ls0.ld(x, y) < 0.0f ? mag : 1e30f;
+                    mn = first ? lo : std::fmin(mn, lo);
+                    mx = first ? mag : std::fmax(mx, mag);
+                    first = false;
+                }
+            pmin[wy * gx + wx] = mn;
+            pmax[wy * gx + wx] = mx;
+        }
+    float rmin = 0.0f, rmax = 0.0f;
+    for (int lane = 0; lane < 512; ++lane) {
+        float a = 0.0f, b = 0.0f;
+        for (int i = lane; i < n; i += 512) {
+            a += pmin[i];
+            b += pmax[i];
+        }
+        rmin = lane == 0 ? a : std::fmin(rmin, a);
+        rmax = lane == 0 ? b : std::fmax(rmax, b);
+    }
+    if (min_mag) *min_mag = rmin;
+    if (max_mag) *max_mag = rmax;
+    return EFL_OK;
+}
+
 efl_status eflo_fluid_volume(eflo_sim* s, uint64_t* cells) {
     if (!s || !cells) return EFL_ERR_INVALID_ARGUMENT;
     uint64_t c = 0;

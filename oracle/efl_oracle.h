@@ -46,6 +46,7 @@ EFL_API efl_status eflo_get_field(eflo_sim* sim, int32_t field, void* host_dst, 
 EFL_API efl_status eflo_set_field(eflo_sim* sim, int32_t field, const void* host_src, size_t bytes);
 EFL_API efl_status eflo_residual(eflo_sim* sim, double* relative, double* norm_r, double* norm_b);
 EFL_API efl_status eflo_fluid_volume(eflo_sim* sim, uint64_t* cells);
+EFL_API efl_status eflo_velocity_magnitude(eflo_sim* sim, float* min_mag, float* max_mag);
 
 /* Number of OpenMP threads the oracle uses (0 = OpenMP default). */
 EFL_API void eflo_set_threads(int32_t n);

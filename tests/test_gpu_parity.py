@@ -243,3 +243,15 @@ def test_device_coupling_matches_host_loop(gpu_api):
         assert abs(g.rotation - b.rotation) < 1e-4
     d = rel_max_err(dev.get(capi.FIELD_PRESSURE), host.get(capi.FIELD_PRESSURE))
     assert d < 1e-3, d
+
+
+def test_velocity_magnitude_diagnostics(oracle_api, gpu_api):
+    """diagnostics/{min,max}_velocity.wgsl on both backends, bit for bit."""
+    for n in (128, 512):  # 64 and 1024 workgroups: below and above the second pass's 512 lanes
+        sc = scenes.dam_break(n)
+        o, g = make_pair(sc, oracle_api, gpu_api)
+        for _ in range(4):
+            o.step(sc.dt)
+            g.step(sc.dt)
+        copy_state(o, g)
+        assert g.velocity_magnitude() == o.velocity_magnitude()

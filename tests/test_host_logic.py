@@ -161,3 +161,20 @@ def test_mgpcg_requires_tolerance(oracle_api):
     cfg.projection.tolerance = 0.0
     with pytest.raises(capi.EflError):
         capi.Sim(oracle_api, cfg)
+
+
+def test_velocity_magnitude_oracle_semantics(oracle_api):
+    """The reference's second reduction pass adds partials per lane from 0.0,
+    so a grid of fewer than 512 16x16 workgroups reports a minimum of 0; the
+    maximum there is the true maximum of the cell-centred speed."""
+    sc = scenes.dam_break(64)
+    sim = sc.make(oracle_api)
+    for _ in range(5):
+        sim.step(sc.dt)
+    mn, mx = sim.velocity_magnitude()
+    u, v = sim.get(capi.FIELD_U), sim.get(capi.FIELD_V)
+    uc = 0.5 * (u[:, :-1] + u[:, 1:])
+    vc = 0.5 * (v[:-1, :] + v[1:, :])
+    speed = np.sqrt(uc * uc + vc * vc).astype(np.float32)
+    assert mn == 0.0
+    assert mx == pytest.approx(float(speed.max()), rel=1e-6)
