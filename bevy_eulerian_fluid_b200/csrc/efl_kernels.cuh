@@ -696,6 +696,83 @@ __global__ void k_extrapolate(PF f, PI vin, PI vout, int x1, int y1) {
     }
 }
 
+// initialize_{u,v}_valid + the 10 extrapolation sweeps of render_node.rs:540-608
+// in ONE launch, for grids whose dispatches cover every face (nx and ny
+// multiples of 64): blockIdx.z = component; each CTA owns a 32 x 32 tile of
+// faces, holds it with a 10-face halo in shared memory and runs the sweeps
+// there (each sweep reads the valid flags of the previous one and only
+// valid neighbours' velocities, so the result equals 10 global sweeps).
+// Writes the velocity, the final flags (the "in" plane) and the flags after
+// the ninth sweep (the "out" plane), as the per-sweep kernels leave them.
+constexpr int EX_T = 32, EX_H = 10, EX_E = EX_T + 2 * EX_H;
+struct ExtrapArgs {
+    PF f[2];
+    PI vin[2], vout[2];
+    PF ls;
+};
+__global__ void __launch_bounds__(256) k_extrapolate_fused(ExtrapArgs a) {
+    __shared__ float sf[EX_E][EX_E];
+    __shared__ unsigned char sv[2][EX_E][EX_E];
+    const int comp = blockIdx.z;
+    const PF f = a.f[comp];
+    const int W = f.w, H = f.h;
+    const int x0 = blockIdx.x * EX_T - EX_H, y0 = blockIdx.y * EX_T - EX_H;
+    const int tid = threadIdx.x;
+    for (int i = tid; i < EX_E * EX_E; i += 256) {
+        const int ly = i / EX_E, lx = i - ly * EX_E, x = x0 + lx, y = y0 + ly;
+        float fv = 0.0f;
+        unsigned char v = 0;
+        if ((unsigned)x < (unsigned)W && (unsigned)y < (unsigned)H) {
+            fv = f.at(x, y);
+            float c0, c1, c2, c3, c4, c5;  // extrapolate/initialize_{u,v}_valid.wgsl
+            if (comp == 0) {
+                c0 = a.ls.ld(x - 1, y - 1); c1 = a.ls.ld(x, y - 1); c2 = a.ls.ld(x - 1, y);
+                c3 = a.ls.ld(x, y); c4 = a.ls.ld(x - 1, y + 1); c5 = a.ls.ld(x, y + 1);
+            } else {
+                c0 = a.ls.ld(x - 1, y - 1); c1 = a.ls.ld(x - 1, y); c2 = a.ls.ld(x, y - 1);
+                c3 = a.ls.ld(x, y); c4 = a.ls.ld(x + 1, y - 1); c5 = a.ls.ld(x + 1, y);
+            }
+            const float vm = 0.25f * (c0 + c1 + c2 + c3);
+            const float vp = 0.25f * (c2 + c3 + c4 + c5);
+            v = area_fraction(vm, vp) > 0.0f ? 0 : 1;
+        }
+        sf[ly][lx] = fv;
+        sv[0][ly][lx] = v;
+    }
+    __syncthreads();
+    for (int s = 0; s < 10; ++s) {
+        const int in = s & 1, out = in ^ 1, lo = 1 + s, n = EX_E - 2 * lo;
+        for (int i = tid; i < n * n; i += 256) {
+            const int ly = lo + i / n, lx = lo + i % n, x = x0 + lx, y = y0 + ly;
+            if ((unsigned)x >= (unsigned)W || (unsigned)y >= (unsigned)H) continue;
+            if (sv[in][ly][lx] == 1) {
+                sv[out][ly][lx] = 1;
+                continue;
+            }
+            int count = 0;
+            float nu = 0.0f;  // extrapolate_{u,v}.wgsl:5-63, neighbour order and bounds as the reference
+            if (x + 1 < W && sv[in][ly][lx + 1] == 1) { nu += sf[ly][lx + 1]; count += 1; }
+            if (x - 1 > 0 && y > 0 && sv[in][ly][lx - 1] == 1) { nu += sf[ly][lx - 1]; count += 1; }
+            if (y + 1 < H && sv[in][ly + 1][lx] == 1) { nu += sf[ly + 1][lx]; count += 1; }
+            if (x > 0 && y - 1 > 0 && sv[in][ly - 1][lx] == 1) { nu += sf[ly - 1][lx]; count += 1; }
+            if (count > 0) {
+                sf[ly][lx] = nu / (float)count;
+                sv[out][ly][lx] = 1;
+            } else {
+                sv[out][ly][lx] = 0;
+            }
+        }
+        __syncthreads();
+    }
+    for (int i = tid; i < EX_T * EX_T; i += 256) {
+        const int ly = EX_H + i / EX_T, lx = EX_H + i % EX_T, x = x0 + lx, y = y0 + ly;
+        if ((unsigned)x >= (unsigned)W || (unsigned)y >= (unsigned)H) continue;
+        f.at(x, y) = sf[ly][lx];
+        a.vin[comp].at(x, y) = sv[0][ly][lx];   // after the tenth sweep
+        a.vout[comp].at(x, y) = sv[1][ly][lx];  // after the ninth
+    }
+}
+
 // advect_levelset.wgsl:49-74
 EFL_DEV float cubic1d(float y0, float y1, float y2, float y3, float t) {
     float d1 = 0.5f * (y2 - y0);

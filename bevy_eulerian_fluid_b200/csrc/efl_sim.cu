@@ -781,6 +781,13 @@ efl_status st_solve_velocity(efl_sim* s) {
 }
 efl_status st_extrapolate(efl_sim* s) {  // render_node.rs:540-608
     Dom d = s->dom();
+    if (d.nx % 64 == 0 && d.ny % 64 == 0) {  // every face covered: one fused launch
+        ExtrapArgs a{{s->u0, s->v0}, {s->uvi, s->vvi}, {s->uvo, s->vvo}, s->ls0};
+        const dim3 g((d.nx + 1 + EX_T - 1) / EX_T, (d.ny + 1 + EX_T - 1) / EX_T, 2);
+        k_extrapolate_fused<<<g, 256, count_launch(), s->stream>>>(a);
+        LAUNCH_CHECK();
+        return EFL_OK;
+    }
     dim3 gu = grid2d(d.nx + 1, d.ny, kBlock), gv = grid2d(d.nx, d.ny + 1, kBlock);
     int xrows = (d.ny / 64) * 64, ycols = (d.nx / 64) * 64;
     k_init_valid<0><<<gu, kBlock, count_launch(), s->stream>>>(s->uvi, s->ls0, d);
