@@ -255,3 +255,59 @@ def test_velocity_magnitude_diagnostics(oracle_api, gpu_api):
             g.step(sc.dt)
         copy_state(o, g)
         assert g.velocity_magnitude() == o.velocity_magnitude()
+
+
+# ---------------------------------------------------------------------------
+# Edge cases of the domain: empty fluid, ragged (non-square, not a multiple of
+# 64) grids, the maximum number of obstacles and sources.
+
+@pytest.mark.parametrize("tolerance", [0.0, 1e-5])
+def test_empty_domain(oracle_api, gpu_api, tolerance):
+    """No water at all: the solve has nothing to do (b = 0), every field stays
+    bit-exact, the volume is 0."""
+    cfg = scenes.base_config(64, 48)
+    cfg.projection.tolerance = tolerance
+    o, g = capi.Sim(oracle_api, cfg), capi.Sim(gpu_api, cfg)
+    for _ in range(4):
+        so, sg = o.step(scenes.DT), g.step(scenes.DT)
+        assert so.pressure_iterations == sg.pressure_iterations
+    assert not compare_fields(g, o)
+    assert g.fluid_volume() == o.fluid_volume() == 0
+
+
+@pytest.mark.parametrize("nx,ny", [(136, 88), (200, 40)])
+def test_ragged_grid_steps(oracle_api, gpu_api, nx, ny):
+    """Grids whose dispatches do not cover every face (sizes not multiples of
+    64): the reference's floor(n/64) coverage is replicated, bit-exact."""
+    cfg = scenes.base_config(nx, ny)
+    src = scenes.aabb_source((0.0, -0.2 * ny), (0.5 * nx, 0.3 * ny))
+    sc = scenes.Scene(f"ragged_{nx}x{ny}", cfg, oneshot=[src])
+    o, g = make_pair(sc, oracle_api, gpu_api)
+    for _ in range(8):
+        o.step(sc.dt)
+        g.step(sc.dt)
+    assert not compare_fields(g, o)
+
+
+def test_maximum_obstacles_and_sources(oracle_api, gpu_api):
+    """256 obstacles (EFL_MAX_SOLIDS) and 16 continuous sources, bit-exact,
+    force bins included."""
+    from bevy_eulerian_fluid_b200.plugin import Collider, RigidBody, RigidBodyKind, pack_obstacles
+    n = 128
+    cfg = scenes.base_config(n, n)
+    bodies = []
+    for i in range(capi.MAX_SOLIDS):
+        x, y = -56.0 + 7.0 * (i % 16), -50.0 + 6.5 * (i // 16)
+        bodies.append(RigidBody(Collider.circle(1.5 + 0.5 * (i % 3)), (x, y), 0.0, kind=RigidBodyKind.Static,
+                                density=scenes.RHO))
+    srcs = [scenes.circle_source((-60.0 + 8.0 * k, 40.0), 3.0, velocity=(0.0, -5.0)) for k in range(16)]
+    sc = scenes.Scene("crowded_128", cfg, continuous=srcs)
+    o, g = make_pair(sc, oracle_api, gpu_api)
+    obs = pack_obstacles(bodies)
+    o.set_obstacles(obs)
+    g.set_obstacles(obs)
+    for _ in range(6):
+        o.step(sc.dt)
+        g.step(sc.dt)
+    assert not compare_fields(g, o)
+    assert np.array_equal(g.force_bins(), o.force_bins())
