@@ -86,6 +86,18 @@ class RigidBodyC(C.Structure):  # efl_rigid_body
                 ("extent", C.c_double), ("dynamic", C.c_int32), ("obstacle", C.c_int32)]
 
 
+class Particle(C.Structure):  # efl_particle (particle.wgsl:5-11, storage stride 24)
+    _fields_ = [("position", C.c_float * 2), ("radius", C.c_float), ("sign", C.c_float), ("escaped", C.c_uint32),
+                ("_pad", C.c_uint32)]
+
+
+# numpy view of an efl_particle array
+PARTICLE_DTYPE = np.dtype([("position", "<f4", (2,)), ("radius", "<f4"), ("sign", "<f4"), ("escaped", "<u4"),
+                           ("_pad", "<u4")])
+PLS_POSITIVE, PLS_NEGATIVE = 0, 1
+PLS_INITIALIZE, PLS_ADVECT, PLS_CORRECT, PLS_CORRECT_SECOND, PLS_RESEED = 0, 1, 2, 3, 4
+
+
 class StepStats(C.Structure):
     _fields_ = [("initialized_only", C.c_int32), ("pressure_iterations", C.c_uint32), ("converged", C.c_int32),
                 ("_pad", C.c_int32), ("residual", C.c_double), ("residual_initial", C.c_double)]
@@ -100,6 +112,7 @@ assert C.sizeof(SolidObstacle) == 176
 assert C.sizeof(Force) == 16
 assert C.sizeof(Source) == 32
 assert C.sizeof(SolidForce) == 16
+assert C.sizeof(Particle) == 24 == PARTICLE_DTYPE.itemsize
 
 # Exported symbols of include/efl.h: name -> (restype, argtypes); "X" stands for the handle.
 SIGNATURES = {
@@ -129,6 +142,11 @@ SIGNATURES = {
     "residual": (C.c_int, ["X", C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "fluid_volume": (C.c_int, ["X", C.POINTER(C.c_uint64)]),
     "velocity_magnitude": (C.c_int, ["X", C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+    "set_particle_levelset": (C.c_int, ["X", C.c_int32]),
+    "particle_counts": (C.c_int, ["X", C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
+    "read_particles": (C.c_int, ["X", C.c_int32, C.c_void_p, C.c_uint32, C.POINTER(C.c_uint32)]),
+    "write_particles": (C.c_int, ["X", C.c_int32, C.c_void_p, C.c_uint32]),
+    "pls_run_phase": (C.c_int, ["X", C.c_int32, C.c_float]),
     "kernel_launches": (C.c_uint64, []),
     "pressure_sweeps": (C.c_int, ["X", C.c_int32, C.c_uint32]),
     "residual_norms_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
@@ -369,6 +387,34 @@ class Sim:
         a, b = C.c_float(), C.c_float()
         self._check(self.api.velocity_magnitude(self.h, C.byref(a), C.byref(b)))
         return a.value, b.value
+
+    # -- two-layer particle level set
+    def set_particle_levelset(self, enable: bool = True):
+        """ParticleLevelsetTwoLayersPlugin on this simulation (seeded by the next init sequence)."""
+        self._check(self.api.set_particle_levelset(self.h, 1 if enable else 0))
+
+    def particle_counts(self):
+        """((positive, negative) live counts, particles dropped for lack of capacity)."""
+        c = (C.c_uint32 * 2)()
+        d = C.c_uint32()
+        self._check(self.api.particle_counts(self.h, c, C.byref(d)))
+        return (c[0], c[1]), d.value
+
+    def read_particles(self, layer: int) -> np.ndarray:
+        """A layer's particles as a PARTICLE_DTYPE array."""
+        (n0, n1), _ = self.particle_counts()
+        n = (n0, n1)[layer]
+        out = np.zeros(n, dtype=PARTICLE_DTYPE)
+        got = C.c_uint32()
+        self._check(self.api.read_particles(self.h, layer, out.ctypes.data if n else None, n, C.byref(got)))
+        return out[:min(n, got.value)]
+
+    def write_particles(self, layer: int, parts: np.ndarray):
+        arr = np.ascontiguousarray(parts, dtype=PARTICLE_DTYPE)
+        self._check(self.api.write_particles(self.h, layer, arr.ctypes.data if len(arr) else None, len(arr)))
+
+    def pls_run_phase(self, phase: int, dt: float = 0.0):
+        self._check(self.api.pls_run_phase(self.h, phase, dt))
 
     def synchronize(self):
         self._check(self.api.synchronize(self.h))

@@ -25,6 +25,7 @@
 #include "efl_batch.cuh"
 #include "efl_mgpcg.cuh"
 #include "efl_unet.cuh"
+#include "efl_pls.cuh"
 
 using namespace efl;
 
@@ -79,6 +80,18 @@ struct GraphCache {
     }
 };
 
+// Two-layer particle level set state (particle_levelset_two_layers/plugin.rs,
+// PLSResources).  Allocated when first enabled.
+struct PlsState {
+    bool on = false;
+    bool ready = false;
+    PlsArgs a{};
+    uint32_t* part32 = nullptr;            // scan block totals, [2][nb]
+    unsigned long long* part64 = nullptr;  // scan block totals, [2][nb]
+    uint32_t nb = 0;                       // scan blocks per layer
+    uint32_t* h_read = nullptr;            // pinned: count[2], dropped
+};
+
 struct efl_sim {
     efl_config cfg{};
     int nx = 0, ny = 0, P = 0;
@@ -131,6 +144,7 @@ struct efl_sim {
     int* h_err = nullptr;  // pinned copy of the TMA sweep's error flag
     cudaEvent_t ev_proj[2] = {nullptr, nullptr};  // around the last projection stage
     bool proj_timed = false;
+    PlsState pls;
 
     Dom dom() const { return Dom{nx, ny}; }
 };
@@ -322,8 +336,120 @@ efl_status st_reinit(efl_sim* s) {  // reinitialize_levelset.rs:162-243
     return EFL_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Two-layer particle level set (particle_levelset_two_layers/**)
+
+efl_status pls_alloc(efl_sim* s) {
+    PlsState& P = s->pls;
+    PlsArgs& a = P.a;
+    a.nx = s->nx;
+    a.ny = s->ny;
+    a.L = (uint32_t)s->nx * (uint32_t)s->ny;
+    a.cap = a.L * PLS_MAX_PER_CELL;  // plugin.rs:212-215
+    for (int l = 0; l < 2; ++l) {
+        TRY(alloc_raw(s, a.px[l], a.cap));
+        TRY(alloc_raw(s, a.py[l], a.cap));
+        TRY(alloc_raw(s, a.rad[l], a.cap));
+        TRY(alloc_raw(s, a.esc[l], a.cap));
+        TRY(alloc_raw(s, a.qx[l], a.cap));
+        TRY(alloc_raw(s, a.qy[l], a.cap));
+        TRY(alloc_raw(s, a.qrad[l], a.cap));
+        TRY(alloc_raw(s, a.qesc[l], a.cap));
+    }
+    TRY(alloc_raw(s, a.count, 2));
+    TRY(alloc_raw(s, a.cnt, 2 * (size_t)a.L));
+    TRY(alloc_raw(s, a.cur, 2 * (size_t)a.L));
+    TRY(alloc_raw(s, a.off, 2 * (size_t)a.L));
+    TRY(alloc_raw(s, a.sidx, 2 * (size_t)a.cap));
+    TRY(alloc_raw(s, a.alive, 2 * (size_t)a.cap));
+    TRY(alloc_raw(s, a.val, 2 * (size_t)a.L));
+    TRY(alloc_raw(s, a.tot, 2));
+    TRY(alloc_raw(s, a.ctot, 2));
+    TRY(alloc_raw(s, a.addn, 2 * (size_t)a.L));
+    TRY(alloc_raw(s, a.phip, (size_t)a.L));
+    TRY(alloc_raw(s, a.phim, (size_t)a.L));
+    TRY(alloc_raw(s, a.dropped, 1));
+    P.nb = (a.L + SC_N - 1) / SC_N;
+    TRY(alloc_raw(s, P.part32, 2 * (size_t)P.nb));
+    TRY(alloc_raw(s, P.part64, 2 * (size_t)P.nb));
+    CU(cudaMallocHost(&P.h_read, 4 * sizeof(uint32_t)));
+    P.ready = true;
+    return EFL_OK;
+}
+
+// Grid-stride launches over the particles of both layers, and one thread per
+// cell (and layer).
+dim3 pls_pgrid(const PlsArgs& a) {
+    return dim3((unsigned)std::min<uint32_t>((a.cap + PLS_THREADS - 1) / PLS_THREADS, 148u * 8u), 2);
+}
+dim3 pls_cgrid(const PlsArgs& a, int layers) { return dim3((a.L + PLS_THREADS - 1) / PLS_THREADS, layers); }
+
+// Exclusive scan of each layer's L values (common_pass/prefix_sum.rs).
+template <class Tin, class T>
+efl_status pls_scan(efl_sim* s, const Tin* in, T* out, T* part, T* tot) {
+    const PlsArgs& a = s->pls.a;
+    const uint32_t nb = s->pls.nb;
+    k_scan_local<Tin, T><<<dim3(nb, 2), SC_T, count_launch(), s->stream>>>(in, out, part, a.L, a.L, nb);
+    k_scan_parts<T><<<dim3(1, 2), SC_T, count_launch(), s->stream>>>(part, tot, nb);
+    k_scan_add<T><<<pls_cgrid(a, 2), PLS_THREADS, count_launch(), s->stream>>>(out, part, a.L, a.L, nb);
+    LAUNCH_CHECK();
+    return EFL_OK;
+}
+
+// plugin.rs:131-158 (dispatch_initialize): band mask and seeding from
+// levelset_air0 and its gradient.
+efl_status pls_initialize(efl_sim* s) {
+    PlsArgs& a = s->pls.a;
+    k_pls_seed_count<<<pls_cgrid(a, 2), PLS_THREADS, count_launch(), s->stream>>>(a, s->ls0, s->grad);
+    TRY(pls_scan(s, a.val, a.val, s->pls.part64, a.tot));
+    k_pls_emit<<<pls_cgrid(a, 2), PLS_THREADS, count_launch(), s->stream>>>(a, s->ls0, s->grad, 1);
+    k_pls_set_count<<<1, 32, count_launch(), s->stream>>>(a, 1);
+    LAUNCH_CHECK();
+    return EFL_OK;
+}
+
+// plugin.rs:160-182 (dispatch_update)
+efl_status pls_advect(efl_sim* s, float dt) {
+    PlsArgs& a = s->pls.a;
+    k_pls_advect<<<pls_pgrid(a), PLS_THREADS, count_launch(), s->stream>>>(a, s->u0, s->v0, dt);
+    LAUNCH_CHECK();
+    return EFL_OK;
+}
+
+// levelset_correction.rs:96-155 (dispatch, on levelset_air1) and :157-236
+// (dispatch_second, on levelset_air0, then the particle radii).
+efl_status pls_correct(efl_sim* s, PF ls, bool second) {
+    PlsArgs& a = s->pls.a;
+    k_pls_reset<<<pls_cgrid(a, 1), PLS_THREADS, count_launch(), s->stream>>>(a, ls);
+    k_pls_mark_accumulate<<<pls_pgrid(a), PLS_THREADS, count_launch(), s->stream>>>(a, ls);
+    k_pls_correct<<<pls_cgrid(a, 1), PLS_THREADS, count_launch(), s->stream>>>(a, ls);
+    if (second) k_pls_radii<<<pls_pgrid(a), PLS_THREADS, count_launch(), s->stream>>>(a, ls);
+    LAUNCH_CHECK();
+    return EFL_OK;
+}
+
+// reseed.rs:130-296: bin, counting sort, per-cell heap, compaction, refill.
+efl_status pls_reseed(efl_sim* s) {
+    PlsArgs& a = s->pls.a;
+    CU(cudaMemsetAsync(a.cnt, 0, 2 * (size_t)a.L * sizeof(uint32_t), s->stream));
+    CU(cudaMemsetAsync(a.cur, 0, 2 * (size_t)a.L * sizeof(uint32_t), s->stream));
+    k_pls_bin<<<pls_pgrid(a), PLS_THREADS, count_launch(), s->stream>>>(a);
+    LAUNCH_CHECK();
+    TRY(pls_scan(s, a.cnt, a.off, s->pls.part32, a.ctot));
+    k_pls_scatter<<<pls_pgrid(a), PLS_THREADS, count_launch(), s->stream>>>(a);
+    k_pls_reseed<<<pls_cgrid(a, 2), PLS_THREADS, count_launch(), s->stream>>>(a, s->ls0, s->grad);
+    LAUNCH_CHECK();
+    TRY(pls_scan(s, a.val, a.val, s->pls.part64, a.tot));
+    k_pls_emit<<<pls_cgrid(a, 2), PLS_THREADS, count_launch(), s->stream>>>(a, s->ls0, s->grad, 0);
+    k_pls_set_count<<<1, 32, count_launch(), s->stream>>>(a, 0);
+    k_pls_copyback<<<pls_pgrid(a), PLS_THREADS, count_launch(), s->stream>>>(a);
+    LAUNCH_CHECK();
+    return EFL_OK;
+}
+
 efl_status run_init(efl_sim* s) {
     TRY(st_init(s));
+    if (s->pls.on) TRY(pls_initialize(s));  // render_node.rs:250-258
     TRY(st_fluid_source(s, s->src_once));
     TRY(st_reinit(s));
     return EFL_OK;
@@ -912,8 +1038,20 @@ efl_status run_stage(efl_sim* s, int stage, efl_step_stats* st) {
         case EFL_STAGE_SOLVE_VELOCITY: return st_solve_velocity(s);
         case EFL_STAGE_EXTRAPOLATE: return st_extrapolate(s);
         case EFL_STAGE_ADVECT_LEVELSET: return st_advect_levelset(s);
-        case EFL_STAGE_FLUID_SOURCE: return st_fluid_source(s, s->src_cont);
-        case EFL_STAGE_REINITIALIZE: return st_reinit(s);
+        case EFL_STAGE_FLUID_SOURCE:  // + render_node.rs:389-419 (particles advected, first correction)
+            TRY(st_fluid_source(s, s->src_cont));
+            if (s->pls.on) {
+                TRY(pls_advect(s, s->U.dt));
+                TRY(pls_correct(s, s->ls1, false));
+            }
+            return EFL_OK;
+        case EFL_STAGE_REINITIALIZE:  // + render_node.rs:421-441 (second correction, reseed)
+            TRY(st_reinit(s));
+            if (s->pls.on) {
+                TRY(pls_correct(s, s->ls0, true));
+                TRY(pls_reseed(s));
+            }
+            return EFL_OK;
         case EFL_STAGE_LEVELSET_GRADIENT: return st_gradient(s);
         case EFL_STAGE_SOLID_FORCES: TRY(st_solid_forces(s)); return st_rigid(s);
         default: return set_err(s, EFL_ERR_INVALID_ARGUMENT, "unknown stage %d", stage);
@@ -1110,6 +1248,7 @@ efl_status efl_destroy(efl_sim* s) {
     if (s->h_norms) cudaFreeHost(s->h_norms);
     if (s->cg.h_read) cudaFreeHost(s->cg.h_read);
     if (s->d_vel) cudaFree(s->d_vel);
+    if (s->pls.h_read) cudaFreeHost(s->pls.h_read);
     for (cudaEvent_t e : s->ev_proj)
         if (e) cudaEventDestroy(e);
     s->gc.clear();
@@ -1462,6 +1601,107 @@ efl_status efl_velocity_magnitude(efl_sim* s, float* min_mag, float* max_mag) {
     if (min_mag) *min_mag = r[0];
     if (max_mag) *max_mag = r[1];
     return EFL_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Two-layer particle level set (ParticleLevelsetTwoLayersPlugin, plugin.rs)
+
+efl_status efl_set_particle_levelset(efl_sim* s, int32_t enable) {
+    if (!s) return set_err(nullptr, EFL_ERR_INVALID_ARGUMENT, "null sim");
+    cudaSetDevice(s->device);
+    if (enable && !s->pls.ready) TRY(pls_alloc(s));
+    s->pls.on = enable != 0;
+    ++s->graph_epoch;
+    return EFL_OK;
+}
+
+efl_status efl_particle_counts(efl_sim* s, uint32_t counts[2], uint32_t* dropped) {
+    if (!s || !counts) return set_err(s, EFL_ERR_INVALID_ARGUMENT, "null argument");
+    counts[0] = counts[1] = 0;
+    if (dropped) *dropped = 0;
+    if (!s->pls.ready) return EFL_OK;
+    cudaSetDevice(s->device);
+    uint32_t* h = s->pls.h_read;
+    CU(cudaMemcpyAsync(h, s->pls.a.count, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
+    CU(cudaMemcpyAsync(h + 2, s->pls.a.dropped, sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
+    CU(cudaStreamSynchronize(s->stream));
+    counts[0] = h[0];
+    counts[1] = h[1];
+    if (dropped) *dropped = h[2];
+    return EFL_OK;
+}
+
+efl_status efl_read_particles(efl_sim* s, int32_t layer, efl_particle* dst, uint32_t capacity, uint32_t* n) {
+    if (!s || !n || (capacity && !dst)) return set_err(s, EFL_ERR_INVALID_ARGUMENT, "null argument");
+    if (layer != EFL_PLS_POSITIVE && layer != EFL_PLS_NEGATIVE)
+        return set_err(s, EFL_ERR_INVALID_ARGUMENT, "unknown particle layer %d", layer);
+    uint32_t counts[2];
+    TRY(efl_particle_counts(s, counts, nullptr));
+    *n = counts[layer];
+    const uint32_t m = std::min(counts[layer], capacity);
+    if (!m) return EFL_OK;
+    const PlsArgs& a = s->pls.a;
+    std::vector<float> x(m), y(m), r(m);
+    std::vector<uint8_t> e(m);
+    CU(cudaMemcpyAsync(x.data(), a.px[layer], m * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
+    CU(cudaMemcpyAsync(y.data(), a.py[layer], m * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
+    CU(cudaMemcpyAsync(r.data(), a.rad[layer], m * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
+    CU(cudaMemcpyAsync(e.data(), a.esc[layer], m, cudaMemcpyDeviceToHost, s->stream));
+    CU(cudaStreamSynchronize(s->stream));
+    const float sgn = layer == EFL_PLS_POSITIVE ? 1.0f : -1.0f;
+    for (uint32_t i = 0; i < m; ++i) {
+        dst[i].position[0] = x[i];
+        dst[i].position[1] = y[i];
+        dst[i].radius = r[i];
+        dst[i].sign = sgn;
+        dst[i].escaped = e[i];
+        dst[i]._pad = 0;
+    }
+    return EFL_OK;
+}
+
+efl_status efl_write_particles(efl_sim* s, int32_t layer, const efl_particle* src, uint32_t n) {
+    if (!s || (n && !src)) return set_err(s, EFL_ERR_INVALID_ARGUMENT, "null argument");
+    if (layer != EFL_PLS_POSITIVE && layer != EFL_PLS_NEGATIVE)
+        return set_err(s, EFL_ERR_INVALID_ARGUMENT, "unknown particle layer %d", layer);
+    if (!s->pls.ready) return set_err(s, EFL_ERR_STATE, "the particle level set is not enabled");
+    const PlsArgs& a = s->pls.a;
+    if (n > a.cap) return set_err(s, EFL_ERR_TOO_MANY, "%u particles exceed the capacity %u", n, a.cap);
+    const float sgn = layer == EFL_PLS_POSITIVE ? 1.0f : -1.0f;
+    std::vector<float> x(n), y(n), r(n);
+    std::vector<uint8_t> e(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        if (src[i].sign != sgn)
+            return set_err(s, EFL_ERR_INVALID_ARGUMENT, "particle %u has sign %g in layer %d", i, src[i].sign, layer);
+        x[i] = src[i].position[0];
+        y[i] = src[i].position[1];
+        r[i] = src[i].radius;
+        e[i] = src[i].escaped ? 1 : 0;
+    }
+    cudaSetDevice(s->device);
+    if (n) {
+        CU(cudaMemcpyAsync(a.px[layer], x.data(), n * sizeof(float), cudaMemcpyHostToDevice, s->stream));
+        CU(cudaMemcpyAsync(a.py[layer], y.data(), n * sizeof(float), cudaMemcpyHostToDevice, s->stream));
+        CU(cudaMemcpyAsync(a.rad[layer], r.data(), n * sizeof(float), cudaMemcpyHostToDevice, s->stream));
+        CU(cudaMemcpyAsync(a.esc[layer], e.data(), n, cudaMemcpyHostToDevice, s->stream));
+    }
+    CU(cudaMemcpyAsync(a.count + layer, &n, sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
+    CU(cudaStreamSynchronize(s->stream));
+    return EFL_OK;
+}
+
+efl_status efl_pls_run_phase(efl_sim* s, int32_t phase, float dt) {
+    if (!s) return set_err(nullptr, EFL_ERR_INVALID_ARGUMENT, "null sim");
+    if (!s->pls.ready) return set_err(s, EFL_ERR_STATE, "the particle level set is not enabled");
+    cudaSetDevice(s->device);
+    switch (phase) {
+        case EFL_PLS_INITIALIZE: return pls_initialize(s);
+        case EFL_PLS_ADVECT: return pls_advect(s, dt);
+        case EFL_PLS_CORRECT: return pls_correct(s, s->ls1, false);
+        case EFL_PLS_CORRECT_SECOND: return pls_correct(s, s->ls0, true);
+        case EFL_PLS_RESEED: return pls_reseed(s);
+        default: return set_err(s, EFL_ERR_INVALID_ARGUMENT, "unknown particle level set phase %d", phase);
+    }
 }
 
 uint64_t efl_kernel_launches(void) { return efl::launches_total(); }

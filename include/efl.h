@@ -365,6 +365,55 @@ EFL_API efl_status efl_set_rigid_bodies(efl_sim* sim, const efl_rigid_body* bodi
                                         double grid_length, uint32_t substeps);
 EFL_API efl_status efl_get_rigid_bodies(efl_sim* sim, efl_rigid_body* bodies, uint32_t n);
 
+/* ---- Two-layer particle level set -------------------------------------- */
+
+/* ParticleLevelsetTwoLayersPlugin (particle_levelset_two_layers/plugin.rs,
+ * Enright et al. 2002; commented out of the reference's FluidPlugin at
+ * euler_fluid.rs:81).  Positive particles (sign +1, layer 0) and negative
+ * particles (sign -1, layer 1) seeded in the band |phi| < 3 around the
+ * interface, at most 16 per cell and layer; capacity nx*ny*16 per layer
+ * (plugin.rs:212-215).  When enabled, every efl_step / init sequence runs:
+ *   init  : seed from levelset_air and its gradient (render_node.rs:250-258);
+ *   step  : after the fluid sources, advect the particles (TVD RK3) and
+ *           correct levelset_air1 with the escaped ones; after the
+ *           reinitialisation, correct levelset_air0 again, update the radii,
+ *           then reseed: delete far-off particles, keep at most 16 per band
+ *           cell ranked by the per-cell heap, refill to 16
+ *           (render_node.rs:389-441).
+ * The particle order is fixed (cell order, then attempt order; a stable
+ * counting sort by cell), one of the orders the reference's atomic appends
+ * can produce, so results are reproducible run to run. */
+typedef struct efl_particle {   /* particle.wgsl:5-11 (storage stride 24) */
+    float position[2];          /* grid cells, cell (i, j) centre at (i, j) */
+    float radius;
+    float sign;                 /* +1 layer 0, -1 layer 1 */
+    uint32_t escaped;           /* set by the last level-set correction */
+    uint32_t _pad;
+} efl_particle;
+enum { EFL_PLS_POSITIVE = 0, EFL_PLS_NEGATIVE = 1 };
+typedef enum efl_pls_phase {
+    EFL_PLS_INITIALIZE = 0,     /* plugin.rs:131-158 (band mask + seeding)      */
+    EFL_PLS_ADVECT = 1,         /* plugin.rs:160-182 (advect_particles.wgsl)     */
+    EFL_PLS_CORRECT = 2,        /* levelset_correction.rs:96-155, levelset_air1  */
+    EFL_PLS_CORRECT_SECOND = 3, /* levelset_correction.rs:157-236, levelset_air0 */
+    EFL_PLS_RESEED = 4          /* reseed.rs:130-296                             */
+} efl_pls_phase;
+/* enable != 0 allocates the particle buffers (first time) and runs the
+ * plugin in every following efl_step; 0 stops it (particles are kept).
+ * Enabling an initialised simulation starts from no particles: the next
+ * reseed fills the band. */
+EFL_API efl_status efl_set_particle_levelset(efl_sim* sim, int32_t enable);
+/* Live particles per layer; dropped = particles that did not fit the
+ * capacity since creation (0 unless the capacity was exceeded). */
+EFL_API efl_status efl_particle_counts(efl_sim* sim, uint32_t counts[2], uint32_t* dropped);
+/* Copies min(count, capacity) particles of a layer; *n = the live count. */
+EFL_API efl_status efl_read_particles(efl_sim* sim, int32_t layer, efl_particle* dst, uint32_t capacity,
+                                      uint32_t* n);
+/* Replaces a layer's particles (sign must match the layer; n <= nx*ny*16). */
+EFL_API efl_status efl_write_particles(efl_sim* sim, int32_t layer, const efl_particle* src, uint32_t n);
+/* Runs one phase on the current state (testing); dt is used by EFL_PLS_ADVECT. */
+EFL_API efl_status efl_pls_run_phase(efl_sim* sim, int32_t phase, float dt);
+
 /* ---- Batches of independent simulations ------------------------------ */
 
 /* N independent simulations of possibly different sizes stepped together

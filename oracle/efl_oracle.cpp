@@ -135,6 +135,12 @@ struct LevelT {
 using Level = LevelT<float>;
 using Level64 = LevelT<double>;
 
+// particle.wgsl:5-11
+struct OParticle {
+    float x, y, radius, sign;
+    uint32_t escaped;
+};
+
 }  // namespace
 
 struct eflo_sim {
@@ -160,6 +166,12 @@ struct eflo_sim {
     std::vector<efl_source> src_once, src_cont;
     int32_t bins[3][EFL_MAX_SOLIDS];
     efl_solid_force out_forces[EFL_MAX_SOLIDS];
+
+    // two-layer particle level set (particle_levelset_two_layers/plugin.rs)
+    bool pls_on = false;
+    std::vector<OParticle> parts[2];      // [0] positive, [1] negative
+    std::vector<int32_t> phi_plus, phi_minus;
+    uint32_t pls_dropped = 0;
 
     // dispatch domains (pipeline.rs:175-186)
     int cx() const { return (nx / 8) * 8; }
@@ -1537,10 +1549,342 @@ void k_solid_forces(eflo_sim& s) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// Two-layer particle level set (particle_levelset_two_layers/**).
+//
+// The reference appends with atomicAdd and sorts into cells with an atomic
+// cursor; here every append runs in cell order (x fastest) and attempt order,
+// and the sort is a stable counting sort, the order the CUDA library fixes.
+
+constexpr uint32_t PLS_PER_CELL = 16;  // constants.wgsl:3
+constexpr float PLS_BAND = 3.0f;       // constants.wgsl:5
+constexpr float PLS_SCALE = 10000.0f;  // fixed_point.wgsl:3
+
+inline uint32_t f2u(float v) {  // WGSL u32(f32): truncate, saturate, NaN -> 0
+    if (!(v > 0.0f)) return 0u;
+    if (v >= 4294967296.0f) return 0xffffffffu;
+    return (uint32_t)v;
+}
+inline int32_t pls_fixed(float v) { return f2i(v * PLS_SCALE); }           // fixed_point.wgsl:8-10
+inline float pls_float(int32_t v) { return (float)v / PLS_SCALE; }          // fixed_point.wgsl:4-6
+
+// utils/coordinate.wgsl:19-33
+inline float interp_center(const Tex<float>& t, float x, float y) {
+    int i = f2i(std::floor(x));
+    int j = f2i(std::floor(y));
+    float fi = x - (float)i;
+    float fj = y - (float)j;
+    float l00 = t.ld(i, j), l10 = t.ld(i + 1, j), l01 = t.ld(i, j + 1), l11 = t.ld(i + 1, j + 1);
+    return wmix(wmix(l00, l10, fi), wmix(l01, l11, fi), fj);
+}
+// utils/coordinate.wgsl:35-49
+inline F2 interp_center_rg(const Tex<F2>& t, float x, float y) {
+    int i = f2i(std::floor(x));
+    int j = f2i(std::floor(y));
+    float fi = x - (float)i;
+    float fj = y - (float)j;
+    F2 l00 = t.ld(i, j), l10 = t.ld(i + 1, j), l01 = t.ld(i, j + 1), l11 = t.ld(i + 1, j + 1);
+    return F2{wmix(wmix(l00.x, l10.x, fi), wmix(l01.x, l11.x, fi), fj),
+              wmix(wmix(l00.y, l10.y, fi), wmix(l01.y, l11.y, fi), fj)};
+}
+
+// utils/hash.wgsl:3-74 (both rotations by 15 bits, as written there)
+inline uint32_t rotl32(uint32_t x) { return (x << 15u) | (x >> 17u); }
+inline uint32_t murmur3_block(uint32_t src, uint32_t seed) {
+    uint32_t k = src, h = seed;
+    k *= 0xcc9e2d51u;
+    k = rotl32(k);
+    k *= 0x1b873593u;
+    h ^= k;
+    h = rotl32(h);
+    h = h * 5u + 0xe6546b64u;
+    h ^= 4u;
+    h ^= h >> 16;
+    h *= 0x85ebca6bu;
+    h ^= h >> 13;
+    h *= 0xc2b2ae35u;
+    h ^= h >> 16;
+    return h;
+}
+inline float bits_to_unit(uint32_t h) {
+    uint32_t b = (h & 0x007fffffu) | 0x3f800000u;
+    float f;
+    std::memcpy(&f, &b, 4);
+    return f - 1.0f;
+}
+inline uint32_t fbits(float v) {
+    uint32_t b;
+    std::memcpy(&b, &v, 4);
+    return b;
+}
+inline F2 hash22(F2 v) {
+    return F2{bits_to_unit(murmur3_block(fbits(v.x), 12345u)), bits_to_unit(murmur3_block(fbits(v.y), 98765u))};
+}
+inline float hash11(float v) { return bits_to_unit(murmur3_block(fbits(v), 11111u)); }
+
+// particle.wgsl:50-54
+inline float particle_radius(float phi) { return fclamp(std::fabs(phi), 0.1f, 0.5f); }
+
+// particle.wgsl:19-30
+inline bool is_escaped(const OParticle& p, const Tex<float>& ls) {
+    float phi = interp_center(ls, p.x, p.y);
+    return p.sign * phi + p.radius < 0.0f;
+}
+
+// particle.wgsl:36-82; normalize(g) = g / length(g)
+bool spawn_and_attract(const eflo_sim& s, F2 x, float phi_goal, float bmin, float bmax, float sign, OParticle* out) {
+    const Tex<float>& ls = s.ls0;
+    float lambda = 1.0f;
+    float phi = interp_center(ls, x.x, x.y);
+    F2 g = interp_center_rg(s.grad, x.x, x.y);
+    float len = wlength(g.x, g.y);
+    F2 gn{g.x / len, g.y / len};
+    float step = lambda * (phi_goal - phi);
+    F2 xn{x.x + step * gn.x, x.y + step * gn.y};
+    float fx = (float)s.nx, fy = (float)s.ny;
+    if (!(0.0f < xn.x && 0.0f < xn.y && xn.x < fx - 1.0f && xn.y < fy - 1.0f)) return false;
+    float phi_new = interp_center(ls, xn.x, xn.y);
+    if (!(bmin <= phi_new && phi_new <= bmax)) return false;
+    *out = OParticle{xn.x, xn.y, particle_radius(phi_new), sign, 0u};
+    return true;
+}
+
+void pls_append(eflo_sim& s, int layer, const OParticle& p) {
+    if (s.parts[layer].size() >= (size_t)s.nx * s.ny * PLS_PER_CELL) {
+        ++s.pls_dropped;
+        return;
+    }
+    s.parts[layer].push_back(p);
+}
+
+// update_interface_band_mask.wgsl:7-17 + initialize_particles.wgsl:17-58
+void pls_initialize(eflo_sim& s) {
+    const float bmin = 0.1f, bmax = PLS_BAND;
+    const float bmin_neg = -bmax, bmax_neg = -bmin;
+    for (int y = 0; y < s.cy(); ++y)
+        for (int x = 0; x < s.cx(); ++x) {
+            if (!(std::fabs(s.ls0.ld(x, y)) < PLS_BAND)) continue;
+            const F2 xb{(float)x, (float)y};
+            const uint32_t cell_id = (uint32_t)x + (uint32_t)s.nx * (uint32_t)y;
+            for (uint32_t i = 0; i < PLS_PER_CELL; ++i) {
+                uint32_t seed = cell_id + i;
+                F2 h = hash22(F2{xb.x + (float)seed, xb.y + (float)seed});
+                F2 xp{xb.x + h.x, xb.y + h.y};
+                float goal = hash11((float)seed) * (bmax - bmin) + bmin;
+                OParticle p;
+                if (spawn_and_attract(s, xp, goal, bmin, bmax, 1.0f, &p)) pls_append(s, 0, p);
+                uint32_t seed_neg = cell_id + i + 1000u;
+                float goal_neg = hash11((float)seed_neg) * (bmax_neg - bmin_neg) + bmin_neg;
+                // initialize_particles.wgsl:50 spawns from x, not x_neg
+                if (spawn_and_attract(s, xp, goal_neg, bmin_neg, bmax_neg, -1.0f, &p)) pls_append(s, 1, p);
+            }
+        }
+}
+
+// advect_particles.wgsl:15-33, utils/coordinate.wgsl:96-109
+void pls_advect(eflo_sim& s) {
+    const float dt = s.U.dt;
+    for (auto& layer : s.parts) {
+        const int64_t n = (int64_t)layer.size();
+#pragma omp parallel for schedule(static) if (g_threads != 1)
+        for (int64_t i = 0; i < n; ++i) {
+            OParticle& p = layer[i];
+            float x = p.x, y = p.y;
+            float u0x = interp_edge_x(s.u0, x, y), u0y = interp_edge_y(s.v0, x, y);
+            float x1 = x + dt * u0x, y1 = y + dt * u0y;
+            float u1x = interp_edge_x(s.u0, x1, y1), u1y = interp_edge_y(s.v0, x1, y1);
+            float x2 = 0.75f * x + 0.25f * (x1 + dt * u1x);
+            float y2 = 0.75f * y + 0.25f * (y1 + dt * u1y);
+            float u2x = interp_edge_x(s.u0, x2, y2), u2y = interp_edge_y(s.v0, x2, y2);
+            p.x = (float)(1.0 / 3.0) * x + (float)(2.0 / 3.0) * (x2 + dt * u2x);
+            p.y = (float)(1.0 / 3.0) * y + (float)(2.0 / 3.0) * (y2 + dt * u2y);
+        }
+    }
+}
+
+// levelset_correction.rs:96-155 / :157-236 in dispatch order:
+// mark_escaped_particles, reset_levelset_correction,
+// accumulate_levelset_correction (+, then -), correct_levelset
+// [, update_particle_radii for both layers].
+void pls_correct(eflo_sim& s, Tex<float>& ls, bool second) {
+    for (auto& layer : s.parts)
+        for (auto& p : layer) p.escaped = is_escaped(p, ls) ? 1u : 0u;
+    const uint32_t nx = (uint32_t)s.nx, ny = (uint32_t)s.ny;
+    s.phi_plus.assign((size_t)nx * ny, 0);
+    s.phi_minus.assign((size_t)nx * ny, 0);
+    for (int y = 0; y < s.cy(); ++y)
+        for (int x = 0; x < s.cx(); ++x) {
+            int32_t q = pls_fixed(ls.ld(x, y));
+            s.phi_plus[(size_t)y * nx + x] = q;
+            s.phi_minus[(size_t)y * nx + x] = q;
+        }
+    for (int layer = 0; layer < 2; ++layer) {
+        std::vector<int32_t>& phi = layer == 0 ? s.phi_plus : s.phi_minus;
+        for (const OParticle& p : s.parts[layer]) {
+            if (p.escaped != 1u) continue;
+            const uint32_t bx = f2u(p.x), by = f2u(p.y);
+            for (uint32_t i = 0; i < 2; ++i)
+                for (uint32_t j = 0; j < 2; ++j) {
+                    const uint32_t cx = bx + i, cy = by + j;
+                    if (nx <= cx || ny <= cy) continue;
+                    const float dx = p.x - (float)cx, dy = p.y - (float)cy;
+                    const float phi_p = p.sign * (p.radius - wlength(dx, dy));
+                    int32_t& dst = phi[(size_t)cx + nx * cy];
+                    const int32_t q = pls_fixed(phi_p);
+                    dst = p.sign > 0.0f ? std::max(dst, q) : std::min(dst, q);
+                }
+        }
+    }
+    for (int y = 0; y < s.cy(); ++y)
+        for (int x = 0; x < s.cx(); ++x) {
+            float pp = pls_float(s.phi_plus[(size_t)y * nx + x]);
+            float pm = pls_float(s.phi_minus[(size_t)y * nx + x]);
+            ls.st(x, y, std::fabs(pp) <= std::fabs(pm) ? pp : pm);
+        }
+    if (!second) return;
+    for (auto& layer : s.parts)
+        for (auto& p : layer) p.radius = particle_radius(ls.ld(f2i(p.x), f2i(p.y)));
+}
+
+// reseed_particles.wgsl:97-148: the heap with WGSL's bounds-checked local
+// array (an index past the end reads and writes element 15) and its
+// zero-initialised contents.
+struct HeapNode {
+    uint32_t index;
+    float value;
+};
+struct CellHeap {
+    HeapNode h[PLS_PER_CELL] = {};
+    HeapNode& at(uint32_t i) { return h[std::min(i, PLS_PER_CELL - 1)]; }
+    void correct(uint32_t capacity, uint32_t start) {  // correct_heap
+        uint32_t i = start;
+        for (;;) {
+            uint32_t l = 2 * i + 1, r = 2 * i + 2, largest = i;
+            if (l < capacity && at(l).value > at(largest).value) largest = l;
+            if (r < capacity && at(r).value > at(largest).value) largest = r;
+            if (largest == i) return;
+            std::swap(at(largest), at(i));
+            i = largest;
+        }
+    }
+    void sift_up(uint32_t capacity) {
+        uint32_t i = capacity - 1;
+        for (;;) {
+            uint32_t p = (i - 1) / 2;
+            if (at(p).value > at(i).value) return;
+            std::swap(at(p), at(i));
+            i = p;
+            if (i == 0) return;
+        }
+    }
+};
+
+// reseed.rs:130-296 for one layer: count_particles_in_cell, prefix sum,
+// sort_particles, reseed_particles, prefix sum of the alive mask,
+// delete_particles, update_particles_count, add_particles.
+void pls_reseed_layer(eflo_sim& s, int layer) {
+    const float sign = layer == 0 ? 1.0f : -1.0f;
+    const uint32_t nx = (uint32_t)s.nx, L = (uint32_t)s.nx * (uint32_t)s.ny;
+    std::vector<OParticle>& parts = s.parts[layer];
+    const uint32_t count = (uint32_t)parts.size();
+    auto cell_of = [&](const OParticle& p) {
+        uint32_t c = f2u(p.x) + nx * f2u(p.y);
+        return std::min(c, L - 1);  // bounds-checked storage index
+    };
+    std::vector<uint32_t> num(L, 0), offsets(L, 0), cursor(L, 0);
+    for (const OParticle& p : parts) ++num[cell_of(p)];
+    for (uint32_t c = 1; c < L; ++c) offsets[c] = offsets[c - 1] + num[c - 1];
+    std::vector<OParticle> sorted(count);
+    for (const OParticle& p : parts) {
+        uint32_t c = cell_of(p);
+        sorted[offsets[c] + cursor[c]++] = p;
+    }
+    std::vector<uint32_t> alive(count, 0), to_add(L, 0);
+    for (uint32_t cy = 0; cy < (uint32_t)s.cy(); ++cy)
+        for (uint32_t cx = 0; cx < (uint32_t)s.cx(); ++cx) {
+            const uint32_t c = cx + nx * cy;
+            const uint32_t n = num[c], base = offsets[c];
+            const bool near = std::fabs(interp_center(s.ls0, (float)cx, (float)cy)) < PLS_BAND;
+            CellHeap heap;
+            uint32_t capacity = PLS_PER_CELL, idx = 0;
+            auto mark_dead = [&](uint32_t slot) {
+                // slot 0 of another cell's bucket (a zero node): the racy
+                // write is ordered before that cell's own writes
+                if (slot >= base && slot < base + n) alive[slot] = 0;
+            };
+            for (uint32_t i = 0; i < n; ++i) {
+                const uint32_t slot = base + i;
+                const OParticle& p = sorted[slot];
+                if (!near) {
+                    alive[slot] = 0;
+                    continue;
+                }
+                if (is_escaped(p, s.ls0)) {
+                    if (capacity != 0) {
+                        alive[slot] = 1;
+                        capacity -= 1;
+                        if (idx > capacity) {
+                            mark_dead(heap.at(0).index);
+                            heap.at(0) = heap.at(idx - 1);
+                            idx -= 1;
+                            heap.correct(capacity, 0);
+                        }
+                    } else {
+                        alive[slot] = 0;
+                    }
+                    continue;
+                }
+                const float prio = p.sign * interp_center(s.ls0, p.x, p.y) - p.radius;
+                if (idx < capacity) {
+                    alive[slot] = 1;
+                    heap.at(idx) = HeapNode{slot, prio};
+                    idx += 1;
+                    heap.sift_up(idx);
+                } else if (prio < heap.at(0).value) {
+                    alive[slot] = 1;
+                    mark_dead(heap.at(0).index);
+                    heap.at(0) = HeapNode{slot, prio};
+                    heap.correct(capacity, 0);
+                } else {
+                    alive[slot] = 0;
+                }
+            }
+            to_add[c] = near ? capacity - idx : 0u;
+        }
+    std::vector<uint32_t> scan(count, 0);
+    for (uint32_t i = 1; i < count; ++i) scan[i] = scan[i - 1] + alive[i - 1];
+    const uint32_t kept = count ? scan[count - 1] + alive[count - 1] : 0u;
+    parts.assign(kept, OParticle{});
+    for (uint32_t i = 0; i < count; ++i)
+        if (alive[i]) parts[scan[i]] = sorted[i];
+    // add_particles.wgsl:12-46
+    const float bmin = sign > 0.0f ? 0.1f : -PLS_BAND;
+    const float bmax = sign > 0.0f ? PLS_BAND : -0.1f;
+    for (uint32_t cy = 0; cy < (uint32_t)s.cy(); ++cy)
+        for (uint32_t cx = 0; cx < (uint32_t)s.cx(); ++cx) {
+            const uint32_t c = cx + nx * cy;
+            const F2 xb{(float)cx, (float)cy};
+            for (uint32_t i = 0; i < to_add[c]; ++i) {
+                const uint32_t seed = c + i;
+                F2 h = hash22(F2{xb.x + (float)seed, xb.y + (float)seed});
+                F2 x{xb.x + h.x, xb.y + h.y};
+                float goal = hash11((float)seed) * (bmax - bmin) + bmin;
+                OParticle p;
+                if (spawn_and_attract(s, x, goal, bmin, bmax, sign, &p)) pls_append(s, layer, p);
+            }
+        }
+}
+
+void pls_reseed(eflo_sim& s) {
+    pls_reseed_layer(s, 0);
+    pls_reseed_layer(s, 1);
+}
+
 // render_node.rs:219-277
 void run_init(eflo_sim& s) {
     k_init_center(s);
     k_init_edge(s);
+    if (s.pls_on) pls_initialize(s);  // render_node.rs:250-258
     k_fluid_source(s, s.src_once);
     k_reinit(s);
 }
@@ -1557,8 +1901,20 @@ efl_status run_stage(eflo_sim& s, int stage, efl_step_stats* st) {
         case EFL_STAGE_SOLVE_VELOCITY: k_solve_velocity(s); return EFL_OK;
         case EFL_STAGE_EXTRAPOLATE: k_extrapolate(s); return EFL_OK;
         case EFL_STAGE_ADVECT_LEVELSET: k_advect_levelset(s); return EFL_OK;
-        case EFL_STAGE_FLUID_SOURCE: k_fluid_source(s, s.src_cont); return EFL_OK;
-        case EFL_STAGE_REINITIALIZE: k_reinit(s); return EFL_OK;
+        case EFL_STAGE_FLUID_SOURCE:  // + render_node.rs:389-419
+            k_fluid_source(s, s.src_cont);
+            if (s.pls_on) {
+                pls_advect(s);
+                pls_correct(s, s.ls1, false);
+            }
+            return EFL_OK;
+        case EFL_STAGE_REINITIALIZE:  // + render_node.rs:421-441
+            k_reinit(s);
+            if (s.pls_on) {
+                pls_correct(s, s.ls0, true);
+                pls_reseed(s);
+            }
+            return EFL_OK;
         case EFL_STAGE_LEVELSET_GRADIENT: k_gradient(s); return EFL_OK;
         case EFL_STAGE_SOLID_FORCES: k_solid_forces(s); return EFL_OK;
         default: return fail(&s, EFL_ERR_INVALID_ARGUMENT, "unknown stage");
@@ -1937,6 +2293,69 @@ float eflo_exp(float x) { return exp_for_test(x); }
 
 void eflo_set_fim_serial(eflo_sim* s, int32_t on) {
     if (s) s->fim_serial = on != 0;
+}
+
+efl_status eflo_set_particle_levelset(eflo_sim* s, int32_t enable) {
+    if (!s) return EFL_ERR_INVALID_ARGUMENT;
+    s->pls_on = enable != 0;
+    return EFL_OK;
+}
+
+efl_status eflo_particle_counts(eflo_sim* s, uint32_t counts[2], uint32_t* dropped) {
+    if (!s || !counts) return EFL_ERR_INVALID_ARGUMENT;
+    counts[0] = (uint32_t)s->parts[0].size();
+    counts[1] = (uint32_t)s->parts[1].size();
+    if (dropped) *dropped = s->pls_dropped;
+    return EFL_OK;
+}
+
+efl_status eflo_read_particles(eflo_sim* s, int32_t layer, efl_particle* dst, uint32_t capacity, uint32_t* n) {
+    if (!s || !n || (capacity && !dst)) return EFL_ERR_INVALID_ARGUMENT;
+    if (layer != EFL_PLS_POSITIVE && layer != EFL_PLS_NEGATIVE) return fail(s, EFL_ERR_INVALID_ARGUMENT, "layer");
+    const std::vector<OParticle>& v = s->parts[layer];
+    *n = (uint32_t)v.size();
+    const uint32_t m = std::min(*n, capacity);
+    for (uint32_t i = 0; i < m; ++i) {
+        dst[i].position[0] = v[i].x;
+        dst[i].position[1] = v[i].y;
+        dst[i].radius = v[i].radius;
+        dst[i].sign = v[i].sign;
+        dst[i].escaped = v[i].escaped;
+        dst[i]._pad = 0;
+    }
+    return EFL_OK;
+}
+
+efl_status eflo_write_particles(eflo_sim* s, int32_t layer, const efl_particle* src, uint32_t n) {
+    if (!s || (n && !src)) return EFL_ERR_INVALID_ARGUMENT;
+    if (layer != EFL_PLS_POSITIVE && layer != EFL_PLS_NEGATIVE) return fail(s, EFL_ERR_INVALID_ARGUMENT, "layer");
+    if ((uint64_t)n > (uint64_t)s->nx * s->ny * PLS_PER_CELL) return fail(s, EFL_ERR_TOO_MANY, "capacity");
+    const float sign = layer == EFL_PLS_POSITIVE ? 1.0f : -1.0f;
+    std::vector<OParticle> v(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        if (src[i].sign != sign) return fail(s, EFL_ERR_INVALID_ARGUMENT, "sign does not match the layer");
+        v[i] = OParticle{src[i].position[0], src[i].position[1], src[i].radius, sign, src[i].escaped ? 1u : 0u};
+    }
+    s->parts[layer] = std::move(v);
+    return EFL_OK;
+}
+
+efl_status eflo_pls_run_phase(eflo_sim* s, int32_t phase, float dt) {
+    if (!s) return EFL_ERR_INVALID_ARGUMENT;
+    switch (phase) {
+        case EFL_PLS_INITIALIZE: pls_initialize(*s); return EFL_OK;
+        case EFL_PLS_ADVECT: {
+            const float keep = s->U.dt;
+            s->U.dt = dt;
+            pls_advect(*s);
+            s->U.dt = keep;
+            return EFL_OK;
+        }
+        case EFL_PLS_CORRECT: pls_correct(*s, s->ls1, false); return EFL_OK;
+        case EFL_PLS_CORRECT_SECOND: pls_correct(*s, s->ls0, true); return EFL_OK;
+        case EFL_PLS_RESEED: pls_reseed(*s); return EFL_OK;
+        default: return fail(s, EFL_ERR_INVALID_ARGUMENT, "unknown phase");
+    }
 }
 
 }  // extern "C"

@@ -48,6 +48,14 @@ EFL_API efl_status eflo_residual(eflo_sim* sim, double* relative, double* norm_r
 EFL_API efl_status eflo_fluid_volume(eflo_sim* sim, uint64_t* cells);
 EFL_API efl_status eflo_velocity_magnitude(eflo_sim* sim, float* min_mag, float* max_mag);
 
+/* Two-layer particle level set (src/euler_fluid/particle_levelset_two_layers). */
+EFL_API efl_status eflo_set_particle_levelset(eflo_sim* sim, int32_t enable);
+EFL_API efl_status eflo_particle_counts(eflo_sim* sim, uint32_t counts[2], uint32_t* dropped);
+EFL_API efl_status eflo_read_particles(eflo_sim* sim, int32_t layer, efl_particle* dst, uint32_t capacity,
+                                       uint32_t* n);
+EFL_API efl_status eflo_write_particles(eflo_sim* sim, int32_t layer, const efl_particle* src, uint32_t n);
+EFL_API efl_status eflo_pls_run_phase(eflo_sim* sim, int32_t phase, float dt);
+
 /* Number of OpenMP threads the oracle uses (0 = OpenMP default). */
 EFL_API void eflo_set_threads(int32_t n);
 EFL_API int32_t eflo_get_threads(void);

@@ -1,0 +1,506 @@
+"""Two-layer particle level set (src/euler_fluid/particle_levelset_two_layers/**).
+
+CPU tests pin the oracle's restatement against an independent float32 numpy
+restatement of the WGSL (hash.wgsl, particle.wgsl, initialize_particles.wgsl,
+reseed_particles.wgsl, the level-set correction shaders); GPU tests check the
+CUDA path against the oracle bit for bit, phase by phase and over whole steps.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from bevy_eulerian_fluid_b200 import _capi as capi
+from bevy_eulerian_fluid_b200 import scenes
+from tests.helpers import STATE_FIELDS, compare_fields
+
+f32 = np.float32
+MAX_PER_CELL = 16
+BAND = f32(3.0)
+
+
+# ---------------------------------------------------------------------------
+# float32 restatement of the WGSL helpers
+
+def _u32(v):
+    return v & 0xFFFFFFFF
+
+
+def _rotl(x):
+    return _u32((x << 15) | (x >> 17))
+
+
+def murmur(k, h):  # utils/hash.wgsl:9-36 (one 4-byte block)
+    k = _u32(k * 0xCC9E2D51)
+    k = _rotl(k)
+    k = _u32(k * 0x1B873593)
+    h ^= k
+    h = _rotl(h)
+    h = _u32(h * 5 + 0xE6546B64)
+    h ^= 4
+    h ^= h >> 16
+    h = _u32(h * 0x85EBCA6B)
+    h ^= h >> 13
+    h = _u32(h * 0xC2B2AE35)
+    h ^= h >> 16
+    return h
+
+
+def _bits(v):
+    return int(np.array([v], dtype=np.float32).view(np.uint32)[0])
+
+
+def _unit(h):
+    return np.array([(h & 0x007FFFFF) | 0x3F800000], dtype=np.uint32).view(np.float32)[0] - f32(1.0)
+
+
+def hash22(x, y):
+    return _unit(murmur(_bits(x), 12345)), _unit(murmur(_bits(y), 98765))
+
+
+def hash11(v):
+    return _unit(murmur(_bits(v), 11111))
+
+
+def wi32(v):  # WGSL i32(f32)
+    v = float(v)
+    if v != v:
+        return 0
+    return int(max(min(v, 2147483647.0), -2147483648.0))
+
+
+def ld(t, i, j):
+    h, w = t.shape[:2]
+    return t[j, i] if 0 <= i < w and 0 <= j < h else (np.zeros(t.shape[2:], np.float32) if t.ndim == 3 else f32(0))
+
+
+def mix(a, b, t):
+    return a * (f32(1.0) - t) + b * t
+
+
+def interp(t, x, y):  # utils/coordinate.wgsl:19-49
+    i, j = wi32(np.floor(x)), wi32(np.floor(y))
+    fi, fj = f32(x - f32(i)), f32(y - f32(j))
+    return mix(mix(ld(t, i, j), ld(t, i + 1, j), fi), mix(ld(t, i, j + 1), ld(t, i + 1, j + 1), fi), fj)
+
+
+def radius_of(phi):
+    return min(max(f32(abs(phi)), f32(0.1)), f32(0.5))
+
+
+def spawn(ls, grad, x, y, goal, bmin, bmax):  # particle.wgsl:56-82
+    ny, nx = ls.shape
+    phi = interp(ls, x, y)
+    g = interp(grad, x, y)
+    ln = np.sqrt(g[0] * g[0] + g[1] * g[1])
+    gx, gy = g[0] / ln, g[1] / ln
+    k = f32(1.0) * (goal - phi)
+    xn, yn = x + k * gx, y + k * gy
+    if not (f32(0) < xn and f32(0) < yn and xn < f32(nx) - f32(1) and yn < f32(ny) - f32(1)):
+        return None
+    pn = interp(ls, xn, yn)
+    if not (bmin <= pn <= bmax):
+        return None
+    return f32(xn), f32(yn), radius_of(pn)
+
+
+def seed_reference(ls, grad):
+    """initialize_particles.wgsl over every band cell, in cell order."""
+    ny, nx = ls.shape
+    pos, neg = [], []
+    bmin, bmax = f32(0.1), BAND
+    for y in range(ny):
+        for x in range(nx):
+            if not abs(ls[y, x]) < BAND:
+                continue
+            cell = x + nx * y
+            xb, yb = f32(x), f32(y)
+            for i in range(MAX_PER_CELL):
+                seed = cell + i
+                hx, hy = hash22(xb + f32(seed), yb + f32(seed))
+                px, py = xb + hx, yb + hy
+                goal = hash11(f32(seed)) * (bmax - bmin) + bmin
+                p = spawn(ls, grad, px, py, goal, bmin, bmax)
+                if p:
+                    pos.append(p)
+                goal_n = hash11(f32(seed + 1000)) * ((-bmin) - (-bmax)) + (-bmax)
+                q = spawn(ls, grad, px, py, goal_n, -bmax, -bmin)
+                if q:
+                    neg.append(q)
+    return pos, neg
+
+
+def heap_reference(prios, escaped, near, base=0):
+    """reseed_particles.wgsl:14-97 for one bucket: alive flags and the number to add.
+
+    Local-array indices past 15 are clamped (bounds-checked access); the heap
+    starts zero-initialised.  Heap nodes hold global slots (base + i); the
+    eviction of a zero node names global slot 0, which only acts when this
+    bucket starts there (for another bucket it is the reference's racy write,
+    ordered before that bucket's own writes)."""
+    n = len(prios)
+    heap = [[0, f32(0.0)] for _ in range(MAX_PER_CELL)]
+    cl = lambda i: min(i, MAX_PER_CELL - 1)
+    alive = [0] * n
+
+    def correct(cap):
+        i = 0
+        while True:
+            l, r, big = 2 * i + 1, 2 * i + 2, i
+            if l < cap and heap[l][1] > heap[big][1]:
+                big = l
+            if r < cap and heap[r][1] > heap[big][1]:
+                big = r
+            if big == i:
+                return
+            heap[big], heap[i] = heap[i], heap[big]
+            i = big
+
+    def sift_up(size):
+        i = size - 1
+        while True:
+            p = ((i - 1) & 0xFFFFFFFF) // 2
+            if heap[cl(p)][1] > heap[cl(i)][1]:
+                return
+            heap[cl(p)], heap[cl(i)] = heap[cl(i)], heap[cl(p)]
+            i = p
+            if i == 0:
+                return
+
+    def kill(slot):
+        if base <= slot < base + n:
+            alive[slot - base] = 0
+
+    cap, idx = MAX_PER_CELL, 0
+    for i in range(n):
+        if not near:
+            alive[i] = 0
+            continue
+        if escaped[i]:
+            if cap != 0:
+                alive[i] = 1
+                cap -= 1
+                if idx > cap:
+                    kill(heap[0][0])
+                    heap[0] = list(heap[idx - 1])
+                    idx -= 1
+                    correct(cap)
+            else:
+                alive[i] = 0
+            continue
+        if idx < cap:
+            alive[i] = 1
+            heap[idx] = [base + i, prios[i]]
+            idx += 1
+            sift_up(idx)
+        elif prios[i] < heap[0][1]:
+            alive[i] = 1
+            kill(heap[0][0])
+            heap[0] = [base + i, prios[i]]
+            correct(cap)
+        else:
+            alive[i] = 0
+    return alive, (cap - idx if near else 0)
+
+
+def circle_levelset(n, cx, cy, r):
+    y, x = np.mgrid[0:n, 0:n].astype(np.float64)
+    ls = (np.sqrt((x - cx) ** 2 + (y - cy) ** 2) - r).astype(np.float32)
+    gy, gx = np.gradient(ls.astype(np.float64))
+    grad = np.stack([gx, gy], axis=-1).astype(np.float32)
+    return ls, grad
+
+
+def particles_array(rows, sign):
+    a = np.zeros(len(rows), dtype=capi.PARTICLE_DTYPE)
+    for k, r in enumerate(rows):
+        a[k]["position"] = r[0], r[1]
+        a[k]["radius"] = r[2]
+        a[k]["sign"] = sign
+        a[k]["escaped"] = r[3] if len(r) > 3 else 0
+    return a
+
+
+def fresh(api, n=32, ls=None, grad=None):
+    sim = capi.Sim(api, scenes.base_config(n, n))
+    sim.set_particle_levelset(True)
+    if ls is not None:
+        sim.set(capi.FIELD_LEVELSET_AIR, ls)
+        sim.set(capi.FIELD_LEVELSET_AIR1, ls)
+    if grad is not None:
+        sim.set(capi.FIELD_GRAD_LEVELSET, grad)
+    return sim
+
+
+# ---------------------------------------------------------------------------
+# CPU: the oracle against the numpy restatement
+
+def test_murmur_known_values():
+    # MurmurHash3_x86_32 of one 4-byte block differs from the published hash
+    # only in the h rotation (15 instead of 13): with seed 0 and key 0 the
+    # finaliser of the published hash gives 0x2362F9DE; check that the
+    # restatement reproduces it when given the published rotation.
+    def published(k, h):
+        k = _u32(k * 0xCC9E2D51)
+        k = _rotl(k)
+        k = _u32(k * 0x1B873593)
+        h ^= k
+        h = _u32((h << 13) | (h >> 19))
+        h = _u32(h * 5 + 0xE6546B64)
+        h ^= 4
+        h ^= h >> 16
+        h = _u32(h * 0x85EBCA6B)
+        h ^= h >> 13
+        h = _u32(h * 0xC2B2AE35)
+        h ^= h >> 16
+        return h
+    assert published(0, 0) == 0x2362F9DE
+    assert 0.0 <= hash11(f32(7.0)) < 1.0
+    hx, hy = hash22(f32(3.0), f32(3.0))
+    assert hx != hy  # different seeds per component
+
+
+def test_oracle_seeding_matches_restatement(oracle_api):
+    ls, grad = circle_levelset(32, 15.3, 16.7, 7.2)
+    sim = fresh(oracle_api, 32, ls, grad)
+    sim.pls_run_phase(capi.PLS_INITIALIZE)
+    pos, neg = seed_reference(ls, grad)
+    got_p, got_n = sim.read_particles(0), sim.read_particles(1)
+    assert len(pos) > 100 and len(neg) > 100
+    assert len(got_p) == len(pos) and len(got_n) == len(neg)
+    for got, ref, sign in ((got_p, pos, 1.0), (got_n, neg, -1.0)):
+        r = np.array(ref, dtype=np.float32)
+        assert np.array_equal(got["position"], r[:, :2])
+        assert np.array_equal(got["radius"], r[:, 2])
+        assert np.all(got["sign"] == sign) and np.all(got["escaped"] == 0)
+    sim.close()
+
+
+def test_oracle_initial_scene_seeds_only_positive_particles(oracle_api):
+    # initialize_grid_center.wgsl: phi = ny - y >= 1 everywhere, so negative
+    # goals in [-3, -0.1] land outside the domain and are rejected
+    sc = scenes.dam_break(64)
+    sim = sc.make(oracle_api)
+    sim.set_particle_levelset(True)
+    sim.step(sc.dt)  # init sequence
+    (p, n), dropped = sim.particle_counts()
+    assert p > 0 and n == 0 and dropped == 0
+    pp = sim.read_particles(0)
+    assert np.all(pp["position"][:, 1] > 64 - 1 - 3.0 - 1e-3)
+    sim.close()
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_oracle_reseed_heap_matches_restatement(oracle_api, seed):
+    rng = np.random.default_rng(seed)
+    n = 32
+    ls = rng.uniform(-1.5, 1.5, (n, n)).astype(np.float32)  # every cell in the band, some escapes
+    grad = np.zeros((n, n, 2), np.float32)  # refill attempts all fail (normalize(0) = NaN)
+    sim = fresh(oracle_api, n, ls, grad)
+    cells = [(5, 7), (20, 9), (11, 25)]
+    rows = []
+    for cx, cy in cells:
+        k = int(rng.integers(1, 40))
+        for _ in range(k):
+            x, y = cx + rng.uniform(0.0, 0.999), cy + rng.uniform(0.0, 0.999)
+            r = f32(rng.choice([0.1, 0.3, 0.5, 2.5]))  # 2.5: never escaped; 0.1: may be
+            rows.append((f32(x), f32(y), r))
+    rng.shuffle(rows)
+    sim.write_particles(0, particles_array(rows, 1.0))
+    sim.pls_run_phase(capi.PLS_RESEED)
+    got = sim.read_particles(0)
+    # restatement: stable bucket order = index order inside each cell, cells in raster order
+    expect = []
+    base = 0
+    for cx, cy in sorted(cells, key=lambda c: c[0] + n * c[1]):
+        idx = [i for i, r in enumerate(rows) if int(r[0]) == cx and int(r[1]) == cy]
+        pr, es = [], []
+        for i in idx:
+            x, y, r = rows[i]
+            phi = interp(ls, x, y)
+            es.append(bool(f32(1.0) * phi + r < f32(0)))
+            pr.append(f32(f32(1.0) * phi - r))
+        alive, _ = heap_reference(pr, es, True, base)
+        expect += [rows[i] for i, a in zip(idx, alive) if a]
+        base += len(idx)
+    assert len(got) == len(expect)
+    assert np.array_equal(got["position"], np.array([(e[0], e[1]) for e in expect], np.float32))
+    assert np.array_equal(got["radius"], np.array([e[2] for e in expect], np.float32))
+    sim.close()
+
+
+def test_heap_restatement_keeps_lowest_priorities():
+    prios = [f32(v) for v in np.random.default_rng(3).uniform(-1, 1, 40)]
+    alive, add = heap_reference(prios, [False] * 40, True)
+    kept = sorted(p for p, a in zip(prios, alive) if a)
+    assert kept == sorted(prios)[:16] and add == 0
+    alive, add = heap_reference(prios[:5], [False] * 5, True)
+    assert alive == [1] * 5 and add == 11
+    alive, add = heap_reference(prios[:5], [False] * 5, False)
+    assert alive == [0] * 5 and add == 0
+
+
+def test_oracle_correction_matches_restatement(oracle_api):
+    n = 32
+    ls, grad = circle_levelset(n, 16.0, 16.0, 6.0)
+    sim = fresh(oracle_api, n, ls, grad)
+    rng = np.random.default_rng(11)
+    # positive particles inside the fluid (escaped), negative ones outside
+    pos = [(f32(16 + rng.uniform(-3, 3)), f32(16 + rng.uniform(-3, 3)), f32(0.5)) for _ in range(40)]
+    neg = [(f32(rng.uniform(1, 30)), f32(rng.uniform(1, 3)), f32(0.3)) for _ in range(40)]
+    sim.write_particles(0, particles_array(pos, 1.0))
+    sim.write_particles(1, particles_array(neg, -1.0))
+    sim.pls_run_phase(capi.PLS_CORRECT)
+    got = sim.get(capi.FIELD_LEVELSET_AIR1)
+
+    def fixed(v):
+        return wi32(f32(v) * f32(10000.0))
+    plus = np.vectorize(fixed)(ls).astype(np.int64)
+    minus = plus.copy()
+    for parts, sign, acc in ((pos, 1.0, plus), (neg, -1.0, minus)):
+        for x, y, r in parts:
+            if not (f32(sign) * interp(ls, x, y) + r < 0):
+                continue
+            bx, by = int(x), int(y)
+            for i in range(2):
+                for j in range(2):
+                    cx, cy = bx + i, by + j
+                    if cx >= n or cy >= n:
+                        continue
+                    dx, dy = f32(x - f32(cx)), f32(y - f32(cy))
+                    q = fixed(f32(sign) * (r - np.sqrt(dx * dx + dy * dy)))
+                    acc[cy, cx] = max(acc[cy, cx], q) if sign > 0 else min(acc[cy, cx], q)
+    pp = plus.astype(np.float32) / f32(10000.0)
+    pm = minus.astype(np.float32) / f32(10000.0)
+    expect = np.where(np.abs(pp) <= np.abs(pm), pp, pm)
+    assert np.array_equal(got, expect)
+    assert np.any(plus != np.vectorize(fixed)(ls))  # the particles did correct something
+    esc = sim.read_particles(0)["escaped"]
+    assert esc.sum() > 0
+    sim.close()
+
+
+def test_write_particles_checks(oracle_api):
+    sim = fresh(oracle_api, 16)
+    bad = particles_array([(f32(1), f32(1), f32(0.1))], -1.0)
+    with pytest.raises(capi.EflError):
+        sim.write_particles(0, bad)
+    sim.close()
+
+
+# ---------------------------------------------------------------------------
+# GPU parity (bit-exact)
+
+def _compare_particles(a: capi.Sim, b: capi.Sim):
+    ca, cb = a.particle_counts(), b.particle_counts()
+    assert ca == cb, (ca, cb)
+    for layer in (0, 1):
+        pa, pb = a.read_particles(layer), b.read_particles(layer)
+        for f in ("position", "radius", "sign", "escaped"):
+            if not np.array_equal(pa[f], pb[f]):
+                bad = np.nonzero(np.any((pa[f] != pb[f]).reshape(len(pa), -1), axis=1))[0]
+                raise AssertionError(f"layer {layer} field {f}: {len(bad)} particles differ, first {bad[:5]}")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("phase", ["init", "advect", "correct", "correct_second", "reseed"])
+def test_gpu_pls_phase_parity(oracle_api, gpu_api, phase):
+    n = 64
+    ls, grad = circle_levelset(n, 30.2, 33.9, 14.5)
+    pair = [fresh(api, n, ls, grad) for api in (oracle_api, gpu_api)]
+    o, g = pair
+    u = np.random.default_rng(7).uniform(-30, 30, o.get(capi.FIELD_U).shape).astype(np.float32)
+    v = np.random.default_rng(8).uniform(-30, 30, o.get(capi.FIELD_V).shape).astype(np.float32)
+    for s in pair:
+        s.set(capi.FIELD_U, u)
+        s.set(capi.FIELD_V, v)
+        s.pls_run_phase(capi.PLS_INITIALIZE)
+    _compare_particles(o, g)
+    if phase == "init":
+        return
+    # perturb: move particles so that some escape and cells overflow
+    for layer in (0, 1):
+        p = o.read_particles(layer)
+        jit = np.random.default_rng(20 + layer).normal(0, 1.5, p["position"].shape).astype(np.float32)
+        p["position"] += jit
+        for s in pair:
+            s.write_particles(layer, p)
+    ph = {"advect": capi.PLS_ADVECT, "correct": capi.PLS_CORRECT, "correct_second": capi.PLS_CORRECT_SECOND,
+          "reseed": capi.PLS_RESEED}[phase]
+    for s in pair:
+        s.pls_run_phase(ph, 0.05)
+    _compare_particles(o, g)
+    assert compare_fields(o, g, [capi.FIELD_LEVELSET_AIR, capi.FIELD_LEVELSET_AIR1]) == []
+    for s in pair:
+        s.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n,steps", [(64, 16), (128, 8)])
+def test_gpu_pls_scene_parity(oracle_api, gpu_api, n, steps):
+    sc = scenes.dam_break(n)
+    o, g = sc.make(oracle_api), sc.make(gpu_api)
+    for s in (o, g):
+        s.set_particle_levelset(True)
+    for k in range(steps):
+        for s in (o, g):
+            s.step(sc.dt)
+        _compare_particles(o, g)
+        bad = compare_fields(o, g, STATE_FIELDS)
+        assert bad == [], (k, bad)
+    (p, q), dropped = g.particle_counts()
+    assert p > 0 and q > 0 and dropped == 0
+    for s in (o, g):
+        s.close()
+
+
+@pytest.mark.gpu
+def test_gpu_pls_coupled_parity(oracle_api, gpu_api):
+    from tests.helpers import small_coupled
+    sc = small_coupled(64)
+    o, g = sc.make(oracle_api), sc.make(gpu_api)
+    for s in (o, g):
+        s.set_particle_levelset(True)
+    for k in range(6):
+        for s in (o, g):
+            s.step(sc.dt)
+        _compare_particles(o, g)
+        assert compare_fields(o, g, STATE_FIELDS) == [], k
+    for s in (o, g):
+        s.close()
+
+
+@pytest.mark.gpu
+def test_gpu_pls_capacity_overflow(oracle_api, gpu_api):
+    n = 16
+    ls, grad = circle_levelset(n, 7.5, 8.0, 4.0)
+    full = np.zeros(n * n * MAX_PER_CELL, dtype=capi.PARTICLE_DTYPE)
+    full["position"] = 0.5
+    full["radius"] = 0.1
+    full["sign"] = 1.0
+    out = []
+    for api in (oracle_api, gpu_api):
+        s = fresh(api, n, ls, grad)
+        s.write_particles(0, full)
+        s.pls_run_phase(capi.PLS_INITIALIZE)
+        out.append(s.particle_counts())
+        s.close()
+    assert out[0] == out[1]
+    (p, q), dropped = out[1]
+    assert p == n * n * MAX_PER_CELL and dropped > 0 and q > 0
+
+
+@pytest.mark.gpu
+def test_gpu_pls_graph_replay_matches_eager(gpu_api):
+    sc = scenes.dam_break(64)
+    runs = []
+    for graphs in (True, False):
+        s = sc.make(gpu_api)
+        s.set_particle_levelset(True)
+        s.set_graph_capture(graphs)
+        for _ in range(10):
+            s.step(sc.dt)
+        runs.append((s.read_particles(0), s.read_particles(1), s.get(capi.FIELD_LEVELSET_AIR)))
+        s.close()
+    for a, b in zip(runs[0], runs[1]):
+        assert np.array_equal(a, b)
