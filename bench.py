@@ -71,7 +71,8 @@ def parse():
     ap.add_argument("--no-learned", action="store_true")
     ap.add_argument("--c3-size", type=int, default=4096, help="grid of the C3 scale scene (4096 in the benchmark)")
     ap.add_argument("--batch-sims", type=int, default=96, help="simulations of the C4 batch (96 in the benchmark)")
-    ap.add_argument("--only", choices=["coupled", "microbench", "batch", "c3", "learned"], default=None,
+    ap.add_argument("--no-pls", action="store_true")
+    ap.add_argument("--only", choices=["coupled", "microbench", "batch", "c3", "learned", "pls"], default=None,
                     help="profiling aid: run one part only and print its numbers")
     return ap.parse_args()
 
@@ -233,6 +234,9 @@ def main():
     if args.only == "c3":
         print(json.dumps(c3_leg(capi.load(), torch, args, local, measured_peaks()[0])), flush=True)
         return 0
+    if args.only == "pls":
+        print(json.dumps(pls_leg(capi.load(), torch, args, local, measured_peaks()[0])), flush=True)
+        return 0
     if args.only == "batch":
         dist = None
         if world > 1:
@@ -363,6 +367,9 @@ def main():
     lw = None
     if not args.no_learned and rank == 0 and args.only is None:
         lw = learned_leg(api, args, local)
+    pls = None
+    if not args.no_pls and rank == 0 and args.only is None:
+        pls = pls_leg(api, torch, args, local, peak)
 
     sim.close()
     if dist:
@@ -401,6 +408,8 @@ def main():
         line["c3"] = c3
     if lw:
         line["learned"] = lw
+    if pls:
+        line["particle_levelset"] = pls
     print(json.dumps(line), flush=True)
     return 0
 
@@ -615,6 +624,66 @@ def coupled_mgpcg(api, torch, args, local, flush, dist):
             "value": world * sc.cells * args.steps / (ms / 1e3), "unit": "cell-steps/s",
             "ms_per_step": ms / args.steps, "pressure_solve_ms_per_step": sum(solve) / args.steps,
             "cg_iterations_per_step": iters}
+
+
+PLS_SETTLE_STEPS = 20  # steps after the init sequence that let the particles fill the band
+
+
+def pls_leg(api, torch, args, local, peak):
+    """dam_break (C1 scene) at --size with the two-layer particle level set: device time per step with
+    and without it (CUDA events on the simulation's stream, L2 flushed before each step), and each
+    particle phase re-run on the live state (efl_pls_run_phase), timed the same way."""
+    from bevy_eulerian_fluid_b200 import _capi as capi
+    from bevy_eulerian_fluid_b200 import scenes
+    sc = scenes.dam_break(args.size)
+    sc.cfg.device = local
+    flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device=f"cuda:{local}")
+    out = {"workload": f"dam_break_{args.size} with the two-layer particle level set (C1 scene, 20 RBGS)",
+           "settle_steps": PLS_SETTLE_STEPS, "steps": args.steps, "l2": "flushed (256 MiB write) before each step"}
+    ms = {}
+    for on in (False, True):
+        sim = sc.make(api)
+        sim.set_particle_levelset(on)
+        stream = torch.cuda.ExternalStream(sim.stream(), device=f"cuda:{local}")
+        for _ in range(1 + PLS_SETTLE_STEPS + args.warmup):
+            sim.step(sc.dt)
+        torch.cuda.synchronize()
+        ev = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(args.steps)]
+        l0 = api.kernel_launches()
+        for k in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            ev[k][0].record(stream)
+            sim.step(sc.dt)
+            ev[k][1].record(stream)
+        torch.cuda.synchronize()
+        launches = api.kernel_launches() - l0
+        ms[on] = sum(e[0].elapsed_time(e[1]) for e in ev) / args.steps
+        if on:
+            (n_pos, n_neg), dropped = sim.particle_counts()
+            phases = {}
+            for name, ph in (("advect", capi.PLS_ADVECT), ("correct", capi.PLS_CORRECT),
+                             ("correct_second", capi.PLS_CORRECT_SECOND), ("reseed", capi.PLS_RESEED)):
+                t = []
+                for _ in range(3):
+                    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    with torch.cuda.stream(stream):
+                        flush.zero_()
+                    a.record(stream)
+                    sim.pls_run_phase(ph, sc.dt)
+                    b.record(stream)
+                    torch.cuda.synchronize()
+                    t.append(a.elapsed_time(b))
+                phases[name] = round(statistics.median(t), 4)
+            out.update({"particles": {"positive": n_pos, "negative": n_neg, "dropped": dropped},
+                        "gpu_launches_per_step": launches / args.steps, "phase_ms": phases})
+        sim.close()
+    n = out["particles"]["positive"] + out["particles"]["negative"]
+    extra = ms[True] - ms[False]
+    out.update({"ms_per_step": {"with": round(ms[True], 4), "without": round(ms[False], 4),
+                                "particle_pass": round(extra, 4)},
+                "particle_steps_per_s": n / (extra / 1e3) if extra > 0 else None})
+    return out
 
 
 def tensor_peak():

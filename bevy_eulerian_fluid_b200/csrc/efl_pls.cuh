@@ -27,33 +27,54 @@ constexpr float PLS_BAND = 3.0f;       // constants.wgsl:5 (BAND_WIDTH)
 constexpr float PLS_SCALE = 10000.0f;  // fixed_point.wgsl:3
 constexpr int PLS_THREADS = 256;       // constants.wgsl:4 (PARTICLE_WORKWGROUP_SIZE)
 
-// Everything the particle kernels touch.  [l] = layer.
+// Everything the particle kernels touch.  [l] = layer, [b] = buffer.
+// Each layer has two particle buffers; sel[l] names the live one and the
+// reseed compacts into the other, then flips sel (no copy back, and the
+// launch arguments stay the same from step to step for graph replay).
 struct PlsArgs {
-    float* px[2];
-    float* py[2];
-    float* rad[2];
-    uint8_t* esc[2];
-    float* qx[2];  // compaction target (reseed), copied back afterwards
-    float* qy[2];
-    float* qrad[2];
-    uint8_t* qesc[2];
+    float* px[2][2];
+    float* py[2][2];
+    float* rad[2][2];
+    uint8_t* esc[2][2];
+    int* sel;                 // [2] live buffer per layer
     uint32_t* count;          // [2] live particles
     uint32_t* cnt;            // [2][L] particles per cell
     uint32_t* cur;            // [2][L] scatter cursors
     uint32_t* off;            // [2][L] exclusive scan of cnt
-    uint32_t* sidx;           // [2][cap] particle index per sorted slot
+    uint32_t* sidx;           // [2][cap] particle index per slot (scatter order)
+    uint32_t* scell;          // [2][cap] cell of the slot
+    uint32_t* sorted;         // [2][cap] particle index per slot, buckets in index order
+    float* prio;              // [2][cap] heap priority per sorted slot (buckets of > 16)
+    uint8_t* sesc;            // [2][cap] escaped per sorted slot (buckets of > 16)
     uint8_t* alive;           // [2][cap] reseed decision per sorted slot
+    uint32_t* prank;          // [2][cap] rank of a kept slot among its bucket's kept slots
     unsigned long long* val;  // [2][L] kept | new << 32, then its exclusive scan
     unsigned long long* tot;  // [2] totals of val
     uint32_t* ctot;           // [2] totals of cnt
-    uint8_t* addn;            // [2][L] particles to add per cell
+    uint8_t* addn;            // [2][L] refill attempts per cell
+    uint16_t* vmask;          // [2][L] accepted refill attempts per cell (bit i = attempt i)
+    uint32_t* work;           // [2][L] cells with attempts to make (any order)
+    uint32_t* nwork;          // [2] length of work
+    uint32_t* slow;           // [2][L] band cells of more than 16 particles (any order)
+    uint32_t* nslow;          // [2] length of slow
     int32_t* phip;            // [L] phi_plus  (fixed point)
     int32_t* phim;            // [L] phi_minus (fixed point)
     uint32_t* dropped;        // particles not stored for lack of capacity
+    uint32_t* ticket;         // blocks of k_pls_emit done (0 between launches)
     uint32_t cap;             // per layer
     uint32_t L;               // nx * ny
     int nx, ny;
 };
+
+struct PView {
+    float* x;
+    float* y;
+    float* r;
+    uint8_t* e;
+};
+EFL_DEV PView pls_buf(const PlsArgs& a, int l, int b) { return PView{a.px[l][b], a.py[l][b], a.rad[l][b], a.esc[l][b]}; }
+EFL_DEV PView pls_live(const PlsArgs& a, int l) { return pls_buf(a, l, a.sel[l]); }
+EFL_DEV PView pls_spare(const PlsArgs& a, int l) { return pls_buf(a, l, 1 - a.sel[l]); }
 
 // ---------------------------------------------------------------------------
 // WGSL helpers used by the plugin
@@ -256,19 +277,18 @@ __global__ void k_scan_add(T* out, const T* part, uint32_t n, uint32_t stride, u
 // advect_particles.wgsl:15-33 with utils/coordinate.wgsl:96-109 (tvd_rk3).
 __global__ void k_pls_advect(PlsArgs a, PF u, PF v, float dt) {
     const int l = blockIdx.y;
-    uint32_t n = a.count[l];
-    float* px = a.px[l];
-    float* py = a.py[l];
+    const uint32_t n = a.count[l];
+    const PView P = pls_live(a, l);
     const float third = 1.0f / 3.0f, two_thirds = 2.0f / 3.0f;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        float x = px[i], y = py[i];
+        float x = P.x[i], y = P.y[i];
         float u0 = interp_edge_x(u, x, y), v0 = interp_edge_y(v, x, y);
         float x1 = x + dt * u0, y1 = y + dt * v0;
         float u1 = interp_edge_x(u, x1, y1), v1 = interp_edge_y(v, x1, y1);
         float x2 = 0.75f * x + 0.25f * (x1 + dt * u1), y2 = 0.75f * y + 0.25f * (y1 + dt * v1);
         float u2 = interp_edge_x(u, x2, y2), v2 = interp_edge_y(v, x2, y2);
-        px[i] = third * x + two_thirds * (x2 + dt * u2);
-        py[i] = third * y + two_thirds * (y2 + dt * v2);
+        P.x[i] = third * x + two_thirds * (x2 + dt * u2);
+        P.y[i] = third * y + two_thirds * (y2 + dt * v2);
     }
 }
 
@@ -290,12 +310,13 @@ __global__ void k_pls_reset(PlsArgs a, PF ls) {
 __global__ void k_pls_mark_accumulate(PlsArgs a, PF ls) {
     const int l = blockIdx.y;
     const float sgn = l == 0 ? 1.0f : -1.0f;
-    uint32_t n = a.count[l];
+    const uint32_t n = a.count[l];
+    const PView P = pls_live(a, l);
     int32_t* phi = l == 0 ? a.phip : a.phim;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        float x = a.px[l][i], y = a.py[l][i], r = a.rad[l][i];
+        float x = P.x[i], y = P.y[i], r = P.r[i];
         bool e = sgn * interp_center(ls, x, y) + r < 0.0f;
-        a.esc[l][i] = e ? 1 : 0;
+        P.e[i] = e ? 1 : 0;
         if (!e) continue;
         uint32_t bx = f2u(x), by = f2u(y);
         for (uint32_t di = 0; di < 2; ++di)
@@ -328,45 +349,117 @@ __global__ void k_pls_correct(PlsArgs a, PF ls) {
 // particle's cell (no interpolation; 0 outside the grid -> radius 0.1).
 __global__ void k_pls_radii(PlsArgs a, PF ls) {
     const int l = blockIdx.y;
-    uint32_t n = a.count[l];
+    const uint32_t n = a.count[l];
+    const PView P = pls_live(a, l);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        a.rad[l][i] = pls_radius(ls.ld(f2i(a.px[l][i]), f2i(a.py[l][i])));
+        P.r[i] = pls_radius(ls.ld(f2i(P.x[i]), f2i(P.y[i])));
 }
 
-// count_particles_in_cell.wgsl:10-21
-__global__ void k_pls_bin(PlsArgs a) {
+// Warp-aggregated bucket append: lanes of a warp that share a cell make one
+// atomicAdd; returns this lane's position among the appends to its cell.
+EFL_DEV uint32_t pls_aggregated_add(uint32_t* counter, uint32_t cell, bool active) {
+    const unsigned act = __ballot_sync(0xffffffffu, active);
+    if (!active) return 0;
+    const unsigned peers = __match_any_sync(act, cell);
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(peers) - 1;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(counter, (uint32_t)__popc(peers));
+    base = __shfl_sync(peers, base, leader);
+    return base + (uint32_t)__popc(peers & ((1u << lane) - 1u));
+}
+
+// count_particles_in_cell.wgsl:10-21; with radii != 0 also the preceding
+// update_particle_radii.wgsl on ls (one pass over the positions for both).
+__global__ void k_pls_bin(PlsArgs a, PF ls, int radii) {
     const int l = blockIdx.y;
-    uint32_t n = a.count[l];
+    const uint32_t n = a.count[l];
+    const PView P = pls_live(a, l);
     uint32_t* cnt = a.cnt + (size_t)l * a.L;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        atomicAdd(&cnt[pls_bin(a.px[l][i], a.py[l][i], (uint32_t)a.nx, a.L)], 1u);
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i0 = blockIdx.x * blockDim.x; i0 < n; i0 += stride) {  // warp-uniform trip count
+        const uint32_t i = i0 + threadIdx.x;
+        const bool on = i < n;
+        const float x = on ? P.x[i] : 0.0f, y = on ? P.y[i] : 0.0f;
+        if (on && radii) P.r[i] = pls_radius(ls.ld(f2i(x), f2i(y)));
+        const uint32_t c = on ? pls_bin(x, y, (uint32_t)a.nx, a.L) : 0u;
+        const unsigned act = __ballot_sync(0xffffffffu, on);
+        if (on) {
+            const unsigned peers = __match_any_sync(act, c);
+            if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&cnt[c], (uint32_t)__popc(peers));
+        }
+    }
 }
 
-// sort_particles.wgsl:12-26: the slot of each particle in its cell's bucket
-// (arbitrary order inside the bucket; k_pls_reseed orders it).
+// sort_particles.wgsl:12-26: each particle's slot in its cell's bucket (the
+// order inside a bucket depends on atomic arrival; k_pls_rank orders it).
 __global__ void k_pls_scatter(PlsArgs a) {
     const int l = blockIdx.y;
-    uint32_t n = a.count[l];
+    const uint32_t n = a.count[l];
+    const PView P = pls_live(a, l);
     const uint32_t* off = a.off + (size_t)l * a.L;
     uint32_t* cur = a.cur + (size_t)l * a.L;
     uint32_t* sidx = a.sidx + (size_t)l * a.cap;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        uint32_t c = pls_bin(a.px[l][i], a.py[l][i], (uint32_t)a.nx, a.L);
-        sidx[off[c] + atomicAdd(&cur[c], 1u)] = i;
+    uint32_t* scell = a.scell + (size_t)l * a.cap;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i0 = blockIdx.x * blockDim.x; i0 < n; i0 += stride) {
+        const uint32_t i = i0 + threadIdx.x;
+        const bool on = i < n;
+        const uint32_t c = on ? pls_bin(P.x[i], P.y[i], (uint32_t)a.nx, a.L) : 0u;
+        const uint32_t k = pls_aggregated_add(&cur[c], c, on);
+        if (on) {
+            const uint32_t slot = off[c] + k;
+            sidx[slot] = i;
+            scell[slot] = c;
+        }
+    }
+}
+
+// The stable order: each slot's rank among its bucket's particle indices
+// (distinct), so bucket order = particle-index order.  For buckets of more
+// than 16 particles the heap inputs of reseed_particles.wgsl are staged here
+// in sorted order: priority sign * phi(x) - r (eval_priority, :101-103) and
+// the escaped test (particle.wgsl:19-30), on levelset_air0.
+__global__ void k_pls_rank(PlsArgs a, PF ls) {
+    const int l = blockIdx.y;
+    const uint32_t n = a.count[l];
+    const float sgn = l == 0 ? 1.0f : -1.0f;
+    const PView P = pls_live(a, l);
+    const size_t lc = (size_t)l * a.cap, ll = (size_t)l * a.L;
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+        const uint32_t c = a.scell[lc + s];
+        const uint32_t o = a.off[ll + c], m = a.cnt[ll + c];
+        const uint32_t v = a.sidx[lc + s];
+        const uint32_t* b = a.sidx + lc + o;
+        uint32_t r = 0;
+        for (uint32_t t = 0; t < m; ++t) r += b[t] < v ? 1u : 0u;
+        const size_t d = lc + o + r;
+        a.sorted[d] = v;
+        if (m > PLS_MAX_PER_CELL) {
+            const float rad = P.r[v];
+            const float phi = interp_center(ls, P.x[v], P.y[v]);
+            a.prio[d] = sgn * phi - rad;
+            a.sesc[d] = sgn * phi + rad < 0.0f ? 1 : 0;
+        }
     }
 }
 
 // ---------------------------------------------------------------------------
-// reseed_particles.wgsl:14-148, one thread per cell and layer.
+// reseed_particles.wgsl:14-148 per cell and layer.
 //
-// The heap is the reference's, including its index arithmetic: sift_up from
-// slot 0 computes the parent (0 - 1) / 2 in u32, and an index past the
-// 16-entry array is clamped to 15 (bounds-checked local array access); the
-// heap starts zero-initialised.  An eviction of a zero node (capacity used
-// up by escaped particles before any insertion) names slot 0 of the whole
-// buffer; inside this cell's bucket it applies, for another cell's bucket it
-// is the racy write the reference orders arbitrarily -- taken as landing
-// before that cell's own writes, i.e. without effect.
+// A bucket of at most 16 particles in a band cell keeps every particle and
+// asks for 16 - n new ones whatever their escape state: the heap never
+// overflows (inserted + escaped <= n <= 16 = capacity), so no eviction
+// happens.  Larger buckets get the heap's outcome from k_pls_select, or run
+// the reference's heap itself (pls_heap_serial), including its index
+// arithmetic: sift_up from slot 0 computes the parent (0 - 1) / 2 in u32,
+// and an index past the 16-entry array is clamped to 15 (bounds-checked
+// local array access); the heap starts zero-initialised.  An eviction of a
+// zero node (capacity used up by escaped particles before any insertion)
+// names slot 0 of the whole buffer; inside this cell's bucket it applies,
+// for another cell's bucket it is the racy write the reference orders
+// arbitrarily -- taken as landing before that cell's own writes, i.e.
+// without effect.
 struct PlsNode {
     uint32_t index;
     float value;
@@ -400,48 +493,60 @@ EFL_DEV void pls_sift_up(PlsNode* h, uint32_t size) {
     }
 }
 
-__global__ void k_pls_reseed(PlsArgs a, PF ls, P2 grad) {
+// Band cells of at most 16 particles and cells outside the band, one thread
+// per cell; band cells of more than 16 particles are listed for
+// k_pls_select.  Cells that will make refill attempts are listed in work.
+__global__ void k_pls_heap(PlsArgs a, PF ls) {
     const int l = blockIdx.y;
-    uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= a.L) return;
-    const float sgn = l == 0 ? 1.0f : -1.0f;
-    const int x = (int)(c % (uint32_t)a.nx), y = (int)(c / (uint32_t)a.nx);
-    const uint32_t n = a.cnt[(size_t)l * a.L + c];
-    const uint32_t off = a.off[(size_t)l * a.L + c];
-    uint32_t* b = a.sidx + (size_t)l * a.cap + off;
-    uint8_t* alive = a.alive + (size_t)l * a.cap;
-    const bool near = fabsf(interp_center(ls, (float)x, (float)y)) < PLS_BAND;
-
-    // stable order: the bucket by particle index
-    for (uint32_t i = 1; i < n; ++i) {
-        uint32_t v = b[i];
-        uint32_t j = i;
-        while (j > 0 && b[j - 1] > v) {
-            b[j] = b[j - 1];
-            --j;
+    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = c < a.L;
+    const uint32_t cc = valid ? c : 0u;
+    const int x = (int)(cc % (uint32_t)a.nx), y = (int)(cc / (uint32_t)a.nx);
+    const size_t ll = (size_t)l * a.L, lc = (size_t)l * a.cap;
+    const uint32_t n = valid ? a.cnt[ll + cc] : 0u;
+    const uint32_t off = a.off[ll + cc];
+    const bool near = valid && fabsf(interp_center(ls, (float)x, (float)y)) < PLS_BAND;
+    const bool slow = near && n > PLS_MAX_PER_CELL;
+    uint32_t to_add = 0;
+    if (valid && !slow) {
+        uint8_t* alive = a.alive + lc + off;
+        uint32_t* prank = a.prank + lc + off;
+        for (uint32_t i = 0; i < n; ++i) {
+            alive[i] = near ? 1 : 0;
+            prank[i] = i;
         }
-        b[j] = v;
+        to_add = near ? PLS_MAX_PER_CELL - n : 0u;
+        a.val[ll + c] = near ? n : 0u;
+        a.addn[ll + c] = (uint8_t)to_add;
     }
+    const uint32_t ks = pls_aggregated_add(a.nslow + l, 0u, slow);  // every lane of the warp
+    if (slow) a.slow[ll + ks] = c;
+    const uint32_t kw = pls_aggregated_add(a.nwork + l, 0u, to_add != 0);
+    if (to_add) a.work[ll + kw] = c;
+}
 
+// The reference's heap, serially, for one listed cell (the exact fallback of
+// k_pls_select).  Returns the number of refill attempts.
+EFL_DEV uint32_t pls_heap_serial(const PlsArgs& a, int l, uint32_t c) {
+    const size_t ll = (size_t)l * a.L, lc = (size_t)l * a.cap;
+    const uint32_t n = a.cnt[ll + c];
+    const uint32_t off = a.off[ll + c];
+    uint8_t* alive = a.alive + lc + off;
+    uint32_t* prank = a.prank + lc + off;
+    const float* prio = a.prio + lc + off;
+    const uint8_t* esc = a.sesc + lc + off;
     PlsNode heap[PLS_MAX_PER_CELL];
-#pragma unroll
     for (int k = 0; k < PLS_MAX_PER_CELL; ++k) heap[k] = PlsNode{0u, 0.0f};
     uint32_t hcap = PLS_MAX_PER_CELL, hidx = 0;
-    auto kill = [&](uint32_t slot) {
-        if (slot >= off && slot - off < n) alive[slot] = 0;
+    auto kill = [&](uint32_t slot) {  // heap nodes hold global slots
+        if (slot >= off && slot - off < n) alive[slot - off] = 0;
     };
     for (uint32_t i = 0; i < n; ++i) {
-        uint32_t slot = off + i;
-        if (!near) {
-            alive[slot] = 0;
-            continue;
-        }
-        uint32_t j = b[i];
-        float r = a.rad[l][j];
-        float phi = interp_center(ls, a.px[l][j], a.py[l][j]);
-        if (sgn * phi + r < 0.0f) {  // escaped
+        const uint32_t slot = off + i;
+        const float pr = prio[i];
+        if (esc[i]) {
             if (hcap != 0) {
-                alive[slot] = 1;
+                alive[i] = 1;
                 hcap -= 1;
                 if (hidx > hcap) {
                     kill(heap[0].index);
@@ -450,131 +555,301 @@ __global__ void k_pls_reseed(PlsArgs a, PF ls, P2 grad) {
                     pls_correct_heap(heap, hcap);
                 }
             } else {
-                alive[slot] = 0;
+                alive[i] = 0;
             }
             continue;
         }
-        float prio = sgn * phi - r;
         if (hidx < hcap) {
-            alive[slot] = 1;
-            heap[hidx] = PlsNode{slot, prio};
+            alive[i] = 1;
+            heap[hidx] = PlsNode{slot, pr};
             hidx += 1;
             pls_sift_up(heap, hidx);
-        } else if (prio < heap[0].value) {
-            alive[slot] = 1;
+        } else if (pr < heap[0].value) {
+            alive[i] = 1;
             kill(heap[0].index);
-            heap[0] = PlsNode{slot, prio};
+            heap[0] = PlsNode{slot, pr};
             pls_correct_heap(heap, hcap);
         } else {
-            alive[slot] = 0;
+            alive[i] = 0;
         }
     }
-    uint32_t to_add = near ? hcap - hidx : 0u;
     uint32_t kept = 0;
-    for (uint32_t i = 0; i < n; ++i) kept += alive[off + i];
-    uint32_t fresh = 0;
-    for (uint32_t i = 0; i < to_add; ++i) {
-        float ox, oy, orad;
-        fresh += pls_attempt(false, l, x, y, i, ls, grad, a.nx, a.ny, ox, oy, orad) ? 1u : 0u;
-    }
-    a.val[(size_t)l * a.L + c] = (unsigned long long)kept | ((unsigned long long)fresh << 32);
-    a.addn[(size_t)l * a.L + c] = (uint8_t)to_add;
+    for (uint32_t i = 0; i < n; ++i)
+        if (alive[i]) prank[i] = kept++;
+    a.val[ll + c] = kept;
+    a.addn[ll + c] = (uint8_t)(hcap - hidx);
+    return hcap - hidx;
 }
 
-// initialize_particles.wgsl:17-58 with update_interface_band_mask.wgsl:7-17:
-// the number of accepted attempts per cell and layer.
-__global__ void k_pls_seed_count(PlsArgs a, PF ls, P2 grad) {
+// The heap's outcome for the listed band cells of more than 16 particles,
+// one warp per cell.  Let E be the number of escaped particles.
+//
+// E < 16: the heap of reseed_particles.wgsl keeps every escaped particle
+// and, of the others, those whose priority is among the keep = 16 - E
+// lowest, and asks for keep - min(others, keep) new ones.  Why: every step
+// keeps the MULTISET of heap values equal to the lowest min(seen, capacity)
+// values of the non-escaped seen so far (insert while not full; replace the
+// maximum by a strictly lower newcomer; an escaped arrival lowers the
+// capacity and evicts the maximum of a full heap) -- decisions depend on
+// values only -- and the capacity never reaches 0, so no zero node is ever
+// evicted.  A full heap stays full and its maximum never rises, so a value
+// below the final maximum is never evicted or rejected, and a value above it
+// never survives.  The particles are therefore determined unless equal
+// priorities straddle the cut (r_lt lower and r_eq equal others with
+// r_lt < keep <= r_lt + r_eq); then which of them the heap keeps depends on
+// its internal order.
+//
+// E >= 16: the first 16 escaped particles are kept and the capacity reaches
+// 0 at the 16th (position q); the heap is emptied then, so every other
+// particle before q is dropped, and heap[0] keeps the last node evicted --
+// the lowest of them, value v0 -- or, with none, the zero node (value 0,
+// slot 0 of the buffer).  After q, escaped particles are dropped and each
+// other particle replaces heap[0] when strictly lower (evicting the
+// previous holder), so the one kept is the first occurrence of the lowest
+// value after q, if that value is below v0; no refill.  The zero node's
+// eviction drops slot 0 of this bucket when the bucket starts the buffer.
+//
+// A NaN priority, or a straddling tie with E < 16, runs the heap itself
+// (pls_heap_serial).
+__global__ void k_pls_select(PlsArgs a) {
     const int l = blockIdx.y;
-    uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= a.L) return;
-    const int x = (int)(c % (uint32_t)a.nx), y = (int)(c / (uint32_t)a.nx);
-    uint32_t fresh = 0;
-    if (fabsf(ls.ld(x, y)) < PLS_BAND) {
-        for (uint32_t i = 0; i < PLS_MAX_PER_CELL; ++i) {
-            float ox, oy, orad;
-            fresh += pls_attempt(true, l, x, y, i, ls, grad, a.nx, a.ny, ox, oy, orad) ? 1u : 0u;
-        }
-    }
-    a.val[(size_t)l * a.L + c] = (unsigned long long)fresh << 32;
-}
-
-// The writes: kept particles of the cell's bucket (reseed), then its new
-// ones.  init: new particles are appended to the live set after count[l]
-// (initialize_particles.wgsl:44-56 appends to the existing count); reseed:
-// kept ones go to the compaction target at their rank, new ones after all
-// kept ones (delete_particles.wgsl, update_particles_count.wgsl,
-// add_particles.wgsl).
-__global__ void k_pls_emit(PlsArgs a, PF ls, P2 grad, int init) {
-    const int l = blockIdx.y;
-    uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= a.L) return;
-    const int x = (int)(c % (uint32_t)a.nx), y = (int)(c / (uint32_t)a.nx);
-    unsigned long long e = a.val[(size_t)l * a.L + c];
-    unsigned long long t = a.tot[l];
-    float* dx = init ? a.px[l] : a.qx[l];
-    float* dy = init ? a.py[l] : a.qy[l];
-    float* dr = init ? a.rad[l] : a.qrad[l];
-    uint8_t* de = init ? a.esc[l] : a.qesc[l];
-    uint64_t dst;
-    uint32_t attempts;
-    if (init) {
-        dst = (uint64_t)a.count[l] + (e >> 32);
-        attempts = fabsf(ls.ld(x, y)) < PLS_BAND ? PLS_MAX_PER_CELL : 0u;
-    } else {
-        const uint32_t n = a.cnt[(size_t)l * a.L + c];
-        const uint32_t off = a.off[(size_t)l * a.L + c];
-        const uint32_t* b = a.sidx + (size_t)l * a.cap + off;
-        const uint8_t* alive = a.alive + (size_t)l * a.cap + off;
-        uint64_t k = e & 0xffffffffull;
-        for (uint32_t i = 0; i < n; ++i) {
-            if (!alive[i]) continue;
-            uint32_t j = b[i];
-            if (k < a.cap) {
-                dx[k] = a.px[l][j];
-                dy[k] = a.py[l][j];
-                dr[k] = a.rad[l][j];
-                de[k] = a.esc[l][j];
-            } else {
-                atomicAdd(a.dropped, 1u);
+    const uint32_t ns = a.nslow[l];
+    const size_t ll = (size_t)l * a.L, lc = (size_t)l * a.cap;
+    const uint32_t lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    const uint32_t wpb = blockDim.x / 32;
+    const float inf = __int_as_float(0x7f800000);
+    for (uint32_t w = blockIdx.x * wpb + threadIdx.x / 32; w < ns; w += gridDim.x * wpb) {  // warp-uniform
+        const uint32_t c = a.slow[ll + w];
+        const uint32_t n = a.cnt[ll + c];
+        const uint32_t off = a.off[ll + c];
+        const float* prio = a.prio + lc + off;
+        const uint8_t* esc = a.sesc + lc + off;
+        uint8_t* alive = a.alive + lc + off;
+        uint32_t* prank = a.prank + lc + off;
+        // escaped count, the position q of the 16th escaped, NaN priorities
+        uint32_t nesc = 0, q = n;
+        bool nan = false;
+        for (uint32_t b = 0; b < n; b += 32) {
+            const uint32_t i = b + lane;
+            const bool e = i < n && esc[i] != 0;
+            nan |= i < n && !e && prio[i] != prio[i];
+            const unsigned me = __ballot_sync(0xffffffffu, e);
+            if (nesc < PLS_MAX_PER_CELL && nesc + __popc(me) >= PLS_MAX_PER_CELL) {
+                unsigned m = me;  // the (16 - nesc)-th set bit: drop the lowest 15 - nesc
+                for (uint32_t k = nesc + 1; k < PLS_MAX_PER_CELL; ++k) m &= m - 1;
+                q = b + (uint32_t)(__ffs(m) - 1);
             }
-            ++k;
+            nesc += (uint32_t)__popc(me);
         }
-        dst = (t & 0xffffffffull) + (e >> 32);
-        attempts = a.addn[(size_t)l * a.L + c];
-    }
-    for (uint32_t i = 0; i < attempts; ++i) {
-        float ox, oy, orad;
-        if (!pls_attempt(init != 0, l, x, y, i, ls, grad, a.nx, a.ny, ox, oy, orad)) continue;
-        if (dst < a.cap) {
-            dx[dst] = ox;
-            dy[dst] = oy;
-            dr[dst] = orad;
-            de[dst] = 0;
+        bool bad = __any_sync(0xffffffffu, nan);
+        const bool full = nesc >= PLS_MAX_PER_CELL;
+        const uint32_t keep = full ? 0u : PLS_MAX_PER_CELL - nesc;
+        // E >= 16: v0, then the first occurrence of the lowest value after q
+        float v0 = 0.0f;
+        uint32_t holder = n;
+        bool zero_kill = false;
+        if (!bad && full) {
+            float lo = inf, lo_after = inf;
+            bool before = false;
+            for (uint32_t b = 0; b < n; b += 32) {
+                const uint32_t i = b + lane;
+                if (i < n && !esc[i]) {
+                    const float p = prio[i];
+                    if (i < q) {
+                        before = true;
+                        lo = fminf(lo, p);
+                    } else {
+                        lo_after = fminf(lo_after, p);
+                    }
+                }
+            }
+            for (int o = 16; o; o >>= 1) {
+                lo = fminf(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+                lo_after = fminf(lo_after, __shfl_xor_sync(0xffffffffu, lo_after, o));
+            }
+            before = __any_sync(0xffffffffu, before);
+            v0 = before ? lo : 0.0f;
+            if (lo_after < v0) {
+                uint32_t first = n;
+                for (uint32_t b = 0; b < n; b += 32) {
+                    const uint32_t i = b + lane;
+                    if (i < n && i > q && !esc[i] && prio[i] == lo_after) first = min(first, i);
+                }
+                for (int o = 16; o; o >>= 1) first = min(first, __shfl_xor_sync(0xffffffffu, first, o));
+                holder = first;
+                zero_kill = !before && off == 0;
+            }
+        }
+        if (!bad && !full) {
+            // rank of each non-escaped particle among the non-escaped, kept in prank for now
+            bool tie = false;
+            for (uint32_t b = 0; b < n; b += 32) {
+                const uint32_t i = b + lane;
+                if (i < n && !esc[i]) {
+                    const float p = prio[i];
+                    uint32_t r = 0, eq = 0;
+                    for (uint32_t j = 0; j < n; ++j) {
+                        if (esc[j]) continue;
+                        const float qv = prio[j];
+                        r += qv < p ? 1u : 0u;
+                        eq += qv == p ? 1u : 0u;  // includes i itself
+                    }
+                    tie |= r < keep && keep <= r + eq - 1;
+                    prank[i] = r;
+                }
+            }
+            bad = __any_sync(0xffffffffu, tie);
+        }
+        uint32_t to_add;
+        if (bad) {
+            uint32_t t = 0;
+            if (lane == 0) t = pls_heap_serial(a, l, c);
+            to_add = __shfl_sync(0xffffffffu, t, 0);
         } else {
-            atomicAdd(a.dropped, 1u);
+            const uint32_t others = n - nesc;
+            uint32_t kept = 0;
+            for (uint32_t b = 0; b < n; b += 32) {
+                const uint32_t i = b + lane;
+                bool v = false;
+                if (i < n) {
+                    if (full) v = esc[i] ? (i <= q && !(zero_kill && i == 0)) : i == holder;
+                    else v = esc[i] != 0 || prank[i] < keep;
+                }
+                const unsigned m = __ballot_sync(0xffffffffu, v);
+                if (i < n) {
+                    alive[i] = v ? 1 : 0;
+                    if (v) prank[i] = kept + (uint32_t)__popc(m & lt);
+                }
+                kept += (uint32_t)__popc(m);
+            }
+            to_add = keep - (others < keep ? others : keep);
+            if (lane == 0) {
+                a.val[ll + c] = kept;
+                a.addn[ll + c] = (uint8_t)to_add;
+            }
         }
-        ++dst;
+        if (lane == 0 && to_add) a.work[ll + atomicAdd(a.nwork + l, 1u)] = c;
     }
 }
 
-// New live counts (capped at the capacity; the overflow is in a.dropped).
-__global__ void k_pls_set_count(PlsArgs a, int init) {
-    int l = threadIdx.x;
-    if (l >= 2) return;
-    unsigned long long t = a.tot[l];
-    uint64_t n = init ? (uint64_t)a.count[l] + (t >> 32) : (t & 0xffffffffull) + (t >> 32);
-    a.count[l] = (uint32_t)(n < a.cap ? n : a.cap);
+// ---------------------------------------------------------------------------
+// Seeding and refill, 16 lanes per listed cell (one lane per attempt), over
+// the work list of cells that make attempts.  Which list entry a cell has
+// does not matter: positions come from the cell-order scan of val.
+// init = 1: initialize_particles.wgsl:17-58 with update_interface_band_mask
+// (16 attempts in every cell with |levelset_air0| < 3); init = 0: the
+// reseed's add_particles.wgsl (addn[c] attempts).
+constexpr int PLS_GROUP = 16;
+
+// update_interface_band_mask.wgsl:7-17: the band cells, listed.
+__global__ void k_pls_band(PlsArgs a, PF ls) {
+    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool on = c < a.L && fabsf(ls.ld((int)(c % (uint32_t)a.nx), (int)(c / (uint32_t)a.nx))) < PLS_BAND;
+    if (c < a.L) a.val[c] = a.val[(size_t)a.L + c] = 0;  // cells without attempts add nothing
+    const uint32_t k = pls_aggregated_add(a.nwork, 0u, on);
+    if (on) a.work[k] = a.work[(size_t)a.L + k] = c;
 }
 
-// The compacted set back into the live arrays.
-__global__ void k_pls_copyback(PlsArgs a) {
+EFL_DEV bool pls_group_attempt(const PlsArgs& a, const PF& ls, const P2& grad, int init, int l, uint32_t c,
+                               uint32_t i, float& ox, float& oy, float& orad) {
+    const int x = (int)(c % (uint32_t)a.nx), y = (int)(c / (uint32_t)a.nx);
+    const uint32_t attempts = init ? PLS_MAX_PER_CELL : (uint32_t)a.addn[(size_t)l * a.L + c];
+    if (i >= attempts) return false;
+    return pls_attempt(init != 0, l, x, y, i, ls, grad, a.nx, a.ny, ox, oy, orad);
+}
+
+// Accepted attempts per listed cell: vmask (bit i = attempt i) and val's
+// high half (val's low half = kept particles, from k_pls_heap; 0 at init).
+__global__ void k_pls_spawn_count(PlsArgs a, PF ls, P2 grad, int init) {
     const int l = blockIdx.y;
-    uint32_t n = a.count[l];
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        a.px[l][i] = a.qx[l][i];
-        a.py[l][i] = a.qy[l][i];
-        a.rad[l][i] = a.qrad[l][i];
-        a.esc[l][i] = a.qesc[l][i];
+    const uint32_t nw = init ? a.nwork[0] : a.nwork[l];
+    const uint32_t* work = a.work + (size_t)l * a.L;
+    const uint32_t i = threadIdx.x % PLS_GROUP;
+    const uint32_t per = blockDim.x / PLS_GROUP;
+    for (uint32_t w0 = blockIdx.x * per; w0 < nw; w0 += gridDim.x * per) {  // block-uniform
+        const uint32_t w = w0 + threadIdx.x / PLS_GROUP;
+        const bool on = w < nw;
+        const uint32_t c = on ? work[w] : 0u;
+        float ox, oy, orad;
+        const bool ok = on && pls_group_attempt(a, ls, grad, init, l, c, i, ox, oy, orad);
+        const uint32_t m = (__ballot_sync(0xffffffffu, ok) >> (threadIdx.x & 16)) & 0xffffu;
+        if (on && i == 0) {
+            const size_t k = (size_t)l * a.L + c;
+            a.vmask[k] = (uint16_t)m;
+            a.val[k] = (a.val[k] & 0xffffffffull) | ((unsigned long long)__popc(m) << 32);
+        }
+    }
+}
+
+// The writes of a seeding or a reseed, one launch: blocks [0, kb) move the
+// kept particles (reseed only; delete_particles.wgsl:12-17) to the spare
+// buffer at (kept before this cell) + (rank in the cell's bucket); the
+// other blocks write the accepted attempts of the listed cells, 16 lanes per
+// cell -- init appends them to the live buffer after count[l]
+// (initialize_particles.wgsl:44-56 appends to the existing count), a reseed
+// writes them after all kept particles (update_particles_count.wgsl,
+// add_particles.wgsl:36-45).  The last block to finish sets the new counts
+// (capped at the capacity; the overflow is in a.dropped) and, after a
+// reseed, makes the compacted buffer live.
+__global__ void k_pls_emit(PlsArgs a, PF ls, P2 grad, int init, uint32_t kb) {
+    const int l = blockIdx.y;
+    if (!init && blockIdx.x < kb) {
+        const uint32_t n = a.count[l];
+        const PView S = pls_live(a, l), D = pls_spare(a, l);
+        const size_t lc = (size_t)l * a.cap, ll = (size_t)l * a.L;
+        for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += kb * blockDim.x) {
+            if (!a.alive[lc + s]) continue;
+            const uint32_t dst = (uint32_t)(a.val[ll + a.scell[lc + s]] & 0xffffffffull) + a.prank[lc + s];
+            const uint32_t j = a.sorted[lc + s];
+            D.x[dst] = S.x[j];
+            D.y[dst] = S.y[j];
+            D.r[dst] = S.r[j];
+            D.e[dst] = S.e[j];
+        }
+    } else {
+        const uint32_t nb = gridDim.x - (init ? 0u : kb), b0 = blockIdx.x - (init ? 0u : kb);
+        const uint32_t nw = init ? a.nwork[0] : a.nwork[l];
+        const uint32_t* work = a.work + (size_t)l * a.L;
+        const uint32_t i = threadIdx.x % PLS_GROUP;
+        const uint32_t per = blockDim.x / PLS_GROUP;
+        const uint64_t base = init ? (uint64_t)a.count[l] : (a.tot[l] & 0xffffffffull);
+        const PView D = init ? pls_live(a, l) : pls_spare(a, l);
+        for (uint32_t w = b0 * per + threadIdx.x / PLS_GROUP; w < nw; w += nb * per) {
+            const uint32_t c = work[w];
+            const size_t k = (size_t)l * a.L + c;
+            const uint32_t m = a.vmask[k];
+            if (!((m >> i) & 1u)) continue;
+            float ox, oy, orad;
+            pls_group_attempt(a, ls, grad, init, l, c, i, ox, oy, orad);
+            const uint64_t dst = base + (a.val[k] >> 32) + (uint64_t)__popc(m & ((1u << i) - 1u));
+            if (dst >= a.cap) {
+                atomicAdd(a.dropped, 1u);
+                continue;
+            }
+            D.x[dst] = ox;
+            D.y[dst] = oy;
+            D.r[dst] = orad;
+            D.e[dst] = 0;
+        }
+    }
+    // last block of the launch: counts and the live buffer
+    __shared__ bool s_last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const uint32_t ticket = atomicAdd(a.ticket, 1u);
+        s_last = ticket == gridDim.x * gridDim.y - 1;
+    }
+    __syncthreads();
+    if (s_last && threadIdx.x < 2) {
+        __threadfence();
+        const int m = threadIdx.x;
+        const unsigned long long t = a.tot[m];
+        const uint64_t nn = init ? (uint64_t)a.count[m] + (t >> 32) : (t & 0xffffffffull) + (t >> 32);
+        a.count[m] = (uint32_t)(nn < a.cap ? nn : a.cap);
+        if (!init) a.sel[m] = 1 - a.sel[m];
+        if (m == 0) *a.ticket = 0;
     }
 }
 

@@ -346,29 +346,39 @@ efl_status pls_alloc(efl_sim* s) {
     a.ny = s->ny;
     a.L = (uint32_t)s->nx * (uint32_t)s->ny;
     a.cap = a.L * PLS_MAX_PER_CELL;  // plugin.rs:212-215
-    for (int l = 0; l < 2; ++l) {
-        TRY(alloc_raw(s, a.px[l], a.cap));
-        TRY(alloc_raw(s, a.py[l], a.cap));
-        TRY(alloc_raw(s, a.rad[l], a.cap));
-        TRY(alloc_raw(s, a.esc[l], a.cap));
-        TRY(alloc_raw(s, a.qx[l], a.cap));
-        TRY(alloc_raw(s, a.qy[l], a.cap));
-        TRY(alloc_raw(s, a.qrad[l], a.cap));
-        TRY(alloc_raw(s, a.qesc[l], a.cap));
-    }
+    for (int l = 0; l < 2; ++l)
+        for (int b = 0; b < 2; ++b) {
+            TRY(alloc_raw(s, a.px[l][b], a.cap));
+            TRY(alloc_raw(s, a.py[l][b], a.cap));
+            TRY(alloc_raw(s, a.rad[l][b], a.cap));
+            TRY(alloc_raw(s, a.esc[l][b], a.cap));
+        }
+    const size_t L2 = 2 * (size_t)a.L, C2 = 2 * (size_t)a.cap;
+    TRY(alloc_raw(s, a.sel, 2));
     TRY(alloc_raw(s, a.count, 2));
-    TRY(alloc_raw(s, a.cnt, 2 * (size_t)a.L));
-    TRY(alloc_raw(s, a.cur, 2 * (size_t)a.L));
-    TRY(alloc_raw(s, a.off, 2 * (size_t)a.L));
-    TRY(alloc_raw(s, a.sidx, 2 * (size_t)a.cap));
-    TRY(alloc_raw(s, a.alive, 2 * (size_t)a.cap));
-    TRY(alloc_raw(s, a.val, 2 * (size_t)a.L));
+    TRY(alloc_raw(s, a.cnt, L2));
+    TRY(alloc_raw(s, a.cur, L2));
+    TRY(alloc_raw(s, a.off, L2));
+    TRY(alloc_raw(s, a.sidx, C2));
+    TRY(alloc_raw(s, a.scell, C2));
+    TRY(alloc_raw(s, a.sorted, C2));
+    TRY(alloc_raw(s, a.prio, C2));
+    TRY(alloc_raw(s, a.sesc, C2));
+    TRY(alloc_raw(s, a.alive, C2));
+    TRY(alloc_raw(s, a.prank, C2));
+    TRY(alloc_raw(s, a.val, L2));
     TRY(alloc_raw(s, a.tot, 2));
     TRY(alloc_raw(s, a.ctot, 2));
-    TRY(alloc_raw(s, a.addn, 2 * (size_t)a.L));
+    TRY(alloc_raw(s, a.addn, L2));
+    TRY(alloc_raw(s, a.vmask, L2));
+    TRY(alloc_raw(s, a.work, L2));
+    TRY(alloc_raw(s, a.nwork, 2));
+    TRY(alloc_raw(s, a.slow, L2));
+    TRY(alloc_raw(s, a.nslow, 2));
     TRY(alloc_raw(s, a.phip, (size_t)a.L));
     TRY(alloc_raw(s, a.phim, (size_t)a.L));
     TRY(alloc_raw(s, a.dropped, 1));
+    TRY(alloc_raw(s, a.ticket, 1));
     P.nb = (a.L + SC_N - 1) / SC_N;
     TRY(alloc_raw(s, P.part32, 2 * (size_t)P.nb));
     TRY(alloc_raw(s, P.part64, 2 * (size_t)P.nb));
@@ -383,6 +393,10 @@ dim3 pls_pgrid(const PlsArgs& a) {
     return dim3((unsigned)std::min<uint32_t>((a.cap + PLS_THREADS - 1) / PLS_THREADS, 148u * 8u), 2);
 }
 dim3 pls_cgrid(const PlsArgs& a, int layers) { return dim3((a.L + PLS_THREADS - 1) / PLS_THREADS, layers); }
+// Grid-stride launches over the work list, 16 lanes per listed cell.
+dim3 pls_ggrid(const PlsArgs& a) {
+    return dim3((unsigned)std::min<size_t>(((size_t)a.L * PLS_GROUP + PLS_THREADS - 1) / PLS_THREADS, 148u * 8u), 2);
+}
 
 // Exclusive scan of each layer's L values (common_pass/prefix_sum.rs).
 template <class Tin, class T>
@@ -400,10 +414,12 @@ efl_status pls_scan(efl_sim* s, const Tin* in, T* out, T* part, T* tot) {
 // levelset_air0 and its gradient.
 efl_status pls_initialize(efl_sim* s) {
     PlsArgs& a = s->pls.a;
-    k_pls_seed_count<<<pls_cgrid(a, 2), PLS_THREADS, count_launch(), s->stream>>>(a, s->ls0, s->grad);
+    CU(cudaMemsetAsync(a.nwork, 0, 2 * sizeof(uint32_t), s->stream));
+    k_pls_band<<<pls_cgrid(a, 1), PLS_THREADS, count_launch(), s->stream>>>(a, s->ls0);
+    k_pls_spawn_count<<<pls_ggrid(a), PLS_THREADS, count_launch(), s->stream>>>(a, s->ls0, s->grad, 1);
+    LAUNCH_CHECK();
     TRY(pls_scan(s, a.val, a.val, s->pls.part64, a.tot));
-    k_pls_emit<<<pls_cgrid(a, 2), PLS_THREADS, count_launch(), s->stream>>>(a, s->ls0, s->grad, 1);
-    k_pls_set_count<<<1, 32, count_launch(), s->stream>>>(a, 1);
+    k_pls_emit<<<pls_ggrid(a), PLS_THREADS, count_launch(), s->stream>>>(a, s->ls0, s->grad, 1, 0u);
     LAUNCH_CHECK();
     return EFL_OK;
 }
@@ -417,32 +433,38 @@ efl_status pls_advect(efl_sim* s, float dt) {
 }
 
 // levelset_correction.rs:96-155 (dispatch, on levelset_air1) and :157-236
-// (dispatch_second, on levelset_air0, then the particle radii).
-efl_status pls_correct(efl_sim* s, PF ls, bool second) {
+// (dispatch_second, on levelset_air0, then the particle radii unless the
+// reseed that follows does them with its binning pass).
+efl_status pls_correct(efl_sim* s, PF ls, bool second, bool radii = true) {
     PlsArgs& a = s->pls.a;
     k_pls_reset<<<pls_cgrid(a, 1), PLS_THREADS, count_launch(), s->stream>>>(a, ls);
     k_pls_mark_accumulate<<<pls_pgrid(a), PLS_THREADS, count_launch(), s->stream>>>(a, ls);
     k_pls_correct<<<pls_cgrid(a, 1), PLS_THREADS, count_launch(), s->stream>>>(a, ls);
-    if (second) k_pls_radii<<<pls_pgrid(a), PLS_THREADS, count_launch(), s->stream>>>(a, ls);
+    if (second && radii) k_pls_radii<<<pls_pgrid(a), PLS_THREADS, count_launch(), s->stream>>>(a, ls);
     LAUNCH_CHECK();
     return EFL_OK;
 }
 
 // reseed.rs:130-296: bin, counting sort, per-cell heap, compaction, refill.
-efl_status pls_reseed(efl_sim* s) {
+// radii: the binning pass first does update_particle_radii on levelset_air0.
+efl_status pls_reseed(efl_sim* s, bool radii = false) {
     PlsArgs& a = s->pls.a;
     CU(cudaMemsetAsync(a.cnt, 0, 2 * (size_t)a.L * sizeof(uint32_t), s->stream));
     CU(cudaMemsetAsync(a.cur, 0, 2 * (size_t)a.L * sizeof(uint32_t), s->stream));
-    k_pls_bin<<<pls_pgrid(a), PLS_THREADS, count_launch(), s->stream>>>(a);
+    CU(cudaMemsetAsync(a.nwork, 0, 2 * sizeof(uint32_t), s->stream));
+    CU(cudaMemsetAsync(a.nslow, 0, 2 * sizeof(uint32_t), s->stream));
+    k_pls_bin<<<pls_pgrid(a), PLS_THREADS, count_launch(), s->stream>>>(a, s->ls0, radii ? 1 : 0);
     LAUNCH_CHECK();
     TRY(pls_scan(s, a.cnt, a.off, s->pls.part32, a.ctot));
     k_pls_scatter<<<pls_pgrid(a), PLS_THREADS, count_launch(), s->stream>>>(a);
-    k_pls_reseed<<<pls_cgrid(a, 2), PLS_THREADS, count_launch(), s->stream>>>(a, s->ls0, s->grad);
+    k_pls_rank<<<pls_pgrid(a), PLS_THREADS, count_launch(), s->stream>>>(a, s->ls0);
+    k_pls_heap<<<pls_cgrid(a, 2), PLS_THREADS, count_launch(), s->stream>>>(a, s->ls0);
+    k_pls_select<<<dim3(std::min<uint32_t>((a.L + 7) / 8, 148u * 16u), 2), PLS_THREADS, count_launch(), s->stream>>>(a);
+    k_pls_spawn_count<<<pls_ggrid(a), PLS_THREADS, count_launch(), s->stream>>>(a, s->ls0, s->grad, 0);
     LAUNCH_CHECK();
     TRY(pls_scan(s, a.val, a.val, s->pls.part64, a.tot));
-    k_pls_emit<<<pls_cgrid(a, 2), PLS_THREADS, count_launch(), s->stream>>>(a, s->ls0, s->grad, 0);
-    k_pls_set_count<<<1, 32, count_launch(), s->stream>>>(a, 0);
-    k_pls_copyback<<<pls_pgrid(a), PLS_THREADS, count_launch(), s->stream>>>(a);
+    const uint32_t kb = pls_pgrid(a).x;
+    k_pls_emit<<<dim3(kb + pls_ggrid(a).x, 2), PLS_THREADS, count_launch(), s->stream>>>(a, s->ls0, s->grad, 0, kb);
     LAUNCH_CHECK();
     return EFL_OK;
 }
@@ -1048,8 +1070,8 @@ efl_status run_stage(efl_sim* s, int stage, efl_step_stats* st) {
         case EFL_STAGE_REINITIALIZE:  // + render_node.rs:421-441 (second correction, reseed)
             TRY(st_reinit(s));
             if (s->pls.on) {
-                TRY(pls_correct(s, s->ls0, true));
-                TRY(pls_reseed(s));
+                TRY(pls_correct(s, s->ls0, true, false));
+                TRY(pls_reseed(s, true));
             }
             return EFL_OK;
         case EFL_STAGE_LEVELSET_GRADIENT: return st_gradient(s);
@@ -1641,12 +1663,15 @@ efl_status efl_read_particles(efl_sim* s, int32_t layer, efl_particle* dst, uint
     const uint32_t m = std::min(counts[layer], capacity);
     if (!m) return EFL_OK;
     const PlsArgs& a = s->pls.a;
+    int b = 0;
+    CU(cudaMemcpyAsync(&b, a.sel + layer, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+    CU(cudaStreamSynchronize(s->stream));
     std::vector<float> x(m), y(m), r(m);
     std::vector<uint8_t> e(m);
-    CU(cudaMemcpyAsync(x.data(), a.px[layer], m * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
-    CU(cudaMemcpyAsync(y.data(), a.py[layer], m * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
-    CU(cudaMemcpyAsync(r.data(), a.rad[layer], m * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
-    CU(cudaMemcpyAsync(e.data(), a.esc[layer], m, cudaMemcpyDeviceToHost, s->stream));
+    CU(cudaMemcpyAsync(x.data(), a.px[layer][b], m * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
+    CU(cudaMemcpyAsync(y.data(), a.py[layer][b], m * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
+    CU(cudaMemcpyAsync(r.data(), a.rad[layer][b], m * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
+    CU(cudaMemcpyAsync(e.data(), a.esc[layer][b], m, cudaMemcpyDeviceToHost, s->stream));
     CU(cudaStreamSynchronize(s->stream));
     const float sgn = layer == EFL_PLS_POSITIVE ? 1.0f : -1.0f;
     for (uint32_t i = 0; i < m; ++i) {
@@ -1679,12 +1704,14 @@ efl_status efl_write_particles(efl_sim* s, int32_t layer, const efl_particle* sr
         e[i] = src[i].escaped ? 1 : 0;
     }
     cudaSetDevice(s->device);
-    if (n) {
-        CU(cudaMemcpyAsync(a.px[layer], x.data(), n * sizeof(float), cudaMemcpyHostToDevice, s->stream));
-        CU(cudaMemcpyAsync(a.py[layer], y.data(), n * sizeof(float), cudaMemcpyHostToDevice, s->stream));
-        CU(cudaMemcpyAsync(a.rad[layer], r.data(), n * sizeof(float), cudaMemcpyHostToDevice, s->stream));
-        CU(cudaMemcpyAsync(a.esc[layer], e.data(), n, cudaMemcpyHostToDevice, s->stream));
+    if (n) {  // into buffer 0, which becomes the live one
+        CU(cudaMemcpyAsync(a.px[layer][0], x.data(), n * sizeof(float), cudaMemcpyHostToDevice, s->stream));
+        CU(cudaMemcpyAsync(a.py[layer][0], y.data(), n * sizeof(float), cudaMemcpyHostToDevice, s->stream));
+        CU(cudaMemcpyAsync(a.rad[layer][0], r.data(), n * sizeof(float), cudaMemcpyHostToDevice, s->stream));
+        CU(cudaMemcpyAsync(a.esc[layer][0], e.data(), n, cudaMemcpyHostToDevice, s->stream));
     }
+    const int zero = 0;
+    CU(cudaMemcpyAsync(a.sel + layer, &zero, sizeof(int), cudaMemcpyHostToDevice, s->stream));
     CU(cudaMemcpyAsync(a.count + layer, &n, sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
     CU(cudaStreamSynchronize(s->stream));
     return EFL_OK;

@@ -245,7 +245,7 @@ __global__ void __launch_bounds__(WG_THREADS) k_wgrad_tc(WgradArgs a) {
     const uint32_t tmem = s_tmem;
     const uint32_t idesc = umma_idesc_bf16(128, a.cout);
     const uint32_t sbo = (WG_K / 8) * 128;
-    const int cg = a.cin >> 3, og = a.cout >> 3;
+    const int og = a.cout >> 3;
     const int pbeg = chunk * a.pix_per_cta, pend = min(npix, pbeg + a.pix_per_cta);
     bool ok = true;
     int stage = 0;

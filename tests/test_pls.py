@@ -504,3 +504,144 @@ def test_gpu_pls_graph_replay_matches_eager(gpu_api):
         s.close()
     for a, b in zip(runs[0], runs[1]):
         assert np.array_equal(a, b)
+
+
+def _edge_bucket_scene(n=32):
+    """Band everywhere; columns alternate phi = -2 / +2, so inside a cell
+    phi = 4 fx - 2 (even x): fx < ~0.45 escapes (positive layer), and the
+    priority phi - r is set by fx.  Buckets: (0, 0) 17 escaped then
+    non-escaped ones of negative priority (capacity 0, zero-node eviction in
+    the bucket at slot 0); (4, 2) 40 particles with duplicated pairs (tied
+    priorities); (6, 3) 20 escaped mixed with 12 others; (10, 5) 30 distinct."""
+    ls = np.where(np.arange(n)[None, :] % 2 == 0, -2.0, 2.0).astype(np.float32) * np.ones((n, 1), np.float32)
+    grad = np.zeros((n, n, 2), np.float32)
+    rng = np.random.default_rng(17)
+    rows = []
+    for _ in range(17):
+        rows.append((f32(0 + rng.uniform(0.0, 0.3)), f32(0 + rng.uniform(0.05, 0.95)), f32(0.1)))
+    for fx in (0.5, 0.52, 0.49, 0.51):
+        rows.append((f32(0 + fx), f32(0.5), f32(0.1)))
+    dup = []
+    for _ in range(20):
+        x, y, r = f32(4 + rng.uniform(0.6, 0.99)), f32(2 + rng.uniform(0.05, 0.95)), f32(rng.choice([0.1, 0.5]))
+        dup += [(x, y, r), (x, y, r)]
+    rows += dup
+    mix = [(f32(6 + rng.uniform(0.0, 0.3)), f32(3 + rng.uniform(0.05, 0.95)), f32(0.1)) for _ in range(20)]
+    mix += [(f32(6 + rng.uniform(0.6, 0.99)), f32(3 + rng.uniform(0.05, 0.95)), f32(0.3)) for _ in range(12)]
+    rng.shuffle(mix)
+    rows += mix
+    rows += [(f32(10 + rng.uniform(0.0, 0.99)), f32(5 + rng.uniform(0.05, 0.95)), f32(rng.choice([0.1, 0.3, 0.5])))
+             for _ in range(30)]
+    return ls, grad, rows
+
+
+def _expected_reseed(ls, rows, n):
+    cells = sorted({(int(r[0]), int(r[1])) for r in rows}, key=lambda c: c[0] + n * c[1])
+    expect, base = [], 0
+    for cx, cy in cells:
+        idx = [i for i, r in enumerate(rows) if int(r[0]) == cx and int(r[1]) == cy]
+        pr, es = [], []
+        for i in idx:
+            x, y, r = rows[i]
+            phi = interp(ls, x, y)
+            es.append(bool(phi + r < f32(0)))
+            pr.append(f32(phi - r))
+        alive, _ = heap_reference(pr, es, True, base)
+        expect += [rows[i] for i, a in zip(idx, alive) if a]
+        base += len(idx)
+    return expect
+
+
+def test_oracle_reseed_edge_buckets(oracle_api):
+    n = 32
+    ls, grad, rows = _edge_bucket_scene(n)
+    sim = fresh(oracle_api, n, ls, grad)
+    sim.write_particles(0, particles_array(rows, 1.0))
+    sim.pls_run_phase(capi.PLS_RESEED)
+    got = sim.read_particles(0)
+    expect = _expected_reseed(ls, rows, n)
+    assert len(got) == len(expect)
+    assert np.array_equal(got["position"], np.array([(e[0], e[1]) for e in expect], np.float32))
+    # the first bucket: 16 escaped kept (capacity 0), the 17th dropped; the first non-escaped one of
+    # negative priority evicts the zero node, i.e. slot 0 of the buffer = this bucket's first particle;
+    # later ones replace it only when lower (fx 0.49) -> 15 escaped + 1 other
+    first = [e for e in expect if int(e[0]) == 0 and int(e[1]) == 0]
+    assert len(first) == 16 and (rows[0][0], rows[0][1]) not in [(e[0], e[1]) for e in first]
+    assert [e[0] for e in first if e[0] > f32(0.45)] == [f32(0.49)]
+    sim.close()
+
+
+@pytest.mark.gpu
+def test_gpu_pls_reseed_edge_buckets(oracle_api, gpu_api):
+    n = 32
+    ls, grad, rows = _edge_bucket_scene(n)
+    neg = [(x, y, r) for x, y, r in rows]
+    pair = []
+    for api in (oracle_api, gpu_api):
+        s = fresh(api, n, -ls, grad)  # negative layer: the same buckets mirrored in phi
+        s.write_particles(1, particles_array(neg, -1.0))
+        s.set(capi.FIELD_LEVELSET_AIR, ls)
+        s.write_particles(0, particles_array(rows, 1.0))
+        pair.append(s)
+    for s in pair:
+        s.pls_run_phase(capi.PLS_RESEED)
+    _compare_particles(*pair)
+    assert pair[1].particle_counts()[0][0] > 0
+    for s in pair:
+        s.close()
+
+
+def _random_buckets(seed, n=64, cells=48):
+    """Band everywhere (alternating phi = -2 / +2 columns); `cells` buckets of
+    17..90 particles with escaped fractions from 0 to 90 % and duplicated
+    particles (tied priorities), in random index order."""
+    rng = np.random.default_rng(seed)
+    ls = np.where(np.arange(n)[None, :] % 2 == 0, -2.0, 2.0).astype(np.float32) * np.ones((n, 1), np.float32)
+    rows = []
+    picks = rng.choice(n * n // 2, size=cells, replace=False)
+    for k in picks:
+        cx, cy = 2 * (int(k) % (n // 2)), int(k) // (n // 2)
+        m = int(rng.integers(17, 91))
+        frac = rng.choice([0.0, 0.1, 0.3, 0.6, 0.9])
+        for _ in range(m):
+            fx = rng.uniform(0.0, 0.4) if rng.random() < frac else rng.uniform(0.46, 0.99)
+            r = f32(rng.choice([0.1, 0.2, 0.5]))
+            p = (f32(cx + fx), f32(cy + rng.uniform(0.02, 0.98)), r)
+            rows.append(p)
+            if rng.random() < 0.15:
+                rows.append(p)
+    order = rng.permutation(len(rows))
+    return ls, [rows[i] for i in order]
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_oracle_reseed_random_buckets(oracle_api, seed):
+    n = 64
+    ls, rows = _random_buckets(seed, n)
+    sim = fresh(oracle_api, n, ls, np.zeros((n, n, 2), np.float32))
+    sim.write_particles(0, particles_array(rows, 1.0))
+    sim.pls_run_phase(capi.PLS_RESEED)
+    got = sim.read_particles(0)
+    expect = _expected_reseed(ls, rows, n)
+    assert len(got) == len(expect)
+    assert np.array_equal(got["position"], np.array([(e[0], e[1]) for e in expect], np.float32))
+    sim.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("seed", [1, 2, 3, 4, 5, 6])
+def test_gpu_pls_reseed_random_buckets(oracle_api, gpu_api, seed):
+    n = 64
+    ls, rows = _random_buckets(seed, n)
+    grad = np.zeros((n, n, 2), np.float32)
+    grad[..., 0] = 1.0  # refill attempts move along x
+    pair = []
+    for api in (oracle_api, gpu_api):
+        s = fresh(api, n, ls, grad)
+        s.write_particles(0, particles_array(rows, 1.0))
+        s.write_particles(1, particles_array(rows, -1.0))
+        s.pls_run_phase(capi.PLS_RESEED)
+        pair.append(s)
+    _compare_particles(*pair)
+    for s in pair:
+        s.close()
