@@ -53,6 +53,9 @@ struct PlsArgs {
     uint32_t* ctot;           // [2] totals of cnt
     uint8_t* addn;            // [2][L] refill attempts per cell
     uint16_t* vmask;          // [2][L] accepted refill attempts per cell (bit i = attempt i)
+    float* stx;               // [2][L*16] accepted attempt i of cell c at c*16 + i (staged)
+    float* sty;
+    float* str;
     uint32_t* work;           // [2][L] cells with attempts to make (any order)
     uint32_t* nwork;          // [2] length of work
     uint32_t* slow;           // [2][L] band cells of more than 16 particles (any order)
@@ -418,8 +421,9 @@ __global__ void k_pls_scatter(PlsArgs a) {
 // The stable order: each slot's rank among its bucket's particle indices
 // (distinct), so bucket order = particle-index order.  For buckets of more
 // than 16 particles the heap inputs of reseed_particles.wgsl are staged here
-// in sorted order: priority sign * phi(x) - r (eval_priority, :101-103) and
-// the escaped test (particle.wgsl:19-30), on levelset_air0.
+// in sorted order: priority sign * phi(x) - r (eval_priority, :101-103;
+// +inf for escaped particles, whose priority the heap never reads) and the
+// escaped test (particle.wgsl:19-30), on levelset_air0.
 __global__ void k_pls_rank(PlsArgs a, PF ls) {
     const int l = blockIdx.y;
     const uint32_t n = a.count[l];
@@ -438,8 +442,10 @@ __global__ void k_pls_rank(PlsArgs a, PF ls) {
         if (m > PLS_MAX_PER_CELL) {
             const float rad = P.r[v];
             const float phi = interp_center(ls, P.x[v], P.y[v]);
-            a.prio[d] = sgn * phi - rad;
-            a.sesc[d] = sgn * phi + rad < 0.0f ? 1 : 0;
+            const bool e = sgn * phi + rad < 0.0f;
+            // escaped: +inf, so that k_pls_select ranks the others without a branch
+            a.prio[d] = e ? __int_as_float(0x7f800000) : sgn * phi - rad;
+            a.sesc[d] = e ? 1 : 0;
         }
     }
 }
@@ -609,8 +615,8 @@ EFL_DEV uint32_t pls_heap_serial(const PlsArgs& a, int l, uint32_t c) {
 // value after q, if that value is below v0; no refill.  The zero node's
 // eviction drops slot 0 of this bucket when the bucket starts the buffer.
 //
-// A NaN priority, or a straddling tie with E < 16, runs the heap itself
-// (pls_heap_serial).
+// A NaN or infinite priority, or a straddling tie with E < 16, runs the heap
+// itself (pls_heap_serial).
 __global__ void k_pls_select(PlsArgs a) {
     const int l = blockIdx.y;
     const uint32_t ns = a.nslow[l];
@@ -633,7 +639,7 @@ __global__ void k_pls_select(PlsArgs a) {
         for (uint32_t b = 0; b < n; b += 32) {
             const uint32_t i = b + lane;
             const bool e = i < n && esc[i] != 0;
-            nan |= i < n && !e && prio[i] != prio[i];
+            nan |= i < n && !e && !(prio[i] < inf);  // NaN or +inf (+inf marks escaped ones)
             const unsigned me = __ballot_sync(0xffffffffu, e);
             if (nesc < PLS_MAX_PER_CELL && nesc + __popc(me) >= PLS_MAX_PER_CELL) {
                 unsigned m = me;  // the (16 - nesc)-th set bit: drop the lowest 15 - nesc
@@ -687,10 +693,13 @@ __global__ void k_pls_select(PlsArgs a) {
             for (uint32_t b = 0; b < n; b += 32) {
                 const uint32_t i = b + lane;
                 if (i < n && !esc[i]) {
+                    // escaped particles are staged as +inf: never lower, never
+                    // equal (a finite p; a NaN p has already sent the bucket
+                    // to the serial heap)
                     const float p = prio[i];
                     uint32_t r = 0, eq = 0;
+#pragma unroll 8
                     for (uint32_t j = 0; j < n; ++j) {
-                        if (esc[j]) continue;
                         const float qv = prio[j];
                         r += qv < p ? 1u : 0u;
                         eq += qv == p ? 1u : 0u;  // includes i itself
@@ -759,8 +768,9 @@ EFL_DEV bool pls_group_attempt(const PlsArgs& a, const PF& ls, const P2& grad, i
     return pls_attempt(init != 0, l, x, y, i, ls, grad, a.nx, a.ny, ox, oy, orad);
 }
 
-// Accepted attempts per listed cell: vmask (bit i = attempt i) and val's
-// high half (val's low half = kept particles, from k_pls_heap; 0 at init).
+// Accepted attempts per listed cell: vmask (bit i = attempt i), val's high
+// half (val's low half = kept particles, from k_pls_heap; 0 at init), and
+// the particles themselves, staged for k_pls_emit.
 __global__ void k_pls_spawn_count(PlsArgs a, PF ls, P2 grad, int init) {
     const int l = blockIdx.y;
     const uint32_t nw = init ? a.nwork[0] : a.nwork[l];
@@ -773,6 +783,12 @@ __global__ void k_pls_spawn_count(PlsArgs a, PF ls, P2 grad, int init) {
         const uint32_t c = on ? work[w] : 0u;
         float ox, oy, orad;
         const bool ok = on && pls_group_attempt(a, ls, grad, init, l, c, i, ox, oy, orad);
+        if (ok) {
+            const size_t t = ((size_t)l * a.L + c) * PLS_GROUP + i;
+            a.stx[t] = ox;
+            a.sty[t] = oy;
+            a.str[t] = orad;
+        }
         const uint32_t m = (__ballot_sync(0xffffffffu, ok) >> (threadIdx.x & 16)) & 0xffffu;
         if (on && i == 0) {
             const size_t k = (size_t)l * a.L + c;
@@ -785,8 +801,8 @@ __global__ void k_pls_spawn_count(PlsArgs a, PF ls, P2 grad, int init) {
 // The writes of a seeding or a reseed, one launch: blocks [0, kb) move the
 // kept particles (reseed only; delete_particles.wgsl:12-17) to the spare
 // buffer at (kept before this cell) + (rank in the cell's bucket); the
-// other blocks write the accepted attempts of the listed cells, 16 lanes per
-// cell -- init appends them to the live buffer after count[l]
+// other blocks write the accepted attempts of the listed cells (staged by
+// k_pls_spawn_count), 16 lanes per cell -- init appends them to the live buffer after count[l]
 // (initialize_particles.wgsl:44-56 appends to the existing count), a reseed
 // writes them after all kept particles (update_particles_count.wgsl,
 // add_particles.wgsl:36-45).  The last block to finish sets the new counts
@@ -799,13 +815,17 @@ __global__ void k_pls_emit(PlsArgs a, PF ls, P2 grad, int init, uint32_t kb) {
         const PView S = pls_live(a, l), D = pls_spare(a, l);
         const size_t lc = (size_t)l * a.cap, ll = (size_t)l * a.L;
         for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += kb * blockDim.x) {
-            if (!a.alive[lc + s]) continue;
-            const uint32_t dst = (uint32_t)(a.val[ll + a.scell[lc + s]] & 0xffffffffull) + a.prank[lc + s];
-            const uint32_t j = a.sorted[lc + s];
-            D.x[dst] = S.x[j];
-            D.y[dst] = S.y[j];
-            D.r[dst] = S.r[j];
-            D.e[dst] = S.e[j];
+            // independent loads first, one dependent round for val and the particle
+            const bool keep = a.alive[lc + s] != 0;
+            const uint32_t c = a.scell[lc + s], r = a.prank[lc + s], j = a.sorted[lc + s];
+            if (!keep) continue;
+            const uint32_t dst = (uint32_t)(a.val[ll + c] & 0xffffffffull) + r;
+            const float x = S.x[j], y = S.y[j], rad = S.r[j];
+            const uint8_t e = S.e[j];
+            D.x[dst] = x;
+            D.y[dst] = y;
+            D.r[dst] = rad;
+            D.e[dst] = e;
         }
     } else {
         const uint32_t nb = gridDim.x - (init ? 0u : kb), b0 = blockIdx.x - (init ? 0u : kb);
@@ -820,8 +840,8 @@ __global__ void k_pls_emit(PlsArgs a, PF ls, P2 grad, int init, uint32_t kb) {
             const size_t k = (size_t)l * a.L + c;
             const uint32_t m = a.vmask[k];
             if (!((m >> i) & 1u)) continue;
-            float ox, oy, orad;
-            pls_group_attempt(a, ls, grad, init, l, c, i, ox, oy, orad);
+            const size_t t = k * PLS_GROUP + i;
+            const float ox = a.stx[t], oy = a.sty[t], orad = a.str[t];
             const uint64_t dst = base + (a.val[k] >> 32) + (uint64_t)__popc(m & ((1u << i) - 1u));
             if (dst >= a.cap) {
                 atomicAdd(a.dropped, 1u);

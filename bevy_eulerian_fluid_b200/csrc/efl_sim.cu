@@ -371,6 +371,9 @@ efl_status pls_alloc(efl_sim* s) {
     TRY(alloc_raw(s, a.ctot, 2));
     TRY(alloc_raw(s, a.addn, L2));
     TRY(alloc_raw(s, a.vmask, L2));
+    TRY(alloc_raw(s, a.stx, L2 * PLS_GROUP));
+    TRY(alloc_raw(s, a.sty, L2 * PLS_GROUP));
+    TRY(alloc_raw(s, a.str, L2 * PLS_GROUP));
     TRY(alloc_raw(s, a.work, L2));
     TRY(alloc_raw(s, a.nwork, 2));
     TRY(alloc_raw(s, a.slow, L2));
