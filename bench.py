@@ -627,6 +627,41 @@ def coupled_mgpcg(api, torch, args, local, flush, dist):
 
 
 PLS_SETTLE_STEPS = 20  # steps after the init sequence that let the particles fill the band
+# Algorithmic bytes of one particle pass (both layers): per particle, advect 16 + two corrections 2 x 13 +
+# radii with binning 12 + scatter 16 + bucket rank 12 + selection 10 + compaction 39; per cell, the two
+# corrections' reset and correct 48, counts and cursors 16, two scans 48, the per-cell reseed 42.
+PLS_BYTES_PER_PARTICLE = 131
+PLS_BYTES_PER_CELL = 154
+
+
+def pls_cpu_baseline(size: int, warmup: int, steps: int = 3):
+    """The particle pass on the CPU oracle: the same scene with and without the particle level set, the same
+    settle and warm-up steps, `steps` timed steps each; the pass = the difference of the step times."""
+    from bevy_eulerian_fluid_b200 import scenes
+    from oracle import py_oracle
+    api = py_oracle.load()
+    py_oracle.set_threads(os.cpu_count() or 1)
+    sc = scenes.dam_break(size)
+    ms, n = {}, 0
+    for on in (False, True):
+        sim = sc.make(api)
+        sim.set_particle_levelset(on)
+        for _ in range(1 + PLS_SETTLE_STEPS + warmup):
+            sim.step(sc.dt)
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            sim.step(sc.dt)
+        ms[on] = (time.perf_counter() - t0) / steps * 1e3
+        if on:
+            n = sum(sim.particle_counts()[0])
+        sim.close()
+    extra = ms[True] - ms[False]
+    cores = py_oracle.get_threads()
+    return {"value": n / (extra / 1e3) if extra > 0 else None, "unit": "particle-steps/s", "cores": cores,
+            "kind": "port", "ms_per_step": {"with": round(ms[True], 2), "without": round(ms[False], 2)},
+            "sample": f"{steps} steps of dam_break_{size} after {1 + PLS_SETTLE_STEPS + warmup} untimed ones, with and "
+                      f"without the particle level set, on the CPU oracle ({cores} host threads; its particle "
+                      f"phases run on one), {n} particles"}
 
 
 def pls_leg(api, torch, args, local, peak):
@@ -682,7 +717,16 @@ def pls_leg(api, torch, args, local, peak):
     extra = ms[True] - ms[False]
     out.update({"ms_per_step": {"with": round(ms[True], 4), "without": round(ms[False], 4),
                                 "particle_pass": round(extra, 4)},
-                "particle_steps_per_s": n / (extra / 1e3) if extra > 0 else None})
+                "particle_steps_per_s": n / (extra / 1e3) if extra > 0 else None, "unit": "particle-steps/s"})
+    if extra > 0:
+        algo = PLS_BYTES_PER_PARTICLE * n + PLS_BYTES_PER_CELL * sc.cells
+        achieved = algo / (extra / 1e3) / 1e9
+        out["roofline"] = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                           "frac": round(achieved / peak, 4), "algorithmic_bytes_per_pass": algo,
+                           "note": f"{PLS_BYTES_PER_PARTICLE} B/particle + {PLS_BYTES_PER_CELL} B/cell over the "
+                                   "whole particle pass (about 25 launches, latency-bound at this size)"}
+    if not args.no_cpu_baseline:
+        out["cpu_baseline"] = pls_cpu_baseline(args.size, args.warmup)
     return out
 
 

@@ -8,13 +8,14 @@ from . import _capi as capi  # noqa: F401
 from .plugin import (  # noqa: F401
     Collider, FastIterativeMethodConfig, Fluid, FluidPlugin, FluidSettings, FluidSource, FluidSourceMode,
     FluidSourceOneshot, FluidSourceShape, FluidSourceVelocity, FluidStatus, FluidTextures, FluidToSolidForce,
-    ForcesToFluid, ForceToFluid, GaussSeidelConfig, LocalForces, MultiGridConfig, ProjectionMethod,
-    ReinitializeMethod, RigidBody, RigidBodyKind,
+    ForcesToFluid, ForceToFluid, GaussSeidelConfig, LevelsetParticles, LocalForces, MultiGridConfig,
+    ParticleLevelsetTwoLayersPlugin, ProjectionMethod, ReinitializeMethod, RigidBody, RigidBodyKind,
 )
 
 __all__ = [
     "capi", "Collider", "FastIterativeMethodConfig", "Fluid", "FluidPlugin", "FluidSettings", "FluidSource",
     "FluidSourceMode", "FluidSourceOneshot", "FluidSourceShape", "FluidSourceVelocity", "FluidStatus",
-    "FluidTextures", "FluidToSolidForce", "ForcesToFluid", "ForceToFluid", "GaussSeidelConfig", "LocalForces",
-    "MultiGridConfig", "ProjectionMethod", "ReinitializeMethod", "RigidBody", "RigidBodyKind",
+    "FluidTextures", "FluidToSolidForce", "ForcesToFluid", "ForceToFluid", "GaussSeidelConfig", "LevelsetParticles",
+    "LocalForces", "MultiGridConfig", "ParticleLevelsetTwoLayersPlugin", "ProjectionMethod", "ReinitializeMethod",
+    "RigidBody", "RigidBodyKind",
 ]

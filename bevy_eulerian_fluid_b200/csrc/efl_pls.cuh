@@ -5,7 +5,7 @@
 // Layout: one struct-of-arrays set per layer (0 = positive particles,
 // 1 = negative), x, y, radius as f32 planes and the escaped flag as a byte;
 // the sign is implied by the layer.  Capacity per layer is nx*ny*16 like the
-// reference's particle buffers (plugin.rs:212-215).  The live count stays on
+// reference's particle buffers (plugin.rs:221-225).  The live count stays on
 // the device; per-particle kernels are grid-stride loops that read it, so a
 // step never waits for the host and the whole pass can be graph-captured.
 //

@@ -345,7 +345,7 @@ efl_status pls_alloc(efl_sim* s) {
     a.nx = s->nx;
     a.ny = s->ny;
     a.L = (uint32_t)s->nx * (uint32_t)s->ny;
-    a.cap = a.L * PLS_MAX_PER_CELL;  // plugin.rs:212-215
+    a.cap = a.L * PLS_MAX_PER_CELL;  // plugin.rs:221-225
     for (int l = 0; l < 2; ++l)
         for (int b = 0; b < 2; ++b) {
             TRY(alloc_raw(s, a.px[l][b], a.cap));

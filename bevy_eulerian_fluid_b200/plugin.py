@@ -31,6 +31,17 @@ class FluidPlugin:
         if not length_unit > 0.0:
             raise ValueError("length_unit must be positive value.")  # euler_fluid.rs:49-51
         self.length_unit = float(length_unit)
+        self.particle_levelset = False
+
+    def add_plugins(self, *plugins) -> "FluidPlugin":
+        """App::add_plugins for the fluid's optional plugins: ParticleLevelsetTwoLayersPlugin (the
+        reference adds it inside FluidPlugin::build, commented out at euler_fluid.rs:81)."""
+        for p in plugins:
+            if isinstance(p, ParticleLevelsetTwoLayersPlugin):
+                self.particle_levelset = True
+            else:
+                raise TypeError(f"unknown plugin {p!r}")
+        return self
 
     @property
     def grid_length(self) -> float:  # FluidGridLength (euler_fluid.rs:89)
@@ -42,6 +53,12 @@ class FluidPlugin:
         """Spawns FluidSettings (+ its required components) and allocates the fluid."""
         return Fluid(self, settings, transform, projection or ProjectionMethod.default(),
                      reinitialize or ReinitializeMethod.default(), device)
+
+
+class ParticleLevelsetTwoLayersPlugin:
+    """particle_levelset_two_layers/plugin.rs:93-118: the two-layer particle level set (Enright et al. 2002) on
+    every fluid spawned afterwards -- particles seeded by the init sequence, advected and used to correct the
+    level set before and after its reinitialisation, reseeded every step."""
 
 
 @dataclass
@@ -384,6 +401,8 @@ class Fluid:
         self.projection = projection
         self.reinitialize = reinitialize
         self.sim = capi.Sim(api or capi.load(), cfg)
+        if plugin.particle_levelset:
+            self.sim.set_particle_levelset(True)
         self.forces_to_fluid = ForcesToFluid()
         self.children: List[_SourceChild] = []
         self.status = FluidStatus.Reset
@@ -465,6 +484,11 @@ class Fluid:
         n = capi.MAX_SOLIDS if n is None else n
         return [FluidToSolidForce((float(a[0]), float(a[1])), float(a[2])) for a in arr[:n]]
 
+    def particles(self) -> "LevelsetParticles":
+        """PLSResources.positive_particles / negative_particles (plugin.rs:186-211) and their counts:
+        capi.PARTICLE_DTYPE arrays (position in grid cells, radius, sign, escaped)."""
+        return LevelsetParticles(self.sim.read_particles(capi.PLS_POSITIVE), self.sim.read_particles(capi.PLS_NEGATIVE))
+
     # diagnostics (diagnostics/component.rs: FluidVolume, FluidMin/MaxVelocityMagnitude)
     def diagnostics(self) -> "FluidDiagnostics":
         mn, mx = self.sim.velocity_magnitude()
@@ -472,6 +496,12 @@ class Fluid:
 
     def close(self):
         self.sim.close()
+
+
+@dataclass
+class LevelsetParticles:
+    positive: np.ndarray  # sign +1, seeded on the air side (phi > 0)
+    negative: np.ndarray  # sign -1, seeded on the fluid side (phi < 0)
 
 
 @dataclass

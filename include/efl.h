@@ -372,7 +372,7 @@ EFL_API efl_status efl_get_rigid_bodies(efl_sim* sim, efl_rigid_body* bodies, ui
  * euler_fluid.rs:81).  Positive particles (sign +1, layer 0) and negative
  * particles (sign -1, layer 1) seeded in the band |phi| < 3 around the
  * interface, at most 16 per cell and layer; capacity nx*ny*16 per layer
- * (plugin.rs:212-215).  When enabled, every efl_step / init sequence runs:
+ * (plugin.rs:221-225).  When enabled, every efl_step / init sequence runs:
  *   init  : seed from levelset_air and its gradient (render_node.rs:250-258);
  *   step  : after the fluid sources, advect the particles (TVD RK3) and
  *           correct levelset_air1 with the escaped ones; after the

@@ -645,3 +645,22 @@ def test_gpu_pls_reseed_random_buckets(oracle_api, gpu_api, seed):
     _compare_particles(*pair)
     for s in pair:
         s.close()
+
+
+def test_plugin_mirror_enables_particles(oracle_api):
+    from bevy_eulerian_fluid_b200 import (FluidPlugin, FluidSettings, FluidSource, FluidSourceOneshot,
+                                          FluidSourceShape, ParticleLevelsetTwoLayersPlugin)
+    plugin = FluidPlugin(10.0).add_plugins(ParticleLevelsetTwoLayersPlugin())
+    assert plugin.particle_levelset
+    from bevy_eulerian_fluid_b200.plugin import Fluid, ProjectionMethod, ReinitializeMethod
+    fluid = Fluid(plugin, FluidSettings(rho=997.0, gravity=(0.0, 9.8), size=(64, 64)), None,
+                  ProjectionMethod.default(), ReinitializeMethod.default(), api=oracle_api)
+    fluid.add_source(FluidSource(), FluidSourceShape.Aabb((32.0, 10.0)), (0.0, -20.0), oneshot=True)
+    for _ in range(3):
+        fluid.step(1.0 / 60.0)
+    parts = fluid.particles()
+    assert len(parts.positive) > 0 and len(parts.negative) > 0
+    assert np.all(parts.positive["sign"] == 1.0) and np.all(parts.negative["sign"] == -1.0)
+    with pytest.raises(TypeError):
+        FluidPlugin(10.0).add_plugins(object())
+    fluid.close()
