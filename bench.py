@@ -626,6 +626,7 @@ def coupled_mgpcg(api, torch, args, local, flush, dist):
             "cg_iterations_per_step": iters}
 
 
+C5_EVAL_SIZE = 1024  # the learned warm start's evaluation scene
 PLS_SETTLE_STEPS = 20  # steps after the init sequence that let the particles fill the band
 # Algorithmic bytes of one particle pass (both layers): per particle, advect 16 + two corrections 2 x 13 +
 # radii with binning 12 + scatter 16 + bucket rank 12 + selection 10 + compaction 39; per cell, the two
@@ -742,20 +743,26 @@ def tensor_peak():
 
 def learned_leg(api, args, local):
     """The learned warm start: trained on the GPU (tensor-core forward and
-    backward) from C2-style scenes with seeds 1-8 at 256^2, then coupled_512
-    (the benchmark scene, RBGS to 1e-5) stepped twice from the same states,
-    warm-started by the network and from the previous pressure."""
-    from bevy_eulerian_fluid_b200 import learned, scenes
-    net, log = learned.train(api, size=256, seeds=tuple(range(1, 9)), steps=100, lr=1e-3, max_size=args.size,
-                             device=local)
+    backward) from C2-style scenes (seeds 1-8 at 256^2, 9-10 at 512^2), then
+    coupled_512 (the benchmark scene, RBGS to 1e-5) and the 1024^2 evaluation
+    scene with 32 bodies (MGPCG to 1e-5) each stepped twice from the same
+    states, warm-started by the network and from the previous pressure."""
+    from bevy_eulerian_fluid_b200 import capi, learned, scenes
+    net, log = learned.train(api, size=256, seeds=tuple(range(1, 9)), steps=100, lr=1e-3,
+                             max_size=max(args.size, C5_EVAL_SIZE), device=local, extra=((512, 9), (512, 10)))
     sc = scenes.coupled(args.size)
     sc.cfg.device = local
     cmp = learned.compare(api, net, sc, warmup=args.warmup, steps=max(1, min(args.steps, 6)))
+    # C5's evaluation scene: 1024^2 with 32 random bodies (8 per shape), solved with MGPCG to 1e-5
+    ev = scenes.coupled(C5_EVAL_SIZE, n_per_shape=8, seed=0xC5, method=capi.PROJECTION_MGPCG)
+    ev.cfg.device = local
+    cmp5 = learned.compare(api, net, ev, warmup=args.warmup, steps=max(1, min(args.steps, 6)))
     ms = net.time_forward(args.size, args.size, 20)
     tf = learned.forward_flops(args.size, args.size) / (ms / 1e3) / 1e12
     peak, kind = tensor_peak()
     q = len(log.losses) // 4
-    out = {"training": {"samples": log.samples, "seconds": round(log.seconds, 2), "grid": "256^2",
+    out = {"training": {"samples": log.samples, "seconds": round(log.seconds, 2),
+                        "grid": "256^2 (seeds 1-8) and 512^2 (seeds 9, 10)",
                         "relative_loss_by_quarter": [round(sum(log.losses[i * q:(i + 1) * q]) / max(1, q), 4)
                                                      for i in range(4)]},
            "workload": f"coupled_{args.size} (RBGS to 1e-5), {len(cmp['plain'])} steps after {args.warmup} warm-up",
@@ -764,6 +771,15 @@ def learned_leg(api, args, local):
                                 "plain": [round(x[1], 5) for x in cmp["plain"]]},
            "pressure_solve_ms_per_step": {"learned": sum(x[2] for x in cmp["learned"]) / len(cmp["learned"]),
                                           "plain": sum(x[2] for x in cmp["plain"]) / len(cmp["plain"])},
+           "c5_evaluation": {
+               "workload": f"coupled_{C5_EVAL_SIZE} with 32 bodies (seed 0xC5), MGPCG to 1e-5, {len(cmp5['plain'])} "
+                           f"steps after {args.warmup} warm-up",
+               "cg_iterations": {"learned": [x[0] for x in cmp5["learned"]], "plain": [x[0] for x in cmp5["plain"]]},
+               "initial_residual": {"learned": [round(x[1], 5) for x in cmp5["learned"]],
+                                    "plain": [round(x[1], 5) for x in cmp5["plain"]]},
+               "pressure_solve_ms_per_step": {
+                   "learned": sum(x[2] for x in cmp5["learned"]) / len(cmp5["learned"]),
+                   "plain": sum(x[2] for x in cmp5["plain"]) / len(cmp5["plain"])}},
            "forward": {"ms": round(ms, 4), "grid": f"{args.size}^2", "tflops": round(tf, 2), "peak": peak,
                        "peak_kind": kind, "frac": round(tf / peak, 4),
                        "kernel": "k_conv3x3_tc (tcgen05.mma kind::f16, BF16 x BF16 -> FP32 in TMEM)"}}

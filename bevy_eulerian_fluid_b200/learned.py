@@ -38,12 +38,15 @@ class TrainLog:
 
 def train(api: capi.Api, size: int = 256, seeds=(1, 2, 3, 4), steps: int = 200, lr: float = 1e-3,
           n_per_shape: int = 6, net: capi.UNet | None = None, max_size: int | None = None,
-          device: int = 0) -> tuple[capi.UNet, TrainLog]:
-    """Online training: every simulation step records one sample, one Adam step follows."""
-    net = net or capi.UNet(api, max_size or size, max_size or size, seed=0xC5, device=device)
+          device: int = 0, extra=()) -> tuple[capi.UNet, TrainLog]:
+    """Online training: every simulation step records one sample, one Adam step follows.
+    Scenes: C2-style coupled scenes at `size` for `seeds`, plus (size, seed) pairs in `extra`."""
+    runs = [(size, s) for s in seeds] + list(extra)
+    big = max(sz for sz, _ in runs)
+    net = net or capi.UNet(api, max(max_size or 0, big), max(max_size or 0, big), seed=0xC5, device=device)
     sims = []
-    for s in seeds:
-        sc = scenes.coupled(size, seed=s, n_per_shape=n_per_shape, method=capi.PROJECTION_MGPCG)
+    for sz, s in runs:
+        sc = scenes.coupled(sz, seed=s, n_per_shape=n_per_shape, method=capi.PROJECTION_MGPCG)
         sc.cfg.device = device
         sim = sc.make(api)
         sim.step(sc.dt)  # init sequence
