@@ -5,15 +5,17 @@
 // Memory Accelerator copies five boxes -- air level set (with a one-cell
 // ring), x- and y-face fractions, divergence and pressure, each covering
 // the tile plus a halo of 2K = 4 cells -- from HBM into shared memory
-// (cp.async.bulk.tensor, completion on an mbarrier), while the CTA is still
-// working on the previous tile from the other staging buffer.  TMA fills
+// (cp.async.bulk.tensor, completion on an mbarrier) two tiles ahead: a
+// staging buffer is refilled as soon as its tile's coefficients are built.  TMA fills
 // boxes outside the field with zeros, which is the out-of-bounds
 // convention of the reference's robust texture loads.  The CTA builds the
 // per-cell coefficients of gauss_seidel.wgsl:44-80 in the reference's f32
 // operation order, runs K = 2 red-black iterations from a
-// checkerboard-compressed shared-memory image, and writes its 64 x 32
-// owned cells to the other buffer of a ping-pong pair: one pass over HBM per
-// two iterations, bit-identical to four global half-sweeps.
+// checkerboard-compressed shared-memory image (each half-sweep over the
+// cells within the distance the remaining half-sweeps still need), and
+// writes its 64 x 32 owned cells to the other buffer of a ping-pong pair: one
+// pass over HBM per two iterations, bit-identical to four global
+// half-sweeps.
 //
 // Every mbarrier wait is bounded; a wait that gives up sets the error flag,
 // waits (bounded again) for the CTA's own copies still in flight, and
@@ -88,6 +90,37 @@ EFL_DEV bool mbar_wait(uint64_t* bar, unsigned parity) {
     return false;
 }
 
+// One half-sweep of color c over the cells within D of the owned tile
+// (gauss_seidel.wgsl:12-88).  A pass of K iterations needs, after half-sweep
+// h (0-based), correct values only within 2K - 1 - h cells of the owned
+// tile (each half-sweep reads distance-1 neighbours), so the sweeps shrink
+// from the halo inwards and the owned cells come out the same.
+template <int D>
+EFL_DEV void ts_sweep_half(GsTile32<TS_EX, TS_EY>& T, int c, int base, float weight, float omw) {
+    constexpr int NJ = TS_TX / 2 + D, ROWS = TS_TY + 2 * D, TOTAL = NJ * ROWS;
+    constexpr int Y0 = TS_H - D, X0 = TS_H - D;
+    const int o = 1 - c;
+    for (int i = threadIdx.x; i < TOTAL; i += TS_THREADS) {
+        const int r = i / NJ;
+        const int ly = Y0 + r;
+        const int odd = (base + ly + c) & 1;  // color-c cells of row ly sit at x = 2j + odd
+        const int k = ly * TS_W2 + ((X0 - odd + 1) >> 1) + (i - r * NJ);
+        const unsigned char m = T.mode[c][k];
+        if (m & MODE_UPDATE) {
+            const float4 wk = T.w[c][k];
+            float nume = T.cb[c][k];
+            nume = nume + wk.x * T.p[o][k - 1 + odd];
+            nume = nume + wk.y * T.p[o][k + odd];
+            nume = nume + wk.z * T.p[o][k - TS_W2];
+            nume = nume + wk.w * T.p[o][k + TS_W2];
+            const float pn = nume / T.den[c][k];
+            T.p[c][k] = weight * pn + omw * T.p[c][k];
+        } else if (m & MODE_ZERO) {
+            T.p[c][k] = 0.0f;
+        }
+    }
+}
+
 __global__ void __launch_bounds__(TS_THREADS, 1)
     k_gs32_tma(const __grid_constant__ SweepMaps maps, int nx, int ny, PF out, int pin, float dx_scaled, float rho,
                float dt, float weight, int tiles_x, int ntiles, int iters, int* err) {
@@ -112,15 +145,18 @@ __global__ void __launch_bounds__(TS_THREADS, 1)
     };
     const float cdiv = dx_scaled * dx_scaled * rho / dt;  // gauss_seidel.wgsl:58
     const float omw = 1.0f - weight;
+    // Tile n is staged in buffer n & 1.  Tiles 0 and 1 are issued up front; tile n + 2 goes into
+    // buffer n & 1 as soon as tile n's coefficients are built (the stage is not read after that),
+    // so every load has about two tiles of work to complete behind.
     int t = blockIdx.x;
-    if (threadIdx.x == 0 && t < ntiles) issue(t, 0);
+    if (threadIdx.x == 0) {
+        if (t < ntiles) issue(t, 0);
+        if (t + (int)gridDim.x < ntiles) issue(t + gridDim.x, 1);
+    }
     for (int n = 0; t < ntiles; t += gridDim.x, ++n) {
         const int b = n & 1;
         const bool next = t + (int)gridDim.x < ntiles;
-        if (threadIdx.x == 0 && next) {
-            fence_proxy_async();  // generic reads of stage[b^1] (previous tile) before the async writes
-            issue(t + gridDim.x, b ^ 1);
-        }
+        const bool after = t + 2 * (int)gridDim.x < ntiles;
         const bool got = mbar_wait(&bars[b], (n >> 1) & 1);  // (the wait is uniform per CTA)
         if (__syncthreads_or(!got)) {
             if (threadIdx.x == 0) atomicExch(err, 1);
@@ -141,6 +177,9 @@ __global__ void __launch_bounds__(TS_THREADS, 1)
             const int ly = i / TS_EX, lx = i - ly * TS_EX;
             const int gx = gx0 + lx, gy = gy0 + ly;
             const int c = (base + lx + ly) & 1, k = ly * TS_W2 + (lx >> 1);
+            T.p[c][k] = p_s[ly * BOX_C_W + lx];
+            // the outermost ring is only read as neighbour pressure
+            if (lx == 0 || ly == 0 || lx == TS_EX - 1 || ly == TS_EY - 1) continue;
             unsigned char m = MODE_SKIP;
             float den = 0.0f, cb = 0.0f;
             float4 wk = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -172,38 +211,27 @@ __global__ void __launch_bounds__(TS_THREADS, 1)
                         update = !(fabsf(den) < 1.0e-6f);
                     }
                 }
-                const bool ring = lx == 0 || ly == 0 || lx == TS_EX - 1 || ly == TS_EY - 1;
-                if (!ring) m = update ? MODE_UPDATE : MODE_ZERO;
+                m = update ? MODE_UPDATE : MODE_ZERO;
             }
-            T.p[c][k] = p_s[ly * BOX_C_W + lx];
             T.cb[c][k] = cb;
             T.den[c][k] = den;
             T.w[c][k] = wk;
             T.mode[c][k] = m;
         }
         __syncthreads();
+        if (threadIdx.x == 0 && after) {
+            fence_proxy_async();  // the generic reads of stage[b] above before the async writes
+            issue(t + 2 * gridDim.x, b);
+        }
         for (int it = 0; it < iters; ++it) {
 #pragma unroll
             for (int half = 0; half < 2; ++half) {
-                const int c = half == 0 ? 1 : 0, o = 1 - c;  // red ((x+y) odd) first
-                constexpr int TOTAL = (TS_EY - 2) * TS_W2;
-                for (int i = threadIdx.x; i < TOTAL; i += TS_THREADS) {
-                    const int ly = 1 + i / TS_W2;
-                    const int k = ly * TS_W2 + (i - (ly - 1) * TS_W2);
-                    const unsigned char m = T.mode[c][k];
-                    if (m & MODE_UPDATE) {
-                        const int odd = (base + ly + c) & 1;
-                        const float4 wk = T.w[c][k];
-                        float nume = T.cb[c][k];
-                        nume = nume + wk.x * T.p[o][k - 1 + odd];
-                        nume = nume + wk.y * T.p[o][k + odd];
-                        nume = nume + wk.z * T.p[o][k - TS_W2];
-                        nume = nume + wk.w * T.p[o][k + TS_W2];
-                        const float pn = nume / T.den[c][k];
-                        T.p[c][k] = weight * pn + omw * T.p[c][k];
-                    } else if (m & MODE_ZERO) {
-                        T.p[c][k] = 0.0f;
-                    }
+                const int c = half == 0 ? 1 : 0;  // red ((x+y) odd) first
+                switch (2 * (iters - it) - 1 - half) {  // distance still needed after this half-sweep
+                    case 3: ts_sweep_half<3>(T, c, base, weight, omw); break;
+                    case 2: ts_sweep_half<2>(T, c, base, weight, omw); break;
+                    case 1: ts_sweep_half<1>(T, c, base, weight, omw); break;
+                    default: ts_sweep_half<0>(T, c, base, weight, omw); break;
                 }
                 __syncthreads();
             }
