@@ -157,11 +157,15 @@ __global__ void __launch_bounds__(TS_THREADS, 1)
         const int b = n & 1;
         const bool next = t + (int)gridDim.x < ntiles;
         const bool after = t + 2 * (int)gridDim.x < ntiles;
-        const bool got = mbar_wait(&bars[b], (n >> 1) & 1);  // (the wait is uniform per CTA)
+        // Warp 0 waits for the copies; the barrier then orders the other warps' reads after its
+        // acquire (the other 31 warps sleep in the barrier instead of spinning on the mbarrier).
+        const bool got = threadIdx.x < 32 ? mbar_wait(&bars[b], (n >> 1) & 1) : true;
         if (__syncthreads_or(!got)) {
-            if (threadIdx.x == 0) atomicExch(err, 1);
-            mbar_wait(&bars[b], (n >> 1) & 1);  // copies of this CTA still in flight
-            if (next) mbar_wait(&bars[b ^ 1], ((n + 1) >> 1) & 1);
+            if (threadIdx.x == 0) {
+                atomicExch(err, 1);
+                mbar_wait(&bars[b], (n >> 1) & 1);  // copies of this CTA still in flight
+                if (next) mbar_wait(&bars[b ^ 1], ((n + 1) >> 1) & 1);
+            }
             return;
         }
         const unsigned char* stb = sm + b * ST_BYTES;
