@@ -56,7 +56,7 @@ struct SolverWorkspace {
     int max_blocks = 0;
 };
 
-constexpr int PS_THREADS = 512;
+constexpr int PS_THREADS = 1024;
 constexpr long long kBarrierSpinLimit = 1ll << 25;  // acquire polls (~ 1 s)
 
 // Grid-wide barrier for a cooperative launch (all CTAs co-resident), with a
