@@ -362,8 +362,16 @@ __global__ void __launch_bounds__(PS_THREADS, 1) k_gsmix_persistent(PersistentPa
     bool ok = grid_barrier(P.barrier, nblocks);
     double r = ok ? ps_total_relative(P.partials, nblocks) : 0.0;
     const double r0 = r;
-    while (ok && !(r <= P.tol) && iters < P.max_iters) {
+    // pending: the partials of the current p are written but their total is not read yet.  A check
+    // whose next block has more than KMAX iterations skips its own grid barrier: the total is read
+    // at the next block's first halo exchange, and if the solve had converged, the iterations run
+    // meanwhile only changed the correction d, which is dropped -- p, the iteration count and r
+    // are those of the check.
+    bool pending = false;
+    while (ok && (pending || (!(r <= P.tol) && iters < P.max_iters))) {
         unsigned todo = min(P.check_interval, P.max_iters - iters);
+        unsigned done = 0;
+        bool converged = false;
         while (ok && todo > 0) {
             const unsigned kk = min((unsigned)KMAX, todo);
             for (unsigned it = 0; it < kk; ++it) {
@@ -373,7 +381,7 @@ __global__ void __launch_bounds__(PS_THREADS, 1) k_gsmix_persistent(PersistentPa
                 __syncthreads();
             }
             todo -= kk;
-            iters += kk;
+            done += kk;
             if (todo > 0) {  // exchange the correction's halo
                 for (int i = threadIdx.x; i < tx * ty; i += PS_THREADS) {
                     const int ly = H + i / tx, lx = H + i % tx, gx = gx0 + lx, gy = gy0 + ly;
@@ -382,6 +390,14 @@ __global__ void __launch_bounds__(PS_THREADS, 1) k_gsmix_persistent(PersistentPa
                 }
                 ok = grid_barrier(P.barrier, nblocks);
                 if (!ok) break;
+                if (pending) {
+                    pending = false;
+                    r = ps_total_relative(P.partials, nblocks);
+                    if (r <= P.tol) {
+                        converged = true;
+                        break;
+                    }
+                }
                 for (int i = threadIdx.x; i < EX * EY; i += PS_THREADS) {
                     const int ly = i / EX, lx = i - ly * EX;
                     if (owned(lx, ly)) continue;
@@ -393,7 +409,8 @@ __global__ void __launch_bounds__(PS_THREADS, 1) k_gsmix_persistent(PersistentPa
                 __syncthreads();
             }
         }
-        if (!ok) break;
+        if (!ok || converged) break;
+        iters += done;
         // p += d on the owned cells (0 where the reference zeroes p), then exchange p.
         for (int i = threadIdx.x; i < tx * ty; i += PS_THREADS) {
             const int ly = H + i / tx, lx = H + i % tx, gx = gx0 + lx, gy = gy0 + ly;
@@ -416,9 +433,13 @@ __global__ void __launch_bounds__(PS_THREADS, 1) k_gsmix_persistent(PersistentPa
         __syncthreads();
         part = mix_check(T, base, H, tx, ty, cdiv, factor);
         if (threadIdx.x == 0) P.partials[blockIdx.x] = part;
-        ok = grid_barrier(P.barrier, nblocks);
-        if (!ok) break;
-        r = ps_total_relative(P.partials, nblocks);
+        if (min(P.check_interval, P.max_iters - iters) > (unsigned)KMAX) {
+            pending = true;  // read at the next block's first halo exchange
+        } else {
+            ok = grid_barrier(P.barrier, nblocks);
+            if (!ok) break;
+            r = ps_total_relative(P.partials, nblocks);
+        }
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         P.result->iterations = iters;
