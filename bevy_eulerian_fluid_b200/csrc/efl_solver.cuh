@@ -32,7 +32,7 @@ namespace efl {
 
 struct GridBarrier {
     unsigned int count;
-    unsigned int gen;
+    unsigned int gen;  // unused (layout kept)
     int error;
     int pad;
 };
@@ -60,35 +60,39 @@ constexpr int PS_THREADS = 1024;
 constexpr long long kBarrierSpinLimit = 1ll << 25;  // acquire polls (~ 1 s)
 
 // Grid-wide barrier for a cooperative launch (all CTAs co-resident), with a
-// bounded spin: a CTA that polls more than kBarrierSpinLimit times sets
-// barrier->error and every CTA leaves the solve.  Arrival is an acq_rel
-// atomic, the release of the generation a release reduction, polling an
-// acquire load (about 2 us for 128 CTAs on B200).
+// bounded spin.  count only grows (it is zeroed before each launch): a CTA's
+// acq_rel arrival returns its arrival number, arrivals of barrier e are
+// numbers [e * nblocks, (e + 1) * nblocks) because no CTA reaches barrier
+// e + 1 before all have arrived at e, so the CTA waits (acquire loads) until
+// count reaches the end of its barrier's range; the last arriver leaves at
+// once.  One atomic round trip on the way in, none on the way out.  A CTA
+// that polls more than kBarrierSpinLimit times sets barrier->error and
+// leaves; the others see the flag while they wait (checked every 1024
+// polls) and leave too.
 EFL_DEV bool grid_barrier(GridBarrier* gb, unsigned nblocks) {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
         int ok = 1;
-        unsigned gen, arrived, cur;
-        asm volatile("ld.acquire.gpu.u32 %0, [%1];" : "=r"(gen) : "l"(&gb->gen) : "memory");
+        unsigned arrived, cur;
         asm volatile("atom.acq_rel.gpu.add.u32 %0, [%1], 1;" : "=r"(arrived) : "l"(&gb->count) : "memory");
-        if (arrived == nblocks - 1) {
-            asm volatile("st.relaxed.gpu.u32 [%0], 0;" ::"l"(&gb->count) : "memory");
-            asm volatile("red.release.gpu.add.u32 [%0], 1;" ::"l"(&gb->gen) : "memory");
-        } else {
+        const unsigned target = (arrived / nblocks + 1) * nblocks;
+        if (arrived + 1 != target) {
             long long spins = 0;
-            do {
-                asm volatile("ld.acquire.gpu.u32 %0, [%1];" : "=r"(cur) : "l"(&gb->gen) : "memory");
-                if (++spins > kBarrierSpinLimit) {
-                    atomicExch(&gb->error, 1);
-                    ok = 0;
-                    break;
+            for (;;) {
+                asm volatile("ld.acquire.gpu.u32 %0, [%1];" : "=r"(cur) : "l"(&gb->count) : "memory");
+                if ((int)(cur - target) >= 0) break;
+                if ((++spins & 1023) == 0) {
+                    int e;
+                    asm volatile("ld.acquire.gpu.s32 %0, [%1];" : "=r"(e) : "l"(&gb->error) : "memory");
+                    if (e || spins > kBarrierSpinLimit) {
+                        atomicExch(&gb->error, 1);
+                        ok = 0;
+                        break;
+                    }
                 }
-            } while (cur == gen);
+            }
         }
-        int e;
-        asm volatile("ld.acquire.gpu.s32 %0, [%1];" : "=r"(e) : "l"(&gb->error) : "memory");
-        if (e) ok = 0;
         s_ok = ok;
     }
     __syncthreads();
