@@ -293,6 +293,43 @@ EFL_DEV double2 mix_check(MixTile<EX, EY>& T, int base, int H, int tx, int ty, d
     return out;
 }
 
+// The halo ring of an EX x EY tile image with owned interior [H, EX - H) x [H, EY - H): 2 H rows of EX
+// cells (top, then bottom), then 2 H columns of each interior row.  Every thread loads its (at most
+// ceil(ring / threads)) cells from global memory before it stores any into the image, so a reload
+// costs one round of L2 latency.
+template <int EX, int EY, int H, class V>
+EFL_DEV void halo_reload(V (*img)[(EX / 2) * EY], const V* src, size_t pitch, int gx0, int gy0, int base, int nx,
+                         int ny) {
+    constexpr int TY = EY - 2 * H, RING = 2 * H * EX + 2 * H * TY;
+    constexpr int PER = (RING + PS_THREADS - 1) / PS_THREADS;
+    V v[PER];
+    int at[PER];
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+        const int i = threadIdx.x + q * PS_THREADS;
+        at[q] = -1;
+        v[q] = V(0);
+        if (i < RING) {
+            int lx, ly;
+            if (i < 2 * H * EX) {
+                const int r = i / EX;
+                lx = i - r * EX;
+                ly = r < H ? r : TY + r;  // rows [0, H) then [EY - H, EY)
+            } else {
+                const int j = i - 2 * H * EX, r = j / (2 * H), c = j - r * (2 * H);
+                ly = H + r;
+                lx = c < H ? c : EX - 2 * H + c;  // columns [0, H) then [EX - H, EX)
+            }
+            const int gx = gx0 + lx, gy = gy0 + ly;
+            if ((unsigned)gx < (unsigned)nx && (unsigned)gy < (unsigned)ny) v[q] = __ldcg(&src[(size_t)gy * pitch + gx]);
+            at[q] = (((base + lx + ly) & 1) << 24) | (ly * (EX / 2) + (lx >> 1));
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < PER; ++q)
+        if (at[q] >= 0) img[at[q] >> 24][at[q] & 0xffffff] = v[q];
+}
+
 template <int EX, int EY, int KMAX>
 __global__ void __launch_bounds__(PS_THREADS, 1) k_gsmix_persistent(PersistentParams P, PF dbuf) {
     extern __shared__ __align__(16) unsigned char ps_raw[];
@@ -402,14 +439,7 @@ __global__ void __launch_bounds__(PS_THREADS, 1) k_gsmix_persistent(PersistentPa
                         break;
                     }
                 }
-                for (int i = threadIdx.x; i < EX * EY; i += PS_THREADS) {
-                    const int ly = i / EX, lx = i - ly * EX;
-                    if (owned(lx, ly)) continue;
-                    const int gx = gx0 + lx, gy = gy0 + ly;
-                    const bool in = (unsigned)gx < (unsigned)L.nx && (unsigned)gy < (unsigned)L.ny;
-                    T.d[(base + lx + ly) & 1][ly * W2 + (lx >> 1)] =
-                        in ? __ldcg(&dbuf.p[(size_t)gy * dbuf.P + gx]) : 0.0f;
-                }
+                halo_reload<EX, EY, H>(T.d, dbuf.p, (size_t)dbuf.P, gx0, gy0, base, L.nx, L.ny);
                 __syncthreads();
             }
         }
@@ -427,13 +457,7 @@ __global__ void __launch_bounds__(PS_THREADS, 1) k_gsmix_persistent(PersistentPa
         }
         ok = grid_barrier(P.barrier, nblocks);
         if (!ok) break;
-        for (int i = threadIdx.x; i < EX * EY; i += PS_THREADS) {
-            const int ly = i / EX, lx = i - ly * EX;
-            if (owned(lx, ly)) continue;
-            const int gx = gx0 + lx, gy = gy0 + ly;
-            const bool in = (unsigned)gx < (unsigned)L.nx && (unsigned)gy < (unsigned)L.ny;
-            T.p[(base + lx + ly) & 1][ly * W2 + (lx >> 1)] = in ? __ldcg(&L.x.p[(size_t)gy * L.x.P + gx]) : 0.0;
-        }
+        halo_reload<EX, EY, H>(T.p, L.x.p, (size_t)L.x.P, gx0, gy0, base, L.nx, L.ny);
         __syncthreads();
         part = mix_check(T, base, H, tx, ty, cdiv, factor);
         if (threadIdx.x == 0) P.partials[blockIdx.x] = part;
