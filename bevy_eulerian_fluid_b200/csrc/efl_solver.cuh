@@ -125,7 +125,20 @@ EFL_DEV double ps_total_relative(const double2* partials, int nblocks) {
     __shared__ double s_rel;
     if (threadIdx.x < 32) {
         double r = 0.0, b = 0.0;
-        for (int i = threadIdx.x; i < nblocks; i += 32) {
+        int i = threadIdx.x;
+        for (; i + 96 < nblocks; i += 128) {  // four loads in flight, added in the same order
+            const double2 v0 = __ldcg(&partials[i]), v1 = __ldcg(&partials[i + 32]);
+            const double2 v2 = __ldcg(&partials[i + 64]), v3 = __ldcg(&partials[i + 96]);
+            r += v0.x;
+            b += v0.y;
+            r += v1.x;
+            b += v1.y;
+            r += v2.x;
+            b += v2.y;
+            r += v3.x;
+            b += v3.y;
+        }
+        for (; i < nblocks; i += 32) {
             const double2 v = __ldcg(&partials[i]);
             r += v.x;
             b += v.y;
@@ -219,18 +232,21 @@ struct MixTile {
     unsigned char mode[2][N2];
 };
 
-template <int EX, int EY>
-EFL_DEV void mix_half_sweep(MixTile<EX, EY>& T, int base, int c, int h, float w, float omw) {
-    constexpr int W2 = EX / 2;
+// Half-sweep h (0-based within a block of red-black iterations) of colour c
+// over the cells of rings >= 1 + h: rows and columns [1 + h, EX - 1 - h), the
+// region the remaining half-sweeps of the block still read.  Colour-c cells
+// of row ly sit at x = 2 j + odd, so a row has exactly (EX - 2 - 2 h) / 2 of
+// them and the work is a dense index range.
+template <int EX, int EY, int HH>
+EFL_DEV void mix_half_sweep_h(MixTile<EX, EY>& T, int base, int c, float w, float omw) {
+    constexpr int W2 = EX / 2, NJ = W2 - 1 - HH, ROWS = EY - 2 - 2 * HH, TOTAL = NJ * ROWS;
+    constexpr int X0 = 1 + HH, Y0 = 1 + HH;
     const int o = 1 - c;
-    const int total = (EY - 2 - 2 * h) * W2;
-    for (int i = threadIdx.x; i < total; i += PS_THREADS) {
-        const int ly = 1 + h + i / W2;
-        const int j = i - (ly - 1 - h) * W2;
+    for (int i = threadIdx.x; i < TOTAL; i += PS_THREADS) {
+        const int r = i / NJ;
+        const int ly = Y0 + r;
         const int odd = (base + ly + c) & 1;
-        const int lx = 2 * j + odd;
-        if (lx < 1 + h || lx > EX - 2 - h) continue;
-        const int k = ly * W2 + j;
+        const int k = ly * W2 + ((X0 - odd + 1) >> 1) + (i - r * NJ);
         if (T.mode[c][k] & MODE_UPDATE) {
             const float4 wk = T.w[c][k];
             float nume = T.rc[c][k];
@@ -240,6 +256,19 @@ EFL_DEV void mix_half_sweep(MixTile<EX, EY>& T, int base, int c, int h, float w,
             nume = nume + wk.w * T.d[o][k + W2];
             T.d[c][k] = w * (nume * T.inv[c][k]) + omw * T.d[c][k];
         }
+    }
+}
+template <int EX, int EY>
+EFL_DEV void mix_half_sweep(MixTile<EX, EY>& T, int base, int c, int h, float w, float omw) {
+    switch (h) {  // h < 2 * KMAX <= 8
+        case 0: mix_half_sweep_h<EX, EY, 0>(T, base, c, w, omw); break;
+        case 1: mix_half_sweep_h<EX, EY, 1>(T, base, c, w, omw); break;
+        case 2: mix_half_sweep_h<EX, EY, 2>(T, base, c, w, omw); break;
+        case 3: mix_half_sweep_h<EX, EY, 3>(T, base, c, w, omw); break;
+        case 4: mix_half_sweep_h<EX, EY, 4>(T, base, c, w, omw); break;
+        case 5: mix_half_sweep_h<EX, EY, 5>(T, base, c, w, omw); break;
+        case 6: mix_half_sweep_h<EX, EY, 6>(T, base, c, w, omw); break;
+        default: mix_half_sweep_h<EX, EY, 7>(T, base, c, w, omw); break;
     }
 }
 
@@ -332,6 +361,7 @@ EFL_DEV void halo_reload(V (*img)[(EX / 2) * EY], const V* src, size_t pitch, in
 
 template <int EX, int EY, int KMAX>
 __global__ void __launch_bounds__(PS_THREADS, 1) k_gsmix_persistent(PersistentParams P, PF dbuf) {
+    static_assert(KMAX >= 1 && KMAX <= 4, "mix_half_sweep dispatches h < 8");
     extern __shared__ __align__(16) unsigned char ps_raw[];
     MixTile<EX, EY>& T = *reinterpret_cast<MixTile<EX, EY>*>(ps_raw);
     constexpr int H = 2 * KMAX;
