@@ -372,7 +372,6 @@ __global__ void __launch_bounds__(PS_THREADS, 1) k_gsmix_persistent(PersistentPa
     const int gx0 = (tile % P.tiles_x) * tx - H, gy0 = (tile / P.tiles_x) * ty - H;
     const int base = (gx0 + gy0) & 1;
     const unsigned nblocks = gridDim.x;
-    auto owned = [&](int lx, int ly) { return lx >= H && lx < H + tx && ly >= H && ly < H + ty; };
 
     for (int i = threadIdx.x; i < EX * EY; i += PS_THREADS) {
         const int ly = i / EX, lx = i - ly * EX;
