@@ -129,6 +129,8 @@ struct efl_sim {
     bool mixp_ready = false;
     CgPlanes cg{};  // MGPCG vectors, allocated on first use
     bool cg_ready = false;
+    PF alt32{};          // the MGPCG preconditioner's level-0 ping-pong plane
+    SweepTma tma_pre;    // TMA maps of the preconditioner's level 0 (error flag shared with tma)
     GraphCache gc;                // captured step segments
     uint64_t graph_epoch = 1;     // counts the setters that change kernel arguments
     PF mix_d2{};       // second correction buffer (batched solve)
@@ -740,6 +742,14 @@ efl_status mgpcg(efl_sim* s, SolveResult* res) {
         TRY(alloc_raw(s, s->cg.totals, 3));
         TRY(alloc_raw(s, s->cg.sc, 1));
         CU(cudaMallocHost(&s->cg.h_read, sizeof(CgRead)));
+        TRY(alloc_plane(s, s->alt32, nx, ny, s->P, R));
+        if (s->tma.ok) {  // maps of (phi, fractions, b = r32, p = z32 / alt32)
+            Level pre0 = s->mg[0];
+            pre0.x = s->cg.z32;
+            pre0.b = s->cg.r32;
+            s->tma_pre.d_err = s->tma.d_err;
+            sweep_tma_init(s->tma_pre, pre0, s->alt32);
+        }
         s->cg_ready = true;
     }
     Level64& L = s->mg64[0];
@@ -760,9 +770,31 @@ efl_status mgpcg(efl_sim* s, SolveResult* res) {
     std::vector<Level> pre = s->mg;
     pre[0].x = C.z32;
     pre[0].b = C.r32;
+    // Level 0's smoothing (2 + 2 red-black iterations) as two passes of the
+    // TMA-streamed sweep: z32 (zero) -> alt32 red first, the coarse
+    // correction on alt32, alt32 -> z32 black first; the same iterates as
+    // four k_gs_color launches each.
+    const bool tma0 = s->tma_pre.ok && P.mg_pre == 2 && P.mg_post == 2 && pre.size() > 1;
     auto precondition = [&]() -> efl_status {  // z = M r, then r . z into totals[2]
         CU(cudaMemset2DAsync(C.z32.p, (size_t)C.z32.P * sizeof(float), 0, (size_t)nx * sizeof(float), ny, s->stream));
-        TRY(v_cycle(s, pre, 0, true));
+        if (tma0) {
+            const float dxs = s->U.dx;  // resolution scale 1 at level 0
+            TRY(tma_sweep_pass(s->tma_pre, nx, ny, s->alt32, 0, s->solver.num_sms, dxs, s->U.rho, s->U.dt, 1.0f, 2,
+                               1, s->tma.d_err, s->stream));
+            Level L0 = pre[0];
+            L0.x = s->alt32;
+            const Level& C1 = pre[1];
+            k_residual<float><<<grid2d(nx, ny, kBlock), kBlock, count_launch(), s->stream>>>(L0, s->U.dt, s->U.rho, dxs);
+            k_restriction<float><<<grid2d(C1.nx, C1.ny, kBlock), kBlock, count_launch(), s->stream>>>(L0, C1);
+            LAUNCH_CHECK();
+            TRY(v_cycle(s, pre, 1, true));
+            k_prolongation<float><<<grid2d(C1.nx, C1.ny, kBlock), kBlock, count_launch(), s->stream>>>(L0, C1);
+            LAUNCH_CHECK();
+            TRY(tma_sweep_pass(s->tma_pre, nx, ny, C.z32, 1, s->solver.num_sms, dxs, s->U.rho, s->U.dt, 1.0f, 2,
+                               0, s->tma.d_err, s->stream));
+        } else {
+            TRY(v_cycle(s, pre, 0, true));
+        }
         cg_sum_enqueue(s, TermDotRZ{C.r, C.z32, M}, 2);
         return EFL_OK;
     };

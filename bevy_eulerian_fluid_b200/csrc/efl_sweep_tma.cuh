@@ -123,7 +123,7 @@ EFL_DEV void ts_sweep_half(GsTile32<TS_EX, TS_EY>& T, int c, int base, float wei
 
 __global__ void __launch_bounds__(TS_THREADS, 1)
     k_gs32_tma(const __grid_constant__ SweepMaps maps, int nx, int ny, PF out, int pin, float dx_scaled, float rho,
-               float dt, float weight, int tiles_x, int ntiles, int iters, int* err) {
+               float dt, float weight, int tiles_x, int ntiles, int iters, int* err, int first = 1) {
     extern __shared__ __align__(128) unsigned char sm[];
     GsTile32<TS_EX, TS_EY>& T = *reinterpret_cast<GsTile32<TS_EX, TS_EY>*>(sm + TS_TILE_OFF);
     uint64_t* bars = reinterpret_cast<uint64_t*>(sm + TS_BAR_OFF);
@@ -230,7 +230,7 @@ __global__ void __launch_bounds__(TS_THREADS, 1)
         for (int it = 0; it < iters; ++it) {
 #pragma unroll
             for (int half = 0; half < 2; ++half) {
-                const int c = half == 0 ? 1 : 0;  // red ((x+y) odd) first
+                const int c = half == 0 ? first : 1 - first;  // red ((x+y) odd) first unless first = 0
                 switch (2 * (iters - it) - 1 - half) {  // distance still needed after this half-sweep
                     case 3: ts_sweep_half<3>(T, c, base, weight, omw); break;
                     case 2: ts_sweep_half<2>(T, c, base, weight, omw); break;
@@ -298,6 +298,31 @@ inline bool sweep_tma_init(SweepTma& st, const Level& L, const PF& alt) {
 inline void sweep_tma_free(SweepTma& st) {
     if (st.d_err) cudaFree(st.d_err);
     st = SweepTma{};
+}
+
+// One pass of `iters` (<= 2) red-black iterations, first colour `first`
+// (1 = red, the reference's order), reading the pressure of map p[pin] and
+// writing `out`.
+inline efl_status tma_sweep_pass(const SweepTma& st, int nx, int ny, const PF& out, int pin, int num_sms,
+                                 float dx_scaled, float rho, float dt, float weight, int iters, int first, int* err,
+                                 cudaStream_t stream) {
+    if (!st.ok || iters < 1 || iters > TS_K) return EFL_ERR_STATE;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    static bool attr_done[64] = {};
+    if (dev < 0 || dev >= 64) return EFL_ERR_STATE;
+    if (!attr_done[dev]) {
+        if (cudaFuncSetAttribute(k_gs32_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TS_SMEM) !=
+            cudaSuccess) {
+            cudaGetLastError();
+            return EFL_ERR_STATE;
+        }
+        attr_done[dev] = true;
+    }
+    const int tiles_x = (nx + TS_TX - 1) / TS_TX, ntiles = tiles_x * ((ny + TS_TY - 1) / TS_TY);
+    k_gs32_tma<<<std::min(ntiles, num_sms), TS_THREADS, TS_SMEM + count_launch(), stream>>>(
+        st.maps, nx, ny, out, pin, dx_scaled, rho, dt, weight, tiles_x, ntiles, iters, err, first);
+    return cudaGetLastError() == cudaSuccess ? EFL_OK : EFL_ERR_CUDA;
 }
 
 // n fixed f32 red-black iterations at level 0 with the TMA kernel,
