@@ -68,9 +68,8 @@ EFL_DEV void bt_tile_origin(const BatchSim& S, int lt, int tx, int ty, int* x0, 
     *y0 = (lt / S.tiles_x) * ty;
 }
 
-// A cell whose four neighbours are fluid with full faces: w = (1, 1, 1, 1),
-// den = 4, inv = 0.25f, so none of its coefficients is read from memory.
-constexpr unsigned char MODE_STD = 8;
+// A cell whose four neighbours are fluid with full faces (MODE_STD): w = (1, 1,
+// 1, 1), den = 4, inv = 0.25f, so none of its coefficients is read from memory.
 // Per-tile flags of the owned region.
 constexpr int TILE_UPDATE = 1, TILE_COUNTED = 2;
 

@@ -117,6 +117,7 @@ constexpr unsigned char MODE_SKIP = 0;     // outside the domain or on the tile'
 constexpr unsigned char MODE_ZERO = 1;     // air, fully solid or |denom| < 1e-6: p = 0
 constexpr unsigned char MODE_UPDATE = 2;   // regular update
 constexpr unsigned char MODE_COUNTED = 4;  // counted in the residual norms
+constexpr unsigned char MODE_STD = 8;      // update cell with w = (1, 1, 1, 1), inv = 0.25 (coefficients implied)
 
 // Sum of all CTAs' partials in CTA order; identical in every CTA.
 EFL_DEV double ps_total_relative(const double2* partials, int nblocks) {
@@ -247,7 +248,15 @@ EFL_DEV void mix_half_sweep_h(MixTile<EX, EY>& T, int base, int c, float w, floa
         const int ly = Y0 + r;
         const int odd = (base + ly + c) & 1;
         const int k = ly * W2 + ((X0 - odd + 1) >> 1) + (i - r * NJ);
-        if (T.mode[c][k] & MODE_UPDATE) {
+        const unsigned char m = T.mode[c][k];
+        if (m & MODE_STD) {  // 1 * d is d exactly and inv is 0.25: the general update, without its loads
+            float nume = T.rc[c][k];
+            nume = nume + T.d[o][k - 1 + odd];
+            nume = nume + T.d[o][k + odd];
+            nume = nume + T.d[o][k - W2];
+            nume = nume + T.d[o][k + W2];
+            T.d[c][k] = w * (nume * 0.25f) + omw * T.d[c][k];
+        } else if (m & MODE_UPDATE) {
             const float4 wk = T.w[c][k];
             float nume = T.rc[c][k];
             nume = nume + wk.x * T.d[o][k - 1 + odd];
@@ -415,6 +424,7 @@ __global__ void __launch_bounds__(PS_THREADS, 1) k_gsmix_persistent(PersistentPa
             }
             if (counted) m |= MODE_COUNTED;
             if (!ring) m |= update ? MODE_UPDATE : MODE_ZERO;  // the outer ring never updates here
+            if (!ring && update && wk.x == 1.0f && wk.y == 1.0f && wk.z == 1.0f && wk.w == 1.0f) m |= MODE_STD;
         }
         T.mode[c][k] = m;
         T.den[c][k] = den;
