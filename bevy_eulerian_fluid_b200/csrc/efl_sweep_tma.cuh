@@ -106,7 +106,14 @@ EFL_DEV void ts_sweep_half(GsTile32<TS_EX, TS_EY>& T, int c, int base, float wei
         const int odd = (base + ly + c) & 1;  // color-c cells of row ly sit at x = 2j + odd
         const int k = ly * TS_W2 + ((X0 - odd + 1) >> 1) + (i - r * NJ);
         const unsigned char m = T.mode[c][k];
-        if (m & MODE_UPDATE) {
+        if (m & MODE_STD) {  // w = 1 (1 * p is p) and den = 4 (nume / 4 is nume * 0.25 exactly)
+            float nume = T.cb[c][k];
+            nume = nume + T.p[o][k - 1 + odd];
+            nume = nume + T.p[o][k + odd];
+            nume = nume + T.p[o][k - TS_W2];
+            nume = nume + T.p[o][k + TS_W2];
+            T.p[c][k] = weight * (nume * 0.25f) + omw * T.p[c][k];
+        } else if (m & MODE_UPDATE) {
             const float4 wk = T.w[c][k];
             float nume = T.cb[c][k];
             nume = nume + wk.x * T.p[o][k - 1 + odd];
@@ -216,6 +223,7 @@ __global__ void __launch_bounds__(TS_THREADS, 1)
                     }
                 }
                 m = update ? MODE_UPDATE : MODE_ZERO;
+                if (update && wk.x == 1.0f && wk.y == 1.0f && wk.z == 1.0f && wk.w == 1.0f) m |= MODE_STD;
             }
             T.cb[c][k] = cb;
             T.den[c][k] = den;
