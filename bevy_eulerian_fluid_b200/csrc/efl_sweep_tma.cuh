@@ -308,25 +308,30 @@ inline void sweep_tma_free(SweepTma& st) {
     st = SweepTma{};
 }
 
+// The kernel's dynamic shared-memory size, set once per device.
+inline bool tma_kernel_ready() {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    static bool attr_done[64] = {};
+    if (dev < 0 || dev >= 64) return false;
+    if (!attr_done[dev]) {
+        if (cudaFuncSetAttribute(k_gs32_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TS_SMEM) !=
+            cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        attr_done[dev] = true;
+    }
+    return true;
+}
+
 // One pass of `iters` (<= 2) red-black iterations, first colour `first`
 // (1 = red, the reference's order), reading the pressure of map p[pin] and
 // writing `out`.
 inline efl_status tma_sweep_pass(const SweepTma& st, int nx, int ny, const PF& out, int pin, int num_sms,
                                  float dx_scaled, float rho, float dt, float weight, int iters, int first, int* err,
                                  cudaStream_t stream) {
-    if (!st.ok || iters < 1 || iters > TS_K) return EFL_ERR_STATE;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    static bool attr_done[64] = {};
-    if (dev < 0 || dev >= 64) return EFL_ERR_STATE;
-    if (!attr_done[dev]) {
-        if (cudaFuncSetAttribute(k_gs32_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TS_SMEM) !=
-            cudaSuccess) {
-            cudaGetLastError();
-            return EFL_ERR_STATE;
-        }
-        attr_done[dev] = true;
-    }
+    if (!st.ok || iters < 1 || iters > TS_K || !tma_kernel_ready()) return EFL_ERR_STATE;
     const int tiles_x = (nx + TS_TX - 1) / TS_TX, ntiles = tiles_x * ((ny + TS_TY - 1) / TS_TY);
     k_gs32_tma<<<std::min(ntiles, num_sms), TS_THREADS, TS_SMEM + count_launch(), stream>>>(
         st.maps, nx, ny, out, pin, dx_scaled, rho, dt, weight, tiles_x, ntiles, iters, err, first);
@@ -339,19 +344,7 @@ inline efl_status tma_sweep_pass(const SweepTma& st, int nx, int ny, const PF& o
 inline efl_status solve_gs32_tma(SweepTma& st, const Level& L, const PF& alt, int num_sms, float dx_scaled,
                                  float rho, float dt, float weight, uint32_t n, cudaStream_t stream,
                                  std::string* err) {
-    if (!st.ok) return EFL_ERR_STATE;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    static bool attr_done[64] = {};
-    if (dev < 0 || dev >= 64) return EFL_ERR_STATE;
-    if (!attr_done[dev]) {
-        if (cudaFuncSetAttribute(k_gs32_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TS_SMEM) !=
-            cudaSuccess) {
-            cudaGetLastError();
-            return EFL_ERR_STATE;
-        }
-        attr_done[dev] = true;
-    }
+    if (!st.ok || !tma_kernel_ready()) return EFL_ERR_STATE;
     const int tiles_x = (L.nx + TS_TX - 1) / TS_TX, tiles_y = (L.ny + TS_TY - 1) / TS_TY;
     const int ntiles = tiles_x * tiles_y;
     const int grid = std::min(ntiles, num_sms);
