@@ -782,7 +782,9 @@ def learned_leg(api, args, local):
                    "plain": sum(x[2] for x in cmp5["plain"]) / len(cmp5["plain"])}},
            "forward": {"ms": round(ms, 4), "grid": f"{args.size}^2", "tflops": round(tf, 2), "peak": peak,
                        "peak_kind": kind, "frac": round(tf / peak, 4),
-                       "kernel": "k_conv3x3_tc (tcgen05.mma kind::f16, BF16 x BF16 -> FP32 in TMEM)"}}
+                       "kernel": "k_conv3x3_rows (widths a multiple of 128) and k_conv3x3_tc (tcgen05.mma kind::f16, "
+                                 "BF16 x BF16 -> FP32 in TMEM)",
+                       "timing": "one forward replayed from a CUDA graph, as the simulation step runs it"}}
     net.close()
     return out
 

@@ -582,7 +582,8 @@ class UNet:
         self._check(self.api.unet_attach(sim.h, self.h if flags else None, flags))
 
     def time_forward(self, nx: int, ny: int, reps: int = 20) -> float:
-        """Device ms of one forward pass at nx x ny."""
+        """Device ms of one forward pass at nx x ny, replayed from a CUDA graph
+        of the pass (as a simulation step runs it)."""
         ms = C.c_float()
         self._check(self.api.unet_time_forward(self.h, nx, ny, reps, C.byref(ms)))
         return ms.value

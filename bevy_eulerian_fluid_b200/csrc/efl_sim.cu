@@ -2301,6 +2301,11 @@ efl_status unet_err(efl_unet* u, efl_status st, const std::string& m) {
 // Sets up the kernels' shared-memory limits once per device.
 bool unet_kernel_attrs() {
     return cudaFuncSetAttribute(k_conv3x3_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, CV_SMEM) == cudaSuccess &&
+           cudaFuncSetAttribute(k_conv3x3_rows<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, CV_SMEM) ==
+               cudaSuccess &&
+           cudaFuncSetAttribute(k_conv3x3_rows<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, CV_SMEM) ==
+               cudaSuccess &&
+           conv_sm_count_init() &&
            cudaFuncSetAttribute(k_wgrad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, WG_SMEM) == cudaSuccess;
 }
 efl_status unet_finish(efl_unet* u, cudaStream_t st) {
@@ -2464,18 +2469,39 @@ efl_status efl_unet_time_forward(efl_unet* u, uint32_t nx, uint32_t ny, uint32_t
     if (nx < 16 || ny < 16 || nx % 8 || ny % 8 || (int)nx > u->net.maxW || (int)ny > u->net.maxH)
         return unet_err(u, EFL_ERR_INVALID_ARGUMENT, "bad grid");
     cudaSetDevice(u->net.device);
-    cudaEvent_t e0, e1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
-    unet_forward(u->net, (int)ny, (int)nx, 0);  // warm-up
-    cudaEventRecord(e0, 0);
-    for (uint32_t i = 0; i < reps; ++i) unet_forward(u->net, (int)ny, (int)nx, 0);
-    cudaEventRecord(e1, 0);
-    efl_status st = unet_finish(u, 0);
+    cudaStream_t sm = nullptr;
+    if (cudaStreamCreateWithFlags(&sm, cudaStreamNonBlocking) != cudaSuccess)
+        return unet_err(u, EFL_ERR_CUDA, "stream creation failed");
+    unet_forward(u->net, (int)ny, (int)nx, sm);  // warm-up
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    bool captured = cudaStreamBeginCapture(sm, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+    if (captured) {
+        unet_forward(u->net, (int)ny, (int)nx, sm);
+        captured = cudaStreamEndCapture(sm, &graph) == cudaSuccess && graph &&
+                   cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+    }
+    efl_status st = EFL_OK;
     float t = 0.0f;
-    cudaEventElapsedTime(&t, e0, e1);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+    if (captured) {
+        cudaEvent_t e0, e1;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        cudaGraphLaunch(exec, sm);  // warm-up replay
+        cudaEventRecord(e0, sm);
+        for (uint32_t i = 0; i < reps; ++i) cudaGraphLaunch(exec, sm);
+        cudaEventRecord(e1, sm);
+        st = unet_finish(u, sm);
+        cudaEventElapsedTime(&t, e0, e1);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+    } else {
+        st = unet_err(u, EFL_ERR_CUDA, "graph capture of the forward pass failed");
+    }
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    cudaStreamSynchronize(sm);
+    cudaStreamDestroy(sm);
     *ms = t / (float)reps;
     return st;
 }

@@ -5,8 +5,9 @@
 //
 // Activations are NHWC bf16 with the channel count a multiple of 16; a tensor
 // may be a channel slice (stride, offset) of a wider one, which is how the
-// skip connections are concatenated without copies.  Weights are bf16
-// [tap = 9][cout][cin] (tap = (dy + 1) * 3 + (dx + 1)); biases fp32.
+// skip connections are concatenated without copies.  Master weights are fp32
+// [tap = 9][cout][cin] (tap = (dy + 1) * 3 + (dx + 1)), biases fp32; the
+// convolutions read BF16 copies laid out as one K-major tile per tap.
 //
 // One convolution = one implicit GEMM per CTA: 128 consecutive output pixels
 // (M = 128) x cout (N), accumulated over 9 taps x cin / 16 MMAs of K = 16.
@@ -98,15 +99,47 @@ EFL_DEV uint32_t kmajor_off(int row, int k, int K) {
 // 3x3 convolution, stride 1, zero padding.
 
 constexpr int CV_THREADS = 128, CV_MAX_CIN = 128, CV_MAX_COUT = 128;
-constexpr int CV_SMEM = 128 * CV_MAX_CIN * 2 + CV_MAX_COUT * CV_MAX_CIN * 2 + 64;
+constexpr int CV_STAGES = 4;              // A stages: taps t + 1 and t + 2 load while tap t multiplies
+constexpr int CV_SMEM = 226 * 1024;       // dynamic shared memory ceiling (227 KB per CTA less static)
+constexpr int CV_BULK_CHUNK = 32768;      // bytes per bulk weight copy
 
-// Dynamic shared memory of one convolution CTA: the A and B tiles, then the mbarrier.
-__host__ __device__ constexpr int conv_smem_bytes(int cin, int cout) { return 128 * cin * 2 + cout * cin * 2 + 64; }
+// Shared memory of one convolution CTA, in this order:
+//  - CV_STAGES A stages (128 x cin, K-major core matrices), tap t in stage
+//    t % CV_STAGES, filled by 16-byte asynchronous copies two taps ahead;
+//  - the weight tiles (cout x cin per tap, K-major, bulk-copied): all nine
+//    taps when that costs no occupancy, else a ring of three filled one tap
+//    ahead;
+//  - mbarriers: one per A stage (its MMAs done), three for the weight copies.
+__host__ __device__ constexpr int conv_a_bytes(int cin) { return 128 * cin * 2; }
+__host__ __device__ constexpr int conv_b_bytes(int cin, int cout) { return cout * cin * 2; }
+__host__ __device__ constexpr int conv_smem_with(int cin, int cout, int btiles) {
+    return CV_STAGES * conv_a_bytes(cin) + btiles * conv_b_bytes(cin, cout) + 64;
+}
+// CTAs per SM: shared memory (228 KB per SM, 1 KB reserved per CTA), tensor
+// memory columns (512 per SM) and threads (2048 per SM).
+__host__ __device__ constexpr int conv_ctas_per_sm(int smem, int cout) {
+    return (228 * 1024) / (smem + 1024) < 512 / (int)tmem_cols(cout)
+               ? ((228 * 1024) / (smem + 1024) < 2048 / CV_THREADS ? (228 * 1024) / (smem + 1024) : 2048 / CV_THREADS)
+               : (512 / (int)tmem_cols(cout) < 2048 / CV_THREADS ? 512 / (int)tmem_cols(cout) : 2048 / CV_THREADS);
+}
+__host__ __device__ constexpr bool conv_weights_resident(int cin, int cout) {
+    return conv_smem_with(cin, cout, 9) <= CV_SMEM &&
+           conv_ctas_per_sm(conv_smem_with(cin, cout, 9), cout) >= conv_ctas_per_sm(conv_smem_with(cin, cout, 3), cout);
+}
+__host__ __device__ constexpr int conv_smem_bytes(int cin, int cout) {
+    return conv_smem_with(cin, cout, conv_weights_resident(cin, cout) ? 9 : 3);
+}
+
+// Element index of (row, k) in a K-major non-swizzled tile with K columns
+// (the element form of kmajor_off).
+__host__ __device__ constexpr int kmajor_index(int row, int k, int K) {
+    return ((row >> 3) * (K >> 3) + (k >> 3)) * 64 + (row & 7) * 8 + (k & 7);
+}
 
 struct ConvArgs {
     const bf16* x;  // input [H*W][xs], channels [xo, xo + cin)
     int xs, xo;
-    const bf16* w;       // [9][cout][cin]
+    const bf16* w;       // 9 tap tiles of cout x cin, each K-major (kmajor_index(co, ci, cin))
     const float* bias;   // [cout] or null
     bf16* y;             // bf16 output [H*W][ys] at [yo, yo + cout), or null
     int ys, yo;
@@ -116,60 +149,140 @@ struct ConvArgs {
     int* err;
 };
 
+// 16-byte asynchronous copy global -> shared through L1 (the nine taps of a
+// pixel tile re-read overlapping rows); zero-fills when !full.
+EFL_DEV void cp_async16(void* dst, const void* src, bool full) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(full ? 16 : 0)
+                 : "memory");
+}
+EFL_DEV void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+EFL_DEV void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+// Bulk copy global -> shared of `bytes` (a multiple of 16, both addresses
+// 16-byte aligned), completing on bar's transaction count.
+EFL_DEV void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+// One thread: arms bar for `bytes` and copies them in chunks.
+EFL_DEV void bulk_load_all(unsigned char* dst, const unsigned char* src, uint32_t bytes, uint64_t* bar) {
+    mbar_expect_tx(bar, bytes);
+    for (uint32_t o = 0; o < bytes; o += CV_BULK_CHUNK)
+        bulk_load(dst + o, src + o, bytes - o < (uint32_t)CV_BULK_CHUNK ? bytes - o : (uint32_t)CV_BULK_CHUNK, bar);
+}
+// This thread's input row of one tap (zero outside the image) into an A stage.
+EFL_DEV void conv_load_tap(const ConvArgs& a, int tap, int m, int py, int px, bool inside, unsigned char* As) {
+    const int sy = py + tap / 3 - 1, sx = px + tap % 3 - 1;
+    const bool valid = inside && (unsigned)sy < (unsigned)a.H && (unsigned)sx < (unsigned)a.W;
+    const bf16* src = valid ? a.x + (size_t)(sy * a.W + sx) * a.xs + a.xo : a.x;
+    for (int j = 0; j < (a.cin >> 3); ++j) cp_async16(As + kmajor_off(m, 8 * j, a.cin), src + (valid ? 8 * j : 0), valid);
+}
+
 __global__ void __launch_bounds__(CV_THREADS) k_conv3x3_tc(ConvArgs a) {
     extern __shared__ __align__(128) unsigned char cv_smem[];
-    unsigned char* As = cv_smem;                  // 128 x cin
-    unsigned char* Bs = cv_smem + 128 * a.cin * 2;  // cout x cin
-    uint64_t* bar = reinterpret_cast<uint64_t*>(cv_smem + conv_smem_bytes(a.cin, a.cout) - 64);
+    const int abytes = conv_a_bytes(a.cin), bbytes = conv_b_bytes(a.cin, a.cout);
+    const bool resident = conv_weights_resident(a.cin, a.cout);
+    unsigned char* Ab = cv_smem;
+    unsigned char* Bb = Ab + CV_STAGES * abytes;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(Bb + (resident ? 9 : 3) * bbytes);  // [CV_STAGES]: MMAs done
+    uint64_t* wbar = bar + CV_STAGES;                                                // [3]: weight copies done
+    const unsigned char* wsrc = reinterpret_cast<const unsigned char*>(a.w);
     __shared__ uint32_t s_tmem;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int npix = a.H * a.W, p0 = blockIdx.x * 128;
     const uint32_t ncols = tmem_cols(a.cout);
+    const int m = tid, p = p0 + m;
+    const int py = p / a.W, px = p - py * a.W;
+    // The first taps' rows start loading before anything else (one copy group per tap).
+    for (int t = 0; t < CV_STAGES - 2; ++t) {
+        conv_load_tap(a, t, m, py, px, p < npix, Ab + t * abytes);
+        cp_async_commit();
+    }
     if (warp == 0) tmem_alloc(&s_tmem, ncols);
     if (tid == 0) {
-        mbar_init(bar, 1);
+        for (int i = 0; i < CV_STAGES + 3; ++i) mbar_init(&bar[i], 1);
         fence_mbar_init();
     }
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
+    // Weight copies, issued and awaited by thread 0 in order: unit u is the
+    // whole resident block (u = 0) or ring tap u, on wbar[u % 3] with phase
+    // parity (u / 3) & 1.
+    int wissued = 0, wdone = 0;
+    if (tid == 0) {
+        if (resident) {
+            bulk_load_all(Bb, wsrc, 9 * bbytes, &wbar[0]);
+            wissued = 1;
+        } else {
+            bulk_load_all(Bb, wsrc, bbytes, &wbar[0]);
+            bulk_load_all(Bb + bbytes, wsrc + bbytes, bbytes, &wbar[1]);
+            wissued = 2;
+        }
+    }
     const uint32_t tmem = s_tmem;
     const uint32_t idesc = umma_idesc_bf16(128, a.cout);
-    const int kg = a.cin >> 3;  // 16-byte groups per row
-    const uint32_t sbo_a = (uint32_t)kg * 128, sbo_b = sbo_a;
-    const int m = tid, p = p0 + m;
-    const int py = p / a.W, px = p - py * a.W;
+    const uint32_t sbo = (uint32_t)(a.cin >> 3) * 128;
+    // Tap t is the (t / CV_STAGES)-th completion of bar[t % CV_STAGES], so its
+    // phase parity is (t / CV_STAGES) & 1; each completion is awaited (two taps
+    // after its issue) before the next one on the same barrier can happen.
     bool ok = true;
-    for (int tap = 0; tap < 9 && ok; ++tap) {
-        const int dy = tap / 3 - 1, dx = tap % 3 - 1;
-        const int sy = py + dy, sx = px + dx;
-        const bool valid = p < npix && (unsigned)sy < (unsigned)a.H && (unsigned)sx < (unsigned)a.W;
-        const uint4* src = reinterpret_cast<const uint4*>(a.x + (size_t)(valid ? sy * a.W + sx : 0) * a.xs + a.xo);
-        for (int j = 0; j < kg; ++j) {
-            const uint4 v = valid ? __ldg(src + j) : make_uint4(0u, 0u, 0u, 0u);
-            *reinterpret_cast<uint4*>(As + kmajor_off(m, 8 * j, a.cin)) = v;
-        }
-        const uint4* wsrc = reinterpret_cast<const uint4*>(a.w + (size_t)tap * a.cout * a.cin);
-        for (int c = tid; c < a.cout * kg; c += CV_THREADS) {
-            const int n = c / kg, j = c - n * kg;
-            *reinterpret_cast<uint4*>(Bs + kmajor_off(n, 8 * j, a.cin)) = __ldg(wsrc + c);
-        }
+    int last = -1;  // last tap whose MMAs were committed
+    for (int tap = 0; tap < 9; ++tap) {
+        const int s = tap % CV_STAGES;
+        unsigned char* As = Ab + s * abytes;
+        unsigned char* Bs = Bb + (resident ? tap : tap % 3) * bbytes;
+        cp_async_wait<CV_STAGES - 3>();  // this thread's rows of this tap have landed
         fence_proxy_async();
-        __syncthreads();
-        if (tid == 0) {
-            tc_fence_after();
-            const uint32_t sa = smem_u32(As), sb = smem_u32(Bs);
-            for (int kc = 0; kc < (a.cin >> 4); ++kc)
-                umma_bf16(tmem, umma_desc(sa + kc * 256, 128, sbo_a), umma_desc(sb + kc * 256, 128, sbo_b), idesc,
-                          (tap | kc) != 0);
-            umma_commit(bar);
+        if (__syncthreads_or(!ok)) {
+            ok = false;
+            break;
         }
-        ok = mbar_wait(bar, tap & 1);
-        if (__syncthreads_or(!ok)) ok = false;
+        if (tid == 0) {
+            if (ok && (!resident || tap == 0)) {
+                const int u = resident ? 0 : tap;
+                if (mbar_wait(&wbar[u % 3], (u / 3) & 1)) wdone = u + 1;
+                else ok = false;
+            }
+            tc_fence_after();
+            if (ok) {
+                const uint32_t sa = smem_u32(As), sb = smem_u32(Bs);
+                for (int kc = 0; kc < (a.cin >> 4); ++kc)
+                    umma_bf16(tmem, umma_desc(sa + kc * 256, 128, sbo), umma_desc(sb + kc * 256, 128, sbo), idesc,
+                              (tap | kc) != 0);
+            }
+            umma_commit(&bar[s]);  // also when skipped, so that the waits on it end
+        }
+        last = tap;
+        if (tap >= 2) {  // the MMAs of tap - 2 are done with their A stage and weight tile
+            const int d = tap - 2;
+            ok = mbar_wait(&bar[d % CV_STAGES], (d / CV_STAGES) & 1) && ok;
+        }
+        if (ok && tap + CV_STAGES - 2 < 9) {
+            const int u = tap + CV_STAGES - 2;  // into the A stage the MMAs of tap - 2 read
+            conv_load_tap(a, u, m, py, px, p < npix, Ab + (u % CV_STAGES) * abytes);
+        }
+        cp_async_commit();
+        if (!resident && tid == 0 && ok && tap >= 1 && tap + 1 < 9) {
+            const int u = tap + 1;  // into ring tile u % 3, last read by the MMAs of tap - 2
+            bulk_load_all(Bb + (u % 3) * bbytes, wsrc + (size_t)u * bbytes, bbytes, &wbar[u % 3]);
+            wissued = u + 1;
+        }
     }
+    if (ok) ok = mbar_wait(&bar[8 % CV_STAGES], (8 / CV_STAGES) & 1);  // tap 8's commit tracks every earlier MMA
+    cp_async_wait<0>();
+    ok = !__syncthreads_or(!ok);
     if (!ok) {
-        if (tid == 0) atomicExch(a.err, 1);
-        mbar_wait(bar, 0);  // give outstanding MMAs a last bounded chance before releasing TMEM
+        if (tid == 0) {
+            atomicExch(a.err, 1);
+            for (int u = wdone; u < wissued; ++u) mbar_wait(&wbar[u % 3], (u / 3) & 1);  // copies in flight
+        }
+        // give the MMAs in flight a last bounded chance before releasing TMEM
+        if (last >= 0) mbar_wait(&bar[last % CV_STAGES], (last / CV_STAGES) & 1);
     }
     tc_fence_after();
     if (ok) {
@@ -194,6 +307,164 @@ __global__ void __launch_bounds__(CV_THREADS) k_conv3x3_tc(ConvArgs a) {
                 dst[1] = reinterpret_cast<const uint4*>(o)[1];
             } else {
                 float* dst = a.yf + (size_t)pp * a.ys + a.yo + c0;
+#pragma unroll
+                for (int i = 0; i < 16; ++i) dst[i] = v[i];
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(tmem, ncols);
+}
+
+// ---------------------------------------------------------------------------
+// 3x3 convolution for image widths that are a multiple of 128: a CTA's 128
+// output pixels are one stretch of one image row, so the input it needs is
+// three rows of 130 pixels (the stretch and one pixel either side, zero
+// outside the image), staged once.  In shared memory the 3 x 130 rows form
+// one plane per 8-channel group (16 bytes per row, planes CR_PLANE bytes
+// apart), and tap (dy, dx)'s A operand is the 128 rows from
+// (dy + 1) * 130 + dx + 1 on: a K-major non-swizzled operand with core
+// matrices 128 bytes apart along M (SBO) and one plane apart along K (LBO).
+// The nine taps' MMAs then go out back to back with no copies or block
+// barriers between them.
+
+constexpr int CR_SEG = 130;                // pixels x0 - 1 .. x0 + 128 of one tap row
+constexpr int CR_PLANE = 3 * CR_SEG * 16;  // bytes per 8-channel group: 3 rows x 130 pixels x 16 bytes
+
+__host__ __device__ constexpr int crow_seg_bytes(int cin) { return ((cin >> 3) * CR_PLANE + 127) & ~127; }
+constexpr int CR_RING = 4;                 // weight tiles in flight when not all nine are resident
+__host__ __device__ constexpr int crow_smem_with(int cin, int cout, int btiles) {
+    return crow_seg_bytes(cin) + btiles * conv_b_bytes(cin, cout) + 128;
+}
+__host__ __device__ constexpr int crow_smem_bytes(int cin, int cout, bool resident) {
+    return crow_smem_with(cin, cout, resident ? 9 : CR_RING);
+}
+
+// RESIDENT: all nine weight tiles in one bulk copy, else the ring.
+template <bool RESIDENT>
+__global__ void __launch_bounds__(CV_THREADS) k_conv3x3_rows(ConvArgs a) {
+    extern __shared__ __align__(128) unsigned char cv_smem[];
+    const int kg = a.cin >> 3, bbytes = conv_b_bytes(a.cin, a.cout);
+    constexpr bool resident = RESIDENT;
+    unsigned char* seg = cv_smem;
+    unsigned char* Bb = cv_smem + crow_seg_bytes(a.cin);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(Bb + (resident ? 9 : CR_RING) * bbytes);  // [CR_RING]: slot's MMAs done
+    uint64_t* wbar = bar + CR_RING;                                                         // [CR_RING]: slot's copy done
+    uint64_t* done = bar + 2 * CR_RING;                                                     // every MMA done
+    const unsigned char* wsrc = reinterpret_cast<const unsigned char*>(a.w);
+    __shared__ uint32_t s_tmem;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int tiles_per_row = a.W >> 7;
+    const int y = blockIdx.x / tiles_per_row, x0 = (blockIdx.x - y * tiles_per_row) << 7;
+    const uint32_t ncols = tmem_cols(a.cout);
+    {  // segment row r * 130 + o holds pixel (y + r - 1, x0 - 1 + o); channel group fastest across threads
+        const int total = 3 * CR_SEG * kg;
+        const int drow = CV_THREADS / kg, dg = CV_THREADS - drow * kg;
+        int row = tid / kg, g = tid - row * kg;  // of element c = row * kg + g
+        for (int c = tid; c < total; c += CV_THREADS) {
+            const int r = row >= 2 * CR_SEG ? 2 : row >= CR_SEG ? 1 : 0;
+            const int sy = y + r - 1, sx = x0 - 1 + (row - r * CR_SEG);
+            const bool in = (unsigned)sy < (unsigned)a.H && (unsigned)sx < (unsigned)a.W;
+            cp_async16(seg + g * CR_PLANE + row * 16, in ? a.x + (size_t)(sy * a.W + sx) * a.xs + a.xo + 8 * g : a.x,
+                       in);
+            row += drow;
+            g += dg;
+            if (g >= kg) {
+                g -= kg;
+                ++row;
+            }
+        }
+        cp_async_commit();
+    }
+    if (warp == 0) tmem_alloc(&s_tmem, ncols);
+    if (tid == 0) {
+        for (int i = 0; i < 2 * CR_RING + 1; ++i) mbar_init(&bar[i], 1);
+        fence_mbar_init();
+    }
+    cp_async_wait<0>();
+    fence_proxy_async();  // the segment writes before the tensor cores read them
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = s_tmem;
+    bool ok = true;
+    if (tid == 0) {
+        // Weight copies, issued and awaited in order: unit u is the whole
+        // resident block (u = 0) or ring tap u, on wbar[u % CR_RING] with
+        // phase parity (u / CR_RING) & 1; ring slot u % CR_RING is refilled
+        // with tap u + CR_RING once the MMAs of tap u are done, two taps later.
+        int wissued, wdone = 0;
+        if (resident) {
+            bulk_load_all(Bb, wsrc, 9 * bbytes, &wbar[0]);
+            wissued = 1;
+        } else {
+            for (int u = 0; u < CR_RING; ++u)
+                bulk_load_all(Bb + u * bbytes, wsrc + (size_t)u * bbytes, bbytes, &wbar[u]);
+            wissued = CR_RING;
+        }
+        const uint32_t idesc = umma_idesc_bf16(128, a.cout);
+        const uint32_t sseg = smem_u32(seg), sbo_b = (uint32_t)kg * 128;
+        for (int tap = 0; tap < 9 && ok; ++tap) {
+            if (!resident || tap == 0) {
+                const int u = resident ? 0 : tap;
+                if (!mbar_wait(&wbar[u % CR_RING], (u / CR_RING) & 1)) {
+                    ok = false;
+                    break;
+                }
+                wdone = u + 1;
+            }
+            tc_fence_after();
+            const uint32_t sa = sseg + (uint32_t)(((tap / 3) * CR_SEG + tap % 3) * 16);
+            const uint32_t sb = smem_u32(Bb + (resident ? tap : tap % CR_RING) * bbytes);
+            for (int kc = 0; kc < (a.cin >> 4); ++kc)
+                umma_bf16(tmem, umma_desc(sa + (uint32_t)(2 * kc * CR_PLANE), CR_PLANE, 128),
+                          umma_desc(sb + kc * 256, 128, sbo_b), idesc, (tap | kc) != 0);
+            if (!resident) {
+                umma_commit(&bar[tap % CR_RING]);
+                const int d = tap + 2 - CR_RING, u = tap + 2;
+                if (d >= 0 && u < 9) {  // ring slot of tap d takes tap u once d's MMAs are done
+                    if (!mbar_wait(&bar[d % CR_RING], (d / CR_RING) & 1)) {
+                        ok = false;
+                        break;
+                    }
+                    bulk_load_all(Bb + (u % CR_RING) * bbytes, wsrc + (size_t)u * bbytes, bbytes, &wbar[u % CR_RING]);
+                    wissued = u + 1;
+                }
+            }
+        }
+        umma_commit(done);  // also after a failure, so that the waits on it end
+        if (!ok) {
+            atomicExch(a.err, 1);
+            for (int u = wdone; u < wissued; ++u) mbar_wait(&wbar[u % CR_RING], (u / CR_RING) & 1);  // in flight
+        }
+    }
+    ok = mbar_wait(done, 0) && ok;
+    ok = !__syncthreads_or(!ok);
+    if (!ok && tid == 0) atomicExch(a.err, 1);
+    tc_fence_after();
+    if (ok) {
+        const int row = 32 * warp + lane;
+        const size_t pp = (size_t)y * a.W + x0 + row;
+        const uint32_t taddr = tmem + ((uint32_t)(32 * warp) << 16);
+        for (int c0 = 0; c0 < a.cout; c0 += 16) {
+            float v[16];
+            tmem_ld16(taddr + (uint32_t)c0, v);
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+                float t = v[i] + (a.bias ? a.bias[c0 + i] : 0.0f);
+                if (a.relu) t = fmaxf(t, 0.0f);
+                v[i] = t;
+            }
+            if (a.y) {
+                __align__(16) bf16 o[16];
+#pragma unroll
+                for (int i = 0; i < 16; ++i) o[i] = __float2bfloat16_rn(v[i]);
+                uint4* dst = reinterpret_cast<uint4*>(a.y + pp * a.ys + a.yo + c0);
+                dst[0] = reinterpret_cast<const uint4*>(o)[0];
+                dst[1] = reinterpret_cast<const uint4*>(o)[1];
+            } else {
+                float* dst = a.yf + pp * a.ys + a.yo + c0;
 #pragma unroll
                 for (int i = 0; i < 16; ++i) dst[i] = v[i];
             }
@@ -350,43 +621,64 @@ __global__ void k_bgrad_reduce(const float* part, int blocks, int cout, float* d
 // ---------------------------------------------------------------------------
 // Elementwise parts of the network.
 
-// out[Y, X] = mean of the 2x2 block of in (bf16, fp32 sum).
+// The resampling kernels move 8 bf16 (or 4 fp32) channels per thread; every
+// channel count, tensor stride and slice offset is a multiple of 8, so the
+// 16-byte accesses are aligned.  Per-element arithmetic is the scalar form's.
+
+// out[Y, X] = the mean of in's 2x2 block (in is a channel slice), summed as
+// ((a + b) + c) + d in fp32.
 __global__ void k_pool2(const bf16* in, int is, int io, int H, int W, int C, bf16* out) {
-    const int h = H / 2, w = W / 2;
-    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (size_t)h * w * C) return;
-    const int c = (int)(i % C);
-    const int q = (int)(i / C), Y = q / w, X = q - Y * w;
-    auto at = [&](int y, int x) { return __bfloat162float(in[(size_t)(y * W + x) * is + io + c]); };
-    const float s = ((at(2 * Y, 2 * X) + at(2 * Y, 2 * X + 1)) + at(2 * Y + 1, 2 * X)) + at(2 * Y + 1, 2 * X + 1);
-    out[(size_t)q * C + c] = __float2bfloat16_rn(0.25f * s);
+    const int h = H / 2, w = W / 2, g8 = C / 8;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;  // over h * w * C / 8
+    if (i >= h * w * g8) return;
+    const int g = i % g8, q = i / g8, Y = q / w, X = q - Y * w;
+    auto at = [&](int y, int x) { return *reinterpret_cast<const uint4*>(in + (size_t)(y * W + x) * is + io + 8 * g); };
+    const uint4 va = at(2 * Y, 2 * X), vb = at(2 * Y, 2 * X + 1), vc = at(2 * Y + 1, 2 * X), vd = at(2 * Y + 1, 2 * X + 1);
+    const bf16 *a = reinterpret_cast<const bf16*>(&va), *b = reinterpret_cast<const bf16*>(&vb),
+               *c = reinterpret_cast<const bf16*>(&vc), *d = reinterpret_cast<const bf16*>(&vd);
+    __align__(16) bf16 o[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const float s = ((__bfloat162float(a[k]) + __bfloat162float(b[k])) + __bfloat162float(c[k])) + __bfloat162float(d[k]);
+        o[k] = __float2bfloat16_rn(0.25f * s);
+    }
+    *reinterpret_cast<uint4*>(out + (size_t)q * C + 8 * g) = *reinterpret_cast<const uint4*>(o);
 }
 // g_in[2Y+i, 2X+j] += g_out[Y, X] / 4 (fp32 gradients; g_in is a channel slice).
 __global__ void k_pool2_bwd(const float* gout, int H, int W, int C, float* gin, int gs, int go) {
-    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (size_t)H * W * C) return;
-    const int c = (int)(i % C);
-    const int q = (int)(i / C), y = q / W, x = q - y * W;
-    const int w = W / 2;
-    gin[(size_t)q * gs + go + c] += 0.25f * gout[(size_t)((y >> 1) * w + (x >> 1)) * C + c];
+    const int g4 = C / 4;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;  // over H * W * C / 4
+    if (i >= H * W * g4) return;
+    const int g = i % g4, q = i / g4, y = q / W, x = q - y * W;
+    const float4 v = *reinterpret_cast<const float4*>(gout + (size_t)((y >> 1) * (W / 2) + (x >> 1)) * C + 4 * g);
+    float4* dst = reinterpret_cast<float4*>(gin + (size_t)q * gs + go + 4 * g);
+    float4 t = *dst;
+    t.x += 0.25f * v.x;
+    t.y += 0.25f * v.y;
+    t.z += 0.25f * v.z;
+    t.w += 0.25f * v.w;
+    *dst = t;
 }
 // out slice [y, x] = in[y / 2, x / 2] (nearest upsampling into a channel slice).
 __global__ void k_up2(const bf16* in, int H, int W, int C, bf16* out, int os, int oo) {
-    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (size_t)H * W * C) return;
-    const int c = (int)(i % C);
-    const int q = (int)(i / C), y = q / W, x = q - y * W;
-    out[(size_t)q * os + oo + c] = in[(size_t)((y >> 1) * (W / 2) + (x >> 1)) * C + c];
+    const int g8 = C / 8;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;  // over H * W * C / 8
+    if (i >= H * W * g8) return;
+    const int g = i % g8, q = i / g8, y = q / W, x = q - y * W;
+    *reinterpret_cast<uint4*>(out + (size_t)q * os + oo + 8 * g) =
+        *reinterpret_cast<const uint4*>(in + (size_t)((y >> 1) * (W / 2) + (x >> 1)) * C + 8 * g);
 }
-// g_in[Y, X] = sum of the 2x2 block of g_out's channel slice.
+// g_in[Y, X] = sum of the 2x2 block of g_out's channel slice, ((a + b) + c) + d.
 __global__ void k_up2_bwd(const float* gout, int gs, int go, int H, int W, int C, float* gin) {
-    const int h = H / 2, w = W / 2;
-    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (size_t)h * w * C) return;
-    const int c = (int)(i % C);
-    const int q = (int)(i / C), Y = q / w, X = q - Y * w;
-    auto at = [&](int y, int x) { return gout[(size_t)(y * W + x) * gs + go + c]; };
-    gin[(size_t)q * C + c] = ((at(2 * Y, 2 * X) + at(2 * Y, 2 * X + 1)) + at(2 * Y + 1, 2 * X)) + at(2 * Y + 1, 2 * X + 1);
+    const int h = H / 2, w = W / 2, g4 = C / 4;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;  // over h * w * C / 4
+    if (i >= h * w * g4) return;
+    const int g = i % g4, q = i / g4, Y = q / w, X = q - Y * w;
+    auto at = [&](int y, int x) { return *reinterpret_cast<const float4*>(gout + (size_t)(y * W + x) * gs + go + 4 * g); };
+    const float4 a = at(2 * Y, 2 * X), b = at(2 * Y, 2 * X + 1), c = at(2 * Y + 1, 2 * X), d = at(2 * Y + 1, 2 * X + 1);
+    *reinterpret_cast<float4*>(gin + (size_t)q * C + 4 * g) =
+        make_float4(((a.x + b.x) + c.x) + d.x, ((a.y + b.y) + c.y) + d.y, ((a.z + b.z) + c.z) + d.z,
+                    ((a.w + b.w) + c.w) + d.w);
 }
 // dy = bf16(g) where the forward output y > 0 (relu) or everywhere (relu = 0).
 __global__ void k_relu_bwd(const float* g, int gs, int go, const bf16* y, int ys, int yo, int npix, int C, int relu,
@@ -399,14 +691,17 @@ __global__ void k_relu_bwd(const float* g, int gs, int go, const bf16* y, int ys
     if (relu && !(__bfloat162float(y[p * ys + yo + c]) > 0.0f)) v = 0.0f;
     dy[i] = __float2bfloat16_rn(v);
 }
-// Weights for the backward pass over the data: wt[tap'][ci][co] = w[8 - tap'][co][ci].
+// BF16 weight tiles of the convolutions, each tap's cout x cin tile in the
+// K-major order the tensor cores read (so a CTA fetches it with one bulk
+// copy), and those of the backward pass over the data:
+// wt[tap'][ci][co] = w[8 - tap'][co][ci].
 __global__ void k_flip_transpose(const float* w32, int cin, int cout, bf16* w16, bf16* wt16) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= 9 * cin * cout) return;
     const int tap = i / (cout * cin), rem = i - tap * cout * cin, co = rem / cin, ci = rem - co * cin;
     const bf16 v = __float2bfloat16_rn(w32[i]);
-    w16[i] = v;
-    wt16[((size_t)(8 - tap) * cin + ci) * cout + co] = v;
+    w16[(size_t)tap * cout * cin + kmajor_index(co, ci, cin)] = v;
+    wt16[(size_t)(8 - tap) * cin * cout + kmajor_index(ci, co, cout)] = v;
 }
 // Per-block sums of g^2 (1024 elements per block), for the global-norm clip.
 __global__ void __launch_bounds__(256) k_sumsq(const float* g, int n, float* part) {
@@ -633,6 +928,18 @@ constexpr UConvSpec kUnetSpec[UNET_NCONV] = {
     {48, 16, 1}, {16, 16, 1},   // up to level 0 (32 up + 16 skip)
     {16, 16, 0},                // head
 };
+// Every convolution (forward, and backward over the data with cin and cout
+// swapped) fits one CTA's shared memory.
+constexpr bool unet_convs_fit() {
+    for (int i = 0; i < UNET_NCONV; ++i)
+        if (conv_smem_bytes(kUnetSpec[i].cin, kUnetSpec[i].cout) > CV_SMEM ||
+            conv_smem_bytes(kUnetSpec[i].cout, kUnetSpec[i].cin) > CV_SMEM ||
+            crow_smem_bytes(kUnetSpec[i].cin, kUnetSpec[i].cout, false) > CV_SMEM ||
+            crow_smem_bytes(kUnetSpec[i].cout, kUnetSpec[i].cin, false) > CV_SMEM)
+            return false;
+    return true;
+}
+static_assert(unet_convs_fit(), "a U-Net convolution exceeds the shared-memory budget");
 
 struct UNet {
     int device = 0, maxH = 0, maxW = 0;
@@ -739,6 +1046,39 @@ inline void unet_sync_weights(UNet& n, cudaStream_t st) {
     }
 }
 
+// SMs of the device, read when the network's kernels are set up (outside any
+// stream capture; the devices of a node are alike).
+inline int& conv_sm_count() {
+    static int n = 0;
+    return n;
+}
+inline bool conv_sm_count_init() {
+    int dev = 0, n = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return false;
+    conv_sm_count() = n;
+    return true;
+}
+
+// Widths that are a multiple of 128 take the row-tile kernel (input rows
+// staged once, no per-tap copies), the others the multistage one.  The row
+// kernel keeps all nine weight tiles resident when the grid is one CTA per SM
+// at most; larger grids take the ring, whose smaller footprint lets more CTAs
+// share an SM (each CTA allocates tensor memory, which throttles how fast CTAs
+// start on an SM, so the grids that need several rounds per SM want as many
+// resident at once as possible).
+inline void conv3x3_launch(const ConvArgs& a, cudaStream_t st) {
+    const int ntiles = a.H * a.W / 128;
+    if (a.W % 128 == 0) {
+        if (ntiles <= conv_sm_count() && crow_smem_bytes(a.cin, a.cout, true) <= CV_SMEM)
+            k_conv3x3_rows<true><<<ntiles, CV_THREADS, crow_smem_bytes(a.cin, a.cout, true) + count_launch(), st>>>(a);
+        else
+            k_conv3x3_rows<false><<<ntiles, CV_THREADS, crow_smem_bytes(a.cin, a.cout, false) + count_launch(), st>>>(a);
+    } else {
+        k_conv3x3_tc<<<(a.H * a.W + 127) / 128, CV_THREADS, conv_smem_bytes(a.cin, a.cout) + count_launch(), st>>>(a);
+    }
+}
+
 inline void unet_conv(UNet& n, int i, const bf16* x, int xs, int xo, int H, int W, bf16* y, int ys, int yo,
                       float* yf, cudaStream_t st) {
     ConvArgs a;
@@ -757,29 +1097,29 @@ inline void unet_conv(UNet& n, int i, const bf16* x, int xs, int xo, int H, int 
     a.cin = kUnetSpec[i].cin;
     a.cout = kUnetSpec[i].cout;
     a.err = n.err;
-    k_conv3x3_tc<<<(H * W + 127) / 128, CV_THREADS, conv_smem_bytes(a.cin, a.cout) + count_launch(), st>>>(a);
+    conv3x3_launch(a, st);
 }
 
 inline void unet_forward(UNet& n, int H, int W, cudaStream_t st) {
     const int H1 = H / 2, W1 = W / 2, H2 = H / 4, W2 = W / 4, H3 = H / 8, W3 = W / 8;
     unet_conv(n, 0, n.X0, 16, 0, H, W, n.t0, 16, 0, nullptr, st);
     unet_conv(n, 1, n.t0, 16, 0, H, W, n.cat0, 48, 32, nullptr, st);
-    k_pool2<<<lin_grid((size_t)H1 * W1 * 16), 256, count_launch(), st>>>(n.cat0, 48, 32, H, W, 16, n.p1);
+    k_pool2<<<lin_grid((size_t)H1 * W1 * 16 / 8), 256, count_launch(), st>>>(n.cat0, 48, 32, H, W, 16, n.p1);
     unet_conv(n, 2, n.p1, 16, 0, H1, W1, n.t1, 32, 0, nullptr, st);
     unet_conv(n, 3, n.t1, 32, 0, H1, W1, n.cat1, 96, 64, nullptr, st);
-    k_pool2<<<lin_grid((size_t)H2 * W2 * 32), 256, count_launch(), st>>>(n.cat1, 96, 64, H1, W1, 32, n.p2);
+    k_pool2<<<lin_grid((size_t)H2 * W2 * 32 / 8), 256, count_launch(), st>>>(n.cat1, 96, 64, H1, W1, 32, n.p2);
     unet_conv(n, 4, n.p2, 32, 0, H2, W2, n.t2, 64, 0, nullptr, st);
     unet_conv(n, 5, n.t2, 64, 0, H2, W2, n.cat2, 128, 64, nullptr, st);
-    k_pool2<<<lin_grid((size_t)H3 * W3 * 64), 256, count_launch(), st>>>(n.cat2, 128, 64, H2, W2, 64, n.p3);
+    k_pool2<<<lin_grid((size_t)H3 * W3 * 64 / 8), 256, count_launch(), st>>>(n.cat2, 128, 64, H2, W2, 64, n.p3);
     unet_conv(n, 6, n.p3, 64, 0, H3, W3, n.t3, 64, 0, nullptr, st);
     unet_conv(n, 7, n.t3, 64, 0, H3, W3, n.u3, 64, 0, nullptr, st);
-    k_up2<<<lin_grid((size_t)H2 * W2 * 64), 256, count_launch(), st>>>(n.u3, H2, W2, 64, n.cat2, 128, 0);
+    k_up2<<<lin_grid((size_t)H2 * W2 * 64 / 8), 256, count_launch(), st>>>(n.u3, H2, W2, 64, n.cat2, 128, 0);
     unet_conv(n, 8, n.cat2, 128, 0, H2, W2, n.t4, 64, 0, nullptr, st);
     unet_conv(n, 9, n.t4, 64, 0, H2, W2, n.u4, 64, 0, nullptr, st);
-    k_up2<<<lin_grid((size_t)H1 * W1 * 64), 256, count_launch(), st>>>(n.u4, H1, W1, 64, n.cat1, 96, 0);
+    k_up2<<<lin_grid((size_t)H1 * W1 * 64 / 8), 256, count_launch(), st>>>(n.u4, H1, W1, 64, n.cat1, 96, 0);
     unet_conv(n, 10, n.cat1, 96, 0, H1, W1, n.t5, 32, 0, nullptr, st);
     unet_conv(n, 11, n.t5, 32, 0, H1, W1, n.u5, 32, 0, nullptr, st);
-    k_up2<<<lin_grid((size_t)H * W * 32), 256, count_launch(), st>>>(n.u5, H, W, 32, n.cat0, 48, 0);
+    k_up2<<<lin_grid((size_t)H * W * 32 / 8), 256, count_launch(), st>>>(n.u5, H, W, 32, n.cat0, 48, 0);
     unet_conv(n, 12, n.cat0, 48, 0, H, W, n.t6, 16, 0, nullptr, st);
     unet_conv(n, 13, n.t6, 16, 0, H, W, n.u6, 16, 0, nullptr, st);
     unet_conv(n, 14, n.u6, 16, 0, H, W, nullptr, 16, 0, n.out, st);
@@ -830,7 +1170,7 @@ inline void unet_conv_bwd(UNet& n, int i, const bf16* x, int xs, int xo, const b
         a.cin = cout;
         a.cout = cin;
         a.err = n.err;
-        k_conv3x3_tc<<<(npix + 127) / 128, CV_THREADS, conv_smem_bytes(a.cin, a.cout) + count_launch(), st>>>(a);
+        conv3x3_launch(a, st);
     }
 }
 
@@ -840,22 +1180,22 @@ inline void unet_backward(UNet& n, int H, int W, cudaStream_t st) {
     unet_conv_bwd(n, 14, n.u6, 16, 0, nullptr, 16, 0, n.g_out, 16, 0, H, W, n.g_u6, 16, 0, st);
     unet_conv_bwd(n, 13, n.t6, 16, 0, n.u6, 16, 0, n.g_u6, 16, 0, H, W, n.g_t6, 16, 0, st);
     unet_conv_bwd(n, 12, n.cat0, 48, 0, n.t6, 16, 0, n.g_t6, 16, 0, H, W, n.g_cat0, 48, 0, st);
-    k_up2_bwd<<<lin_grid((size_t)H1 * W1 * 32), 256, count_launch(), st>>>(n.g_cat0, 48, 0, H, W, 32, n.g_u5);
+    k_up2_bwd<<<lin_grid((size_t)H1 * W1 * 32 / 4), 256, count_launch(), st>>>(n.g_cat0, 48, 0, H, W, 32, n.g_u5);
     unet_conv_bwd(n, 11, n.t5, 32, 0, n.u5, 32, 0, n.g_u5, 32, 0, H1, W1, n.g_t5, 32, 0, st);
     unet_conv_bwd(n, 10, n.cat1, 96, 0, n.t5, 32, 0, n.g_t5, 32, 0, H1, W1, n.g_cat1, 96, 0, st);
-    k_up2_bwd<<<lin_grid((size_t)H2 * W2 * 64), 256, count_launch(), st>>>(n.g_cat1, 96, 0, H1, W1, 64, n.g_u4);
+    k_up2_bwd<<<lin_grid((size_t)H2 * W2 * 64 / 4), 256, count_launch(), st>>>(n.g_cat1, 96, 0, H1, W1, 64, n.g_u4);
     unet_conv_bwd(n, 9, n.t4, 64, 0, n.u4, 64, 0, n.g_u4, 64, 0, H2, W2, n.g_t4, 64, 0, st);
     unet_conv_bwd(n, 8, n.cat2, 128, 0, n.t4, 64, 0, n.g_t4, 64, 0, H2, W2, n.g_cat2, 128, 0, st);
-    k_up2_bwd<<<lin_grid((size_t)H3 * W3 * 64), 256, count_launch(), st>>>(n.g_cat2, 128, 0, H2, W2, 64, n.g_u3);
+    k_up2_bwd<<<lin_grid((size_t)H3 * W3 * 64 / 4), 256, count_launch(), st>>>(n.g_cat2, 128, 0, H2, W2, 64, n.g_u3);
     unet_conv_bwd(n, 7, n.t3, 64, 0, n.u3, 64, 0, n.g_u3, 64, 0, H3, W3, n.g_t3, 64, 0, st);
     unet_conv_bwd(n, 6, n.p3, 64, 0, n.t3, 64, 0, n.g_t3, 64, 0, H3, W3, n.g_p3, 64, 0, st);
-    k_pool2_bwd<<<lin_grid((size_t)H2 * W2 * 64), 256, count_launch(), st>>>(n.g_p3, H2, W2, 64, n.g_cat2, 128, 64);
+    k_pool2_bwd<<<lin_grid((size_t)H2 * W2 * 64 / 4), 256, count_launch(), st>>>(n.g_p3, H2, W2, 64, n.g_cat2, 128, 64);
     unet_conv_bwd(n, 5, n.t2, 64, 0, n.cat2, 128, 64, n.g_cat2, 128, 64, H2, W2, n.g_t2, 64, 0, st);
     unet_conv_bwd(n, 4, n.p2, 32, 0, n.t2, 64, 0, n.g_t2, 64, 0, H2, W2, n.g_p2, 32, 0, st);
-    k_pool2_bwd<<<lin_grid((size_t)H1 * W1 * 32), 256, count_launch(), st>>>(n.g_p2, H1, W1, 32, n.g_cat1, 96, 64);
+    k_pool2_bwd<<<lin_grid((size_t)H1 * W1 * 32 / 4), 256, count_launch(), st>>>(n.g_p2, H1, W1, 32, n.g_cat1, 96, 64);
     unet_conv_bwd(n, 3, n.t1, 32, 0, n.cat1, 96, 64, n.g_cat1, 96, 64, H1, W1, n.g_t1, 32, 0, st);
     unet_conv_bwd(n, 2, n.p1, 16, 0, n.t1, 32, 0, n.g_t1, 32, 0, H1, W1, n.g_p1, 16, 0, st);
-    k_pool2_bwd<<<lin_grid((size_t)H * W * 16), 256, count_launch(), st>>>(n.g_p1, H, W, 16, n.g_cat0, 48, 32);
+    k_pool2_bwd<<<lin_grid((size_t)H * W * 16 / 4), 256, count_launch(), st>>>(n.g_p1, H, W, 16, n.g_cat0, 48, 32);
     unet_conv_bwd(n, 1, n.t0, 16, 0, n.cat0, 48, 32, n.g_cat0, 48, 32, H, W, n.g_t0, 16, 0, st);
     unet_conv_bwd(n, 0, n.X0, 16, 0, n.t0, 16, 0, n.g_t0, 16, 0, H, W, nullptr, 0, 0, st);
 }

@@ -480,7 +480,8 @@ EFL_API efl_status efl_unet_forward(efl_unet* net, uint32_t nx, uint32_t ny, con
 EFL_API efl_status efl_unet_gradients(efl_unet* net, uint32_t nx, uint32_t ny, const float* features,
                                       const float* target, const uint8_t* mask, float* loss, float* grads);
 /* Device time of one forward pass on the input already in the network (the
- * last recorded or uploaded one), averaged over reps passes. */
+ * last recorded or uploaded one), averaged over reps passes, each replayed
+ * from a CUDA graph of the pass (as a simulation step runs it). */
 EFL_API efl_status efl_unet_time_forward(efl_unet* net, uint32_t nx, uint32_t ny, uint32_t reps, float* ms);
 /* flags: EFL_UNET_WARM_START (warm-start sim's tolerance-driven solves),
  * EFL_UNET_RECORD (record each solve as a training sample); 0 detaches.

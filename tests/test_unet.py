@@ -8,7 +8,8 @@ from bevy_eulerian_fluid_b200 import _capi as capi
 from oracle import unet_ref
 
 
-def _random_case(seed, n=32, head_scale=0.05):
+def _random_case(seed, n=32, head_scale=0.05, nx=None):
+    nx = n if nx is None else nx
     rng = np.random.default_rng(seed)
     params = []
     for ci, co, relu in unet_ref.SPEC:
@@ -16,10 +17,10 @@ def _random_case(seed, n=32, head_scale=0.05):
         params.append(rng.normal(0, std, 9 * ci * co))
         params.append(rng.normal(0, 0.05, co))
     params = np.concatenate(params).astype(np.float32)
-    feats = np.zeros((n, n, 16), np.float32)
-    feats[:, :, :5] = rng.normal(0, 1, (n, n, 5))
-    target = rng.normal(0, 0.1, (n, n)).astype(np.float32)
-    mask = (rng.random((n, n)) < 0.7).astype(np.uint8)
+    feats = np.zeros((n, nx, 16), np.float32)
+    feats[:, :, :5] = rng.normal(0, 1, (n, nx, 5))
+    target = rng.normal(0, 0.1, (n, nx)).astype(np.float32)
+    mask = (rng.random((n, nx)) < 0.7).astype(np.uint8)
     return params, feats, target, mask
 
 
@@ -68,6 +69,35 @@ def test_unet_forward_matches_oracle(gpu_api):
     pred = net.forward(feats)
     ref = unet_ref.Net(params).forward(feats)
     assert _rel(pred, ref) < 1e-2
+
+
+@pytest.mark.gpu
+def test_unet_wide_rows_match_oracle(gpu_api):
+    """At 64 x 256 the 256- and 128-wide levels run the row-tile convolution
+    (widths that are a multiple of 128) and the 64- and 32-wide ones the
+    multistage one, forward and backward; both agree with the oracle."""
+    params, feats, target, mask = _random_case(6, n=64, nx=256)
+    net = capi.UNet(gpu_api, 256, 64, seed=5)
+    net.set_params(params)
+    ref = unet_ref.Net(params)
+    assert _rel(net.forward(feats), ref.forward(feats)) < 1e-2
+    loss, g = net.gradients(feats, target, mask)
+    rloss, rg = ref.backward(target, mask)
+    assert loss == pytest.approx(rloss, rel=1e-2)
+    cos = float(g.astype(np.float64) @ rg / (np.linalg.norm(g) * np.linalg.norm(rg)))
+    assert cos > 0.998 and _rel(g, rg) < 6e-2, (cos, _rel(g, rg))
+
+
+@pytest.mark.gpu
+def test_unet_forward_512_matches_oracle(gpu_api):
+    """At 512 x 512 the row-tile convolution streams its weights through the
+    ring at the 512- and 256-wide levels (2048 and 512 tiles) and keeps them
+    resident at the 128-wide one (128 tiles); the forward agrees with the
+    oracle."""
+    params, feats, _, _ = _random_case(8, n=512)
+    net = capi.UNet(gpu_api, 512, 512, seed=5)
+    net.set_params(params)
+    assert _rel(net.forward(feats), unet_ref.Net(params).forward(feats)) < 1e-2
 
 
 @pytest.mark.gpu
