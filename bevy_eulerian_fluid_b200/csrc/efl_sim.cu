@@ -2301,9 +2301,11 @@ efl_status unet_err(efl_unet* u, efl_status st, const std::string& m) {
 // Sets up the kernels' shared-memory limits once per device.
 bool unet_kernel_attrs() {
     return cudaFuncSetAttribute(k_conv3x3_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, CV_SMEM) == cudaSuccess &&
-           cudaFuncSetAttribute(k_conv3x3_rows<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, CV_SMEM) ==
+           cudaFuncSetAttribute(k_conv3x3_rows<true, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, CV_SMEM) ==
                cudaSuccess &&
-           cudaFuncSetAttribute(k_conv3x3_rows<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, CV_SMEM) ==
+           cudaFuncSetAttribute(k_conv3x3_rows<false, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, CV_SMEM) ==
+               cudaSuccess &&
+           cudaFuncSetAttribute(k_conv3x3_rows<false, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, CV_SMEM) ==
                cudaSuccess &&
            conv_sm_count_init() &&
            cudaFuncSetAttribute(k_wgrad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, WG_SMEM) == cudaSuccess;

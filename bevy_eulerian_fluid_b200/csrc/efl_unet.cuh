@@ -318,56 +318,62 @@ __global__ void __launch_bounds__(CV_THREADS) k_conv3x3_tc(ConvArgs a) {
 }
 
 // ---------------------------------------------------------------------------
-// 3x3 convolution for image widths that are a multiple of 128: a CTA's 128
-// output pixels are one stretch of one image row, so the input it needs is
-// three rows of 130 pixels (the stretch and one pixel either side, zero
-// outside the image), staged once.  In shared memory the 3 x 130 rows form
-// one plane per 8-channel group (16 bytes per row, planes CR_PLANE bytes
-// apart), and tap (dy, dx)'s A operand is the 128 rows from
-// (dy + 1) * 130 + dx + 1 on: a K-major non-swizzled operand with core
-// matrices 128 bytes apart along M (SBO) and one plane apart along K (LBO).
-// The nine taps' MMAs then go out back to back with no copies or block
-// barriers between them.
+// 3x3 convolution for image widths that are a multiple of 128: a CTA's
+// output pixels are 128-pixel stretches of one image row, so the input it
+// needs is three rows of those pixels and one pixel either side (130 for one
+// stretch; zero outside the image), staged once.  In shared memory the three
+// rows form one plane per 8-channel group (16 bytes per pixel), and tap
+// (dy, dx)'s A operand for a stretch is its 128 rows shifted by dx within
+// segment row dy: a K-major non-swizzled operand with core matrices 128 bytes
+// apart along M (SBO) and one plane apart along K (LBO), starting on a
+// 16-byte boundary.  The nine taps' MMAs then go out back to back with no
+// copies or block barriers between them.
 
-constexpr int CR_SEG = 130;                // pixels x0 - 1 .. x0 + 128 of one tap row
-constexpr int CR_PLANE = 3 * CR_SEG * 16;  // bytes per 8-channel group: 3 rows x 130 pixels x 16 bytes
+constexpr int CR_RING = 4;  // weight tiles in flight when not all nine are resident
 
-__host__ __device__ constexpr int crow_seg_bytes(int cin) { return ((cin >> 3) * CR_PLANE + 127) & ~127; }
-constexpr int CR_RING = 4;                 // weight tiles in flight when not all nine are resident
-__host__ __device__ constexpr int crow_smem_with(int cin, int cout, int btiles) {
-    return crow_seg_bytes(cin) + btiles * conv_b_bytes(cin, cout) + 128;
+// A CTA of the row-tile kernel covers TILES adjacent 128-pixel stretches of
+// one row (threads 128 * TILES); its input segment per tap row is those
+// pixels and one either side.
+__host__ __device__ constexpr int crow_seg_rows(int tiles) { return 128 * tiles + 2; }
+__host__ __device__ constexpr int crow_plane(int tiles) { return 3 * crow_seg_rows(tiles) * 16; }
+__host__ __device__ constexpr int crow_seg_bytes(int cin, int tiles) { return ((cin >> 3) * crow_plane(tiles) + 127) & ~127; }
+__host__ __device__ constexpr int crow_smem_with(int cin, int cout, int btiles, int tiles) {
+    return crow_seg_bytes(cin, tiles) + btiles * conv_b_bytes(cin, cout) + 128;
 }
-__host__ __device__ constexpr int crow_smem_bytes(int cin, int cout, bool resident) {
-    return crow_smem_with(cin, cout, resident ? 9 : CR_RING);
+__host__ __device__ constexpr int crow_smem_bytes(int cin, int cout, bool resident, int tiles) {
+    return crow_smem_with(cin, cout, resident ? 9 : CR_RING, tiles);
 }
 
-// RESIDENT: all nine weight tiles in one bulk copy, else the ring.
-template <bool RESIDENT>
-__global__ void __launch_bounds__(CV_THREADS) k_conv3x3_rows(ConvArgs a) {
+// RESIDENT: all nine weight tiles in one bulk copy, else the ring.  TILES
+// (1 or 2): 128-pixel stretches per CTA, each with its own accumulator; two
+// halve the CTAs (and tensor-memory allocations) of the large grids and share
+// one segment and one weight stream.
+template <bool RESIDENT, int TILES>
+__global__ void __launch_bounds__(CV_THREADS * TILES) k_conv3x3_rows(ConvArgs a) {
     extern __shared__ __align__(128) unsigned char cv_smem[];
+    constexpr int SEG = crow_seg_rows(TILES), PLANE = crow_plane(TILES), NT = CV_THREADS * TILES;
     const int kg = a.cin >> 3, bbytes = conv_b_bytes(a.cin, a.cout);
     constexpr bool resident = RESIDENT;
     unsigned char* seg = cv_smem;
-    unsigned char* Bb = cv_smem + crow_seg_bytes(a.cin);
+    unsigned char* Bb = cv_smem + crow_seg_bytes(a.cin, TILES);
     uint64_t* bar = reinterpret_cast<uint64_t*>(Bb + (resident ? 9 : CR_RING) * bbytes);  // [CR_RING]: slot's MMAs done
     uint64_t* wbar = bar + CR_RING;                                                         // [CR_RING]: slot's copy done
     uint64_t* done = bar + 2 * CR_RING;                                                     // every MMA done
     const unsigned char* wsrc = reinterpret_cast<const unsigned char*>(a.w);
     __shared__ uint32_t s_tmem;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int tiles_per_row = a.W >> 7;
-    const int y = blockIdx.x / tiles_per_row, x0 = (blockIdx.x - y * tiles_per_row) << 7;
-    const uint32_t ncols = tmem_cols(a.cout);
-    {  // segment row r * 130 + o holds pixel (y + r - 1, x0 - 1 + o); channel group fastest across threads
-        const int total = 3 * CR_SEG * kg;
-        const int drow = CV_THREADS / kg, dg = CV_THREADS - drow * kg;
+    const int ctas_per_row = a.W / (128 * TILES);
+    const int y = blockIdx.x / ctas_per_row, x0 = (blockIdx.x - y * ctas_per_row) * 128 * TILES;
+    const uint32_t acols = tmem_cols(a.cout), ncols = TILES * acols;
+    {  // segment row r * SEG + o holds pixel (y + r - 1, x0 - 1 + o); channel group fastest across threads
+        const int total = 3 * SEG * kg;
+        const int drow = NT / kg, dg = NT - drow * kg;
         int row = tid / kg, g = tid - row * kg;  // of element c = row * kg + g
-        for (int c = tid; c < total; c += CV_THREADS) {
-            const int r = row >= 2 * CR_SEG ? 2 : row >= CR_SEG ? 1 : 0;
-            const int sy = y + r - 1, sx = x0 - 1 + (row - r * CR_SEG);
+        for (int c = tid; c < total; c += NT) {
+            const int r = row >= 2 * SEG ? 2 : row >= SEG ? 1 : 0;
+            const int sy = y + r - 1, sx = x0 - 1 + (row - r * SEG);
             const bool in = (unsigned)sy < (unsigned)a.H && (unsigned)sx < (unsigned)a.W;
-            cp_async16(seg + g * CR_PLANE + row * 16, in ? a.x + (size_t)(sy * a.W + sx) * a.xs + a.xo + 8 * g : a.x,
-                       in);
+            cp_async16(seg + g * PLANE + row * 16, in ? a.x + (size_t)(sy * a.W + sx) * a.xs + a.xo + 8 * g : a.x, in);
             row += drow;
             g += dg;
             if (g >= kg) {
@@ -415,11 +421,14 @@ __global__ void __launch_bounds__(CV_THREADS) k_conv3x3_rows(ConvArgs a) {
                 wdone = u + 1;
             }
             tc_fence_after();
-            const uint32_t sa = sseg + (uint32_t)(((tap / 3) * CR_SEG + tap % 3) * 16);
             const uint32_t sb = smem_u32(Bb + (resident ? tap : tap % CR_RING) * bbytes);
-            for (int kc = 0; kc < (a.cin >> 4); ++kc)
-                umma_bf16(tmem, umma_desc(sa + (uint32_t)(2 * kc * CR_PLANE), CR_PLANE, 128),
-                          umma_desc(sb + kc * 256, 128, sbo_b), idesc, (tap | kc) != 0);
+            for (int t = 0; t < TILES; ++t) {
+                // tile t's rows start 128 * t further along the segment
+                const uint32_t sa = sseg + (uint32_t)(((tap / 3) * SEG + tap % 3 + 128 * t) * 16);
+                for (int kc = 0; kc < (a.cin >> 4); ++kc)
+                    umma_bf16(tmem + t * acols, umma_desc(sa + (uint32_t)(2 * kc * PLANE), PLANE, 128),
+                              umma_desc(sb + kc * 256, 128, sbo_b), idesc, (tap | kc) != 0);
+            }
             if (!resident) {
                 umma_commit(&bar[tap % CR_RING]);
                 const int d = tap + 2 - CR_RING, u = tap + 2;
@@ -443,18 +452,18 @@ __global__ void __launch_bounds__(CV_THREADS) k_conv3x3_rows(ConvArgs a) {
     ok = !__syncthreads_or(!ok);
     if (!ok && tid == 0) atomicExch(a.err, 1);
     tc_fence_after();
-    if (ok) {
-        const int row = 32 * warp + lane;
-        const size_t pp = (size_t)y * a.W + x0 + row;
-        const uint32_t taddr = tmem + ((uint32_t)(32 * warp) << 16);
+    if (ok) {  // warp w drains tile w / 4 from TMEM lanes 32 * (w % 4) ..
+        const int t = warp >> 2, row = 32 * (warp & 3) + lane;
+        const size_t pp = (size_t)y * a.W + x0 + 128 * t + row;
+        const uint32_t taddr = tmem + t * acols + ((uint32_t)(32 * (warp & 3)) << 16);
         for (int c0 = 0; c0 < a.cout; c0 += 16) {
             float v[16];
             tmem_ld16(taddr + (uint32_t)c0, v);
 #pragma unroll
             for (int i = 0; i < 16; ++i) {
-                float t = v[i] + (a.bias ? a.bias[c0 + i] : 0.0f);
-                if (a.relu) t = fmaxf(t, 0.0f);
-                v[i] = t;
+                float tv = v[i] + (a.bias ? a.bias[c0 + i] : 0.0f);
+                if (a.relu) tv = fmaxf(tv, 0.0f);
+                v[i] = tv;
             }
             if (a.y) {
                 __align__(16) bf16 o[16];
@@ -934,8 +943,8 @@ constexpr bool unet_convs_fit() {
     for (int i = 0; i < UNET_NCONV; ++i)
         if (conv_smem_bytes(kUnetSpec[i].cin, kUnetSpec[i].cout) > CV_SMEM ||
             conv_smem_bytes(kUnetSpec[i].cout, kUnetSpec[i].cin) > CV_SMEM ||
-            crow_smem_bytes(kUnetSpec[i].cin, kUnetSpec[i].cout, false) > CV_SMEM ||
-            crow_smem_bytes(kUnetSpec[i].cout, kUnetSpec[i].cin, false) > CV_SMEM)
+            crow_smem_bytes(kUnetSpec[i].cin, kUnetSpec[i].cout, false, 1) > CV_SMEM ||
+            crow_smem_bytes(kUnetSpec[i].cout, kUnetSpec[i].cin, false, 1) > CV_SMEM)
             return false;
     return true;
 }
@@ -1064,16 +1073,22 @@ inline bool conv_sm_count_init() {
 // staged once, no per-tap copies), the others the multistage one.  The row
 // kernel keeps all nine weight tiles resident when the grid is one CTA per SM
 // at most; larger grids take the ring, whose smaller footprint lets more CTAs
-// share an SM (each CTA allocates tensor memory, which throttles how fast CTAs
-// start on an SM, so the grids that need several rounds per SM want as many
-// resident at once as possible).
+// share an SM, and two 128-pixel stretches per CTA where the width allows
+// (each CTA allocates tensor memory, which throttles how fast CTAs start on an
+// SM, so the grids that need several rounds per SM want few, fat CTAs and as
+// many of them resident at once as possible).
 inline void conv3x3_launch(const ConvArgs& a, cudaStream_t st) {
     const int ntiles = a.H * a.W / 128;
     if (a.W % 128 == 0) {
-        if (ntiles <= conv_sm_count() && crow_smem_bytes(a.cin, a.cout, true) <= CV_SMEM)
-            k_conv3x3_rows<true><<<ntiles, CV_THREADS, crow_smem_bytes(a.cin, a.cout, true) + count_launch(), st>>>(a);
+        if (ntiles <= conv_sm_count() && crow_smem_bytes(a.cin, a.cout, true, 1) <= CV_SMEM)
+            k_conv3x3_rows<true, 1>
+                <<<ntiles, CV_THREADS, crow_smem_bytes(a.cin, a.cout, true, 1) + count_launch(), st>>>(a);
+        else if (a.W % 256 == 0 && crow_smem_bytes(a.cin, a.cout, false, 2) <= CV_SMEM)
+            k_conv3x3_rows<false, 2>
+                <<<ntiles / 2, 2 * CV_THREADS, crow_smem_bytes(a.cin, a.cout, false, 2) + count_launch(), st>>>(a);
         else
-            k_conv3x3_rows<false><<<ntiles, CV_THREADS, crow_smem_bytes(a.cin, a.cout, false) + count_launch(), st>>>(a);
+            k_conv3x3_rows<false, 1>
+                <<<ntiles, CV_THREADS, crow_smem_bytes(a.cin, a.cout, false, 1) + count_launch(), st>>>(a);
     } else {
         k_conv3x3_tc<<<(a.H * a.W + 127) / 128, CV_THREADS, conv_smem_bytes(a.cin, a.cout) + count_launch(), st>>>(a);
     }

@@ -73,11 +73,13 @@ def test_unet_forward_matches_oracle(gpu_api):
 
 @pytest.mark.gpu
 def test_unet_wide_rows_match_oracle(gpu_api):
-    """At 64 x 256 the 256- and 128-wide levels run the row-tile convolution
-    (widths that are a multiple of 128) and the 64- and 32-wide ones the
-    multistage one, forward and backward; both agree with the oracle."""
-    params, feats, target, mask = _random_case(6, n=64, nx=256)
-    net = capi.UNet(gpu_api, 256, 64, seed=5)
+    """At 128 x 512, forward and backward: the 512-wide level runs the row-tile
+    convolution with two stretches per CTA and the weight ring (512 tiles),
+    the 256- and 128-wide ones with resident weights, or the ring where nine
+    tiles do not fit (128 -> 64 channels), and the 64-wide one the multistage
+    kernel; all agree with the oracle."""
+    params, feats, target, mask = _random_case(6, n=128, nx=512)
+    net = capi.UNet(gpu_api, 512, 128, seed=5)
     net.set_params(params)
     ref = unet_ref.Net(params)
     assert _rel(net.forward(feats), ref.forward(feats)) < 1e-2
@@ -90,10 +92,10 @@ def test_unet_wide_rows_match_oracle(gpu_api):
 
 @pytest.mark.gpu
 def test_unet_forward_512_matches_oracle(gpu_api):
-    """At 512 x 512 the row-tile convolution streams its weights through the
-    ring at the 512- and 256-wide levels (2048 and 512 tiles) and keeps them
-    resident at the 128-wide one (128 tiles); the forward agrees with the
-    oracle."""
+    """At 512 x 512 the row-tile convolution covers two stretches per CTA and
+    streams its weights through the ring at the 512- and 256-wide levels
+    (1024 and 256 CTAs), and keeps them resident at the 128-wide one (128
+    tiles); the forward agrees with the oracle."""
     params, feats, _, _ = _random_case(8, n=512)
     net = capi.UNet(gpu_api, 512, 512, seed=5)
     net.set_params(params)
