@@ -330,6 +330,11 @@ __global__ void __launch_bounds__(CV_THREADS) k_conv3x3_tc(ConvArgs a) {
 // copies or block barriers between them.
 
 constexpr int CR_RING = 4;  // weight tiles in flight when not all nine are resident
+// Two stretches per CTA only while the CTA stays this small (three or more per
+// SM): at 48 -> 16 and 96 -> 32 channels the larger CTAs lost more residency
+// than the halved CTA count gained (40 vs 33 us and 30 vs 25 us at 512^2 and
+// 256^2), at cin <= 32 they gained (19 vs 25 us at 16 -> 16, 512^2).
+constexpr int CR_PAIR_SMEM = 64 * 1024;
 
 // A CTA of the row-tile kernel covers TILES adjacent 128-pixel stretches of
 // one row (threads 128 * TILES); its input segment per tap row is those
@@ -1083,7 +1088,7 @@ inline void conv3x3_launch(const ConvArgs& a, cudaStream_t st) {
         if (ntiles <= conv_sm_count() && crow_smem_bytes(a.cin, a.cout, true, 1) <= CV_SMEM)
             k_conv3x3_rows<true, 1>
                 <<<ntiles, CV_THREADS, crow_smem_bytes(a.cin, a.cout, true, 1) + count_launch(), st>>>(a);
-        else if (a.W % 256 == 0 && crow_smem_bytes(a.cin, a.cout, false, 2) <= CV_SMEM)
+        else if (a.W % 256 == 0 && crow_smem_bytes(a.cin, a.cout, false, 2) <= CR_PAIR_SMEM)
             k_conv3x3_rows<false, 2>
                 <<<ntiles / 2, 2 * CV_THREADS, crow_smem_bytes(a.cin, a.cout, false, 2) + count_launch(), st>>>(a);
         else
