@@ -143,7 +143,7 @@ struct ConvArgs {
     const float* bias;   // [cout] or null
     bf16* y;             // bf16 output [H*W][ys] at [yo, yo + cout), or null
     int ys, yo;
-    float* yf;           // fp32 output [H*W][ys] at [yo, yo + cout) (used when y is null)
+    float* yf;           // fp32 output [H*W][ys] at [yo, yo + cout) (used when y is null; ys, yo multiples of 4)
     int relu;
     int H, W, cin, cout;
     int* err;
@@ -306,9 +306,9 @@ __global__ void __launch_bounds__(CV_THREADS) k_conv3x3_tc(ConvArgs a) {
                 dst[0] = reinterpret_cast<const uint4*>(o)[0];
                 dst[1] = reinterpret_cast<const uint4*>(o)[1];
             } else {
-                float* dst = a.yf + (size_t)pp * a.ys + a.yo + c0;
+                float4* dst = reinterpret_cast<float4*>(a.yf + (size_t)pp * a.ys + a.yo + c0);  // 16-byte aligned
 #pragma unroll
-                for (int i = 0; i < 16; ++i) dst[i] = v[i];
+                for (int i = 0; i < 4; ++i) dst[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
             }
         }
     }
@@ -478,9 +478,9 @@ __global__ void __launch_bounds__(CV_THREADS * TILES) k_conv3x3_rows(ConvArgs a)
                 dst[0] = reinterpret_cast<const uint4*>(o)[0];
                 dst[1] = reinterpret_cast<const uint4*>(o)[1];
             } else {
-                float* dst = a.yf + pp * a.ys + a.yo + c0;
+                float4* dst = reinterpret_cast<float4*>(a.yf + pp * a.ys + a.yo + c0);  // 16-byte aligned
 #pragma unroll
-                for (int i = 0; i < 16; ++i) dst[i] = v[i];
+                for (int i = 0; i < 4; ++i) dst[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
             }
         }
     }
