@@ -96,7 +96,9 @@ EFL_DEV uint32_t kmajor_off(int row, int k, int K) {
 }
 
 // ---------------------------------------------------------------------------
-// 3x3 convolution, stride 1, zero padding.
+// 3x3 convolution, stride 1, zero padding: the multistage form, for any width
+// (the network runs it where the width is not a multiple of 128; the row-tile
+// form below covers the others).
 
 constexpr int CV_THREADS = 128, CV_MAX_CIN = 128, CV_MAX_COUT = 128;
 constexpr int CV_STAGES = 4;              // A stages: taps t + 1 and t + 2 load while tap t multiplies
