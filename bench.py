@@ -72,7 +72,8 @@ def parse():
     ap.add_argument("--c3-size", type=int, default=4096, help="grid of the C3 scale scene (4096 in the benchmark)")
     ap.add_argument("--batch-sims", type=int, default=96, help="simulations of the C4 batch (96 in the benchmark)")
     ap.add_argument("--no-pls", action="store_true")
-    ap.add_argument("--only", choices=["coupled", "microbench", "batch", "c3", "learned", "pls"], default=None,
+    ap.add_argument("--no-c1", action="store_true")
+    ap.add_argument("--only", choices=["coupled", "microbench", "batch", "c3", "learned", "pls", "c1"], default=None,
                     help="profiling aid: run one part only and print its numbers")
     return ap.parse_args()
 
@@ -95,14 +96,28 @@ def measured_peaks():
 
 def profile_traffic():
     """DRAM bytes per red-black iteration of the persistent mixed solve, from the
-    committed ncu summary of that kernel on coupled_512 (None if absent)."""
+    committed ncu summary of that kernel on coupled_512: (bytes, source label) or
+    (None, None) if absent.  The label names the file and a hash of its content,
+    so a stale profile is visible next to the number."""
+    import hashlib
     p = os.path.join(REPO, "profiles", "k_gsmix_persistent_coupled_512.txt")
     if not os.path.exists(p):
-        return None
-    for line in open(p):
+        return None, None
+    data = open(p, "rb").read()
+    tag = f"from committed ncu profile profiles/k_gsmix_persistent_coupled_512.txt (sha256 " \
+          f"{hashlib.sha256(data).hexdigest()[:12]}), not measured in this run"
+    for line in data.decode().splitlines():
         if line.startswith("dram_bytes_per_rb_iteration:"):
-            return float(line.split(":")[1])
-    return None
+            return float(line.split(":")[1]), tag
+    return None, None
+
+
+def config_of(size: int) -> dict:
+    """The workload description both arms print (identical keys and values)."""
+    return {"workload": f"coupled_{size}", "cells": size * size, "bodies": 24, "reinit": "jump flooding",
+            "solver": "RBGS (SOR 1.9) on an FP64 iterate to 1e-5 relative residual",
+            "coupling": "two-way: force read-back, host rigid integration, obstacle upload every step",
+            "l2": "GPU arm: flushed (256 MiB write) between timed steps, outside the timed region"}
 
 
 class ClockSampler:
@@ -201,10 +216,7 @@ def run_reference(args, world, rank):
     line = {"impl": "reference", "metric": "cell-steps/s to 1e-5 rel. residual", "value": val, "unit": "cell-steps/s",
             "n_gpus": world, "steps": n, "warmup": args.warmup, "ms_per_step": 1000 * el / n,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64", "data": "synthetic",
-            "config": {"workload": f"coupled_{args.size}", "cells": args.size * args.size, "bodies": 24,
-                       "reinit": "jump flooding",
-                       "solver": "RBGS (SOR 1.9) on an FP64 iterate to 1e-5 relative residual",
-                       "pressure_iterations_per_step": iters},
+            "config": config_of(args.size), "pressure_iterations_per_step": iters,
             "cpu_baseline": {"value": val, "unit": "cell-steps/s", "cores": cores, "kind": "port",
                              "sample": f"{n} coupled steps after {args.warmup} warm-up steps (budget {budget:.0f} s)"},
             "e2e": {"value": val, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -233,6 +245,11 @@ def main():
         return 0
     if args.only == "c3":
         print(json.dumps(c3_leg(capi.load(), torch, args, local, measured_peaks()[0])), flush=True)
+        return 0
+    if args.only == "c1":
+        print(json.dumps(c1_leg(capi.load(), torch, args, local, measured_peaks()[0],
+                                torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device=f"cuda:{local}"))),
+              flush=True)
         return 0
     if args.only == "pls":
         print(json.dumps(pls_leg(capi.load(), torch, args, local, measured_peaks()[0])), flush=True)
@@ -283,7 +300,7 @@ def main():
     # ---- one coupled loop: per step, events around the device step (value) and
     # around the whole coupled iteration (e2e); L2 flushed before each step, outside both.
     ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
-    iters = []
+    iters, proj_ms = [], []
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
@@ -304,6 +321,7 @@ def main():
             sim.set_obstacles(pack_obstacles(rigid.bodies))  # H2D: packed obstacles
             ev[k][2].record(stream)
             iters.append(int(st.pressure_iterations))
+            proj_ms.append(sim.projection_ms())  # the step's projection stage, CUDA events on the sim's stream
             if not st.converged:
                 print(f"warning: step {k} not converged (residual {st.residual})", file=sys.stderr)
         torch.cuda.synchronize()
@@ -319,33 +337,25 @@ def main():
     h2d = len(bodies) * 176
     d2h = capi.MAX_SOLIDS * 16
 
-    # ---- roofline of the dominant kernel: the persistent mixed-precision solve,
-    # re-run three times from the same pre-projection state.
-    for stage in range(capi.STAGE_UPDATE_SOLID, capi.STAGE_DIVERGENCE + 1):
-        sim.run_stage(stage, sc.dt)
-    p_in = sim.get(capi.FIELD_PRESSURE)
-    solve = []
-    for _ in range(3):
-        sim.set(capi.FIELD_PRESSURE, p_in)
-        with torch.cuda.stream(stream):
-            flush.zero_()
-        st = sim.run_stage(capi.STAGE_PROJECTION, sc.dt)
-        solve.append((sim.projection_ms(), int(st.pressure_iterations)))
-    solve_ms = statistics.median(x[0] for x in solve)
-    solve_it = solve[0][1]
-    it_ms = solve_ms / max(1, solve_it)
+    # ---- roofline of the dominant kernel over the timed steps: each step's projection stage is one
+    # k_gsmix_persistent launch (the whole tolerance-driven solve) plus the FP32 <-> FP64 copies around it.
+    solve_ms = sum(proj_ms)
+    solve_it = sum(iters)
     peak, peak_kind = measured_peaks()
     achieved = ALGO_BYTES_PER_CELL_ITER * sc.cells * solve_it / (solve_ms / 1e3) / 1e9
-    per_it = profile_traffic()
-    traffic = per_it * solve_it if per_it is not None else None
+    per_it, traffic_src = profile_traffic()
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                "frac": round(achieved / peak, 4), "traffic": traffic,
-                "kernel": "k_gsmix_persistent (one launch = one tolerance-driven solve)",
-                "launch_ms": round(solve_ms, 3), "iterations_per_launch": solve_it,
-                "iteration_us": round(it_ms * 1e3, 3), "peak_kind": peak_kind,
-                "note": f"32 B/cell/RB-iteration x {sc.cells} cells x {solve_it} iterations per launch; "
-                        "the launch keeps its tiles in shared memory, so DRAM traffic (ncu) is far "
-                        "below the algorithmic bytes"}
+                "frac": round(achieved / peak, 4),
+                "traffic": round(per_it * solve_it / args.steps) if per_it is not None else None,
+                "traffic_source": traffic_src,
+                "algorithmic_bytes_per_launch": round(ALGO_BYTES_PER_CELL_ITER * sc.cells * solve_it / args.steps),
+                "kernel": "k_gsmix_persistent (one launch per step = one tolerance-driven solve)",
+                "launch_ms": round(solve_ms / args.steps, 4), "iterations_per_launch": round(solve_it / args.steps, 1),
+                "iteration_us": round(solve_ms * 1e3 / max(1, solve_it), 4), "peak_kind": peak_kind,
+                "timing": "CUDA events around every timed step's projection stage (efl_projection_ms), summed",
+                "note": f"32 B/cell/RB-iteration x {sc.cells} cells x RB iterations of the timed steps / their "
+                        "projection time; the launch keeps its tiles in shared memory, so DRAM traffic (ncu) is "
+                        "far below the algorithmic bytes"}
 
     # ---- the same coupled loop with the MGPCG projection (an extension), device time per step
     alt = None
@@ -355,6 +365,9 @@ def main():
         dev_rbgs = coupled_device(api, torch, args, local, flush, capi.PROJECTION_GAUSS_SEIDEL)
         dev_mgpcg = coupled_device(api, torch, args, local, flush, capi.PROJECTION_MGPCG)
 
+    c1 = None
+    if not args.no_c1 and rank == 0 and args.only is None:
+        c1 = c1_leg(api, torch, args, local, peak, flush)
     micro = None
     if not args.no_microbench and rank == 0 and args.only is None:
         micro = microbench(api, stream, torch, peak)
@@ -382,36 +395,148 @@ def main():
     if world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args.size, args.warmup, min(args.steps, 3))
 
+    legs = {"coupled_mgpcg": alt, "coupled_device_coupling": ({"rbgs": dev_rbgs, "mgpcg": dev_mgpcg} if dev_rbgs else None),
+            "c1": c1, "microbench": micro, "batch": batch, "c3": c3, "learned": lw, "particle_levelset": pls}
+    # Each leg's full record on a line of its own (prefixed, so it is not the result line), then the
+    # result line with a compact summary of every leg last.
+    for name, leg in legs.items():
+        if leg:
+            print(f"# leg {name} " + json.dumps(leg), flush=True)
     line = {
         "metric": "cell-steps/s to 1e-5 rel. residual", "value": value, "unit": "cell-steps/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64", "data": "synthetic",
-        "config": {"workload": f"coupled_{args.size}", "cells": sc.cells, "bodies": len(bodies),
-                   "reinit": "jump flooding", "solver": "RBGS (SOR 1.9) on an FP64 iterate to 1e-5 relative residual",
-                   "pressure_iterations_per_step": iters, "l2": "flushed (256 MiB write) between timed steps",
-                   "parallelism": f"replicas x{world}"},
+        "config": config_of(args.size), "pressure_iterations_per_step": iters,
+        "parallelism": f"replicas x{world}",
         "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": e2e_ms / args.steps},
         "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(), "gpu_launches": int(launches),
+        "legs": compact_legs(legs),
     }
-    if micro:
-        line["microbench"] = micro
-    if alt:
-        line["coupled_mgpcg"] = alt
-    if dev_rbgs:
-        line["coupled_device_coupling"] = {"note": "bodies integrated on the GPU (no per-step force read-back or "
-                                                   "obstacle upload); the body states read back each step",
-                                           "rbgs": dev_rbgs, "mgpcg": dev_mgpcg}
-    if batch:
-        line["batch"] = batch
-    if c3:
-        line["c3"] = c3
-    if lw:
-        line["learned"] = lw
-    if pls:
-        line["particle_levelset"] = pls
     print(json.dumps(line), flush=True)
     return 0
+
+
+def _r(x, n=4):
+    return None if x is None else round(x, n)
+
+
+def compact_legs(legs: dict) -> dict:
+    """A few numbers of every leg for the result line (the full records are printed above it)."""
+    out = {}
+    if legs.get("c1"):
+        c = legs["c1"]
+        out["c1_dam_break_256"] = {"value": _r(c["value"], 0), "ms_per_step": _r(c["ms_per_step"]),
+                                   "hbm_frac": c["roofline"]["frac"], "residual_mean": _r(c["residual"]["mean"], 6),
+                                   "cpu_value": _r((c.get("cpu_baseline") or {}).get("value"), 0)}
+    if legs.get("microbench"):
+        m = legs["microbench"]
+        out["microbench_4096"] = {"ms_per_rb_iteration": m["ms_per_rb_iteration"], "hbm_frac": m["frac_of_hbm"]}
+    if legs.get("batch"):
+        b = legs["batch"]
+        out["batch_96"] = {"batched": _r(b["value"], 0), "plain": _r(b["plain_value"], 0),
+                           "speedup_vs_plain": b["speedup_vs_plain"],
+                           "solve_ms_per_step": {k: _r(v, 3) for k, v in b["pressure_solve_ms_per_step"].items()}}
+        if b.get("learned"):
+            out["batch_96"]["learned"] = {k: b["learned"][k] for k in ("value", "speedup_vs_plain")
+                                          if k in b["learned"]}
+    if legs.get("c3"):
+        c = legs["c3"]
+        out["c3_scale_4096"] = {"mgpcg": _r(c["mgpcg"]["value"], 0), "vcycles": _r(c["vcycles"]["value"], 0),
+                                "v_cycle_hbm_frac": c["vcycles"]["v_cycle_rate"]["frac"],
+                                "cpu_value": _r((c.get("cpu_baseline") or {}).get("value"), 0)}
+    if legs.get("coupled_mgpcg"):
+        out["coupled_mgpcg"] = {"value": _r(legs["coupled_mgpcg"]["value"], 0)}
+    if legs.get("learned"):
+        l = legs["learned"]
+        out["learned"] = {"solve_ms_per_step": {k: _r(v, 3) for k, v in l["pressure_solve_ms_per_step"].items()},
+                          "c5_solve_ms_per_step": {k: _r(v, 3) for k, v in
+                                                   l["c5_evaluation"]["pressure_solve_ms_per_step"].items()},
+                          "forward_ms_512": l["forward"]["ms"]}
+    if legs.get("particle_levelset"):
+        p = legs["particle_levelset"]
+        out["particle_levelset"] = {"particle_steps_per_s": _r(p["particle_steps_per_s"], 0),
+                                    "pass_ms": p["ms_per_step"]["particle_pass"]}
+    return out
+
+
+C1_STEPS = 600
+C1_BYTES_PER_CELL_STEP = 1200  # algorithmic bytes of one full step at the reference defaults (GS 20, FIM(10))
+
+
+def c1_cpu_baseline(steps: int = 60):
+    """The CPU oracle on dam_break_256: the first `steps` steps after the init sequence."""
+    from bevy_eulerian_fluid_b200 import scenes
+    from oracle import py_oracle
+    api = py_oracle.load()
+    py_oracle.set_threads(os.cpu_count() or 1)
+    sc = scenes.dam_break(256)
+    sim = sc.make(api)
+    sim.step(sc.dt)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        sim.step(sc.dt)
+    el = time.perf_counter() - t0
+    sim.close()
+    cores = py_oracle.get_threads()
+    return {"value": sc.cells * steps / el, "unit": "cell-steps/s", "cores": cores, "kind": "port",
+            "sample": f"the first {steps} of the 600 steps after the init sequence on the CPU oracle, {cores} host "
+                      f"threads, {el:.2f} s"}
+
+
+def c1_leg(api, torch, args, local, peak, flush):
+    """C1 (the reference's CPU-runnable case): dam_break_256, Gauss-Seidel 20 at weight 1.9, FIM(10), 600
+    steps from the init sequence through efl_step (graph replay), CUDA events around every step, L2 flushed
+    (256 MiB write) before each step.  A warm-up handle runs --warmup steps first.  The achieved residual
+    is read after every projection on a second handle stepped stage by stage (bit-identical states)."""
+    from bevy_eulerian_fluid_b200 import _capi as capi
+    from bevy_eulerian_fluid_b200 import scenes
+    sc = scenes.dam_break(256)
+    sc.cfg.device = local
+    warm = sc.make(api)
+    for _ in range(1 + args.warmup):
+        warm.step(sc.dt)
+    warm.close()
+    sim = sc.make(api)
+    stream = torch.cuda.ExternalStream(sim.stream(), device=f"cuda:{local}")
+    sim.step(sc.dt)  # init sequence
+    torch.cuda.synchronize()
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(C1_STEPS)]
+    l0 = api.kernel_launches()
+    for k in range(C1_STEPS):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        ev[k][0].record(stream)
+        sim.step(sc.dt)
+        ev[k][1].record(stream)
+    torch.cuda.synchronize()
+    launches = api.kernel_launches() - l0
+    ms = sum(a.elapsed_time(b) for a, b in ev)
+    vol = sim.fluid_volume()
+    sim.close()
+    res = []
+    sim = sc.make(api)
+    sim.step(sc.dt)
+    for k in range(C1_STEPS):
+        for stage in range(capi.STAGE_UPDATE_SOLID, capi.STAGE_SOLID_FORCES + 1):
+            sim.run_stage(stage, sc.dt)
+            if stage == capi.STAGE_PROJECTION:
+                res.append(sim.residual()[0])
+    sim.close()
+    achieved = C1_BYTES_PER_CELL_STEP * sc.cells * C1_STEPS / (ms / 1e3) / 1e9
+    out = {"workload": "dam_break_256: 256^2, Gauss-Seidel 20 (weight 1.9), FIM(10), dt 1/60, 600 steps from init",
+           "value": sc.cells * C1_STEPS / (ms / 1e3), "unit": "cell-steps/s", "steps": C1_STEPS,
+           "ms_per_step": ms / C1_STEPS, "gpu_launches_per_step": launches / C1_STEPS,
+           "l2": "flushed (256 MiB write) before each step", "fluid_volume_end": vol,
+           "residual": {"mean": float(np.mean(res)), "max": float(np.max(res)), "last": float(res[-1]),
+                        "note": "relative residual after each step's 20 red-black iterations"},
+           "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                        "frac": round(achieved / peak, 4),
+                        "note": f"{C1_BYTES_PER_CELL_STEP} algorithmic B per cell per full step x cells x steps / "
+                                "device time of the steps"}}
+    if not args.no_cpu_baseline:
+        out["cpu_baseline"] = c1_cpu_baseline()
+    return out
 
 
 def batch_shard(n_sims: int, world: int, rank: int):

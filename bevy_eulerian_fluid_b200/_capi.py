@@ -141,6 +141,7 @@ SIGNATURES = {
     "synchronize": (C.c_int, ["X"]),
     "residual": (C.c_int, ["X", C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "fluid_volume": (C.c_int, ["X", C.POINTER(C.c_uint64)]),
+    "divergence_norms": (C.c_int, ["X", C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "velocity_magnitude": (C.c_int, ["X", C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "set_particle_levelset": (C.c_int, ["X", C.c_int32]),
     "particle_counts": (C.c_int, ["X", C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
@@ -162,6 +163,8 @@ SIGNATURES = {
     "batch_tiles": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                               C.POINTER(C.c_double)]),
     "projection_ms": (C.c_int, ["X", C.POINTER(C.c_float)]),
+    "set_wait_limits": (C.c_int, ["X", C.c_uint64, C.c_uint64]),
+    "batch_set_wait_limits": (C.c_int, [C.c_void_p, C.c_uint64]),
     "set_graph_capture": (C.c_int, ["X", C.c_int32]),
     "set_rigid_bodies": (C.c_int, ["X", C.POINTER(RigidBodyC), C.c_uint32, C.c_double, C.c_double, C.c_uint32]),
     "get_rigid_bodies": (C.c_int, ["X", C.POINTER(RigidBodyC), C.c_uint32]),
@@ -181,7 +184,8 @@ SIGNATURES = {
 # Functions of efl.h that the oracle restatement does not mirror.
 PRODUCT_ONLY = {"abi_version", "default_config", "field_device_ptr", "stream", "synchronize", "kernel_launches",
                 "pressure_sweeps", "residual_norms_noalloc", "batch_create", "batch_destroy", "batch_last_error",
-                "batch_sim", "batch_step", "batch_projection_ms", "batch_set_tiles", "batch_tiles", "projection_ms", "set_graph_capture", "set_rigid_bodies", "get_rigid_bodies",
+                "batch_sim", "batch_step", "batch_projection_ms", "batch_set_tiles", "batch_tiles", "batch_set_wait_limits",
+                "projection_ms", "set_graph_capture", "set_wait_limits", "set_rigid_bodies", "get_rigid_bodies",
                 "unet_create", "unet_destroy", "unet_last_error", "unet_num_params", "unet_get_params",
                 "unet_set_params", "unet_forward", "unet_gradients", "unet_attach", "unet_train_step",
                 "unet_time_forward"}
@@ -382,6 +386,12 @@ class Sim:
         self._check(self.api.fluid_volume(self.h, C.byref(c)))
         return c.value
 
+    def divergence_norms(self):
+        """(L2, Linf) of the divergence of the current velocity over the counted cells (1/s)."""
+        a, b = C.c_double(), C.c_double()
+        self._check(self.api.divergence_norms(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
     def velocity_magnitude(self):
         """(min over fluid cells, max) of the cell-centred speed, as the reference's diagnostics compute them."""
         a, b = C.c_float(), C.c_float()
@@ -453,6 +463,10 @@ class Sim:
     def pressure_sweeps(self, precision: int, iterations: int):
         self._check(self.api.pressure_sweeps(self.h, precision, iterations))
 
+    def set_wait_limits(self, barrier_polls: int = 0, mbarrier_polls: int = 0):
+        """Polls of the device-side waits before they give up (0 = the defaults)."""
+        self._check(self.api.set_wait_limits(self.h, barrier_polls, mbarrier_polls))
+
 
 class Batch:
     """N independent simulations stepped together (efl_batch_*): one shared
@@ -501,6 +515,10 @@ class Batch:
         cost = (C.c_double * 4)()
         self._check(self.api.batch_tiles(self.h, C.byref(tx), C.byref(ty), C.byref(k), cost))
         return (tx.value, ty.value, k.value), list(cost)
+
+    def set_wait_limits(self, barrier_polls: int = 0):
+        """Grid-barrier polls of the batched solve before it gives up (0 = the default)."""
+        self._check(self.api.batch_set_wait_limits(self.h, barrier_polls))
 
     def projection_ms(self) -> float:
         """Device time of the last batched pressure solve (ms)."""

@@ -49,6 +49,7 @@ struct BatchParams {
     int* work_count;
     BatchState* state;  // one per simulation
     GridBarrier* barrier;
+    long long spin_limit;  // grid-barrier polls before giving up
 };
 
 template <int EX, int EY>
@@ -182,7 +183,7 @@ __global__ void __launch_bounds__(BT_THREADS, 2) k_batch_mix(BatchParams P) {
         }
     }
     __syncthreads();
-    bool ok = grid_barrier(P.barrier, nb);
+    bool ok = grid_barrier(P.barrier, nb, P.spin_limit);
     int cur = 0;
     unsigned iters = 0;
     bool first = true, first_apply = true;
@@ -218,7 +219,7 @@ __global__ void __launch_bounds__(BT_THREADS, 2) k_batch_mix(BatchParams P) {
                 }
             }
             first_apply = false;
-            ok = grid_barrier(P.barrier, nb);
+            ok = grid_barrier(P.barrier, nb, P.spin_limit);
             if (!ok) break;
         }
         if (blockIdx.x == 0 && threadIdx.x == 0) *P.work_count = 0;  // nobody reads it in this phase
@@ -295,7 +296,7 @@ __global__ void __launch_bounds__(BT_THREADS, 2) k_batch_mix(BatchParams P) {
             }
             __syncthreads();
         }
-        ok = grid_barrier(P.barrier, nb);
+        ok = grid_barrier(P.barrier, nb, P.spin_limit);
         if (!ok) break;
         // Per-simulation reduction (CTA 0, one warp per simulation, a fixed order).
         if (blockIdx.x == 0) {
@@ -328,7 +329,7 @@ __global__ void __launch_bounds__(BT_THREADS, 2) k_batch_mix(BatchParams P) {
             __syncthreads();
             if (threadIdx.x == 0) *P.n_active = s_cnt;
         }
-        ok = grid_barrier(P.barrier, nb);
+        ok = grid_barrier(P.barrier, nb, P.spin_limit);
         if (!ok) break;
         if (threadIdx.x == 0) s_any = __ldcg(P.n_active);
         for (int j = threadIdx.x; j < nown; j += BT_THREADS) s_act[j] = s_act[j] && __ldcg(&P.state[s_sim[j]].active);
@@ -349,7 +350,7 @@ __global__ void __launch_bounds__(BT_THREADS, 2) k_batch_mix(BatchParams P) {
             const int j = s_list[q];
             P.work[s_cnt + q] = make_int2(s_sim[j], (int)blockIdx.x + j * nb);
         }
-        ok = grid_barrier(P.barrier, nb);
+        ok = grid_barrier(P.barrier, nb, P.spin_limit);
         const int nwork = __ldcg(P.work_count);
         unsigned todo = min(P.check_interval, P.max_iters - iters);
         while (ok && todo > 0) {
@@ -433,7 +434,7 @@ __global__ void __launch_bounds__(BT_THREADS, 2) k_batch_mix(BatchParams P) {
                 }
                 __syncthreads();
             }
-            ok = grid_barrier(P.barrier, nb);
+            ok = grid_barrier(P.barrier, nb, P.spin_limit);
             cur ^= 1;
             todo -= (unsigned)kk;
         }

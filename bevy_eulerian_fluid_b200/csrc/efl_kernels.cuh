@@ -572,6 +572,57 @@ __global__ void __launch_bounds__(NORM_THREADS)
         partials[blockIdx.x] = make_double2(tr, tb);
     }
 }
+// Post-projection divergence diagnostic: the operator of divergence.wgsl:16-42
+// applied to the projected velocity (u0, v0) at the cells the residual
+// counts (phi < 0, not fully solid).  Per block: x = FP64 sum of squares,
+// y = the largest magnitude; k_div_norm_finalize sums x in block order and
+// takes the maximum of y (deterministic).
+__global__ void __launch_bounds__(NORM_THREADS)
+    k_divergence_norm(PF u0, PF v0, PF us, PF vs, PF fu, PF fv, PF ls0, float dx, Dom d, double2* partials) {
+    __shared__ double ss[NORM_THREADS / 32], sm[NORM_THREADS / 32];
+    const int n = d.nx * d.ny;
+    double a2 = 0.0, amax = 0.0;
+    for (int i = blockIdx.x * NORM_THREADS + threadIdx.x; i < n; i += gridDim.x * NORM_THREADS) {
+        const int y = i / d.nx, x = i - y * d.nx;
+        if (!(ls0.at(x, y) < 0.0f)) continue;
+        const float fx0 = fu.ld(x, y), fx1 = fu.ld(x + 1, y), fy0 = fv.ld(x, y), fy1 = fv.ld(x, y + 1);
+        if (fx0 == 0.0f && fx1 == 0.0f && fy0 == 0.0f && fy1 == 0.0f) continue;
+        const float du_f = fx1 * u0.ld(x + 1, y) - fx0 * u0.ld(x, y);
+        const float dv_f = fy1 * v0.ld(x, y + 1) - fy0 * v0.ld(x, y);
+        const float du_s = (1.0f - fx1) * us.ld(x + 1, y) - (1.0f - fx0) * us.ld(x, y);
+        const float dv_s = (1.0f - fy1) * vs.ld(x, y + 1) - (1.0f - fy0) * vs.ld(x, y);
+        const double dv = (double)(-(du_f + dv_f + du_s + dv_s) / dx);
+        a2 += dv * dv;
+        amax = fmax(amax, fabs(dv));
+    }
+    a2 = warp_sum(a2);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) amax = fmax(amax, __shfl_down_sync(0xffffffffu, amax, o));
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) {
+        ss[w] = a2;
+        sm[w] = amax;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t2 = 0.0, tm = 0.0;
+        for (int k = 0; k < NORM_THREADS / 32; ++k) {
+            t2 += ss[k];
+            tm = fmax(tm, sm[k]);
+        }
+        partials[blockIdx.x] = make_double2(t2, tm);
+    }
+}
+__global__ void k_div_norm_finalize(const double2* partials, int n, double* out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double a2 = 0.0, m = 0.0;
+    for (int i = 0; i < n; ++i) {
+        a2 += partials[i].x;
+        m = fmax(m, partials[i].y);
+    }
+    out[0] = a2;
+    out[1] = m;
+}
 __global__ void k_norm_finalize(const double2* partials, int n, double* out) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     double r = 0.0, b = 0.0;

@@ -1470,6 +1470,21 @@ efl_status efl_step(efl_sim* s, float dt, efl_step_stats* st) {
     return ret;
 }
 
+efl_status efl_set_wait_limits(efl_sim* s, uint64_t barrier_polls, uint64_t mbarrier_polls) {
+    if (!s) return set_err(nullptr, EFL_ERR_INVALID_ARGUMENT, "null sim");
+    const uint64_t cap = (uint64_t)1 << 40;
+    if (barrier_polls > cap || mbarrier_polls > cap)
+        return set_err(s, EFL_ERR_INVALID_ARGUMENT, "wait limits above 2^40 polls");
+    cudaSetDevice(s->device);
+    CU(cudaStreamSynchronize(s->stream));
+    s->solver.spin_limit = (long long)barrier_polls;  // 0: kBarrierSpinLimit
+    const long long mb = mbarrier_polls ? (long long)mbarrier_polls : kMbarSpinLimit;
+    s->tma.wait_limit = mb;
+    s->tma_pre.wait_limit = mb;
+    ++s->graph_epoch;  // captured sweeps hold the old limit as a kernel argument
+    return EFL_OK;
+}
+
 efl_status efl_set_graph_capture(efl_sim* s, int32_t enable) {
     if (!s) return set_err(nullptr, EFL_ERR_INVALID_ARGUMENT, "null sim");
     cudaSetDevice(s->device);
@@ -1622,6 +1637,21 @@ efl_status efl_residual(efl_sim* s, double* rel, double* nr, double* nb) {
     if (nr) *nr = std::sqrt(R);
     if (nb) *nb = std::sqrt(B);
     if (rel) *rel = rel_from(R, B);
+    return EFL_OK;
+}
+
+efl_status efl_divergence_norms(efl_sim* s, double* l2, double* linf) {
+    if (!s) return set_err(nullptr, EFL_ERR_INVALID_ARGUMENT, "null sim");
+    cudaSetDevice(s->device);
+    k_divergence_norm<<<s->n_partials, NORM_THREADS, count_launch(), s->stream>>>(s->u0, s->v0, s->us, s->vs, s->fu,
+                                                                                 s->fv, s->ls0, s->U.dx, s->dom(),
+                                                                                 s->d_partials);
+    k_div_norm_finalize<<<1, 32, count_launch(), s->stream>>>(s->d_partials, s->n_partials, s->d_norms);
+    LAUNCH_CHECK();
+    double a2, m;
+    TRY(read_norms(s, &a2, &m));
+    if (l2) *l2 = std::sqrt(a2);
+    if (linf) *linf = m;
     return EFL_OK;
 }
 
@@ -1813,15 +1843,33 @@ static __device__ __align__(256) double2 g_noalloc_partials[kNoAllocMaxBlocks];
 std::mutex g_noalloc_mu;
 double2* g_noalloc_addr[kNoAllocMaxDevices] = {};
 
-__global__ void k_norm_finalize_rel(const double2* partials, int n, double* out) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+// One block sums the per-block partials: thread t adds partials t, t + 256,
+// ... in order, then a shared-memory tree halves the 256 sums in a fixed
+// pattern, so the result does not depend on scheduling.
+constexpr int kNoAllocFinalizeThreads = 256;
+__global__ void __launch_bounds__(kNoAllocFinalizeThreads)
+    k_norm_finalize_rel(const double2* partials, int n, double* out) {
+    __shared__ double sr[kNoAllocFinalizeThreads], sb[kNoAllocFinalizeThreads];
+    const int t = threadIdx.x;
     double r = 0.0, b = 0.0;
-    for (int i = 0; i < n; ++i) {
-        r += partials[i].x;
-        b += partials[i].y;
+    for (int i = t; i < n; i += kNoAllocFinalizeThreads) {
+        const double2 q = partials[i];
+        r += q.x;
+        b += q.y;
     }
-    double nr = sqrt(r), nb = sqrt(b);
-    out[0] = b > 0.0 ? nr / nb : (r > 0.0 ? INFINITY : 0.0);
+    sr[t] = r;
+    sb[t] = b;
+    __syncthreads();
+    for (int h = kNoAllocFinalizeThreads / 2; h > 0; h >>= 1) {
+        if (t < h) {
+            sr[t] += sr[t + h];
+            sb[t] += sb[t + h];
+        }
+        __syncthreads();
+    }
+    if (t != 0) return;
+    const double nr = sqrt(sr[0]), nb = sqrt(sb[0]);
+    out[0] = sb[0] > 0.0 ? nr / nb : (sr[0] > 0.0 ? INFINITY : 0.0);
     out[1] = nr;
     out[2] = nb;
 }
@@ -1874,7 +1922,7 @@ extern "C" efl_status efl_residual_norms_noalloc(const float* pressure, const fl
     const int blocks = (int)(((uint64_t)nx * ny + kNoAllocCellsPerBlock - 1) / kNoAllocCellsPerBlock);
     cudaStream_t st = (cudaStream_t)stream;
     k_residual_norm<float><<<blocks, NORM_THREADS, count_launch(), st>>>(L, dt, rho, dx, partials);
-    k_norm_finalize_rel<<<1, 32, count_launch(), st>>>(partials, blocks, out_device);
+    k_norm_finalize_rel<<<1, kNoAllocFinalizeThreads, count_launch(), st>>>(partials, blocks, out_device);
     LAUNCH_CHECK();
     return EFL_OK;
 }
@@ -1908,6 +1956,7 @@ struct efl_batch {
     int tile_fixed = -1;         // set by efl_batch_set_tiles, -1 = autotune
     int tune_next = 0;
     std::vector<double> tune_cost;  // ns per cell-iteration, per configuration (0 = not tried)
+    long long spin_limit = 0;       // grid-barrier polls of the batched solve (0: the default)
 };
 
 namespace {
@@ -2014,6 +2063,7 @@ efl_status batch_solve(efl_batch* b, const std::vector<int>& which, efl_step_sta
     Pm.work_count = b->d_work_count;
     Pm.state = b->d_state;
     Pm.barrier = b->d_barrier;
+    Pm.spin_limit = b->spin_limit > 0 ? b->spin_limit : kBarrierSpinLimit;
     const size_t smem = cfg.smem;
     const void* kern = cfg.kern;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
@@ -2156,6 +2206,13 @@ efl_status efl_batch_tiles(const efl_batch* b, int32_t* tx, int32_t* ty, int32_t
     if (ns_per_cell_iteration)
         for (int i = 0; i < kBatchConfigs; ++i)
             ns_per_cell_iteration[i] = i < (int)b->tune_cost.size() ? b->tune_cost[i] : 0.0;
+    return EFL_OK;
+}
+
+efl_status efl_batch_set_wait_limits(efl_batch* b, uint64_t barrier_polls) {
+    if (!b) return set_err(nullptr, EFL_ERR_INVALID_ARGUMENT, "null batch");
+    if (barrier_polls > ((uint64_t)1 << 40)) return batch_err(b, EFL_ERR_INVALID_ARGUMENT, "wait limit above 2^40 polls");
+    b->spin_limit = (long long)barrier_polls;
     return EFL_OK;
 }
 

@@ -54,6 +54,7 @@ struct SolverWorkspace {
     SolveResult* h_result = nullptr;  // pinned host
     double2* partials = nullptr;
     int max_blocks = 0;
+    long long spin_limit = 0;  // grid-barrier polls before giving up (0: kBarrierSpinLimit)
 };
 
 constexpr int PS_THREADS = 1024;
@@ -66,10 +67,10 @@ constexpr long long kBarrierSpinLimit = 1ll << 25;  // acquire polls (~ 1 s)
 // e + 1 before all have arrived at e, so the CTA waits (acquire loads) until
 // count reaches the end of its barrier's range; the last arriver leaves at
 // once.  One atomic round trip on the way in, none on the way out.  A CTA
-// that polls more than kBarrierSpinLimit times sets barrier->error and
-// leaves; the others see the flag while they wait (checked every 1024
-// polls) and leave too.
-EFL_DEV bool grid_barrier(GridBarrier* gb, unsigned nblocks) {
+// that polls `limit` times (kBarrierSpinLimit unless the caller set a
+// shorter limit) sets barrier->error and leaves; the others see the flag
+// while they wait (checked every 1024 polls) and leave too.
+EFL_DEV bool grid_barrier(GridBarrier* gb, unsigned nblocks, long long limit) {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -82,10 +83,10 @@ EFL_DEV bool grid_barrier(GridBarrier* gb, unsigned nblocks) {
             for (;;) {
                 asm volatile("ld.acquire.gpu.u32 %0, [%1];" : "=r"(cur) : "l"(&gb->count) : "memory");
                 if ((int)(cur - target) >= 0) break;
-                if ((++spins & 1023) == 0) {
+                if ((++spins & 1023) == 0 || spins >= limit) {
                     int e;
                     asm volatile("ld.acquire.gpu.s32 %0, [%1];" : "=r"(e) : "l"(&gb->error) : "memory");
-                    if (e || spins > kBarrierSpinLimit) {
+                    if (e || spins >= limit) {
                         atomicExch(&gb->error, 1);
                         ok = 0;
                         break;
@@ -111,6 +112,7 @@ struct PersistentParams {
     double2* partials;
     GridBarrier* barrier;
     SolveResult* result;
+    long long spin_limit;  // grid-barrier polls before giving up
 };
 
 constexpr unsigned char MODE_SKIP = 0;     // outside the domain or on the tile's outer ring
@@ -439,7 +441,7 @@ __global__ void __launch_bounds__(PS_THREADS, 1) k_gsmix_persistent(PersistentPa
     unsigned iters = 0;
     double2 part = mix_check(T, base, H, tx, ty, cdiv, factor);
     if (threadIdx.x == 0) P.partials[blockIdx.x] = part;
-    bool ok = grid_barrier(P.barrier, nblocks);
+    bool ok = grid_barrier(P.barrier, nblocks, P.spin_limit);
     double r = ok ? ps_total_relative(P.partials, nblocks) : 0.0;
     const double r0 = r;
     // pending: the partials of the current p are written but their total is not read yet.  A check
@@ -468,7 +470,7 @@ __global__ void __launch_bounds__(PS_THREADS, 1) k_gsmix_persistent(PersistentPa
                     if ((unsigned)gx < (unsigned)L.nx && (unsigned)gy < (unsigned)L.ny)
                         __stcg(&dbuf.p[(size_t)gy * dbuf.P + gx], T.d[(base + lx + ly) & 1][ly * W2 + (lx >> 1)]);
                 }
-                ok = grid_barrier(P.barrier, nblocks);
+                ok = grid_barrier(P.barrier, nblocks, P.spin_limit);
                 if (!ok) break;
                 if (pending) {
                     pending = false;
@@ -494,7 +496,7 @@ __global__ void __launch_bounds__(PS_THREADS, 1) k_gsmix_persistent(PersistentPa
                 __stcg(&L.x.p[(size_t)gy * L.x.P + gx], pv);
             }
         }
-        ok = grid_barrier(P.barrier, nblocks);
+        ok = grid_barrier(P.barrier, nblocks, P.spin_limit);
         if (!ok) break;
         halo_reload<EX, EY, H>(T.p, L.x.p, (size_t)L.x.P, gx0, gy0, base, L.nx, L.ny);
         __syncthreads();
@@ -503,7 +505,7 @@ __global__ void __launch_bounds__(PS_THREADS, 1) k_gsmix_persistent(PersistentPa
         if (min(P.check_interval, P.max_iters - iters) > (unsigned)KMAX) {
             pending = true;  // read at the next block's first halo exchange
         } else {
-            ok = grid_barrier(P.barrier, nblocks);
+            ok = grid_barrier(P.barrier, nblocks, P.spin_limit);
             if (!ok) break;
             r = ps_total_relative(P.partials, nblocks);
         }
@@ -841,6 +843,7 @@ inline efl_status solve_gsmix_persistent(SolverWorkspace& ws, const Level64& L, 
     P.partials = ws.partials;
     P.barrier = ws.barrier;
     P.result = ws.result;
+    P.spin_limit = ws.spin_limit > 0 ? ws.spin_limit : kBarrierSpinLimit;
     if (cudaMemsetAsync(ws.barrier, 0, sizeof(GridBarrier), stream) != cudaSuccess) {
         *err = "barrier reset failed";
         return EFL_ERR_CUDA;

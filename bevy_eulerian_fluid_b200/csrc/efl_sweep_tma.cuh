@@ -77,7 +77,24 @@ EFL_DEV void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64
         "l"((uint64_t)map), "r"(x), "r"(y), "r"(smem_u32(bar))
         : "memory");
 }
-EFL_DEV bool mbar_wait(uint64_t* bar, unsigned parity) {
+// Waits for phase `parity` of an mbarrier, at most `limit` polls.  The
+// default limit polls with try_wait, which may suspend the warp for a while
+// per poll; a shorter limit (set by the caller to bound the wait tightly)
+// polls with the non-blocking test_wait, so it runs out after that many
+// polls whatever the hardware's suspend time.
+EFL_DEV bool mbar_wait(uint64_t* bar, unsigned parity, long long limit = kMbarSpinLimit) {
+    if (limit < kMbarSpinLimit) {
+        for (long long i = 0; i < limit; ++i) {
+            uint32_t done;
+            asm volatile(
+                "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+                : "=r"(done)
+                : "r"(smem_u32(bar)), "r"(parity)
+                : "memory");
+            if (done) return true;
+        }
+        return false;
+    }
     for (long long i = 0; i < kMbarSpinLimit; ++i) {
         uint32_t done;
         asm volatile(
@@ -130,7 +147,8 @@ EFL_DEV void ts_sweep_half(GsTile32<TS_EX, TS_EY>& T, int c, int base, float wei
 
 __global__ void __launch_bounds__(TS_THREADS, 1)
     k_gs32_tma(const __grid_constant__ SweepMaps maps, int nx, int ny, PF out, int pin, float dx_scaled, float rho,
-               float dt, float weight, int tiles_x, int ntiles, int iters, int* err, int first = 1) {
+               float dt, float weight, int tiles_x, int ntiles, int iters, int* err, int first,
+               long long wait_limit) {
     extern __shared__ __align__(128) unsigned char sm[];
     GsTile32<TS_EX, TS_EY>& T = *reinterpret_cast<GsTile32<TS_EX, TS_EY>*>(sm + TS_TILE_OFF);
     uint64_t* bars = reinterpret_cast<uint64_t*>(sm + TS_BAR_OFF);
@@ -166,11 +184,11 @@ __global__ void __launch_bounds__(TS_THREADS, 1)
         const bool after = t + 2 * (int)gridDim.x < ntiles;
         // Warp 0 waits for the copies; the barrier then orders the other warps' reads after its
         // acquire (the other 31 warps sleep in the barrier instead of spinning on the mbarrier).
-        const bool got = threadIdx.x < 32 ? mbar_wait(&bars[b], (n >> 1) & 1) : true;
+        const bool got = threadIdx.x < 32 ? mbar_wait(&bars[b], (n >> 1) & 1, wait_limit) : true;
         if (__syncthreads_or(!got)) {
             if (threadIdx.x == 0) {
                 atomicExch(err, 1);
-                mbar_wait(&bars[b], (n >> 1) & 1);  // copies of this CTA still in flight
+                mbar_wait(&bars[b], (n >> 1) & 1);  // copies of this CTA still in flight (default limit)
                 if (next) mbar_wait(&bars[b ^ 1], ((n + 1) >> 1) & 1);
             }
             return;
@@ -263,6 +281,7 @@ struct SweepTma {
     SweepMaps maps;
     bool ok = false;
     int* d_err = nullptr;
+    long long wait_limit = kMbarSpinLimit;  // polls of a tile's mbarrier wait before giving up
 };
 
 inline PFN_cuTensorMapEncodeTiled tensor_map_encoder() {
@@ -334,7 +353,7 @@ inline efl_status tma_sweep_pass(const SweepTma& st, int nx, int ny, const PF& o
     if (!st.ok || iters < 1 || iters > TS_K || !tma_kernel_ready()) return EFL_ERR_STATE;
     const int tiles_x = (nx + TS_TX - 1) / TS_TX, ntiles = tiles_x * ((ny + TS_TY - 1) / TS_TY);
     k_gs32_tma<<<std::min(ntiles, num_sms), TS_THREADS, TS_SMEM + count_launch(), stream>>>(
-        st.maps, nx, ny, out, pin, dx_scaled, rho, dt, weight, tiles_x, ntiles, iters, err, first);
+        st.maps, nx, ny, out, pin, dx_scaled, rho, dt, weight, tiles_x, ntiles, iters, err, first, st.wait_limit);
     return cudaGetLastError() == cudaSuccess ? EFL_OK : EFL_ERR_CUDA;
 }
 
@@ -356,7 +375,7 @@ inline efl_status solve_gs32_tma(SweepTma& st, const Level& L, const PF& alt, in
         PF out = pin == 0 ? alt : L.x;
         k_gs32_tma<<<grid, TS_THREADS, TS_SMEM + count_launch(), stream>>>(st.maps, L.nx, L.ny, out, pin, dx_scaled,
                                                                            rho, dt, weight, tiles_x, ntiles, k,
-                                                                           st.d_err);
+                                                                           st.d_err, 1, st.wait_limit);
         pin ^= 1;
         done += (uint32_t)k;
         ++launches;

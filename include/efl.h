@@ -338,11 +338,31 @@ EFL_API efl_status efl_residual(efl_sim* sim, double* relative, double* norm_r, 
  * own launch (results are identical).  Default on.  No reference
  * counterpart (the reference records wgpu command buffers per frame). */
 EFL_API efl_status efl_set_graph_capture(efl_sim* sim, int32_t enable);
+/* Bounds of the device-side waits (extension, no reference counterpart).
+ * barrier_polls: polls of the grid barrier inside the cooperative pressure
+ * solves before a CTA gives up; every CTA then leaves the launch and the
+ * step returns EFL_ERR_CUDA ("... a grid barrier timed out").
+ * mbarrier_polls: polls of the TMA sweep's wait for a tile's copies; a CTA
+ * that gives up waits (default bound) for its own copies still in flight and
+ * leaves, and the next efl_synchronize / efl_read_solid_forces returns
+ * EFL_ERR_CUDA ("TMA sweep: an mbarrier wait timed out").  0 restores the
+ * defaults (2^25 and 2^24 polls, about a second).  A short limit turns a
+ * stalled wait into an error status instead of a long spin, and lets a test
+ * make a wait run out without any fault or hang. */
+EFL_API efl_status efl_set_wait_limits(efl_sim* sim, uint64_t barrier_polls, uint64_t mbarrier_polls);
 /* Device time of the last projection stage (efl_step or efl_run_stage), in
  * milliseconds; waits for it to finish.  No reference counterpart (the
  * reference has no per-stage timing). */
 EFL_API efl_status efl_projection_ms(efl_sim* sim, float* ms);
 
+/* Post-projection divergence: the operator of divergence.wgsl:16-42 applied
+ * to the current velocity u0 / v0 (with the current face fractions and solid
+ * velocities) at the cells the residual counts (levelset_air < 0, not fully
+ * solid).  l2 = sqrt of the FP64 sum of squares, linf = the largest
+ * magnitude (1/s).  Call it between EFL_STAGE_SOLVE_VELOCITY and the next
+ * stage for the divergence the projection leaves (the reference evaluates
+ * no such diagnostic; its volume diagnostic is efl_fluid_volume). */
+EFL_API efl_status efl_divergence_norms(efl_sim* sim, double* l2, double* linf);
 /* Number of cells with levelset_air < 0 (calculate_volume.wgsl:11-75). */
 EFL_API efl_status efl_fluid_volume(efl_sim* sim, uint64_t* cells);
 /* FluidMinVelocityMagnitude / FluidMaxVelocityMagnitude
@@ -445,6 +465,11 @@ EFL_API efl_status efl_batch_set_tiles(efl_batch* batch, int32_t config);
  * each (ns_per_cell_iteration: 4 entries or NULL; 0 = not tried). */
 EFL_API efl_status efl_batch_tiles(const efl_batch* batch, int32_t* tx, int32_t* ty, int32_t* k,
                                    double* ns_per_cell_iteration);
+/* Grid-barrier poll limit of the batched solve (efl_set_wait_limits'
+ * barrier_polls; 0 = the default).  A barrier that runs out makes
+ * efl_batch_step return EFL_ERR_CUDA ("batched solver: a grid barrier timed
+ * out"). */
+EFL_API efl_status efl_batch_set_wait_limits(efl_batch* batch, uint64_t barrier_polls);
 /* Device time of the last batched pressure solve (the cooperative launch), in
  * milliseconds; waits for it to finish. */
 EFL_API efl_status efl_batch_projection_ms(efl_batch* batch, float* ms);
@@ -524,6 +549,9 @@ EFL_API efl_status efl_pressure_sweeps(efl_sim* sim, int32_t precision, uint32_t
  *    rejected with EFL_ERR_INVALID_ARGUMENT.
  *  - The first call on a device looks up that array's device address (with
  *    that device current); make that first call before any stream capture.
+ *    The address is kept for the life of the process, so a device reset
+ *    (cudaDeviceReset, or tearing down and recreating the primary context)
+ *    between calls is not supported.
  *  - All calls share the one array: calls whose work overlaps on the GPU
  *    (different streams, or different host threads, at the same time) race
  *    and may return wrong norms.  Each call overwrites every partial it

@@ -2268,6 +2268,31 @@ efl_status eflo_velocity_magnitude(eflo_sim* s, float* min_mag, float* max_mag) 
     return EFL_OK;
 }
 
+// divergence.wgsl:16-42 applied to the projected velocity (u0, v0) at the
+// cells the residual counts (phi < 0, not fully solid): sqrt of the FP64 sum
+// of squares in row order and the largest magnitude.
+efl_status eflo_divergence_norms(eflo_sim* s, double* l2, double* linf) {
+    if (!s) return EFL_ERR_INVALID_ARGUMENT;
+    const float dx = s->U.dx;
+    double a2 = 0.0, m = 0.0;
+    for (int y = 0; y < s->ny; ++y)
+        for (int x = 0; x < s->nx; ++x) {
+            if (!(s->ls0.ld(x, y) < 0.0f)) continue;
+            const F4 f = s->af.ld(x, y);
+            if (f.x == 0.0f && f.y == 0.0f && f.z == 0.0f && f.w == 0.0f) continue;
+            const float du_f = f.y * s->u0.ld(x + 1, y) - f.x * s->u0.ld(x, y);
+            const float dv_f = f.w * s->v0.ld(x, y + 1) - f.z * s->v0.ld(x, y);
+            const float du_s = (1.0f - f.y) * s->us.ld(x + 1, y) - (1.0f - f.x) * s->us.ld(x, y);
+            const float dv_s = (1.0f - f.w) * s->vs.ld(x, y + 1) - (1.0f - f.z) * s->vs.ld(x, y);
+            const double d = (double)(-(du_f + dv_f + du_s + dv_s) / dx);
+            a2 += d * d;
+            m = std::fmax(m, std::fabs(d));
+        }
+    if (l2) *l2 = std::sqrt(a2);
+    if (linf) *linf = m;
+    return EFL_OK;
+}
+
 efl_status eflo_fluid_volume(eflo_sim* s, uint64_t* cells) {
     if (!s || !cells) return EFL_ERR_INVALID_ARGUMENT;
     uint64_t c = 0;

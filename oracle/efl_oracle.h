@@ -47,6 +47,7 @@ EFL_API efl_status eflo_set_field(eflo_sim* sim, int32_t field, const void* host
 EFL_API efl_status eflo_residual(eflo_sim* sim, double* relative, double* norm_r, double* norm_b);
 EFL_API efl_status eflo_fluid_volume(eflo_sim* sim, uint64_t* cells);
 EFL_API efl_status eflo_velocity_magnitude(eflo_sim* sim, float* min_mag, float* max_mag);
+EFL_API efl_status eflo_divergence_norms(eflo_sim* sim, double* l2, double* linf);
 
 /* Two-layer particle level set (src/euler_fluid/particle_levelset_two_layers). */
 EFL_API efl_status eflo_set_particle_levelset(eflo_sim* sim, int32_t enable);

@@ -326,3 +326,32 @@ def test_maximum_obstacles_and_sources(oracle_api, gpu_api):
         g.step(sc.dt)
     assert not compare_fields(g, o)
     assert np.array_equal(g.force_bins(), o.force_bins())
+
+
+def test_reset_matches_oracle_reset(oracle_api, gpu_api):
+    """FluidStatus::Reset (fluid_status.rs:15-38, render_node.rs:177-189): efl_reset makes the next step re-run the
+    init sequence only.  The fields it writes equal a fresh handle's init; the rest carry over, and the run that
+    follows stays bit-exact with the oracle doing the same reset."""
+    sc = small_coupled(128, tolerance=1e-5)
+    o, g = make_pair(sc, oracle_api, gpu_api)
+    for _ in range(4):
+        o.step(sc.dt)
+        g.step(sc.dt)
+    o.reset()
+    g.reset()
+    so, sg = o.step(sc.dt), g.step(sc.dt)
+    assert so.initialized_only == sg.initialized_only == 1
+    fresh = sc.make(gpu_api)
+    assert fresh.step(sc.dt).initialized_only == 1
+    init_fields = [capi.FIELD_U, capi.FIELD_V, capi.FIELD_U1, capi.FIELD_V1, capi.FIELD_LEVELSET_AIR,
+                   capi.FIELD_LEVELSET_AIR1, capi.FIELD_JFA_SEEDS, capi.FIELD_GRAD_LEVELSET]
+    assert not compare_fields(g, fresh, fields=init_fields)
+    assert not compare_fields(g, o)
+    for _ in range(3):
+        so, sg = o.step(sc.dt), g.step(sc.dt)
+        assert so.pressure_iterations == sg.pressure_iterations
+    assert not compare_fields(g, o)
+    assert np.array_equal(g.force_bins(), o.force_bins())
+    fresh.close()
+    o.close()
+    g.close()

@@ -178,3 +178,24 @@ def test_velocity_magnitude_oracle_semantics(oracle_api):
     speed = np.sqrt(uc * uc + vc * vc).astype(np.float32)
     assert mn == 0.0
     assert mx == pytest.approx(float(speed.max()), rel=1e-6)
+
+
+def test_cfl_dt_bounds_the_displacement(oracle_api):
+    """plugin.cfl_dt: the step moves no fluid more than `cfl` cells at the monitored maximum speed
+    (velocities are in grid cells per second: coordinate.wgsl:83-94 moves x by dt * velocity)."""
+    from bevy_eulerian_fluid_b200.plugin import cfl_dt
+    assert cfl_dt(0.0) == 1.0 / 60.0
+    assert cfl_dt(float("nan")) == 1.0 / 60.0
+    assert cfl_dt(30.0) == 1.0 / 60.0  # slower than 60 cells/s: the cap
+    assert cfl_dt(120.0) == 1.0 / 120.0
+    assert cfl_dt(120.0, cfl=0.5) == 0.5 / 120.0
+    assert cfl_dt(10.0, dt_max=0.01) == 0.01
+    sc = scenes.dam_break(64)
+    o = sc.make(oracle_api)
+    for _ in range(30):
+        o.step(sc.dt)
+    _, mx = o.velocity_magnitude()
+    assert mx > 0.0
+    dt = cfl_dt(mx, cfl=0.5, dt_max=1.0)
+    assert dt * mx <= 0.5 * (1 + 1e-6)
+    o.close()

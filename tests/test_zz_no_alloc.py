@@ -41,6 +41,9 @@ def test_noalloc_matches_efl_residual_twice():
         sim.step(sc.dt)
     dx = float(np.float32(1.0) / np.float32(sc.cfg.length_unit))
     out = torch.full((3,), -1.0, dtype=torch.float64, device="cuda")
+    # The fill runs on torch's stream and the entry point on the simulation's
+    # non-blocking stream: finish the fill before the first call writes `out`.
+    torch.cuda.synchronize()
     for call in range(2):
         st = _call(api, sim, out.data_ptr(), dx, sc.dt, sc.cfg.rho)
         assert st == capi.OK, (api.last_error(None) or b"").decode()
