@@ -180,6 +180,8 @@ SIGNATURES = {
     "unet_attach": (C.c_int, ["X", C.c_void_p, C.c_uint32]),
     "unet_train_step": (C.c_int, [C.c_void_p, C.c_float, C.POINTER(C.c_float)]),
     "unet_time_forward": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(C.c_float)]),
+    "unet_set_coarsening": (C.c_int, [C.c_void_p, C.c_uint32]),
+    "batch_attach_unet": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32]),
 }
 # Functions of efl.h that the oracle restatement does not mirror.
 PRODUCT_ONLY = {"abi_version", "default_config", "field_device_ptr", "stream", "synchronize", "kernel_launches",
@@ -188,7 +190,7 @@ PRODUCT_ONLY = {"abi_version", "default_config", "field_device_ptr", "stream", "
                 "projection_ms", "set_graph_capture", "set_wait_limits", "set_rigid_bodies", "get_rigid_bodies",
                 "unet_create", "unet_destroy", "unet_last_error", "unet_num_params", "unet_get_params",
                 "unet_set_params", "unet_forward", "unet_gradients", "unet_attach", "unet_train_step",
-                "unet_time_forward"}
+                "unet_time_forward", "unet_set_coarsening", "batch_attach_unet"}
 
 
 class EflError(RuntimeError):
@@ -516,6 +518,11 @@ class Batch:
         self._check(self.api.batch_tiles(self.h, C.byref(tx), C.byref(ty), C.byref(k), cost))
         return (tx.value, ty.value, k.value), list(cost)
 
+    def attach_unet(self, net: "UNet", warm_start: bool = True):
+        """Warm-starts every simulation's solve with the network (one forward workspace per simulation)."""
+        self._check(self.api.batch_attach_unet(self.h, net.h if warm_start else None,
+                                               UNET_WARM_START if warm_start else 0))
+
     def set_wait_limits(self, barrier_polls: int = 0):
         """Grid-barrier polls of the batched solve before it gives up (0 = the default)."""
         self._check(self.api.batch_set_wait_limits(self.h, barrier_polls))
@@ -598,6 +605,10 @@ class UNet:
     def attach(self, sim: "Sim", warm_start: bool = True, record: bool = False):
         flags = (UNET_WARM_START if warm_start else 0) | (UNET_RECORD if record else 0)
         self._check(self.api.unet_attach(sim.h, self.h if flags else None, flags))
+
+    def set_coarsening(self, factor: int):
+        """Run the network on the grid coarsened by factor (1, 2, 4 or 8); see efl_unet_set_coarsening."""
+        self._check(self.api.unet_set_coarsening(self.h, factor))
 
     def time_forward(self, nx: int, ny: int, reps: int = 20) -> float:
         """Device ms of one forward pass at nx x ny, replayed from a CUDA graph

@@ -57,6 +57,7 @@ struct DevBuf {
 struct efl_unet {
     UNet net;
     int rec_nx = 0, rec_ny = 0;  // size of the recorded training sample (0: none)
+    bool rec_coarse = false;     // the recorded sample is on the coarse grid (targetc / maskc)
 };
 
 // Captured CUDA graphs of step segments, keyed by a signature of the
@@ -134,6 +135,7 @@ struct efl_sim {
     GraphCache gc;                // captured step segments
     uint64_t graph_epoch = 1;     // counts the setters that change kernel arguments
     PF mix_d2{};       // second correction buffer (batched solve)
+    PF dbuf2{};        // second halo-exchange buffer of the persistent solve, allocated on first use
     bool owns_stream = true;
     float* d_vel = nullptr;  // velocity-magnitude partials (efl_velocity_magnitude)
     int cap_vel = 0;
@@ -143,6 +145,7 @@ struct efl_sim {
     int rigid_substeps = 1;
     struct efl_unet* unet = nullptr;  // learned warm start / training recorder
     uint32_t unet_flags = 0;
+    UNet* unet_view = nullptr;  // forward-only workspace of the network (batch members), owned
     int* h_err = nullptr;  // pinned copy of the TMA sweep's error flag
     cudaEvent_t ev_proj[2] = {nullptr, nullptr};  // around the last projection stage
     bool proj_timed = false;
@@ -619,8 +622,9 @@ efl_status ensure_mix_planes(efl_sim* s) {
 efl_status gs_mixed(efl_sim* s, float weight, double tol, uint32_t max_iters, uint32_t check, SolveResult* res) {
     const Level64& L = s->mg64[0];
     std::string perr;
-    efl_status ps = solve_gsmix_persistent(s->solver, L, s->r0, s->U, weight, tol, max_iters, check, s->stream, res,
-                                           &perr);
+    if (!s->dbuf2.p) TRY(alloc_plane(s, s->dbuf2, s->nx, s->ny, s->P, s->ny + 1));
+    efl_status ps = solve_gsmix_persistent(s->solver, L, s->r0, s->dbuf2, s->U, weight, tol, max_iters, check,
+                                           s->stream, res, &perr);
     if (ps == EFL_OK) return EFL_OK;
     if (ps != EFL_ERR_STATE) return set_err(s, ps, "%s", perr.c_str());
     TRY(ensure_mix_planes(s));
@@ -858,7 +862,10 @@ efl_status check_device_errors(efl_sim* s) {
 // Learned warm start: the features of the system about to be solved, and
 // (when warm-starting) x += sigma * prediction on the counted cells.
 efl_status unet_before_solve(efl_sim* s) {
-    UNet& n = s->unet->net;
+    UNet& n = s->unet_view ? *s->unet_view : s->unet->net;
+    const int f = s->unet->net.coarse;
+    if (n.coarse != f)
+        return set_err(s, EFL_ERR_STATE, "the network's coarsening changed after efl_batch_attach_unet: attach again");
     const Level64& L = s->mg64[0];
     const dim3 g = grid2d(s->nx, s->ny, kBlock);
     const double dx = (double)s->U.dx;
@@ -866,21 +873,37 @@ efl_status unet_before_solve(efl_sim* s) {
                       (double)s->U.dt / (double)s->U.rho / dx / dx, s->nx, s->ny};
     k_unet_residual<<<g, kBlock, count_launch(), s->stream>>>(a, n.res32, n.prev32, n.mask, n.lpart);
     k_unet_sigma<<<1, 32, count_launch(), s->stream>>>(n.lpart, (int)(g.x * g.y), n.sigma);
-    k_unet_features<<<g, kBlock, count_launch(), s->stream>>>(n.res32, a, n.mask, n.sigma, n.X0);
+    if (f > 1) {
+        k_unet_features_coarse<<<grid2d(s->nx / f, s->ny / f, kBlock), kBlock, count_launch(), s->stream>>>(
+            n.res32, a, n.mask, n.sigma, f, n.X0, n.maskc);
+    } else {
+        k_unet_features<<<g, kBlock, count_launch(), s->stream>>>(n.res32, a, n.mask, n.sigma, n.X0);
+    }
     if (s->unet_flags & EFL_UNET_WARM_START) {
-        unet_forward(n, s->ny, s->nx, s->stream);
-        k_unet_warm<<<g, kBlock, count_launch(), s->stream>>>(L.x, n.out, n.mask, n.sigma, s->nx, s->ny);
+        unet_forward(n, s->ny / f, s->nx / f, s->stream);
+        if (f > 1)
+            k_unet_warm_coarse<<<g, kBlock, count_launch(), s->stream>>>(L.x, n.out, n.mask, n.sigma, s->nx, s->ny, f);
+        else
+            k_unet_warm<<<g, kBlock, count_launch(), s->stream>>>(L.x, n.out, n.mask, n.sigma, s->nx, s->ny);
     }
     LAUNCH_CHECK();
     return EFL_OK;
 }
 efl_status unet_after_solve(efl_sim* s) {
     UNet& n = s->unet->net;
-    k_unet_target<<<grid2d(s->nx, s->ny, kBlock), kBlock, count_launch(), s->stream>>>(s->mg64[0].x, n.prev32, n.sigma,
-                                                                                      s->nx, s->ny, n.target);
+    const int f = n.coarse;
+    if (f > 1) {
+        k_unet_target_coarse<<<grid2d(s->nx / f, s->ny / f, kBlock), kBlock, count_launch(), s->stream>>>(
+            s->mg64[0].x, n.prev32, n.mask, n.sigma, s->nx, s->ny, f, n.targetc);
+    } else {
+        k_unet_target<<<grid2d(s->nx, s->ny, kBlock), kBlock, count_launch(), s->stream>>>(s->mg64[0].x, n.prev32,
+                                                                                          n.sigma, s->nx, s->ny,
+                                                                                          n.target);
+    }
     LAUNCH_CHECK();
-    s->unet->rec_nx = s->nx;
-    s->unet->rec_ny = s->ny;
+    s->unet->rec_nx = s->nx / f;
+    s->unet->rec_ny = s->ny / f;
+    s->unet->rec_coarse = f > 1;
     return EFL_OK;
 }
 
@@ -915,7 +938,12 @@ efl_status st_projection(efl_sim* s, efl_step_stats* st) {
         dim3 g = grid2d(d.nx, d.ny, kBlock);
         k_widen<<<g, kBlock, count_launch(), s->stream>>>(s->p0, s->div, L.x, L.b);
         LAUNCH_CHECK();
-        if (s->unet && s->unet_flags) TRY(unet_before_solve(s));
+        if (s->unet && s->unet_flags) {
+            if ((s->unet_flags & EFL_UNET_RECORD) && s->unet_view)
+                return set_err(s, EFL_ERR_STATE, "a batch member's network workspace is forward-only: record "
+                                                 "training samples on a simulation of its own");
+            TRY(unet_before_solve(s));
+        }
         double r = -1.0;
         bool done = false;
         if (P.method == EFL_PROJECTION_GAUSS_SEIDEL || P.method == EFL_PROJECTION_MGPCG) {
@@ -1306,6 +1334,10 @@ efl_status efl_destroy(efl_sim* s) {
     if (s->cg.h_read) cudaFreeHost(s->cg.h_read);
     if (s->d_vel) cudaFree(s->d_vel);
     if (s->pls.h_read) cudaFreeHost(s->pls.h_read);
+    if (s->unet_view) {
+        cudaFree(s->unet_view->arena);
+        delete s->unet_view;
+    }
     for (cudaEvent_t e : s->ev_proj)
         if (e) cudaEventDestroy(e);
     s->gc.clear();
@@ -1957,6 +1989,12 @@ struct efl_batch {
     int tune_next = 0;
     std::vector<double> tune_cost;  // ns per cell-iteration, per configuration (0 = not tried)
     long long spin_limit = 0;       // grid-barrier polls of the batched solve (0: the default)
+    // The simulations' stages run on one work stream each, forked from and joined back into the batch
+    // stream, so that the small kernels of different simulations overlap on the GPU (and, captured into
+    // a CUDA graph, form independent branches).  The simulations' public stream stays the batch stream.
+    std::vector<cudaStream_t> work;
+    std::vector<cudaEvent_t> ev_join;
+    cudaEvent_t ev_fork = nullptr;
 };
 
 namespace {
@@ -2003,8 +2041,38 @@ void batch_free(efl_batch* b) {
     for (cudaEvent_t e : b->ev)
         if (e) cudaEventDestroy(e);
     b->gc.clear();
+    for (cudaStream_t w : b->work)
+        if (w) cudaStreamDestroy(w);
+    for (cudaEvent_t e : b->ev_join)
+        if (e) cudaEventDestroy(e);
+    if (b->ev_fork) cudaEventDestroy(b->ev_fork);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
+}
+
+// Runs per_sim(i, s) for every simulation on its own work stream: the work
+// streams wait for the batch stream, each simulation's launches go to its
+// work stream (s->stream is switched for the call), and the batch stream then
+// waits for every work stream.  Inside a stream capture this makes one graph
+// branch per simulation.
+template <class F>
+efl_status batch_fanout(efl_batch* b, F per_sim) {
+    if (cudaEventRecord(b->ev_fork, b->stream) != cudaSuccess) return EFL_ERR_CUDA;
+    for (cudaStream_t w : b->work)
+        if (cudaStreamWaitEvent(w, b->ev_fork, 0) != cudaSuccess) return EFL_ERR_CUDA;
+    efl_status st = EFL_OK;
+    for (size_t i = 0; i < b->sims.size() && st == EFL_OK; ++i) {
+        efl_sim* s = b->sims[i];
+        s->stream = b->work[i];
+        st = per_sim(i, s);
+        s->stream = b->stream;
+    }
+    for (size_t i = 0; i < b->sims.size(); ++i) {  // always rejoin, so that a capture stays well formed
+        if (cudaEventRecord(b->ev_join[i], b->work[i]) != cudaSuccess ||
+            cudaStreamWaitEvent(b->stream, b->ev_join[i], 0) != cudaSuccess)
+            return EFL_ERR_CUDA;
+    }
+    return st;
 }
 
 // One cooperative launch for the tolerance-driven solves of the batch's
@@ -2161,6 +2229,16 @@ efl_status efl_batch_create(const efl_config* cfgs, uint32_t n, efl_batch** out)
         total_tiles += ((s->nx + kMinTile - 1) / kMinTile) * ((s->ny + kMinTile - 1) / kMinTile);
     }
     b->ntiles = total_tiles;
+    b->work.assign(n, nullptr);
+    b->ev_join.assign(n, nullptr);
+    bool ok = cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming) == cudaSuccess;
+    for (uint32_t i = 0; i < n && ok; ++i)
+        ok = cudaStreamCreateWithFlags(&b->work[i], cudaStreamNonBlocking) == cudaSuccess &&
+             cudaEventCreateWithFlags(&b->ev_join[i], cudaEventDisableTiming) == cudaSuccess;
+    if (!ok) {
+        batch_free(b);
+        return batch_err(nullptr, EFL_ERR_CUDA, "batch work stream creation failed");
+    }
     if (cudaMalloc(&b->d_sims, n * sizeof(BatchSim)) != cudaSuccess ||
         cudaMalloc(&b->d_tiles, total_tiles * sizeof(int2)) != cudaSuccess ||
         cudaMalloc(&b->d_partials, total_tiles * sizeof(double2)) != cudaSuccess ||
@@ -2209,6 +2287,35 @@ efl_status efl_batch_tiles(const efl_batch* b, int32_t* tx, int32_t* ty, int32_t
     return EFL_OK;
 }
 
+efl_status efl_batch_attach_unet(efl_batch* b, efl_unet* u, uint32_t flags) {
+    if (!b) return batch_err(nullptr, EFL_ERR_INVALID_ARGUMENT, "null batch");
+    if (flags & ~(uint32_t)EFL_UNET_WARM_START)
+        return batch_err(b, EFL_ERR_INVALID_ARGUMENT, "a batch takes EFL_UNET_WARM_START only (record on a single "
+                                                      "simulation)");
+    cudaSetDevice(b->device);
+    if (cudaStreamSynchronize(b->stream) != cudaSuccess) return batch_err(b, EFL_ERR_CUDA, "batch stream failed");
+    for (efl_sim* s : b->sims) {
+        if (efl_unet_attach(s, flags ? u : nullptr, flags) != EFL_OK)
+            return batch_err(b, EFL_ERR_INVALID_ARGUMENT, std::string("attach: ") + efl_unet_last_error(u));
+        if (!flags || !u) continue;
+        if (s->unet_view && s->unet_view->coarse != u->net.coarse) {  // sized for another coarsening
+            cudaFree(s->unet_view->arena);
+            delete s->unet_view;
+            s->unet_view = nullptr;
+        }
+        if (!s->unet_view) {
+            UNet* v = new UNet();
+            if (unet_alloc_forward(*v, u->net, s->ny, s->nx) != cudaSuccess) {
+                if (v->arena) cudaFree(v->arena);
+                delete v;
+                return batch_err(b, EFL_ERR_OUT_OF_MEMORY, "network workspace allocation failed");
+            }
+            s->unet_view = v;
+        }
+    }
+    return EFL_OK;
+}
+
 efl_status efl_batch_set_wait_limits(efl_batch* b, uint64_t barrier_polls) {
     if (!b) return set_err(nullptr, EFL_ERR_INVALID_ARGUMENT, "null batch");
     if (barrier_polls > ((uint64_t)1 << 40)) return batch_err(b, EFL_ERR_INVALID_ARGUMENT, "wait limit above 2^40 polls");
@@ -2253,13 +2360,13 @@ efl_status efl_batch_step(efl_batch* b, float dt, efl_step_stats* stats) {
             sig_post = fnv(sig_post, segment_sig(s, SEG_POST));
         }
         efl_status st = run_segment(b->gc, b->stream, sig_pre | 1, SEG_PRE, [&]() -> efl_status {
-            for (efl_sim* s : b->sims) {
-                efl_status r = run_stages(s, EFL_STAGE_UPDATE_SOLID, EFL_STAGE_DIVERGENCE, nullptr);
-                if (r != EFL_OK) return r;
+            return batch_fanout(b, [&](size_t, efl_sim* s) -> efl_status {
+                TRY(run_stages(s, EFL_STAGE_UPDATE_SOLID, EFL_STAGE_DIVERGENCE, nullptr));
                 const Level64& L = s->mg64[0];
                 k_widen<<<grid2d(s->nx, s->ny, kBlock), kBlock, count_launch(), s->stream>>>(s->p0, s->div, L.x, L.b);
-            }
-            return EFL_OK;
+                if (s->unet && (s->unet_flags & EFL_UNET_WARM_START)) TRY(unet_before_solve(s));
+                return EFL_OK;
+            });
         });
         if (st != EFL_OK) return batch_err(b, st, "batched stages before the solve failed");
         std::vector<int> all(n);
@@ -2275,12 +2382,10 @@ efl_status efl_batch_step(efl_batch* b, float dt, efl_step_stats* stats) {
         for (size_t i = 0; i < n; ++i)
             if (!sp[i].converged) ret = EFL_NOT_CONVERGED;
         st = run_segment(b->gc, b->stream, sig_post | 1, SEG_POST, [&]() -> efl_status {
-            for (efl_sim* s : b->sims) {
+            return batch_fanout(b, [&](size_t, efl_sim* s) -> efl_status {
                 k_narrow<<<grid2d(s->nx, s->ny, kBlock), kBlock, count_launch(), s->stream>>>(s->mg64[0].x, s->p0);
-                efl_status r = run_stages(s, EFL_STAGE_SOLVE_VELOCITY, EFL_STAGE_SOLID_FORCES, nullptr);
-                if (r != EFL_OK) return r;
-            }
-            return EFL_OK;
+                return run_stages(s, EFL_STAGE_SOLVE_VELOCITY, EFL_STAGE_SOLID_FORCES, nullptr);
+            });
         });
         if (st != EFL_OK) return batch_err(b, st, "batched stages after the solve failed");
         for (efl_sim* s : b->sims) s->n_forces = 0;
@@ -2310,6 +2415,10 @@ efl_status efl_batch_step(efl_batch* b, float dt, efl_step_stats* stats) {
         if (batchable) {
             const Level64& L = s->mg64[0];
             k_widen<<<grid2d(s->nx, s->ny, kBlock), kBlock, count_launch(), s->stream>>>(s->p0, s->div, L.x, L.b);
+            if (s->unet && (s->unet_flags & EFL_UNET_WARM_START)) {
+                efl_status st = unet_before_solve(s);
+                if (st != EFL_OK) return fail(s, st);
+            }
             solve_batched.push_back((int)i);
         } else {
             efl_status st = run_stage(s, EFL_STAGE_PROJECTION, stats ? &stats[i] : nullptr);
@@ -2392,14 +2501,16 @@ efl_status unet_loss_and_grads(efl_unet* u, int H, int W, cudaStream_t st, float
     UNet& n = u->net;
     const int npix = H * W, blocks = (npix + 1023) / 1024;
     std::vector<float2> part(blocks);
-    k_target_stats<<<blocks, 256, count_launch(), st>>>(n.target, n.mask, npix, 1024, n.lpart);
+    const float* target = u->rec_coarse ? n.targetc : n.target;
+    const unsigned char* mask = u->rec_coarse ? n.maskc : n.mask;
+    k_target_stats<<<blocks, 256, count_launch(), st>>>(target, mask, npix, 1024, n.lpart);
     cudaMemcpyAsync(part.data(), n.lpart, blocks * sizeof(float2), cudaMemcpyDeviceToHost, st);
     unet_forward(n, H, W, st);
     TRY_U(unet_finish(u, st));
     double t2 = 0.0;
     for (auto& q : part) t2 += q.y;
     const float inv = t2 > 0.0 ? (float)(1.0 / t2) : 0.0f;
-    k_unet_loss<<<blocks, 256, count_launch(), st>>>(n.out, n.target, n.mask, npix, 1024, inv, n.g_out, n.lpart);
+    k_unet_loss<<<blocks, 256, count_launch(), st>>>(n.out, target, mask, npix, 1024, inv, n.g_out, n.lpart);
     unet_backward(n, H, W, st);
     cudaMemcpyAsync(part.data(), n.lpart, blocks * sizeof(float2), cudaMemcpyDeviceToHost, st);
     TRY_U(unet_finish(u, st));
@@ -2569,8 +2680,27 @@ efl_status efl_unet_attach(efl_sim* s, efl_unet* u, uint32_t flags) {
     if (!s) return unet_err(u, EFL_ERR_INVALID_ARGUMENT, "null sim");
     if (u && (s->nx > u->net.maxW || s->ny > u->net.maxH || s->cfg.device != u->net.device))
         return unet_err(u, EFL_ERR_INVALID_ARGUMENT, "simulation larger than the network, or on another device");
+    if (u && flags && (s->nx % (8 * u->net.coarse) || s->ny % (8 * u->net.coarse)))
+        return unet_err(u, EFL_ERR_INVALID_ARGUMENT,
+                        "grid size must be a multiple of 8 x the network's coarsening factor");
+    if (s->unet_view && (!u || flags == 0 || s->unet != u)) {  // the workspace belonged to the previous network
+        cudaStreamSynchronize(s->stream);
+        cudaFree(s->unet_view->arena);
+        delete s->unet_view;
+        s->unet_view = nullptr;
+    }
     s->unet = flags ? u : nullptr;
     s->unet_flags = u ? flags : 0;
+    ++s->graph_epoch;  // captured segments hold the previous network's launches
+    return EFL_OK;
+}
+
+efl_status efl_unet_set_coarsening(efl_unet* u, uint32_t factor) {
+    if (!u) return unet_err(nullptr, EFL_ERR_INVALID_ARGUMENT, "null network");
+    if (factor != 1 && factor != 2 && factor != 4 && factor != 8)
+        return unet_err(u, EFL_ERR_INVALID_ARGUMENT, "coarsening factor must be 1, 2, 4 or 8");
+    u->net.coarse = (int)factor;
+    u->rec_nx = u->rec_ny = 0;  // a recorded sample of the other form is void
     return EFL_OK;
 }
 

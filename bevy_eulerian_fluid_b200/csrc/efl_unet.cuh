@@ -866,6 +866,81 @@ __global__ void k_unet_target(Plane<double> x, const float* prev32, const float*
     const size_t p = (size_t)gy * nx + gx;
     target[p] = (float)((x.at(gx, gy) - (double)prev32[p]) / (double)*sigma);
 }
+// Coarse form of the warm start.  The red-black sweeps remove the
+// basin-scale part of the error slowest (hundreds of iterations per e-fold at
+// 512^2), and that part is smooth: the network therefore runs on the grid
+// coarsened by f (one coarse cell per f x f cells), where four levels of
+// pooling span the whole domain, and its output is interpolated back
+// bilinearly; the sweeps then remove the fine-scale remainder quickly.
+// Coarse features: the mean over the block of each fine channel; maskc = 1
+// where the block holds a counted cell.
+__global__ void k_unet_features_coarse(const float* res, const UnetFeatureArgs a, const unsigned char* mask,
+                                       const float* sigma, int f, bf16* x0, unsigned char* maskc) {
+    const int Wc = a.nx / f, Hc = a.ny / f;
+    const int cx = blockIdx.x * blockDim.x + threadIdx.x, cy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (cx >= Wc || cy >= Hc) return;
+    const float inv = 1.0f / *sigma;
+    float acc[5] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+    for (int j = 0; j < f; ++j)
+        for (int i = 0; i < f; ++i) {
+            const int gx = cx * f + i, gy = cy * f + j;
+            const size_t p = (size_t)gy * a.nx + gx;
+            acc[0] += res[p] * inv;
+            acc[1] += 0.5f * (a.fu.at(gx, gy) + a.fu.at(gx + 1, gy));
+            acc[2] += 0.5f * (a.fv.at(gx, gy) + a.fv.at(gx, gy + 1));
+            acc[3] += fminf(1.0f, fmaxf(-1.0f, a.ls.at(gx, gy) / (float)a.ny));
+            acc[4] += mask[p] ? 1.0f : 0.0f;
+        }
+    const float nrm = 1.0f / (float)(f * f);
+    __align__(16) bf16 v[16];
+#pragma unroll
+    for (int c = 0; c < 16; ++c) v[c] = __float2bfloat16_rn(c < 5 ? acc[c] * nrm : 0.0f);
+    const size_t q = (size_t)cy * Wc + cx;
+    uint4* dst = reinterpret_cast<uint4*>(x0 + q * 16);
+    dst[0] = reinterpret_cast<const uint4*>(v)[0];
+    dst[1] = reinterpret_cast<const uint4*>(v)[1];
+    maskc[q] = acc[4] > 0.0f ? 1 : 0;
+}
+// x += sigma * (the coarse prediction interpolated bilinearly, coarse cell
+// (i, j) centred on fine coordinate ((i + 1/2) f - 1/2, ...), clamped at the
+// edges) on the counted cells.
+__global__ void k_unet_warm_coarse(Plane<double> x, const float* outc, const unsigned char* mask, const float* sigma,
+                                   int nx, int ny, int f) {
+    const int gx = blockIdx.x * blockDim.x + threadIdx.x, gy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (gx >= nx || gy >= ny || !mask[(size_t)gy * nx + gx]) return;
+    const int Wc = nx / f, Hc = ny / f;
+    const float u = ((float)gx + 0.5f) / (float)f - 0.5f, v = ((float)gy + 0.5f) / (float)f - 0.5f;
+    int i0 = (int)floorf(u), j0 = (int)floorf(v);
+    float tu = u - (float)i0, tv = v - (float)j0;
+    if (i0 < 0) i0 = 0, tu = 0.0f;
+    if (i0 >= Wc - 1) i0 = Wc - 1, tu = 0.0f;
+    if (j0 < 0) j0 = 0, tv = 0.0f;
+    if (j0 >= Hc - 1) j0 = Hc - 1, tv = 0.0f;
+    const int i1 = min(i0 + 1, Wc - 1), j1 = min(j0 + 1, Hc - 1);
+    const float o00 = outc[((size_t)j0 * Wc + i0) * 16], o10 = outc[((size_t)j0 * Wc + i1) * 16];
+    const float o01 = outc[((size_t)j1 * Wc + i0) * 16], o11 = outc[((size_t)j1 * Wc + i1) * 16];
+    const float val = (o00 * (1.0f - tu) + o10 * tu) * (1.0f - tv) + (o01 * (1.0f - tu) + o11 * tu) * tv;
+    x.at(gx, gy) = x.at(gx, gy) + (double)*sigma * (double)val;
+}
+// Coarse training target: the mean of (p - p_prev) / sigma over the block's counted cells (0 if none).
+__global__ void k_unet_target_coarse(Plane<double> x, const float* prev32, const unsigned char* mask,
+                                     const float* sigma, int nx, int ny, int f, float* targetc) {
+    const int Wc = nx / f, Hc = ny / f;
+    const int cx = blockIdx.x * blockDim.x + threadIdx.x, cy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (cx >= Wc || cy >= Hc) return;
+    double acc = 0.0;
+    int cnt = 0;
+    for (int j = 0; j < f; ++j)
+        for (int i = 0; i < f; ++i) {
+            const int gx = cx * f + i, gy = cy * f + j;
+            const size_t p = (size_t)gy * nx + gx;
+            if (mask[p]) {
+                acc += x.at(gx, gy) - (double)prev32[p];
+                ++cnt;
+            }
+        }
+    targetc[(size_t)cy * Wc + cx] = cnt ? (float)(acc / cnt / (double)*sigma) : 0.0f;
+}
 // Relative squared error of one sample, sum_mask (pred - t)^2 / sum_mask t^2:
 // g_out[p][0] = 2 (pred - t) * inv_norm (inv_norm = 1 / sum_mask t^2), and
 // per-block partial sums of (pred - t)^2.
@@ -975,6 +1050,9 @@ struct UNet {
     float2* lpart;
     float *target, *prev32, *res32, *sigma;
     unsigned char* mask;
+    int coarse = 1;          // the grid coarsening factor f of the warm start (1, 2, 4 or 8)
+    float* targetc;          // coarse training target and mask (coarse form)
+    unsigned char* maskc;
     int* err;
     void* arena = nullptr;
     std::vector<void*> extra;
@@ -1036,6 +1114,8 @@ inline cudaError_t unet_alloc(UNet& n, int maxH, int maxW) {
     F(&n.res32, P0);
     F(&n.sigma, 64);
     items.push_back({(void**)&n.mask, up256(P0)});
+    F(&n.targetc, P0);
+    items.push_back({(void**)&n.maskc, up256(P0)});
     items.push_back({(void**)&n.err, 256});
     size_t total = 0;
     for (auto& it : items) total += it.bytes;
@@ -1048,6 +1128,60 @@ inline cudaError_t unet_alloc(UNet& n, int maxH, int maxW) {
         *it.ptr = base;
         base += it.bytes;
     }
+    return cudaSuccess;
+}
+
+// A forward-only workspace of a network for one simulation of a batch: a
+// copy of `net` (weights, biases and their device copies shared) whose
+// activations and feature buffers are its own, sized for that simulation's
+// fine grid fh x fw and its network grid (fh / f) x (fw / f).  Forwards of
+// different simulations can then run at the same time on their own streams.
+inline cudaError_t unet_alloc_forward(UNet& v, const UNet& net, int fh, int fw) {
+    v = net;
+    v.arena = nullptr;
+    v.extra.clear();
+    v.last_error.clear();
+    const int f = net.coarse;
+    v.maxH = fh;
+    v.maxW = fw;
+    const size_t P0 = (size_t)(fh / f) * (fw / f), P1 = P0 / 4, P2 = P0 / 16, P3 = P0 / 64, PF_ = (size_t)fh * fw;
+    struct Item {
+        void** ptr;
+        size_t bytes;
+    };
+    std::vector<Item> items;
+    auto F = [&](float** p, size_t n_) { items.push_back({(void**)p, up256(n_ * 4)}); };
+    auto B = [&](bf16** p, size_t n_) { items.push_back({(void**)p, up256(n_ * 2)}); };
+    B(&v.X0, P0 * 16); B(&v.t0, P0 * 16); B(&v.cat0, P0 * 48);
+    B(&v.p1, P1 * 16); B(&v.t1, P1 * 32); B(&v.cat1, P1 * 96);
+    B(&v.p2, P2 * 32); B(&v.t2, P2 * 64); B(&v.cat2, P2 * 128);
+    B(&v.p3, P3 * 64); B(&v.t3, P3 * 64); B(&v.u3, P3 * 64);
+    B(&v.t4, P2 * 64); B(&v.u4, P2 * 64); B(&v.t5, P1 * 32); B(&v.u5, P1 * 32);
+    B(&v.t6, P0 * 16); B(&v.u6, P0 * 16);
+    F(&v.out, P0 * 16);
+    items.push_back({(void**)&v.lpart, up256((PF_ / 256 + (size_t)fw / 32 + (size_t)fh / 8 + 8) * sizeof(float2))});
+    F(&v.prev32, PF_);
+    F(&v.res32, PF_);
+    F(&v.sigma, 64);
+    items.push_back({(void**)&v.mask, up256(PF_)});
+    items.push_back({(void**)&v.maskc, up256(P0)});
+    items.push_back({(void**)&v.err, 256});
+    size_t total = 0;
+    for (auto& it : items) total += it.bytes;
+    cudaError_t e = cudaMalloc(&v.arena, total);
+    if (e != cudaSuccess) return e;
+    e = cudaMemset(v.arena, 0, total);
+    if (e != cudaSuccess) return e;
+    char* base = (char*)v.arena;
+    for (auto& it : items) {
+        *it.ptr = base;
+        base += it.bytes;
+    }
+    // nothing of the training state belongs to a forward-only workspace
+    v.grads = v.adam_m = v.adam_v = nullptr;
+    v.target = v.targetc = nullptr;
+    v.wpart = v.bpart = nullptr;
+    v.dym = nullptr;
     return cudaSuccess;
 }
 

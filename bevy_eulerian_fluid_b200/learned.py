@@ -10,12 +10,21 @@ compares the solver's iterations and time.
 """
 from __future__ import annotations
 
+import copy
+import math
+import os
 import time
 from dataclasses import dataclass, field
-from typing import List
+from typing import List, Optional
+
+import numpy as np
 
 from . import _capi as capi
 from . import scenes
+
+# Weights of the network trained offline by `pretrain` (python -m bevy_eulerian_fluid_b200.learned):
+# the FP32 master parameters, the coarsening factor they were trained for, and how they were made.
+WEIGHTS_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights", "unet_warm_start.npz")
 
 
 # (cin, cout) of the network's 15 convolutions and the level each runs at
@@ -38,12 +47,14 @@ class TrainLog:
 
 def train(api: capi.Api, size: int = 256, seeds=(1, 2, 3, 4), steps: int = 200, lr: float = 1e-3,
           n_per_shape: int = 6, net: capi.UNet | None = None, max_size: int | None = None,
-          device: int = 0, extra=()) -> tuple[capi.UNet, TrainLog]:
+          device: int = 0, extra=(), coarse: int = 1) -> tuple[capi.UNet, TrainLog]:
     """Online training: every simulation step records one sample, one Adam step follows.
-    Scenes: C2-style coupled scenes at `size` for `seeds`, plus (size, seed) pairs in `extra`."""
+    Scenes: C2-style coupled scenes at `size` for `seeds`, plus (size, seed) pairs in `extra`;
+    the network runs on the grid coarsened by `coarse`."""
     runs = [(size, s) for s in seeds] + list(extra)
     big = max(sz for sz, _ in runs)
     net = net or capi.UNet(api, max(max_size or 0, big), max(max_size or 0, big), seed=0xC5, device=device)
+    net.set_coarsening(coarse)
     sims = []
     for sz, s in runs:
         sc = scenes.coupled(sz, seed=s, n_per_shape=n_per_shape, method=capi.PROJECTION_MGPCG)
@@ -102,3 +113,188 @@ def compare(api: capi.Api, net: capi.UNet, scene: scenes.Scene, warmup: int = 5,
     a.close()
     b.close()
     return out
+
+
+def fp64_solve(phi: np.ndarray, af: np.ndarray, b: np.ndarray, dx: float, dt: float, rho: float):
+    """Sparse direct FP64 solve (CPU) of the pressure system the projection iterates on: the operator of
+    residual.wgsl:33-54 (ghost-fluid weights f (1 - phi_j / phi_i) for air neighbours) over the counted
+    cells (phi < 0, not fully solid).  Returns (x on a full grid, the counted-cell mask)."""
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spla
+    H, W = phi.shape
+    phi = phi.astype(np.float64)
+    act = (phi < 0) & ~(af == 0).all(-1)
+    idx = -np.ones((H, W), np.int64)
+    idx[act] = np.arange(int(act.sum()))
+    fac = dt / rho / dx / dx
+    ys, xs = np.nonzero(act)
+    rows, cols, vals = [], [], []
+    diag = np.zeros(len(ys))
+    for k, (ox, oy) in enumerate(((-1, 0), (1, 0), (0, -1), (0, 1))):
+        jx, jy = xs + ox, ys + oy
+        inb = (jx >= 0) & (jx < W) & (jy >= 0) & (jy < H)
+        f = af[ys, xs, k].astype(np.float64)
+        pj = np.where(inb, phi[np.clip(jy, 0, H - 1), np.clip(jx, 0, W - 1)], 0.0)
+        fluid = inb & (pj < 0)
+        air = inb & ~fluid
+        diag += np.where(fluid, f, 0.0) + np.where(air, f * (1.0 - pj / phi[ys, xs]), 0.0)
+        nb = np.where(fluid, idx[np.clip(jy, 0, H - 1), np.clip(jx, 0, W - 1)], -1)
+        sel = nb >= 0
+        rows.append(idx[ys, xs][sel])
+        cols.append(nb[sel])
+        vals.append(-f[sel] * fac)
+    rows.append(idx[ys, xs])
+    cols.append(idx[ys, xs])
+    vals.append(diag * fac)
+    n = int(act.sum())
+    A = sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))), shape=(n, n))
+    x = np.zeros((H, W))
+    x[act] = spla.spsolve(A.tocsc(), b[act].astype(np.float64))
+    return x, act
+
+
+def _block_mean(a: np.ndarray, m: np.ndarray, f: int) -> np.ndarray:
+    H, W = a.shape
+    s = (a * m).reshape(H // f, f, W // f, f).sum(axis=(1, 3))
+    c = m.reshape(H // f, f, W // f, f).sum(axis=(1, 3))
+    return np.where(c > 0, s / np.maximum(c, 1), 0.0)
+
+
+def prediction_error(api: capi.Api, net: capi.UNet, scene: scenes.Scene, warmup: int = 5, block: int = 8) -> dict:
+    """The network's warm start judged against an FP64 CPU solve of the same Poisson system: after `warmup`
+    steps, the stages before the projection, then the projection with no iterations (the start iterate
+    only: previous pressure + the network's correction), against a sparse direct solve x* of that system.
+    captured = 1 - |x_start - x*| / |p_prev - x*| (the share of the correction the network supplies, 1 =
+    all of it), also for the block means over `block` x `block` cells (the part the sweeps remove slowest),
+    and |x_start - x*| / |x*|."""
+    sim = scene.make(api)
+    sim.step(scene.dt)
+    for _ in range(warmup):
+        sim.step(scene.dt)
+    for st in range(capi.STAGE_UPDATE_SOLID, capi.STAGE_DIVERGENCE + 1):
+        sim.run_stage(st, scene.dt)
+    p_prev = sim.get(capi.FIELD_PRESSURE).astype(np.float64)
+    proj = capi.Projection()
+    import ctypes
+    ctypes.memmove(ctypes.byref(proj), ctypes.byref(scene.cfg.projection), ctypes.sizeof(proj))
+    proj.max_iterations = 0
+    sim.set_projection(proj)
+    net.attach(sim, warm_start=True)
+    sim.run_stage(capi.STAGE_PROJECTION, scene.dt)
+    net.attach(sim, warm_start=False)
+    start = sim.get(capi.FIELD_PRESSURE).astype(np.float64)
+    phi, af, b = sim.get(capi.FIELD_LEVELSET_AIR), sim.get(capi.FIELD_AREA_FRACTION), sim.get(capi.FIELD_DIVERGENCE)
+    sim.close()
+    dx = float(np.float32(1.0) / np.float32(scene.cfg.length_unit))
+    x, act = fp64_solve(phi, af, b, dx, float(np.float32(scene.dt)), float(np.float32(scene.cfg.rho)))
+    m = act.astype(np.float64)
+    e_prev = np.linalg.norm((p_prev - x)[act])
+    e_start = np.linalg.norm((start - x)[act])
+    bp, bs, bx = (_block_mean(v, m, block) for v in (p_prev, start, x))
+    ce_prev, ce_start = np.linalg.norm(bp - bx), np.linalg.norm(bs - bx)
+    return {"captured": float(1.0 - e_start / e_prev) if e_prev > 0 else 0.0,
+            "captured_block_means": float(1.0 - ce_start / ce_prev) if ce_prev > 0 else 0.0,
+            "relative_error_start": float(e_start / np.linalg.norm(x[act])),
+            "relative_error_previous": float(e_prev / np.linalg.norm(x[act])), "block": block,
+            "cells": int(act.sum())}
+
+
+def save_weights(net: capi.UNet, coarse: int, info: dict, path: str = WEIGHTS_PATH) -> None:
+    os.makedirs(os.path.dirname(path), exist_ok=True)
+    np.savez(path, params=net.get_params(), coarse=np.int32(coarse),
+             info=np.array(repr(sorted(info.items()))))
+
+
+def load_weights(api: capi.Api, max_nx: int, max_ny: int, path: str = WEIGHTS_PATH,
+                 device: int = 0) -> Optional[capi.UNet]:
+    """The pretrained network (None if the weights file is absent), coarsening set as trained."""
+    if not os.path.exists(path):
+        return None
+    d = np.load(path)
+    net = capi.UNet(api, max_nx, max_ny, seed=0xC5, device=device)
+    net.set_params(d["params"])
+    net.set_coarsening(int(d["coarse"]))
+    return net
+
+
+def pretrain(api: capi.Api, samples: int = 50000, coarse: int = 8, lr: float = 1e-3, lr_final: float = 5e-5,
+             episode: int = 120, live: int = 8, sizes=((256, 3), (512, 1)), seed0: int = 1000,
+             device: int = 0, log=print) -> tuple[capi.UNet, TrainLog]:
+    """Offline training for the committed weights: `samples` (input, converged correction) pairs from
+    C2-style scenes (water in the lower 40 %, 24 random bodies) with the two-way coupling loop, solved
+    by MGPCG to 1e-5.  `live` scenes step round-robin; each lives `episode` steps and is then replaced
+    by a scene of a fresh seed (seeds from seed0, sizes drawn with the given weights), so the samples
+    span the splash and the settling of many configurations.  Every step records one sample and one
+    Adam step (cosine learning-rate decay from lr to lr_final) follows."""
+    from .plugin import pack_obstacles
+    from .rigid import RigidWorld
+    big = max(sz for sz, _ in sizes)
+    net = capi.UNet(api, big, big, seed=0xC5, device=device)
+    net.set_coarsening(coarse)
+    rng = np.random.default_rng(seed0)
+    pool = [sz for sz, w in sizes for _ in range(w)]
+    next_seed = [seed0]
+
+    def spawn():
+        sz = int(pool[int(rng.integers(0, len(pool)))])
+        sc = scenes.coupled(sz, seed=next_seed[0], method=capi.PROJECTION_MGPCG)
+        next_seed[0] += 1
+        sc.cfg.device = device
+        sim = sc.make(api)
+        sim.step(sc.dt)
+        rigid = RigidWorld(copy.deepcopy(list(sc.bodies)), (sz, sz), gravity=9.8 * scenes.LENGTH_UNIT,
+                           grid_length=1.0 / scenes.LENGTH_UNIT)
+        net.attach(sim, warm_start=False, record=True)
+        return [sc, sim, rigid, 0]
+
+    live_sims = [spawn() for _ in range(live)]
+    tl = TrainLog()
+    t0 = time.time()
+    while tl.samples < samples:
+        for slot in range(live):
+            sc, sim, rigid, age = live_sims[slot]
+            sim.step(sc.dt)
+            rigid.apply_fluid_forces(sim.solid_forces(), sc.dt)
+            rigid.step(sc.dt)
+            sim.set_obstacles(pack_obstacles(rigid.bodies))
+            frac = tl.samples / samples
+            rate = lr_final + 0.5 * (lr - lr_final) * (1.0 + math.cos(math.pi * frac))
+            tl.losses.append(net.train_step(rate))
+            tl.samples += 1
+            live_sims[slot][3] = age + 1
+            if age + 1 >= episode:
+                net.attach(sim, warm_start=False, record=False)
+                sim.close()
+                live_sims[slot] = spawn()
+            if tl.samples % 5000 == 0 and log:
+                log(f"{tl.samples} samples, {time.time() - t0:.0f} s, mean relative loss of the last 1000 "
+                    f"{np.mean(tl.losses[-1000:]):.4f}")
+            if tl.samples >= samples:
+                break
+    tl.seconds = time.time() - t0
+    for _, sim, _, _ in live_sims:
+        net.attach(sim, warm_start=False, record=False)
+        sim.close()
+    return net, tl
+
+
+def main():
+    import argparse
+    ap = argparse.ArgumentParser(description="offline training of the learned warm start's weights")
+    ap.add_argument("--samples", type=int, default=50000)
+    ap.add_argument("--coarse", type=int, default=8)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--out", default=WEIGHTS_PATH)
+    args = ap.parse_args()
+    api = capi.load()
+    net, tl = pretrain(api, samples=args.samples, coarse=args.coarse, lr=args.lr)
+    q = max(1, len(tl.losses) // 10)
+    info = {"samples": tl.samples, "seconds": round(tl.seconds, 1), "coarse": args.coarse,
+            "scenes": "C2-style coupled 256^2 (3 of 4) and 512^2 (1 of 4), seeds from 1000, MGPCG to 1e-5",
+            "relative_loss_by_tenth": [round(float(np.mean(tl.losses[i * q:(i + 1) * q])), 4) for i in range(10)]}
+    save_weights(net, args.coarse, info, args.out)
+    print(info)
+
+
+if __name__ == "__main__":
+    main()

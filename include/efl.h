@@ -510,8 +510,23 @@ EFL_API efl_status efl_unet_gradients(efl_unet* net, uint32_t nx, uint32_t ny, c
 EFL_API efl_status efl_unet_time_forward(efl_unet* net, uint32_t nx, uint32_t ny, uint32_t reps, float* ms);
 /* flags: EFL_UNET_WARM_START (warm-start sim's tolerance-driven solves),
  * EFL_UNET_RECORD (record each solve as a training sample); 0 detaches.
- * Batches (efl_batch_step) do not use it. */
+ * For the simulations of a batch use efl_batch_attach_unet. */
 EFL_API efl_status efl_unet_attach(efl_sim* sim, efl_unet* net, uint32_t flags);
+/* Runs the network on the grid coarsened by `factor` (1, 2, 4 or 8): the
+ * features are averaged over factor x factor cells, the prediction is
+ * interpolated back bilinearly, and recorded training targets are the block
+ * means of the correction.  The sweeps remove the basin-scale error slowest,
+ * and four levels of pooling on the coarse grid span it.  Attached grids must
+ * be multiples of 8 x factor.  Default 1 (the network on the simulation's own
+ * grid); a recorded sample of the other form is dropped. */
+EFL_API efl_status efl_unet_set_coarsening(efl_unet* net, uint32_t factor);
+/* Attaches the network to every simulation of a batch (flags:
+ * EFL_UNET_WARM_START, or 0 to detach).  Each simulation gets a forward-only
+ * workspace of its own (weights shared), so that the simulations' forwards
+ * run side by side inside the batch step, and each simulation's warm start,
+ * iterates and iteration counts are those of its own efl_step with the
+ * network attached.  Attach again after efl_unet_set_coarsening. */
+EFL_API efl_status efl_batch_attach_unet(efl_batch* batch, efl_unet* net, uint32_t flags);
 /* One Adam step (lr; beta 0.9 / 0.999; gradient clipped to global norm 1)
  * on the last recorded sample. */
 EFL_API efl_status efl_unet_train_step(efl_unet* net, float lr, float* loss);

@@ -91,3 +91,42 @@ def test_batch_fast_path_graphs_match_oracle(oracle_api, gpu_api):
         for i, (g, o) in enumerate(zip(batch.sims, oracles)):
             bad = compare_fields(g, o)
             assert not bad, (i, bad)
+
+
+@pytest.mark.parametrize("coarse", [4, 1])
+def test_batch_with_network_matches_single_sims(gpu_api, coarse):
+    """efl_batch_attach_unet: every simulation's solve is warm-started by the network inside the batch step (one
+    forward workspace per simulation, forwards side by side); each simulation still equals the same simulation
+    stepped alone by efl_step with the network attached -- bit-exact fields, equal iteration counts -- and every
+    solve still reaches the tolerance."""
+    b = _small_batch(5, seed=0xB1)
+    net = capi.UNet(gpu_api, 192, 192, seed=7)
+    rng = np.random.default_rng(1)
+    p = net.get_params()
+    net.set_params(p + rng.standard_normal(p.size).astype(np.float32) * 0.02)  # a non-zero head: a real warm start
+    net.set_coarsening(coarse)
+    singles = [sc.make(gpu_api) for sc in b.scenes]
+    for s in singles:
+        net.attach(s, warm_start=True)
+    with capi.Batch(gpu_api, b.configs()) as batch:
+        b.setup(batch.sims)
+        batch.attach_unet(net)
+        for k in range(5):
+            for i, s in enumerate(singles):
+                f = b.forces(i, k)
+                if f:
+                    s.set_local_forces(f)
+                    batch[i].set_local_forces(f)
+            gst = batch.step(b.scenes[0].dt)
+            sst = [s.step(b.scenes[0].dt) for s in singles]
+            for i, (g, s) in enumerate(zip(gst, sst)):
+                assert g.pressure_iterations == s.pressure_iterations, (k, i)
+                assert g.converged == s.converged == 1, (k, i)
+                assert abs(g.residual - s.residual) <= 1e-9 * max(1.0, abs(s.residual)), (k, i)
+        for i, (g, s) in enumerate(zip(batch.sims, singles)):
+            bad = compare_fields(g, s)
+            assert not bad, (i, bad)
+        batch.attach_unet(net, warm_start=False)
+    for s in singles:
+        s.close()
+    net.close()

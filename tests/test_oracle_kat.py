@@ -244,3 +244,17 @@ def test_error_behaviour(oracle_api):
     with pytest.raises(capi.EflError) as e:
         s.set_sources([capi.Source() for _ in range(capi.MAX_FLUID_SOURCE + 1)], False)
     assert e.value.status == capi.ERR_TOO_MANY
+
+
+def test_learned_fp64_solve_matches_operator_restatement(oracle_api):
+    """learned.fp64_solve (the FP64 CPU solve that judges the network's prediction) builds the same system as
+    the loop restatement above and solves it: equal matrices, and A x = b to round-off."""
+    from bevy_eulerian_fluid_b200 import learned
+    sc, s = _projection_inputs(oracle_api)
+    phi, af, b = s.get(capi.FIELD_LEVELSET_AIR), s.get(capi.FIELD_AREA_FRACTION), s.get(capi.FIELD_DIVERGENCE)
+    dx, dt, rho = float(np.float32(1) / np.float32(10)), float(np.float32(sc.dt)), float(np.float32(sc.cfg.rho))
+    A, act = _operator(phi, af, dx, dt, rho)
+    x, act2 = learned.fp64_solve(phi, af, b, dx, dt, rho)
+    assert np.array_equal(act, act2)
+    r = A @ x[act] - b[act].astype(np.float64)
+    assert np.linalg.norm(r) <= 1e-9 * np.linalg.norm(b[act].astype(np.float64))
