@@ -956,7 +956,31 @@ def c3_leg(api, torch, args, local, peak):
                                       "note": "272 algorithmic B per fine cell per V-cycle x V-cycles / solve time"}}
     out["value"] = out["mgpcg"]["value"]
     out["speedup_mgpcg_vs_vcycles"] = round(out["mgpcg"]["value"] / out["vcycles"]["value"], 2)
+    if not args.no_cpu_baseline:
+        out["cpu_baseline"] = c3_cpu_baseline(n)
     return out
+
+
+def c3_cpu_baseline(n: int, steps: int = 2):
+    """The CPU oracle on scale_n with MGPCG to 1e-5: the first `steps` steps after the init sequence (the
+    early steps need the most CG iterations, so this sample is slower per step than the GPU's window)."""
+    from bevy_eulerian_fluid_b200 import _capi as capi
+    from bevy_eulerian_fluid_b200 import scenes
+    from oracle import py_oracle
+    api = py_oracle.load()
+    py_oracle.set_threads(os.cpu_count() or 1)
+    sc = scenes.scale(n)
+    sc.cfg.projection.method = capi.PROJECTION_MGPCG
+    sim = sc.make(api)
+    sim.step(sc.dt)
+    t0 = time.perf_counter()
+    iters = [int(sim.step(sc.dt).pressure_iterations) for _ in range(steps)]
+    el = time.perf_counter() - t0
+    sim.close()
+    cores = py_oracle.get_threads()
+    return {"value": n * n * steps / el, "unit": "cell-steps/s", "cores": cores, "kind": "port",
+            "sample": f"the first {steps} steps after the init sequence of scale_{n} (MGPCG to 1e-5, CG iterations "
+                      f"{iters}) on the CPU oracle, {cores} host threads, {el:.1f} s"}
 
 
 def microbench(api, stream, torch, peak):
