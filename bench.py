@@ -545,10 +545,11 @@ def batch_shard(n_sims: int, world: int, rank: int):
 
 
 def batch_leg(api, torch, args, world, rank, local, dist):
-    """C4: the batched path and the plain path over this rank's shard of the
+    """C4: the batched path, the batched path with the learned warm start (the pretrained network attached
+    to every simulation, forwards inside the batch step), and the plain path over this rank's shard of the
     96-simulation batch; value = all ranks' cells x steps / max-over-ranks time."""
     from bevy_eulerian_fluid_b200 import _capi as capi
-    from bevy_eulerian_fluid_b200 import scenes
+    from bevy_eulerian_fluid_b200 import learned, scenes
     bs = scenes.batch(args.batch_sims)
     shard = batch_shard(len(bs.scenes), world, rank)
     cfgs = bs.configs()
@@ -563,37 +564,45 @@ def batch_leg(api, torch, args, world, rank, local, dist):
             if f:
                 sims[j].set_local_forces(f)
 
-    # batched
-    bt = capi.Batch(api, [cfgs[i] for i in shard])
-    for j, i in enumerate(shard):
-        bt[j].set_sources(bs.scenes[i].oneshot, True)
-    bstream = torch.cuda.ExternalStream(bt[0].stream(), device=f"cuda:{local}")
-    bt.step(dt)
-    k = 0
     warm_b = max(args.warmup, 5)  # the tile autotuner tries its four configurations on the first four solves
-    for _ in range(warm_b):
-        k += 1
-        forces(bt.sims, k)
+
+    def batched(net=None):
+        bt = capi.Batch(api, [cfgs[i] for i in shard])
+        for j, i in enumerate(shard):
+            bt[j].set_sources(bs.scenes[i].oneshot, True)
+        if net is not None:
+            bt.attach_unet(net)
+        bstream = torch.cuda.ExternalStream(bt[0].stream(), device=f"cuda:{local}")
         bt.step(dt)
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    solve_b, iters = [], []
-    launches0 = api.kernel_launches()
-    e0.record(bstream)
-    for _ in range(steps):
-        k += 1
-        forces(bt.sims, k)
-        st = bt.step(dt)
-        solve_b.append(bt.projection_ms())
-        iters.extend(int(x.pressure_iterations) for x in st)
-    e1.record(bstream)
-    torch.cuda.synchronize()
-    launches_b = api.kernel_launches() - launches0
-    ms_b = e0.elapsed_time(e1)
-    tiles, tile_cost = bt.tiles()
-    bt.close()
+        k = 0
+        for _ in range(warm_b):
+            k += 1
+            forces(bt.sims, k)
+            bt.step(dt)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        solve, its = [], []
+        l0 = api.kernel_launches()
+        e0.record(bstream)
+        for _ in range(steps):
+            k += 1
+            forces(bt.sims, k)
+            st = bt.step(dt)
+            solve.append(bt.projection_ms())
+            its.extend(int(x.pressure_iterations) for x in st)
+        e1.record(bstream)
+        torch.cuda.synchronize()
+        out = (e0.elapsed_time(e1), solve, its, api.kernel_launches() - l0, bt.tiles())
+        bt.close()
+        return out
+
+    ms_b, solve_b, iters, launches_b, (tiles, tile_cost) = batched()
+    net = learned.load_weights(api, 768, 768, device=local)
+    lw = batched(net) if net is not None else None
+    if net is not None:
+        net.close()
 
     # plain: efl_step per simulation, device time summed over the simulations' streams
     sims = []
@@ -632,7 +641,7 @@ def batch_leg(api, torch, args, world, rank, local, dist):
         s_.close()
 
     cells_rank = sum(bs.scenes[i].cells for i in shard)
-    t = [ms_b, ms_p, sum(solve_b), sum(solve_p)]
+    t = [ms_b, ms_p, sum(solve_b), sum(solve_p), lw[0] if lw else 0.0, sum(lw[1]) if lw else 0.0]
     if dist:
         tt = torch.tensor(t, device=f"cuda:{local}", dtype=torch.float64)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
@@ -652,6 +661,12 @@ def batch_leg(api, torch, args, world, rank, local, dist):
                       "simulations; tile shape and iterations per round chosen by the autotuner)",
             "autotuner_ns_per_cell_iteration": {"64x32x2": round(tile_cost[0], 4), "64x32x4": round(tile_cost[1], 4),
                                                 "32x32x2": round(tile_cost[2], 4), "64x32x8": round(tile_cost[3], 4)},
+            "learned": ({"value": cells * steps / (t[4] / 1e3), "speedup_vs_plain": round(t[1] / t[4], 3),
+                         "ms_per_step": t[4] / steps, "pressure_solve_ms_per_step": t[5] / steps,
+                         "pressure_iterations": {"max": max(lw[2]), "mean": round(sum(lw[2]) / len(lw[2]), 1)},
+                         "network": "pretrained weights (bevy_eulerian_fluid_b200/weights), attached with "
+                                    "efl_batch_attach_unet: one forward per simulation inside the batch step"}
+                        if lw else None),
             "gpu_launches_batched": int(launches_b),
             "l2": "not flushed: the batch's working set (GBs) exceeds L2",
             "sharding": f"simulation i on rank i % {world}"}
@@ -867,14 +882,21 @@ def tensor_peak():
 
 
 def learned_leg(api, args, local):
-    """The learned warm start: trained on the GPU (tensor-core forward and
-    backward) from C2-style scenes (seeds 1-8 at 256^2, 9-10 at 512^2), then
-    coupled_512 (the benchmark scene, RBGS to 1e-5) and the 1024^2 evaluation
-    scene with 32 bodies (MGPCG to 1e-5) each stepped twice from the same
-    states, warm-started by the network and from the previous pressure."""
+    """The learned warm start: the network pretrained offline on the GPU (tensor-core forward and backward;
+    weights committed under bevy_eulerian_fluid_b200/weights), or, without that file, a short online training
+    on C2-style scenes; then coupled_512 (the benchmark scene, RBGS to 1e-5) and the 1024^2 evaluation scene
+    with 32 bodies (MGPCG to 1e-5) each stepped twice from the same states, warm-started by the network and
+    from the previous pressure, and the prediction judged against an FP64 CPU solve of the same system."""
     from bevy_eulerian_fluid_b200 import capi, learned, scenes
-    net, log = learned.train(api, size=256, seeds=tuple(range(1, 9)), steps=100, lr=1e-3,
-                             max_size=max(args.size, C5_EVAL_SIZE), device=local, extra=((512, 9), (512, 10)))
+    big = max(args.size, C5_EVAL_SIZE)
+    net = learned.load_weights(api, big, big, device=local)
+    pretrained = net is not None
+    if pretrained:
+        info = str(np.load(learned.WEIGHTS_PATH)["info"])
+        log = None
+    else:  # no committed weights: a short online training on the GPU
+        net, log = learned.train(api, size=256, seeds=tuple(range(1, 9)), steps=100, lr=1e-3, max_size=big,
+                                 device=local, extra=((512, 9), (512, 10)))
     sc = scenes.coupled(args.size)
     sc.cfg.device = local
     cmp = learned.compare(api, net, sc, warmup=args.warmup, steps=max(1, min(args.steps, 6)))
@@ -885,11 +907,20 @@ def learned_leg(api, args, local):
     ms = net.time_forward(args.size, args.size, 20)
     tf = learned.forward_flops(args.size, args.size) / (ms / 1e3) / 1e12
     peak, kind = tensor_peak()
-    q = len(log.losses) // 4
-    out = {"training": {"samples": log.samples, "seconds": round(log.seconds, 2),
-                        "grid": "256^2 (seeds 1-8) and 512^2 (seeds 9, 10)",
-                        "relative_loss_by_quarter": [round(sum(log.losses[i * q:(i + 1) * q]) / max(1, q), 4)
-                                                     for i in range(4)]},
+    if pretrained:
+        training = {"weights": "pretrained offline (python -m bevy_eulerian_fluid_b200.learned), loaded from "
+                               "bevy_eulerian_fluid_b200/weights/unet_warm_start.npz", "info": info}
+    else:
+        q = len(log.losses) // 4
+        training = {"samples": log.samples, "seconds": round(log.seconds, 2),
+                    "grid": "256^2 (seeds 1-8) and 512^2 (seeds 9, 10)",
+                    "relative_loss_by_quarter": [round(sum(log.losses[i * q:(i + 1) * q]) / max(1, q), 4)
+                                                 for i in range(4)]}
+    fp64 = learned.prediction_error(api, net, scenes.coupled(args.size), warmup=args.warmup)
+    out = {"training": training,
+           "prediction_vs_fp64_solve": dict(fp64, note="start iterate (previous pressure + the network's "
+                                                        "correction) against a sparse direct FP64 CPU solve of the "
+                                                        "same system; captured = share of the correction supplied"),
            "workload": f"coupled_{args.size} (RBGS to 1e-5), {len(cmp['plain'])} steps after {args.warmup} warm-up",
            "iterations": {"learned": [x[0] for x in cmp["learned"]], "plain": [x[0] for x in cmp["plain"]]},
            "initial_residual": {"learned": [round(x[1], 5) for x in cmp["learned"]],

@@ -1075,6 +1075,118 @@ __global__ void k_fim_phase_b(PF T, PU LT, PF S, PU L, Dom d) {
     }
 }
 
+// All iterations of the two-phase FIM update (k_fim_phase_a then
+// k_fim_phase_b, `iters` times) in one launch, temporally blocked: a CTA
+// holds its 32 x 32 tile plus a halo of FIM_HALO cells in shared memory and
+// runs the iterations there.  One iteration's result at a cell depends on
+// cells at most 2 away (phase A reads radius 1, phase B reads phase A's
+// result at radius 1), so values go wrong only near the image edge, 2 cells
+// deeper per iteration: with iters <= FIM_HALO / 2 the owned tile is exact.
+// A cell changes only while it is active, and activity spreads one cell per
+// iteration, so a tile whose image holds no active cell is left untouched
+// (most of a large grid, away from the interface): such CTAs read the labels
+// and leave.
+constexpr int FIM_TILE = 32, FIM_HALO = 20, FIM_IMG = FIM_TILE + 2 * FIM_HALO, FIM_THREADS = 512;
+constexpr size_t FIM_SMEM = (size_t)4 * FIM_IMG * FIM_IMG * 4;
+__global__ void __launch_bounds__(FIM_THREADS) k_fim_tiled(PF S, PU L, Dom d, int iters, int tiles_x) {
+    extern __shared__ __align__(16) unsigned char fim_raw[];
+    constexpr int N = FIM_IMG * FIM_IMG;
+    float* s = reinterpret_cast<float*>(fim_raw);
+    float* t = s + N;
+    uint32_t* l = reinterpret_cast<uint32_t*>(t + N);
+    uint32_t* lt = l + N;
+    const int x0 = (int)(blockIdx.x % tiles_x) * FIM_TILE - FIM_HALO, y0 = (int)(blockIdx.x / tiles_x) * FIM_TILE - FIM_HALO;
+    const int W = d.nx, H = d.ny;  // the dispatch domain (sizes are multiples of 8) and the planes' extent
+    int act = 0;
+    for (int i = threadIdx.x; i < N; i += FIM_THREADS) {
+        const int gx = x0 + i % FIM_IMG, gy = y0 + i / FIM_IMG;
+        const bool in = gx >= 0 && gy >= 0 && gx < W && gy < H;
+        const uint32_t lv = in ? L.at(gx, gy) : LABEL_NONE;
+        l[i] = lv;
+        act |= lv == LABEL_ACTIVE;
+    }
+    if (!__syncthreads_or(act)) return;
+    for (int i = threadIdx.x; i < N; i += FIM_THREADS) {
+        const int gx = x0 + i % FIM_IMG, gy = y0 + i / FIM_IMG;
+        s[i] = (gx >= 0 && gy >= 0 && gx < W && gy < H) ? S.at(gx, gy) : 0.0f;
+    }
+    __syncthreads();
+    // |phi| of a neighbour: FIM_LARGE outside the domain (update.wgsl:56-60) and, where the image ends,
+    // a stand-in whose error stays in the halo.
+    auto absphi = [&](const float* a, int ix, int iy) -> float {
+        const int gx = x0 + ix, gy = y0 + iy;
+        if (gx < 0 || gy < 0 || gx >= W || gy >= H) return FIM_LARGE;
+        if (ix < 0 || iy < 0 || ix >= FIM_IMG || iy >= FIM_IMG) return FIM_LARGE;
+        return fabsf(a[iy * FIM_IMG + ix]);
+    };
+    auto quad = [&](const float* a, int ix, int iy) -> float {  // solve_quadratic_2d (update.wgsl:62-83)
+        const float xm = fminf(absphi(a, ix - 1, iy), absphi(a, ix + 1, iy));
+        const float ym = fminf(absphi(a, ix, iy - 1), absphi(a, ix, iy + 1));
+        const float dd = xm - ym;
+        if (dd > SQRT2_F) return ym + 1.0f;
+        if (dd < -SQRT2_F) return xm + 1.0f;
+        return 0.5f * (xm + ym + sqrtf(2.0f - dd * dd));
+    };
+    for (int it = 0; it < iters; ++it) {
+        for (int i = threadIdx.x; i < N; i += FIM_THREADS) {  // phase A
+            const int ix = i % FIM_IMG, iy = i / FIM_IMG;
+            const uint32_t lv = l[i];
+            const float p = s[i];
+            if (lv != LABEL_ACTIVE) {
+                t[i] = p;
+                lt[i] = lv;
+            } else {
+                const float q = quad(s, ix, iy) * wsign(p);
+                t[i] = q;
+                lt[i] = (fabsf(p - q) > FIM_EPS) ? LABEL_ACTIVE : LABEL_CONVERGED;
+            }
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < N; i += FIM_THREADS) {  // phase B
+            const int ix = i % FIM_IMG, iy = i / FIM_IMG;
+            const int gx = x0 + ix, gy = y0 + iy;
+            const uint32_t lv = lt[i];
+            const float tv = t[i];
+            if (lv == LABEL_NONE) {
+                const int wo[4][2] = {{0, 1}, {1, 0}, {-1, 0}, {0, -1}};
+                int wi = -1;
+                for (int k = 0; k < 4; ++k) {
+                    const int ax = ix + wo[k][0], ay = iy + wo[k][1];
+                    const int bx = gx + wo[k][0], by = gy + wo[k][1];
+                    if (bx >= 0 && by >= 0 && bx < W && by < H && ax >= 0 && ay >= 0 && ax < FIM_IMG &&
+                        ay < FIM_IMG && lt[ay * FIM_IMG + ax] == LABEL_CONVERGED) {
+                        wi = ay * FIM_IMG + ax;
+                        break;
+                    }
+                }
+                if (wi >= 0) {
+                    const float pn = fabsf(tv);
+                    const float qn = quad(t, ix, iy);
+                    if (pn > qn) {
+                        s[i] = qn * wsign(t[wi]);
+                        l[i] = LABEL_ACTIVE;
+                        continue;
+                    }
+                }
+                s[i] = tv;
+                l[i] = LABEL_NONE;
+            } else {
+                s[i] = tv;
+                l[i] = lv == LABEL_CONVERGED ? LABEL_NONE : lv;
+            }
+        }
+        __syncthreads();
+    }
+    for (int i = threadIdx.x; i < FIM_TILE * FIM_TILE; i += FIM_THREADS) {
+        const int ix = FIM_HALO + i % FIM_TILE, iy = FIM_HALO + i / FIM_TILE;
+        const int gx = x0 + ix, gy = y0 + iy;
+        if (gx < W && gy < H) {
+            S.at(gx, gy) = s[iy * FIM_IMG + ix];
+            L.at(gx, gy) = l[iy * FIM_IMG + ix];
+        }
+    }
+}
+
 // levelset_gradient.wgsl:4-21
 __global__ void k_gradient(PF ls0, P2 grad, Dom d) {
     int x = gx(), y = gy();

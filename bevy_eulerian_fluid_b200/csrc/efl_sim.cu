@@ -135,7 +135,6 @@ struct efl_sim {
     GraphCache gc;                // captured step segments
     uint64_t graph_epoch = 1;     // counts the setters that change kernel arguments
     PF mix_d2{};       // second correction buffer (batched solve)
-    PF dbuf2{};        // second halo-exchange buffer of the persistent solve, allocated on first use
     bool owns_stream = true;
     float* d_vel = nullptr;  // velocity-magnitude partials (efl_velocity_magnitude)
     int cap_vel = 0;
@@ -317,6 +316,22 @@ std::vector<int> jfa_steps(int nx, int ny) {  // jump_flooding.rs:201-209
     return st;
 }
 
+// The tiled FIM kernel's dynamic shared memory (above the 48 KB default), set once per device.
+bool fim_tiled_ready() {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    static int state[64] = {};  // 0 unknown, 1 ready, 2 refused
+    if (dev < 0 || dev >= 64) return false;
+    if (!state[dev]) {
+        state[dev] = cudaFuncSetAttribute(k_fim_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FIM_SMEM) ==
+                             cudaSuccess
+                         ? 1
+                         : 2;
+        cudaGetLastError();
+    }
+    return state[dev] == 1;
+}
+
 efl_status st_reinit(efl_sim* s) {  // reinitialize_levelset.rs:162-243
     Dom d = s->dom();
     dim3 g = grid2d(d.nx, d.ny, kBlock);
@@ -332,9 +347,17 @@ efl_status st_reinit(efl_sim* s) {  // reinitialize_levelset.rs:162-243
     } else {
         k_fim_init<<<g, kBlock, count_launch(), s->stream>>>(s->ls1, s->ls0, s->lab0, d);
         k_fim_active<<<g, kBlock, count_launch(), s->stream>>>(s->lab0, s->lab, d);
-        for (uint32_t k = 0; k < s->cfg.reinit.fim_iterations; ++k) {
-            k_fim_phase_a<<<g, kBlock, count_launch(), s->stream>>>(s->ls0, s->lab, s->phiT, s->labT, d);
-            k_fim_phase_b<<<g, kBlock, count_launch(), s->stream>>>(s->phiT, s->labT, s->ls0, s->lab, d);
+        if (fim_tiled_ready()) {  // the iterations, FIM_HALO / 2 per launch
+            const int tx = (d.nx + FIM_TILE - 1) / FIM_TILE, ty = (d.ny + FIM_TILE - 1) / FIM_TILE;
+            for (uint32_t k = 0; k < s->cfg.reinit.fim_iterations; k += FIM_HALO / 2) {
+                const int n = (int)std::min<uint32_t>(FIM_HALO / 2, s->cfg.reinit.fim_iterations - k);
+                k_fim_tiled<<<tx * ty, FIM_THREADS, FIM_SMEM + count_launch(), s->stream>>>(s->ls0, s->lab, d, n, tx);
+            }
+        } else {
+            for (uint32_t k = 0; k < s->cfg.reinit.fim_iterations; ++k) {
+                k_fim_phase_a<<<g, kBlock, count_launch(), s->stream>>>(s->ls0, s->lab, s->phiT, s->labT, d);
+                k_fim_phase_b<<<g, kBlock, count_launch(), s->stream>>>(s->phiT, s->labT, s->ls0, s->lab, d);
+            }
         }
     }
     LAUNCH_CHECK();
@@ -622,9 +645,8 @@ efl_status ensure_mix_planes(efl_sim* s) {
 efl_status gs_mixed(efl_sim* s, float weight, double tol, uint32_t max_iters, uint32_t check, SolveResult* res) {
     const Level64& L = s->mg64[0];
     std::string perr;
-    if (!s->dbuf2.p) TRY(alloc_plane(s, s->dbuf2, s->nx, s->ny, s->P, s->ny + 1));
-    efl_status ps = solve_gsmix_persistent(s->solver, L, s->r0, s->dbuf2, s->U, weight, tol, max_iters, check,
-                                           s->stream, res, &perr);
+    efl_status ps = solve_gsmix_persistent(s->solver, L, s->r0, s->U, weight, tol, max_iters, check, s->stream, res,
+                                           &perr);
     if (ps == EFL_OK) return EFL_OK;
     if (ps != EFL_ERR_STATE) return set_err(s, ps, "%s", perr.c_str());
     TRY(ensure_mix_planes(s));

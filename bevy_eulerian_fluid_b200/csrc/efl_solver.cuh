@@ -53,13 +53,13 @@ struct SolverWorkspace {
     SolveResult* result = nullptr;    // device
     SolveResult* h_result = nullptr;  // pinned host
     double2* partials = nullptr;
-    unsigned* flags = nullptr;  // max_blocks exchange flags
     int max_blocks = 0;
     long long spin_limit = 0;  // grid-barrier polls before giving up (0: kBarrierSpinLimit)
     bool use_reg = true;       // register-resident form of the persistent solve (else the shared-memory form)
 };
 
 constexpr int PS_THREADS = 1024;
+
 constexpr long long kBarrierSpinLimit = 1ll << 25;  // acquire polls (~ 1 s)
 
 // Grid-wide barrier for a cooperative launch (all CTAs co-resident), with a
@@ -115,9 +115,6 @@ struct PersistentParams {
     GridBarrier* barrier;
     SolveResult* result;
     long long spin_limit;  // grid-barrier polls before giving up
-    unsigned* flags;       // per CTA: the last halo exchange it published (neighbour-synchronised form)
-    int tiles_y;
-    PF dbuf2;              // second correction buffer: exchanges alternate between dbuf and dbuf2
 };
 
 constexpr unsigned char MODE_SKIP = 0;     // outside the domain or on the tile's outer ring
@@ -180,7 +177,6 @@ inline efl_status solver_init(SolverWorkspace& ws, int nx, int ny, int device, s
     if (cudaMalloc(&ws.barrier, sizeof(GridBarrier)) != cudaSuccess ||
         cudaMalloc(&ws.result, sizeof(SolveResult)) != cudaSuccess ||
         cudaMalloc(&ws.partials, ws.max_blocks * sizeof(double2)) != cudaSuccess ||
-        cudaMalloc(&ws.flags, ws.max_blocks * sizeof(unsigned)) != cudaSuccess ||
         cudaMallocHost(&ws.h_result, sizeof(SolveResult)) != cudaSuccess) {
         *err = "solver workspace allocation failed";
         return EFL_ERR_OUT_OF_MEMORY;
@@ -191,7 +187,6 @@ inline void solver_free(SolverWorkspace& ws) {
     if (ws.barrier) cudaFree(ws.barrier);
     if (ws.result) cudaFree(ws.result);
     if (ws.partials) cudaFree(ws.partials);
-    if (ws.flags) cudaFree(ws.flags);
     if (ws.h_result) cudaFreeHost(ws.h_result);
     ws = SolverWorkspace{};
 }
@@ -529,108 +524,145 @@ __global__ void __launch_bounds__(PS_THREADS, 1) k_gsmix_persistent(PersistentPa
 // ---------------------------------------------------------------------------
 // Register-resident form of the persistent mixed solve.
 //
-// The same iterates as k_gsmix_persistent (same f32 update in the same
-// operation order, same checks), with the work laid out for the register
-// file instead of shared memory.  Thread (cx, s) owns the R cells of column
-// cx, rows [s R, s R + R) of the extended tile for the whole solve: their
-// coefficients (w, 1/den), right-hand side rc and correction d live in
-// registers, so an update loads only the neighbours that other threads own
-// (left and right, plus the up / down neighbour at the segment's ends) from
-// the shared-memory image of d.  Every thread has the same number of
-// updates per half-sweep, so the block barrier after it waits for no
-// straggler.  The FP64 iterate, right-hand side and diagonal stay in shared
-// memory; only the residual checks read them.
-// Halo exchange between neighbouring tiles without a grid barrier: the CTA
-// publishes `epoch` in its flag (release, after all of its threads' stores),
-// then lanes 1-9 of warp 0 wait (acquire) until each of the up to eight
-// neighbouring tiles has published it.  A CTA only reads its neighbours'
-// halo, so this is all the ordering an exchange needs; the correction
-// buffers alternate between exchanges, so a neighbour that runs one exchange
-// ahead writes the other buffer.  Bounded like grid_barrier: a wait that
-// reaches spin_limit polls sets barrier->error, and every waiting CTA polls
-// the error flag.
-EFL_DEV bool neighbour_sync(const PersistentParams& P, int tile, unsigned epoch) {
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        asm volatile("st.release.gpu.u32 [%0], %1;" ::"l"(&P.flags[tile]), "r"(epoch) : "memory");
-    }
-    int fail = 0;
-    if (threadIdx.x >= 1 && threadIdx.x <= 9 && threadIdx.x != 5) {  // the 3 x 3 neighbourhood minus the centre
-        const int k = threadIdx.x - 1, dx = k % 3 - 1, dy = k / 3 - 1;
-        const int tx = tile % P.tiles_x + dx, ty = tile / P.tiles_x + dy;
-        if (tx >= 0 && tx < P.tiles_x && ty >= 0 && ty < P.tiles_y) {
-            const unsigned* f = &P.flags[ty * P.tiles_x + tx];
-            long long spins = 0;
-            for (;;) {
-                unsigned v;
-                asm volatile("ld.acquire.gpu.u32 %0, [%1];" : "=r"(v) : "l"(f) : "memory");
-                if ((int)(v - epoch) >= 0) break;
-                if ((++spins & 1023) == 0 || spins >= P.spin_limit) {
-                    int e;
-                    asm volatile("ld.acquire.gpu.s32 %0, [%1];" : "=r"(e) : "l"(&P.barrier->error) : "memory");
-                    if (e || spins >= P.spin_limit) {
-                        atomicExch(&P.barrier->error, 1);
-                        fail = 1;
-                        break;
-                    }
-                }
-            }
-        }
-    }
-    return !__syncthreads_or(fail);
-}
-
+// The same iterates as k_gsmix_persistent on every owned cell (the same f32
+// update in the same operation order, the same checks), with the sweep made
+// branch-free and short:
+//  * Thread (bx, by) owns the 2 x 2 block of cells (2bx + i, 2by + j) of the
+//    extended tile for the whole solve.  The tile origin is even, so the
+//    block's colours are fixed: cells 0 = (0, 0) and 3 = (1, 1) have the
+//    tile's base colour, cells 1 = (1, 0) and 2 = (0, 1) the other.  A
+//    half-sweep updates two of a thread's cells; of each cell's four
+//    neighbours, two are the thread's own cells (registers) and two belong to
+//    the blocks beside it (shared memory).
+//  * The correction d, right-hand side rc and 1/den live in registers; the
+//    face weights in shared memory in thread order (one 16-byte load per
+//    update, conflict-free); the shared image of d is stored per colour,
+//    compressed along x, so a warp's neighbour loads are consecutive words.
+//  * Every cell of rings >= 1 updates in every half-sweep (no shrinking
+//    ranges, no per-cell tests): a wrong value from the stale outer ring
+//    moves inwards one ring per half-sweep, so after the K iterations between
+//    two halo exchanges (2K half-sweeps, halo 2K) the owned cells are exact.
+//    Cells that are not update cells keep d = 0 (rc = 0, 1/den = 0); the
+//    outermost ring, which only the halo exchange writes, is skipped.
+// The FP64 iterate, right-hand side and diagonal stay in shared memory; only
+// the residual checks read them.
 template <int EX, int EY>
-struct RegTile {
+struct QuadTile {
+    static constexpr int W2 = EX / 2, NB = (EX / 2) * (EY / 2);
     double p[EY][EX];
     double b[EY][EX];
     double den[EY][EX];
-    float4 w[EY][EX];
-    float d[EY][EX];
+    float4 w[4][NB];     // face weights of cell q of block t at [q][t]
+    float d[2][EY][W2];  // [k][y][x / 2] with k = (x + y) & 1 in the image (k = 0: the tile's base colour)
 };
 
-template <int EX, int EY, int KMAX, int R, bool NBR>
-__global__ void __launch_bounds__(PS_THREADS, 1) k_gsmix_reg(PersistentParams P, PF dbuf) {
-    static_assert(KMAX >= 1 && 2 * KMAX <= 8, "halo of 2 KMAX <= 8");
-    static_assert(EY % R == 0 && (EY / R) * EX <= PS_THREADS, "one thread per column segment");
+// FP64 residual of the block's cells of rings >= 1 (rc = f32(cdiv r) on update
+// cells, d = 0) and the block's norms over its owned counted cells, summed in
+// a fixed order (returned by thread 0).
+template <int EX, int EY, int NT>
+EFL_DEV double2 quad_check(QuadTile<EX, EY>& T, int bx, int by, bool active, unsigned fl, float (&rc)[4],
+                           float (&dv)[4], double cdiv, double factor) {
+    constexpr int NB = QuadTile<EX, EY>::NB;
+    double ar = 0.0, ab = 0.0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int lx = 2 * bx + (q & 1), ly = 2 * by + (q >> 1);
+        float rcv = 0.0f;
+        if ((fl >> (8 + q)) & 1u) {  // counted and not on the outermost ring
+            const float4 wq = T.w[q][threadIdx.x < NB ? threadIdx.x : 0];
+            double sum = (double)wq.x * T.p[ly][lx - 1];
+            sum = sum + (double)wq.y * T.p[ly][lx + 1];
+            sum = sum + (double)wq.z * T.p[ly - 1][lx];
+            sum = sum + (double)wq.w * T.p[ly + 1][lx];
+            const double bb = T.b[ly][lx];
+            const double r = bb - factor * (T.den[ly][lx] * T.p[ly][lx] - sum);
+            if ((fl >> q) & 1u) rcv = (float)(cdiv * r);
+            if ((fl >> (16 + q)) & 1u) {
+                ar += r * r;
+                ab += bb * bb;
+            }
+        }
+        rc[q] = rcv;
+        dv[q] = 0.0f;
+    }
+    if (active) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) T.d[q == 0 || q == 3 ? 0 : 1][2 * by + (q >> 1)][bx] = 0.0f;
+    }
+    ar = warp_sum(ar);
+    ab = warp_sum(ab);
+    __shared__ double red_r[NT / 32], red_b[NT / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) {
+        red_r[wid] = ar;
+        red_b[wid] = ab;
+    }
+    __syncthreads();
+    double2 out = make_double2(0.0, 0.0);
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < NT / 32; ++k) {
+            out.x += red_r[k];
+            out.y += red_b[k];
+        }
+    }
+    __syncthreads();
+    return out;
+}
+
+// One cell update (gauss_seidel.wgsl:45-88 on the correction, in the
+// reference's operation order: left, right, up, down).
+EFL_DEV float quad_update(float rc, float4 w, float inv, float d, float dl, float dr, float du, float dd, float wgt,
+                          float omw) {
+    float nume = rc;
+    nume = nume + w.x * dl;
+    nume = nume + w.y * dr;
+    nume = nume + w.z * du;
+    nume = nume + w.w * dd;
+    return wgt * (nume * inv) + omw * d;
+}
+
+template <int EX, int EY, int KMAX, int NT>
+__global__ void __launch_bounds__(NT, 1) k_gsmix_quad(PersistentParams P, PF dbuf) {
+    static_assert(KMAX >= 1 && EX % 2 == 0 && EY % 2 == 0, "even tile image");
+    static_assert((EX / 2) * (EY / 2) <= NT && NT % 32 == 0, "one thread per 2 x 2 block");
     extern __shared__ __align__(16) unsigned char ps_raw[];
-    RegTile<EX, EY>& T = *reinterpret_cast<RegTile<EX, EY>*>(ps_raw);
-    constexpr int H = 2 * KMAX;
+    QuadTile<EX, EY>& T = *reinterpret_cast<QuadTile<EX, EY>*>(ps_raw);
+    constexpr int H = 2 * KMAX, W2 = EX / 2, NB = QuadTile<EX, EY>::NB;
     constexpr int TXo = EX - 2 * H, TYo = EY - 2 * H;
+    static_assert(H % 2 == 0, "even halo: blocks are wholly owned or wholly halo");
     const Level64& L = P.L;
     const int tile = blockIdx.x;
     const int gx0 = (tile % P.tiles_x) * TXo - H, gy0 = (tile / P.tiles_x) * TYo - H;
     const unsigned nblocks = gridDim.x;
-    const bool active = threadIdx.x < (EY / R) * EX;
-    const int cx = threadIdx.x % EX;
-    const int r0 = active ? (threadIdx.x / EX) * R : 0;
-    const int gx = gx0 + cx;
-    const bool colx = (unsigned)gx < (unsigned)L.nx;
-    const bool ownx = cx >= H && cx < H + TXo;
-    const int cring = min(cx, EX - 1 - cx);
-    const int par0 = (gx0 + gy0 + cx + r0) & 1;  // colour ((x + y) & 1, 1 = red) of row r0
-
-    auto ring_of = [&](int q) { return min(cring, min(r0 + q, EY - 1 - r0 - q)); };  // distance to the image's edge
-    float inv[R], rc[R], dv[R];
-    unsigned fl = 0;  // bit q: update cell; bit 8 + q: counted; bit 16 + q: owned and in the domain
+    const bool active = threadIdx.x < NB;
+    const int bx = active ? (int)threadIdx.x % W2 : 0, by = active ? (int)threadIdx.x / W2 : 0;
+    const int base = (gx0 + gy0) & 1;  // colour of cells 0 and 3 (1 = red, (x + y) odd)
+    const bool owned = bx >= H / 2 && bx < (H + TXo) / 2 && by >= H / 2 && by < (H + TYo) / 2;
+    const bool ring0x = bx == 0 || bx == W2 - 1, ring0y = by == 0 || by == EY / 2 - 1;
+    float inv[4], rc[4], dv[4];
+    // bit q: update cell; bit 4 + q: live (not on the outermost ring); bit 8 + q: counted and live;
+    // bit 16 + q: owned and in the domain
+    unsigned fl = 0;
 #pragma unroll
-    for (int q = 0; q < R; ++q) {
-        const int ly = r0 + q, gy = gy0 + ly;
+    for (int q = 0; q < 4; ++q) {
+        const int lx = 2 * bx + (q & 1), ly = 2 * by + (q >> 1);
+        const int gx = gx0 + lx, gy = gy0 + ly;
+        const bool edge = (ring0x && ((q & 1) == (bx == 0 ? 0 : 1))) || (ring0y && ((q >> 1) == (by == 0 ? 0 : 1)));
+        if (active && !edge) fl |= 1u << (4 + q);
         float4 wq = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         inv[q] = 0.0f;
         rc[q] = 0.0f;
         dv[q] = 0.0f;
         double den = 0.0, bb = 0.0, pv = 0.0;
-        if (active && colx && (unsigned)gy < (unsigned)L.ny) {
+        if (active && (unsigned)gx < (unsigned)L.nx && (unsigned)gy < (unsigned)L.ny) {
             const float phi = L.ls.at(gx, gy);
             bb = L.b.at(gx, gy);
             pv = __ldcg(&L.x.p[(size_t)gy * L.x.P + gx]);
-            if (ownx && ly >= H && ly < H + TYo) fl |= 1u << (16 + q);
+            if (owned) fl |= 1u << (16 + q);
             if (phi < 0.0f) {
                 const float f[4] = {L.fu.at(gx, gy), L.fu.at(gx + 1, gy), L.fv.at(gx, gy), L.fv.at(gx, gy + 1)};
                 if (!(f[0] == 0.0f && f[1] == 0.0f && f[2] == 0.0f && f[3] == 0.0f)) {
-                    fl |= 1u << (8 + q);
+                    if (!edge) fl |= 1u << (8 + q);
                     const int ox[4] = {-1, 1, 0, 0}, oy[4] = {0, 0, -1, 1};
                     float wv[4] = {0.0f, 0.0f, 0.0f, 0.0f};
 #pragma unroll
@@ -647,7 +679,7 @@ __global__ void __launch_bounds__(PS_THREADS, 1) k_gsmix_reg(PersistentParams P,
                         }
                     }
                     wq = make_float4(wv[0], wv[1], wv[2], wv[3]);
-                    if (!(fabs(den) < (double)1.0e-6f) && ring_of(q) > 0) {  // the image's outer ring never updates
+                    if (!(fabs(den) < (double)1.0e-6f) && !edge) {
                         fl |= 1u << q;
                         inv[q] = (float)(1.0 / den);
                     }
@@ -655,86 +687,58 @@ __global__ void __launch_bounds__(PS_THREADS, 1) k_gsmix_reg(PersistentParams P,
             }
         }
         if (active) {
-            T.p[ly][cx] = pv;
-            T.b[ly][cx] = bb;
-            T.den[ly][cx] = den;
-            T.w[ly][cx] = wq;
-            T.d[ly][cx] = 0.0f;
+            T.p[ly][lx] = pv;
+            T.b[ly][lx] = bb;
+            T.den[ly][lx] = den;
+            T.w[q][threadIdx.x] = wq;
         }
     }
     __syncthreads();
     const double cdiv = P.cdiv, factor = P.factor;
     const float wgt = (float)P.weight, omw = 1.0f - (float)P.weight;
-
-    // FP64 residual of the cells of rings >= 1 (rc = f32(cdiv r) on update cells, d = 0) and the block's
-    // norms over its owned counted cells, summed in a fixed order.
-    auto check = [&]() -> double2 {
-        double ar = 0.0, ab = 0.0;
-#pragma unroll
-        for (int q = 0; q < R; ++q) {
-            const int ly = r0 + q;
-            float rcv = 0.0f;
-            if (((fl >> (8 + q)) & 1u) && ring_of(q) > 0) {
-                const float4 wq = T.w[ly][cx];
-                double sum = (double)wq.x * T.p[ly][cx - 1];
-                sum = sum + (double)wq.y * T.p[ly][cx + 1];
-                sum = sum + (double)wq.z * T.p[ly - 1][cx];
-                sum = sum + (double)wq.w * T.p[ly + 1][cx];
-                const double bb = T.b[ly][cx];
-                const double r = bb - factor * (T.den[ly][cx] * T.p[ly][cx] - sum);
-                if ((fl >> q) & 1u) rcv = (float)(cdiv * r);
-                if ((fl >> (16 + q)) & 1u) {
-                    ar += r * r;
-                    ab += bb * bb;
-                }
-            }
-            rc[q] = rcv;
-            dv[q] = 0.0f;
-            if (active) T.d[ly][cx] = 0.0f;
+    const int t = active ? (int)threadIdx.x : 0;
+    const int r0 = 2 * by, r1 = 2 * by + 1;
+    // Shared-memory rows of the neighbours that belong to other blocks (clamped inside the image for the
+    // outermost blocks, whose loads are skipped).
+    const int bxl = bx > 0 ? bx - 1 : 0, bxr = bx < W2 - 1 ? bx + 1 : bx;
+    const int rup = r0 > 0 ? r0 - 1 : 0, rdn = r1 < EY - 1 ? r1 + 1 : r1;
+    auto sweep_base = [&]() {  // cells 0 and 3 (the base colour c0 = base); neighbours of the other colour
+        float(*Do)[W2] = T.d[1];
+        const float dl0 = (fl & 0x10u) ? Do[r0][bxl] : 0.0f, du0 = (fl & 0x10u) ? Do[rup][bx] : 0.0f;
+        const float dr3 = (fl & 0x80u) ? Do[r1][bxr] : 0.0f, dd3 = (fl & 0x80u) ? Do[rdn][bx] : 0.0f;
+        if (fl & 0x10u) {
+            dv[0] = quad_update(rc[0], T.w[0][t], inv[0], dv[0], dl0, dv[1], du0, dv[2], wgt, omw);
+            T.d[0][r0][bx] = dv[0];
         }
-        ar = warp_sum(ar);
-        ab = warp_sum(ab);
-        __shared__ double red_r[PS_THREADS / 32], red_b[PS_THREADS / 32];
-        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-        if (lane == 0) {
-            red_r[wid] = ar;
-            red_b[wid] = ab;
+        if (fl & 0x80u) {
+            dv[3] = quad_update(rc[3], T.w[3][t], inv[3], dv[3], dv[2], dr3, dv[1], dd3, wgt, omw);
+            T.d[0][r1][bx] = dv[3];
         }
-        __syncthreads();
-        double2 out = make_double2(0.0, 0.0);
-        if (threadIdx.x == 0) {
-            for (int k = 0; k < PS_THREADS / 32; ++k) {
-                out.x += red_r[k];
-                out.y += red_b[k];
-            }
-        }
-        __syncthreads();
-        return out;
     };
-    // Half-sweep h (0-based within a block of red-black iterations) of colour c over the cells of rings
-    // >= 1 + h (the region the remaining half-sweeps still read).
-    auto half_sweep = [&](int c, int h) {
-#pragma unroll
-        for (int q = 0; q < R; ++q) {
-            if (((par0 ^ q) & 1) == c && ((fl >> q) & 1u) && ring_of(q) >= 1 + h) {
-                const int ly = r0 + q;
-                const float4 wq = T.w[ly][cx];
-                const float dl = T.d[ly][cx - 1], dr = T.d[ly][cx + 1];
-                const float du = q > 0 ? dv[q > 0 ? q - 1 : 0] : T.d[ly - 1][cx];
-                const float dd = q < R - 1 ? dv[q < R - 1 ? q + 1 : 0] : T.d[ly + 1][cx];
-                float nume = rc[q];
-                nume = nume + wq.x * dl;
-                nume = nume + wq.y * dr;
-                nume = nume + wq.z * du;
-                nume = nume + wq.w * dd;
-                dv[q] = wgt * (nume * inv[q]) + omw * dv[q];
-                T.d[ly][cx] = dv[q];
-            }
+    auto sweep_other = [&]() {  // cells 1 and 2; neighbours of the base colour
+        float(*Do)[W2] = T.d[0];
+        const float dr1 = (fl & 0x20u) ? Do[r0][bxr] : 0.0f, du1 = (fl & 0x20u) ? Do[rup][bx] : 0.0f;
+        const float dl2 = (fl & 0x40u) ? Do[r1][bxl] : 0.0f, dd2 = (fl & 0x40u) ? Do[rdn][bx] : 0.0f;
+        if (fl & 0x20u) {
+            dv[1] = quad_update(rc[1], T.w[1][t], inv[1], dv[1], dv[0], dr1, du1, dv[3], wgt, omw);
+            T.d[1][r0][bx] = dv[1];
+        }
+        if (fl & 0x40u) {
+            dv[2] = quad_update(rc[2], T.w[2][t], inv[2], dv[2], dl2, dv[3], dv[0], dd2, wgt, omw);
+            T.d[1][r1][bx] = dv[2];
+        }
+    };
+    auto store_d = [&]() {  // all four cells into the shared image
+        if (active) {
+            T.d[0][r0][bx] = dv[0];
+            T.d[1][r0][bx] = dv[1];
+            T.d[1][r1][bx] = dv[2];
+            T.d[0][r1][bx] = dv[3];
         }
     };
 
-    unsigned iters = 0, epoch = 0;  // epoch: halo exchanges of the correction so far
-    double2 part = check();
+    unsigned iters = 0;
+    double2 part = quad_check<EX, EY, NT>(T, bx, by, active, fl, rc, dv, cdiv, factor);
     if (threadIdx.x == 0) P.partials[blockIdx.x] = part;
     bool ok = grid_barrier(P.barrier, nblocks, P.spin_limit);
     double r = ok ? ps_total_relative(P.partials, nblocks) : 0.0;
@@ -747,21 +751,24 @@ __global__ void __launch_bounds__(PS_THREADS, 1) k_gsmix_reg(PersistentParams P,
         while (ok && todo > 0) {
             const unsigned kk = min((unsigned)KMAX, todo);
             for (unsigned it = 0; it < kk; ++it) {
-                half_sweep(1, 2 * it);  // red: (x+y) odd
+                if (base) sweep_base();  // red ((x + y) odd) first
+                else sweep_other();
                 __syncthreads();
-                half_sweep(0, 2 * it + 1);  // black
+                if (base) sweep_other();
+                else sweep_base();
                 __syncthreads();
             }
             todo -= kk;
             done += kk;
-            if (todo > 0) {  // exchange the correction's halo
-                const PF& db = (NBR && (epoch & 1)) ? P.dbuf2 : dbuf;
-                ++epoch;
+            if (todo > 0) {  // exchange the correction's halo through L2
+                if (owned) {
 #pragma unroll
-                for (int q = 0; q < R; ++q)
-                    if ((fl >> (16 + q)) & 1u) __stcg(&db.p[(size_t)(gy0 + r0 + q) * db.P + gx], dv[q]);
-                // The first exchange after a check also reads the check's total: every CTA's partial must be in.
-                ok = (NBR && !pending) ? neighbour_sync(P, tile, epoch) : grid_barrier(P.barrier, nblocks, P.spin_limit);
+                    for (int q = 0; q < 4; ++q)
+                        if ((fl >> (16 + q)) & 1u)
+                            __stcg(&dbuf.p[(size_t)(gy0 + 2 * by + (q >> 1)) * dbuf.P + gx0 + 2 * bx + (q & 1)],
+                                   dv[q]);
+                }
+                ok = grid_barrier(P.barrier, nblocks, P.spin_limit);
                 if (!ok) break;
                 if (pending) {
                     pending = false;
@@ -771,19 +778,18 @@ __global__ void __launch_bounds__(PS_THREADS, 1) k_gsmix_reg(PersistentParams P,
                         break;
                     }
                 }
-                float hv[R];
+                if (active && !owned) {
+                    float hv[4];
 #pragma unroll
-                for (int q = 0; q < R; ++q) {
-                    const int ly = r0 + q, gy = gy0 + ly;
-                    const bool ring = !(ownx && ly >= H && ly < H + TYo);
-                    hv[q] = (active && ring && colx && (unsigned)gy < (unsigned)L.ny)
-                                ? __ldcg(&db.p[(size_t)gy * db.P + gx])
-                                : dv[q];
-                }
+                    for (int q = 0; q < 4; ++q) {
+                        const int gx = gx0 + 2 * bx + (q & 1), gy = gy0 + 2 * by + (q >> 1);
+                        hv[q] = ((unsigned)gx < (unsigned)L.nx && (unsigned)gy < (unsigned)L.ny)
+                                    ? __ldcg(&dbuf.p[(size_t)gy * dbuf.P + gx])
+                                    : 0.0f;
+                    }
 #pragma unroll
-                for (int q = 0; q < R; ++q) {
-                    dv[q] = hv[q];
-                    if (active) T.d[r0 + q][cx] = hv[q];
+                    for (int q = 0; q < 4; ++q) dv[q] = hv[q];
+                    store_d();
                 }
                 __syncthreads();
             }
@@ -791,36 +797,33 @@ __global__ void __launch_bounds__(PS_THREADS, 1) k_gsmix_reg(PersistentParams P,
         if (!ok || converged) break;
         iters += done;
         // p += d on the owned cells (0 where the reference zeroes p), then exchange p.
+        if (owned) {
 #pragma unroll
-        for (int q = 0; q < R; ++q) {
-            if ((fl >> (16 + q)) & 1u) {
-                const int ly = r0 + q;
-                const double pv = ((fl >> q) & 1u) ? T.p[ly][cx] + (double)dv[q] : 0.0;
-                T.p[ly][cx] = pv;
-                __stcg(&L.x.p[(size_t)(gy0 + ly) * L.x.P + gx], pv);
+            for (int q = 0; q < 4; ++q) {
+                if ((fl >> (16 + q)) & 1u) {
+                    const int lx = 2 * bx + (q & 1), ly = 2 * by + (q >> 1);
+                    const double pv = ((fl >> q) & 1u) ? T.p[ly][lx] + (double)dv[q] : 0.0;
+                    T.p[ly][lx] = pv;
+                    __stcg(&L.x.p[(size_t)(gy0 + ly) * L.x.P + gx0 + lx], pv);
+                }
             }
         }
         ok = grid_barrier(P.barrier, nblocks, P.spin_limit);
         if (!ok) break;
-        {
-            double hp[R];
+        if (active && !owned) {
+            double hp[4];
 #pragma unroll
-            for (int q = 0; q < R; ++q) {
-                const int ly = r0 + q, gy = gy0 + ly;
-                const bool ring = !(ownx && ly >= H && ly < H + TYo);
-                hp[q] = (active && ring && colx && (unsigned)gy < (unsigned)L.ny)
+            for (int q = 0; q < 4; ++q) {
+                const int gx = gx0 + 2 * bx + (q & 1), gy = gy0 + 2 * by + (q >> 1);
+                hp[q] = ((unsigned)gx < (unsigned)L.nx && (unsigned)gy < (unsigned)L.ny)
                             ? __ldcg(&L.x.p[(size_t)gy * L.x.P + gx])
                             : 0.0;
             }
 #pragma unroll
-            for (int q = 0; q < R; ++q) {
-                const int ly = r0 + q, gy = gy0 + ly;
-                const bool ring = !(ownx && ly >= H && ly < H + TYo);
-                if (active && ring && colx && (unsigned)gy < (unsigned)L.ny) T.p[ly][cx] = hp[q];
-            }
+            for (int q = 0; q < 4; ++q) T.p[2 * by + (q >> 1)][2 * bx + (q & 1)] = hp[q];
         }
         __syncthreads();
-        part = check();
+        part = quad_check<EX, EY, NT>(T, bx, by, active, fl, rc, dv, cdiv, factor);
         if (threadIdx.x == 0) P.partials[blockIdx.x] = part;
         if (min(P.check_interval, P.max_iters - iters) > (unsigned)KMAX) {
             pending = true;
@@ -1095,6 +1098,7 @@ inline efl_status solve_gs32_tiled(const Level& L, const PF& alt, float dx_scale
 
 struct PersistentPlan {
     int tx = 0, ty = 0, kmax = 0, tiles_x = 0, tiles_y = 0;
+    int threads = PS_THREADS;
     size_t smem = 0;
     const void* kernel = nullptr;
     bool ok = false;
@@ -1115,27 +1119,28 @@ inline bool try_plan_mix(const SolverWorkspace& ws, int nx, int ny, PersistentPl
     if (p->tiles_x * p->tiles_y > ws.num_sms || p->tiles_x * p->tiles_y > ws.max_blocks) return false;
     return true;
 }
-// Plans for the register-resident form (RegTile: 44 bytes of shared memory per cell).
-template <int EX, int EY, int KMAX, int R>
-inline bool try_plan_reg(const SolverWorkspace& ws, int nx, int ny, PersistentPlan* p) {
+// Plans for the register-resident form (QuadTile: 44 bytes of shared memory per cell).
+template <int EX, int EY, int KMAX, int NT>
+inline bool try_plan_quad(const SolverWorkspace& ws, int nx, int ny, PersistentPlan* p) {
     const int tx = EX - 4 * KMAX, ty = EY - 4 * KMAX;
     p->kmax = KMAX;
     p->tx = tx;
     p->ty = ty;
     p->tiles_x = (nx + tx - 1) / tx;
     p->tiles_y = (ny + ty - 1) / ty;
-    p->smem = sizeof(RegTile<EX, EY>);
-    p->kernel = (const void*)k_gsmix_reg<EX, EY, KMAX, R, false>;
-    if (p->smem + 1024 > ws.max_smem) return false;
+    p->smem = sizeof(QuadTile<EX, EY>);
+    p->kernel = (const void*)k_gsmix_quad<EX, EY, KMAX, NT>;
+    p->threads = NT;
+    if (p->smem + 2048 > ws.max_smem) return false;
     if (p->tiles_x * p->tiles_y > ws.num_sms || p->tiles_x * p->tiles_y > ws.max_blocks) return false;
     return true;
 }
 inline PersistentPlan plan_mix(const SolverWorkspace& ws, int nx, int ny) {
     PersistentPlan p;
-    if (ws.use_reg && (try_plan_reg<80, 48, 4, 4>(ws, nx, ny, &p) ||  // 64 x 32 owned
-                       try_plan_reg<48, 48, 4, 3>(ws, nx, ny, &p) ||  // 32 x 32
-                       try_plan_reg<72, 56, 2, 4>(ws, nx, ny, &p) ||  // 64 x 48
-                       try_plan_reg<40, 40, 4, 2>(ws, nx, ny, &p))) {  // 24 x 24
+    if (ws.use_reg && (try_plan_quad<80, 48, 4, 960>(ws, nx, ny, &p) ||  // 64 x 32 owned
+                       try_plan_quad<48, 48, 4, 576>(ws, nx, ny, &p) ||  // 32 x 32
+                       try_plan_quad<72, 56, 2, 1024>(ws, nx, ny, &p) ||  // 64 x 48
+                       try_plan_quad<40, 40, 4, 416>(ws, nx, ny, &p))) {  // 24 x 24
         p.ok = true;
         return p;
     }
@@ -1152,8 +1157,7 @@ inline PersistentPlan plan_mix(const SolverWorkspace& ws, int nx, int ny) {
 // Tolerance-driven solve, one cooperative launch.  dbuf: an f32 plane of the
 // level's extent for the correction's halo exchange.  EFL_ERR_STATE: the grid
 // does not fit the persistent scheme.
-inline efl_status solve_gsmix_persistent(SolverWorkspace& ws, const Level64& L, const PF& dbuf, const PF& dbuf2,
-                                         const Uniform& U,
+inline efl_status solve_gsmix_persistent(SolverWorkspace& ws, const Level64& L, const PF& dbuf, const Uniform& U,
                                          float weight, double tol, uint32_t max_iters, uint32_t check_interval,
                                          cudaStream_t stream, SolveResult* out, std::string* err) {
     PersistentPlan plan = plan_mix(ws, L.nx, L.ny);
@@ -1164,7 +1168,7 @@ inline efl_status solve_gsmix_persistent(SolverWorkspace& ws, const Level64& L, 
         return EFL_ERR_STATE;
     }
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, plan.kernel, PS_THREADS, plan.smem) != cudaSuccess ||
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, plan.kernel, plan.threads, plan.smem) != cudaSuccess ||
         per_sm < 1 || plan.tiles_x * plan.tiles_y > per_sm * ws.num_sms) {
         cudaGetLastError();
         return EFL_ERR_STATE;
@@ -1187,18 +1191,14 @@ inline efl_status solve_gsmix_persistent(SolverWorkspace& ws, const Level64& L, 
     P.barrier = ws.barrier;
     P.result = ws.result;
     P.spin_limit = ws.spin_limit > 0 ? ws.spin_limit : kBarrierSpinLimit;
-    P.flags = ws.flags;
-    P.tiles_y = plan.tiles_y;
-    P.dbuf2 = dbuf2;
-    if (cudaMemsetAsync(ws.flags, 0, (size_t)plan.tiles_x * plan.tiles_y * sizeof(unsigned), stream) != cudaSuccess ||
-        cudaMemsetAsync(ws.barrier, 0, sizeof(GridBarrier), stream) != cudaSuccess) {
+    if (cudaMemsetAsync(ws.barrier, 0, sizeof(GridBarrier), stream) != cudaSuccess) {
         *err = "barrier reset failed";
         return EFL_ERR_CUDA;
     }
     PF db = dbuf;
     void* args[] = {&P, &db};
     count_launch();
-    cudaError_t e = cudaLaunchCooperativeKernel(plan.kernel, dim3(plan.tiles_x * plan.tiles_y), dim3(PS_THREADS),
+    cudaError_t e = cudaLaunchCooperativeKernel(plan.kernel, dim3(plan.tiles_x * plan.tiles_y), dim3(plan.threads),
                                                 args, plan.smem, stream);
     if (e != cudaSuccess) {
         *err = std::string("cooperative launch of the mixed solver failed: ") + cudaGetErrorString(e);

@@ -319,7 +319,10 @@ inline bool sweep_tma_init(SweepTma& st, const Level& L, const PF& alt) {
             make_map_2d(&st.maps.div, L.b.p, nx, ny, L.b.P, BOX_C_W, BOX_C_H) &&
             make_map_2d(&st.maps.p[0], L.x.p, nx, ny, L.x.P, BOX_C_W, BOX_C_H) &&
             make_map_2d(&st.maps.p[1], alt.p, nx, ny, alt.P, BOX_C_W, BOX_C_H);
-    if (st.ok && !st.d_err) st.ok = cudaMalloc(&st.d_err, sizeof(int)) == cudaSuccess;
+    // The flag starts clear: cudaMalloc returns memory with whatever an earlier allocation left in it, and
+    // only the fixed-count solve clears the flag before its sweeps (the MGPCG preconditioner's do not).
+    if (st.ok && !st.d_err)
+        st.ok = cudaMalloc(&st.d_err, sizeof(int)) == cudaSuccess && cudaMemset(st.d_err, 0, sizeof(int)) == cudaSuccess;
     return st.ok;
 }
 inline void sweep_tma_free(SweepTma& st) {
