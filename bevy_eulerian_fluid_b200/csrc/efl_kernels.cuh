@@ -497,9 +497,7 @@ __global__ void k_residual(LevelT<T> L, float dt, float rho, float dx_scaled) {
 }
 // restriction.wgsl:10-60 (the fractions on face planes)
 template <class T>
-__global__ void k_restriction(LevelT<T> F, LevelT<T> C) {
-    int x = gx(), y = gy();
-    if (x >= C.nx || y >= C.ny) return;
+EFL_DEV void restrict_cell(const LevelT<T>& F, const LevelT<T>& C, int x, int y) {
     int fx = 2 * x, fy = 2 * y;
     T br = T(0.25) * (F.r.ld(fx, fy) + F.r.ld(fx, fy + 1) + F.r.ld(fx + 1, fy) + F.r.ld(fx + 1, fy + 1));
     float ph0 = F.ls.ld(fx, fy), ph1 = F.ls.ld(fx, fy + 1), ph2 = F.ls.ld(fx + 1, fy), ph3 = F.ls.ld(fx + 1, fy + 1);
@@ -515,17 +513,94 @@ __global__ void k_restriction(LevelT<T> F, LevelT<T> C) {
     if (y == C.ny - 1) C.fv.at(x, y + 1) = 0.5f * (F.fv.ld(fx, fy + 2) + F.fv.ld(fx + 1, fy + 2));
     C.x.at(x, y) = T(0);
 }
-// prolongation.wgsl:5-34
 template <class T>
-__global__ void k_prolongation(LevelT<T> F, LevelT<T> C) {
+__global__ void k_restriction(LevelT<T> F, LevelT<T> C) {
     int x = gx(), y = gy();
     if (x >= C.nx || y >= C.ny) return;
+    restrict_cell(F, C, x, y);
+}
+// prolongation.wgsl:5-34
+template <class T>
+EFL_DEV void prolong_cell(const LevelT<T>& F, const LevelT<T>& C, int x, int y) {
     T corr = C.x.at(x, y);
     const int ox[4] = {0, 1, 0, 1}, oy[4] = {0, 0, 1, 1};
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
         int fx = 2 * x + ox[i], fy = 2 * y + oy[i];
         if (F.ls.ld(fx, fy) < 0.0f && F.x.in(fx, fy)) F.x.at(fx, fy) = corr + F.x.at(fx, fy);
+    }
+}
+template <class T>
+__global__ void k_prolongation(LevelT<T> F, LevelT<T> C) {
+    int x = gx(), y = gy();
+    if (x >= C.nx || y >= C.ny) return;
+    prolong_cell(F, C, x, y);
+}
+
+// The coarse tail of a V-cycle (multi_grid.rs:390-475) in ONE launch of one
+// CTA: every level from `first` down (each at most VT_MAX_CELLS cells, held
+// in L2) with block barriers between the steps instead of a launch per
+// half-sweep, residual, restriction and prolongation.  Same per-cell
+// functions and the same step order as the launch-per-step form (smoother
+// weight 1, resolution scale 2^level; `symmetric`: post-smoothing black then
+// red), so the result is identical.
+constexpr int VT_THREADS = 1024, VT_MAX_LEVELS = 14;
+constexpr int VT_MAX_CELLS = 128 * 128;
+template <class T>
+struct VTailArgs {
+    LevelT<T> lv[VT_MAX_LEVELS];
+    int first, count;  // levels first .. count - 1
+    float dx, rho, dt;
+    int pre, post, coarsest, symmetric;
+};
+template <class T>
+EFL_DEV void vt_sweeps(const LevelT<T>& L, float dxs, float rho, float dt, int n, int c0) {
+    const T cd = gs_cdiv<T>(dxs, rho, dt);
+    const int hw = (L.nx + 1) / 2;
+    for (int k = 0; k < n; ++k) {
+        for (int h = 0; h < 2; ++h) {
+            const int color = h == 0 ? c0 : 1 - c0;
+            for (int i = threadIdx.x; i < hw * L.ny; i += VT_THREADS) {
+                const int y = i / hw, x = 2 * (i - y * hw) + ((y + color) & 1);
+                if (x < L.nx) L.x.at(x, y) = gs_update(L, cd, T(1), x, y);
+            }
+            __syncthreads();
+        }
+    }
+}
+template <class T>
+__global__ void __launch_bounds__(VT_THREADS, 1) k_vcycle_tail(VTailArgs<T> a) {
+    const int last = a.count - 1;
+    // down: pre-smoothing, residual, restriction
+    for (int i = a.first; i < last; ++i) {
+        const LevelT<T>& L = a.lv[i];
+        const LevelT<T>& C = a.lv[i + 1];
+        const float dxs = (float)(1u << i) * a.dx;
+        vt_sweeps(L, dxs, a.rho, a.dt, a.pre, 1);
+        const T fac = residual_factor<T>(a.dt, a.rho, dxs);
+        for (int j = threadIdx.x; j < L.nx * L.ny; j += VT_THREADS) {
+            const int y = j / L.nx, x = j - y * L.nx;
+            bool c;
+            L.r.at(x, y) = residual_at(L, fac, x, y, &c);
+        }
+        __syncthreads();
+        for (int j = threadIdx.x; j < C.nx * C.ny; j += VT_THREADS) {
+            const int y = j / C.nx;
+            restrict_cell(L, C, j - y * C.nx, y);
+        }
+        __syncthreads();
+    }
+    vt_sweeps(a.lv[last], (float)(1u << last) * a.dx, a.rho, a.dt, a.coarsest, 1);
+    // up: prolongation, post-smoothing
+    for (int i = last - 1; i >= a.first; --i) {
+        const LevelT<T>& L = a.lv[i];
+        const LevelT<T>& C = a.lv[i + 1];
+        for (int j = threadIdx.x; j < C.nx * C.ny; j += VT_THREADS) {
+            const int y = j / C.nx;
+            prolong_cell(L, C, j - y * C.nx, y);
+        }
+        __syncthreads();
+        vt_sweeps(L, (float)(1u << i) * a.dx, a.rho, a.dt, a.post, a.symmetric ? 0 : 1);
     }
 }
 
@@ -790,7 +865,28 @@ __global__ void __launch_bounds__(256) k_extrapolate_fused(ExtrapArgs a) {
         sf[ly][lx] = fv;
         sv[0][ly][lx] = v;
     }
-    __syncthreads();
+    // A tile whose image is all valid or all invalid (away from the fluid's boundary: most of a large grid)
+    // comes out of the ten sweeps unchanged, with both flag planes equal to the start flag: write the flags
+    // and skip the sweeps and the face values (only faces inside the domain count).
+    int any_valid = 0, any_invalid = 0;
+    for (int i = tid; i < EX_E * EX_E; i += 256) {
+        const int ly = i / EX_E, lx = i - ly * EX_E, x = x0 + lx, y = y0 + ly;
+        if ((unsigned)x < (unsigned)W && (unsigned)y < (unsigned)H) {
+            if (sv[0][ly][lx]) any_valid = 1;
+            else any_invalid = 1;
+        }
+    }
+    const bool mixed = __syncthreads_or(any_valid) && __syncthreads_or(any_invalid);
+    if (!mixed) {
+        for (int i = tid; i < EX_T * EX_T; i += 256) {
+            const int ly = EX_H + i / EX_T, lx = EX_H + i % EX_T, x = x0 + lx, y = y0 + ly;
+            if ((unsigned)x >= (unsigned)W || (unsigned)y >= (unsigned)H) continue;
+            const int v = sv[0][ly][lx];
+            a.vin[comp].at(x, y) = v;
+            a.vout[comp].at(x, y) = v;
+        }
+        return;
+    }
     for (int s = 0; s < 10; ++s) {
         const int in = s & 1, out = in ^ 1, lo = 1 + s, n = EX_E - 2 * lo;
         for (int i = tid; i < n * n; i += 256) {

@@ -135,6 +135,7 @@ struct efl_sim {
     GraphCache gc;                // captured step segments
     uint64_t graph_epoch = 1;     // counts the setters that change kernel arguments
     PF mix_d2{};       // second correction buffer (batched solve)
+    PF xbuf{};         // second halo-exchange plane of the persistent solves, allocated on first use
     bool owns_stream = true;
     float* d_vel = nullptr;  // velocity-magnitude partials (efl_velocity_magnitude)
     int cap_vel = 0;
@@ -347,8 +348,10 @@ efl_status st_reinit(efl_sim* s) {  // reinitialize_levelset.rs:162-243
     } else {
         k_fim_init<<<g, kBlock, count_launch(), s->stream>>>(s->ls1, s->ls0, s->lab0, d);
         k_fim_active<<<g, kBlock, count_launch(), s->stream>>>(s->lab0, s->lab, d);
-        if (fim_tiled_ready()) {  // the iterations, FIM_HALO / 2 per launch
-            const int tx = (d.nx + FIM_TILE - 1) / FIM_TILE, ty = (d.ny + FIM_TILE - 1) / FIM_TILE;
+        const int tx = (d.nx + FIM_TILE - 1) / FIM_TILE, ty = (d.ny + FIM_TILE - 1) / FIM_TILE;
+        // The tiled form pays where the grid is large and the interface a small part of it (C3: 4096^2);
+        // on small grids the per-phase launches are cheaper (the tiles hold the interface almost everywhere).
+        if (tx * ty >= 4 * s->solver.num_sms && fim_tiled_ready()) {  // the iterations, FIM_HALO / 2 per launch
             for (uint32_t k = 0; k < s->cfg.reinit.fim_iterations; k += FIM_HALO / 2) {
                 const int n = (int)std::min<uint32_t>(FIM_HALO / 2, s->cfg.reinit.fim_iterations - k);
                 k_fim_tiled<<<tx * ty, FIM_THREADS, FIM_SMEM + count_launch(), s->stream>>>(s->ls0, s->lab, d, n, tx);
@@ -594,6 +597,22 @@ template <class T>
 efl_status v_cycle(efl_sim* s, std::vector<LevelT<T>>& mg, size_t i, bool symmetric = false) {
     const efl_projection& P = s->cfg.projection;
     const LevelT<T>& L = mg[i];
+    if ((int64_t)L.nx * L.ny <= VT_MAX_CELLS && mg.size() <= VT_MAX_LEVELS) {  // the rest in one launch
+        VTailArgs<T> a{};
+        for (size_t k = 0; k < mg.size(); ++k) a.lv[k] = mg[k];
+        a.first = (int)i;
+        a.count = (int)mg.size();
+        a.dx = s->U.dx;
+        a.rho = s->U.rho;
+        a.dt = s->U.dt;
+        a.pre = (int)P.mg_pre;
+        a.post = (int)P.mg_post;
+        a.coarsest = (int)P.mg_coarsest;
+        a.symmetric = symmetric ? 1 : 0;
+        k_vcycle_tail<T><<<1, VT_THREADS, count_launch(), s->stream>>>(a);
+        LAUNCH_CHECK();
+        return EFL_OK;
+    }
     float scale = (float)(1u << i);
     if (i == mg.size() - 1) return gs_iterations(s, L, 1.0f, scale, P.mg_coarsest);
     TRY(gs_iterations(s, L, 1.0f, scale, P.mg_pre));
@@ -612,8 +631,17 @@ efl_status v_cycle(efl_sim* s, std::vector<LevelT<T>>& mg, size_t i, bool symmet
 // unavailable.
 efl_status sweeps_f32(efl_sim* s, float weight, uint32_t n) {
     std::string e;
-    efl_status st = solve_gs32_tma(s->tma, s->mg[0], s->p1, s->solver.num_sms, s->U.dx, s->U.rho, s->U.dt, weight, n,
-                                   s->stream, &e);
+    // Grids of at most one 64 x 32 tile per SM: all n iterations in one cooperative launch.
+    if (!s->xbuf.p) TRY(alloc_plane(s, s->xbuf, s->nx, s->ny, s->P, s->ny + 1));
+    efl_status st = solve_gs32_persistent(s->solver, s->mg[0], s->p1, s->xbuf, s->U.dx, s->U.rho, s->U.dt, weight, n,
+                                          s->tma.d_err, s->stream, &e);
+    if (st == EFL_OK) {
+        LAUNCH_CHECK();
+        return EFL_OK;
+    }
+    if (st != EFL_ERR_STATE) return set_err(s, st, "%s", e.c_str());
+    st = solve_gs32_tma(s->tma, s->mg[0], s->p1, s->solver.num_sms, s->U.dx, s->U.rho, s->U.dt, weight, n,
+                        s->stream, &e);
     if (st == EFL_ERR_STATE) {
         if (solve_gs32_tiled(s->mg[0], s->p1, s->U.dx, s->U.rho, s->U.dt, weight, n, s->stream) != EFL_OK)
             return set_err(s, EFL_ERR_CUDA, "tiled Gauss-Seidel launch failed: %s",
@@ -645,8 +673,9 @@ efl_status ensure_mix_planes(efl_sim* s) {
 efl_status gs_mixed(efl_sim* s, float weight, double tol, uint32_t max_iters, uint32_t check, SolveResult* res) {
     const Level64& L = s->mg64[0];
     std::string perr;
-    efl_status ps = solve_gsmix_persistent(s->solver, L, s->r0, s->U, weight, tol, max_iters, check, s->stream, res,
-                                           &perr);
+    if (!s->xbuf.p) TRY(alloc_plane(s, s->xbuf, s->nx, s->ny, s->P, s->ny + 1));
+    efl_status ps = solve_gsmix_persistent(s->solver, L, s->r0, s->xbuf, s->U, weight, tol, max_iters, check,
+                                           s->stream, res, &perr);
     if (ps == EFL_OK) return EFL_OK;
     if (ps != EFL_ERR_STATE) return set_err(s, ps, "%s", perr.c_str());
     TRY(ensure_mix_planes(s));
@@ -874,8 +903,10 @@ efl_status check_device_errors(efl_sim* s) {
     if (!s->tma.d_err) return EFL_OK;
     CU(cudaMemcpy(s->h_err, s->tma.d_err, sizeof(int), cudaMemcpyDeviceToHost));
     if (*s->h_err) {
+        const int code = *s->h_err;
         *s->h_err = 0;
         cudaMemset(s->tma.d_err, 0, sizeof(int));
+        if (code == 2) return set_err(s, EFL_ERR_CUDA, "fixed-count sweep: a grid barrier timed out");
         return set_err(s, EFL_ERR_CUDA, "TMA sweep: an mbarrier wait timed out");
     }
     return EFL_OK;
@@ -907,6 +938,14 @@ efl_status unet_before_solve(efl_sim* s) {
             k_unet_warm_coarse<<<g, kBlock, count_launch(), s->stream>>>(L.x, n.out, n.mask, n.sigma, s->nx, s->ny, f);
         else
             k_unet_warm<<<g, kBlock, count_launch(), s->stream>>>(L.x, n.out, n.mask, n.sigma, s->nx, s->ny);
+        // The guard: kept only if it lowers the block-summed residual (block = the coarsening, at least 8).
+        const int gb = std::max(8, f);
+        const dim3 gg = grid2d((s->nx + gb - 1) / gb, (s->ny + gb - 1) / gb, kBlock);
+        const int nb = (int)(gg.x * gg.y);
+        k_unet_block_residual<<<gg, kBlock, count_launch(), s->stream>>>(a, n.prev32, gb, n.epart);
+        k_unet_guard<<<1, 32, count_launch(), s->stream>>>(n.epart, nb, (double*)(n.epart + nb));
+        k_unet_guard_restore<<<g, kBlock, count_launch(), s->stream>>>(L.x, n.prev32, n.mask,
+                                                                        (double*)(n.epart + nb), s->nx, s->ny);
     }
     LAUNCH_CHECK();
     return EFL_OK;

@@ -115,6 +115,7 @@ struct PersistentParams {
     GridBarrier* barrier;
     SolveResult* result;
     long long spin_limit;  // grid-barrier polls before giving up
+    PF dbuf2;              // the exchanges alternate between the correction planes dbuf and dbuf2
 };
 
 constexpr unsigned char MODE_SKIP = 0;     // outside the domain or on the tile's outer ring
@@ -549,11 +550,12 @@ __global__ void __launch_bounds__(PS_THREADS, 1) k_gsmix_persistent(PersistentPa
 template <int EX, int EY>
 struct QuadTile {
     static constexpr int W2 = EX / 2, NB = (EX / 2) * (EY / 2);
+    static constexpr int WP = W2 % 16 == 4 ? W2 : W2 + ((4 - W2 % 16) + 16) % 16;  // row stride of d
     double p[EY][EX];
     double b[EY][EX];
     double den[EY][EX];
     float4 w[4][NB];     // face weights of cell q of block t at [q][t]
-    float d[2][EY][W2];  // [k][y][x / 2] with k = (x + y) & 1 in the image (k = 0: the tile's base colour)
+    float d[2][EY][WP];  // [k][y][x / 2] with k = (x + y) & 1 in the image (k = 0: the tile's base colour)
 };
 
 // FP64 residual of the block's cells of rings >= 1 (rc = f32(cdiv r) on update
@@ -702,8 +704,10 @@ __global__ void __launch_bounds__(NT, 1) k_gsmix_quad(PersistentParams P, PF dbu
     // outermost blocks, whose loads are skipped).
     const int bxl = bx > 0 ? bx - 1 : 0, bxr = bx < W2 - 1 ? bx + 1 : bx;
     const int rup = r0 > 0 ? r0 - 1 : 0, rdn = r1 < EY - 1 ? r1 + 1 : r1;
+    // ring of the block (its outermost cell's distance to the image edge, + 1 for its inner cells)
+    const int bring = min(min(2 * bx + 1, EX - 2 * bx), min(2 * by + 1, EY - 2 * by)) - 1;
     auto sweep_base = [&]() {  // cells 0 and 3 (the base colour c0 = base); neighbours of the other colour
-        float(*Do)[W2] = T.d[1];
+        float(*Do)[QuadTile<EX, EY>::WP] = T.d[1];
         const float dl0 = (fl & 0x10u) ? Do[r0][bxl] : 0.0f, du0 = (fl & 0x10u) ? Do[rup][bx] : 0.0f;
         const float dr3 = (fl & 0x80u) ? Do[r1][bxr] : 0.0f, dd3 = (fl & 0x80u) ? Do[rdn][bx] : 0.0f;
         if (fl & 0x10u) {
@@ -716,7 +720,7 @@ __global__ void __launch_bounds__(NT, 1) k_gsmix_quad(PersistentParams P, PF dbu
         }
     };
     auto sweep_other = [&]() {  // cells 1 and 2; neighbours of the base colour
-        float(*Do)[W2] = T.d[0];
+        float(*Do)[QuadTile<EX, EY>::WP] = T.d[0];
         const float dr1 = (fl & 0x20u) ? Do[r0][bxr] : 0.0f, du1 = (fl & 0x20u) ? Do[rup][bx] : 0.0f;
         const float dl2 = (fl & 0x40u) ? Do[r1][bxl] : 0.0f, dd2 = (fl & 0x40u) ? Do[rdn][bx] : 0.0f;
         if (fl & 0x20u) {
@@ -737,7 +741,7 @@ __global__ void __launch_bounds__(NT, 1) k_gsmix_quad(PersistentParams P, PF dbu
         }
     };
 
-    unsigned iters = 0;
+    unsigned iters = 0, xch = 0;  // xch: correction exchanges so far
     double2 part = quad_check<EX, EY, NT>(T, bx, by, active, fl, rc, dv, cdiv, factor);
     if (threadIdx.x == 0) P.partials[blockIdx.x] = part;
     bool ok = grid_barrier(P.barrier, nblocks, P.spin_limit);
@@ -751,22 +755,29 @@ __global__ void __launch_bounds__(NT, 1) k_gsmix_quad(PersistentParams P, PF dbu
         while (ok && todo > 0) {
             const unsigned kk = min((unsigned)KMAX, todo);
             for (unsigned it = 0; it < kk; ++it) {
-                if (base) sweep_base();  // red ((x + y) odd) first
-                else sweep_other();
+                if (bring + 1 >= 1 + 2 * (int)it) {  // a cell of the block lies in the region still needed
+                    if (base) sweep_base();  // red ((x + y) odd) first
+                    else sweep_other();
+                }
                 __syncthreads();
-                if (base) sweep_other();
-                else sweep_base();
+                if (bring + 1 >= 2 + 2 * (int)it) {
+                    if (base) sweep_other();
+                    else sweep_base();
+                }
                 __syncthreads();
             }
             todo -= kk;
             done += kk;
             if (todo > 0) {  // exchange the correction's halo through L2
+                // Alternate planes: a CTA that runs on to the next exchange writes the other plane, so it
+                // cannot overwrite values a slower neighbour is still reloading (two exchanges apart there
+                // is always a grid barrier).
+                const PF& db = (xch++ & 1) ? P.dbuf2 : dbuf;
                 if (owned) {
 #pragma unroll
                     for (int q = 0; q < 4; ++q)
                         if ((fl >> (16 + q)) & 1u)
-                            __stcg(&dbuf.p[(size_t)(gy0 + 2 * by + (q >> 1)) * dbuf.P + gx0 + 2 * bx + (q & 1)],
-                                   dv[q]);
+                            __stcg(&db.p[(size_t)(gy0 + 2 * by + (q >> 1)) * db.P + gx0 + 2 * bx + (q & 1)], dv[q]);
                 }
                 ok = grid_barrier(P.barrier, nblocks, P.spin_limit);
                 if (!ok) break;
@@ -784,7 +795,7 @@ __global__ void __launch_bounds__(NT, 1) k_gsmix_quad(PersistentParams P, PF dbu
                     for (int q = 0; q < 4; ++q) {
                         const int gx = gx0 + 2 * bx + (q & 1), gy = gy0 + 2 * by + (q >> 1);
                         hv[q] = ((unsigned)gx < (unsigned)L.nx && (unsigned)gy < (unsigned)L.ny)
-                                    ? __ldcg(&dbuf.p[(size_t)gy * dbuf.P + gx])
+                                    ? __ldcg(&db.p[(size_t)gy * db.P + gx])
                                     : 0.0f;
                     }
 #pragma unroll
@@ -840,6 +851,242 @@ __global__ void __launch_bounds__(NT, 1) k_gsmix_quad(PersistentParams P, PF dbu
         P.result->r0 = r0v;
         P.result->r1 = r;
     }
+}
+
+// The reference's fixed-count f32 sweeps (gauss_seidel.wgsl:12-88, `iters`
+// red-black iterations, red first) as ONE cooperative launch for grids of at
+// most one 64 x 32 tile per SM (C1's 256^2, 512^2): the 2 x 2-block layout
+// of k_gsmix_quad on the pressure itself.  Per cell, with the reference's f32
+// coefficients: update cells p = w (nume / den) + (1 - w) p, zero cells
+// (air, fully solid, |den| < 1e-6) p = 0, the outermost ring untouched.  The
+// owned cells are exchanged through L2 every 4 iterations (alternating
+// planes) and stored to `out` after a last grid barrier (no CTA may still be
+// loading its first image from `out`).
+template <int EX, int EY>
+struct Quad32Tile {
+    static constexpr int W2 = EX / 2, NB = (EX / 2) * (EY / 2);
+    static constexpr int WP = W2 % 16 == 4 ? W2 : W2 + ((4 - W2 % 16) + 16) % 16;
+    float4 w[4][NB];
+    float p[2][EY][WP];  // [k][y][x / 2], k = (x + y) & 1 in the image (k = 0: the tile's base colour)
+};
+struct Gs32Params {
+    Level L;  // x = the pressure (read at the start, written at the end), b, ls, fu, fv
+    PF xb[2];  // exchange planes
+    int tiles_x, iters;
+    float cdiv, weight;
+    GridBarrier* barrier;
+    long long spin_limit;
+    int* err;  // set to 2 if a grid barrier timed out (reported with the TMA sweep's flag)
+};
+EFL_DEV float gs32_update(float cb, float4 w, float den, float p, float pl, float pr, float pu, float pd, float wgt,
+                          float omw, unsigned upd, unsigned zero) {
+    float nume = cb;
+    nume = nume + w.x * pl;
+    nume = nume + w.y * pr;
+    nume = nume + w.z * pu;
+    nume = nume + w.w * pd;
+    const float pn = nume / den;
+    const float v = wgt * pn + omw * p;
+    return upd ? v : (zero ? 0.0f : p);
+}
+template <int EX, int EY, int KMAX, int NT>
+__global__ void __launch_bounds__(NT, 1) k_gs32_quad(Gs32Params P) {
+    static_assert((EX / 2) * (EY / 2) <= NT && NT % 32 == 0 && EX % 2 == 0 && EY % 2 == 0, "2 x 2 blocks");
+    extern __shared__ __align__(16) unsigned char q32_raw[];
+    Quad32Tile<EX, EY>& T = *reinterpret_cast<Quad32Tile<EX, EY>*>(q32_raw);
+    constexpr int H = 2 * KMAX, W2 = EX / 2, NB = Quad32Tile<EX, EY>::NB, WP = Quad32Tile<EX, EY>::WP;
+    constexpr int TXo = EX - 2 * H, TYo = EY - 2 * H;
+    const Level& L = P.L;
+    const int gx0 = (blockIdx.x % P.tiles_x) * TXo - H, gy0 = (blockIdx.x / P.tiles_x) * TYo - H;
+    const unsigned nblocks = gridDim.x;
+    const bool active = threadIdx.x < NB;
+    const int bx = active ? (int)threadIdx.x % W2 : 0, by = active ? (int)threadIdx.x / W2 : 0;
+    const int base = (gx0 + gy0) & 1;
+    const bool owned = bx >= H / 2 && bx < (H + TXo) / 2 && by >= H / 2 && by < (H + TYo) / 2;
+    const bool ring0x = bx == 0 || bx == W2 - 1, ring0y = by == 0 || by == EY / 2 - 1;
+    float pv[4], cb[4], den[4];
+    unsigned fl = 0;  // bit q: update; bit 4 + q: zero; bit 8 + q: live (in the domain, not the outer ring);
+                      // bit 16 + q: owned and in the domain
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int lx = 2 * bx + (q & 1), ly = 2 * by + (q >> 1);
+        const int gx = gx0 + lx, gy = gy0 + ly;
+        const bool edge = (ring0x && ((q & 1) == (bx == 0 ? 0 : 1))) || (ring0y && ((q >> 1) == (by == 0 ? 0 : 1)));
+        float4 wk = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        pv[q] = 0.0f;
+        cb[q] = 0.0f;
+        den[q] = 0.0f;
+        if (active && (unsigned)gx < (unsigned)L.nx && (unsigned)gy < (unsigned)L.ny) {
+            pv[q] = L.x.at(gx, gy);
+            if (owned) fl |= 1u << (16 + q);
+            const float lij = L.ls.at(gx, gy);
+            bool update = false;
+            float dn = 0.0f;
+            if (lij < 0.0f) {
+                const float f[4] = {L.fu.at(gx, gy), L.fu.at(gx + 1, gy), L.fv.at(gx, gy), L.fv.at(gx, gy + 1)};
+                if (!(f[0] == 0.0f && f[1] == 0.0f && f[2] == 0.0f && f[3] == 0.0f)) {
+                    cb[q] = P.cdiv * L.b.at(gx, gy);
+                    const int ox[4] = {-1, 1, 0, 0}, oy[4] = {0, 0, -1, 1};
+                    float wv[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        const int jx = gx + ox[k], jy = gy + oy[k];
+                        if ((unsigned)jx < (unsigned)L.nx && (unsigned)jy < (unsigned)L.ny) {
+                            const float level = L.ls.at(jx, jy);
+                            if (level < 0.0f) {
+                                dn += f[k];
+                                wv[k] = f[k];
+                            } else {
+                                dn += f[k] * (1.0f - level / lij);
+                            }
+                        }
+                    }
+                    wk = make_float4(wv[0], wv[1], wv[2], wv[3]);
+                    update = !(fabsf(dn) < 1.0e-6f);
+                }
+            }
+            den[q] = update ? dn : 1.0f;
+            if (!edge) fl |= (update ? 1u << q : 1u << (4 + q)) | (1u << (8 + q));
+        }
+        if (active) {
+            T.w[q][threadIdx.x] = wk;
+            T.p[(q == 0 || q == 3) ? 0 : 1][ly][bx] = pv[q];
+        }
+    }
+    __syncthreads();
+    const float wgt = P.weight, omw = 1.0f - P.weight;
+    const int t = active ? (int)threadIdx.x : 0;
+    const int r0 = 2 * by, r1 = 2 * by + 1;
+    const int bxl = bx > 0 ? bx - 1 : 0, bxr = bx < W2 - 1 ? bx + 1 : bx;
+    const int rup = r0 > 0 ? r0 - 1 : 0, rdn = r1 < EY - 1 ? r1 + 1 : r1;
+    const int bring = min(min(2 * bx + 1, EX - 2 * bx), min(2 * by + 1, EY - 2 * by)) - 1;
+    auto sweep_base = [&]() {  // cells 0 and 3; neighbours of the other colour
+        float(*Po)[WP] = T.p[1];
+        const float pl0 = Po[r0][bxl], pu0 = Po[rup][bx], pr3 = Po[r1][bxr], pd3 = Po[rdn][bx];
+        if (fl & 0x100u) {
+            pv[0] = gs32_update(cb[0], T.w[0][t], den[0], pv[0], pl0, pv[1], pu0, pv[2], wgt, omw, fl & 1u, fl & 0x10u);
+            T.p[0][r0][bx] = pv[0];
+        }
+        if (fl & 0x800u) {
+            pv[3] = gs32_update(cb[3], T.w[3][t], den[3], pv[3], pv[2], pr3, pv[1], pd3, wgt, omw, fl & 8u, fl & 0x80u);
+            T.p[0][r1][bx] = pv[3];
+        }
+    };
+    auto sweep_other = [&]() {  // cells 1 and 2; neighbours of the base colour
+        float(*Po)[WP] = T.p[0];
+        const float pr1 = Po[r0][bxr], pu1 = Po[rup][bx], pl2 = Po[r1][bxl], pd2 = Po[rdn][bx];
+        if (fl & 0x200u) {
+            pv[1] = gs32_update(cb[1], T.w[1][t], den[1], pv[1], pv[0], pr1, pu1, pv[3], wgt, omw, fl & 2u, fl & 0x20u);
+            T.p[1][r0][bx] = pv[1];
+        }
+        if (fl & 0x400u) {
+            pv[2] = gs32_update(cb[2], T.w[2][t], den[2], pv[2], pl2, pv[3], pv[0], pd2, wgt, omw, fl & 4u, fl & 0x40u);
+            T.p[1][r1][bx] = pv[2];
+        }
+    };
+    bool ok = true;
+    int xch = 0;
+    for (int done = 0; done < P.iters && ok;) {
+        const int kk = min(KMAX, P.iters - done);
+        for (int it = 0; it < kk; ++it) {
+            if (bring + 1 >= 1 + 2 * it) {  // a cell of the block lies in the region still needed
+                if (base) sweep_base();       // red ((x + y) odd) first
+                else sweep_other();
+            }
+            __syncthreads();
+            if (bring + 1 >= 2 + 2 * it) {
+                if (base) sweep_other();
+                else sweep_base();
+            }
+            __syncthreads();
+        }
+        done += kk;
+        if (done < P.iters) {  // exchange the halo through L2 (alternating planes)
+            const PF& xb = P.xb[xch++ & 1];
+            if (owned) {
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    if ((fl >> (16 + q)) & 1u)
+                        __stcg(&xb.p[(size_t)(gy0 + 2 * by + (q >> 1)) * xb.P + gx0 + 2 * bx + (q & 1)], pv[q]);
+            }
+            ok = grid_barrier(P.barrier, nblocks, P.spin_limit);
+            if (!ok) break;
+            if (active && !owned) {
+                float hv[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int gx = gx0 + 2 * bx + (q & 1), gy = gy0 + 2 * by + (q >> 1);
+                    hv[q] = ((unsigned)gx < (unsigned)L.nx && (unsigned)gy < (unsigned)L.ny)
+                                ? __ldcg(&xb.p[(size_t)gy * xb.P + gx])
+                                : 0.0f;
+                }
+#pragma unroll
+                for (int q = 0; q < 4; ++q) pv[q] = hv[q];
+                T.p[0][r0][bx] = pv[0];
+                T.p[1][r0][bx] = pv[1];
+                T.p[1][r1][bx] = pv[2];
+                T.p[0][r1][bx] = pv[3];
+            }
+            __syncthreads();
+        }
+    }
+    if (ok) ok = grid_barrier(P.barrier, nblocks, P.spin_limit);  // every CTA has read its first image of x
+    if (!ok && threadIdx.x == 0) atomicExch(P.err, 2);
+    if (ok && owned) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            if ((fl >> (16 + q)) & 1u) L.x.at(gx0 + 2 * bx + (q & 1), gy0 + 2 * by + (q >> 1)) = pv[q];
+    }
+}
+
+// n fixed f32 red-black iterations at level 0 as one cooperative launch, when
+// the grid fits one 64 x 32 tile per SM.  EFL_ERR_STATE: it does not (use the
+// TMA-streamed sweeps).
+inline efl_status solve_gs32_persistent(SolverWorkspace& ws, const Level& L, const PF& xa, const PF& xb,
+                                        float dx_scaled, float rho, float dt, float weight, uint32_t n,
+                                        int* dev_err, cudaStream_t stream, std::string* err) {
+    constexpr int EX = 80, EY = 48, KMAX = 4, NT = 960;
+    constexpr int TXo = EX - 4 * KMAX, TYo = EY - 4 * KMAX;
+    const int tiles_x = (L.nx + TXo - 1) / TXo, tiles_y = (L.ny + TYo - 1) / TYo;
+    if (n == 0) return EFL_OK;
+    if (tiles_x * tiles_y > ws.num_sms) return EFL_ERR_STATE;
+    const void* kern = (const void*)k_gs32_quad<EX, EY, KMAX, NT>;
+    const size_t smem = sizeof(Quad32Tile<EX, EY>);
+    static bool attr_done[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return EFL_ERR_STATE;
+    if (!attr_done[dev]) {
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+            cudaGetLastError();
+            return EFL_ERR_STATE;
+        }
+        attr_done[dev] = true;
+    }
+    Gs32Params P;
+    P.L = L;
+    P.xb[0] = xa;
+    P.xb[1] = xb;
+    P.tiles_x = tiles_x;
+    P.iters = (int)n;
+    P.cdiv = dx_scaled * dx_scaled * rho / dt;  // gauss_seidel.wgsl:58
+    P.weight = weight;
+    P.barrier = ws.barrier;
+    P.spin_limit = ws.spin_limit > 0 ? ws.spin_limit : kBarrierSpinLimit;
+    P.err = dev_err;
+    if (!dev_err) return EFL_ERR_STATE;
+    if (cudaMemsetAsync(ws.barrier, 0, sizeof(GridBarrier), stream) != cudaSuccess) {
+        *err = "barrier reset failed";
+        return EFL_ERR_CUDA;
+    }
+    void* args[] = {&P};
+    count_launch();
+    const cudaError_t e = cudaLaunchCooperativeKernel(kern, dim3(tiles_x * tiles_y), dim3(NT), args, smem, stream);
+    if (e != cudaSuccess) {
+        *err = std::string("cooperative launch of the fixed-count sweep failed: ") + cudaGetErrorString(e);
+        return EFL_ERR_CUDA;
+    }
+    return EFL_OK;
 }
 
 // Global-memory form of the same solve for grids the persistent scheme
@@ -1157,7 +1404,8 @@ inline PersistentPlan plan_mix(const SolverWorkspace& ws, int nx, int ny) {
 // Tolerance-driven solve, one cooperative launch.  dbuf: an f32 plane of the
 // level's extent for the correction's halo exchange.  EFL_ERR_STATE: the grid
 // does not fit the persistent scheme.
-inline efl_status solve_gsmix_persistent(SolverWorkspace& ws, const Level64& L, const PF& dbuf, const Uniform& U,
+inline efl_status solve_gsmix_persistent(SolverWorkspace& ws, const Level64& L, const PF& dbuf, const PF& dbuf2,
+                                         const Uniform& U,
                                          float weight, double tol, uint32_t max_iters, uint32_t check_interval,
                                          cudaStream_t stream, SolveResult* out, std::string* err) {
     PersistentPlan plan = plan_mix(ws, L.nx, L.ny);
@@ -1191,6 +1439,7 @@ inline efl_status solve_gsmix_persistent(SolverWorkspace& ws, const Level64& L, 
     P.barrier = ws.barrier;
     P.result = ws.result;
     P.spin_limit = ws.spin_limit > 0 ? ws.spin_limit : kBarrierSpinLimit;
+    P.dbuf2 = dbuf2;
     if (cudaMemsetAsync(ws.barrier, 0, sizeof(GridBarrier), stream) != cudaSuccess) {
         *err = "barrier reset failed";
         return EFL_ERR_CUDA;

@@ -866,6 +866,88 @@ __global__ void k_unet_target(Plane<double> x, const float* prev32, const float*
     const size_t p = (size_t)gy * nx + gx;
     target[p] = (float)((x.at(gx, gy) - (double)prev32[p]) / (double)*sigma);
 }
+// The warm start's guard.  The sweeps remove smooth error slowest, and a
+// residual norm hardly sees it (A damps smooth modes), so a prediction can
+// lower ||r|| and still add the error that costs the iterations.  Summed
+// over g x g blocks, the residual of smooth error adds up while the
+// fine-scale part cancels, so the guard compares the norms of the block sums
+// of r before and after the warm start and keeps the warm start only if it
+// made them smaller.  One thread per block; .x = (sum of r over the block)^2
+// for the start iterate p (= prev32) and .y for the warm-started x, per
+// 32 x 8 group of blocks.
+__global__ void __launch_bounds__(256) k_unet_block_residual(UnetFeatureArgs a, const float* prev32, int g,
+                                                             double2* part) {
+    const int cx = blockIdx.x * blockDim.x + threadIdx.x, cy = blockIdx.y * blockDim.y + threadIdx.y;
+    const int Wc = (a.nx + g - 1) / g, Hc = (a.ny + g - 1) / g;
+    double sp = 0.0, sx = 0.0;
+    if (cx < Wc && cy < Hc) {
+        for (int j = 0; j < g; ++j)
+            for (int i = 0; i < g; ++i) {
+                const int gx = cx * g + i, gy = cy * g + j;
+                if (gx >= a.nx || gy >= a.ny) continue;
+                const float phi = a.ls.at(gx, gy);
+                const float f[4] = {a.fu.at(gx, gy), a.fu.at(gx + 1, gy), a.fv.at(gx, gy), a.fv.at(gx, gy + 1)};
+                if (!(phi < 0.0f) || (f[0] == 0.0f && f[1] == 0.0f && f[2] == 0.0f && f[3] == 0.0f)) continue;
+                const int ox[4] = {-1, 1, 0, 0}, oy[4] = {0, 0, -1, 1};
+                double den = 0.0, s1 = 0.0, s2 = 0.0;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int jx = gx + ox[q], jy = gy + oy[q];
+                    if ((unsigned)jx < (unsigned)a.nx && (unsigned)jy < (unsigned)a.ny) {
+                        const float level = a.ls.at(jx, jy);
+                        if (level < 0.0f) {
+                            den += (double)f[q];
+                            s1 += (double)f[q] * (double)prev32[(size_t)jy * a.nx + jx];
+                            s2 += (double)f[q] * a.prev.at(jx, jy);
+                        } else {
+                            den += (double)f[q] * (1.0 - (double)level / (double)phi);
+                        }
+                    }
+                }
+                const double bb = a.b.at(gx, gy);
+                sp += bb - a.factor * (den * (double)prev32[(size_t)gy * a.nx + gx] - s1);
+                sx += bb - a.factor * (den * a.prev.at(gx, gy) - s2);
+            }
+    }
+    double vp = sp * sp, vx = sx * sx;
+    vp = warp_sum(vp);
+    vx = warp_sum(vx);
+    __shared__ double red_p[8], red_x[8];
+    const int t = threadIdx.y * blockDim.x + threadIdx.x;
+    if ((t & 31) == 0) {
+        red_p[t >> 5] = vp;
+        red_x[t >> 5] = vx;
+    }
+    __syncthreads();
+    if (t == 0) {
+        double a1 = 0.0, a2 = 0.0;
+        for (int w = 0; w < (int)(blockDim.x * blockDim.y) / 32; ++w) {
+            a1 += red_p[w];
+            a2 += red_x[w];
+        }
+        part[blockIdx.y * gridDim.x + blockIdx.x] = make_double2(a1, a2);
+    }
+}
+// keep (*alpha = 1) or drop (*alpha = 0) the warm start, from the block-residual partials summed in order.
+__global__ void k_unet_guard(const double2* part, int n, double* alpha) {
+    if (threadIdx.x != 0) return;
+    double before = 0.0, after = 0.0;
+    for (int i = 0; i < n; ++i) {
+        before += part[i].x;
+        after += part[i].y;
+    }
+    *alpha = after < before ? 1.0 : 0.0;
+}
+// Where the guard dropped it, the start iterate p (= prev32, exactly: it is the f32 pressure widened) back on
+// the counted cells.
+__global__ void k_unet_guard_restore(Plane<double> x, const float* prev32, const unsigned char* mask,
+                                     const double* alpha, int nx, int ny) {
+    const int gx = blockIdx.x * blockDim.x + threadIdx.x, gy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (gx >= nx || gy >= ny || *alpha != 0.0) return;
+    const size_t p = (size_t)gy * nx + gx;
+    if (mask[p]) x.at(gx, gy) = (double)prev32[p];
+}
+
 // Coarse form of the warm start.  The red-black sweeps remove the
 // basin-scale part of the error slowest (hundreds of iterations per e-fold at
 // 512^2), and that part is smooth: the network therefore runs on the grid
@@ -1049,6 +1131,7 @@ struct UNet {
     size_t wpart_elems = 0;
     float2* lpart;
     float *target, *prev32, *res32, *sigma;
+    double2* epart;  // the warm start guard's partials (one per 32 x 8 group of blocks) and its decision after them
     unsigned char* mask;
     int coarse = 1;          // the grid coarsening factor f of the warm start (1, 2, 4 or 8)
     float* targetc;          // coarse training target and mask (coarse form)
@@ -1109,6 +1192,7 @@ inline cudaError_t unet_alloc(UNet& n, int maxH, int maxW) {
     F(&n.bpart, ((P0 + 1023) / 1024) * 64);
     // per-block partials: loss blocks of 1024 pixels, residual blocks of 32 x 8 cells
     items.push_back({(void**)&n.lpart, up256((P0 / 256 + (size_t)maxW / 32 + (size_t)maxH / 8 + 8) * sizeof(float2))});
+    items.push_back({(void**)&n.epart, up256((P0 / 256 + (size_t)maxW / 32 + (size_t)maxH / 8 + 9) * sizeof(double2))});
     F(&n.target, P0);
     F(&n.prev32, P0);
     F(&n.res32, P0);
@@ -1160,6 +1244,7 @@ inline cudaError_t unet_alloc_forward(UNet& v, const UNet& net, int fh, int fw) 
     B(&v.t6, P0 * 16); B(&v.u6, P0 * 16);
     F(&v.out, P0 * 16);
     items.push_back({(void**)&v.lpart, up256((PF_ / 256 + (size_t)fw / 32 + (size_t)fh / 8 + 8) * sizeof(float2))});
+    items.push_back({(void**)&v.epart, up256((PF_ / 256 + (size_t)fw / 32 + (size_t)fh / 8 + 9) * sizeof(double2))});
     F(&v.prev32, PF_);
     F(&v.res32, PF_);
     F(&v.sigma, 64);

@@ -218,61 +218,77 @@ def load_weights(api: capi.Api, max_nx: int, max_ny: int, path: str = WEIGHTS_PA
 
 
 def pretrain(api: capi.Api, samples: int = 50000, coarse: int = 8, lr: float = 1e-3, lr_final: float = 5e-5,
-             episode: int = 120, live: int = 8, sizes=((256, 3), (512, 1)), seed0: int = 1000,
+             episode: int = 120, live: int = 8, pools: float = 0.5, seed0: int = 1000,
              device: int = 0, log=print) -> tuple[capi.UNet, TrainLog]:
-    """Offline training for the committed weights: `samples` (input, converged correction) pairs from
-    C2-style scenes (water in the lower 40 %, 24 random bodies) with the two-way coupling loop, solved
-    by MGPCG to 1e-5.  `live` scenes step round-robin; each lives `episode` steps and is then replaced
-    by a scene of a fresh seed (seeds from seed0, sizes drawn with the given weights), so the samples
-    span the splash and the settling of many configurations.  Every step records one sample and one
-    Adam step (cosine learning-rate decay from lr to lr_final) follows."""
+    """Offline training for the committed weights: `samples` (input, converged correction) pairs, MGPCG to
+    1e-5 for the targets, from two kinds of scenes with seeds from seed0 (never the benchmark's):
+      * C2-style coupled scenes (water in the lower 40 %, 24 random bodies, the two-way coupling loop) at
+        256^2 (three in four) and 512^2;
+      * C4-style pools (a fraction `pools` of the scenes): a pool with 1-4 droplets at one of the C4 sizes
+        (128^2 ... 768x512), 8 local forces every 30 steps.
+    `live` scenes step round-robin; each lives `episode` steps and is then replaced by a scene of a fresh
+    seed, so the samples span splashes and settling of many configurations.  Every step records one sample
+    and one Adam step (cosine learning-rate decay from lr to lr_final) follows."""
     from .plugin import pack_obstacles
     from .rigid import RigidWorld
-    big = max(sz for sz, _ in sizes)
+    big = max(768, max(w for w, _ in scenes.BATCH_SHAPES))
     net = capi.UNet(api, big, big, seed=0xC5, device=device)
     net.set_coarsening(coarse)
     rng = np.random.default_rng(seed0)
-    pool = [sz for sz, w in sizes for _ in range(w)]
     next_seed = [seed0]
 
     def spawn():
-        sz = int(pool[int(rng.integers(0, len(pool)))])
-        sc = scenes.coupled(sz, seed=next_seed[0], method=capi.PROJECTION_MGPCG)
+        seed = next_seed[0]
         next_seed[0] += 1
+        if rng.uniform() < pools:
+            bs = scenes.batch(1, seed=seed)
+            bs.force_every = 30
+            sc = bs.scenes[0]
+            sc.cfg.projection.method = capi.PROJECTION_MGPCG
+            rigid = None
+        else:
+            sz = 256 if rng.uniform() < 0.75 else 512
+            bs = None
+            sc = scenes.coupled(sz, seed=seed, method=capi.PROJECTION_MGPCG)
+            rigid = RigidWorld(copy.deepcopy(list(sc.bodies)), (sz, sz), gravity=9.8 * scenes.LENGTH_UNIT,
+                               grid_length=1.0 / scenes.LENGTH_UNIT)
         sc.cfg.device = device
         sim = sc.make(api)
         sim.step(sc.dt)
-        rigid = RigidWorld(copy.deepcopy(list(sc.bodies)), (sz, sz), gravity=9.8 * scenes.LENGTH_UNIT,
-                           grid_length=1.0 / scenes.LENGTH_UNIT)
         net.attach(sim, warm_start=False, record=True)
-        return [sc, sim, rigid, 0]
+        return [sc, sim, rigid, bs, 0]
 
     live_sims = [spawn() for _ in range(live)]
     tl = TrainLog()
     t0 = time.time()
     while tl.samples < samples:
         for slot in range(live):
-            sc, sim, rigid, age = live_sims[slot]
+            sc, sim, rigid, bs, age = live_sims[slot]
+            if bs is not None:
+                f = bs.forces(0, age + 1)
+                if f:
+                    sim.set_local_forces(f)
             sim.step(sc.dt)
-            rigid.apply_fluid_forces(sim.solid_forces(), sc.dt)
-            rigid.step(sc.dt)
-            sim.set_obstacles(pack_obstacles(rigid.bodies))
+            if rigid is not None:
+                rigid.apply_fluid_forces(sim.solid_forces(), sc.dt)
+                rigid.step(sc.dt)
+                sim.set_obstacles(pack_obstacles(rigid.bodies))
             frac = tl.samples / samples
             rate = lr_final + 0.5 * (lr - lr_final) * (1.0 + math.cos(math.pi * frac))
             tl.losses.append(net.train_step(rate))
             tl.samples += 1
-            live_sims[slot][3] = age + 1
+            live_sims[slot][4] = age + 1
             if age + 1 >= episode:
                 net.attach(sim, warm_start=False, record=False)
                 sim.close()
                 live_sims[slot] = spawn()
             if tl.samples % 5000 == 0 and log:
-                log(f"{tl.samples} samples, {time.time() - t0:.0f} s, mean relative loss of the last 1000 "
-                    f"{np.mean(tl.losses[-1000:]):.4f}")
+                log(f"{tl.samples} samples, {time.time() - t0:.0f} s, median relative loss of the last 1000 "
+                    f"{np.median(tl.losses[-1000:]):.4f}")
             if tl.samples >= samples:
                 break
     tl.seconds = time.time() - t0
-    for _, sim, _, _ in live_sims:
+    for _, sim, _, _, _ in live_sims:
         net.attach(sim, warm_start=False, record=False)
         sim.close()
     return net, tl
@@ -290,8 +306,10 @@ def main():
     net, tl = pretrain(api, samples=args.samples, coarse=args.coarse, lr=args.lr)
     q = max(1, len(tl.losses) // 10)
     info = {"samples": tl.samples, "seconds": round(tl.seconds, 1), "coarse": args.coarse,
-            "scenes": "C2-style coupled 256^2 (3 of 4) and 512^2 (1 of 4), seeds from 1000, MGPCG to 1e-5",
-            "relative_loss_by_tenth": [round(float(np.mean(tl.losses[i * q:(i + 1) * q])), 4) for i in range(10)]}
+            "scenes": "half C2-style coupled (256^2, 512^2), half C4-style pools (C4 sizes), seeds from 1000, "
+                      "MGPCG to 1e-5",
+            "median_relative_loss_by_tenth": [round(float(np.median(tl.losses[i * q:(i + 1) * q])), 4)
+                                              for i in range(10)]}
     save_weights(net, args.coarse, info, args.out)
     print(info)
 

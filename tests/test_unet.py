@@ -158,3 +158,33 @@ def test_learned_warm_start_gain(gpu_api):
     r_p = np.mean([x[1] for x in out["plain"]])
     assert r_l < 0.8 * r_p, (r_l, r_p)
     assert all(x[3] for x in out["learned"] + out["plain"])
+
+
+@pytest.mark.gpu
+def test_pretrained_warm_start_saves_iterations(gpu_api):
+    """What the trained network gains, in iterations: the committed network (run on the grid coarsened 8x,
+    trained offline on seeds other than the benchmark's) warm-starts the benchmark scene coupled_512.  From the
+    same states, the warm-started RBGS solves reach the same 1e-5 in at least a third fewer iterations in total
+    than solves started from the previous pressure, and every one converges."""
+    from bevy_eulerian_fluid_b200 import learned, scenes
+    net = learned.load_weights(gpu_api, 512, 512)
+    assert net is not None, "the pretrained weights file is missing"
+    out = learned.compare(gpu_api, net, scenes.coupled(512), warmup=5, steps=3)
+    it_l = sum(x[0] for x in out["learned"])
+    it_p = sum(x[0] for x in out["plain"])
+    assert all(x[3] for x in out["learned"] + out["plain"])
+    assert it_l < 0.67 * it_p, (it_l, it_p)
+    net.close()
+
+
+@pytest.mark.gpu
+def test_prediction_judged_against_fp64_solve(gpu_api):
+    """The warm start's error stated against an FP64 CPU solve of the same Poisson system (a sparse direct solve
+    of the operator of residual.wgsl:33-54): the start iterate is closer to that solution than the previous
+    pressure, and supplies most of the correction's block means (the part the sweeps remove slowest)."""
+    from bevy_eulerian_fluid_b200 import learned, scenes
+    net = learned.load_weights(gpu_api, 512, 512)
+    pe = learned.prediction_error(gpu_api, net, scenes.coupled(512), warmup=5)
+    assert pe["relative_error_start"] < pe["relative_error_previous"], pe
+    assert pe["captured_block_means"] > 0.5, pe
+    net.close()

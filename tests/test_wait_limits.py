@@ -45,9 +45,31 @@ def test_grid_barrier_runs_out(oracle_api, gpu_api):
     o.close()
 
 
-def test_mbarrier_wait_runs_out(oracle_api, gpu_api):
-    """Fixed-count f32 sweep through the TMA-streamed kernel: a one-poll mbarrier limit."""
+def test_fixed_count_sweep_barrier_runs_out(oracle_api, gpu_api):
+    """Fixed-count f32 sweeps as one cooperative launch (grids of at most one tile per SM, here 256^2): a
+    one-poll grid-barrier limit; the flag is reported at the next synchronisation."""
     sc = scenes.dam_break(256)
+    g = sc.make(gpu_api)
+    g.step(sc.dt)  # init sequence
+    g.set_wait_limits(barrier_polls=1)
+    g.step(sc.dt)
+    _expect_cuda_error(g.synchronize, "grid barrier timed out")
+    g.set_wait_limits(0, 0)
+    g.close()
+    g, o = sc.make(gpu_api), sc.make(oracle_api)
+    for _ in range(4):
+        g.step(sc.dt)
+        o.step(sc.dt)
+    g.synchronize()
+    assert not compare_fields(g, o)
+    g.close()
+    o.close()
+
+
+def test_mbarrier_wait_runs_out(oracle_api, gpu_api):
+    """Fixed-count f32 sweep through the TMA-streamed kernel (grids of more tiles than SMs, here 1024^2): a
+    one-poll mbarrier limit."""
+    sc = scenes.dam_break(1024)
     g = sc.make(gpu_api)
     g.step(sc.dt)  # init sequence
     g.set_wait_limits(mbarrier_polls=1)
