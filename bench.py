@@ -452,7 +452,7 @@ def compact_legs(legs: dict) -> dict:
         out["learned"] = {"solve_ms_per_step": {k: _r(v, 3) for k, v in l["pressure_solve_ms_per_step"].items()},
                           "c5_solve_ms_per_step": {k: _r(v, 3) for k, v in
                                                    l["c5_evaluation"]["pressure_solve_ms_per_step"].items()},
-                          "forward_ms_512": l["forward"]["ms"]}
+                          "forward_ms_as_used": l["forward_as_used"]["ms"], "forward_ms_512": l["forward"]["ms"]}
     if legs.get("particle_levelset"):
         p = legs["particle_levelset"]
         out["particle_levelset"] = {"particle_steps_per_s": _r(p["particle_steps_per_s"], 0),
@@ -906,6 +906,8 @@ def learned_leg(api, args, local):
     cmp5 = learned.compare(api, net, ev, warmup=args.warmup, steps=max(1, min(args.steps, 6)))
     ms = net.time_forward(args.size, args.size, 20)
     tf = learned.forward_flops(args.size, args.size) / (ms / 1e3) / 1e12
+    coarse = int(np.load(learned.WEIGHTS_PATH)["coarse"]) if pretrained else 1
+    ms_c = net.time_forward(args.size // coarse, args.size // coarse, 20)
     peak, kind = tensor_peak()
     if pretrained:
         training = {"weights": "pretrained offline (python -m bevy_eulerian_fluid_b200.learned), loaded from "
@@ -936,6 +938,8 @@ def learned_leg(api, args, local):
                "pressure_solve_ms_per_step": {
                    "learned": sum(x[2] for x in cmp5["learned"]) / len(cmp5["learned"]),
                    "plain": sum(x[2] for x in cmp5["plain"]) / len(cmp5["plain"])}},
+           "forward_as_used": {"ms": round(ms_c, 4), "grid": f"{args.size // coarse}^2",
+                               "note": f"the warm start runs the network on the grid coarsened {coarse}x"},
            "forward": {"ms": round(ms, 4), "grid": f"{args.size}^2", "tflops": round(tf, 2), "peak": peak,
                        "peak_kind": kind, "frac": round(tf / peak, 4),
                        "kernel": "k_conv3x3_rows (widths a multiple of 128) and k_conv3x3_tc (tcgen05.mma kind::f16, "
