@@ -70,6 +70,7 @@ def parse():
     ap.add_argument("--no-c3", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
     ap.add_argument("--c3-size", type=int, default=4096, help="grid of the C3 scale scene (4096 in the benchmark)")
+    ap.add_argument("--c3-steps", type=int, default=200, help="timed steps of each C3 arm (200: the scene's length)")
     ap.add_argument("--batch-sims", type=int, default=96, help="simulations of the C4 batch (96 in the benchmark)")
     ap.add_argument("--no-pls", action="store_true")
     ap.add_argument("--no-c1", action="store_true")
@@ -130,16 +131,41 @@ class ClockSampler:
         self.samples = []
         self._stop = threading.Event()
         self._t = None
+        self._nvml = None
+        try:  # NVML read-only queries every 10 ms; nvidia-smi every 200 ms when NVML is not usable
+            import pynvml
+            import torch
+            pynvml.nvmlInit()
+            try:
+                uuid = str(torch.cuda.get_device_properties(device).uuid)
+                h = pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+            except Exception:
+                h = pynvml.nvmlDeviceGetHandleByIndex(device)
+            self._nvml = (pynvml, h, pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+        except Exception:
+            self._nvml = None
+
+    def _sample_nvml(self):
+        nv, h, mx = self._nvml
+        r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+        bits = [nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
+                nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap]
+        return [str(self.device), str(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)), str(mx),
+                str(nv.nvmlDeviceGetPowerUsage(h) / 1000.0), hex(r)] + ["Active" if r & b else "Not Active" for b in bits]
 
     def _run(self):
         while not self._stop.is_set():
             try:
+                if self._nvml is not None:
+                    self.samples.append(self._sample_nvml())
+                    self._stop.wait(0.01)
+                    continue
                 out = subprocess.run(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
                                       "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
                 if out.returncode == 0 and out.stdout.strip():
                     self.samples.append([c.strip() for c in out.stdout.strip().split(",")])
             except Exception:
-                pass
+                self._nvml = None
             self._stop.wait(0.2)
 
     def __enter__(self):
@@ -160,7 +186,8 @@ class ClockSampler:
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[i] for s in self.samples for i in range(4) if len(s) > 5 + i and s[5 + i] == "Active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.samples)}
+                "reasons": reasons, "samples": len(self.samples),
+                "source": "NVML every 10 ms" if self._nvml is not None else "nvidia-smi every 200 ms"}
 
 
 def coupled_cpu_run(size: int, warmup: int, steps: int, budget_s: float):
@@ -444,6 +471,8 @@ def compact_legs(legs: dict) -> dict:
         c = legs["c3"]
         out["c3_scale_4096"] = {"mgpcg": _r(c["mgpcg"]["value"], 0), "vcycles": _r(c["vcycles"]["value"], 0),
                                 "v_cycle_hbm_frac": c["vcycles"]["v_cycle_rate"]["frac"],
+                                "steps": c["mgpcg"]["steps"],
+                                "other_stages_ms_per_step": _r(c["mgpcg"]["other_stages_ms_per_step"], 3),
                                 "cpu_value": _r((c.get("cpu_baseline") or {}).get("value"), 0)}
     if legs.get("coupled_mgpcg"):
         out["coupled_mgpcg"] = {"value": _r(legs["coupled_mgpcg"]["value"], 0)}
@@ -961,8 +990,8 @@ def c3_leg(api, torch, args, local, peak):
                        "MG 2/2 sweeps, coarsest 16^2, to 1e-5 relative residual",
            "cells": n * n, "unit": "cell-steps/s",
            "l2": "not flushed: the working set (GBs) exceeds L2"}
-    for name, method, steps in (("mgpcg", capi.PROJECTION_MGPCG, max(1, min(args.steps, 10))),
-                                ("vcycles", capi.PROJECTION_MULTIGRID, 2)):
+    for name, method, steps in (("mgpcg", capi.PROJECTION_MGPCG, max(1, args.c3_steps)),
+                                ("vcycles", capi.PROJECTION_MULTIGRID, max(1, args.c3_steps))):
         sc = scenes.scale(n)
         sc.cfg.projection.method = method
         sc.cfg.device = local
@@ -986,7 +1015,9 @@ def c3_leg(api, torch, args, local, peak):
         vcycles = sum(iters) + (steps if method == capi.PROJECTION_MGPCG else 0)  # MGPCG: one more per solve
         vc_gbs = 272 * n * n * vcycles / (sum(solve) / 1e3) / 1e9
         out[name] = {"value": n * n * steps / (ms / 1e3), "steps": steps, "ms_per_step": ms / steps,
-                     "pressure_solve_ms_per_step": sum(solve) / steps, "iterations": iters,
+                     "pressure_solve_ms_per_step": sum(solve) / steps,
+                     "other_stages_ms_per_step": (ms - sum(solve)) / steps,
+                     "iterations": {"sum": sum(iters), "max": max(iters), "first": iters[:10]},
                      "v_cycle_rate": {"achieved": round(vc_gbs, 1), "unit": "GB/s", "frac": round(vc_gbs / peak, 4),
                                       "note": "272 algorithmic B per fine cell per V-cycle x V-cycles / solve time"}}
     out["value"] = out["mgpcg"]["value"]

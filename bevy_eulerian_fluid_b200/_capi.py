@@ -98,6 +98,15 @@ PLS_POSITIVE, PLS_NEGATIVE = 0, 1
 PLS_INITIALIZE, PLS_ADVECT, PLS_CORRECT, PLS_CORRECT_SECOND, PLS_RESEED = 0, 1, 2, 3, 4
 
 
+class SlabDesc(C.Structure):
+    _fields_ = [("device", C.c_int32), ("nx", C.c_uint32), ("ny", C.c_uint32), ("row0", C.c_uint32),
+                ("rows", C.c_uint32), ("dx", C.c_float), ("dt", C.c_float), ("rho", C.c_float),
+                ("sor_weight", C.c_float)]
+
+
+SLAB_X, SLAB_D, SLAB_LEVELSET = 0, 1, 2
+
+
 class StepStats(C.Structure):
     _fields_ = [("initialized_only", C.c_int32), ("pressure_iterations", C.c_uint32), ("converged", C.c_int32),
                 ("_pad", C.c_int32), ("residual", C.c_double), ("residual_initial", C.c_double)]
@@ -182,6 +191,15 @@ SIGNATURES = {
     "unet_time_forward": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(C.c_float)]),
     "unet_set_coarsening": (C.c_int, [C.c_void_p, C.c_uint32]),
     "batch_attach_unet": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32]),
+    "slab_create": (C.c_int, [C.POINTER(SlabDesc), C.POINTER(C.c_void_p)]),
+    "slab_destroy": (C.c_int, [C.c_void_p]),
+    "slab_load": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "slab_halo": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p]),
+    "slab_prepare": (C.c_int, [C.c_void_p]),
+    "slab_residual": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "slab_sweep": (C.c_int, [C.c_void_p, C.c_int32]),
+    "slab_apply": (C.c_int, [C.c_void_p]),
+    "slab_read": (C.c_int, [C.c_void_p, C.c_void_p]),
 }
 # Functions of efl.h that the oracle restatement does not mirror.
 PRODUCT_ONLY = {"abi_version", "default_config", "field_device_ptr", "stream", "synchronize", "kernel_launches",
@@ -190,7 +208,8 @@ PRODUCT_ONLY = {"abi_version", "default_config", "field_device_ptr", "stream", "
                 "projection_ms", "set_graph_capture", "set_wait_limits", "set_rigid_bodies", "get_rigid_bodies",
                 "unet_create", "unet_destroy", "unet_last_error", "unet_num_params", "unet_get_params",
                 "unet_set_params", "unet_forward", "unet_gradients", "unet_attach", "unet_train_step",
-                "unet_time_forward", "unet_set_coarsening", "batch_attach_unet"}
+                "unet_time_forward", "unet_set_coarsening", "batch_attach_unet", "slab_create", "slab_destroy",
+                "slab_load", "slab_halo", "slab_prepare", "slab_residual", "slab_sweep", "slab_apply", "slab_read"}
 
 
 class EflError(RuntimeError):

@@ -26,6 +26,7 @@
 #include "efl_mgpcg.cuh"
 #include "efl_unet.cuh"
 #include "efl_pls.cuh"
+#include "efl_slab.cuh"
 
 using namespace efl;
 
@@ -2791,6 +2792,194 @@ efl_status efl_unet_train_step(efl_unet* u, float lr, float* loss) {
                                                              lr, b1, b2, 1e-8f, c1, c2, gscale);
     unet_sync_weights(n, 0);
     return unet_finish(u, 0);
+}
+
+}  // extern "C"
+
+// ---- Row slabs of one domain ----------------------------------------------
+
+struct efl_slab {
+    efl_slab_desc desc{};
+    SlabPlanes S{};
+    cudaStream_t stream = nullptr;
+    void* block = nullptr;  // every plane, one allocation
+    double* h_part = nullptr;
+};
+
+namespace {
+
+efl_status slab_free(efl_slab* sl) {
+    if (!sl) return EFL_OK;
+    cudaSetDevice(sl->desc.device);
+    if (sl->stream) cudaStreamSynchronize(sl->stream);
+    if (sl->block) cudaFree(sl->block);
+    if (sl->h_part) cudaFreeHost(sl->h_part);
+    if (sl->stream) cudaStreamDestroy(sl->stream);
+    delete sl;
+    return EFL_OK;
+}
+
+efl_status slab_finish(efl_slab* sl) {
+    efl_sim* s = nullptr;
+    LAUNCH_CHECK();
+    CU(cudaStreamSynchronize(sl->stream));
+    return EFL_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+efl_status efl_slab_create(const efl_slab_desc* d, efl_slab** out) {
+    efl_sim* s = nullptr;  // errors go to efl_last_error(NULL)
+    if (!d || !out) return set_err(s, EFL_ERR_INVALID_ARGUMENT, "efl_slab_create: null argument");
+    *out = nullptr;
+    if (d->nx == 0 || d->ny == 0 || d->rows == 0 || (uint64_t)d->row0 + d->rows > d->ny)
+        return set_err(s, EFL_ERR_INVALID_ARGUMENT, "efl_slab_create: rows [%u, %u) outside a grid of %u rows",
+                       d->row0, d->row0 + d->rows, d->ny);
+    if ((uint64_t)d->nx * (d->rows + 2) > (1ull << 31))
+        return set_err(s, EFL_ERR_INVALID_ARGUMENT, "efl_slab_create: slab of %u x %u cells too large", d->nx,
+                       d->rows);
+    if (!(d->dx > 0.0f) || !(d->dt > 0.0f) || !(d->rho > 0.0f) || !(d->sor_weight > 0.0f && d->sor_weight < 2.0f))
+        return set_err(s, EFL_ERR_INVALID_ARGUMENT, "efl_slab_create: dx, dt, rho must be > 0 and sor_weight in (0, 2)");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return set_err(s, EFL_ERR_NO_DEVICE, "efl_slab_create: no CUDA device");
+    if (d->device < 0 || d->device >= ndev)
+        return set_err(s, EFL_ERR_INVALID_ARGUMENT, "efl_slab_create: device %d of %d", d->device, ndev);
+    CU(cudaSetDevice(d->device));
+    efl_slab* sl = new efl_slab();
+    sl->desc = *d;
+    SlabPlanes& S = sl->S;
+    S.nx = (int)d->nx;
+    S.ny = (int)d->ny;
+    S.row0 = (int)d->row0;
+    S.rows = (int)d->rows;
+    const size_t hal = (size_t)S.nx * (S.rows + 2), own = (size_t)S.nx * S.rows;
+    auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    const size_t sizes[] = {al(hal * 8), al(hal * 4), al(hal * 4), al(own * 16), al(own * 8), al(own * 4),
+                            al(own * 16), al(own * 4), al(own * 8), al(own), al((size_t)S.rows * 16)};
+    size_t total = 0;
+    for (size_t z : sizes) total += z;
+    cudaError_t e = cudaMalloc(&sl->block, total);
+    if (e == cudaSuccess) e = cudaMemset(sl->block, 0, total);  // halo rows beyond the domain stay zero
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&sl->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMallocHost(&sl->h_part, (size_t)S.rows * 16);
+    if (e != cudaSuccess) {
+        slab_free(sl);
+        return set_err(s, e == cudaErrorMemoryAllocation ? EFL_ERR_OUT_OF_MEMORY : EFL_ERR_CUDA,
+                       "efl_slab_create: %s", cudaGetErrorString(e));
+    }
+    char* p = (char*)sl->block;
+    auto take = [&](int i) {
+        char* q = p;
+        p += sizes[i];
+        return q;
+    };
+    S.x = (double*)take(0);
+    S.d = (float*)take(1);
+    S.ls = (float*)take(2);
+    S.af = (float4*)take(3);
+    S.b = (double*)take(4);
+    S.rc = (float*)take(5);
+    S.w = (float4*)take(6);
+    S.inv = (float*)take(7);
+    S.den = (double*)take(8);
+    S.mode = (unsigned char*)take(9);
+    S.rowpart = (double2*)take(10);
+    *out = sl;
+    return EFL_OK;
+}
+
+efl_status efl_slab_destroy(efl_slab* sl) { return slab_free(sl); }
+
+efl_status efl_slab_load(efl_slab* sl, const float* ls, const float* af, const float* div, const float* p) {
+    efl_sim* s = nullptr;
+    if (!sl || !ls || !af || !div || !p) return set_err(s, EFL_ERR_INVALID_ARGUMENT, "efl_slab_load: null argument");
+    CU(cudaSetDevice(sl->desc.device));
+    SlabPlanes& S = sl->S;
+    const size_t own = (size_t)S.nx * S.rows;
+    // The f32 pressure and divergence rows go through the (not yet built) coefficient planes as staging.
+    CU(cudaMemcpyAsync(S.ls + S.nx, ls, own * 4, cudaMemcpyDefault, sl->stream));
+    CU(cudaMemcpyAsync(S.af, af, own * 16, cudaMemcpyDefault, sl->stream));
+    CU(cudaMemcpyAsync(S.rc, p, own * 4, cudaMemcpyDefault, sl->stream));
+    CU(cudaMemcpyAsync(S.inv, div, own * 4, cudaMemcpyDefault, sl->stream));
+    k_slab_widen<<<grid2d(S.nx, S.rows, kBlock), kBlock, count_launch(), sl->stream>>>(S, S.rc, S.inv);
+    return slab_finish(sl);
+}
+
+efl_status efl_slab_halo(efl_slab* sl, int32_t field, int32_t side, int32_t write, void* buf) {
+    efl_sim* s = nullptr;
+    if (!sl || !buf) return set_err(s, EFL_ERR_INVALID_ARGUMENT, "efl_slab_halo: null argument");
+    if (field < EFL_SLAB_X || field > EFL_SLAB_LEVELSET || (side != 0 && side != 1) || (write != 0 && write != 1))
+        return set_err(s, EFL_ERR_INVALID_ARGUMENT, "efl_slab_halo: field %d, side %d, write %d", field, side, write);
+    SlabPlanes& S = sl->S;
+    if (write && ((side == 0 && S.row0 == 0) || (side == 1 && S.row0 + S.rows == S.ny)))
+        return set_err(s, EFL_ERR_INVALID_ARGUMENT, "efl_slab_halo: no halo row beyond the domain's %s edge",
+                       side == 0 ? "top" : "bottom");
+    CU(cudaSetDevice(sl->desc.device));
+    const size_t es = field == EFL_SLAB_X ? 8 : 4;
+    char* base = field == EFL_SLAB_X ? (char*)S.x : field == EFL_SLAB_D ? (char*)S.d : (char*)S.ls;
+    // halo plane rows: 0 = halo above, 1 .. rows = own, rows + 1 = halo below
+    const int row = write ? (side == 0 ? 0 : S.rows + 1) : (side == 0 ? 1 : S.rows);
+    char* dev = base + (size_t)row * S.nx * es;
+    if (write) CU(cudaMemcpyAsync(dev, buf, (size_t)S.nx * es, cudaMemcpyDefault, sl->stream));
+    else CU(cudaMemcpyAsync(buf, dev, (size_t)S.nx * es, cudaMemcpyDefault, sl->stream));
+    CU(cudaStreamSynchronize(sl->stream));
+    return EFL_OK;
+}
+
+efl_status efl_slab_prepare(efl_slab* sl) {
+    efl_sim* s = nullptr;
+    if (!sl) return set_err(s, EFL_ERR_INVALID_ARGUMENT, "efl_slab_prepare: null slab");
+    CU(cudaSetDevice(sl->desc.device));
+    k_slab_coeffs<<<grid2d(sl->S.nx, sl->S.rows, kBlock), kBlock, count_launch(), sl->stream>>>(sl->S);
+    return slab_finish(sl);
+}
+
+efl_status efl_slab_residual(efl_slab* sl, double* row_partials) {
+    efl_sim* s = nullptr;
+    if (!sl || !row_partials) return set_err(s, EFL_ERR_INVALID_ARGUMENT, "efl_slab_residual: null argument");
+    CU(cudaSetDevice(sl->desc.device));
+    const efl_slab_desc& d = sl->desc;
+    const double dx = (double)d.dx;
+    const double cdiv = dx * dx * (double)d.rho / (double)d.dt;
+    const double factor = (double)d.dt / (double)d.rho / dx / dx;
+    k_slab_residual<<<sl->S.rows, kSlabRowThreads, count_launch(), sl->stream>>>(sl->S, factor, cdiv);
+    LAUNCH_CHECK();
+    CU(cudaMemcpyAsync(sl->h_part, sl->S.rowpart, (size_t)sl->S.rows * 16, cudaMemcpyDeviceToHost, sl->stream));
+    CU(cudaStreamSynchronize(sl->stream));
+    std::memcpy(row_partials, sl->h_part, (size_t)sl->S.rows * 16);
+    return EFL_OK;
+}
+
+efl_status efl_slab_sweep(efl_slab* sl, int32_t color) {
+    efl_sim* s = nullptr;
+    if (!sl || (color != 0 && color != 1))
+        return set_err(s, EFL_ERR_INVALID_ARGUMENT, "efl_slab_sweep: null slab or color %d", color);
+    CU(cudaSetDevice(sl->desc.device));
+    const SlabPlanes& S = sl->S;
+    k_slab_sweep<<<grid2d((S.nx + 1) / 2, S.rows, kBlock), kBlock, count_launch(), sl->stream>>>(
+        S, color, sl->desc.sor_weight);
+    return slab_finish(sl);
+}
+
+efl_status efl_slab_apply(efl_slab* sl) {
+    efl_sim* s = nullptr;
+    if (!sl) return set_err(s, EFL_ERR_INVALID_ARGUMENT, "efl_slab_apply: null slab");
+    CU(cudaSetDevice(sl->desc.device));
+    k_slab_apply<<<grid2d(sl->S.nx, sl->S.rows, kBlock), kBlock, count_launch(), sl->stream>>>(sl->S);
+    return slab_finish(sl);
+}
+
+efl_status efl_slab_read(efl_slab* sl, double* x) {
+    efl_sim* s = nullptr;
+    if (!sl || !x) return set_err(s, EFL_ERR_INVALID_ARGUMENT, "efl_slab_read: null argument");
+    CU(cudaSetDevice(sl->desc.device));
+    const SlabPlanes& S = sl->S;
+    CU(cudaMemcpyAsync(x, S.x + S.nx, (size_t)S.nx * S.rows * 8, cudaMemcpyDefault, sl->stream));
+    CU(cudaStreamSynchronize(sl->stream));
+    return EFL_OK;
 }
 
 }  // extern "C"

@@ -218,7 +218,7 @@ def load_weights(api: capi.Api, max_nx: int, max_ny: int, path: str = WEIGHTS_PA
 
 
 def pretrain(api: capi.Api, samples: int = 50000, coarse: int = 8, lr: float = 1e-3, lr_final: float = 5e-5,
-             episode: int = 120, live: int = 8, pools: float = 0.5, seed0: int = 1000,
+             episode: int = 120, live: int = 8, pools: float = 0.0, seed0: int = 1000,
              target_tolerance: float = 1e-5, device: int = 0, log=print) -> tuple[capi.UNet, TrainLog]:
     """Offline training for the committed weights: `samples` (input, converged correction) pairs, MGPCG to
     1e-5 for the targets, from two kinds of scenes with seeds from seed0 (never the benchmark's):
@@ -304,7 +304,7 @@ def main():
     ap.add_argument("--samples", type=int, default=50000)
     ap.add_argument("--coarse", type=int, default=8)
     ap.add_argument("--lr", type=float, default=1e-3)
-    ap.add_argument("--pools", type=float, default=0.5, help="share of C4-style pool scenes")
+    ap.add_argument("--pools", type=float, default=0.0, help="share of C4-style pool scenes")
     ap.add_argument("--target-tolerance", type=float, default=1e-5)
     ap.add_argument("--out", default=WEIGHTS_PATH)
     args = ap.parse_args()

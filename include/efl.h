@@ -543,6 +543,73 @@ EFL_API uint64_t efl_kernel_launches(void);
  * iterate of the tolerance-driven solve, in place. */
 EFL_API efl_status efl_pressure_sweeps(efl_sim* sim, int32_t precision, uint32_t iterations);
 
+/* ---- Row slabs of one domain across devices ---------------------------- */
+
+/* One row slab of the tolerance-driven red-black Gauss-Seidel pressure solve
+ * (the FP64-iterate form of EFL_PROJECTION_GAUSS_SEIDEL with tolerance > 0:
+ * residual of residual.wgsl:33-54, update of gauss_seidel.wgsl:44-88 on an
+ * f32 correction), for a domain split into horizontal slabs with one process
+ * (and one device) per slab.  No counterpart in the reference, which runs
+ * one domain on one device (render_node.rs:193-476).
+ * The slab owns rows [row0, row0 + rows) of the nx x ny grid and holds one
+ * halo row above and one below for the iterate x (f64), the correction d
+ * (f32) and the level set (f32); the caller fills the halos from the
+ * neighbouring slabs (efl_slab_halo) at the points the solve needs them:
+ *   load own rows -> level-set halos -> efl_slab_prepare ->
+ *   x halos -> efl_slab_residual -> [ per half-sweep (color 1, then 0):
+ *   d halos -> efl_slab_sweep ] x check_interval -> efl_slab_apply ->
+ *   x halos -> efl_slab_residual -> ...
+ * and sums the per-row partials of all slabs in row order for the relative
+ * residual sqrt(sum r^2) / sqrt(sum b^2) (bevy_eulerian_fluid_b200/slab.py
+ * is that driver).  With the halos exchanged as above, the slabs together
+ * compute the unsplit solve's iterates bit for bit.
+ * Every call is synchronous on the slab's own stream.  Errors are reported
+ * through efl_last_error(NULL). */
+typedef struct efl_slab efl_slab;
+
+typedef struct efl_slab_desc {
+    int32_t device;
+    uint32_t nx, ny;     /* the whole domain */
+    uint32_t row0, rows; /* this slab: 1 <= rows, row0 + rows <= ny */
+    float dx;            /* 1 / length_unit, as in the step */
+    float dt, rho;
+    float sor_weight;
+} efl_slab_desc;
+
+enum efl_slab_field {
+    EFL_SLAB_X = 0,        /* FP64 iterate (double)          */
+    EFL_SLAB_D = 1,        /* f32 correction (float)         */
+    EFL_SLAB_LEVELSET = 2  /* levelset_air (float)           */
+};
+
+EFL_API efl_status efl_slab_create(const efl_slab_desc* desc, efl_slab** out);
+EFL_API efl_status efl_slab_destroy(efl_slab* slab);
+/* Own rows (rows x nx, row-major; area_fraction rows x nx x 4 in the order
+ * of EFL_FIELD_AREA_FRACTION): levelset_air, face fractions, divergence and
+ * the previous pressure (the start iterate, widened to f64).  Host or device
+ * pointers (copied with cudaMemcpyDefault). */
+EFL_API efl_status efl_slab_load(efl_slab* slab, const float* levelset_air, const float* area_fraction,
+                                 const float* divergence, const float* pressure);
+/* side 0: the top edge (own row 0, halo row above), 1: the bottom edge (own
+ * row rows-1, halo row below).  write 0 copies the own edge row of `field`
+ * into buf (nx elements), write 1 copies buf into the halo row on that side.
+ * buf: host or device memory.  A halo row beyond the domain's edge is never
+ * read; writing it returns EFL_ERR_INVALID_ARGUMENT. */
+EFL_API efl_status efl_slab_halo(efl_slab* slab, int32_t field, int32_t side, int32_t write, void* buf);
+/* Builds the stencil coefficients of the own rows (needs the level-set halos). */
+EFL_API efl_status efl_slab_prepare(efl_slab* slab);
+/* FP64 residual of the current iterate (needs the x halos), the next
+ * correction's right-hand side, d = 0; row_partials (host, 2 x rows
+ * doubles): per own row the sum of r^2 and of b^2 over the counted cells. */
+EFL_API efl_status efl_slab_residual(efl_slab* slab, double* row_partials);
+/* One half-sweep of the correction on the cells with (x + y) % 2 == color
+ * (global coordinates; the solve runs color 1 first); needs the d halos. */
+EFL_API efl_status efl_slab_sweep(efl_slab* slab, int32_t color);
+/* x += d on updated cells, x = 0 on air, fully solid and singular cells. */
+EFL_API efl_status efl_slab_apply(efl_slab* slab);
+/* The own rows of the iterate (rows x nx doubles, host or device memory). */
+EFL_API efl_status efl_slab_read(efl_slab* slab, double* x);
+
 /* ---- Allocation-free entry point -------------------------------------- */
 
 /* Relative residual ||b - A p||_2 / ||b||_2 (operator of residual.wgsl:33-54,
