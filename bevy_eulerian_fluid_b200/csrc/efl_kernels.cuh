@@ -835,7 +835,36 @@ struct ExtrapArgs {
     PF f[2];
     PI vin[2], vout[2];
     PF ls;
+    const float2* range;  // per 32 x 32 cell tile of ls: (min, max)
+    int rtx, rty;         // cell tiles per row / column
 };
+// (min, max) of the level set over each 32 x 32 tile of cells (one CTA per tile).
+__global__ void __launch_bounds__(256) k_ls_tile_range(PF ls, float2* range, int rtx) {
+    const int x0 = blockIdx.x * EX_T, y0 = blockIdx.y * EX_T;
+    float lo = INFINITY, hi = -INFINITY;
+    for (int i = threadIdx.x; i < EX_T * EX_T; i += 256) {
+        const int x = x0 + (i & (EX_T - 1)), y = y0 + i / EX_T;
+        if (x < ls.w && y < ls.h) {
+            const float v = ls.at(x, y);
+            lo = fminf(lo, v);
+            hi = fmaxf(hi, v);
+            if (v != v) lo = hi = NAN;  // a NaN makes the tile non-uniform below
+        }
+    }
+    __shared__ float slo[256], shi[256];
+    slo[threadIdx.x] = lo;
+    shi[threadIdx.x] = hi;
+    __syncthreads();
+    for (int k = 128; k > 0; k >>= 1) {
+        if (threadIdx.x < k) {
+            const float a = slo[threadIdx.x + k], b = shi[threadIdx.x + k];
+            slo[threadIdx.x] = (a != a || slo[threadIdx.x] != slo[threadIdx.x]) ? NAN : fminf(slo[threadIdx.x], a);
+            shi[threadIdx.x] = (b != b || shi[threadIdx.x] != shi[threadIdx.x]) ? NAN : fmaxf(shi[threadIdx.x], b);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) range[blockIdx.y * rtx + blockIdx.x] = make_float2(slo[0], shi[0]);
+}
 __global__ void __launch_bounds__(256) k_extrapolate_fused(ExtrapArgs a) {
     __shared__ float sf[EX_E][EX_E];
     __shared__ unsigned char sv[2][EX_E][EX_E];
@@ -844,6 +873,31 @@ __global__ void __launch_bounds__(256) k_extrapolate_fused(ExtrapArgs a) {
     const int W = f.w, H = f.h;
     const int x0 = blockIdx.x * EX_T - EX_H, y0 = blockIdx.y * EX_T - EX_H;
     const int tid = threadIdx.x;
+    // Every face the tile's image and flags read lies over the 3 x 3 cell tiles around it (the 10-face halo
+    // and the one-cell level-set stencil stay within one tile).  All of their level set < 0: every face is
+    // valid (area_fraction <= 0); all of it > 1e-30: none is (area_fraction > 0; the bound keeps the corner
+    // averages normal).  Either way the ten sweeps change nothing: write the flags only.
+    {
+        int neg = 1, pos = 1;
+        if (tid < 9) {
+            const int tx = min(max((int)blockIdx.x - 1 + tid % 3, 0), a.rtx - 1);
+            const int ty = min(max((int)blockIdx.y - 1 + tid / 3, 0), a.rty - 1);
+            const float2 r = a.range[ty * a.rtx + tx];
+            neg = r.y < 0.0f;    // false for NaN
+            pos = r.x > 1e-30f;  // false for NaN
+        }
+        const int all_neg = __syncthreads_and(neg), all_pos = __syncthreads_and(pos);
+        if (all_neg || all_pos) {
+            const int v = all_neg ? 1 : 0;
+            for (int i = tid; i < EX_T * EX_T; i += 256) {
+                const int x = x0 + EX_H + (i & (EX_T - 1)), y = y0 + EX_H + i / EX_T;
+                if ((unsigned)x >= (unsigned)W || (unsigned)y >= (unsigned)H) continue;
+                a.vin[comp].at(x, y) = v;
+                a.vout[comp].at(x, y) = v;
+            }
+            return;
+        }
+    }
     for (int i = tid; i < EX_E * EX_E; i += 256) {
         const int ly = i / EX_E, lx = i - ly * EX_E, x = x0 + lx, y = y0 + ly;
         float fv = 0.0f;
@@ -1085,8 +1139,9 @@ __global__ void k_fim_init(PF ls1, PF ls0, PU lab0, Dom d) {
         lab0.st(x, y, LABEL_NONE);
     }
 }
-// fast_iterative_method/initialize_active_label.wgsl:8-40
-__global__ void k_fim_active(PU lab0, PU lab, Dom d) {
+// fast_iterative_method/initialize_active_label.wgsl:8-40.  tile_active (optional): set to 1 for every
+// 32 x 32 tile (FIM_TILE) that holds an active cell.
+__global__ void k_fim_active(PU lab0, PU lab, Dom d, unsigned* tile_active, int tiles_x) {
     int x = gx(), y = gy();
     if (x >= d.cx() || y >= d.cy()) return;
     if (lab0.ld(x, y) == LABEL_SOURCE) {
@@ -1103,6 +1158,10 @@ __global__ void k_fim_active(PU lab0, PU lab, Dom d) {
         }
     }
     lab.st(x, y, out);
+    if (tile_active && out == LABEL_ACTIVE) {
+        unsigned* f = &tile_active[(y / 32) * tiles_x + x / 32];
+        if (*f == 0u) atomicOr(f, 1u);
+    }
 }
 // fast_iterative_method/update.wgsl:56-83
 EFL_DEV float abs_get_phi(const PF& p, int x, int y) {
@@ -1184,9 +1243,23 @@ __global__ void k_fim_phase_b(PF T, PU LT, PF S, PU L, Dom d) {
 // and leave.
 constexpr int FIM_TILE = 32, FIM_HALO = 20, FIM_IMG = FIM_TILE + 2 * FIM_HALO, FIM_THREADS = 512;
 constexpr size_t FIM_SMEM = (size_t)4 * FIM_IMG * FIM_IMG * 4;
-__global__ void __launch_bounds__(FIM_THREADS) k_fim_tiled(PF S, PU L, Dom d, int iters, int tiles_x) {
+// tile_active: the flags k_fim_active left (a tile whose 3 x 3 neighbourhood holds no active cell has none in
+// its image, FIM_HALO < FIM_TILE, and leaves at once); valid for the first launch after k_fim_active only.
+__global__ void __launch_bounds__(FIM_THREADS) k_fim_tiled(PF S, PU L, Dom d, int iters, int tiles_x,
+                                                           const unsigned* tile_active) {
     extern __shared__ __align__(16) unsigned char fim_raw[];
     constexpr int N = FIM_IMG * FIM_IMG;
+    static_assert(FIM_HALO < FIM_TILE, "the image lies within the 3 x 3 tiles around the owned one");
+    if (tile_active) {
+        const int tiles_y = (d.ny + FIM_TILE - 1) / FIM_TILE;
+        int any = 0;
+        if (threadIdx.x < 9) {
+            const int tx = (int)(blockIdx.x % tiles_x) - 1 + (int)threadIdx.x % 3;
+            const int ty = (int)(blockIdx.x / tiles_x) - 1 + (int)threadIdx.x / 3;
+            if (tx >= 0 && ty >= 0 && tx < tiles_x && ty < tiles_y) any = tile_active[ty * tiles_x + tx] != 0u;
+        }
+        if (!__syncthreads_or(any)) return;
+    }
     float* s = reinterpret_cast<float*>(fim_raw);
     float* t = s + N;
     uint32_t* l = reinterpret_cast<uint32_t*>(t + N);

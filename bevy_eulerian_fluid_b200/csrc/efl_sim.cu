@@ -122,6 +122,8 @@ struct efl_sim {
     efl_solid_force* d_forces_out = nullptr;
     double2* d_partials = nullptr;
     int n_partials = 0;
+    float2* d_lsrange = nullptr;     // level-set (min, max) per 32 x 32 cell tile (fused extrapolation)
+    unsigned* d_fimtiles = nullptr;  // per 32 x 32 tile: holds an active cell at the start of the FIM iterations
     double* d_norms = nullptr;
     double* h_norms = nullptr;  // pinned
     unsigned long long* d_count = nullptr;
@@ -132,6 +134,9 @@ struct efl_sim {
     CgPlanes cg{};  // MGPCG vectors, allocated on first use
     bool cg_ready = false;
     PF alt32{};          // the MGPCG preconditioner's level-0 ping-pong plane
+    PF alt32_1{};        // its level-1 ping-pong plane (allocated with alt32 when level 1 exists)
+    SweepTma tma_pre1;   // TMA maps of the preconditioner's level 1 (error flag shared with tma)
+    const float* tma_pre1_x = nullptr;  // level 1's iterate plane the maps were built over
     SweepTma tma_pre;    // TMA maps of the preconditioner's level 0 (error flag shared with tma)
     GraphCache gc;                // captured step segments
     uint64_t graph_epoch = 1;     // counts the setters that change kernel arguments
@@ -348,14 +353,18 @@ efl_status st_reinit(efl_sim* s) {  // reinitialize_levelset.rs:162-243
         k_jfa_sdf<<<g, kBlock, count_launch(), s->stream>>>(s->seeds[src], s->ls1, s->ls0, d);
     } else {
         k_fim_init<<<g, kBlock, count_launch(), s->stream>>>(s->ls1, s->ls0, s->lab0, d);
-        k_fim_active<<<g, kBlock, count_launch(), s->stream>>>(s->lab0, s->lab, d);
         const int tx = (d.nx + FIM_TILE - 1) / FIM_TILE, ty = (d.ny + FIM_TILE - 1) / FIM_TILE;
         // The tiled form pays where the grid is large and the interface a small part of it (C3: 4096^2);
         // on small grids the per-phase launches are cheaper (the tiles hold the interface almost everywhere).
-        if (tx * ty >= 4 * s->solver.num_sms && fim_tiled_ready()) {  // the iterations, FIM_HALO / 2 per launch
+        const bool tiled = tx * ty >= 4 * s->solver.num_sms && fim_tiled_ready();
+        if (tiled) CU(cudaMemsetAsync(s->d_fimtiles, 0, (size_t)tx * ty * sizeof(unsigned), s->stream));
+        k_fim_active<<<g, kBlock, count_launch(), s->stream>>>(s->lab0, s->lab, d, tiled ? s->d_fimtiles : nullptr,
+                                                                tx);
+        if (tiled) {  // the iterations, FIM_HALO / 2 per launch
             for (uint32_t k = 0; k < s->cfg.reinit.fim_iterations; k += FIM_HALO / 2) {
                 const int n = (int)std::min<uint32_t>(FIM_HALO / 2, s->cfg.reinit.fim_iterations - k);
-                k_fim_tiled<<<tx * ty, FIM_THREADS, FIM_SMEM + count_launch(), s->stream>>>(s->ls0, s->lab, d, n, tx);
+                k_fim_tiled<<<tx * ty, FIM_THREADS, FIM_SMEM + count_launch(), s->stream>>>(
+                    s->ls0, s->lab, d, n, tx, k == 0 ? s->d_fimtiles : nullptr);
             }
         } else {
             for (uint32_t k = 0; k < s->cfg.reinit.fim_iterations; ++k) {
@@ -799,6 +808,8 @@ efl_status mgpcg(efl_sim* s, SolveResult* res) {
         TRY(alloc_raw(s, s->cg.sc, 1));
         CU(cudaMallocHost(&s->cg.h_read, sizeof(CgRead)));
         TRY(alloc_plane(s, s->alt32, nx, ny, s->P, R));
+        if (s->mg.size() > 1)
+            TRY(alloc_plane(s, s->alt32_1, s->mg[1].nx, s->mg[1].ny, s->mg[1].x.P, s->mg[1].ny + 1));
         if (s->tma.ok) {  // maps of (phi, fractions, b = r32, p = z32 / alt32)
             Level pre0 = s->mg[0];
             pre0.x = s->cg.z32;
@@ -807,6 +818,14 @@ efl_status mgpcg(efl_sim* s, SolveResult* res) {
             sweep_tma_init(s->tma_pre, pre0, s->alt32);
         }
         s->cg_ready = true;
+    }
+    // Level 1 of the preconditioner streams through TMA too where it is too large for the single-CTA tail
+    // (C3: 2048^2); its maps follow the level's planes, which efl_set_projection may reallocate.
+    if (s->tma.ok && s->mg.size() > 2 && s->alt32_1.p && (int64_t)s->mg[1].nx * s->mg[1].ny > VT_MAX_CELLS &&
+        s->tma_pre1_x != s->mg[1].x.p) {
+        s->tma_pre1.d_err = s->tma.d_err;
+        sweep_tma_init(s->tma_pre1, s->mg[1], s->alt32_1);
+        s->tma_pre1_x = s->mg[1].x.p;
     }
     Level64& L = s->mg64[0];
     const MixPlanes& M = s->mixp;
@@ -831,6 +850,7 @@ efl_status mgpcg(efl_sim* s, SolveResult* res) {
     // correction on alt32, alt32 -> z32 black first; the same iterates as
     // four k_gs_color launches each.
     const bool tma0 = s->tma_pre.ok && P.mg_pre == 2 && P.mg_post == 2 && pre.size() > 1;
+    const bool tma1 = tma0 && s->tma_pre1.ok && s->tma_pre1_x == pre[1].x.p && pre.size() > 2;
     auto precondition = [&]() -> efl_status {  // z = M r, then r . z into totals[2]
         CU(cudaMemset2DAsync(C.z32.p, (size_t)C.z32.P * sizeof(float), 0, (size_t)nx * sizeof(float), ny, s->stream));
         if (tma0) {
@@ -843,7 +863,25 @@ efl_status mgpcg(efl_sim* s, SolveResult* res) {
             k_residual<float><<<grid2d(nx, ny, kBlock), kBlock, count_launch(), s->stream>>>(L0, s->U.dt, s->U.rho, dxs);
             k_restriction<float><<<grid2d(C1.nx, C1.ny, kBlock), kBlock, count_launch(), s->stream>>>(L0, C1);
             LAUNCH_CHECK();
-            TRY(v_cycle(s, pre, 1, true));
+            if (tma1) {  // level 1 as at level 0: x (zero) -> alt32_1 red first, coarse correction, back black first
+                const float dxs1 = 2.0f * s->U.dx;  // resolution scale 2 (multi_grid.rs:268-270)
+                TRY(tma_sweep_pass(s->tma_pre1, C1.nx, C1.ny, s->alt32_1, 0, s->solver.num_sms, dxs1, s->U.rho,
+                                   s->U.dt, 1.0f, 2, 1, s->tma.d_err, s->stream));
+                Level L1 = C1;
+                L1.x = s->alt32_1;
+                const Level& C2 = pre[2];
+                k_residual<float><<<grid2d(C1.nx, C1.ny, kBlock), kBlock, count_launch(), s->stream>>>(
+                    L1, s->U.dt, s->U.rho, dxs1);
+                k_restriction<float><<<grid2d(C2.nx, C2.ny, kBlock), kBlock, count_launch(), s->stream>>>(L1, C2);
+                LAUNCH_CHECK();
+                TRY(v_cycle(s, pre, 2, true));
+                k_prolongation<float><<<grid2d(C2.nx, C2.ny, kBlock), kBlock, count_launch(), s->stream>>>(L1, C2);
+                LAUNCH_CHECK();
+                TRY(tma_sweep_pass(s->tma_pre1, C1.nx, C1.ny, C1.x, 1, s->solver.num_sms, dxs1, s->U.rho, s->U.dt,
+                                   1.0f, 2, 0, s->tma.d_err, s->stream));
+            } else {
+                TRY(v_cycle(s, pre, 1, true));
+            }
             k_prolongation<float><<<grid2d(C1.nx, C1.ny, kBlock), kBlock, count_launch(), s->stream>>>(L0, C1);
             LAUNCH_CHECK();
             TRY(tma_sweep_pass(s->tma_pre, nx, ny, C.z32, 1, s->solver.num_sms, dxs, s->U.rho, s->U.dt, 1.0f, 2,
@@ -1055,7 +1093,9 @@ efl_status st_solve_velocity(efl_sim* s) {
 efl_status st_extrapolate(efl_sim* s) {  // render_node.rs:540-608
     Dom d = s->dom();
     if (d.nx % 64 == 0 && d.ny % 64 == 0) {  // every face covered: one fused launch
-        ExtrapArgs a{{s->u0, s->v0}, {s->uvi, s->vvi}, {s->uvo, s->vvo}, s->ls0};
+        const int rtx = (d.nx + EX_T - 1) / EX_T, rty = (d.ny + EX_T - 1) / EX_T;
+        k_ls_tile_range<<<dim3(rtx, rty), 256, count_launch(), s->stream>>>(s->ls0, s->d_lsrange, rtx);
+        ExtrapArgs a{{s->u0, s->v0}, {s->uvi, s->vvi}, {s->uvo, s->vvo}, s->ls0, s->d_lsrange, rtx, rty};
         const dim3 g((d.nx + 1 + EX_T - 1) / EX_T, (d.ny + 1 + EX_T - 1) / EX_T, 2);
         k_extrapolate_fused<<<g, 256, count_launch(), s->stream>>>(a);
         LAUNCH_CHECK();
@@ -1365,6 +1405,8 @@ efl_status efl_create(const efl_config* cfg, efl_sim** out) {
     CTRY(alloc_raw(s, s->d_forces_out, EFL_MAX_SOLIDS));
     s->n_partials = std::min(1024, std::max(1, (nx * ny + NORM_THREADS - 1) / NORM_THREADS));
     CTRY(alloc_raw(s, s->d_partials, s->n_partials));
+    CTRY(alloc_raw(s, s->d_lsrange, (size_t)((nx + EX_T - 1) / EX_T) * ((ny + EX_T - 1) / EX_T)));
+    CTRY(alloc_raw(s, s->d_fimtiles, (size_t)((nx + FIM_TILE - 1) / FIM_TILE) * ((ny + FIM_TILE - 1) / FIM_TILE)));
     CTRY(alloc_raw(s, s->d_norms, 2));
     CTRY(alloc_raw(s, s->d_count, 1));
     if (cudaMallocHost(&s->h_norms, 4 * sizeof(double)) != cudaSuccess)

@@ -198,6 +198,23 @@ def test_mgpcg_bit_exact(oracle_api, gpu_api):
     assert not bad, bad
 
 
+def test_mgpcg_tma_levels_bit_exact(oracle_api, gpu_api):
+    """MGPCG at 512^2: the preconditioner smooths levels 0 (512^2) and 1 (256^2) with the TMA-streamed sweep
+    and the rest in the single-CTA tail; same CG counts and bit-exact fields."""
+    sc = scenes.scale(512)
+    sc.cfg.projection.method = capi.PROJECTION_MGPCG
+    o, g = make_pair(sc, oracle_api, gpu_api)
+    o.step(sc.dt)
+    g.step(sc.dt)
+    for _ in range(3):
+        so, sg = o.step(sc.dt), g.step(sc.dt)
+        assert so.converged and sg.converged
+        assert so.pressure_iterations == sg.pressure_iterations
+        assert so.residual == sg.residual and so.residual_initial == sg.residual_initial
+    bad = compare_fields(g, o)
+    assert not bad, bad
+
+
 def test_mgpcg_with_bodies_bit_exact(oracle_api, gpu_api):
     """MGPCG on the coupled scene (bodies, fractional faces, JFA)."""
     sc = small_coupled(128, method=capi.PROJECTION_MGPCG)
