@@ -14,7 +14,7 @@ metric: cell-steps/s to 1e-5 relative residual = cells x steps / time.
   e2e    -- the same steps through the plugin API with the two-way
             coupling loop: H2D upload of the 24 packed obstacles, the step,
             D2H read-back of the solid forces, host rigid integration.
-  roofline -- the dominant kernel, k_gsmix_quad (one cooperative
+  roofline -- the dominant kernel, k_gsmix_oct (one cooperative
             launch = one whole tolerance-driven solve), re-run from the same
             pre-projection state: 32 algorithmic bytes per cell per red-black
             iteration (p read+write 8, div 4, phi 4, area fractions 16) x
@@ -101,11 +101,11 @@ def profile_traffic():
     (None, None) if absent.  The label names the file and a hash of its content,
     so a stale profile is visible next to the number."""
     import hashlib
-    p = os.path.join(REPO, "profiles", "k_gsmix_quad_coupled_512.txt")
+    p = os.path.join(REPO, "profiles", "k_gsmix_oct_coupled_512.txt")
     if not os.path.exists(p):
         return None, None
     data = open(p, "rb").read()
-    tag = f"from committed ncu profile profiles/k_gsmix_quad_coupled_512.txt (sha256 " \
+    tag = f"from committed ncu profile profiles/k_gsmix_oct_coupled_512.txt (sha256 " \
           f"{hashlib.sha256(data).hexdigest()[:12]}), not measured in this run"
     for line in data.decode().splitlines():
         if line.startswith("dram_bytes_per_rb_iteration:"):
@@ -365,7 +365,7 @@ def main():
     d2h = capi.MAX_SOLIDS * 16
 
     # ---- roofline of the dominant kernel over the timed steps: each step's projection stage is one
-    # k_gsmix_quad launch (the whole tolerance-driven solve) plus the FP32 <-> FP64 copies around it.
+    # k_gsmix_oct launch (the whole tolerance-driven solve) plus the FP32 <-> FP64 copies around it.
     solve_ms = sum(proj_ms)
     solve_it = sum(iters)
     peak, peak_kind = measured_peaks()
@@ -376,7 +376,7 @@ def main():
                 "traffic": round(per_it * solve_it / args.steps) if per_it is not None else None,
                 "traffic_source": traffic_src,
                 "algorithmic_bytes_per_launch": round(ALGO_BYTES_PER_CELL_ITER * sc.cells * solve_it / args.steps),
-                "kernel": "k_gsmix_quad (one launch per step = one tolerance-driven solve)",
+                "kernel": "k_gsmix_oct (one launch per step = one tolerance-driven solve)",
                 "launch_ms": round(solve_ms / args.steps, 4), "iterations_per_launch": round(solve_it / args.steps, 1),
                 "iteration_us": round(solve_ms * 1e3 / max(1, solve_it), 4), "peak_kind": peak_kind,
                 "timing": "CUDA events around every timed step's projection stage (efl_projection_ms), summed",

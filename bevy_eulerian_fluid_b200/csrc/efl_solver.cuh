@@ -116,6 +116,7 @@ struct PersistentParams {
     SolveResult* result;
     long long spin_limit;  // grid-barrier polls before giving up
     PF dbuf2;              // the exchanges alternate between the correction planes dbuf and dbuf2
+    float one;             // 1.0f, passed at run time (see x2_add1)
 };
 
 constexpr unsigned char MODE_SKIP = 0;     // outside the domain or on the tile's outer ring
@@ -853,6 +854,385 @@ __global__ void __launch_bounds__(NT, 1) k_gsmix_quad(PersistentParams P, PF dbu
     }
 }
 
+// ---------------------------------------------------------------------------
+// Paired-lane form of the persistent mixed solve (4 x 2 cells per thread).
+//
+// The same iterates as k_gsmix_quad (the same f32 update in the same
+// operation order on every cell, the same FP64 checks), with each thread
+// owning a 4 x 2 block of the extended tile: cells c0..c3 in its upper row,
+// c4..c7 in its lower one.  A half-sweep updates four of them, in two pairs
+// of one colour (c0, c2) and (c5, c7), or (c1, c3) and (c4, c6), and the two
+// cells of a pair are the two lanes of Blackwell's paired f32 instructions
+// (mul.rn.f32x2 for the products, fma.rn.f32x2 by a run-time 1.0 for the
+// sums: per lane the IEEE-rounded f32 product and sum, so each lane is the
+// scalar update exactly).  The layout makes the operand pairs fall out of it:
+//  * in the colour-compressed shared image of the correction
+//    (d[k][y][x / 2]) a pair's two cells are adjacent words, so one 8-byte
+//    load brings both neighbours above (or below) a pair and one 8-byte store
+//    publishes the pair;
+//  * of the eight neighbour values a pair needs, four come from the thread's
+//    own registers as ready-made pairs, two from one 8-byte load and two
+//    (left of c0 / c4, right of c3 / c7) from a 4-byte load packed with a
+//    register lane;
+//  * the face weights, 1/den and the right-hand side stay in registers as
+//    lane pairs for the whole solve.
+// Cells on the tile image's outermost ring update too, from clamped
+// neighbour values: their results are as wrong as the stale values a frozen
+// ring would hold, and like those they move inwards one ring per half-sweep,
+// so the owned cells are exact after the 2K half-sweeps between exchanges
+// (every value stays finite, and the exchange reloads the ring).
+typedef unsigned long long f32x2;  // lane 0 = low word
+EFL_DEV f32x2 x2_pack(float lo, float hi) {
+    f32x2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+EFL_DEV float x2_lane(f32x2 v, int lane) {
+    float a, b;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
+    return lane ? b : a;
+}
+EFL_DEV f32x2 x2_mul(f32x2 a, f32x2 b) {
+    f32x2 r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+// round(a + c) per lane, written as fma(a, one, c) with one = 1.0 known only at
+// run time.  ptxas contracts a paired product feeding a paired add (mul.rn /
+// add.rn f32x2) into one fused multiply-add, -fmad=false notwithstanding,
+// which drops the product's rounding; a product feeding the multiplicand of
+// an FMA by an unknown factor cannot be contracted, and a * 1 + c rounds once,
+// exactly like the add (signed zeros included).
+EFL_DEV f32x2 x2_add1(f32x2 a, f32x2 one, f32x2 c) {
+    f32x2 r;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(one), "l"(c));
+    return r;
+}
+// The update of two cells: nume = rc + wl L + wr R + wu U + wd D (in that
+// order, each product rounded), d' = wgt (nume inv) + omw d.
+EFL_DEV f32x2 oct_update(f32x2 rc, f32x2 wl, f32x2 wr, f32x2 wu, f32x2 wd, f32x2 inv, f32x2 omw, f32x2 d, f32x2 L,
+                         f32x2 R, f32x2 U, f32x2 D, f32x2 wgt, f32x2 one) {
+    f32x2 n = x2_add1(x2_mul(wl, L), one, rc);
+    n = x2_add1(x2_mul(wr, R), one, n);
+    n = x2_add1(x2_mul(wu, U), one, n);
+    n = x2_add1(x2_mul(wd, D), one, n);
+    return x2_add1(x2_mul(wgt, x2_mul(n, inv)), one, x2_mul(omw, d));
+}
+
+template <int EX, int EY>
+struct OctTile {
+    static constexpr int W2 = EX / 2, W4 = EX / 4, NB = (EX / 4) * (EY / 2);
+    static constexpr int WP = W2 % 16 == 4 ? W2 : W2 + ((4 - W2 % 16) + 16) % 16;  // row stride of d (words)
+    double p[EY][EX];
+    double b[EY][EX];
+    double den[EY][EX];
+    float d[2][EY][WP];  // [k][y][x / 2], k = (x + y) & 1 in the image (k = 0: the tile's base colour)
+};
+
+// Cell q of a thread's block: (q & 3, q >> 2); its pair 2 (q >> 2) + (q & 1) of
+// {(c0, c2), (c1, c3), (c4, c6), (c5, c7)} and its lane (q >> 1) & 1.
+EFL_DEV constexpr int oct_pair(int q) { return 2 * (q >> 2) + (q & 1); }
+EFL_DEV constexpr int oct_lane(int q) { return (q >> 1) & 1; }
+
+template <int EX, int EY, int KMAX, int NT>
+__global__ void __launch_bounds__(NT, 1) k_gsmix_oct(PersistentParams P, PF dbuf) {
+    using Tile = OctTile<EX, EY>;
+    static_assert(KMAX >= 1 && EX % 4 == 0 && EY % 2 == 0, "4 x 2 blocks");
+    static_assert(Tile::NB <= NT && NT % 32 == 0, "one thread per 4 x 2 block");
+    static_assert((2 * KMAX) % 4 == 0, "halo of whole blocks");
+    extern __shared__ __align__(16) unsigned char ps_raw[];
+    Tile& T = *reinterpret_cast<Tile*>(ps_raw);
+    constexpr int H = 2 * KMAX, W2 = Tile::W2, W4 = Tile::W4, NB = Tile::NB, WP = Tile::WP;
+    constexpr int TXo = EX - 2 * H, TYo = EY - 2 * H;
+    const Level64& L = P.L;
+    const int tile = blockIdx.x;
+    const int gx0 = (tile % P.tiles_x) * TXo - H, gy0 = (tile / P.tiles_x) * TYo - H;
+    const unsigned nblocks = gridDim.x;
+    const bool active = threadIdx.x < NB;
+    const int bx = active ? (int)threadIdx.x % W4 : 0, by = active ? (int)threadIdx.x / W4 : 0;
+    const int base = (gx0 + gy0) & 1;  // colour of the k = 0 cells (1 = red, (x + y) odd)
+    const bool owned = active && bx >= H / 4 && bx < (H + TXo) / 4 && by >= H / 2 && by < (H + TYo) / 2;
+    const int x0 = 4 * bx, y0 = 2 * by, y1 = 2 * by + 1;
+    const float wgt = (float)P.weight, omw1 = 1.0f - (float)P.weight;
+    // bit q: update cell; 8 + q: live (not on the outermost ring); 16 + q: counted and live; 24 + q: owned and in
+    // the domain
+    unsigned fl = 0;
+    f32x2 wl[4], wr[4], wu[4], wd[4], inv[4], rc[4], dv[4];
+    {
+        float fw[4][8], finv[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int lx = x0 + (q & 3), ly = y0 + (q >> 2);
+            const int gx = gx0 + lx, gy = gy0 + ly;
+            const bool live = active && lx > 0 && lx < EX - 1 && ly > 0 && ly < EY - 1;
+            if (live) fl |= 1u << (8 + q);
+            float wv[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+            finv[q] = 0.0f;
+            double den = 0.0, bb = 0.0, pv = 0.0;
+            if (active && (unsigned)gx < (unsigned)L.nx && (unsigned)gy < (unsigned)L.ny) {
+                const float phi = L.ls.at(gx, gy);
+                bb = L.b.at(gx, gy);
+                pv = __ldcg(&L.x.p[(size_t)gy * L.x.P + gx]);
+                if (owned) fl |= 1u << (24 + q);
+                if (phi < 0.0f) {
+                    const float f[4] = {L.fu.at(gx, gy), L.fu.at(gx + 1, gy), L.fv.at(gx, gy), L.fv.at(gx, gy + 1)};
+                    if (!(f[0] == 0.0f && f[1] == 0.0f && f[2] == 0.0f && f[3] == 0.0f)) {
+                        if (live) fl |= 1u << (16 + q);
+                        const int ox[4] = {-1, 1, 0, 0}, oy[4] = {0, 0, -1, 1};
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) {
+                            const int jx = gx + ox[k], jy = gy + oy[k];
+                            if ((unsigned)jx < (unsigned)L.nx && (unsigned)jy < (unsigned)L.ny) {
+                                const float level = L.ls.at(jx, jy);
+                                if (level < 0.0f) {
+                                    den += (double)f[k];
+                                    wv[k] = f[k];
+                                } else {
+                                    den += (double)f[k] * (1.0 - (double)level / (double)phi);
+                                }
+                            }
+                        }
+                        if (!(fabs(den) < (double)1.0e-6f)) {
+                            if (live) fl |= 1u << q;
+                            finv[q] = (float)(1.0 / den);
+                        }
+                    }
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < 4; ++k) fw[k][q] = wv[k];
+            if (active) {
+                T.p[ly][lx] = pv;
+                T.b[ly][lx] = bb;
+                T.den[ly][lx] = den;
+            }
+        }
+        // pair i = (cells qa, qb): (0, 2), (1, 3), (4, 6), (5, 7)
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int qa = (i >> 1) * 4 + (i & 1), qb = qa + 2;
+            wl[i] = x2_pack(fw[0][qa], fw[0][qb]);
+            wr[i] = x2_pack(fw[1][qa], fw[1][qb]);
+            wu[i] = x2_pack(fw[2][qa], fw[2][qb]);
+            wd[i] = x2_pack(fw[3][qa], fw[3][qb]);
+            inv[i] = x2_pack(finv[qa], finv[qb]);
+            rc[i] = 0;
+            dv[i] = 0;
+        }
+    }
+    // every word of the correction image starts at 0 (rows' padding included)
+    for (int i = threadIdx.x; i < 2 * EY * WP; i += NT) (&T.d[0][0][0])[i] = 0.0f;
+    __syncthreads();
+    const double cdiv = P.cdiv, factor = P.factor;
+    const f32x2 wgt2 = x2_pack(wgt, wgt), omw2 = x2_pack(omw1, omw1), one2 = x2_pack(P.one, P.one);
+    // Shared-memory words of the neighbours in other blocks, clamped inside the image for the outermost blocks.
+    const int cl = max(2 * bx - 1, 0), cr = min(2 * bx + 2, W2 - 1), ru = max(y0 - 1, 0), rd = min(y1 + 1, EY - 1);
+    // most central ring among the block's cells
+    const int bmax = min(min(x0 + 3, EX - 1 - x0), min(y0 + 1, EY - 1 - y0));
+    // k = 0 half-sweep: pairs (c0, c2) and (c5, c7), neighbours from the k = 1 image
+    auto sweep0 = [&]() {
+        float(*D1)[WP] = T.d[1];
+        const f32x2 up = *reinterpret_cast<const f32x2*>(&D1[ru][2 * bx]);
+        const f32x2 dn = *reinterpret_cast<const f32x2*>(&D1[rd][2 * bx]);
+        const float lf = D1[y0][cl], rt = D1[y1][cr];
+        dv[0] = oct_update(rc[0], wl[0], wr[0], wu[0], wd[0], inv[0], omw2, dv[0], x2_pack(lf, x2_lane(dv[1], 0)),
+                           dv[1], up, dv[2], wgt2, one2);
+        dv[3] = oct_update(rc[3], wl[3], wr[3], wu[3], wd[3], inv[3], omw2, dv[3], dv[2],
+                           x2_pack(x2_lane(dv[2], 1), rt), dv[1], dn, wgt2, one2);
+        if (active) {
+            *reinterpret_cast<f32x2*>(&T.d[0][y0][2 * bx]) = dv[0];
+            *reinterpret_cast<f32x2*>(&T.d[0][y1][2 * bx]) = dv[3];
+        }
+    };
+    // k = 1 half-sweep: pairs (c1, c3) and (c4, c6), neighbours from the k = 0 image
+    auto sweep1 = [&]() {
+        float(*D0)[WP] = T.d[0];
+        const f32x2 up = *reinterpret_cast<const f32x2*>(&D0[ru][2 * bx]);
+        const f32x2 dn = *reinterpret_cast<const f32x2*>(&D0[rd][2 * bx]);
+        const float rt = D0[y0][cr], lf = D0[y1][cl];
+        dv[1] = oct_update(rc[1], wl[1], wr[1], wu[1], wd[1], inv[1], omw2, dv[1], dv[0],
+                           x2_pack(x2_lane(dv[0], 1), rt), up, dv[3], wgt2, one2);
+        dv[2] = oct_update(rc[2], wl[2], wr[2], wu[2], wd[2], inv[2], omw2, dv[2], x2_pack(lf, x2_lane(dv[3], 0)),
+                           dv[3], dv[0], dn, wgt2, one2);
+        if (active) {
+            *reinterpret_cast<f32x2*>(&T.d[1][y0][2 * bx]) = dv[1];
+            *reinterpret_cast<f32x2*>(&T.d[1][y1][2 * bx]) = dv[2];
+        }
+    };
+    // FP64 residual of the live counted cells, rc = f32(cdiv r) on update cells, d = 0, and the CTA's norms over
+    // its owned counted cells (fixed order; returned by thread 0).
+    auto check = [&]() -> double2 {
+        double ar = 0.0, ab = 0.0;
+        float frc[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int lx = x0 + (q & 3), ly = y0 + (q >> 2);
+            const int i = oct_pair(q), ln = oct_lane(q);
+            float rcv = 0.0f;
+            if ((fl >> (16 + q)) & 1u) {
+                double sum = (double)x2_lane(wl[i], ln) * T.p[ly][lx - 1];
+                sum = sum + (double)x2_lane(wr[i], ln) * T.p[ly][lx + 1];
+                sum = sum + (double)x2_lane(wu[i], ln) * T.p[ly - 1][lx];
+                sum = sum + (double)x2_lane(wd[i], ln) * T.p[ly + 1][lx];
+                const double bb = T.b[ly][lx];
+                const double r = bb - factor * (T.den[ly][lx] * T.p[ly][lx] - sum);
+                if ((fl >> q) & 1u) rcv = (float)(cdiv * r);
+                if ((fl >> (24 + q)) & 1u) {
+                    ar += r * r;
+                    ab += bb * bb;
+                }
+            }
+            frc[q] = rcv;
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int qa = (i >> 1) * 4 + (i & 1);
+            rc[i] = x2_pack(frc[qa], frc[qa + 2]);
+            dv[i] = 0;
+        }
+        if (active) {
+            *reinterpret_cast<f32x2*>(&T.d[0][y0][2 * bx]) = 0;
+            *reinterpret_cast<f32x2*>(&T.d[1][y0][2 * bx]) = 0;
+            *reinterpret_cast<f32x2*>(&T.d[1][y1][2 * bx]) = 0;
+            *reinterpret_cast<f32x2*>(&T.d[0][y1][2 * bx]) = 0;
+        }
+        ar = warp_sum(ar);
+        ab = warp_sum(ab);
+        __shared__ double red_r[NT / 32], red_b[NT / 32];
+        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+        if (lane == 0) {
+            red_r[wid] = ar;
+            red_b[wid] = ab;
+        }
+        __syncthreads();
+        double2 out = make_double2(0.0, 0.0);
+        if (threadIdx.x == 0) {
+            for (int k = 0; k < NT / 32; ++k) {
+                out.x += red_r[k];
+                out.y += red_b[k];
+            }
+        }
+        __syncthreads();
+        return out;
+    };
+
+    unsigned iters = 0, xch = 0;
+    double2 part = check();
+    if (threadIdx.x == 0) P.partials[blockIdx.x] = part;
+    bool ok = grid_barrier(P.barrier, nblocks, P.spin_limit);
+    double r = ok ? ps_total_relative(P.partials, nblocks) : 0.0;
+    const double r0v = r;
+    bool pending = false;  // a check's total, read at the next block's first exchange
+    while (ok && (pending || (!(r <= P.tol) && iters < P.max_iters))) {
+        unsigned todo = min(P.check_interval, P.max_iters - iters);
+        unsigned done = 0;
+        bool converged = false;
+        while (ok && todo > 0) {
+            const unsigned kk = min((unsigned)KMAX, todo);
+            for (unsigned it = 0; it < kk; ++it) {
+                if (bmax >= 1 + 2 * (int)it) {  // a cell of the block lies in the region still needed
+                    if (base) sweep0();  // red ((x + y) odd) first
+                    else sweep1();
+                }
+                __syncthreads();
+                if (bmax >= 2 + 2 * (int)it) {
+                    if (base) sweep1();
+                    else sweep0();
+                }
+                __syncthreads();
+            }
+            todo -= kk;
+            done += kk;
+            if (todo > 0) {  // exchange the correction's halo through L2, alternating planes
+                const PF& db = (xch++ & 1) ? P.dbuf2 : dbuf;
+                if (owned) {
+#pragma unroll
+                    for (int q = 0; q < 8; ++q)
+                        if ((fl >> (24 + q)) & 1u)
+                            __stcg(&db.p[(size_t)(gy0 + y0 + (q >> 2)) * db.P + gx0 + x0 + (q & 3)],
+                                   x2_lane(dv[oct_pair(q)], oct_lane(q)));
+                }
+                ok = grid_barrier(P.barrier, nblocks, P.spin_limit);
+                if (!ok) break;
+                if (pending) {
+                    pending = false;
+                    r = ps_total_relative(P.partials, nblocks);
+                    if (r <= P.tol) {
+                        converged = true;
+                        break;
+                    }
+                }
+                if (active && !owned) {
+                    float hv[8];
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) {
+                        const int gx = gx0 + x0 + (q & 3), gy = gy0 + y0 + (q >> 2);
+                        hv[q] = ((unsigned)gx < (unsigned)L.nx && (unsigned)gy < (unsigned)L.ny)
+                                    ? __ldcg(&db.p[(size_t)gy * db.P + gx])
+                                    : 0.0f;
+                    }
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) {
+                        const int qa = (i >> 1) * 4 + (i & 1);
+                        dv[i] = x2_pack(hv[qa], hv[qa + 2]);
+                    }
+                    *reinterpret_cast<f32x2*>(&T.d[0][y0][2 * bx]) = dv[0];
+                    *reinterpret_cast<f32x2*>(&T.d[1][y0][2 * bx]) = dv[1];
+                    *reinterpret_cast<f32x2*>(&T.d[1][y1][2 * bx]) = dv[2];
+                    *reinterpret_cast<f32x2*>(&T.d[0][y1][2 * bx]) = dv[3];
+                }
+                __syncthreads();
+            }
+        }
+        if (!ok || converged) break;
+        iters += done;
+        // p += d on the owned cells (0 where the reference zeroes p), then exchange p.
+        if (owned) {
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                if ((fl >> (24 + q)) & 1u) {
+                    const int lx = x0 + (q & 3), ly = y0 + (q >> 2);
+                    const double pv =
+                        ((fl >> q) & 1u) ? T.p[ly][lx] + (double)x2_lane(dv[oct_pair(q)], oct_lane(q)) : 0.0;
+                    T.p[ly][lx] = pv;
+                    __stcg(&L.x.p[(size_t)(gy0 + ly) * L.x.P + gx0 + lx], pv);
+                }
+            }
+        }
+        ok = grid_barrier(P.barrier, nblocks, P.spin_limit);
+        if (!ok) break;
+        if (active && !owned) {
+            double hp[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const int gx = gx0 + x0 + (q & 3), gy = gy0 + y0 + (q >> 2);
+                hp[q] = ((unsigned)gx < (unsigned)L.nx && (unsigned)gy < (unsigned)L.ny)
+                            ? __ldcg(&L.x.p[(size_t)gy * L.x.P + gx])
+                            : 0.0;
+            }
+#pragma unroll
+            for (int q = 0; q < 8; ++q) T.p[y0 + (q >> 2)][x0 + (q & 3)] = hp[q];
+        }
+        __syncthreads();
+        part = check();
+        if (threadIdx.x == 0) P.partials[blockIdx.x] = part;
+        if (min(P.check_interval, P.max_iters - iters) > (unsigned)KMAX) {
+            pending = true;
+        } else {
+            ok = grid_barrier(P.barrier, nblocks, P.spin_limit);
+            if (!ok) break;
+            r = ps_total_relative(P.partials, nblocks);
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        P.result->iterations = iters;
+        P.result->converged = (ok && r <= P.tol) ? 1 : 0;
+        P.result->error = ok ? 0 : 1;
+        P.result->r0 = r0v;
+        P.result->r1 = r;
+    }
+}
+
 // The reference's fixed-count f32 sweeps (gauss_seidel.wgsl:12-88, `iters`
 // red-black iterations, red first) as ONE cooperative launch for grids of at
 // most one 64 x 32 tile per SM (C1's 256^2, 512^2): the 2 x 2-block layout
@@ -1351,6 +1731,30 @@ struct PersistentPlan {
     bool ok = false;
 };
 
+// One CTA of `threads` threads with `smem` bytes of dynamic shared memory resident per SM (registers and shared
+// memory both; sets the kernel's shared-memory limit), checked once per kernel and device.
+template <const void* (*KernelOf)()>
+inline bool plan_resident(int threads, size_t smem) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    static signed char state[64] = {};  // 0 unknown, 1 resident, -1 not
+    if (dev < 0 || dev >= 64) return false;
+    if (!state[dev]) {
+        const void* k = KernelOf();
+        int per_sm = 0;
+        const bool ok = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) == cudaSuccess &&
+                        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, smem) == cudaSuccess &&
+                        per_sm >= 1;
+        cudaGetLastError();
+        state[dev] = ok ? 1 : -1;
+    }
+    return state[dev] == 1;
+}
+template <int EX, int EY, int KMAX, int NT>
+inline const void* oct_kernel() { return (const void*)k_gsmix_oct<EX, EY, KMAX, NT>; }
+template <int EX, int EY, int KMAX, int NT>
+inline const void* quad_kernel() { return (const void*)k_gsmix_quad<EX, EY, KMAX, NT>; }
+
 // Plans for the mixed persistent solve (MixTile: 53 bytes per cell).
 template <int EX, int EY, int KMAX>
 inline bool try_plan_mix(const SolverWorkspace& ws, int nx, int ny, PersistentPlan* p) {
@@ -1380,10 +1784,33 @@ inline bool try_plan_quad(const SolverWorkspace& ws, int nx, int ny, PersistentP
     p->threads = NT;
     if (p->smem + 2048 > ws.max_smem) return false;
     if (p->tiles_x * p->tiles_y > ws.num_sms || p->tiles_x * p->tiles_y > ws.max_blocks) return false;
-    return true;
+    return plan_resident<quad_kernel<EX, EY, KMAX, NT>>(NT, p->smem);
+}
+// Plans for the paired-lane form (OctTile: 26 bytes of shared memory per cell).
+template <int EX, int EY, int KMAX, int NT>
+inline bool try_plan_oct(const SolverWorkspace& ws, int nx, int ny, PersistentPlan* p) {
+    const int tx = EX - 4 * KMAX, ty = EY - 4 * KMAX;
+    p->kmax = KMAX;
+    p->tx = tx;
+    p->ty = ty;
+    p->tiles_x = (nx + tx - 1) / tx;
+    p->tiles_y = (ny + ty - 1) / ty;
+    p->smem = sizeof(OctTile<EX, EY>);
+    p->kernel = (const void*)k_gsmix_oct<EX, EY, KMAX, NT>;
+    p->threads = NT;
+    if (p->smem + 2048 > ws.max_smem) return false;
+    if (p->tiles_x * p->tiles_y > ws.num_sms || p->tiles_x * p->tiles_y > ws.max_blocks) return false;
+    return plan_resident<oct_kernel<EX, EY, KMAX, NT>>(NT, p->smem);
 }
 inline PersistentPlan plan_mix(const SolverWorkspace& ws, int nx, int ny) {
     PersistentPlan p;
+    if (ws.use_reg && (try_plan_oct<80, 48, 4, 480>(ws, nx, ny, &p) ||   // 64 x 32 owned
+                       try_plan_oct<48, 48, 4, 288>(ws, nx, ny, &p) ||   // 32 x 32
+                       try_plan_oct<72, 56, 2, 512>(ws, nx, ny, &p) ||   // 64 x 48
+                       try_plan_oct<40, 40, 4, 224>(ws, nx, ny, &p))) {  // 24 x 24
+        p.ok = true;
+        return p;
+    }
     if (ws.use_reg && (try_plan_quad<80, 48, 4, 960>(ws, nx, ny, &p) ||  // 64 x 32 owned
                        try_plan_quad<48, 48, 4, 576>(ws, nx, ny, &p) ||  // 32 x 32
                        try_plan_quad<72, 56, 2, 1024>(ws, nx, ny, &p) ||  // 64 x 48
@@ -1440,6 +1867,7 @@ inline efl_status solve_gsmix_persistent(SolverWorkspace& ws, const Level64& L, 
     P.result = ws.result;
     P.spin_limit = ws.spin_limit > 0 ? ws.spin_limit : kBarrierSpinLimit;
     P.dbuf2 = dbuf2;
+    P.one = 1.0f;
     if (cudaMemsetAsync(ws.barrier, 0, sizeof(GridBarrier), stream) != cudaSuccess) {
         *err = "barrier reset failed";
         return EFL_ERR_CUDA;
