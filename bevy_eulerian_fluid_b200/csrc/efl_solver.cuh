@@ -24,6 +24,7 @@
 #include <algorithm>
 #include <cmath>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "efl_kernels.cuh"
@@ -919,9 +920,9 @@ EFL_DEV f32x2 oct_update(f32x2 rc, f32x2 wl, f32x2 wr, f32x2 wu, f32x2 wd, f32x2
     return x2_add1(x2_mul(wgt, x2_mul(n, inv)), one, x2_mul(omw, d));
 }
 
-template <int EX, int EY>
+template <int EX, int EY, int ROWS>
 struct OctTile {
-    static constexpr int W2 = EX / 2, W4 = EX / 4, NB = (EX / 4) * (EY / 2);
+    static constexpr int W2 = EX / 2, W4 = EX / 4, NB = (EX / 4) * (EY / ROWS);
     static constexpr int WP = W2 % 16 == 4 ? W2 : W2 + ((4 - W2 % 16) + 16) % 16;  // row stride of d (words)
     double p[EY][EX];
     double b[EY][EX];
@@ -929,17 +930,20 @@ struct OctTile {
     float d[2][EY][WP];  // [k][y][x / 2], k = (x + y) & 1 in the image (k = 0: the tile's base colour)
 };
 
-// Cell q of a thread's block: (q & 3, q >> 2); its pair 2 (q >> 2) + (q & 1) of
-// {(c0, c2), (c1, c3), (c4, c6), (c5, c7)} and its lane (q >> 1) & 1.
-EFL_DEV constexpr int oct_pair(int q) { return 2 * (q >> 2) + (q & 1); }
-EFL_DEV constexpr int oct_lane(int q) { return (q >> 1) & 1; }
+// Cell q of a thread's 4 x ROWS block sits at (i, j) = (q & 3, q >> 2); its colour in the image is
+// k = (i + j) & 1, and it is lane i >> 1 of pair 2 j + k: the pair of the two cells of colour k in row j,
+// which are adjacent words (2 bx, 2 bx + 1) of the colour-compressed image.
+EFL_DEV constexpr int oct_pair(int q) { return 2 * (q >> 2) + (((q & 3) + (q >> 2)) & 1); }
+EFL_DEV constexpr int oct_lane(int q) { return (q & 3) >> 1; }
 
-template <int EX, int EY, int KMAX, int NT>
+template <int EX, int EY, int KMAX, int NT, int ROWS>
 __global__ void __launch_bounds__(NT, 1) k_gsmix_oct(PersistentParams P, PF dbuf) {
-    using Tile = OctTile<EX, EY>;
-    static_assert(KMAX >= 1 && EX % 4 == 0 && EY % 2 == 0, "4 x 2 blocks");
-    static_assert(Tile::NB <= NT && NT % 32 == 0, "one thread per 4 x 2 block");
-    static_assert((2 * KMAX) % 4 == 0, "halo of whole blocks");
+    using Tile = OctTile<EX, EY, ROWS>;
+    constexpr int NC = 4 * ROWS, NPAIR = 2 * ROWS;
+    static_assert(KMAX >= 1 && EX % 4 == 0 && EY % ROWS == 0 && ROWS % 2 == 0, "4 x ROWS blocks");
+    static_assert(Tile::NB <= NT && NT % 32 == 0, "one thread per block");
+    static_assert((2 * KMAX) % 4 == 0 && (2 * KMAX) % ROWS == 0, "halo of whole blocks");
+    static_assert(NC <= 16, "cell flags in 64 bits");
     extern __shared__ __align__(16) unsigned char ps_raw[];
     Tile& T = *reinterpret_cast<Tile*>(ps_raw);
     constexpr int H = 2 * KMAX, W2 = Tile::W2, W4 = Tile::W4, NB = Tile::NB, WP = Tile::WP;
@@ -951,21 +955,21 @@ __global__ void __launch_bounds__(NT, 1) k_gsmix_oct(PersistentParams P, PF dbuf
     const bool active = threadIdx.x < NB;
     const int bx = active ? (int)threadIdx.x % W4 : 0, by = active ? (int)threadIdx.x / W4 : 0;
     const int base = (gx0 + gy0) & 1;  // colour of the k = 0 cells (1 = red, (x + y) odd)
-    const bool owned = active && bx >= H / 4 && bx < (H + TXo) / 4 && by >= H / 2 && by < (H + TYo) / 2;
-    const int x0 = 4 * bx, y0 = 2 * by, y1 = 2 * by + 1;
+    const bool owned = active && bx >= H / 4 && bx < (H + TXo) / 4 && by >= H / ROWS && by < (H + TYo) / ROWS;
+    const int x0 = 4 * bx, y0 = ROWS * by;
     const float wgt = (float)P.weight, omw1 = 1.0f - (float)P.weight;
-    // bit q: update cell; 8 + q: live (not on the outermost ring); 16 + q: counted and live; 24 + q: owned and in
-    // the domain
-    unsigned fl = 0;
-    f32x2 wl[4], wr[4], wu[4], wd[4], inv[4], rc[4], dv[4];
+    // bit q: update cell; 16 + q: live (not on the outermost ring); 32 + q: counted and live; 48 + q: owned and
+    // in the domain
+    unsigned long long fl = 0;
+    f32x2 wl[NPAIR], wr[NPAIR], wu[NPAIR], wd[NPAIR], inv[NPAIR], rc[NPAIR], dv[NPAIR];
     {
-        float fw[4][8], finv[8];
+        float fw[4][NC], finv[NC];
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
+        for (int q = 0; q < NC; ++q) {
             const int lx = x0 + (q & 3), ly = y0 + (q >> 2);
             const int gx = gx0 + lx, gy = gy0 + ly;
             const bool live = active && lx > 0 && lx < EX - 1 && ly > 0 && ly < EY - 1;
-            if (live) fl |= 1u << (8 + q);
+            if (live) fl |= 1ull << (16 + q);
             float wv[4] = {0.0f, 0.0f, 0.0f, 0.0f};
             finv[q] = 0.0f;
             double den = 0.0, bb = 0.0, pv = 0.0;
@@ -973,11 +977,11 @@ __global__ void __launch_bounds__(NT, 1) k_gsmix_oct(PersistentParams P, PF dbuf
                 const float phi = L.ls.at(gx, gy);
                 bb = L.b.at(gx, gy);
                 pv = __ldcg(&L.x.p[(size_t)gy * L.x.P + gx]);
-                if (owned) fl |= 1u << (24 + q);
+                if (owned) fl |= 1ull << (48 + q);
                 if (phi < 0.0f) {
                     const float f[4] = {L.fu.at(gx, gy), L.fu.at(gx + 1, gy), L.fv.at(gx, gy), L.fv.at(gx, gy + 1)};
                     if (!(f[0] == 0.0f && f[1] == 0.0f && f[2] == 0.0f && f[3] == 0.0f)) {
-                        if (live) fl |= 1u << (16 + q);
+                        if (live) fl |= 1ull << (32 + q);
                         const int ox[4] = {-1, 1, 0, 0}, oy[4] = {0, 0, -1, 1};
 #pragma unroll
                         for (int k = 0; k < 4; ++k) {
@@ -993,7 +997,7 @@ __global__ void __launch_bounds__(NT, 1) k_gsmix_oct(PersistentParams P, PF dbuf
                             }
                         }
                         if (!(fabs(den) < (double)1.0e-6f)) {
-                            if (live) fl |= 1u << q;
+                            if (live) fl |= 1ull << q;
                             finv[q] = (float)(1.0 / den);
                         }
                     }
@@ -1007,18 +1011,20 @@ __global__ void __launch_bounds__(NT, 1) k_gsmix_oct(PersistentParams P, PF dbuf
                 T.den[ly][lx] = den;
             }
         }
-        // pair i = (cells qa, qb): (0, 2), (1, 3), (4, 6), (5, 7)
+        // pair 2 j + k = the cells (i0, j), (i0 + 2, j) with i0 = (k + j) & 1
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            const int qa = (i >> 1) * 4 + (i & 1), qb = qa + 2;
-            wl[i] = x2_pack(fw[0][qa], fw[0][qb]);
-            wr[i] = x2_pack(fw[1][qa], fw[1][qb]);
-            wu[i] = x2_pack(fw[2][qa], fw[2][qb]);
-            wd[i] = x2_pack(fw[3][qa], fw[3][qb]);
-            inv[i] = x2_pack(finv[qa], finv[qb]);
-            rc[i] = 0;
-            dv[i] = 0;
-        }
+        for (int j = 0; j < ROWS; ++j)
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const int i0 = (k + j) & 1, qa = 4 * j + i0, qb = qa + 2, pi = 2 * j + k;
+                wl[pi] = x2_pack(fw[0][qa], fw[0][qb]);
+                wr[pi] = x2_pack(fw[1][qa], fw[1][qb]);
+                wu[pi] = x2_pack(fw[2][qa], fw[2][qb]);
+                wd[pi] = x2_pack(fw[3][qa], fw[3][qb]);
+                inv[pi] = x2_pack(finv[qa], finv[qb]);
+                rc[pi] = 0;
+                dv[pi] = 0;
+            }
     }
     // every word of the correction image starts at 0 (rows' padding included)
     for (int i = threadIdx.x; i < 2 * EY * WP; i += NT) (&T.d[0][0][0])[i] = 0.0f;
@@ -1026,58 +1032,61 @@ __global__ void __launch_bounds__(NT, 1) k_gsmix_oct(PersistentParams P, PF dbuf
     const double cdiv = P.cdiv, factor = P.factor;
     const f32x2 wgt2 = x2_pack(wgt, wgt), omw2 = x2_pack(omw1, omw1), one2 = x2_pack(P.one, P.one);
     // Shared-memory words of the neighbours in other blocks, clamped inside the image for the outermost blocks.
-    const int cl = max(2 * bx - 1, 0), cr = min(2 * bx + 2, W2 - 1), ru = max(y0 - 1, 0), rd = min(y1 + 1, EY - 1);
+    const int cl = max(2 * bx - 1, 0), cr = min(2 * bx + 2, W2 - 1);
+    const int ru = max(y0 - 1, 0), rd = min(y0 + ROWS, EY - 1);
     // most central ring among the block's cells
-    const int bmax = min(min(x0 + 3, EX - 1 - x0), min(y0 + 1, EY - 1 - y0));
-    // k = 0 half-sweep: pairs (c0, c2) and (c5, c7), neighbours from the k = 1 image
-    auto sweep0 = [&]() {
-        float(*D1)[WP] = T.d[1];
-        const f32x2 up = *reinterpret_cast<const f32x2*>(&D1[ru][2 * bx]);
-        const f32x2 dn = *reinterpret_cast<const f32x2*>(&D1[rd][2 * bx]);
-        const float lf = D1[y0][cl], rt = D1[y1][cr];
-        dv[0] = oct_update(rc[0], wl[0], wr[0], wu[0], wd[0], inv[0], omw2, dv[0], x2_pack(lf, x2_lane(dv[1], 0)),
-                           dv[1], up, dv[2], wgt2, one2);
-        dv[3] = oct_update(rc[3], wl[3], wr[3], wu[3], wd[3], inv[3], omw2, dv[3], dv[2],
-                           x2_pack(x2_lane(dv[2], 1), rt), dv[1], dn, wgt2, one2);
-        if (active) {
-            *reinterpret_cast<f32x2*>(&T.d[0][y0][2 * bx]) = dv[0];
-            *reinterpret_cast<f32x2*>(&T.d[0][y1][2 * bx]) = dv[3];
+    const int bmax = min(min(x0 + 3, EX - 1 - x0), min(y0 + ROWS - 1, EY - 1 - y0));
+    // Half-sweep of colour K01: the pairs 2 j + K01 of every row j, neighbours of the other colour: above and
+    // below from the pairs of the rows beside it (shared memory past the block's edge rows), left and right
+    // from the other pair of the same row and one word of shared memory past the block's edge columns.
+    auto sweep = [&](auto kc) {
+        constexpr int K01 = decltype(kc)::value;
+        float(*Do)[WP] = T.d[1 - K01];
+        const f32x2 upw = *reinterpret_cast<const f32x2*>(&Do[ru][2 * bx]);
+        const f32x2 dnw = *reinterpret_cast<const f32x2*>(&Do[rd][2 * bx]);
+        float side[ROWS];
+#pragma unroll
+        for (int j = 0; j < ROWS; ++j) side[j] = ((K01 + j) & 1) ? Do[y0 + j][cr] : Do[y0 + j][cl];
+#pragma unroll
+        for (int j = 0; j < ROWS; ++j) {
+            const int pi = 2 * j + K01, po = 2 * j + (1 - K01);
+            const f32x2 U = j > 0 ? dv[2 * (j - 1) + (1 - K01)] : upw;
+            const f32x2 D = j < ROWS - 1 ? dv[2 * (j + 1) + (1 - K01)] : dnw;
+            f32x2 Lf, Rt;
+            if ((K01 + j) & 1) {  // cells 1 and 3: left (0, 2) in registers, right (2, 4)
+                Lf = dv[po];
+                Rt = x2_pack(x2_lane(dv[po], 1), side[j]);
+            } else {  // cells 0 and 2: left (-1, 1), right (1, 3) in registers
+                Lf = x2_pack(side[j], x2_lane(dv[po], 0));
+                Rt = dv[po];
+            }
+            dv[pi] = oct_update(rc[pi], wl[pi], wr[pi], wu[pi], wd[pi], inv[pi], omw2, dv[pi], Lf, Rt, U, D, wgt2,
+                                one2);
         }
-    };
-    // k = 1 half-sweep: pairs (c1, c3) and (c4, c6), neighbours from the k = 0 image
-    auto sweep1 = [&]() {
-        float(*D0)[WP] = T.d[0];
-        const f32x2 up = *reinterpret_cast<const f32x2*>(&D0[ru][2 * bx]);
-        const f32x2 dn = *reinterpret_cast<const f32x2*>(&D0[rd][2 * bx]);
-        const float rt = D0[y0][cr], lf = D0[y1][cl];
-        dv[1] = oct_update(rc[1], wl[1], wr[1], wu[1], wd[1], inv[1], omw2, dv[1], dv[0],
-                           x2_pack(x2_lane(dv[0], 1), rt), up, dv[3], wgt2, one2);
-        dv[2] = oct_update(rc[2], wl[2], wr[2], wu[2], wd[2], inv[2], omw2, dv[2], x2_pack(lf, x2_lane(dv[3], 0)),
-                           dv[3], dv[0], dn, wgt2, one2);
         if (active) {
-            *reinterpret_cast<f32x2*>(&T.d[1][y0][2 * bx]) = dv[1];
-            *reinterpret_cast<f32x2*>(&T.d[1][y1][2 * bx]) = dv[2];
+#pragma unroll
+            for (int j = 0; j < ROWS; ++j) *reinterpret_cast<f32x2*>(&T.d[K01][y0 + j][2 * bx]) = dv[2 * j + K01];
         }
     };
     // FP64 residual of the live counted cells, rc = f32(cdiv r) on update cells, d = 0, and the CTA's norms over
     // its owned counted cells (fixed order; returned by thread 0).
     auto check = [&]() -> double2 {
         double ar = 0.0, ab = 0.0;
-        float frc[8];
+        float frc[NC];
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
+        for (int q = 0; q < NC; ++q) {
             const int lx = x0 + (q & 3), ly = y0 + (q >> 2);
             const int i = oct_pair(q), ln = oct_lane(q);
             float rcv = 0.0f;
-            if ((fl >> (16 + q)) & 1u) {
+            if ((fl >> (32 + q)) & 1ull) {
                 double sum = (double)x2_lane(wl[i], ln) * T.p[ly][lx - 1];
                 sum = sum + (double)x2_lane(wr[i], ln) * T.p[ly][lx + 1];
                 sum = sum + (double)x2_lane(wu[i], ln) * T.p[ly - 1][lx];
                 sum = sum + (double)x2_lane(wd[i], ln) * T.p[ly + 1][lx];
                 const double bb = T.b[ly][lx];
                 const double r = bb - factor * (T.den[ly][lx] * T.p[ly][lx] - sum);
-                if ((fl >> q) & 1u) rcv = (float)(cdiv * r);
-                if ((fl >> (24 + q)) & 1u) {
+                if ((fl >> q) & 1ull) rcv = (float)(cdiv * r);
+                if ((fl >> (48 + q)) & 1ull) {
                     ar += r * r;
                     ab += bb * bb;
                 }
@@ -1085,16 +1094,19 @@ __global__ void __launch_bounds__(NT, 1) k_gsmix_oct(PersistentParams P, PF dbuf
             frc[q] = rcv;
         }
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            const int qa = (i >> 1) * 4 + (i & 1);
-            rc[i] = x2_pack(frc[qa], frc[qa + 2]);
-            dv[i] = 0;
-        }
+        for (int j = 0; j < ROWS; ++j)
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const int qa = 4 * j + ((k + j) & 1);
+                rc[2 * j + k] = x2_pack(frc[qa], frc[qa + 2]);
+                dv[2 * j + k] = 0;
+            }
         if (active) {
-            *reinterpret_cast<f32x2*>(&T.d[0][y0][2 * bx]) = 0;
-            *reinterpret_cast<f32x2*>(&T.d[1][y0][2 * bx]) = 0;
-            *reinterpret_cast<f32x2*>(&T.d[1][y1][2 * bx]) = 0;
-            *reinterpret_cast<f32x2*>(&T.d[0][y1][2 * bx]) = 0;
+#pragma unroll
+            for (int j = 0; j < ROWS; ++j) {
+                *reinterpret_cast<f32x2*>(&T.d[0][y0 + j][2 * bx]) = 0;
+                *reinterpret_cast<f32x2*>(&T.d[1][y0 + j][2 * bx]) = 0;
+            }
         }
         ar = warp_sum(ar);
         ab = warp_sum(ab);
@@ -1115,6 +1127,8 @@ __global__ void __launch_bounds__(NT, 1) k_gsmix_oct(PersistentParams P, PF dbuf
         __syncthreads();
         return out;
     };
+    const std::integral_constant<int, 0> c0{};
+    const std::integral_constant<int, 1> c1{};
 
     unsigned iters = 0, xch = 0;
     double2 part = check();
@@ -1131,13 +1145,13 @@ __global__ void __launch_bounds__(NT, 1) k_gsmix_oct(PersistentParams P, PF dbuf
             const unsigned kk = min((unsigned)KMAX, todo);
             for (unsigned it = 0; it < kk; ++it) {
                 if (bmax >= 1 + 2 * (int)it) {  // a cell of the block lies in the region still needed
-                    if (base) sweep0();  // red ((x + y) odd) first
-                    else sweep1();
+                    if (base) sweep(c0);  // red ((x + y) odd) first
+                    else sweep(c1);
                 }
                 __syncthreads();
                 if (bmax >= 2 + 2 * (int)it) {
-                    if (base) sweep1();
-                    else sweep0();
+                    if (base) sweep(c1);
+                    else sweep(c0);
                 }
                 __syncthreads();
             }
@@ -1147,8 +1161,8 @@ __global__ void __launch_bounds__(NT, 1) k_gsmix_oct(PersistentParams P, PF dbuf
                 const PF& db = (xch++ & 1) ? P.dbuf2 : dbuf;
                 if (owned) {
 #pragma unroll
-                    for (int q = 0; q < 8; ++q)
-                        if ((fl >> (24 + q)) & 1u)
+                    for (int q = 0; q < NC; ++q)
+                        if ((fl >> (48 + q)) & 1ull)
                             __stcg(&db.p[(size_t)(gy0 + y0 + (q >> 2)) * db.P + gx0 + x0 + (q & 3)],
                                    x2_lane(dv[oct_pair(q)], oct_lane(q)));
                 }
@@ -1163,23 +1177,22 @@ __global__ void __launch_bounds__(NT, 1) k_gsmix_oct(PersistentParams P, PF dbuf
                     }
                 }
                 if (active && !owned) {
-                    float hv[8];
+                    float hv[NC];
 #pragma unroll
-                    for (int q = 0; q < 8; ++q) {
+                    for (int q = 0; q < NC; ++q) {
                         const int gx = gx0 + x0 + (q & 3), gy = gy0 + y0 + (q >> 2);
                         hv[q] = ((unsigned)gx < (unsigned)L.nx && (unsigned)gy < (unsigned)L.ny)
                                     ? __ldcg(&db.p[(size_t)gy * db.P + gx])
                                     : 0.0f;
                     }
 #pragma unroll
-                    for (int i = 0; i < 4; ++i) {
-                        const int qa = (i >> 1) * 4 + (i & 1);
-                        dv[i] = x2_pack(hv[qa], hv[qa + 2]);
-                    }
-                    *reinterpret_cast<f32x2*>(&T.d[0][y0][2 * bx]) = dv[0];
-                    *reinterpret_cast<f32x2*>(&T.d[1][y0][2 * bx]) = dv[1];
-                    *reinterpret_cast<f32x2*>(&T.d[1][y1][2 * bx]) = dv[2];
-                    *reinterpret_cast<f32x2*>(&T.d[0][y1][2 * bx]) = dv[3];
+                    for (int j = 0; j < ROWS; ++j)
+#pragma unroll
+                        for (int k = 0; k < 2; ++k) {
+                            const int qa = 4 * j + ((k + j) & 1);
+                            dv[2 * j + k] = x2_pack(hv[qa], hv[qa + 2]);
+                            *reinterpret_cast<f32x2*>(&T.d[k][y0 + j][2 * bx]) = dv[2 * j + k];
+                        }
                 }
                 __syncthreads();
             }
@@ -1189,11 +1202,11 @@ __global__ void __launch_bounds__(NT, 1) k_gsmix_oct(PersistentParams P, PF dbuf
         // p += d on the owned cells (0 where the reference zeroes p), then exchange p.
         if (owned) {
 #pragma unroll
-            for (int q = 0; q < 8; ++q) {
-                if ((fl >> (24 + q)) & 1u) {
+            for (int q = 0; q < NC; ++q) {
+                if ((fl >> (48 + q)) & 1ull) {
                     const int lx = x0 + (q & 3), ly = y0 + (q >> 2);
                     const double pv =
-                        ((fl >> q) & 1u) ? T.p[ly][lx] + (double)x2_lane(dv[oct_pair(q)], oct_lane(q)) : 0.0;
+                        ((fl >> q) & 1ull) ? T.p[ly][lx] + (double)x2_lane(dv[oct_pair(q)], oct_lane(q)) : 0.0;
                     T.p[ly][lx] = pv;
                     __stcg(&L.x.p[(size_t)(gy0 + ly) * L.x.P + gx0 + lx], pv);
                 }
@@ -1202,16 +1215,16 @@ __global__ void __launch_bounds__(NT, 1) k_gsmix_oct(PersistentParams P, PF dbuf
         ok = grid_barrier(P.barrier, nblocks, P.spin_limit);
         if (!ok) break;
         if (active && !owned) {
-            double hp[8];
+            double hp[NC];
 #pragma unroll
-            for (int q = 0; q < 8; ++q) {
+            for (int q = 0; q < NC; ++q) {
                 const int gx = gx0 + x0 + (q & 3), gy = gy0 + y0 + (q >> 2);
                 hp[q] = ((unsigned)gx < (unsigned)L.nx && (unsigned)gy < (unsigned)L.ny)
                             ? __ldcg(&L.x.p[(size_t)gy * L.x.P + gx])
                             : 0.0;
             }
 #pragma unroll
-            for (int q = 0; q < 8; ++q) T.p[y0 + (q >> 2)][x0 + (q & 3)] = hp[q];
+            for (int q = 0; q < NC; ++q) T.p[y0 + (q >> 2)][x0 + (q & 3)] = hp[q];
         }
         __syncthreads();
         part = check();
@@ -1750,8 +1763,8 @@ inline bool plan_resident(int threads, size_t smem) {
     }
     return state[dev] == 1;
 }
-template <int EX, int EY, int KMAX, int NT>
-inline const void* oct_kernel() { return (const void*)k_gsmix_oct<EX, EY, KMAX, NT>; }
+template <int EX, int EY, int KMAX, int NT, int ROWS>
+inline const void* oct_kernel() { return (const void*)k_gsmix_oct<EX, EY, KMAX, NT, ROWS>; }
 template <int EX, int EY, int KMAX, int NT>
 inline const void* quad_kernel() { return (const void*)k_gsmix_quad<EX, EY, KMAX, NT>; }
 
@@ -1787,7 +1800,7 @@ inline bool try_plan_quad(const SolverWorkspace& ws, int nx, int ny, PersistentP
     return plan_resident<quad_kernel<EX, EY, KMAX, NT>>(NT, p->smem);
 }
 // Plans for the paired-lane form (OctTile: 26 bytes of shared memory per cell).
-template <int EX, int EY, int KMAX, int NT>
+template <int EX, int EY, int KMAX, int NT, int ROWS>
 inline bool try_plan_oct(const SolverWorkspace& ws, int nx, int ny, PersistentPlan* p) {
     const int tx = EX - 4 * KMAX, ty = EY - 4 * KMAX;
     p->kmax = KMAX;
@@ -1795,19 +1808,20 @@ inline bool try_plan_oct(const SolverWorkspace& ws, int nx, int ny, PersistentPl
     p->ty = ty;
     p->tiles_x = (nx + tx - 1) / tx;
     p->tiles_y = (ny + ty - 1) / ty;
-    p->smem = sizeof(OctTile<EX, EY>);
-    p->kernel = (const void*)k_gsmix_oct<EX, EY, KMAX, NT>;
+    p->smem = sizeof(OctTile<EX, EY, ROWS>);
+    p->kernel = (const void*)k_gsmix_oct<EX, EY, KMAX, NT, ROWS>;
     p->threads = NT;
     if (p->smem + 2048 > ws.max_smem) return false;
     if (p->tiles_x * p->tiles_y > ws.num_sms || p->tiles_x * p->tiles_y > ws.max_blocks) return false;
-    return plan_resident<oct_kernel<EX, EY, KMAX, NT>>(NT, p->smem);
+    return plan_resident<oct_kernel<EX, EY, KMAX, NT, ROWS>>(NT, p->smem);
 }
 inline PersistentPlan plan_mix(const SolverWorkspace& ws, int nx, int ny) {
     PersistentPlan p;
-    if (ws.use_reg && (try_plan_oct<80, 48, 4, 480>(ws, nx, ny, &p) ||   // 64 x 32 owned
-                       try_plan_oct<48, 48, 4, 288>(ws, nx, ny, &p) ||   // 32 x 32
-                       try_plan_oct<72, 56, 2, 512>(ws, nx, ny, &p) ||   // 64 x 48
-                       try_plan_oct<40, 40, 4, 224>(ws, nx, ny, &p))) {  // 24 x 24
+    if (ws.use_reg && (try_plan_oct<96, 64, 8, 384, 4>(ws, nx, ny, &p) ||   // 64 x 32 owned, 8 iterations
+                       try_plan_oct<80, 48, 4, 480, 2>(ws, nx, ny, &p) ||   // 64 x 32
+                       try_plan_oct<48, 48, 4, 288, 2>(ws, nx, ny, &p) ||   // 32 x 32
+                       try_plan_oct<72, 56, 2, 512, 2>(ws, nx, ny, &p) ||   // 64 x 48
+                       try_plan_oct<40, 40, 4, 224, 2>(ws, nx, ny, &p))) {  // 24 x 24
         p.ok = true;
         return p;
     }
