@@ -341,7 +341,11 @@ class Sim:
         self._check(self.api.set_transform(self.h, arr))
 
     def set_obstacles(self, obstacles):
-        arr = (SolidObstacle * max(1, len(obstacles)))(*obstacles)
+        """A sequence of SolidObstacle, or a ctypes array of them (passed on without a copy)."""
+        if isinstance(obstacles, C.Array) and len(obstacles) > 0:
+            arr = obstacles
+        else:
+            arr = (SolidObstacle * max(1, len(obstacles)))(*obstacles)
         self._check(self.api.set_obstacles(self.h, arr, len(obstacles)))
 
     def set_local_forces(self, forces):

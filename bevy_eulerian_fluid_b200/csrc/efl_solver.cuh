@@ -1032,7 +1032,10 @@ __global__ void __launch_bounds__(NT, 1) k_gsmix_oct(PersistentParams P, PF dbuf
     const double cdiv = P.cdiv, factor = P.factor;
     const f32x2 wgt2 = x2_pack(wgt, wgt), omw2 = x2_pack(omw1, omw1), one2 = x2_pack(P.one, P.one);
     // Shared-memory words of the neighbours in other blocks, clamped inside the image for the outermost blocks.
-    const int cl = max(2 * bx - 1, 0), cr = min(2 * bx + 2, W2 - 1);
+    // The one-word neighbours left and right of the block come from 8-byte loads of the aligned word pair that
+    // holds them (the left one is the pair's high word, the right one its low word): a warp's side loads are
+    // then consecutive 8-byte words, free of bank conflicts like the pair loads.
+    const int cl = max(2 * bx - 2, 0), cr = min(2 * bx + 2, W2 - 2);
     const int ru = max(y0 - 1, 0), rd = min(y0 + ROWS, EY - 1);
     // most central ring among the block's cells
     const int bmax = min(min(x0 + 3, EX - 1 - x0), min(y0 + ROWS - 1, EY - 1 - y0));
@@ -1046,7 +1049,10 @@ __global__ void __launch_bounds__(NT, 1) k_gsmix_oct(PersistentParams P, PF dbuf
         const f32x2 dnw = *reinterpret_cast<const f32x2*>(&Do[rd][2 * bx]);
         float side[ROWS];
 #pragma unroll
-        for (int j = 0; j < ROWS; ++j) side[j] = ((K01 + j) & 1) ? Do[y0 + j][cr] : Do[y0 + j][cl];
+        for (int j = 0; j < ROWS; ++j) {
+            const f32x2 w2 = *reinterpret_cast<const f32x2*>(&Do[y0 + j][((K01 + j) & 1) ? cr : cl]);
+            side[j] = x2_lane(w2, ((K01 + j) & 1) ? 0 : 1);
+        }
 #pragma unroll
         for (int j = 0; j < ROWS; ++j) {
             const int pi = 2 * j + K01, po = 2 * j + (1 - K01);

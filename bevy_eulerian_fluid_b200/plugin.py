@@ -7,6 +7,7 @@ each simulation step goes through the C ABI of libefl_b200.so.
 """
 from __future__ import annotations
 
+import ctypes as C
 import math
 from dataclasses import dataclass, field
 from enum import Enum, IntEnum
@@ -330,8 +331,39 @@ class RigidBody:
         return o
 
 
-def pack_obstacles(bodies: Sequence[RigidBody]) -> List[capi.SolidObstacle]:
-    return [b.to_obstacle(i) for i, b in enumerate(bodies)]
+_OBSTACLE_DTYPE = np.dtype([("entity_id", "<u4"), ("shape", "<u4"), ("values", "<f4", (6,)),
+                            ("transform", "<f4", (16,)), ("inverse_transform", "<f4", (16,)),
+                            ("linear_velocity", "<f4", (2,)), ("angular_velocity", "<f4"), ("_pad", "<f4")])
+assert _OBSTACLE_DTYPE.itemsize == C.sizeof(capi.SolidObstacle) == 176
+
+
+def pack_obstacles(bodies: Sequence[RigidBody]):
+    """construct_rigid_body_buffer_for_gpu (obstacle.rs:89-160) for every body at once: the same values as
+    RigidBody.to_obstacle (the transforms' inverses from one stacked np.linalg.inv, which inverts each matrix
+    as the single call does), written straight into a ctypes array that set_obstacles passes on as is."""
+    n = len(bodies)
+    if n == 0:
+        return []
+    arr = (capi.SolidObstacle * n)()
+    v = np.frombuffer(arr, dtype=_OBSTACLE_DTYPE)
+    rot = [(math.cos(b.rotation), math.sin(b.rotation), b.position[0], b.position[1]) for b in bodies]
+    c, sn, px, py = np.array(rot, dtype=np.float64).T  # RigidBody.transform, for every body
+    m = np.zeros((n, 4, 4), dtype=np.float64)
+    m[:, 0, 0], m[:, 0, 1], m[:, 1, 0], m[:, 1, 1] = c, -sn, sn, c
+    m[:, 2, 2] = m[:, 3, 3] = 1.0
+    m[:, 0, 3], m[:, 1, 3] = px, py
+    inv = np.linalg.inv(m)
+    v["entity_id"] = np.arange(n, dtype=np.uint32)
+    v["shape"] = [b.collider.shape for b in bodies]
+    vals = np.zeros((n, 6), dtype=np.float64)
+    for i, b in enumerate(bodies):
+        vals[i, :len(b.collider.values)] = b.collider.values
+    v["values"] = vals
+    v["transform"] = m.transpose(0, 2, 1).reshape(n, 16)
+    v["inverse_transform"] = inv.transpose(0, 2, 1).reshape(n, 16)
+    v["linear_velocity"] = [b.linear_velocity for b in bodies]
+    v["angular_velocity"] = [b.angular_velocity for b in bodies]
+    return arr
 
 
 # ---------------------------------------------------------------------------

@@ -51,6 +51,23 @@ def test_obstacle_packing_layout_and_inverse():
     assert (o.linear_velocity[0], o.linear_velocity[1], o.angular_velocity) == pytest.approx((1.0, 2.0, 0.3))
 
 
+def test_batched_packing_equals_per_body_packing():
+    """pack_obstacles (all bodies at once) writes the same bytes as RigidBody.to_obstacle per body, for every
+    collider kind, over a run of the coupled scene's rigid integration."""
+    import copy
+    sc = scenes.coupled(256)
+    bodies = copy.deepcopy(list(sc.bodies)) + [RigidBody(Collider.triangle((0, 0), (3, 0), (0, 2)), (5.0, 6.0), 1.1)]
+    rigid = RigidWorld(bodies, (256, 256), gravity=9.8 * scenes.LENGTH_UNIT, grid_length=1.0 / scenes.LENGTH_UNIT)
+    forces = np.random.default_rng(3).standard_normal((capi.MAX_SOLIDS, 3)).astype(np.float32) * 0.01
+    for _ in range(20):
+        rigid.apply_fluid_forces(forces, sc.dt)
+        rigid.step(sc.dt)
+        a = pack_obstacles(rigid.bodies)
+        b = [x.to_obstacle(i) for i, x in enumerate(rigid.bodies)]
+        assert len(a) == len(b) and bytes(a) == bytes((capi.SolidObstacle * len(b))(*b))
+    assert pack_obstacles([]) == []
+
+
 def test_collider_areas():
     assert Collider.circle(2.0).area() == pytest.approx(math.pi * 4)
     assert Collider.rectangle(2.0, 3.0).area() == pytest.approx(6.0)
