@@ -496,10 +496,11 @@ __global__ void k_residual(LevelT<T> L, float dt, float rho, float dx_scaled) {
     L.r.at(x, y) = residual_at(L, residual_factor<T>(dt, rho, dx_scaled), x, y, &c);
 }
 // restriction.wgsl:10-60 (the fractions on face planes)
+// The coarse cell (x, y) from its four children's residuals r(2x + i, 2y + j) = rij (0 outside the level).
 template <class T>
-EFL_DEV void restrict_cell(const LevelT<T>& F, const LevelT<T>& C, int x, int y) {
+EFL_DEV void restrict_from(const LevelT<T>& F, const LevelT<T>& C, int x, int y, T r00, T r01, T r10, T r11) {
     int fx = 2 * x, fy = 2 * y;
-    T br = T(0.25) * (F.r.ld(fx, fy) + F.r.ld(fx, fy + 1) + F.r.ld(fx + 1, fy) + F.r.ld(fx + 1, fy + 1));
+    T br = T(0.25) * (r00 + r01 + r10 + r11);
     float ph0 = F.ls.ld(fx, fy), ph1 = F.ls.ld(fx, fy + 1), ph2 = F.ls.ld(fx + 1, fy), ph3 = F.ls.ld(fx + 1, fy + 1);
     float pr = ph0;
     if (fabsf(ph1) < fabsf(pr)) pr = ph1;
@@ -514,10 +515,31 @@ EFL_DEV void restrict_cell(const LevelT<T>& F, const LevelT<T>& C, int x, int y)
     C.x.at(x, y) = T(0);
 }
 template <class T>
+EFL_DEV void restrict_cell(const LevelT<T>& F, const LevelT<T>& C, int x, int y) {
+    int fx = 2 * x, fy = 2 * y;
+    restrict_from(F, C, x, y, F.r.ld(fx, fy), F.r.ld(fx, fy + 1), F.r.ld(fx + 1, fy), F.r.ld(fx + 1, fy + 1));
+}
+template <class T>
 __global__ void k_restriction(LevelT<T> F, LevelT<T> C) {
     int x = gx(), y = gy();
     if (x >= C.nx || y >= C.ny) return;
     restrict_cell(F, C, x, y);
+}
+// k_residual then k_restriction in one pass: each coarse cell computes its four children's residuals
+// (residual_at, 0 outside the level, as the residual plane reads there) and restricts them, so the fine
+// residual plane is neither written nor read back.  The same values, in the same order.
+template <class T>
+__global__ void k_residual_restrict(LevelT<T> F, LevelT<T> C, float dt, float rho, float dx_scaled) {
+    int x = gx(), y = gy();
+    if (x >= C.nx || y >= C.ny) return;
+    const T fac = residual_factor<T>(dt, rho, dx_scaled);
+    auto rr = [&](int ax, int ay) -> T {
+        bool c;
+        return (ax < F.nx && ay < F.ny) ? residual_at(F, fac, ax, ay, &c) : T(0);
+    };
+    const int fx = 2 * x, fy = 2 * y;
+    const T r00 = rr(fx, fy), r01 = rr(fx, fy + 1), r10 = rr(fx + 1, fy), r11 = rr(fx + 1, fy + 1);
+    restrict_from(F, C, x, y, r00, r01, r10, r11);
 }
 // prolongation.wgsl:5-34
 template <class T>

@@ -627,8 +627,8 @@ efl_status v_cycle(efl_sim* s, std::vector<LevelT<T>>& mg, size_t i, bool symmet
     if (i == mg.size() - 1) return gs_iterations(s, L, 1.0f, scale, P.mg_coarsest);
     TRY(gs_iterations(s, L, 1.0f, scale, P.mg_pre));
     const LevelT<T>& C = mg[i + 1];
-    k_residual<T><<<grid2d(L.nx, L.ny, kBlock), kBlock, count_launch(), s->stream>>>(L, s->U.dt, s->U.rho, scale * s->U.dx);
-    k_restriction<T><<<grid2d(C.nx, C.ny, kBlock), kBlock, count_launch(), s->stream>>>(L, C);
+    k_residual_restrict<T><<<grid2d(C.nx, C.ny, kBlock), kBlock, count_launch(), s->stream>>>(L, C, s->U.dt, s->U.rho,
+                                                                                          scale * s->U.dx);
     LAUNCH_CHECK();
     TRY(v_cycle(s, mg, i + 1, symmetric));
     k_prolongation<T><<<grid2d(C.nx, C.ny, kBlock), kBlock, count_launch(), s->stream>>>(L, C);
@@ -860,8 +860,8 @@ efl_status mgpcg(efl_sim* s, SolveResult* res) {
             Level L0 = pre[0];
             L0.x = s->alt32;
             const Level& C1 = pre[1];
-            k_residual<float><<<grid2d(nx, ny, kBlock), kBlock, count_launch(), s->stream>>>(L0, s->U.dt, s->U.rho, dxs);
-            k_restriction<float><<<grid2d(C1.nx, C1.ny, kBlock), kBlock, count_launch(), s->stream>>>(L0, C1);
+            k_residual_restrict<float><<<grid2d(C1.nx, C1.ny, kBlock), kBlock, count_launch(), s->stream>>>(
+                L0, C1, s->U.dt, s->U.rho, dxs);
             LAUNCH_CHECK();
             if (tma1) {  // level 1 as at level 0: x (zero) -> alt32_1 red first, coarse correction, back black first
                 const float dxs1 = 2.0f * s->U.dx;  // resolution scale 2 (multi_grid.rs:268-270)
@@ -870,9 +870,8 @@ efl_status mgpcg(efl_sim* s, SolveResult* res) {
                 Level L1 = C1;
                 L1.x = s->alt32_1;
                 const Level& C2 = pre[2];
-                k_residual<float><<<grid2d(C1.nx, C1.ny, kBlock), kBlock, count_launch(), s->stream>>>(
-                    L1, s->U.dt, s->U.rho, dxs1);
-                k_restriction<float><<<grid2d(C2.nx, C2.ny, kBlock), kBlock, count_launch(), s->stream>>>(L1, C2);
+                k_residual_restrict<float><<<grid2d(C2.nx, C2.ny, kBlock), kBlock, count_launch(), s->stream>>>(
+                    L1, C2, s->U.dt, s->U.rho, dxs1);
                 LAUNCH_CHECK();
                 TRY(v_cycle(s, pre, 2, true));
                 k_prolongation<float><<<grid2d(C2.nx, C2.ny, kBlock), kBlock, count_launch(), s->stream>>>(L1, C2);
