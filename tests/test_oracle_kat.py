@@ -258,3 +258,35 @@ def test_learned_fp64_solve_matches_operator_restatement(oracle_api):
     assert np.array_equal(act, act2)
     r = A @ x[act] - b[act].astype(np.float64)
     assert np.linalg.norm(r) <= 1e-9 * np.linalg.norm(b[act].astype(np.float64))
+
+
+def test_hydrostatic_force_on_a_circle(oracle_api):
+    """sample_forces.wgsl / accumulate_forces.wgsl against the analytic buoyancy: with p = G y (y the cell row,
+    growing downwards) the pressure force on a submerged circle of radius R cells is -(integral of grad p over
+    the disc) = (0, -G pi R^2) per unit depth, times dx for the face length (grid frame, y down: the force points
+    up), with no net torque about the centre.  The reference sums the face terms only over cells whose solid id
+    is the body's (within half a cell of the circle, update_solid.wgsl), so the open faces just outside are left
+    out and the discrete force comes out a few per cent low; the bound below allows 6 %."""
+    dx = float(np.float32(1) / np.float32(10))
+    G = 1000.0
+    for n, R in ((128, 20.0), (256, 40.0), (256, 80.0)):
+        s = _sim(oracle_api, n)
+        body = RigidBody(Collider.circle(R), (0.0, 0.0), 0.0, kind=RigidBodyKind.Static)
+        s.set_obstacles([body.to_obstacle(0)])
+        s.run_stage(capi.STAGE_UPDATE_SOLID, scenes.DT)
+        yy = np.mgrid[0:n, 0:n][0].astype(np.float32)
+        s.set(capi.FIELD_PRESSURE, (np.float32(G) * yy).astype(np.float32))
+        s.run_stage(capi.STAGE_SOLID_FORCES, scenes.DT)
+        fx, fy, tq = (float(v) for v in s.solid_forces()[0])
+        want = -G * math.pi * R * R * dx
+        assert 0.94 * abs(want) <= -fy <= 1.0 * abs(want), (R, fy, want)
+        assert abs(fx) <= 1e-4 * abs(want) and abs(tq) <= 1e-4 * abs(want) * R * dx, (R, fx, tq)
+        # the fixed-point bins (x10, truncated per cell) are what the forces are read from
+        bins = s.force_bins()
+        assert abs(bins[1][0] * 0.1 - fy) <= 0.1
+        # a uniform pressure exerts no net force: the face terms telescope around the body
+        s.set(capi.FIELD_PRESSURE, np.full((n, n), 500.0, np.float32))
+        s.run_stage(capi.STAGE_SOLID_FORCES, scenes.DT)
+        f0 = s.solid_forces()[0]
+        assert abs(float(f0[0])) <= 1e-3 * abs(want) and abs(float(f0[1])) <= 1e-3 * abs(want), (R, f0)
+        s.close()
