@@ -924,9 +924,19 @@ template <int EX, int EY, int ROWS>
 struct OctTile {
     static constexpr int W2 = EX / 2, W4 = EX / 4, NB = (EX / 4) * (EY / ROWS);
     static constexpr int WP = W2 % 16 == 4 ? W2 : W2 + ((4 - W2 % 16) + 16) % 16;  // row stride of d (words)
-    double p[EY][EX];
-    double b[EY][EX];
-    double den[EY][EX];
+    // The FP64 planes hold cell (x, y) at y * RS + (x & 3) * W4 + (x >> 2): the threads of a warp (consecutive
+    // blocks) reading the same cell of their blocks read consecutive words, and RS puts the next row of
+    // blocks (ROWS rows down) 16 banks over, so a half-warp that spans two block rows does not conflict.
+    static constexpr int rs_pad() {
+        int pad = 0;
+        while ((ROWS * (4 * W4 + pad)) % 16 != 8 && pad < 16) ++pad;
+        return pad;
+    }
+    static constexpr int RS = 4 * W4 + rs_pad();
+    EFL_DEV static int ix(int y, int x) { return y * RS + (x & 3) * W4 + (x >> 2); }
+    double p[EY * RS];
+    double b[EY * RS];
+    double den[EY * RS];
     float d[2][EY][WP];  // [k][y][x / 2], k = (x + y) & 1 in the image (k = 0: the tile's base colour)
 };
 
@@ -957,6 +967,9 @@ __global__ void __launch_bounds__(NT, 1) k_gsmix_oct(PersistentParams P, PF dbuf
     const int base = (gx0 + gy0) & 1;  // colour of the k = 0 cells (1 = red, (x + y) odd)
     const bool owned = active && bx >= H / 4 && bx < (H + TXo) / 4 && by >= H / ROWS && by < (H + TYo) / ROWS;
     const int x0 = 4 * bx, y0 = ROWS * by;
+    // FP64 plane index of the cell (x0 + i, y0 + j), i in -1 .. 4 and j in -1 .. ROWS (constants once unrolled)
+    const int pbase = y0 * Tile::RS + bx;
+    auto pix = [&](int i, int j) { return pbase + j * Tile::RS + (i & 3) * W4 + (i >> 2); };
     const float wgt = (float)P.weight, omw1 = 1.0f - (float)P.weight;
     // bit q: update cell; 16 + q: live (not on the outermost ring); 32 + q: counted and live; 48 + q: owned and
     // in the domain
@@ -1006,9 +1019,9 @@ __global__ void __launch_bounds__(NT, 1) k_gsmix_oct(PersistentParams P, PF dbuf
 #pragma unroll
             for (int k = 0; k < 4; ++k) fw[k][q] = wv[k];
             if (active) {
-                T.p[ly][lx] = pv;
-                T.b[ly][lx] = bb;
-                T.den[ly][lx] = den;
+                T.p[pix(q & 3, q >> 2)] = pv;
+                T.b[pix(q & 3, q >> 2)] = bb;
+                T.den[pix(q & 3, q >> 2)] = den;
             }
         }
         // pair 2 j + k = the cells (i0, j), (i0 + 2, j) with i0 = (k + j) & 1
@@ -1085,12 +1098,13 @@ __global__ void __launch_bounds__(NT, 1) k_gsmix_oct(PersistentParams P, PF dbuf
             const int i = oct_pair(q), ln = oct_lane(q);
             float rcv = 0.0f;
             if ((fl >> (32 + q)) & 1ull) {
-                double sum = (double)x2_lane(wl[i], ln) * T.p[ly][lx - 1];
-                sum = sum + (double)x2_lane(wr[i], ln) * T.p[ly][lx + 1];
-                sum = sum + (double)x2_lane(wu[i], ln) * T.p[ly - 1][lx];
-                sum = sum + (double)x2_lane(wd[i], ln) * T.p[ly + 1][lx];
-                const double bb = T.b[ly][lx];
-                const double r = bb - factor * (T.den[ly][lx] * T.p[ly][lx] - sum);
+                const int ci = q & 3, cj = q >> 2;
+                double sum = (double)x2_lane(wl[i], ln) * T.p[pix(ci - 1, cj)];
+                sum = sum + (double)x2_lane(wr[i], ln) * T.p[pix(ci + 1, cj)];
+                sum = sum + (double)x2_lane(wu[i], ln) * T.p[pix(ci, cj - 1)];
+                sum = sum + (double)x2_lane(wd[i], ln) * T.p[pix(ci, cj + 1)];
+                const double bb = T.b[pix(ci, cj)];
+                const double r = bb - factor * (T.den[pix(ci, cj)] * T.p[pix(ci, cj)] - sum);
                 if ((fl >> q) & 1ull) rcv = (float)(cdiv * r);
                 if ((fl >> (48 + q)) & 1ull) {
                     ar += r * r;
@@ -1212,8 +1226,8 @@ __global__ void __launch_bounds__(NT, 1) k_gsmix_oct(PersistentParams P, PF dbuf
                 if ((fl >> (48 + q)) & 1ull) {
                     const int lx = x0 + (q & 3), ly = y0 + (q >> 2);
                     const double pv =
-                        ((fl >> q) & 1ull) ? T.p[ly][lx] + (double)x2_lane(dv[oct_pair(q)], oct_lane(q)) : 0.0;
-                    T.p[ly][lx] = pv;
+                        ((fl >> q) & 1ull) ? T.p[pix(q & 3, q >> 2)] + (double)x2_lane(dv[oct_pair(q)], oct_lane(q)) : 0.0;
+                    T.p[pix(q & 3, q >> 2)] = pv;
                     __stcg(&L.x.p[(size_t)(gy0 + ly) * L.x.P + gx0 + lx], pv);
                 }
             }
@@ -1230,7 +1244,7 @@ __global__ void __launch_bounds__(NT, 1) k_gsmix_oct(PersistentParams P, PF dbuf
                             : 0.0;
             }
 #pragma unroll
-            for (int q = 0; q < NC; ++q) T.p[y0 + (q >> 2)][x0 + (q & 3)] = hp[q];
+            for (int q = 0; q < NC; ++q) T.p[pix(q & 3, q >> 2)] = hp[q];
         }
         __syncthreads();
         part = check();
