@@ -68,7 +68,7 @@ def test_unet_forward_matches_oracle(gpu_api):
     assert np.array_equal(net.get_params(), params)
     pred = net.forward(feats)
     ref = unet_ref.Net(params).forward(feats)
-    assert _rel(pred, ref) < 1e-2
+    assert _rel(pred, ref) < 2e-3  # 1.6e-4 measured
 
 
 @pytest.mark.gpu
@@ -82,12 +82,12 @@ def test_unet_wide_rows_match_oracle(gpu_api):
     net = capi.UNet(gpu_api, 512, 128, seed=5)
     net.set_params(params)
     ref = unet_ref.Net(params)
-    assert _rel(net.forward(feats), ref.forward(feats)) < 1e-2
+    assert _rel(net.forward(feats), ref.forward(feats)) < 1e-2  # 3.1e-3 measured
     loss, g = net.gradients(feats, target, mask)
     rloss, rg = ref.backward(target, mask)
-    assert loss == pytest.approx(rloss, rel=1e-2)
+    assert loss == pytest.approx(rloss, rel=1e-4)  # 6.9e-6 measured
     cos = float(g.astype(np.float64) @ rg / (np.linalg.norm(g) * np.linalg.norm(rg)))
-    assert cos > 0.998 and _rel(g, rg) < 6e-2, (cos, _rel(g, rg))
+    assert cos > 0.9999 and _rel(g, rg) < 5e-3, (cos, _rel(g, rg))  # 1 - 7e-8 and 7.6e-4 measured
 
 
 @pytest.mark.gpu
@@ -118,7 +118,7 @@ def test_unet_gradients_match_oracle(gpu_api, seed):
     ref = unet_ref.Net(params)
     ref.forward(feats)
     rloss, rg = ref.backward(target, mask)
-    assert loss == pytest.approx(rloss, rel=1e-2)
+    assert loss == pytest.approx(rloss, rel=2e-3)  # at most 2.6e-4 measured
     off = 0
     for i, (ci, co, _) in enumerate(unet_ref.SPEC):
         nw = 9 * ci * co
