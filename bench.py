@@ -1,6 +1,6 @@
 """Benchmark of the per-step fluid hot path (one JSON line on rank 0).
 
-Workload (configs[1] of the reference benchmark list): coupled_512 -- a
+Workload (the reference benchmark's headline scene): coupled_512 -- a
 512x512 MAC grid, water in the lower 40 %, 24 rigid bodies drawn from seed
 0xC2 (6 circles, rectangles, capsules, triangles), jump-flooding level-set
 reinitialisation every step, and a pressure solve that iterates red-black
@@ -595,12 +595,15 @@ def batch_leg(api, torch, args, world, rank, local, dist):
 
     warm_b = max(args.warmup, 5)  # the tile autotuner tries its four configurations on the first four solves
 
+    info = {}
+
     def batched(net=None):
         bt = capi.Batch(api, [cfgs[i] for i in shard])
         for j, i in enumerate(shard):
             bt[j].set_sources(bs.scenes[i].oneshot, True)
         if net is not None:
             bt.attach_unet(net)
+            info["canvas"] = bt.unet_canvas()
         bstream = torch.cuda.ExternalStream(bt[0].stream(), device=f"cuda:{local}")
         bt.step(dt)
         k = 0
@@ -694,7 +697,9 @@ def batch_leg(api, torch, args, world, rank, local, dist):
                          "ms_per_step": t[4] / steps, "pressure_solve_ms_per_step": t[5] / steps,
                          "pressure_iterations": {"max": max(lw[2]), "mean": round(sum(lw[2]) / len(lw[2]), 1)},
                          "network": "pretrained weights (bevy_eulerian_fluid_b200/weights), attached with "
-                                    "efl_batch_attach_unet: one forward per simulation inside the batch step"}
+                                    "efl_batch_attach_unet: inside the batch step, one forward pass over a canvas "
+                                    "that packs all simulations' grids coarsened 8x "
+                                    f"({info.get('canvas', (0, 0))[0]} x {info.get('canvas', (0, 0))[1]})"}
                         if lw else None),
             "gpu_launches_batched": int(launches_b),
             "l2": "not flushed: the batch's working set (GBs) exceeds L2",

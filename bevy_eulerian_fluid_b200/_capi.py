@@ -191,6 +191,8 @@ SIGNATURES = {
     "unet_time_forward": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(C.c_float)]),
     "unet_set_coarsening": (C.c_int, [C.c_void_p, C.c_uint32]),
     "batch_attach_unet": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32]),
+    "batch_unet_canvas": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+    "canvas_pack": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "slab_create": (C.c_int, [C.POINTER(SlabDesc), C.POINTER(C.c_void_p)]),
     "slab_destroy": (C.c_int, [C.c_void_p]),
     "slab_load": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
@@ -208,7 +210,8 @@ PRODUCT_ONLY = {"abi_version", "default_config", "field_device_ptr", "stream", "
                 "projection_ms", "set_graph_capture", "set_wait_limits", "set_rigid_bodies", "get_rigid_bodies",
                 "unet_create", "unet_destroy", "unet_last_error", "unet_num_params", "unet_get_params",
                 "unet_set_params", "unet_forward", "unet_gradients", "unet_attach", "unet_train_step",
-                "unet_time_forward", "unet_set_coarsening", "batch_attach_unet", "slab_create", "slab_destroy",
+                "unet_time_forward", "unet_set_coarsening", "batch_attach_unet", "batch_unet_canvas", "canvas_pack",
+                "slab_create", "slab_destroy",
                 "slab_load", "slab_halo", "slab_prepare", "slab_residual", "slab_sweep", "slab_apply", "slab_read"}
 
 
@@ -259,6 +262,19 @@ def load(path: str = LIB_PATH) -> Api:
     if path == LIB_PATH:
         _API = api
     return api
+
+
+def canvas_pack(api: Api, sizes):
+    """The canvas layout of a batch's network forward (efl_canvas_pack; host only): sizes = [(w, h), ...] in
+    pixels, multiples of 8 -> ([(x, y) origin per image], width, height)."""
+    n = len(sizes)
+    wh = (C.c_int32 * max(1, 2 * n))(*[v for s in sizes for v in s])
+    org = (C.c_int32 * max(1, 2 * n))()
+    w, h = C.c_int32(), C.c_int32()
+    st = api.canvas_pack(wh, n, org, C.byref(w), C.byref(h))
+    if st != OK:
+        raise EflError(st, "canvas_pack: sizes must be positive multiples of 8")
+    return [(org[2 * i], org[2 * i + 1]) for i in range(n)], w.value, h.value
 
 
 def default_config(nx: int, ny: int) -> Config:
@@ -542,9 +558,16 @@ class Batch:
         return (tx.value, ty.value, k.value), list(cost)
 
     def attach_unet(self, net: "UNet", warm_start: bool = True):
-        """Warm-starts every simulation's solve with the network (one forward workspace per simulation)."""
+        """Warm-starts every simulation's solve with the network: one forward over a canvas of all the
+        simulations' coarse grids where the coarsening allows, else one forward workspace per simulation."""
         self._check(self.api.batch_attach_unet(self.h, net.h if warm_start else None,
                                                UNET_WARM_START if warm_start else 0))
+
+    def unet_canvas(self):
+        """(width, height) of the canvas of the network's batched forward, (0, 0) without one."""
+        w, h = C.c_int32(), C.c_int32()
+        self._check(self.api.batch_unet_canvas(self.h, C.byref(w), C.byref(h)))
+        return w.value, h.value
 
     def set_wait_limits(self, barrier_polls: int = 0):
         """Grid-barrier polls of the batched solve before it gives up (0 = the default)."""

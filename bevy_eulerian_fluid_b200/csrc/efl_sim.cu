@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -339,6 +340,16 @@ bool fim_tiled_ready() {
     return state[dev] == 1;
 }
 
+// Which FIM form runs: EFL_FIM_TILED=1 the temporally blocked kernel at every size, =0 the per-phase launches at
+// every size, unset (or anything else) the size rule in st_reinit.  Both forms give bit-identical level sets.
+int fim_tiled_override() {
+    static const int v = [] {
+        const char* e = std::getenv("EFL_FIM_TILED");
+        return e && e[0] == '1' && !e[1] ? 1 : e && e[0] == '0' && !e[1] ? 0 : -1;
+    }();
+    return v;
+}
+
 efl_status st_reinit(efl_sim* s) {  // reinitialize_levelset.rs:162-243
     Dom d = s->dom();
     dim3 g = grid2d(d.nx, d.ny, kBlock);
@@ -356,7 +367,8 @@ efl_status st_reinit(efl_sim* s) {  // reinitialize_levelset.rs:162-243
         const int tx = (d.nx + FIM_TILE - 1) / FIM_TILE, ty = (d.ny + FIM_TILE - 1) / FIM_TILE;
         // The tiled form pays where the grid is large and the interface a small part of it (C3: 4096^2);
         // on small grids the per-phase launches are cheaper (the tiles hold the interface almost everywhere).
-        const bool tiled = tx * ty >= 4 * s->solver.num_sms && fim_tiled_ready();
+        const int force = fim_tiled_override();
+        const bool tiled = (force < 0 ? tx * ty >= 4 * s->solver.num_sms : force == 1) && fim_tiled_ready();
         if (tiled) CU(cudaMemsetAsync(s->d_fimtiles, 0, (size_t)tx * ty * sizeof(unsigned), s->stream));
         k_fim_active<<<g, kBlock, count_launch(), s->stream>>>(s->lab0, s->lab, d, tiled ? s->d_fimtiles : nullptr,
                                                                 tx);
@@ -952,40 +964,63 @@ efl_status check_device_errors(efl_sim* s) {
 
 // Learned warm start: the features of the system about to be solved, and
 // (when warm-starting) x += sigma * prediction on the counted cells.
-efl_status unet_before_solve(efl_sim* s) {
+UnetFeatureArgs unet_feature_args(const efl_sim* s) {
+    const Level64& L = s->mg64[0];
+    const double dx = (double)s->U.dx;
+    return UnetFeatureArgs{s->ls0, s->fu, s->fv, L.x, L.b, dx * dx * (double)s->U.rho / (double)s->U.dt,
+                           (double)s->U.dt / (double)s->U.rho / dx / dx, s->nx, s->ny};
+}
+
+// The warm start in two halves around the network's forward pass: the features (into x0, row pitch cs
+// coarse pixels; the workspace's own X0 when x0 is null), then the prediction (read from outc, pitch cs)
+// added to the iterate and the guard that keeps it only where it lowers the residual.
+efl_status unet_features(efl_sim* s, bf16* x0, int cs) {
     UNet& n = s->unet_view ? *s->unet_view : s->unet->net;
     const int f = s->unet->net.coarse;
     if (n.coarse != f)
         return set_err(s, EFL_ERR_STATE, "the network's coarsening changed after efl_batch_attach_unet: attach again");
-    const Level64& L = s->mg64[0];
     const dim3 g = grid2d(s->nx, s->ny, kBlock);
-    const double dx = (double)s->U.dx;
-    UnetFeatureArgs a{s->ls0, s->fu, s->fv, L.x, L.b, dx * dx * (double)s->U.rho / (double)s->U.dt,
-                      (double)s->U.dt / (double)s->U.rho / dx / dx, s->nx, s->ny};
+    const UnetFeatureArgs a = unet_feature_args(s);
     k_unet_residual<<<g, kBlock, count_launch(), s->stream>>>(a, n.res32, n.prev32, n.mask, n.lpart);
     k_unet_sigma<<<1, 32, count_launch(), s->stream>>>(n.lpart, (int)(g.x * g.y), n.sigma);
     if (f > 1) {
         k_unet_features_coarse<<<grid2d(s->nx / f, s->ny / f, kBlock), kBlock, count_launch(), s->stream>>>(
-            n.res32, a, n.mask, n.sigma, f, n.X0, n.maskc);
+            n.res32, a, n.mask, n.sigma, f, x0 ? x0 : n.X0, x0 ? cs : s->nx / f, n.maskc);
     } else {
         k_unet_features<<<g, kBlock, count_launch(), s->stream>>>(n.res32, a, n.mask, n.sigma, n.X0);
     }
-    if (s->unet_flags & EFL_UNET_WARM_START) {
-        unet_forward(n, s->ny / f, s->nx / f, s->stream);
-        if (f > 1)
-            k_unet_warm_coarse<<<g, kBlock, count_launch(), s->stream>>>(L.x, n.out, n.mask, n.sigma, s->nx, s->ny, f);
-        else
-            k_unet_warm<<<g, kBlock, count_launch(), s->stream>>>(L.x, n.out, n.mask, n.sigma, s->nx, s->ny);
-        // The guard: kept only if it lowers the block-summed residual (block = the coarsening, at least 8).
-        const int gb = std::max(8, f);
-        const dim3 gg = grid2d((s->nx + gb - 1) / gb, (s->ny + gb - 1) / gb, kBlock);
-        const int nb = (int)(gg.x * gg.y);
-        k_unet_block_residual<<<gg, kBlock, count_launch(), s->stream>>>(a, n.prev32, gb, n.epart);
-        k_unet_guard<<<1, 32, count_launch(), s->stream>>>(n.epart, nb, (double*)(n.epart + nb));
-        k_unet_guard_restore<<<g, kBlock, count_launch(), s->stream>>>(L.x, n.prev32, n.mask,
-                                                                        (double*)(n.epart + nb), s->nx, s->ny);
-    }
     LAUNCH_CHECK();
+    return EFL_OK;
+}
+efl_status unet_apply(efl_sim* s, const float* outc, int cs) {
+    UNet& n = s->unet_view ? *s->unet_view : s->unet->net;
+    const int f = n.coarse;
+    const Level64& L = s->mg64[0];
+    const dim3 g = grid2d(s->nx, s->ny, kBlock);
+    if (f > 1)
+        k_unet_warm_coarse<<<g, kBlock, count_launch(), s->stream>>>(L.x, outc ? outc : n.out, outc ? cs : s->nx / f,
+                                                                      n.mask, n.sigma, s->nx, s->ny, f);
+    else
+        k_unet_warm<<<g, kBlock, count_launch(), s->stream>>>(L.x, n.out, n.mask, n.sigma, s->nx, s->ny);
+    // The guard: kept only if it lowers the block-summed residual (block = the coarsening, at least 8).
+    const int gb = std::max(8, f);
+    const dim3 gg = grid2d((s->nx + gb - 1) / gb, (s->ny + gb - 1) / gb, kBlock);
+    const int nb = (int)(gg.x * gg.y);
+    const UnetFeatureArgs a = unet_feature_args(s);
+    k_unet_block_residual<<<gg, kBlock, count_launch(), s->stream>>>(a, n.prev32, gb, n.epart);
+    k_unet_guard<<<1, 32, count_launch(), s->stream>>>(n.epart, nb, (double*)(n.epart + nb));
+    k_unet_guard_restore<<<g, kBlock, count_launch(), s->stream>>>(L.x, n.prev32, n.mask, (double*)(n.epart + nb),
+                                                                    s->nx, s->ny);
+    LAUNCH_CHECK();
+    return EFL_OK;
+}
+efl_status unet_before_solve(efl_sim* s) {
+    TRY(unet_features(s, nullptr, 0));
+    if (s->unet_flags & EFL_UNET_WARM_START) {
+        UNet& n = s->unet_view ? *s->unet_view : s->unet->net;
+        unet_forward(n, s->ny / n.coarse, s->nx / n.coarse, s->stream);
+        TRY(unet_apply(s, nullptr, 0));
+    }
     return EFL_OK;
 }
 efl_status unet_after_solve(efl_sim* s) {
@@ -2098,6 +2133,15 @@ struct efl_batch {
     std::vector<cudaStream_t> work;
     std::vector<cudaEvent_t> ev_join;
     cudaEvent_t ev_fork = nullptr;
+    // The network's forward pass for all simulations at once (efl_batch_attach_unet with a coarsening f > 1):
+    // each simulation's coarse features sit in a rectangle of one canvas, 8-pixel gaps around them, and one
+    // launch per layer covers the canvas.
+    UNet* canvas = nullptr;
+    const efl_unet* canvas_net = nullptr;  // the network the canvas was set up for
+    unsigned char* d_gaps = nullptr;       // the four levels' masks (1 inside a rectangle), one allocation
+    const unsigned char* gaps[4] = {};
+    int cw = 0, ch = 0;                    // canvas width and height, coarse pixels
+    std::vector<int2> corigin;             // per simulation: its rectangle's origin
 };
 
 namespace {
@@ -2127,10 +2171,24 @@ efl_status batch_err(efl_batch* b, efl_status st, const std::string& m) {
     return st;
 }
 
+void canvas_free(efl_batch* b) {
+    if (b->canvas) {
+        cudaFree(b->canvas->arena);
+        delete b->canvas;
+    }
+    cudaFree(b->d_gaps);
+    b->canvas = nullptr;
+    b->canvas_net = nullptr;
+    b->d_gaps = nullptr;
+    b->cw = b->ch = 0;
+    b->corigin.clear();
+}
+
 void batch_free(efl_batch* b) {
     if (!b) return;
     cudaSetDevice(b->device);
     if (b->stream) cudaStreamSynchronize(b->stream);
+    canvas_free(b);
     for (efl_sim* s : b->sims) efl_destroy(s);
     cudaFree(b->d_sims);
     cudaFree(b->d_tiles);
@@ -2390,6 +2448,95 @@ efl_status efl_batch_tiles(const efl_batch* b, int32_t* tx, int32_t* ty, int32_t
     return EFL_OK;
 }
 
+// Shelf packing of n images (wh[2 i] x wh[2 i + 1] pixels, multiples of 8) into one canvas: the width is the
+// smallest multiple of 512 that holds the widest image (so that the three finer levels are multiples of 128
+// wide); tallest images first, left to right with 8-pixel gaps, a new shelf 8 pixels below the tallest image
+// of the last one.  Every rectangle starts on a multiple of 8, and none touches another.
+efl_status efl_canvas_pack(const int32_t* wh, uint32_t n, int32_t* origins, int32_t* width, int32_t* height) {
+    if (!wh || !origins || !width || !height) return EFL_ERR_INVALID_ARGUMENT;
+    int maxw = 8;
+    for (uint32_t i = 0; i < n; ++i) {
+        if (wh[2 * i] <= 0 || wh[2 * i + 1] <= 0 || wh[2 * i] % 8 || wh[2 * i + 1] % 8 || wh[2 * i] > (1 << 16) ||
+            wh[2 * i + 1] > (1 << 16))
+            return EFL_ERR_INVALID_ARGUMENT;
+        maxw = std::max(maxw, (int)wh[2 * i]);
+    }
+    const int W = (maxw + 511) / 512 * 512;
+    std::vector<uint32_t> order(n);
+    for (uint32_t i = 0; i < n; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t c) {
+        return wh[2 * a + 1] != wh[2 * c + 1] ? wh[2 * a + 1] > wh[2 * c + 1] : wh[2 * a] > wh[2 * c];
+    });
+    long long x = 0, y = 0, shelf = 0;
+    for (uint32_t i : order) {
+        const int w = wh[2 * i], h = wh[2 * i + 1];
+        if (x > 0 && x + w > W) {
+            y += shelf + 8;
+            x = 0;
+            shelf = 0;
+        }
+        if (y + h > (1 << 20)) return EFL_ERR_INVALID_ARGUMENT;
+        origins[2 * i] = (int32_t)x;
+        origins[2 * i + 1] = (int32_t)y;
+        x += w + 8;
+        shelf = std::max<long long>(shelf, h);
+    }
+    *width = W;
+    *height = (int32_t)(y + shelf);
+    return EFL_OK;
+}
+
+// Lays the batch's simulations out on a canvas for the network's forward pass (see efl_canvas_pack) and
+// allocates its activations and gap masks.  Leaves the batch without a canvas (each simulation's forward
+// then runs on its own) where the coarsening is 1 or a simulation's coarse grid is not a multiple of 8 in
+// both directions.
+efl_status canvas_setup(efl_batch* b, const efl_unet* u) {
+    canvas_free(b);
+    b->gc.clear();  // captured stages before the solve may hold the previous canvas
+    const int f = u->net.coarse;
+    const size_t n = b->sims.size();
+    if (f <= 1 || n == 0) return EFL_OK;
+    std::vector<int32_t> wh(2 * n), org(2 * n);
+    for (size_t i = 0; i < n; ++i) {
+        const efl_sim* s = b->sims[i];
+        if (s->nx % (8 * f) || s->ny % (8 * f)) return EFL_OK;
+        wh[2 * i] = s->nx / f;
+        wh[2 * i + 1] = s->ny / f;
+    }
+    int32_t W = 0, H = 0;
+    if (efl_canvas_pack(wh.data(), (uint32_t)n, org.data(), &W, &H) != EFL_OK) return EFL_OK;
+    UNet* v = new UNet();
+    if (unet_alloc_forward(*v, u->net, H * f, W * f, false) != cudaSuccess) {
+        if (v->arena) cudaFree(v->arena);
+        delete v;
+        return EFL_ERR_OUT_OF_MEMORY;
+    }
+    b->canvas = v;
+    size_t off[4], total = 0;
+    for (int l = 0; l < 4; ++l) {
+        off[l] = total;
+        total += up256((size_t)(W >> l) * (H >> l));
+    }
+    std::vector<unsigned char> m(total, 0);
+    for (size_t i = 0; i < n; ++i)
+        for (int l = 0; l < 4; ++l) {
+            const int x0 = org[2 * i] >> l, y0 = org[2 * i + 1] >> l, w = wh[2 * i] >> l, h = wh[2 * i + 1] >> l;
+            for (int y = y0; y < y0 + h; ++y) std::memset(&m[off[l] + (size_t)y * (W >> l) + x0], 1, (size_t)w);
+        }
+    if (cudaMalloc(&b->d_gaps, total) != cudaSuccess ||
+        cudaMemcpy(b->d_gaps, m.data(), total, cudaMemcpyHostToDevice) != cudaSuccess) {
+        canvas_free(b);
+        return EFL_ERR_OUT_OF_MEMORY;
+    }
+    for (int l = 0; l < 4; ++l) b->gaps[l] = b->d_gaps + off[l];
+    b->cw = W;
+    b->ch = H;
+    b->corigin.resize(n);
+    for (size_t i = 0; i < n; ++i) b->corigin[i] = make_int2(org[2 * i], org[2 * i + 1]);
+    b->canvas_net = u;
+    return EFL_OK;
+}
+
 efl_status efl_batch_attach_unet(efl_batch* b, efl_unet* u, uint32_t flags) {
     if (!b) return batch_err(nullptr, EFL_ERR_INVALID_ARGUMENT, "null batch");
     if (flags & ~(uint32_t)EFL_UNET_WARM_START)
@@ -2416,6 +2563,19 @@ efl_status efl_batch_attach_unet(efl_batch* b, efl_unet* u, uint32_t flags) {
             s->unet_view = v;
         }
     }
+    if (!flags || !u) {
+        canvas_free(b);
+        b->gc.clear();
+        return EFL_OK;
+    }
+    const efl_status cs = canvas_setup(b, u);
+    return cs == EFL_OK ? EFL_OK : batch_err(b, cs, "network canvas allocation failed");
+}
+
+efl_status efl_batch_unet_canvas(const efl_batch* b, int32_t* width, int32_t* height) {
+    if (!b || !width || !height) return set_err(nullptr, EFL_ERR_INVALID_ARGUMENT, "null argument");
+    *width = b->canvas ? b->cw : 0;
+    *height = b->canvas ? b->ch : 0;
     return EFL_OK;
 }
 
@@ -2462,13 +2622,28 @@ efl_status efl_batch_step(efl_batch* b, float dt, efl_step_stats* stats) {
             sig_pre = fnv(sig_pre, segment_sig(s, SEG_PRE));
             sig_post = fnv(sig_post, segment_sig(s, SEG_POST));
         }
+        // With a canvas, the warm start's features of every simulation go into it, one forward pass over the
+        // canvas follows on the batch stream, and each simulation then takes its prediction from its rectangle.
+        auto on_canvas = [&](const efl_sim* s) {
+            return b->canvas && s->unet == b->canvas_net && (s->unet_flags & EFL_UNET_WARM_START);
+        };
+        auto at = [&](size_t i, auto* base) { return base + ((size_t)b->corigin[i].y * b->cw + b->corigin[i].x) * 16; };
+        bool any_canvas = false;
+        for (const efl_sim* s : b->sims) any_canvas = any_canvas || on_canvas(s);
+        sig_pre = fnv(sig_pre, (uint64_t)(uintptr_t)b->canvas + (any_canvas ? 1 : 0));
         efl_status st = run_segment(b->gc, b->stream, sig_pre | 1, SEG_PRE, [&]() -> efl_status {
-            return batch_fanout(b, [&](size_t, efl_sim* s) -> efl_status {
+            TRY(batch_fanout(b, [&](size_t i, efl_sim* s) -> efl_status {
                 TRY(run_stages(s, EFL_STAGE_UPDATE_SOLID, EFL_STAGE_DIVERGENCE, nullptr));
                 const Level64& L = s->mg64[0];
                 k_widen<<<grid2d(s->nx, s->ny, kBlock), kBlock, count_launch(), s->stream>>>(s->p0, s->div, L.x, L.b);
+                if (on_canvas(s)) return unet_features(s, at(i, b->canvas->X0), b->cw);
                 if (s->unet && (s->unet_flags & EFL_UNET_WARM_START)) TRY(unet_before_solve(s));
                 return EFL_OK;
+            }));
+            if (!any_canvas) return EFL_OK;
+            unet_forward(*b->canvas, b->ch, b->cw, b->stream, b->gaps);
+            return batch_fanout(b, [&](size_t i, efl_sim* s) -> efl_status {
+                return on_canvas(s) ? unet_apply(s, at(i, (const float*)b->canvas->out), b->cw) : EFL_OK;
             });
         });
         if (st != EFL_OK) return batch_err(b, st, "batched stages before the solve failed");

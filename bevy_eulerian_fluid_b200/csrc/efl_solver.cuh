@@ -1094,7 +1094,6 @@ __global__ void __launch_bounds__(NT, 1) k_gsmix_oct(PersistentParams P, PF dbuf
         float frc[NC];
 #pragma unroll
         for (int q = 0; q < NC; ++q) {
-            const int lx = x0 + (q & 3), ly = y0 + (q >> 2);
             const int i = oct_pair(q), ln = oct_lane(q);
             float rcv = 0.0f;
             if ((fl >> (32 + q)) & 1ull) {

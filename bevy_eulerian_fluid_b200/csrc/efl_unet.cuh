@@ -956,8 +956,10 @@ __global__ void k_unet_guard_restore(Plane<double> x, const float* prev32, const
 // bilinearly; the sweeps then remove the fine-scale remainder quickly.
 // Coarse features: the mean over the block of each fine channel; maskc = 1
 // where the block holds a counted cell.
+// x0 holds row cy of the coarse features at x0 + cy * cs * 16 (cs = the coarse width, or the row pitch of
+// the canvas that packs a batch's simulations side by side).
 __global__ void k_unet_features_coarse(const float* res, const UnetFeatureArgs a, const unsigned char* mask,
-                                       const float* sigma, int f, bf16* x0, unsigned char* maskc) {
+                                       const float* sigma, int f, bf16* x0, int cs, unsigned char* maskc) {
     const int Wc = a.nx / f, Hc = a.ny / f;
     const int cx = blockIdx.x * blockDim.x + threadIdx.x, cy = blockIdx.y * blockDim.y + threadIdx.y;
     if (cx >= Wc || cy >= Hc) return;
@@ -977,17 +979,16 @@ __global__ void k_unet_features_coarse(const float* res, const UnetFeatureArgs a
     __align__(16) bf16 v[16];
 #pragma unroll
     for (int c = 0; c < 16; ++c) v[c] = __float2bfloat16_rn(c < 5 ? acc[c] * nrm : 0.0f);
-    const size_t q = (size_t)cy * Wc + cx;
-    uint4* dst = reinterpret_cast<uint4*>(x0 + q * 16);
+    uint4* dst = reinterpret_cast<uint4*>(x0 + ((size_t)cy * cs + cx) * 16);
     dst[0] = reinterpret_cast<const uint4*>(v)[0];
     dst[1] = reinterpret_cast<const uint4*>(v)[1];
-    maskc[q] = acc[4] > 0.0f ? 1 : 0;
+    maskc[(size_t)cy * Wc + cx] = acc[4] > 0.0f ? 1 : 0;
 }
 // x += sigma * (the coarse prediction interpolated bilinearly, coarse cell
 // (i, j) centred on fine coordinate ((i + 1/2) f - 1/2, ...), clamped at the
-// edges) on the counted cells.
-__global__ void k_unet_warm_coarse(Plane<double> x, const float* outc, const unsigned char* mask, const float* sigma,
-                                   int nx, int ny, int f) {
+// edges) on the counted cells; row j of the prediction at outc + j * cs * 16.
+__global__ void k_unet_warm_coarse(Plane<double> x, const float* outc, int cs, const unsigned char* mask,
+                                   const float* sigma, int nx, int ny, int f) {
     const int gx = blockIdx.x * blockDim.x + threadIdx.x, gy = blockIdx.y * blockDim.y + threadIdx.y;
     if (gx >= nx || gy >= ny || !mask[(size_t)gy * nx + gx]) return;
     const int Wc = nx / f, Hc = ny / f;
@@ -999,8 +1000,8 @@ __global__ void k_unet_warm_coarse(Plane<double> x, const float* outc, const uns
     if (j0 < 0) j0 = 0, tv = 0.0f;
     if (j0 >= Hc - 1) j0 = Hc - 1, tv = 0.0f;
     const int i1 = min(i0 + 1, Wc - 1), j1 = min(j0 + 1, Hc - 1);
-    const float o00 = outc[((size_t)j0 * Wc + i0) * 16], o10 = outc[((size_t)j0 * Wc + i1) * 16];
-    const float o01 = outc[((size_t)j1 * Wc + i0) * 16], o11 = outc[((size_t)j1 * Wc + i1) * 16];
+    const float o00 = outc[((size_t)j0 * cs + i0) * 16], o10 = outc[((size_t)j0 * cs + i1) * 16];
+    const float o01 = outc[((size_t)j1 * cs + i0) * 16], o11 = outc[((size_t)j1 * cs + i1) * 16];
     const float val = (o00 * (1.0f - tu) + o10 * tu) * (1.0f - tv) + (o01 * (1.0f - tu) + o11 * tu) * tv;
     x.at(gx, gy) = x.at(gx, gy) + (double)*sigma * (double)val;
 }
@@ -1220,7 +1221,10 @@ inline cudaError_t unet_alloc(UNet& n, int maxH, int maxW) {
 // activations and feature buffers are its own, sized for that simulation's
 // fine grid fh x fw and its network grid (fh / f) x (fw / f).  Forwards of
 // different simulations can then run at the same time on their own streams.
-inline cudaError_t unet_alloc_forward(UNet& v, const UNet& net, int fh, int fw) {
+// The forward-only workspace of a network for fh x fw fine cells: its activations, and with `fine` the
+// fine-grid buffers of the warm start (features' residual, guard partials, masks).  A batch's canvas takes
+// the activations alone.
+inline cudaError_t unet_alloc_forward(UNet& v, const UNet& net, int fh, int fw, bool fine = true) {
     v = net;
     v.arena = nullptr;
     v.extra.clear();
@@ -1243,13 +1247,19 @@ inline cudaError_t unet_alloc_forward(UNet& v, const UNet& net, int fh, int fw) 
     B(&v.t4, P2 * 64); B(&v.u4, P2 * 64); B(&v.t5, P1 * 32); B(&v.u5, P1 * 32);
     B(&v.t6, P0 * 16); B(&v.u6, P0 * 16);
     F(&v.out, P0 * 16);
-    items.push_back({(void**)&v.lpart, up256((PF_ / 256 + (size_t)fw / 32 + (size_t)fh / 8 + 8) * sizeof(float2))});
-    items.push_back({(void**)&v.epart, up256((PF_ / 256 + (size_t)fw / 32 + (size_t)fh / 8 + 9) * sizeof(double2))});
-    F(&v.prev32, PF_);
-    F(&v.res32, PF_);
-    F(&v.sigma, 64);
-    items.push_back({(void**)&v.mask, up256(PF_)});
-    items.push_back({(void**)&v.maskc, up256(P0)});
+    v.lpart = nullptr;
+    v.epart = nullptr;
+    v.prev32 = v.res32 = v.sigma = nullptr;
+    v.mask = v.maskc = nullptr;
+    if (fine) {
+        items.push_back({(void**)&v.lpart, up256((PF_ / 256 + (size_t)fw / 32 + (size_t)fh / 8 + 8) * sizeof(float2))});
+        items.push_back({(void**)&v.epart, up256((PF_ / 256 + (size_t)fw / 32 + (size_t)fh / 8 + 9) * sizeof(double2))});
+        F(&v.prev32, PF_);
+        F(&v.res32, PF_);
+        F(&v.sigma, 64);
+        items.push_back({(void**)&v.mask, up256(PF_)});
+        items.push_back({(void**)&v.maskc, up256(P0)});
+    }
     items.push_back({(void**)&v.err, 256});
     size_t total = 0;
     for (auto& it : items) total += it.bytes;
@@ -1341,29 +1351,59 @@ inline void unet_conv(UNet& n, int i, const bf16* x, int xs, int xo, int H, int 
     conv3x3_launch(a, st);
 }
 
-inline void unet_forward(UNet& n, int H, int W, cudaStream_t st) {
-    const int H1 = H / 2, W1 = W / 2, H2 = H / 4, W2 = W / 4, H3 = H / 8, W3 = W / 8;
-    unet_conv(n, 0, n.X0, 16, 0, H, W, n.t0, 16, 0, nullptr, st);
-    unet_conv(n, 1, n.t0, 16, 0, H, W, n.cat0, 48, 32, nullptr, st);
-    k_pool2<<<lin_grid((size_t)H1 * W1 * 16 / 8), 256, count_launch(), st>>>(n.cat0, 48, 32, H, W, 16, n.p1);
-    unet_conv(n, 2, n.p1, 16, 0, H1, W1, n.t1, 32, 0, nullptr, st);
-    unet_conv(n, 3, n.t1, 32, 0, H1, W1, n.cat1, 96, 64, nullptr, st);
-    k_pool2<<<lin_grid((size_t)H2 * W2 * 32 / 8), 256, count_launch(), st>>>(n.cat1, 96, 64, H1, W1, 32, n.p2);
-    unet_conv(n, 4, n.p2, 32, 0, H2, W2, n.t2, 64, 0, nullptr, st);
-    unet_conv(n, 5, n.t2, 64, 0, H2, W2, n.cat2, 128, 64, nullptr, st);
-    k_pool2<<<lin_grid((size_t)H3 * W3 * 64 / 8), 256, count_launch(), st>>>(n.cat2, 128, 64, H2, W2, 64, n.p3);
-    unet_conv(n, 6, n.p3, 64, 0, H3, W3, n.t3, 64, 0, nullptr, st);
-    unet_conv(n, 7, n.t3, 64, 0, H3, W3, n.u3, 64, 0, nullptr, st);
-    k_up2<<<lin_grid((size_t)H2 * W2 * 64 / 8), 256, count_launch(), st>>>(n.u3, H2, W2, 64, n.cat2, 128, 0);
-    unet_conv(n, 8, n.cat2, 128, 0, H2, W2, n.t4, 64, 0, nullptr, st);
-    unet_conv(n, 9, n.t4, 64, 0, H2, W2, n.u4, 64, 0, nullptr, st);
-    k_up2<<<lin_grid((size_t)H1 * W1 * 64 / 8), 256, count_launch(), st>>>(n.u4, H1, W1, 64, n.cat1, 96, 0);
-    unet_conv(n, 10, n.cat1, 96, 0, H1, W1, n.t5, 32, 0, nullptr, st);
-    unet_conv(n, 11, n.t5, 32, 0, H1, W1, n.u5, 32, 0, nullptr, st);
-    k_up2<<<lin_grid((size_t)H * W * 32 / 8), 256, count_launch(), st>>>(n.u5, H, W, 32, n.cat0, 48, 0);
-    unet_conv(n, 12, n.cat0, 48, 0, H, W, n.t6, 16, 0, nullptr, st);
-    unet_conv(n, 13, n.t6, 16, 0, H, W, n.u6, 16, 0, nullptr, st);
-    unet_conv(n, 14, n.u6, 16, 0, H, W, nullptr, 16, 0, n.out, st);
+// Zeroes channels [yo, yo + C) of the pixels that lie in no simulation's rectangle (m[p] == 0): the gaps of a
+// batch's canvas stay zero after every convolution, so that each simulation's image sees zeros around it,
+// as the zero padding of its own forward.
+__global__ void k_canvas_zero(bf16* y, int ys, int yo, int C, const unsigned char* m, int npix) {
+    const int g8 = C / 8;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;  // over npix * C / 8
+    if (i >= npix * g8) return;
+    const int q = i / g8, g = i - q * g8;
+    if (m[q]) return;
+    *reinterpret_cast<uint4*>(y + (size_t)q * ys + yo + 8 * g) = make_uint4(0u, 0u, 0u, 0u);
+}
+
+// The forward pass over an H x W image (H and W multiples of 8).  With `gaps` (four masks, one per level, of a
+// canvas whose rectangles start and end on multiples of 8) the gaps are zeroed after each convolution that
+// feeds another; average pooling and nearest upsampling keep them zero by themselves.
+inline void unet_forward(UNet& n, int H, int W, cudaStream_t st, const unsigned char* const* gaps = nullptr) {
+    const int Hs[4] = {H, H / 2, H / 4, H / 8}, Ws[4] = {W, W / 2, W / 4, W / 8};
+    auto conv = [&](int i, const bf16* x, int xs, int lvl, bf16* y, int ys, int yo) {
+        unet_conv(n, i, x, xs, 0, Hs[lvl], Ws[lvl], y, ys, yo, nullptr, st);
+        if (gaps) {
+            const int np = Hs[lvl] * Ws[lvl], c = kUnetSpec[i].cout;
+            k_canvas_zero<<<lin_grid((size_t)np * c / 8), 256, count_launch(), st>>>(y, ys, yo, c, gaps[lvl], np);
+        }
+    };
+    auto pool = [&](const bf16* in, int is, int io, int lvl, int C, bf16* out) {  // level lvl -> lvl + 1
+        k_pool2<<<lin_grid((size_t)Hs[lvl + 1] * Ws[lvl + 1] * C / 8), 256, count_launch(), st>>>(in, is, io, Hs[lvl],
+                                                                                                   Ws[lvl], C, out);
+    };
+    auto up = [&](const bf16* in, int lvl, int C, bf16* out, int os) {  // level lvl + 1 -> lvl, channels [0, C)
+        k_up2<<<lin_grid((size_t)Hs[lvl] * Ws[lvl] * C / 8), 256, count_launch(), st>>>(in, Hs[lvl], Ws[lvl], C, out,
+                                                                                         os, 0);
+    };
+    conv(0, n.X0, 16, 0, n.t0, 16, 0);
+    conv(1, n.t0, 16, 0, n.cat0, 48, 32);
+    pool(n.cat0, 48, 32, 0, 16, n.p1);
+    conv(2, n.p1, 16, 1, n.t1, 32, 0);
+    conv(3, n.t1, 32, 1, n.cat1, 96, 64);
+    pool(n.cat1, 96, 64, 1, 32, n.p2);
+    conv(4, n.p2, 32, 2, n.t2, 64, 0);
+    conv(5, n.t2, 64, 2, n.cat2, 128, 64);
+    pool(n.cat2, 128, 64, 2, 64, n.p3);
+    conv(6, n.p3, 64, 3, n.t3, 64, 0);
+    conv(7, n.t3, 64, 3, n.u3, 64, 0);
+    up(n.u3, 2, 64, n.cat2, 128);
+    conv(8, n.cat2, 128, 2, n.t4, 64, 0);
+    conv(9, n.t4, 64, 2, n.u4, 64, 0);
+    up(n.u4, 1, 64, n.cat1, 96);
+    conv(10, n.cat1, 96, 1, n.t5, 32, 0);
+    conv(11, n.t5, 32, 1, n.u5, 32, 0);
+    up(n.u5, 0, 32, n.cat0, 48);
+    conv(12, n.cat0, 48, 0, n.t6, 16, 0);
+    conv(13, n.t6, 16, 0, n.u6, 16, 0);
+    unet_conv(n, 14, n.u6, 16, 0, H, W, nullptr, 16, 0, n.out, st);  // the head: fp32, read inside the rectangles
 }
 
 // Backward of conv i: dy = relu'(y) * g (bf16), weight and bias gradients,

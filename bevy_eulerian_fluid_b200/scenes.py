@@ -100,7 +100,7 @@ def base_config(nx: int, ny: int) -> capi.Config:
 
 
 def dam_break(n: int = 256, steps: int = 600) -> Scene:
-    """C1: examples/water_surface.rs scene at n x n."""
+    """C1: the examples/water_surface.rs scene at n x n (the CPU-runnable case)."""
     cfg = base_config(n, n)
     src = aabb_source((0.0, -0.2 * n), (0.5 * 1.0 * n, 0.5 * 0.6 * n))
     return Scene(f"dam_break_{n}", cfg, oneshot=[src], steps=steps)
@@ -135,7 +135,7 @@ def random_bodies(n_per_shape: int, size: int, seed: int, rho: float = RHO) -> L
 
 def coupled(n: int = 512, steps: int = 1000, tolerance: float = 1e-5, seed: int = 0xC2,
             n_per_shape: int = 6, method: int = capi.PROJECTION_GAUSS_SEIDEL) -> Scene:
-    """C2: lower 40 % water, 24 random bodies, JFA, solve to tolerance."""
+    """C2 (the benchmark scene): lower 40 % water, 24 random bodies, JFA, solve to tolerance."""
     cfg = base_config(n, n)
     cfg.reinit.method = capi.REINIT_JUMP_FLOODING
     cfg.projection.method = method
@@ -149,7 +149,7 @@ def coupled(n: int = 512, steps: int = 1000, tolerance: float = 1e-5, seed: int 
 
 
 def scale(n: int = 4096, steps: int = 200, tolerance: float = 1e-5, coarsest: int = 16) -> Scene:
-    """C3 (configs[2]): dam break with a static circle r = n/16 at the centre, MG to tolerance."""
+    """C3: dam break with a static circle r = n/16 at the centre, MG to tolerance."""
     cfg = base_config(n, n)
     cfg.projection.method = capi.PROJECTION_MULTIGRID
     cfg.projection.tolerance = tolerance

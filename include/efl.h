@@ -521,12 +521,24 @@ EFL_API efl_status efl_unet_attach(efl_sim* sim, efl_unet* net, uint32_t flags);
  * grid); a recorded sample of the other form is dropped. */
 EFL_API efl_status efl_unet_set_coarsening(efl_unet* net, uint32_t factor);
 /* Attaches the network to every simulation of a batch (flags:
- * EFL_UNET_WARM_START, or 0 to detach).  Each simulation gets a forward-only
- * workspace of its own (weights shared), so that the simulations' forwards
- * run side by side inside the batch step, and each simulation's warm start,
- * iterates and iteration counts are those of its own efl_step with the
- * network attached.  Attach again after efl_unet_set_coarsening. */
+ * EFL_UNET_WARM_START, or 0 to detach).  With a coarsening above 1 and every
+ * simulation's coarse grid a multiple of 8 in both directions, the
+ * simulations' coarse features are packed into one canvas (efl_canvas_pack)
+ * and one forward pass over it serves them all; otherwise each simulation
+ * gets a forward-only workspace of its own and the forwards run side by side.
+ * Either way each simulation's warm start, iterates and iteration counts are
+ * those of its own efl_step with the network attached.  Attach again after
+ * efl_unet_set_coarsening. */
 EFL_API efl_status efl_batch_attach_unet(efl_batch* batch, efl_unet* net, uint32_t flags);
+/* The canvas of the batch's network forward (width and height in coarse
+ * pixels), 0 x 0 when the simulations' forwards run one by one. */
+EFL_API efl_status efl_batch_unet_canvas(const efl_batch* batch, int32_t* width, int32_t* height);
+/* The canvas layout (host only, no device work): n images of wh[2 i] x
+ * wh[2 i + 1] pixels (multiples of 8) on shelves of a canvas whose width is
+ * the smallest multiple of 512 holding the widest, tallest first, 8-pixel
+ * gaps; origins[2 i], origins[2 i + 1] = image i's top-left corner. */
+EFL_API efl_status efl_canvas_pack(const int32_t* wh, uint32_t n, int32_t* origins, int32_t* width,
+                                   int32_t* height);
 /* One Adam step (lr; beta 0.9 / 0.999; gradient clipped to global norm 1)
  * on the last recorded sample. */
 EFL_API efl_status efl_unet_train_step(efl_unet* net, float lr, float* loss);

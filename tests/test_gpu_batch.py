@@ -95,10 +95,11 @@ def test_batch_fast_path_graphs_match_oracle(oracle_api, gpu_api):
 
 @pytest.mark.parametrize("coarse", [4, 1])
 def test_batch_with_network_matches_single_sims(gpu_api, coarse):
-    """efl_batch_attach_unet: every simulation's solve is warm-started by the network inside the batch step (one
-    forward workspace per simulation, forwards side by side); each simulation still equals the same simulation
-    stepped alone by efl_step with the network attached -- bit-exact fields, equal iteration counts -- and every
-    solve still reaches the tolerance."""
+    """efl_batch_attach_unet: every simulation's solve is warm-started by the network inside the batch step
+    (coarsening 4: one forward over a canvas that packs the simulations' coarse grids, 8-pixel gaps kept zero
+    between them; coarsening 1: one forward workspace per simulation, forwards side by side); each simulation
+    still equals the same simulation stepped alone by efl_step with the network attached -- bit-exact fields,
+    equal iteration counts -- and every solve still reaches the tolerance."""
     b = _small_batch(5, seed=0xB1)
     net = capi.UNet(gpu_api, 192, 192, seed=7)
     rng = np.random.default_rng(1)
@@ -111,6 +112,8 @@ def test_batch_with_network_matches_single_sims(gpu_api, coarse):
     with capi.Batch(gpu_api, b.configs()) as batch:
         b.setup(batch.sims)
         batch.attach_unet(net)
+        cw, ch = batch.unet_canvas()
+        assert (cw > 0) == (coarse > 1), (cw, ch)
         for k in range(5):
             for i, s in enumerate(singles):
                 f = b.forces(i, k)
@@ -127,6 +130,7 @@ def test_batch_with_network_matches_single_sims(gpu_api, coarse):
             bad = compare_fields(g, s)
             assert not bad, (i, bad)
         batch.attach_unet(net, warm_start=False)
+        assert batch.unet_canvas() == (0, 0)
     for s in singles:
         s.close()
     net.close()

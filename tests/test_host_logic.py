@@ -216,3 +216,39 @@ def test_cfl_dt_bounds_the_displacement(oracle_api):
     dt = cfl_dt(mx, cfl=0.5, dt_max=1.0)
     assert dt * mx <= 0.5 * (1 + 1e-6)
     o.close()
+
+
+def _separated(a, b, gap=8):
+    (ax, ay, aw, ah), (bx, by, bw, bh) = a, b
+    return ax + aw + gap <= bx or bx + bw + gap <= ax or ay + ah + gap <= by or by + bh + gap <= ay
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_canvas_pack_layout(seed):
+    """efl_canvas_pack (host only): every image on the canvas, origins on multiples of 8, at least 8 pixels
+    between any two images, the width the smallest multiple of 512 holding the widest image."""
+    api = capi.load()
+    rng = np.random.default_rng(seed)
+    sizes = [(8 * int(rng.integers(1, 100)), 8 * int(rng.integers(1, 60))) for _ in range(int(rng.integers(1, 120)))]
+    org, w, h = capi.canvas_pack(api, sizes)
+    assert w % 512 == 0 and w - 512 < max(s[0] for s in sizes) <= w and h % 8 == 0
+    rects = [(x, y, sw, sh) for (x, y), (sw, sh) in zip(org, sizes)]
+    for x, y, sw, sh in rects:
+        assert x % 8 == 0 and y % 8 == 0 and x + sw <= w and y + sh <= h
+    for i in range(len(rects)):
+        for j in range(i):
+            assert _separated(rects[i], rects[j]), (rects[i], rects[j])
+    with pytest.raises(capi.EflError):
+        capi.canvas_pack(api, [(12, 16)])
+
+
+def test_canvas_of_the_c4_batch():
+    """The 96 simulations of the C4 batch on the grid coarsened 8x: one 512-wide canvas, its rectangles fill
+    more than half of it (the gaps and shelf ends are the rest)."""
+    api = capi.load()
+    bs = scenes.batch(96)
+    sizes = [(sc.cfg.nx // 8, sc.cfg.ny // 8) for sc in bs.scenes]
+    org, w, h = capi.canvas_pack(api, sizes)
+    assert w == 512
+    fill = sum(a * b for a, b in sizes) / (w * h)
+    assert 0.5 < fill <= 1.0, fill
