@@ -971,10 +971,10 @@ UnetFeatureArgs unet_feature_args(const efl_sim* s) {
                            (double)s->U.dt / (double)s->U.rho / dx / dx, s->nx, s->ny};
 }
 
-// The warm start in two halves around the network's forward pass: the features (into x0, row pitch cs
-// coarse pixels; the workspace's own X0 when x0 is null), then the prediction (read from outc, pitch cs)
-// added to the iterate and the guard that keeps it only where it lowers the residual.
-efl_status unet_features(efl_sim* s, bf16* x0, int cs) {
+// The warm start in two halves around the network's forward pass: the features (into x0, row pitch cs coarse
+// pixels: a batch's canvas; the workspace's own input when x0 is null), then the guard that keeps the
+// prediction only where it lowers the block-summed residual, and the prediction added to the iterate.
+efl_status unet_features(efl_sim* s, bf16* x0 = nullptr, int cs = 0) {
     UNet& n = s->unet_view ? *s->unet_view : s->unet->net;
     const int f = s->unet->net.coarse;
     if (n.coarse != f)
@@ -982,44 +982,50 @@ efl_status unet_features(efl_sim* s, bf16* x0, int cs) {
     const dim3 g = grid2d(s->nx, s->ny, kBlock);
     const UnetFeatureArgs a = unet_feature_args(s);
     k_unet_residual<<<g, kBlock, count_launch(), s->stream>>>(a, n.res32, n.prev32, n.mask, n.lpart);
-    k_unet_sigma<<<1, 32, count_launch(), s->stream>>>(n.lpart, (int)(g.x * g.y), n.sigma);
+    k_unet_sigma<<<1, UNET_RED_THREADS, count_launch(), s->stream>>>(n.lpart, (int)(g.x * g.y), n.sigma);
     if (f > 1) {
-        k_unet_features_coarse<<<grid2d(s->nx / f, s->ny / f, kBlock), kBlock, count_launch(), s->stream>>>(
-            n.res32, a, n.mask, n.sigma, f, x0 ? x0 : n.X0, x0 ? cs : s->nx / f, n.maskc);
+        k_unet_features_coarse<<<g, kBlock, count_launch(), s->stream>>>(n.res32, a, n.mask, n.sigma, f,
+                                                                         x0 ? x0 : n.X0, x0 ? cs : s->nx / f, n.maskc);
     } else {
         k_unet_features<<<g, kBlock, count_launch(), s->stream>>>(n.res32, a, n.mask, n.sigma, n.X0);
     }
     LAUNCH_CHECK();
     return EFL_OK;
 }
-efl_status unet_apply(efl_sim* s, const float* outc, int cs) {
+efl_status unet_apply(efl_sim* s) {
     UNet& n = s->unet_view ? *s->unet_view : s->unet->net;
     const int f = n.coarse;
     const Level64& L = s->mg64[0];
     const dim3 g = grid2d(s->nx, s->ny, kBlock);
-    if (f > 1)
-        k_unet_warm_coarse<<<g, kBlock, count_launch(), s->stream>>>(L.x, outc ? outc : n.out, outc ? cs : s->nx / f,
-                                                                      n.mask, n.sigma, s->nx, s->ny, f);
-    else
-        k_unet_warm<<<g, kBlock, count_launch(), s->stream>>>(L.x, n.out, n.mask, n.sigma, s->nx, s->ny);
-    // The guard: kept only if it lowers the block-summed residual (block = the coarsening, at least 8).
-    const int gb = std::max(8, f);
-    const dim3 gg = grid2d((s->nx + gb - 1) / gb, (s->ny + gb - 1) / gb, kBlock);
-    const int nb = (int)(gg.x * gg.y);
     const UnetFeatureArgs a = unet_feature_args(s);
-    k_unet_block_residual<<<gg, kBlock, count_launch(), s->stream>>>(a, n.prev32, gb, n.epart);
-    k_unet_guard<<<1, 32, count_launch(), s->stream>>>(n.epart, nb, (double*)(n.epart + nb));
-    k_unet_guard_restore<<<g, kBlock, count_launch(), s->stream>>>(L.x, n.prev32, n.mask, (double*)(n.epart + nb),
-                                                                    s->nx, s->ny);
+    // The guard: kept only if it lowers the summed squares of the residual's sums over 8 x 8 blocks.
+    if (f > 1) {  // the warm-started iterate formed on the fly for the guard, written only where it is kept
+        const int nb = (int)(g.x * g.y);
+        double* alpha = (double*)(n.epart + nb);
+        k_unet_guard_residual<<<g, kBlock, count_launch(), s->stream>>>(a, n.prev32, n.mask, n.out, s->nx / f, n.sigma,
+                                                                        f, n.epart);
+        k_unet_guard<<<1, UNET_RED_THREADS, count_launch(), s->stream>>>(n.epart, nb, alpha);
+        k_unet_apply_warm<<<g, kBlock, count_launch(), s->stream>>>(L.x, n.out, s->nx / f, n.mask, n.sigma, alpha,
+                                                                    s->nx, s->ny, f);
+    } else {
+        const int gb = 8;
+        const dim3 gg = grid2d((s->nx + gb - 1) / gb, (s->ny + gb - 1) / gb, kBlock);
+        const int nb = (int)(gg.x * gg.y);
+        double* alpha = (double*)(n.epart + nb);
+        k_unet_warm<<<g, kBlock, count_launch(), s->stream>>>(L.x, n.out, n.mask, n.sigma, s->nx, s->ny);
+        k_unet_block_residual<<<gg, kBlock, count_launch(), s->stream>>>(a, n.prev32, gb, n.epart);
+        k_unet_guard<<<1, UNET_RED_THREADS, count_launch(), s->stream>>>(n.epart, nb, alpha);
+        k_unet_guard_restore<<<g, kBlock, count_launch(), s->stream>>>(L.x, n.prev32, n.mask, alpha, s->nx, s->ny);
+    }
     LAUNCH_CHECK();
     return EFL_OK;
 }
 efl_status unet_before_solve(efl_sim* s) {
-    TRY(unet_features(s, nullptr, 0));
+    TRY(unet_features(s));
     if (s->unet_flags & EFL_UNET_WARM_START) {
         UNet& n = s->unet_view ? *s->unet_view : s->unet->net;
         unet_forward(n, s->ny / n.coarse, s->nx / n.coarse, s->stream);
-        TRY(unet_apply(s, nullptr, 0));
+        TRY(unet_apply(s));
     }
     return EFL_OK;
 }
@@ -2142,6 +2148,12 @@ struct efl_batch {
     const unsigned char* gaps[4] = {};
     int cw = 0, ch = 0;                    // canvas width and height, coarse pixels
     std::vector<int2> corigin;             // per simulation: its rectangle's origin
+    // The warm start's phases around the canvas forward, one launch each for the simulations on the canvas:
+    // their descriptors and block starts on the device, and the host copies last uploaded.
+    WarmSim* d_warm = nullptr;
+    int* d_warm_start = nullptr;
+    std::vector<WarmSim> h_warm;
+    std::vector<int> h_warm_start;
 };
 
 namespace {
@@ -2177,6 +2189,12 @@ void canvas_free(efl_batch* b) {
         delete b->canvas;
     }
     cudaFree(b->d_gaps);
+    cudaFree(b->d_warm);
+    cudaFree(b->d_warm_start);
+    b->d_warm = nullptr;
+    b->d_warm_start = nullptr;
+    b->h_warm.clear();
+    b->h_warm_start.clear();
     b->canvas = nullptr;
     b->canvas_net = nullptr;
     b->d_gaps = nullptr;
@@ -2524,7 +2542,9 @@ efl_status canvas_setup(efl_batch* b, const efl_unet* u) {
             for (int y = y0; y < y0 + h; ++y) std::memset(&m[off[l] + (size_t)y * (W >> l) + x0], 1, (size_t)w);
         }
     if (cudaMalloc(&b->d_gaps, total) != cudaSuccess ||
-        cudaMemcpy(b->d_gaps, m.data(), total, cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaMemcpy(b->d_gaps, m.data(), total, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMalloc(&b->d_warm, n * sizeof(WarmSim)) != cudaSuccess ||
+        cudaMalloc(&b->d_warm_start, (n + 1) * sizeof(int)) != cudaSuccess) {
         canvas_free(b);
         return EFL_ERR_OUT_OF_MEMORY;
     }
@@ -2534,6 +2554,53 @@ efl_status canvas_setup(efl_batch* b, const efl_unet* u) {
     b->corigin.resize(n);
     for (size_t i = 0; i < n; ++i) b->corigin[i] = make_int2(org[2 * i], org[2 * i + 1]);
     b->canvas_net = u;
+    return EFL_OK;
+}
+
+// The warm-start descriptors of the simulations `on` (on the canvas), uploaded when the simulations or their
+// time step differ from the last upload's (the batch stream drained first: a replayed graph may still read the
+// old descriptors).  Everything else they hold is fixed from efl_batch_attach_unet on.
+efl_status warm_upload(efl_batch* b, const std::vector<int>& on) {
+    const int n = (int)on.size();
+    std::vector<int> key(on);
+    for (int i : on) {
+        uint32_t dtb;
+        std::memcpy(&dtb, &b->sims[i]->U.dt, 4);
+        key.push_back((int)dtb);
+    }
+    if ((int)b->h_warm.size() == n && b->h_warm_start.size() == key.size() + (size_t)(n + 1) &&
+        std::equal(key.begin(), key.end(), b->h_warm_start.begin() + (n + 1)))
+        return EFL_OK;
+    std::vector<WarmSim> hw(n);
+    std::vector<int> st(n + 1, 0);
+    for (int k = 0; k < n; ++k) {
+        efl_sim* s = b->sims[on[k]];
+        const UNet& v = *s->unet_view;
+        WarmSim& w = hw[k];
+        w.a = unet_feature_args(s);
+        w.res32 = v.res32;
+        w.prev32 = v.prev32;
+        w.sigma = v.sigma;
+        w.mask = v.mask;
+        w.maskc = v.maskc;
+        w.epart = v.epart;
+        const size_t off = ((size_t)b->corigin[on[k]].y * b->cw + b->corigin[on[k]].x) * 16;
+        w.x0 = b->canvas->X0 + off;
+        w.outc = b->canvas->out + off;
+        w.cs = b->cw;
+        w.f = v.coarse;
+        const dim3 fg = grid2d(s->nx, s->ny, kBlock);
+        w.fgx = (int)fg.x;
+        w.fgy = (int)fg.y;
+        st[k + 1] = st[k] + w.fgx * w.fgy;
+    }
+    if (cudaStreamSynchronize(b->stream) != cudaSuccess ||
+        cudaMemcpy(b->d_warm, hw.data(), n * sizeof(WarmSim), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(b->d_warm_start, st.data(), st.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
+        return EFL_ERR_CUDA;
+    b->h_warm = hw;
+    st.insert(st.end(), key.begin(), key.end());
+    b->h_warm_start = st;
     return EFL_OK;
 }
 
@@ -2622,29 +2689,44 @@ efl_status efl_batch_step(efl_batch* b, float dt, efl_step_stats* stats) {
             sig_pre = fnv(sig_pre, segment_sig(s, SEG_PRE));
             sig_post = fnv(sig_post, segment_sig(s, SEG_POST));
         }
-        // With a canvas, the warm start's features of every simulation go into it, one forward pass over the
-        // canvas follows on the batch stream, and each simulation then takes its prediction from its rectangle.
+        // With a canvas, each simulation on it writes its features into its rectangle on its own stream (where
+        // those small kernels overlap the other simulations' stages), one forward pass over the canvas follows
+        // on the batch stream, and the guard and the application run as one launch each for all of them; the
+        // others run their own warm start.
         auto on_canvas = [&](const efl_sim* s) {
             return b->canvas && s->unet == b->canvas_net && (s->unet_flags & EFL_UNET_WARM_START);
         };
-        auto at = [&](size_t i, auto* base) { return base + ((size_t)b->corigin[i].y * b->cw + b->corigin[i].x) * 16; };
-        bool any_canvas = false;
-        for (const efl_sim* s : b->sims) any_canvas = any_canvas || on_canvas(s);
-        sig_pre = fnv(sig_pre, (uint64_t)(uintptr_t)b->canvas + (any_canvas ? 1 : 0));
+        std::vector<int> on;
+        for (size_t i = 0; i < n; ++i)
+            if (on_canvas(b->sims[i])) on.push_back((int)i);
+        if (!on.empty() && warm_upload(b, on) != EFL_OK)
+            return batch_err(b, EFL_ERR_CUDA, "warm-start descriptor upload failed");
+        sig_pre = fnv(sig_pre, (uint64_t)(uintptr_t)b->canvas);
+        for (int i : on) sig_pre = fnv(sig_pre, (uint64_t)i);
         efl_status st = run_segment(b->gc, b->stream, sig_pre | 1, SEG_PRE, [&]() -> efl_status {
             TRY(batch_fanout(b, [&](size_t i, efl_sim* s) -> efl_status {
                 TRY(run_stages(s, EFL_STAGE_UPDATE_SOLID, EFL_STAGE_DIVERGENCE, nullptr));
                 const Level64& L = s->mg64[0];
                 k_widen<<<grid2d(s->nx, s->ny, kBlock), kBlock, count_launch(), s->stream>>>(s->p0, s->div, L.x, L.b);
-                if (on_canvas(s)) return unet_features(s, at(i, b->canvas->X0), b->cw);
+                if (on_canvas(s))
+                    return unet_features(s, b->canvas->X0 + ((size_t)b->corigin[i].y * b->cw + b->corigin[i].x) * 16,
+                                         b->cw);
                 if (s->unet && (s->unet_flags & EFL_UNET_WARM_START)) TRY(unet_before_solve(s));
                 return EFL_OK;
             }));
-            if (!any_canvas) return EFL_OK;
+            if (on.empty()) return EFL_OK;
+            for (int i : on)
+                if (b->sims[i]->unet_view->coarse != b->canvas_net->net.coarse)
+                    return set_err(b->sims[i], EFL_ERR_STATE,
+                                   "the network's coarsening changed after efl_batch_attach_unet: attach again");
+            const int m = (int)on.size(), nblk = b->h_warm_start[m];  // thread blocks over all their cells
+            const WarmSim* W = b->d_warm;
+            const int* S = b->d_warm_start;
             unet_forward(*b->canvas, b->ch, b->cw, b->stream, b->gaps);
-            return batch_fanout(b, [&](size_t i, efl_sim* s) -> efl_status {
-                return on_canvas(s) ? unet_apply(s, at(i, (const float*)b->canvas->out), b->cw) : EFL_OK;
-            });
+            k_warm_batch_guard_residual<<<nblk, kBlock, count_launch(), b->stream>>>(W, S, m);
+            k_warm_batch_guard<<<m, UNET_RED_THREADS, count_launch(), b->stream>>>(W);
+            k_warm_batch_apply<<<nblk, kBlock, count_launch(), b->stream>>>(W, S, m);
+            return cudaGetLastError() == cudaSuccess ? EFL_OK : EFL_ERR_CUDA;
         });
         if (st != EFL_OK) return batch_err(b, st, "batched stages before the solve failed");
         std::vector<int> all(n);

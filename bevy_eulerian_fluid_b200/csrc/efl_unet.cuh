@@ -22,6 +22,7 @@
 #include <cuda_bf16.h>
 #include <stdint.h>
 
+#include <algorithm>
 #include <string>
 #include <vector>
 
@@ -772,9 +773,10 @@ struct UnetFeatureArgs {
 // res[p] = cdiv * (b - A prev) on the counted cells (the operator of
 // residual.wgsl:33-54 in factored form, as the mixed solve builds it), the
 // mask, prev32 = prev, and per-block partial sums (res^2, count).
-__global__ void __launch_bounds__(256) k_unet_residual(UnetFeatureArgs a, float* res, float* prev32, unsigned char* mask,
-                                                        float2* part) {
-    const int gx = blockIdx.x * blockDim.x + threadIdx.x, gy = blockIdx.y * blockDim.y + threadIdx.y;
+// (Block (bx, by) of a grid bgx blocks wide; a batch's launch covers several simulations' grids.)
+EFL_DEV void unet_residual_blk(const UnetFeatureArgs& a, float* res, float* prev32, unsigned char* mask, float2* part,
+                               int bx, int by, int bgx) {
+    const int gx = bx * blockDim.x + threadIdx.x, gy = by * blockDim.y + threadIdx.y;
     float r2 = 0.0f, c = 0.0f;
     if (gx < a.nx && gy < a.ny) {
         const size_t p = (size_t)gy * a.nx + gx;
@@ -818,19 +820,43 @@ __global__ void __launch_bounds__(256) k_unet_residual(UnetFeatureArgs a, float*
             s2.x += red[w].x;
             s2.y += red[w].y;
         }
-        part[blockIdx.y * gridDim.x + blockIdx.x] = s2;
+        part[by * bgx + bx] = s2;
     }
 }
-// sigma = RMS of the residual over the counted cells (1 if there are none), in order.
-__global__ void k_unet_sigma(const float2* part, int n, float* sigma) {
-    if (threadIdx.x != 0) return;
+__global__ void __launch_bounds__(256) k_unet_residual(UnetFeatureArgs a, float* res, float* prev32, unsigned char* mask,
+                                                        float2* part) {
+    unet_residual_blk(a, res, prev32, mask, part, blockIdx.x, blockIdx.y, gridDim.x);
+}
+// The in-order sums of a block's reductions: thread t adds partials t, t + 256, ... in turn, then a fixed tree
+// over the 256 threads (blocks of 256 threads; the same order for a simulation alone and in a batch).
+constexpr int UNET_RED_THREADS = 256;
+EFL_DEV double2 block_sum2(double a, double b) {
+    __shared__ double2 red[UNET_RED_THREADS];
+    const int t = threadIdx.x;
+    red[t] = make_double2(a, b);
+    __syncthreads();
+#pragma unroll
+    for (int o = UNET_RED_THREADS / 2; o > 0; o >>= 1) {
+        if (t < o) red[t] = make_double2(red[t].x + red[t + o].x, red[t].y + red[t + o].y);
+        __syncthreads();
+    }
+    return red[0];
+}
+// sigma = RMS of the residual over the counted cells (1 if there are none).
+EFL_DEV void unet_sigma_blk(const float2* part, int n, float* sigma) {
     double r2 = 0.0, c = 0.0;
-    for (int i = 0; i < n; ++i) {
+    for (int i = threadIdx.x; i < n; i += UNET_RED_THREADS) {
         r2 += part[i].x;
         c += part[i].y;
     }
-    const double v = c > 0.0 ? sqrt(r2 / c) : 0.0;
-    *sigma = v > 0.0 ? (float)v : 1.0f;
+    const double2 s2 = block_sum2(r2, c);
+    if (threadIdx.x == 0) {
+        const double v = s2.y > 0.0 ? sqrt(s2.x / s2.y) : 0.0;
+        *sigma = v > 0.0 ? (float)v : 1.0f;
+    }
+}
+__global__ void __launch_bounds__(UNET_RED_THREADS) k_unet_sigma(const float2* part, int n, float* sigma) {
+    unet_sigma_blk(part, n, sigma);
 }
 __global__ void k_unet_features(const float* res, const UnetFeatureArgs a, const unsigned char* mask,
                                 const float* sigma, bf16* x0) {
@@ -875,9 +901,11 @@ __global__ void k_unet_target(Plane<double> x, const float* prev32, const float*
 // made them smaller.  One thread per block; .x = (sum of r over the block)^2
 // for the start iterate p (= prev32) and .y for the warm-started x, per
 // 32 x 8 group of blocks.
-__global__ void __launch_bounds__(256) k_unet_block_residual(UnetFeatureArgs a, const float* prev32, int g,
-                                                             double2* part) {
-    const int cx = blockIdx.x * blockDim.x + threadIdx.x, cy = blockIdx.y * blockDim.y + threadIdx.y;
+// xv(x, y) is the warm-started iterate at a cell (read from the plane, or formed on the fly).
+template <class XV>
+EFL_DEV void unet_block_residual_blk(const UnetFeatureArgs& a, const float* prev32, int g, double2* part, int bx, int by,
+                                     int bgx, XV xv) {
+    const int cx = bx * blockDim.x + threadIdx.x, cy = by * blockDim.y + threadIdx.y;
     const int Wc = (a.nx + g - 1) / g, Hc = (a.ny + g - 1) / g;
     double sp = 0.0, sx = 0.0;
     if (cx < Wc && cy < Hc) {
@@ -898,7 +926,7 @@ __global__ void __launch_bounds__(256) k_unet_block_residual(UnetFeatureArgs a, 
                         if (level < 0.0f) {
                             den += (double)f[q];
                             s1 += (double)f[q] * (double)prev32[(size_t)jy * a.nx + jx];
-                            s2 += (double)f[q] * a.prev.at(jx, jy);
+                            s2 += (double)f[q] * xv(jx, jy);
                         } else {
                             den += (double)f[q] * (1.0 - (double)level / (double)phi);
                         }
@@ -906,7 +934,7 @@ __global__ void __launch_bounds__(256) k_unet_block_residual(UnetFeatureArgs a, 
                 }
                 const double bb = a.b.at(gx, gy);
                 sp += bb - a.factor * (den * (double)prev32[(size_t)gy * a.nx + gx] - s1);
-                sx += bb - a.factor * (den * a.prev.at(gx, gy) - s2);
+                sx += bb - a.factor * (den * xv(gx, gy) - s2);
             }
     }
     double vp = sp * sp, vx = sx * sx;
@@ -925,18 +953,26 @@ __global__ void __launch_bounds__(256) k_unet_block_residual(UnetFeatureArgs a, 
             a1 += red_p[w];
             a2 += red_x[w];
         }
-        part[blockIdx.y * gridDim.x + blockIdx.x] = make_double2(a1, a2);
+        part[by * bgx + bx] = make_double2(a1, a2);
     }
 }
-// keep (*alpha = 1) or drop (*alpha = 0) the warm start, from the block-residual partials summed in order.
-__global__ void k_unet_guard(const double2* part, int n, double* alpha) {
-    if (threadIdx.x != 0) return;
+__global__ void __launch_bounds__(256) k_unet_block_residual(UnetFeatureArgs a, const float* prev32, int g,
+                                                             double2* part) {
+    unet_block_residual_blk(a, prev32, g, part, blockIdx.x, blockIdx.y, gridDim.x,
+                            [&](int x, int y) { return a.prev.at(x, y); });
+}
+// keep (*alpha = 1) or drop (*alpha = 0) the warm start, from the block-residual partials.
+EFL_DEV void unet_guard_blk(const double2* part, int n, double* alpha) {
     double before = 0.0, after = 0.0;
-    for (int i = 0; i < n; ++i) {
+    for (int i = threadIdx.x; i < n; i += UNET_RED_THREADS) {
         before += part[i].x;
         after += part[i].y;
     }
-    *alpha = after < before ? 1.0 : 0.0;
+    const double2 s2 = block_sum2(before, after);
+    if (threadIdx.x == 0) *alpha = s2.y < s2.x ? 1.0 : 0.0;
+}
+__global__ void __launch_bounds__(UNET_RED_THREADS) k_unet_guard(const double2* part, int n, double* alpha) {
+    unet_guard_blk(part, n, alpha);
 }
 // Where the guard dropped it, the start iterate p (= prev32, exactly: it is the f32 pressure widened) back on
 // the counted cells.
@@ -958,39 +994,55 @@ __global__ void k_unet_guard_restore(Plane<double> x, const float* prev32, const
 // where the block holds a counted cell.
 // x0 holds row cy of the coarse features at x0 + cy * cs * 16 (cs = the coarse width, or the row pitch of
 // the canvas that packs a batch's simulations side by side).
-__global__ void k_unet_features_coarse(const float* res, const UnetFeatureArgs a, const unsigned char* mask,
-                                       const float* sigma, int f, bf16* x0, int cs, unsigned char* maskc) {
-    const int Wc = a.nx / f, Hc = a.ny / f;
-    const int cx = blockIdx.x * blockDim.x + threadIdx.x, cy = blockIdx.y * blockDim.y + threadIdx.y;
-    if (cx >= Wc || cy >= Hc) return;
+// One thread per fine cell, blocks of 32 x 8 threads: a block's cells hold (32 / f) x (8 / f) coarse cells
+// (f = 2, 4 or 8; the grid a multiple of 8 f).  A coarse cell's sums run over the f cells of each row by
+// shuffles, then over its f rows in order.
+EFL_DEV void unet_features_coarse_blk(const float* res, const UnetFeatureArgs& a, const unsigned char* mask,
+                                      const float* sigma, int f, bf16* x0, int cs, unsigned char* maskc, int bx, int by) {
+    __shared__ float rows[8][32][5];
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int gx = bx * 32 + tx, gy = by * 8 + ty;
     const float inv = 1.0f / *sigma;
-    float acc[5] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
-    for (int j = 0; j < f; ++j)
-        for (int i = 0; i < f; ++i) {
-            const int gx = cx * f + i, gy = cy * f + j;
-            const size_t p = (size_t)gy * a.nx + gx;
-            acc[0] += res[p] * inv;
-            acc[1] += 0.5f * (a.fu.at(gx, gy) + a.fu.at(gx + 1, gy));
-            acc[2] += 0.5f * (a.fv.at(gx, gy) + a.fv.at(gx, gy + 1));
-            acc[3] += fminf(1.0f, fmaxf(-1.0f, a.ls.at(gx, gy) / (float)a.ny));
-            acc[4] += mask[p] ? 1.0f : 0.0f;
-        }
-    const float nrm = 1.0f / (float)(f * f);
-    __align__(16) bf16 v[16];
+    float v[5] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+    if (gx < a.nx && gy < a.ny) {
+        const size_t p = (size_t)gy * a.nx + gx;
+        v[0] = res[p] * inv;
+        v[1] = 0.5f * (a.fu.at(gx, gy) + a.fu.at(gx + 1, gy));
+        v[2] = 0.5f * (a.fv.at(gx, gy) + a.fv.at(gx, gy + 1));
+        v[3] = fminf(1.0f, fmaxf(-1.0f, a.ls.at(gx, gy) / (float)a.ny));
+        v[4] = mask[p] ? 1.0f : 0.0f;
+    }
+    for (int o = 1; o < f; o <<= 1)
 #pragma unroll
-    for (int c = 0; c < 16; ++c) v[c] = __float2bfloat16_rn(c < 5 ? acc[c] * nrm : 0.0f);
+        for (int c = 0; c < 5; ++c) v[c] += __shfl_xor_sync(0xffffffffu, v[c], o);
+    if (tx % f == 0)
+#pragma unroll
+        for (int c = 0; c < 5; ++c) rows[ty][tx][c] = v[c];
+    __syncthreads();
+    const int Wc = a.nx / f, Hc = a.ny / f, cx = gx / f, cy = gy / f;
+    if (tx % f != 0 || ty % f != 0 || cx >= Wc || cy >= Hc) return;
+    float acc[5];
+#pragma unroll
+    for (int c = 0; c < 5; ++c) {
+        acc[c] = rows[ty][tx][c];
+        for (int r = 1; r < f; ++r) acc[c] += rows[ty + r][tx][c];
+    }
+    const float nrm = 1.0f / (float)(f * f);
+    __align__(16) bf16 o16[16];
+#pragma unroll
+    for (int c = 0; c < 16; ++c) o16[c] = __float2bfloat16_rn(c < 5 ? acc[c] * nrm : 0.0f);
     uint4* dst = reinterpret_cast<uint4*>(x0 + ((size_t)cy * cs + cx) * 16);
-    dst[0] = reinterpret_cast<const uint4*>(v)[0];
-    dst[1] = reinterpret_cast<const uint4*>(v)[1];
+    dst[0] = reinterpret_cast<const uint4*>(o16)[0];
+    dst[1] = reinterpret_cast<const uint4*>(o16)[1];
     maskc[(size_t)cy * Wc + cx] = acc[4] > 0.0f ? 1 : 0;
 }
-// x += sigma * (the coarse prediction interpolated bilinearly, coarse cell
-// (i, j) centred on fine coordinate ((i + 1/2) f - 1/2, ...), clamped at the
-// edges) on the counted cells; row j of the prediction at outc + j * cs * 16.
-__global__ void k_unet_warm_coarse(Plane<double> x, const float* outc, int cs, const unsigned char* mask,
-                                   const float* sigma, int nx, int ny, int f) {
-    const int gx = blockIdx.x * blockDim.x + threadIdx.x, gy = blockIdx.y * blockDim.y + threadIdx.y;
-    if (gx >= nx || gy >= ny || !mask[(size_t)gy * nx + gx]) return;
+__global__ void k_unet_features_coarse(const float* res, const UnetFeatureArgs a, const unsigned char* mask,
+                                       const float* sigma, int f, bf16* x0, int cs, unsigned char* maskc) {
+    unet_features_coarse_blk(res, a, mask, sigma, f, x0, cs, maskc, blockIdx.x, blockIdx.y);
+}
+// The coarse prediction at fine cell (gx, gy), interpolated bilinearly: coarse cell (i, j) is centred on fine
+// coordinate ((i + 1/2) f - 1/2, ...), clamped at the edges; row j of the prediction at outc + j * cs * 16.
+EFL_DEV float unet_coarse_pred(const float* outc, int cs, int nx, int ny, int f, int gx, int gy) {
     const int Wc = nx / f, Hc = ny / f;
     const float u = ((float)gx + 0.5f) / (float)f - 0.5f, v = ((float)gy + 0.5f) / (float)f - 0.5f;
     int i0 = (int)floorf(u), j0 = (int)floorf(v);
@@ -1002,9 +1054,151 @@ __global__ void k_unet_warm_coarse(Plane<double> x, const float* outc, int cs, c
     const int i1 = min(i0 + 1, Wc - 1), j1 = min(j0 + 1, Hc - 1);
     const float o00 = outc[((size_t)j0 * cs + i0) * 16], o10 = outc[((size_t)j0 * cs + i1) * 16];
     const float o01 = outc[((size_t)j1 * cs + i0) * 16], o11 = outc[((size_t)j1 * cs + i1) * 16];
-    const float val = (o00 * (1.0f - tu) + o10 * tu) * (1.0f - tv) + (o01 * (1.0f - tu) + o11 * tu) * tv;
-    x.at(gx, gy) = x.at(gx, gy) + (double)*sigma * (double)val;
+    // explicit roundings: the guard's on-the-fly value and the applied one agree in every kernel they inline into
+    const float su = __fsub_rn(1.0f, tu), sv = __fsub_rn(1.0f, tv);
+    const float top = __fadd_rn(__fmul_rn(o00, su), __fmul_rn(o10, tu));
+    const float bot = __fadd_rn(__fmul_rn(o01, su), __fmul_rn(o11, tu));
+    return __fadd_rn(__fmul_rn(top, sv), __fmul_rn(bot, tv));
 }
+// The warm-started iterate at (gx, gy): x + sigma * prediction on the counted cells, x elsewhere.
+EFL_DEV double unet_warm_value(const Plane<double>& x, const float* outc, int cs, const unsigned char* mask,
+                               float sigma, int nx, int ny, int f, int gx, int gy) {
+    const double v = x.at(gx, gy);
+    return mask[(size_t)gy * nx + gx]
+               ? __dadd_rn(v, __dmul_rn((double)sigma, (double)unet_coarse_pred(outc, cs, nx, ny, f, gx, gy)))
+               : v;
+}
+// The guard's block residuals of the coarse warm start, one thread per fine cell (blocks of 32 x 8 threads; the
+// guard blocks are 8 x 8, four to a thread block): the residual of the start iterate (prev32) and of the
+// warm-started one, formed on the fly from the coarse prediction (x is still the start iterate) with a one-cell
+// halo in shared memory; each summed over its guard block (the 8 cells of a row by shuffles, then the 8 rows in
+// order) and squared, the four squares added: one partial per thread block.
+EFL_DEV void unet_guard_residual_blk(const UnetFeatureArgs& a, const float* prev32, const unsigned char* mask,
+                                     const float* outc, int cs, const float* sigma, int f, double2* part, int bx,
+                                     int by, int bgx) {
+    __shared__ double wv[10][34];
+    __shared__ float pv[10][34];
+    __shared__ double2 rs[8][4];
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
+    const int X0 = bx * 32 - 1, Y0 = by * 8 - 1;
+    const float sg = *sigma;
+    for (int i = tid; i < 340; i += 256) {
+        const int ly = i / 34, lx = i - ly * 34, hx = X0 + lx, hy = Y0 + ly;
+        const bool in = (unsigned)hx < (unsigned)a.nx && (unsigned)hy < (unsigned)a.ny;
+        wv[ly][lx] = in ? unet_warm_value(a.prev, outc, cs, mask, sg, a.nx, a.ny, f, hx, hy) : 0.0;
+        pv[ly][lx] = in ? prev32[(size_t)hy * a.nx + hx] : 0.0f;
+    }
+    __syncthreads();
+    const int gx = bx * 32 + tx, gy = by * 8 + ty;
+    double rp = 0.0, rx = 0.0;
+    if (gx < a.nx && gy < a.ny) {
+        const float phi = a.ls.at(gx, gy);
+        const float fq[4] = {a.fu.at(gx, gy), a.fu.at(gx + 1, gy), a.fv.at(gx, gy), a.fv.at(gx, gy + 1)};
+        if (phi < 0.0f && !(fq[0] == 0.0f && fq[1] == 0.0f && fq[2] == 0.0f && fq[3] == 0.0f)) {
+            const int ox[4] = {-1, 1, 0, 0}, oy[4] = {0, 0, -1, 1};
+            double den = 0.0, s1 = 0.0, s2 = 0.0;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int jx = gx + ox[q], jy = gy + oy[q];
+                if ((unsigned)jx < (unsigned)a.nx && (unsigned)jy < (unsigned)a.ny) {
+                    const float level = a.ls.at(jx, jy);
+                    if (level < 0.0f) {
+                        den += (double)fq[q];
+                        s1 += (double)fq[q] * (double)pv[ty + 1 + oy[q]][tx + 1 + ox[q]];
+                        s2 += (double)fq[q] * wv[ty + 1 + oy[q]][tx + 1 + ox[q]];
+                    } else {
+                        den += (double)fq[q] * (1.0 - (double)level / (double)phi);
+                    }
+                }
+            }
+            const double bb = a.b.at(gx, gy);
+            rp = bb - a.factor * (den * (double)pv[ty + 1][tx + 1] - s1);
+            rx = bb - a.factor * (den * wv[ty + 1][tx + 1] - s2);
+        }
+    }
+    for (int o = 1; o < 8; o <<= 1) {
+        rp += __shfl_xor_sync(0xffffffffu, rp, o);
+        rx += __shfl_xor_sync(0xffffffffu, rx, o);
+    }
+    if ((tx & 7) == 0) rs[ty][tx >> 3] = make_double2(rp, rx);
+    __syncthreads();
+    if (tid == 0) {
+        double a1 = 0.0, a2 = 0.0;
+        for (int k = 0; k < 4; ++k) {
+            double sp = 0.0, sx = 0.0;
+            for (int r = 0; r < 8; ++r) {
+                sp += rs[r][k].x;
+                sx += rs[r][k].y;
+            }
+            a1 += sp * sp;
+            a2 += sx * sx;
+        }
+        part[by * bgx + bx] = make_double2(a1, a2);
+    }
+}
+__global__ void __launch_bounds__(256) k_unet_guard_residual(UnetFeatureArgs a, const float* prev32,
+                                                             const unsigned char* mask, const float* outc, int cs,
+                                                             const float* sigma, int f, double2* part) {
+    unet_guard_residual_blk(a, prev32, mask, outc, cs, sigma, f, part, blockIdx.x, blockIdx.y, gridDim.x);
+}
+// Where the guard kept it (*alpha != 0), the coarse warm start written into the iterate.
+EFL_DEV void unet_apply_warm_blk(const Plane<double>& x, const float* outc, int cs, const unsigned char* mask,
+                                 const float* sigma, const double* alpha, int nx, int ny, int f, int bx, int by) {
+    const int gx = bx * blockDim.x + threadIdx.x, gy = by * blockDim.y + threadIdx.y;
+    if (gx >= nx || gy >= ny || *alpha == 0.0) return;
+    x.at(gx, gy) = unet_warm_value(x, outc, cs, mask, *sigma, nx, ny, f, gx, gy);
+}
+__global__ void k_unet_apply_warm(Plane<double> x, const float* outc, int cs, const unsigned char* mask,
+                                  const float* sigma, const double* alpha, int nx, int ny, int f) {
+    unet_apply_warm_blk(x, outc, cs, mask, sigma, alpha, nx, ny, f, blockIdx.x, blockIdx.y);
+}
+
+// ---------------------------------------------------------------------------
+// A batch's coarse warm start after the canvas forward pass: the guard and the prediction's application, one
+// launch per phase for all the simulations on the canvas.  Simulation i's blocks in a launch are start[i] ..
+// start[i + 1] - 1, numbered row-major over its own grid of 32 x 8 blocks as its own launches number them, so
+// that every per-block partial, and its place in the in-order sums, is the same as in its own warm start.
+struct WarmSim {
+    UnetFeatureArgs a;
+    float *res32, *prev32, *sigma;
+    unsigned char *mask, *maskc;
+    double2* epart;     // the guard's partials, one per thread block, its decision after them
+    bf16* x0;           // the simulation's rectangle on the canvas (row pitch cs coarse pixels)
+    const float* outc;  // its prediction on the canvas
+    int cs, f;          // canvas pitch, coarsening
+    int fgx, fgy;       // the simulation's grid of 32 x 8 thread blocks
+};
+// The simulation whose block range holds block b (start[0] = 0 <= b < start[n]).
+EFL_DEV int warm_sim_of(const int* start, int n, int b) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (start[mid] <= b)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+// The phases after the forward pass, one thread per fine cell: simulation i owns blocks start[i] .. start[i + 1] - 1.
+__global__ void __launch_bounds__(256) k_warm_batch_guard_residual(const WarmSim* S, const int* start, int n) {
+    const int i = warm_sim_of(start, n, blockIdx.x), t = blockIdx.x - start[i];
+    const WarmSim w = S[i];
+    unet_guard_residual_blk(w.a, w.prev32, w.mask, w.outc, w.cs, w.sigma, w.f, w.epart, t % w.fgx, t / w.fgx, w.fgx);
+}
+__global__ void __launch_bounds__(UNET_RED_THREADS) k_warm_batch_guard(const WarmSim* S) {
+    const WarmSim w = S[blockIdx.x];
+    const int nb = w.fgx * w.fgy;
+    unet_guard_blk(w.epart, nb, (double*)(w.epart + nb));
+}
+__global__ void __launch_bounds__(256) k_warm_batch_apply(const WarmSim* S, const int* start, int n) {
+    const int i = warm_sim_of(start, n, blockIdx.x), t = blockIdx.x - start[i];
+    const WarmSim w = S[i];
+    const int nb = w.fgx * w.fgy;
+    unet_apply_warm_blk(w.a.prev, w.outc, w.cs, w.mask, w.sigma, (const double*)(w.epart + nb), w.a.nx, w.a.ny, w.f,
+                        t % w.fgx, t / w.fgx);
+}
+
 // Coarse training target: the mean of (p - p_prev) / sigma over the block's counted cells (0 if none).
 __global__ void k_unet_target_coarse(Plane<double> x, const float* prev32, const unsigned char* mask,
                                      const float* sigma, int nx, int ny, int f, float* targetc) {
