@@ -981,7 +981,8 @@ efl_status unet_features(efl_sim* s, bf16* x0 = nullptr, int cs = 0) {
         return set_err(s, EFL_ERR_STATE, "the network's coarsening changed after efl_batch_attach_unet: attach again");
     const dim3 g = grid2d(s->nx, s->ny, kBlock);
     const UnetFeatureArgs a = unet_feature_args(s);
-    k_unet_residual<<<g, kBlock, count_launch(), s->stream>>>(a, n.res32, n.prev32, n.mask, n.lpart);
+    k_unet_residual<<<g, kBlock, count_launch(), s->stream>>>(a, n.res32, n.prev32, n.mask, n.lpart,
+                                                              f > 1 ? n.epart : nullptr);
     k_unet_sigma<<<1, UNET_RED_THREADS, count_launch(), s->stream>>>(n.lpart, (int)(g.x * g.y), n.sigma);
     if (f > 1) {
         k_unet_features_coarse<<<g, kBlock, count_launch(), s->stream>>>(n.res32, a, n.mask, n.sigma, f,
@@ -1002,8 +1003,8 @@ efl_status unet_apply(efl_sim* s) {
     if (f > 1) {  // the warm-started iterate formed on the fly for the guard, written only where it is kept
         const int nb = (int)(g.x * g.y);
         double* alpha = (double*)(n.epart + nb);
-        k_unet_guard_residual<<<g, kBlock, count_launch(), s->stream>>>(a, n.prev32, n.mask, n.out, s->nx / f, n.sigma,
-                                                                        f, n.epart);
+        k_unet_guard_residual<<<g, kBlock, count_launch(), s->stream>>>(a, n.mask, n.out, s->nx / f, n.sigma, f,
+                                                                        n.epart);
         k_unet_guard<<<1, UNET_RED_THREADS, count_launch(), s->stream>>>(n.epart, nb, alpha);
         k_unet_apply_warm<<<g, kBlock, count_launch(), s->stream>>>(L.x, n.out, s->nx / f, n.mask, n.sigma, alpha,
                                                                     s->nx, s->ny, f);
@@ -2578,14 +2579,10 @@ efl_status warm_upload(efl_batch* b, const std::vector<int>& on) {
         const UNet& v = *s->unet_view;
         WarmSim& w = hw[k];
         w.a = unet_feature_args(s);
-        w.res32 = v.res32;
-        w.prev32 = v.prev32;
         w.sigma = v.sigma;
         w.mask = v.mask;
-        w.maskc = v.maskc;
         w.epart = v.epart;
         const size_t off = ((size_t)b->corigin[on[k]].y * b->cw + b->corigin[on[k]].x) * 16;
-        w.x0 = b->canvas->X0 + off;
         w.outc = b->canvas->out + off;
         w.cs = b->cw;
         w.f = v.coarse;

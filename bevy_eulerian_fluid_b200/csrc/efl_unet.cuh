@@ -150,6 +150,7 @@ struct ConvArgs {
     int relu;
     int H, W, cin, cout;
     int* err;
+    const unsigned char* gap = nullptr;  // [H*W]: 0 = a canvas gap pixel, whose outputs are written as zeros
 };
 
 // 16-byte asynchronous copy global -> shared through L1 (the nine taps of a
@@ -299,6 +300,7 @@ __global__ void __launch_bounds__(CV_THREADS) k_conv3x3_tc(ConvArgs a) {
             for (int i = 0; i < 16; ++i) {
                 float t = v[i] + (a.bias ? a.bias[c0 + i] : 0.0f);
                 if (a.relu) t = fmaxf(t, 0.0f);
+                if (a.gap && !a.gap[pp]) t = 0.0f;
                 v[i] = t;
             }
             if (a.y) {
@@ -471,6 +473,7 @@ __global__ void __launch_bounds__(CV_THREADS * TILES) k_conv3x3_rows(ConvArgs a)
             for (int i = 0; i < 16; ++i) {
                 float tv = v[i] + (a.bias ? a.bias[c0 + i] : 0.0f);
                 if (a.relu) tv = fmaxf(tv, 0.0f);
+                if (a.gap && !a.gap[pp]) tv = 0.0f;
                 v[i] = tv;
             }
             if (a.y) {
@@ -774,10 +777,29 @@ struct UnetFeatureArgs {
 // residual.wgsl:33-54 in factored form, as the mixed solve builds it), the
 // mask, prev32 = prev, and per-block partial sums (res^2, count).
 // (Block (bx, by) of a grid bgx blocks wide; a batch's launch covers several simulations' grids.)
+// The sum of the squares of the four 8 x 8 guard-block sums of v over a block of 32 x 8 threads (the 8 cells of a
+// row by shuffles, then the 8 rows in order), returned by thread 0; every thread of the block calls it.
+EFL_DEV double guard_block_squares(double v) {
+    __shared__ double rsum[8][4];
+    for (int o = 1; o < 8; o <<= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 7) == 0) rsum[threadIdx.y][threadIdx.x >> 3] = v;
+    __syncthreads();
+    double acc = 0.0;
+    if (threadIdx.x == 0 && threadIdx.y == 0)
+        for (int k = 0; k < 4; ++k) {
+            double sp = 0.0;
+            for (int r = 0; r < 8; ++r) sp += rsum[r][k];
+            acc += sp * sp;
+        }
+    return acc;
+}
+// With epart (the coarse warm start; blocks of 32 x 8 threads), also the guard's "before" half: the squared
+// 8 x 8 block sums of the start iterate's unscaled residual, into epart[block].x.
 EFL_DEV void unet_residual_blk(const UnetFeatureArgs& a, float* res, float* prev32, unsigned char* mask, float2* part,
-                               int bx, int by, int bgx) {
+                               double2* epart, int bx, int by, int bgx) {
     const int gx = bx * blockDim.x + threadIdx.x, gy = by * blockDim.y + threadIdx.y;
     float r2 = 0.0f, c = 0.0f;
+    double rd = 0.0;
     if (gx < a.nx && gy < a.ny) {
         const size_t p = (size_t)gy * a.nx + gx;
         const float phi = a.ls.at(gx, gy);
@@ -800,7 +822,8 @@ EFL_DEV void unet_residual_blk(const UnetFeatureArgs& a, float* res, float* prev
                     }
                 }
             }
-            rv = (float)(a.cdiv * (a.b.at(gx, gy) - a.factor * (den * a.prev.at(gx, gy) - sum)));
+            rd = a.b.at(gx, gy) - a.factor * (den * a.prev.at(gx, gy) - sum);
+            rv = (float)(a.cdiv * rd);
             r2 = rv * rv;
             c = 1.0f;
         }
@@ -822,10 +845,14 @@ EFL_DEV void unet_residual_blk(const UnetFeatureArgs& a, float* res, float* prev
         }
         part[by * bgx + bx] = s2;
     }
+    if (epart) {
+        const double sq = guard_block_squares(rd);
+        if (t == 0) epart[by * bgx + bx].x = sq;
+    }
 }
 __global__ void __launch_bounds__(256) k_unet_residual(UnetFeatureArgs a, float* res, float* prev32, unsigned char* mask,
-                                                        float2* part) {
-    unet_residual_blk(a, res, prev32, mask, part, blockIdx.x, blockIdx.y, gridDim.x);
+                                                        float2* part, double2* epart) {
+    unet_residual_blk(a, res, prev32, mask, part, epart, blockIdx.x, blockIdx.y, gridDim.x);
 }
 // The in-order sums of a block's reductions: thread t adds partials t, t + 256, ... in turn, then a fixed tree
 // over the 256 threads (blocks of 256 threads; the same order for a simulation alone and in a batch).
@@ -1068,17 +1095,13 @@ EFL_DEV double unet_warm_value(const Plane<double>& x, const float* outc, int cs
                ? __dadd_rn(v, __dmul_rn((double)sigma, (double)unet_coarse_pred(outc, cs, nx, ny, f, gx, gy)))
                : v;
 }
-// The guard's block residuals of the coarse warm start, one thread per fine cell (blocks of 32 x 8 threads; the
-// guard blocks are 8 x 8, four to a thread block): the residual of the start iterate (prev32) and of the
-// warm-started one, formed on the fly from the coarse prediction (x is still the start iterate) with a one-cell
-// halo in shared memory; each summed over its guard block (the 8 cells of a row by shuffles, then the 8 rows in
-// order) and squared, the four squares added: one partial per thread block.
-EFL_DEV void unet_guard_residual_blk(const UnetFeatureArgs& a, const float* prev32, const unsigned char* mask,
-                                     const float* outc, int cs, const float* sigma, int f, double2* part, int bx,
-                                     int by, int bgx) {
+// The guard's "after" half for the coarse warm start, one thread per fine cell (blocks of 32 x 8 threads): the
+// residual of the warm-started iterate, formed on the fly from the coarse prediction (x is still the start
+// iterate) with a one-cell halo in shared memory, summed over the 8 x 8 guard blocks and squared, into
+// part[block].y (the residual kernel wrote the start iterate's half into .x, in the same order).
+EFL_DEV void unet_guard_residual_blk(const UnetFeatureArgs& a, const unsigned char* mask, const float* outc, int cs,
+                                     const float* sigma, int f, double2* part, int bx, int by, int bgx) {
     __shared__ double wv[10][34];
-    __shared__ float pv[10][34];
-    __shared__ double2 rs[8][4];
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
     const int X0 = bx * 32 - 1, Y0 = by * 8 - 1;
     const float sg = *sigma;
@@ -1086,17 +1109,16 @@ EFL_DEV void unet_guard_residual_blk(const UnetFeatureArgs& a, const float* prev
         const int ly = i / 34, lx = i - ly * 34, hx = X0 + lx, hy = Y0 + ly;
         const bool in = (unsigned)hx < (unsigned)a.nx && (unsigned)hy < (unsigned)a.ny;
         wv[ly][lx] = in ? unet_warm_value(a.prev, outc, cs, mask, sg, a.nx, a.ny, f, hx, hy) : 0.0;
-        pv[ly][lx] = in ? prev32[(size_t)hy * a.nx + hx] : 0.0f;
     }
     __syncthreads();
     const int gx = bx * 32 + tx, gy = by * 8 + ty;
-    double rp = 0.0, rx = 0.0;
+    double rx = 0.0;
     if (gx < a.nx && gy < a.ny) {
         const float phi = a.ls.at(gx, gy);
         const float fq[4] = {a.fu.at(gx, gy), a.fu.at(gx + 1, gy), a.fv.at(gx, gy), a.fv.at(gx, gy + 1)};
         if (phi < 0.0f && !(fq[0] == 0.0f && fq[1] == 0.0f && fq[2] == 0.0f && fq[3] == 0.0f)) {
             const int ox[4] = {-1, 1, 0, 0}, oy[4] = {0, 0, -1, 1};
-            double den = 0.0, s1 = 0.0, s2 = 0.0;
+            double den = 0.0, s2 = 0.0;
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
                 const int jx = gx + ox[q], jy = gy + oy[q];
@@ -1104,42 +1126,22 @@ EFL_DEV void unet_guard_residual_blk(const UnetFeatureArgs& a, const float* prev
                     const float level = a.ls.at(jx, jy);
                     if (level < 0.0f) {
                         den += (double)fq[q];
-                        s1 += (double)fq[q] * (double)pv[ty + 1 + oy[q]][tx + 1 + ox[q]];
                         s2 += (double)fq[q] * wv[ty + 1 + oy[q]][tx + 1 + ox[q]];
                     } else {
                         den += (double)fq[q] * (1.0 - (double)level / (double)phi);
                     }
                 }
             }
-            const double bb = a.b.at(gx, gy);
-            rp = bb - a.factor * (den * (double)pv[ty + 1][tx + 1] - s1);
-            rx = bb - a.factor * (den * wv[ty + 1][tx + 1] - s2);
+            rx = a.b.at(gx, gy) - a.factor * (den * wv[ty + 1][tx + 1] - s2);
         }
     }
-    for (int o = 1; o < 8; o <<= 1) {
-        rp += __shfl_xor_sync(0xffffffffu, rp, o);
-        rx += __shfl_xor_sync(0xffffffffu, rx, o);
-    }
-    if ((tx & 7) == 0) rs[ty][tx >> 3] = make_double2(rp, rx);
-    __syncthreads();
-    if (tid == 0) {
-        double a1 = 0.0, a2 = 0.0;
-        for (int k = 0; k < 4; ++k) {
-            double sp = 0.0, sx = 0.0;
-            for (int r = 0; r < 8; ++r) {
-                sp += rs[r][k].x;
-                sx += rs[r][k].y;
-            }
-            a1 += sp * sp;
-            a2 += sx * sx;
-        }
-        part[by * bgx + bx] = make_double2(a1, a2);
-    }
+    const double sq = guard_block_squares(rx);
+    if (tid == 0) part[by * bgx + bx].y = sq;
 }
-__global__ void __launch_bounds__(256) k_unet_guard_residual(UnetFeatureArgs a, const float* prev32,
-                                                             const unsigned char* mask, const float* outc, int cs,
-                                                             const float* sigma, int f, double2* part) {
-    unet_guard_residual_blk(a, prev32, mask, outc, cs, sigma, f, part, blockIdx.x, blockIdx.y, gridDim.x);
+__global__ void __launch_bounds__(256) k_unet_guard_residual(UnetFeatureArgs a, const unsigned char* mask,
+                                                             const float* outc, int cs, const float* sigma, int f,
+                                                             double2* part) {
+    unet_guard_residual_blk(a, mask, outc, cs, sigma, f, part, blockIdx.x, blockIdx.y, gridDim.x);
 }
 // Where the guard kept it (*alpha != 0), the coarse warm start written into the iterate.
 EFL_DEV void unet_apply_warm_blk(const Plane<double>& x, const float* outc, int cs, const unsigned char* mask,
@@ -1160,11 +1162,10 @@ __global__ void k_unet_apply_warm(Plane<double> x, const float* outc, int cs, co
 // that every per-block partial, and its place in the in-order sums, is the same as in its own warm start.
 struct WarmSim {
     UnetFeatureArgs a;
-    float *res32, *prev32, *sigma;
-    unsigned char *mask, *maskc;
+    float* sigma;
+    unsigned char* mask;
     double2* epart;     // the guard's partials, one per thread block, its decision after them
-    bf16* x0;           // the simulation's rectangle on the canvas (row pitch cs coarse pixels)
-    const float* outc;  // its prediction on the canvas
+    const float* outc;  // the simulation's prediction on the canvas (row pitch cs coarse pixels)
     int cs, f;          // canvas pitch, coarsening
     int fgx, fgy;       // the simulation's grid of 32 x 8 thread blocks
 };
@@ -1184,7 +1185,7 @@ EFL_DEV int warm_sim_of(const int* start, int n, int b) {
 __global__ void __launch_bounds__(256) k_warm_batch_guard_residual(const WarmSim* S, const int* start, int n) {
     const int i = warm_sim_of(start, n, blockIdx.x), t = blockIdx.x - start[i];
     const WarmSim w = S[i];
-    unet_guard_residual_blk(w.a, w.prev32, w.mask, w.outc, w.cs, w.sigma, w.f, w.epart, t % w.fgx, t / w.fgx, w.fgx);
+    unet_guard_residual_blk(w.a, w.mask, w.outc, w.cs, w.sigma, w.f, w.epart, t % w.fgx, t / w.fgx, w.fgx);
 }
 __global__ void __launch_bounds__(UNET_RED_THREADS) k_warm_batch_guard(const WarmSim* S) {
     const WarmSim w = S[blockIdx.x];
@@ -1525,8 +1526,9 @@ inline void conv3x3_launch(const ConvArgs& a, cudaStream_t st) {
 }
 
 inline void unet_conv(UNet& n, int i, const bf16* x, int xs, int xo, int H, int W, bf16* y, int ys, int yo,
-                      float* yf, cudaStream_t st) {
+                      float* yf, cudaStream_t st, const unsigned char* gap = nullptr) {
     ConvArgs a;
+    a.gap = gap;
     a.x = x;
     a.xs = xs;
     a.xo = xo;
@@ -1545,29 +1547,14 @@ inline void unet_conv(UNet& n, int i, const bf16* x, int xs, int xo, int H, int 
     conv3x3_launch(a, st);
 }
 
-// Zeroes channels [yo, yo + C) of the pixels that lie in no simulation's rectangle (m[p] == 0): the gaps of a
-// batch's canvas stay zero after every convolution, so that each simulation's image sees zeros around it,
-// as the zero padding of its own forward.
-__global__ void k_canvas_zero(bf16* y, int ys, int yo, int C, const unsigned char* m, int npix) {
-    const int g8 = C / 8;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;  // over npix * C / 8
-    if (i >= npix * g8) return;
-    const int q = i / g8, g = i - q * g8;
-    if (m[q]) return;
-    *reinterpret_cast<uint4*>(y + (size_t)q * ys + yo + 8 * g) = make_uint4(0u, 0u, 0u, 0u);
-}
-
 // The forward pass over an H x W image (H and W multiples of 8).  With `gaps` (four masks, one per level, of a
-// canvas whose rectangles start and end on multiples of 8) the gaps are zeroed after each convolution that
-// feeds another; average pooling and nearest upsampling keep them zero by themselves.
+// canvas whose rectangles start and end on multiples of 8) every convolution that feeds another writes zeros
+// at the gap pixels, so that each rectangle sees zeros around it, as the zero padding of its simulation's own
+// forward; average pooling and nearest upsampling keep the gaps zero by themselves.
 inline void unet_forward(UNet& n, int H, int W, cudaStream_t st, const unsigned char* const* gaps = nullptr) {
     const int Hs[4] = {H, H / 2, H / 4, H / 8}, Ws[4] = {W, W / 2, W / 4, W / 8};
     auto conv = [&](int i, const bf16* x, int xs, int lvl, bf16* y, int ys, int yo) {
-        unet_conv(n, i, x, xs, 0, Hs[lvl], Ws[lvl], y, ys, yo, nullptr, st);
-        if (gaps) {
-            const int np = Hs[lvl] * Ws[lvl], c = kUnetSpec[i].cout;
-            k_canvas_zero<<<lin_grid((size_t)np * c / 8), 256, count_launch(), st>>>(y, ys, yo, c, gaps[lvl], np);
-        }
+        unet_conv(n, i, x, xs, 0, Hs[lvl], Ws[lvl], y, ys, yo, nullptr, st, gaps ? gaps[lvl] : nullptr);
     };
     auto pool = [&](const bf16* in, int is, int io, int lvl, int C, bf16* out) {  // level lvl -> lvl + 1
         k_pool2<<<lin_grid((size_t)Hs[lvl + 1] * Ws[lvl + 1] * C / 8), 256, count_launch(), st>>>(in, is, io, Hs[lvl],
