@@ -1252,26 +1252,44 @@ __global__ void k_fim_phase_b(PF T, PU LT, PF S, PU L, Dom d) {
     }
 }
 
-// All iterations of the two-phase FIM update (k_fim_phase_a then
-// k_fim_phase_b, `iters` times) in one launch, temporally blocked: a CTA
-// holds its 32 x 32 tile plus a halo of FIM_HALO cells in shared memory and
-// runs the iterations there.  One iteration's result at a cell depends on
-// cells at most 2 away (phase A reads radius 1, phase B reads phase A's
-// result at radius 1), so values go wrong only near the image edge, 2 cells
-// deeper per iteration: with iters <= FIM_HALO / 2 the owned tile is exact.
-// A cell changes only while it is active, and activity spreads one cell per
-// iteration, so a tile whose image holds no active cell is left untouched
-// (most of a large grid, away from the interface): such CTAs read the labels
-// and leave.
-constexpr int FIM_TILE = 32, FIM_HALO = 20, FIM_IMG = FIM_TILE + 2 * FIM_HALO, FIM_THREADS = 512;
-constexpr size_t FIM_SMEM = (size_t)4 * FIM_IMG * FIM_IMG * 4;
-// tile_active: the flags k_fim_active left (a tile whose 3 x 3 neighbourhood holds no active cell has none in
-// its image, FIM_HALO < FIM_TILE, and leaves at once); valid for the first launch after k_fim_active only.
-__global__ void __launch_bounds__(FIM_THREADS) k_fim_tiled(PF S, PU L, Dom d, int iters, int tiles_x,
-                                                           const unsigned* tile_active) {
+// Iterations of the two-phase FIM update (k_fim_phase_a then k_fim_phase_b,
+// `iters` times) in one launch, temporally blocked: a CTA holds its 32 x 32
+// tile plus a halo of HALO cells in shared memory and runs the iterations
+// there.  One iteration's result at a cell depends on cells at most 2 away
+// (phase A reads radius 1, phase B reads phase A's result at radius 1), so
+// values go wrong only near the image edge, 2 cells deeper per iteration:
+// with iters <= HALO / 2 the owned tile is exact.  A cell changes only while
+// it is active, and activity spreads one cell per iteration, so a tile whose
+// image holds no active cell is left untouched (most of a large grid, away
+// from the interface): such CTAs read the labels and leave.  Two halos: 20
+// (the 10 iterations in one launch; large grids, where most tiles leave at
+// once) and 4 (2 iterations per launch, 1.56x the owned cells in the image;
+// small grids, where a 72 x 72 image per 32 x 32 tile would be 5x the work).
+constexpr int FIM_TILE = 32, FIM_HALO = 20, FIM_THREADS = 512, FIM_HALO_NARROW = 4, FIM_THREADS_NARROW = 256;
+__host__ __device__ constexpr size_t fim_smem(int halo) {
+    return (size_t)4 * (FIM_TILE + 2 * halo) * (FIM_TILE + 2 * halo) * 4;
+}
+constexpr size_t FIM_SMEM = fim_smem(FIM_HALO);
+// Each launch reads (S, L) and writes its tiles into (SD, LD), another pair of planes: a CTA that started late
+// must still see its neighbours' values of the launch's start in its halo.  A tile that leaves early copies its
+// cells across.  tile_active: the flags k_fim_active left (a tile whose 3 x 3 neighbourhood holds no active
+// cell has none in its image, HALO < FIM_TILE, and leaves at once); valid for the first launch only.
+template <int HALO, int THREADS>
+__global__ void __launch_bounds__(THREADS) k_fim_tiled(PF S, PU L, PF SD, PU LD, Dom d, int iters, int tiles_x,
+                                                       const unsigned* tile_active) {
     extern __shared__ __align__(16) unsigned char fim_raw[];
-    constexpr int N = FIM_IMG * FIM_IMG;
-    static_assert(FIM_HALO < FIM_TILE, "the image lies within the 3 x 3 tiles around the owned one");
+    constexpr int FIM_IMG = FIM_TILE + 2 * HALO, N = FIM_IMG * FIM_IMG;
+    static_assert(HALO < FIM_TILE, "the image lies within the 3 x 3 tiles around the owned one");
+    auto copy_across = [&]() {  // the owned tile unchanged
+        const int tx0 = (int)(blockIdx.x % tiles_x) * FIM_TILE, ty0 = (int)(blockIdx.x / tiles_x) * FIM_TILE;
+        for (int i = threadIdx.x; i < FIM_TILE * FIM_TILE; i += THREADS) {
+            const int gx = tx0 + i % FIM_TILE, gy = ty0 + i / FIM_TILE;
+            if (gx < d.nx && gy < d.ny) {
+                SD.at(gx, gy) = S.at(gx, gy);
+                LD.at(gx, gy) = L.at(gx, gy);
+            }
+        }
+    };
     if (tile_active) {
         const int tiles_y = (d.ny + FIM_TILE - 1) / FIM_TILE;
         int any = 0;
@@ -1280,24 +1298,30 @@ __global__ void __launch_bounds__(FIM_THREADS) k_fim_tiled(PF S, PU L, Dom d, in
             const int ty = (int)(blockIdx.x / tiles_x) - 1 + (int)threadIdx.x / 3;
             if (tx >= 0 && ty >= 0 && tx < tiles_x && ty < tiles_y) any = tile_active[ty * tiles_x + tx] != 0u;
         }
-        if (!__syncthreads_or(any)) return;
+        if (!__syncthreads_or(any)) {
+            copy_across();
+            return;
+        }
     }
     float* s = reinterpret_cast<float*>(fim_raw);
     float* t = s + N;
     uint32_t* l = reinterpret_cast<uint32_t*>(t + N);
     uint32_t* lt = l + N;
-    const int x0 = (int)(blockIdx.x % tiles_x) * FIM_TILE - FIM_HALO, y0 = (int)(blockIdx.x / tiles_x) * FIM_TILE - FIM_HALO;
+    const int x0 = (int)(blockIdx.x % tiles_x) * FIM_TILE - HALO, y0 = (int)(blockIdx.x / tiles_x) * FIM_TILE - HALO;
     const int W = d.nx, H = d.ny;  // the dispatch domain (sizes are multiples of 8) and the planes' extent
     int act = 0;
-    for (int i = threadIdx.x; i < N; i += FIM_THREADS) {
+    for (int i = threadIdx.x; i < N; i += THREADS) {
         const int gx = x0 + i % FIM_IMG, gy = y0 + i / FIM_IMG;
         const bool in = gx >= 0 && gy >= 0 && gx < W && gy < H;
         const uint32_t lv = in ? L.at(gx, gy) : LABEL_NONE;
         l[i] = lv;
         act |= lv == LABEL_ACTIVE;
     }
-    if (!__syncthreads_or(act)) return;
-    for (int i = threadIdx.x; i < N; i += FIM_THREADS) {
+    if (!__syncthreads_or(act)) {
+        copy_across();
+        return;
+    }
+    for (int i = threadIdx.x; i < N; i += THREADS) {
         const int gx = x0 + i % FIM_IMG, gy = y0 + i / FIM_IMG;
         s[i] = (gx >= 0 && gy >= 0 && gx < W && gy < H) ? S.at(gx, gy) : 0.0f;
     }
@@ -1319,7 +1343,7 @@ __global__ void __launch_bounds__(FIM_THREADS) k_fim_tiled(PF S, PU L, Dom d, in
         return 0.5f * (xm + ym + sqrtf(2.0f - dd * dd));
     };
     for (int it = 0; it < iters; ++it) {
-        for (int i = threadIdx.x; i < N; i += FIM_THREADS) {  // phase A
+        for (int i = threadIdx.x; i < N; i += THREADS) {  // phase A
             const int ix = i % FIM_IMG, iy = i / FIM_IMG;
             const uint32_t lv = l[i];
             const float p = s[i];
@@ -1333,7 +1357,7 @@ __global__ void __launch_bounds__(FIM_THREADS) k_fim_tiled(PF S, PU L, Dom d, in
             }
         }
         __syncthreads();
-        for (int i = threadIdx.x; i < N; i += FIM_THREADS) {  // phase B
+        for (int i = threadIdx.x; i < N; i += THREADS) {  // phase B
             const int ix = i % FIM_IMG, iy = i / FIM_IMG;
             const int gx = x0 + ix, gy = y0 + iy;
             const uint32_t lv = lt[i];
@@ -1368,12 +1392,12 @@ __global__ void __launch_bounds__(FIM_THREADS) k_fim_tiled(PF S, PU L, Dom d, in
         }
         __syncthreads();
     }
-    for (int i = threadIdx.x; i < FIM_TILE * FIM_TILE; i += FIM_THREADS) {
-        const int ix = FIM_HALO + i % FIM_TILE, iy = FIM_HALO + i / FIM_TILE;
+    for (int i = threadIdx.x; i < FIM_TILE * FIM_TILE; i += THREADS) {
+        const int ix = HALO + i % FIM_TILE, iy = HALO + i / FIM_TILE;
         const int gx = x0 + ix, gy = y0 + iy;
         if (gx < W && gy < H) {
-            S.at(gx, gy) = s[iy * FIM_IMG + ix];
-            L.at(gx, gy) = l[iy * FIM_IMG + ix];
+            SD.at(gx, gy) = s[iy * FIM_IMG + ix];
+            LD.at(gx, gy) = l[iy * FIM_IMG + ix];
         }
     }
 }

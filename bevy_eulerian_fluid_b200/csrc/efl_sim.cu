@@ -144,6 +144,7 @@ struct efl_sim {
     PF mix_d2{};       // second correction buffer (batched solve)
     PF xbuf{};         // second halo-exchange plane of the persistent solves, allocated on first use
     bool owns_stream = true;
+    bool batch_member = false;  // its stages run beside the other simulations' (a batch's fan-out)
     float* d_vel = nullptr;  // velocity-magnitude partials (efl_velocity_magnitude)
     int cap_vel = 0;
     efl_rigid_body* d_rigid = nullptr;  // device-integrated bodies (efl_set_rigid_bodies)
@@ -331,7 +332,8 @@ bool fim_tiled_ready() {
     static int state[64] = {};  // 0 unknown, 1 ready, 2 refused
     if (dev < 0 || dev >= 64) return false;
     if (!state[dev]) {
-        state[dev] = cudaFuncSetAttribute(k_fim_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FIM_SMEM) ==
+        state[dev] = cudaFuncSetAttribute(k_fim_tiled<FIM_HALO, FIM_THREADS>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FIM_SMEM) ==
                              cudaSuccess
                          ? 1
                          : 2;
@@ -340,12 +342,13 @@ bool fim_tiled_ready() {
     return state[dev] == 1;
 }
 
-// Which FIM form runs: EFL_FIM_TILED=1 the temporally blocked kernel at every size, =0 the per-phase launches at
-// every size, unset (or anything else) the size rule in st_reinit.  Both forms give bit-identical level sets.
-int fim_tiled_override() {
+// Which FIM form runs: EFL_FIM_TILED=0 the per-phase launches, =1 the temporally blocked kernel with the
+// 20-cell halo (10 iterations per launch), =2 the one with the 4-cell halo (2 per launch), at every size; unset
+// (or anything else) the size rule in st_reinit.  All forms give bit-identical level sets.
+int fim_form_override() {
     static const int v = [] {
         const char* e = std::getenv("EFL_FIM_TILED");
-        return e && e[0] == '1' && !e[1] ? 1 : e && e[0] == '0' && !e[1] ? 0 : -1;
+        return e && e[0] >= '0' && e[0] <= '2' && !e[1] ? e[0] - '0' : -1;
     }();
     return v;
 }
@@ -363,20 +366,39 @@ efl_status st_reinit(efl_sim* s) {  // reinitialize_levelset.rs:162-243
         s->seeds_final = src;
         k_jfa_sdf<<<g, kBlock, count_launch(), s->stream>>>(s->seeds[src], s->ls1, s->ls0, d);
     } else {
-        k_fim_init<<<g, kBlock, count_launch(), s->stream>>>(s->ls1, s->ls0, s->lab0, d);
         const int tx = (d.nx + FIM_TILE - 1) / FIM_TILE, ty = (d.ny + FIM_TILE - 1) / FIM_TILE;
-        // The tiled form pays where the grid is large and the interface a small part of it (C3: 4096^2);
-        // on small grids the per-phase launches are cheaper (the tiles hold the interface almost everywhere).
-        const int force = fim_tiled_override();
-        const bool tiled = (force < 0 ? tx * ty >= 4 * s->solver.num_sms : force == 1) && fim_tiled_ready();
-        if (tiled) CU(cudaMemsetAsync(s->d_fimtiles, 0, (size_t)tx * ty * sizeof(unsigned), s->stream));
-        k_fim_active<<<g, kBlock, count_launch(), s->stream>>>(s->lab0, s->lab, d, tiled ? s->d_fimtiles : nullptr,
+        // The wide halo pays where the grid is large and the interface a small part of it (C3: 4096^2: one
+        // launch, most tiles leave at once).  On small grids a simulation stepped alone is latency-bound and
+        // takes the per-phase launches (each shorter than a tiled launch); a batch member, whose launches run
+        // beside the other simulations', takes the narrow halo (a quarter of the launches, a fifth of the
+        // traffic).
+        const int force = fim_form_override();
+        int form = force >= 0 ? force : tx * ty >= 4 * s->solver.num_sms ? 1 : s->batch_member ? 2 : 0;
+        if (form == 1 && !fim_tiled_ready()) form = 2;
+        const uint32_t iters = s->cfg.reinit.fim_iterations;
+        const int per = form == 1 ? FIM_HALO / 2 : FIM_HALO_NARROW / 2;
+        const int launches = form ? (int)((iters + per - 1) / per) : 0;
+        // The tiled launches alternate between (ls0, lab) and (phiT, labT) and must end in (ls0, lab): the
+        // start state goes into the pair that makes the last launch land there.
+        PF S[2] = {s->ls0, s->phiT};
+        PU L[2] = {s->lab, s->labT};
+        const int first = launches & 1;
+        k_fim_init<<<g, kBlock, count_launch(), s->stream>>>(s->ls1, S[first], s->lab0, d);
+        if (form) CU(cudaMemsetAsync(s->d_fimtiles, 0, (size_t)tx * ty * sizeof(unsigned), s->stream));
+        k_fim_active<<<g, kBlock, count_launch(), s->stream>>>(s->lab0, L[first], d, form ? s->d_fimtiles : nullptr,
                                                                 tx);
-        if (tiled) {  // the iterations, FIM_HALO / 2 per launch
-            for (uint32_t k = 0; k < s->cfg.reinit.fim_iterations; k += FIM_HALO / 2) {
-                const int n = (int)std::min<uint32_t>(FIM_HALO / 2, s->cfg.reinit.fim_iterations - k);
-                k_fim_tiled<<<tx * ty, FIM_THREADS, FIM_SMEM + count_launch(), s->stream>>>(
-                    s->ls0, s->lab, d, n, tx, k == 0 ? s->d_fimtiles : nullptr);
+        if (form) {  // the iterations, halo / 2 per launch
+            int cur = first;
+            for (uint32_t k = 0; k < iters; k += per, cur ^= 1) {
+                const int n = (int)std::min<uint32_t>(per, iters - k);
+                const unsigned* act = k == 0 ? s->d_fimtiles : nullptr;
+                if (form == 1)
+                    k_fim_tiled<FIM_HALO, FIM_THREADS><<<tx * ty, FIM_THREADS, FIM_SMEM + count_launch(), s->stream>>>(
+                        S[cur], L[cur], S[cur ^ 1], L[cur ^ 1], d, n, tx, act);
+                else
+                    k_fim_tiled<FIM_HALO_NARROW, FIM_THREADS_NARROW>
+                        <<<tx * ty, FIM_THREADS_NARROW, fim_smem(FIM_HALO_NARROW) + count_launch(), s->stream>>>(
+                            S[cur], L[cur], S[cur ^ 1], L[cur ^ 1], d, n, tx, act);
             }
         } else {
             for (uint32_t k = 0; k < s->cfg.reinit.fim_iterations; ++k) {
@@ -2400,6 +2422,7 @@ efl_status efl_batch_create(const efl_config* cfgs, uint32_t n, efl_batch** out)
         cudaStreamDestroy(s->stream);
         s->stream = b->stream;
         s->owns_stream = false;
+        s->batch_member = true;
         b->sims.push_back(s);
         if (ensure_mix_planes(s) != EFL_OK) {
             std::string m = s->err;
