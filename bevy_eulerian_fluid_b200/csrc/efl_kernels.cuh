@@ -288,7 +288,7 @@ EFL_DEV float2 runge_kutta(const PF& u, const PF& v, float px, float py, float d
     return make_float2(px - dt * wx, py - dt * wy);
 }
 // advect_velocity.wgsl:11-27 (x-major) and :29-45 (y-major)
-__global__ void k_advect_u(PF u0, PF v0, PF u1, float dt, Dom d) {
+EFL_DEV void advect_u_at(const PF& u0, const PF& v0, const PF& u1, float dt, const Dom& d) {
     int x = gx(), y = gy();
     if (x > d.nx || y >= d.xrows()) return;
     float px = (float)x + -0.5f, py = (float)y + 0.0f;
@@ -297,7 +297,7 @@ __global__ void k_advect_u(PF u0, PF v0, PF u1, float dt, Dom d) {
     bool inside = b.x >= 0.0f && b.y >= 0.0f && b.x <= dimx - 1.0f && b.y <= dimy - 1.0f;
     u1.st(x, y, inside ? interp_edge_x(u0, b.x, b.y) : u0.ld(x, y));
 }
-__global__ void k_advect_v(PF u0, PF v0, PF v1, float dt, Dom d) {
+EFL_DEV void advect_v_at(const PF& u0, const PF& v0, const PF& v1, float dt, const Dom& d) {
     int x = gx(), y = gy();
     if (x >= d.ycols() || y > d.ny) return;
     float px = (float)x + 0.0f, py = (float)y + -0.5f;
@@ -305,6 +305,13 @@ __global__ void k_advect_v(PF u0, PF v0, PF v1, float dt, Dom d) {
     float dimx = (float)v0.w, dimy = (float)v0.h;
     bool inside = b.x >= 0.0f && b.y >= 0.0f && b.x <= dimx - 1.0f && b.y <= dimy - 1.0f;
     v1.st(x, y, inside ? interp_edge_y(v0, b.x, b.y) : v0.ld(x, y));
+}
+// Both passes in one launch over the larger of their grids: blockIdx.z 0 the x-major faces, 1 the y-major ones.
+__global__ void k_advect_uv(PF u0, PF v0, PF u1, PF v1, float dt, Dom d) {
+    if (blockIdx.z == 0)
+        advect_u_at(u0, v0, u1, dt, d);
+    else
+        advect_v_at(u0, v0, v1, dt, d);
 }
 
 // exp for the Gaussian force splat.  WGSL's exp is implementation-defined
@@ -336,8 +343,8 @@ EFL_DEV float gaussian_2d(float x, float y, float x0, float y0, float sigma) {
 }
 // apply_forces.wgsl:17-43 / 45-71 (comp 0 = u, x-major; comp 1 = v, y-major)
 template <int COMP>
-__global__ void k_apply_forces(PF vel, PF ls0, PF face_frac, const efl_force* __restrict__ forces, int n_forces,
-                               Uniform U, Dom d) {
+EFL_DEV void apply_forces_at(const PF& vel, const PF& ls0, const PF& face_frac, const efl_force* __restrict__ forces,
+                             int n_forces, const Uniform& U, const Dom& d) {
     int x = gx(), y = gy();
     if (COMP == 0 ? (x > d.nx || y >= d.xrows()) : (x >= d.ycols() || y > d.ny)) return;
     float4 f = area_fractions(ls0, x, y);
@@ -356,6 +363,14 @@ __global__ void k_apply_forces(PF vel, PF ls0, PF face_frac, const efl_force* __
     }
     float val = vel.ld(x, y);
     vel.st(x, y, val + net * U.dt / U.dx);
+}
+// Both components in one launch over the larger of their grids (blockIdx.z: 0 = u, 1 = v).
+__global__ void k_apply_forces_uv(PF u, PF v, PF ls0, PF fu, PF fv, const efl_force* __restrict__ forces, int n_forces,
+                                  Uniform U, Dom d) {
+    if (blockIdx.z == 0)
+        apply_forces_at<0>(u, ls0, fu, forces, n_forces, U, d);
+    else
+        apply_forces_at<1>(v, ls0, fv, forces, n_forces, U, d);
 }
 
 // divergence.wgsl:16-42 (fractions of levelset_solid = the face planes)
@@ -779,7 +794,8 @@ __global__ void k_jacobi(PF p_in, PF p_out, PF ls0, PF fu, PF fv, PF div, Unifor
 
 // solve_velocity_u.wgsl:15-47 / solve_velocity_v.wgsl:15-45
 template <int COMP>
-__global__ void k_solve_velocity(PF out0, PF in1, PF solid, PF p0, PF ls0, PF face_frac, Uniform U, Dom d) {
+EFL_DEV void solve_velocity_at(const PF& out0, const PF& in1, const PF& solid, const PF& p0, const PF& ls0,
+                               const PF& face_frac, const Uniform& U, const Dom& d) {
     int x = gx(), y = gy();
     if (COMP == 0 ? (x > d.nx || y >= d.xrows()) : (x >= d.ycols() || y > d.ny)) return;
     const float factor = U.dt / (U.dx * U.rho);
@@ -801,6 +817,14 @@ __global__ void k_solve_velocity(PF out0, PF in1, PF solid, PF p0, PF ls0, PF fa
     }
     float val = in1.ld(x, y);
     out0.st(x, y, val - factor * (pij - pm));
+}
+// Both components in one launch over the larger of their grids (blockIdx.z: 0 = u, 1 = v).
+__global__ void k_solve_velocity_uv(PF u0, PF u1, PF us, PF v0, PF v1, PF vs, PF p0, PF ls0, PF fu, PF fv, Uniform U,
+                                    Dom d) {
+    if (blockIdx.z == 0)
+        solve_velocity_at<0>(u0, u1, us, p0, ls0, fu, U, d);
+    else
+        solve_velocity_at<1>(v0, v1, vs, p0, ls0, fv, U, d);
 }
 
 // extrapolate/initialize_u_valid.wgsl:6-30 / initialize_v_valid.wgsl:6-30

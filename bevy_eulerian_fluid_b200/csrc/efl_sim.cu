@@ -570,17 +570,18 @@ efl_status st_area_fraction(efl_sim* s) {
 }
 efl_status st_advect(efl_sim* s) {
     Dom d = s->dom();
-    k_advect_u<<<grid2d(d.nx + 1, d.ny, kBlock), kBlock, count_launch(), s->stream>>>(s->u0, s->v0, s->u1, s->U.dt, d);
-    k_advect_v<<<grid2d(d.nx, d.ny + 1, kBlock), kBlock, count_launch(), s->stream>>>(s->u0, s->v0, s->v1, s->U.dt, d);
+    dim3 g = grid2d(d.nx + 1, d.ny + 1, kBlock);
+    g.z = 2;  // u and v faces
+    k_advect_uv<<<g, kBlock, count_launch(), s->stream>>>(s->u0, s->v0, s->u1, s->v1, s->U.dt, d);
     LAUNCH_CHECK();
     return EFL_OK;
 }
 efl_status st_apply_forces(efl_sim* s) {
     Dom d = s->dom();
-    k_apply_forces<0><<<grid2d(d.nx + 1, d.ny, kBlock), kBlock, count_launch(), s->stream>>>(s->u1, s->ls0, s->fu, s->d_forces,
-                                                                              s->n_forces, s->U, d);
-    k_apply_forces<1><<<grid2d(d.nx, d.ny + 1, kBlock), kBlock, count_launch(), s->stream>>>(s->v1, s->ls0, s->fv, s->d_forces,
-                                                                               s->n_forces, s->U, d);
+    dim3 g = grid2d(d.nx + 1, d.ny + 1, kBlock);
+    g.z = 2;  // u and v faces
+    k_apply_forces_uv<<<g, kBlock, count_launch(), s->stream>>>(s->u1, s->v1, s->ls0, s->fu, s->fv, s->d_forces,
+                                                                 s->n_forces, s->U, d);
     LAUNCH_CHECK();
     return EFL_OK;
 }
@@ -1146,10 +1147,10 @@ efl_status st_projection(efl_sim* s, efl_step_stats* st) {
 
 efl_status st_solve_velocity(efl_sim* s) {
     Dom d = s->dom();
-    k_solve_velocity<0><<<grid2d(d.nx + 1, d.ny, kBlock), kBlock, count_launch(), s->stream>>>(s->u0, s->u1, s->us, s->p0,
-                                                                                s->ls0, s->fu, s->U, d);
-    k_solve_velocity<1><<<grid2d(d.nx, d.ny + 1, kBlock), kBlock, count_launch(), s->stream>>>(s->v0, s->v1, s->vs, s->p0,
-                                                                                 s->ls0, s->fv, s->U, d);
+    dim3 g = grid2d(d.nx + 1, d.ny + 1, kBlock);
+    g.z = 2;  // u and v faces
+    k_solve_velocity_uv<<<g, kBlock, count_launch(), s->stream>>>(s->u0, s->u1, s->us, s->v0, s->v1, s->vs, s->p0,
+                                                                   s->ls0, s->fu, s->fv, s->U, d);
     LAUNCH_CHECK();
     return EFL_OK;
 }
