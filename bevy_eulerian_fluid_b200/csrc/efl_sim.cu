@@ -2852,6 +2852,8 @@ bool unet_kernel_attrs() {
                cudaSuccess &&
            cudaFuncSetAttribute(k_conv3x3_rows<false, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, CV_SMEM) ==
                cudaSuccess &&
+           cudaFuncSetAttribute(k_conv3x3_rows<true, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, CV_SMEM) ==
+               cudaSuccess &&
            cudaFuncSetAttribute(k_conv3x3_rows<false, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, CV_SMEM) ==
                cudaSuccess &&
            conv_sm_count_init() &&

@@ -151,7 +151,11 @@ struct ConvArgs {
     int H, W, cin, cout;
     int* err;
     const unsigned char* gap = nullptr;  // [H*W]: 0 = a canvas gap pixel, whose outputs are written as zeros
+    int resident = -1;  // k_conv3x3_tc: all nine weight tiles resident (1), the ring of three (0), by the rule (-1)
 };
+// k_conv3x3_tc's weights: resident for a grid of one round (its latency, not the occupancy, counts), else by the
+// occupancy rule.
+inline bool conv_tc_resident(const ConvArgs& a) { return a.resident >= 0 ? a.resident != 0 : conv_weights_resident(a.cin, a.cout); }
 
 // 16-byte asynchronous copy global -> shared through L1 (the nine taps of a
 // pixel tile re-read overlapping rows); zero-fills when !full.
@@ -189,7 +193,7 @@ EFL_DEV void conv_load_tap(const ConvArgs& a, int tap, int m, int py, int px, bo
 __global__ void __launch_bounds__(CV_THREADS) k_conv3x3_tc(ConvArgs a) {
     extern __shared__ __align__(128) unsigned char cv_smem[];
     const int abytes = conv_a_bytes(a.cin), bbytes = conv_b_bytes(a.cin, a.cout);
-    const bool resident = conv_weights_resident(a.cin, a.cout);
+    const bool resident = a.resident >= 0 ? a.resident != 0 : conv_weights_resident(a.cin, a.cout);
     unsigned char* Ab = cv_smem;
     unsigned char* Bb = Ab + CV_STAGES * abytes;
     uint64_t* bar = reinterpret_cast<uint64_t*>(Bb + (resident ? 9 : 3) * bbytes);  // [CV_STAGES]: MMAs done
@@ -1508,20 +1512,39 @@ inline bool conv_sm_count_init() {
 // (each CTA allocates tensor memory, which throttles how fast CTAs start on an
 // SM, so the grids that need several rounds per SM want few, fat CTAs and as
 // many of them resident at once as possible).
+#ifndef EFL_CONV_RESIDENT_BYTES
+#define EFL_CONV_RESIDENT_BYTES 20000
+#endif
+// Nine weight tiles resident on the multi-round grids too while they take at most this many bytes (0: never):
+// the ring makes thread 0 wait for five refills in turn, each behind an MMA commit, and small layers' tiles cost
+// little shared memory (512^2 forward: 0.255 ms with the ring everywhere, 0.244 ms with up to 20 KB resident,
+// 0.254 ms with up to 60 KB).
+inline bool crow_resident_small(int cin, int cout) { return 9 * conv_b_bytes(cin, cout) <= EFL_CONV_RESIDENT_BYTES; }
 inline void conv3x3_launch(const ConvArgs& a, cudaStream_t st) {
     const int ntiles = a.H * a.W / 128;
     if (a.W % 128 == 0) {
+        const bool pair = a.W % 256 == 0;
         if (ntiles <= conv_sm_count() && crow_smem_bytes(a.cin, a.cout, true, 1) <= CV_SMEM)
             k_conv3x3_rows<true, 1>
                 <<<ntiles, CV_THREADS, crow_smem_bytes(a.cin, a.cout, true, 1) + count_launch(), st>>>(a);
-        else if (a.W % 256 == 0 && crow_smem_bytes(a.cin, a.cout, false, 2) <= CR_PAIR_SMEM)
+        else if (pair && crow_resident_small(a.cin, a.cout) && crow_smem_bytes(a.cin, a.cout, false, 2) <= CR_PAIR_SMEM)
+            k_conv3x3_rows<true, 2>
+                <<<ntiles / 2, 2 * CV_THREADS, crow_smem_bytes(a.cin, a.cout, true, 2) + count_launch(), st>>>(a);
+        else if (pair && crow_smem_bytes(a.cin, a.cout, false, 2) <= CR_PAIR_SMEM)
             k_conv3x3_rows<false, 2>
                 <<<ntiles / 2, 2 * CV_THREADS, crow_smem_bytes(a.cin, a.cout, false, 2) + count_launch(), st>>>(a);
+        else if (crow_resident_small(a.cin, a.cout))
+            k_conv3x3_rows<true, 1>
+                <<<ntiles, CV_THREADS, crow_smem_bytes(a.cin, a.cout, true, 1) + count_launch(), st>>>(a);
         else
             k_conv3x3_rows<false, 1>
                 <<<ntiles, CV_THREADS, crow_smem_bytes(a.cin, a.cout, false, 1) + count_launch(), st>>>(a);
     } else {
-        k_conv3x3_tc<<<(a.H * a.W + 127) / 128, CV_THREADS, conv_smem_bytes(a.cin, a.cout) + count_launch(), st>>>(a);
+        ConvArgs b = a;
+        const int ctas = (a.H * a.W + 127) / 128;
+        if (b.resident < 0 && ctas <= conv_sm_count() && conv_smem_with(a.cin, a.cout, 9) <= CV_SMEM) b.resident = 1;
+        const int smem = conv_smem_with(b.cin, b.cout, conv_tc_resident(b) ? 9 : 3);
+        k_conv3x3_tc<<<ctas, CV_THREADS, smem + count_launch(), st>>>(b);
     }
 }
 
