@@ -188,3 +188,39 @@ def test_prediction_judged_against_fp64_solve(gpu_api):
     assert pe["relative_error_start"] < pe["relative_error_previous"], pe
     assert pe["captured_block_means"] > 0.5, pe
     net.close()
+
+
+def test_canvas_forward_equals_per_image_forwards():
+    """The batch's canvas (efl_canvas_pack's layout, 8-pixel gaps): a forward over the canvas whose convolutions
+    write zeros at the gap pixels (all but the head) gives, inside each rectangle, each image's own forward --
+    here with the CPU restatement, so the gap rule itself is checked (the GPU test compares the batched
+    simulations with their own steps)."""
+    rng = np.random.default_rng(12)
+    params, _, _, _ = _random_case(2, n=16)
+    sizes = [(16, 16), (32, 16), (16, 32), (48, 32), (24, 8)]  # (w, h), multiples of 8
+    org, W, H = capi.canvas_pack(capi.load(), sizes)
+    masks = []
+    for lvl in range(4):
+        m = np.zeros((H >> lvl, W >> lvl), bool)
+        for (x, y), (w, h) in zip(org, sizes):
+            m[y >> lvl:(y + h) >> lvl, x >> lvl:(x + w) >> lvl] = True
+        masks.append(m)
+
+    class CanvasNet(unet_ref.Net):
+        def _c(self, i, x):
+            y = super()._c(i, x)
+            if i == len(unet_ref.SPEC) - 1:
+                return y
+            lvl = int(round(np.log2(H / y.shape[0])))
+            return y * masks[lvl][:, :, None]
+
+    feats = np.zeros((H, W, 16), np.float32)
+    single = []
+    for (x, y), (w, h) in zip(org, sizes):
+        f = np.zeros((h, w, 16), np.float32)
+        f[:, :, :5] = rng.normal(0, 1, (h, w, 5))
+        feats[y:y + h, x:x + w] = f
+        single.append(unet_ref.Net(params).forward(f))
+    out = CanvasNet(params).forward(feats)
+    for (x, y), (w, h), ref in zip(org, sizes, single):
+        np.testing.assert_allclose(out[y:y + h, x:x + w], ref, rtol=1e-6, atol=1e-9)
