@@ -995,9 +995,10 @@ UnetFeatureArgs unet_feature_args(const efl_sim* s) {
 }
 
 // The warm start in two halves around the network's forward pass: the features (into x0, row pitch cs coarse
-// pixels: a batch's canvas; the workspace's own input when x0 is null), then the guard that keeps the
-// prediction only where it lowers the block-summed residual, and the prediction added to the iterate.
-efl_status unet_features(efl_sim* s, bf16* x0 = nullptr, int cs = 0) {
+// pixels: a batch's canvas; the workspace's own input when x0 is null; with widen, the f32 pressure and
+// divergence widened into the solve's FP64 planes by the same kernel, in place of k_widen), then the guard that
+// keeps the prediction only where it lowers the block-summed residual, and the prediction added to the iterate.
+efl_status unet_features(efl_sim* s, bf16* x0 = nullptr, int cs = 0, bool widen = false) {
     UNet& n = s->unet_view ? *s->unet_view : s->unet->net;
     const int f = s->unet->net.coarse;
     if (n.coarse != f)
@@ -1005,8 +1006,8 @@ efl_status unet_features(efl_sim* s, bf16* x0 = nullptr, int cs = 0) {
     const dim3 g = grid2d(s->nx, s->ny, kBlock);
     const UnetFeatureArgs a = unet_feature_args(s);
     k_unet_residual<<<g, kBlock, count_launch(), s->stream>>>(a, n.res32, n.prev32, n.mask, n.lpart,
-                                                              f > 1 ? n.epart : nullptr);
-    k_unet_sigma<<<1, UNET_RED_THREADS, count_launch(), s->stream>>>(n.lpart, (int)(g.x * g.y), n.sigma);
+                                                              f > 1 ? n.epart : nullptr, widen ? s->p0 : PF{},
+                                                              widen ? s->div : PF{}, n.red_count, n.sigma);
     if (f > 1) {
         k_unet_features_coarse<<<g, kBlock, count_launch(), s->stream>>>(n.res32, a, n.mask, n.sigma, f,
                                                                          x0 ? x0 : n.X0, x0 ? cs : s->nx / f, n.maskc);
@@ -1044,8 +1045,8 @@ efl_status unet_apply(efl_sim* s) {
     LAUNCH_CHECK();
     return EFL_OK;
 }
-efl_status unet_before_solve(efl_sim* s) {
-    TRY(unet_features(s));
+efl_status unet_before_solve(efl_sim* s, bool widen = false) {
+    TRY(unet_features(s, nullptr, 0, widen));
     if (s->unet_flags & EFL_UNET_WARM_START) {
         UNet& n = s->unet_view ? *s->unet_view : s->unet->net;
         unet_forward(n, s->ny / n.coarse, s->nx / n.coarse, s->stream);
@@ -1100,13 +1101,14 @@ efl_status st_projection(efl_sim* s, efl_step_stats* st) {
     } else {
         const Level64& L = s->mg64[0];
         dim3 g = grid2d(d.nx, d.ny, kBlock);
-        k_widen<<<g, kBlock, count_launch(), s->stream>>>(s->p0, s->div, L.x, L.b);
-        LAUNCH_CHECK();
         if (s->unet && s->unet_flags) {
             if ((s->unet_flags & EFL_UNET_RECORD) && s->unet_view)
                 return set_err(s, EFL_ERR_STATE, "a batch member's network workspace is forward-only: record "
                                                  "training samples on a simulation of its own");
-            TRY(unet_before_solve(s));
+            TRY(unet_before_solve(s, true));  // its residual kernel widens p and b
+        } else {
+            k_widen<<<g, kBlock, count_launch(), s->stream>>>(s->p0, s->div, L.x, L.b);
+            LAUNCH_CHECK();
         }
         double r = -1.0;
         bool done = false;
@@ -2727,12 +2729,12 @@ efl_status efl_batch_step(efl_batch* b, float dt, efl_step_stats* stats) {
         efl_status st = run_segment(b->gc, b->stream, sig_pre | 1, SEG_PRE, [&]() -> efl_status {
             TRY(batch_fanout(b, [&](size_t i, efl_sim* s) -> efl_status {
                 TRY(run_stages(s, EFL_STAGE_UPDATE_SOLID, EFL_STAGE_DIVERGENCE, nullptr));
+                if (on_canvas(s))  // its residual kernel widens p and b
+                    return unet_features(s, b->canvas->X0 + ((size_t)b->corigin[i].y * b->cw + b->corigin[i].x) * 16,
+                                         b->cw, true);
+                if (s->unet && (s->unet_flags & EFL_UNET_WARM_START)) return unet_before_solve(s, true);
                 const Level64& L = s->mg64[0];
                 k_widen<<<grid2d(s->nx, s->ny, kBlock), kBlock, count_launch(), s->stream>>>(s->p0, s->div, L.x, L.b);
-                if (on_canvas(s))
-                    return unet_features(s, b->canvas->X0 + ((size_t)b->corigin[i].y * b->cw + b->corigin[i].x) * 16,
-                                         b->cw);
-                if (s->unet && (s->unet_flags & EFL_UNET_WARM_START)) TRY(unet_before_solve(s));
                 return EFL_OK;
             }));
             if (on.empty()) return EFL_OK;
@@ -2795,10 +2797,11 @@ efl_status efl_batch_step(efl_batch* b, float dt, efl_step_stats* stats) {
                                P.check_interval == Q.check_interval;
         if (batchable) {
             const Level64& L = s->mg64[0];
-            k_widen<<<grid2d(s->nx, s->ny, kBlock), kBlock, count_launch(), s->stream>>>(s->p0, s->div, L.x, L.b);
             if (s->unet && (s->unet_flags & EFL_UNET_WARM_START)) {
-                efl_status st = unet_before_solve(s);
+                efl_status st = unet_before_solve(s, true);  // its residual kernel widens p and b
                 if (st != EFL_OK) return fail(s, st);
+            } else {
+                k_widen<<<grid2d(s->nx, s->ny, kBlock), kBlock, count_launch(), s->stream>>>(s->p0, s->div, L.x, L.b);
             }
             solve_batched.push_back((int)i);
         } else {

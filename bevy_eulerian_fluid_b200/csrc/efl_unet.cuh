@@ -781,6 +781,36 @@ struct UnetFeatureArgs {
 // residual.wgsl:33-54 in factored form, as the mixed solve builds it), the
 // mask, prev32 = prev, and per-block partial sums (res^2, count).
 // (Block (bx, by) of a grid bgx blocks wide; a batch's launch covers several simulations' grids.)
+// The in-order sums of a block's reductions: thread t adds partials t, t + 256, ... in turn, then a fixed tree
+// over the 256 threads (blocks of 256 threads; the same order for a simulation alone and in a batch).
+constexpr int UNET_RED_THREADS = 256;
+EFL_DEV double2 block_sum2(double a, double b, int t) {
+    __shared__ double2 red[UNET_RED_THREADS];
+    red[t] = make_double2(a, b);
+    __syncthreads();
+#pragma unroll
+    for (int o = UNET_RED_THREADS / 2; o > 0; o >>= 1) {
+        if (t < o) red[t] = make_double2(red[t].x + red[t + o].x, red[t].y + red[t + o].y);
+        __syncthreads();
+    }
+    return red[0];
+}
+// sigma = RMS of the residual over the counted cells (1 if there are none); t = the linear thread index of a
+// block of UNET_RED_THREADS threads.  The partials are read through L2 (other blocks of the same launch may
+// have written them).
+EFL_DEV void unet_sigma_blk(const float2* part, int n, float* sigma, int t) {
+    double r2 = 0.0, c = 0.0;
+    for (int i = t; i < n; i += UNET_RED_THREADS) {
+        const float2 q = __ldcg(part + i);
+        r2 += q.x;
+        c += q.y;
+    }
+    const double2 s2 = block_sum2(r2, c, t);
+    if (t == 0) {
+        const double v = s2.y > 0.0 ? sqrt(s2.x / s2.y) : 0.0;
+        *sigma = v > 0.0 ? (float)v : 1.0f;
+    }
+}
 // The sum of the squares of the four 8 x 8 guard-block sums of v over a block of 32 x 8 threads (the 8 cells of a
 // row by shuffles, then the 8 rows in order), returned by thread 0; every thread of the block calls it.
 EFL_DEV double guard_block_squares(double v) {
@@ -798,14 +828,26 @@ EFL_DEV double guard_block_squares(double v) {
     return acc;
 }
 // With epart (the coarse warm start; blocks of 32 x 8 threads), also the guard's "before" half: the squared
-// 8 x 8 block sums of the start iterate's unscaled residual, into epart[block].x.
-EFL_DEV void unet_residual_blk(const UnetFeatureArgs& a, float* res, float* prev32, unsigned char* mask, float2* part,
-                               double2* epart, int bx, int by, int bgx) {
+// 8 x 8 block sums of the start iterate's unscaled residual, into epart[block].x.  With p32 / d32 (the f32
+// pressure and divergence), the cells are widened here into a.prev and a.b, the solve's FP64 start iterate and
+// right-hand side (neighbours read from the f32 planes: the same values).  With count (zero between launches),
+// the block that finishes last sums the partials into sigma (in the fixed order of unet_sigma_blk).
+__global__ void __launch_bounds__(256) k_unet_residual(UnetFeatureArgs a, float* res, float* prev32, unsigned char* mask,
+                                                        float2* part, double2* epart, PF p32, PF d32, unsigned* count,
+                                                        float* sigma) {
+    const int bx = blockIdx.x, by = blockIdx.y, bgx = gridDim.x;
+    const bool wide = p32.p != nullptr;
+    auto X = [&](int x, int y) -> double { return wide ? (double)p32.at(x, y) : a.prev.at(x, y); };
     const int gx = bx * blockDim.x + threadIdx.x, gy = by * blockDim.y + threadIdx.y;
     float r2 = 0.0f, c = 0.0f;
     double rd = 0.0;
     if (gx < a.nx && gy < a.ny) {
         const size_t p = (size_t)gy * a.nx + gx;
+        const double xc = X(gx, gy), bc = wide ? (double)d32.at(gx, gy) : a.b.at(gx, gy);
+        if (wide) {
+            a.prev.at(gx, gy) = xc;
+            a.b.at(gx, gy) = bc;
+        }
         const float phi = a.ls.at(gx, gy);
         const float f[4] = {a.fu.at(gx, gy), a.fu.at(gx + 1, gy), a.fv.at(gx, gy), a.fv.at(gx, gy + 1)};
         const bool counted = phi < 0.0f && !(f[0] == 0.0f && f[1] == 0.0f && f[2] == 0.0f && f[3] == 0.0f);
@@ -820,19 +862,19 @@ EFL_DEV void unet_residual_blk(const UnetFeatureArgs& a, float* res, float* prev
                     const float level = a.ls.at(jx, jy);
                     if (level < 0.0f) {
                         den += (double)f[q];
-                        sum += (double)f[q] * a.prev.at(jx, jy);
+                        sum += (double)f[q] * X(jx, jy);
                     } else {
                         den += (double)f[q] * (1.0 - (double)level / (double)phi);
                     }
                 }
             }
-            rd = a.b.at(gx, gy) - a.factor * (den * a.prev.at(gx, gy) - sum);
+            rd = bc - a.factor * (den * xc - sum);
             rv = (float)(a.cdiv * rd);
             r2 = rv * rv;
             c = 1.0f;
         }
         res[p] = rv;
-        prev32[p] = (float)a.prev.at(gx, gy);
+        prev32[p] = (float)xc;
         mask[p] = counted ? 1 : 0;
     }
     r2 = warp_sum_f(r2);
@@ -853,42 +895,22 @@ EFL_DEV void unet_residual_blk(const UnetFeatureArgs& a, float* res, float* prev
         const double sq = guard_block_squares(rd);
         if (t == 0) epart[by * bgx + bx].x = sq;
     }
-}
-__global__ void __launch_bounds__(256) k_unet_residual(UnetFeatureArgs a, float* res, float* prev32, unsigned char* mask,
-                                                        float2* part, double2* epart) {
-    unet_residual_blk(a, res, prev32, mask, part, epart, blockIdx.x, blockIdx.y, gridDim.x);
-}
-// The in-order sums of a block's reductions: thread t adds partials t, t + 256, ... in turn, then a fixed tree
-// over the 256 threads (blocks of 256 threads; the same order for a simulation alone and in a batch).
-constexpr int UNET_RED_THREADS = 256;
-EFL_DEV double2 block_sum2(double a, double b) {
-    __shared__ double2 red[UNET_RED_THREADS];
-    const int t = threadIdx.x;
-    red[t] = make_double2(a, b);
-    __syncthreads();
-#pragma unroll
-    for (int o = UNET_RED_THREADS / 2; o > 0; o >>= 1) {
-        if (t < o) red[t] = make_double2(red[t].x + red[t + o].x, red[t].y + red[t + o].y);
+    if (count) {
+        __shared__ unsigned s_last;
+        const unsigned nblk = gridDim.x * gridDim.y;
+        if (t == 0) {
+            __threadfence();  // this block's partial before its arrival
+            s_last = atomicAdd(count, 1u) == nblk - 1 ? 1u : 0u;
+        }
         __syncthreads();
-    }
-    return red[0];
-}
-// sigma = RMS of the residual over the counted cells (1 if there are none).
-EFL_DEV void unet_sigma_blk(const float2* part, int n, float* sigma) {
-    double r2 = 0.0, c = 0.0;
-    for (int i = threadIdx.x; i < n; i += UNET_RED_THREADS) {
-        r2 += part[i].x;
-        c += part[i].y;
-    }
-    const double2 s2 = block_sum2(r2, c);
-    if (threadIdx.x == 0) {
-        const double v = s2.y > 0.0 ? sqrt(s2.x / s2.y) : 0.0;
-        *sigma = v > 0.0 ? (float)v : 1.0f;
+        if (s_last) {
+            __threadfence();
+            unet_sigma_blk(part, (int)nblk, sigma, t);
+            if (t == 0) *count = 0u;  // for the next launch
+        }
     }
 }
-__global__ void __launch_bounds__(UNET_RED_THREADS) k_unet_sigma(const float2* part, int n, float* sigma) {
-    unet_sigma_blk(part, n, sigma);
-}
+
 __global__ void k_unet_features(const float* res, const UnetFeatureArgs a, const unsigned char* mask,
                                 const float* sigma, bf16* x0) {
     const int gx = blockIdx.x * blockDim.x + threadIdx.x, gy = blockIdx.y * blockDim.y + threadIdx.y;
@@ -999,7 +1021,7 @@ EFL_DEV void unet_guard_blk(const double2* part, int n, double* alpha) {
         before += part[i].x;
         after += part[i].y;
     }
-    const double2 s2 = block_sum2(before, after);
+    const double2 s2 = block_sum2(before, after, threadIdx.x);
     if (threadIdx.x == 0) *alpha = s2.y < s2.x ? 1.0 : 0.0;
 }
 __global__ void __launch_bounds__(UNET_RED_THREADS) k_unet_guard(const double2* part, int n, double* alpha) {
@@ -1337,6 +1359,7 @@ struct UNet {
     float* targetc;          // coarse training target and mask (coarse form)
     unsigned char* maskc;
     int* err;
+    unsigned* red_count;  // arrivals of k_unet_residual's blocks (its last block computes sigma); zero between launches
     void* arena = nullptr;
     std::vector<void*> extra;
     std::string last_error;
@@ -1412,6 +1435,7 @@ inline cudaError_t unet_alloc(UNet& n, int maxH, int maxW) {
         *it.ptr = base;
         base += it.bytes;
     }
+    n.red_count = reinterpret_cast<unsigned*>(n.err + 32);  // the second half of the zeroed 256-byte flag block
     return cudaSuccess;
 }
 
@@ -1471,6 +1495,7 @@ inline cudaError_t unet_alloc_forward(UNet& v, const UNet& net, int fh, int fw, 
         *it.ptr = base;
         base += it.bytes;
     }
+    v.red_count = reinterpret_cast<unsigned*>(v.err + 32);  // the second half of the zeroed 256-byte flag block
     // nothing of the training state belongs to a forward-only workspace
     v.grads = v.adam_m = v.adam_v = nullptr;
     v.target = v.targetc = nullptr;
