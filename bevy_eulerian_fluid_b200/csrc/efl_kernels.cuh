@@ -534,15 +534,9 @@ EFL_DEV void restrict_cell(const LevelT<T>& F, const LevelT<T>& C, int x, int y)
     int fx = 2 * x, fy = 2 * y;
     restrict_from(F, C, x, y, F.r.ld(fx, fy), F.r.ld(fx, fy + 1), F.r.ld(fx + 1, fy), F.r.ld(fx + 1, fy + 1));
 }
-template <class T>
-__global__ void k_restriction(LevelT<T> F, LevelT<T> C) {
-    int x = gx(), y = gy();
-    if (x >= C.nx || y >= C.ny) return;
-    restrict_cell(F, C, x, y);
-}
-// k_residual then k_restriction in one pass: each coarse cell computes its four children's residuals
-// (residual_at, 0 outside the level, as the residual plane reads there) and restricts them, so the fine
-// residual plane is neither written nor read back.  The same values, in the same order.
+// The residual (k_residual) and the restriction in one pass: each coarse cell computes its four children's
+// residuals (residual_at, 0 outside the level, as the residual plane reads there) and restricts them, so the
+// fine residual plane is neither written nor read back.  The same values, in the same order.
 template <class T>
 __global__ void k_residual_restrict(LevelT<T> F, LevelT<T> C, float dt, float rho, float dx_scaled) {
     int x = gx(), y = gy();
